@@ -1,0 +1,421 @@
+/*
+ * CPU ORACLE (test infrastructure only): the SF-CIS, ground CPS(D) and
+ * EE-CPS(D-3) drivers, restating
+ *   src/EE-CIS.SF/run.f90, src/EE-CIS.SF/calAR.f90,
+ *   src/CPSd.SF/run1.f90, src/CPSd.SF/run2.f90, src/CPSd.SF/calC1.f90, calC2.f90,
+ *   src/EE-CPSd.SF/run.f90, run_order.f90, calV_C.f90, calE_C.f90, calJ.f90,
+ *   calC1_VR2.f90, calC2_VR1.f90, calC2_VR2.f90, calC_JR.f90, calC_VTR.f90,
+ *   solver.f90, orthogonalR2L.f90.
+ * The reference's disk records (IO_stream files CIS_sym<n>, CPSd_T__,
+ * CPSd_sym<n>, CPSdC_sym<n>) are held in memory.
+ */
+#include "cpsd_oracle.h"
+#include "oracle_internal.h"
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+int o_system_init(o_system *s)
+{
+    int rc = o_set_symmetry(s->nirrep, s->dirprd);
+    if (rc != O_OK) return rc;
+    for (i64 r = 1; r <= 8; r++) {
+        if (r > s->nirrep) { s->popo[r - 1] = s->popv[r - 1] = 0; continue; }
+        i64 rb = o_dirprd(r, s->symry);
+        s->popo[r - 1] = s->popa[r - 1] + s->popb[rb - 1];
+        s->popv[r - 1] = s->vrta[r - 1] + s->vrtb[rb - 1];
+    }
+    return O_OK;
+}
+
+/* defaults of src/lib_cc/mod_common.f90:11-44 */
+void o_params_default(o_params *p)
+{
+    memset(p, 0, sizeof(*p));
+    p->davidson_dim = 20;
+    p->davidson_cyc = 50;
+    p->davidson_conv = 8;
+    p->lowest = 0;
+    p->diis_dim = 10;
+    p->diis_cyc = 50;
+    p->diis_max_err = 10.0e-8;
+    p->spin_flip = 1;
+    p->open_shell = 1;
+    p->ex_mult = 1;
+    p->nthreads = 1;
+}
+
+static const i64 Z[8] = {1, 0, 0, 0, 0, 0, 0, 0};
+
+/* integral tensor views (src/EE-CPSd.SF/allocate_mem.f90) */
+typedef struct {
+    o_opt ijkl, ijka, abij, iabj, abci, abcd;
+} ints_t;
+
+static void ints_view(const o_system *s, const o_integrals *I, ints_t *v)
+{
+    const i64 *o = s->popo, *V = s->popv;
+    o_opt_view(&v->ijkl, o, o, o, o, 0, 0, 1, (double *)I->ijkl);
+    o_opt_view(&v->ijka, o, o, o, V, 0, 1, 1, (double *)I->ijka);
+    o_opt_view(&v->abij, V, V, o, o, 0, 0, 1, (double *)I->abij);
+    o_opt_view(&v->iabj, V, o, V, o, 1, 1, 1, (double *)I->iabj);
+    o_opt_view(&v->abci, V, V, V, o, 0, 1, 1, (double *)I->abci);
+    o_opt_view(&v->abcd, V, V, V, V, 0, 0, 1, (double *)I->abcd);
+}
+
+static double *zalloc(i64 n) { return (double *)calloc((size_t)(n > 0 ? n : 1), sizeof(double)); }
+
+/* ---------------- SF-CIS ---------------- */
+typedef struct {
+    const o_system *s;
+    const ints_t *I;
+    const double *oed1;
+    i64 sym;
+} cis_ctx;
+
+/* calAR (src/EE-CIS.SF/calAR.f90:6-34): AR = e(a,i)*r(a,i) + V(fn,ai) r(fn) */
+static void cis_sigma(void *vctx, const double *R, double *AR)
+{
+    cis_ctx *c = (cis_ctx *)vctx;
+    o_opt r1, ar1;
+    o_opt_view(&r1, c->s->popv, c->s->popo, Z, Z, 1, 1, c->sym, (double *)R);
+    o_opt_view(&ar1, c->s->popv, c->s->popo, Z, Z, 1, 1, c->sym, AR);
+    for (i64 i = 0; i < r1.len; i++) AR[i] = c->oed1[i] * R[i];
+    o_c1_r1iabj(&ar1, &r1, &c->I->iabj, 1.0);
+}
+
+int o_cis_run(const o_system *s, const o_integrals *I, const o_params *p,
+              double *omega, double *R, i64 *iters)
+{
+    ints_t v;
+    ints_view(s, I, &v);
+    i64 kroot = 0, roff = 0, itsum = 0;
+    for (i64 sym = 1; sym <= s->nirrep; sym++) {
+        i64 nroot = p->estate_sym[sym - 1];
+        if (nroot == 0) continue;
+        i64 len = o_irpdso(sym, s->popv, s->popo, 1);
+        double *oed1 = zalloc(len);
+        o_eorb_diff1(oed1, I->eorb, s->popv, s->popo, sym);
+        double *file = zalloc((1 + len) * nroot);
+        int rc = o_guess(s, I->eorb, p, sym, nroot, file);
+        if (rc != O_OK) { free(oed1); free(file); return rc; }
+        cis_ctx ctx = {s, &v, oed1, sym};
+        i64 it = 0;
+        rc = o_davidson(file, oed1, len, nroot, 1, p, cis_sigma, &ctx, &it);
+        itsum += it;
+        for (i64 k = 0; k < nroot; k++) {
+            omega[kroot + k] = file[(1 + len) * k];
+            memcpy(R + roff + len * k, file + (1 + len) * k + 1, sizeof(double) * (size_t)len);
+        }
+        kroot += nroot;
+        roff += len * nroot;
+        free(oed1);
+        free(file);
+        if (rc != O_OK) return rc;
+    }
+    if (iters) *iters = itsum;
+    return O_OK;
+}
+
+/* ---------------- ground CPS(D) ---------------- */
+int o_cpsd_ground(const o_system *s, const o_integrals *I, const o_params *p,
+                  double *T2_1, double *T1_2, double *T2_2, double *E2, double *E3,
+                  i64 *diis_iters)
+{
+    ints_t v;
+    ints_view(s, I, &v);
+    const i64 *o = s->popo, *V = s->popv;
+    o_opt t1, t2, t2b, c1, c2, r1;
+    i64 l1 = o_irpdso(1, V, o, 1);
+    i64 l2 = o_idsymsoc(1, V, V, 0, o, o, 0);
+    double *c1a = zalloc(l1), *c2a = zalloc(l2), *r1a = zalloc(l1);
+    o_opt_view(&t1, V, o, Z, Z, 1, 1, 1, T1_2);
+    o_opt_view(&t2, V, V, o, o, 0, 0, 1, T2_1);
+    o_opt_view(&t2b, V, V, o, o, 0, 0, 1, T2_2);
+    o_opt_view(&c1, V, o, Z, Z, 1, 1, 1, c1a);
+    o_opt_view(&c2, V, V, o, o, 0, 0, 1, c2a);
+    o_opt_view(&r1, V, o, Z, Z, 1, 1, 1, r1a);
+    /* run1 (src/CPSd.SF/run1.f90:9-38): T1^(1)=0, T2^(1) = <ab||ij>/D */
+    o_denomT2(T2_1, I->abij, I->eorb, V, o, 1, 0);
+    *E2 = o_ddot(l2, T2_1, I->abij);
+    /* run2 (src/CPSd.SF/run2.f90:8-95) */
+    int rc = o_c1_r2abci(&c1, &t2, &v.abci, 1.0);           /* calC1 -> calC1_VR2 */
+    if (rc == O_OK) rc = o_c1_r2ijka(&c1, &t2, &v.ijka, 1.0);
+    if (rc == O_OK) rc = o_c2_r2Wmbej(&c2, &t2, &v.iabj, 1.0); /* calC2 -> calC2_VR2 */
+    if (rc == O_OK) rc = o_c2_r2Wmnij(&c2, &t2, &v.ijkl, 1.0);
+    if (rc == O_OK) rc = o_c2_r2abcd(&c2, &t2, &v.abcd, 1.0);
+    if (rc != O_OK) goto out;
+    o_denomT2(T2_2, c2a, I->eorb, V, o, 1, 0);
+    memcpy(r1a, c1a, sizeof(double) * (size_t)l1);
+    o_diis dst;
+    o_diis_init(&dst, l1, p->diis_dim);
+    i64 iter = 0;
+    for (;;) {
+        iter++;
+        o_denomT1(T1_2, r1a, I->eorb, V, o, 1);
+        double err = o_diis_step(&dst, iter, T1_2);
+        if (iter > 1 && fabs(err) < p->diis_max_err) break;
+        if (iter > p->diis_cyc) break;
+        memcpy(r1a, c1a, sizeof(double) * (size_t)l1);
+        rc = o_c1_r1iabj(&r1, &t1, &v.iabj, 1.0);
+        if (rc != O_OK) break;
+    }
+    o_diis_free(&dst);
+    if (diis_iters) *diis_iters = iter;
+    *E3 = o_ddot(l2, T2_2, I->abij);
+out:
+    free(c1a); free(c2a); free(r1a);
+    return rc;
+}
+
+/* ---------------- J^(2), J^(3) (src/EE-CPSd.SF/calJ.f90) ---------------- */
+int o_calJ(const o_system *s, const o_integrals *I, const double *T2_1,
+           const double *T1_2, const double *T2_2, o_jints *J)
+{
+    ints_t v;
+    ints_view(s, I, &v);
+    const i64 *o = s->popo, *V = s->popv;
+    o_opt t2a, t1b, t2b, foo, fvv, wvo, woo, foo3, fvv3, wvo3;
+    o_opt_view(&t2a, V, V, o, o, 0, 0, 1, (double *)T2_1);
+    o_opt_view(&t1b, V, o, Z, Z, 1, 1, 1, (double *)T1_2);
+    o_opt_view(&t2b, V, V, o, o, 0, 0, 1, (double *)T2_2);
+    o_opt_view(&foo, o, o, Z, Z, 1, 1, 1, J->J2_Foo);
+    o_opt_view(&fvv, V, V, Z, Z, 1, 1, 1, J->J2_Fvv);
+    o_opt_view(&wvo, V, o, V, o, 1, 1, 1, J->J2_Wovvo);
+    o_opt_view(&woo, o, o, o, V, 0, 1, 1, J->J2_Wovoo);
+    o_opt_view(&foo3, o, o, Z, Z, 1, 1, 1, J->J3_Foo);
+    o_opt_view(&fvv3, V, V, Z, Z, 1, 1, 1, J->J3_Fvv);
+    o_opt_view(&wvo3, V, o, V, o, 1, 1, 1, J->J3_Wovvo);
+    memset(foo.arr, 0, sizeof(double) * (size_t)foo.len);
+    memset(fvv.arr, 0, sizeof(double) * (size_t)fvv.len);
+    memset(wvo.arr, 0, sizeof(double) * (size_t)wvo.len);
+    memset(woo.arr, 0, sizeof(double) * (size_t)woo.len);
+    memset(foo3.arr, 0, sizeof(double) * (size_t)foo3.len);
+    memset(fvv3.arr, 0, sizeof(double) * (size_t)fvv3.len);
+    memset(wvo3.arr, 0, sizeof(double) * (size_t)wvo3.len);
+    int rc = O_OK;
+    /* calJ2 (calJ.f90:6-99) */
+    if (rc == O_OK) rc = o_Fmi_r2abij(&foo, &t2a, &v.abij, 1.0);
+    if (rc == O_OK) rc = o_Fae_r2abij(&fvv, &t2a, &v.abij, 1.0);
+    if (rc == O_OK) rc = o_Wkbij_r2ijka(&woo, &t2a, &v.ijka, 1.0);
+    if (rc == O_OK) rc = o_Wkbij_r2abci(&woo, &t2a, &v.abci, 1.0);
+    if (rc == O_OK) rc = o_Wmbej_r2abij(&wvo, &t2a, &v.abij, 2.0);
+    /* calJ3 (calJ.f90:104-228) */
+    if (rc == O_OK) rc = o_Fmi_r1ijka(&foo3, &t1b, &v.ijka, 1.0);
+    if (rc == O_OK) rc = o_Fmi_r2abij(&foo3, &t2b, &v.abij, 1.0);
+    if (rc == O_OK) rc = o_Fae_r1abci(&fvv3, &t1b, &v.abci, 1.0);
+    if (rc == O_OK) rc = o_Fae_r2abij(&fvv3, &t2b, &v.abij, 1.0);
+    if (rc == O_OK) rc = o_Wmbej_r1ijka(&wvo3, &t1b, &v.ijka, 1.0);
+    if (rc == O_OK) rc = o_Wmbej_r1abci(&wvo3, &t1b, &v.abci, 1.0);
+    if (rc == O_OK) rc = o_Wmbej_r2abij(&wvo3, &t2b, &v.abij, 2.0);
+    return rc;
+}
+
+/* orthogonalR2L (src/EE-CPSd.SF/orthogonalR2L.f90:5-34): note the division
+ * by ||L|| (not ||L||^2), as in the reference */
+static void orth_r2l(double *R, const double *L, i64 n)
+{
+    double nrm = o_dnrm2(n, L);
+    double dot = o_ddot(n, L, R);
+    o_daxpy(n, -dot / nrm, L, R);
+}
+
+/* ---------------- one EE-CPS(D-3) root ---------------- */
+int o_eecpsd_root(const o_system *s, const o_integrals *I, const o_params *p,
+                  const double *T2_1, const o_jints *J, i64 symR, double w0,
+                  const double *L, double *w, double *R2_1_out, double *R1_2_out,
+                  double *R2_2_out, i64 *solver_iters)
+{
+    ints_t v;
+    ints_view(s, I, &v);
+    const i64 *o = s->popo, *V = s->popv;
+    i64 l1 = o_irpdso(symR, V, o, 1);
+    i64 l2 = o_idsymsoc(symR, V, V, 0, o, o, 0);
+    double *R0_1 = zalloc(l1);
+    double *Rn_1[3], *Rn_2[3], *Cn_1 = zalloc(l1), *Cn_2 = zalloc(l2);
+    double *C1a = zalloc(l1), *C2a = zalloc(l2), *tmpa;
+    for (int k = 0; k < 3; k++) { Rn_1[k] = zalloc(l1); Rn_2[k] = zalloc(l2); }
+    double *oed2 = zalloc(l2);
+    o_eorb_diff2(oed2, I->eorb, V, o, symR, 0);
+    memcpy(Rn_1[0], L, sizeof(double) * (size_t)l1);
+    double wk[4] = {0, 0, 0, 0}; /* w^(1..3) at [1..3] */
+    o_opt C1, C2, pR1, pR2, T2, jfoo, jfvv, jwvo, jwoo, j3foo, j3fvv, j3wvo;
+    o_opt_view(&C1, V, o, Z, Z, 1, 1, symR, C1a);
+    o_opt_view(&C2, V, V, o, o, 0, 0, symR, C2a);
+    o_opt_view(&T2, V, V, o, o, 0, 0, 1, (double *)T2_1);
+    o_opt_view(&jfoo, o, o, Z, Z, 1, 1, 1, J->J2_Foo);
+    o_opt_view(&jfvv, V, V, Z, Z, 1, 1, 1, J->J2_Fvv);
+    o_opt_view(&jwvo, V, o, V, o, 1, 1, 1, J->J2_Wovvo);
+    o_opt_view(&jwoo, o, o, o, V, 0, 1, 1, J->J2_Wovoo);
+    o_opt_view(&j3foo, o, o, Z, Z, 1, 1, 1, J->J3_Foo);
+    o_opt_view(&j3fvv, V, V, Z, Z, 1, 1, 1, J->J3_Fvv);
+    o_opt_view(&j3wvo, V, o, V, o, 1, 1, 1, J->J3_Wovvo);
+    int rc = O_OK;
+    i64 sit = 0;
+    for (i64 order = 1; order <= 3 && rc == O_OK; order++) {
+        if (order != 1) {
+            /* calV_C (calV_C.f90): Ctilde^(n-1) = sum_k w^(k) R^(n-1-k) - C^(n-1) */
+            i64 m = order - 1;
+            for (i64 i = 0; i < l1; i++) C1a[i] = -Cn_1[i];
+            for (i64 i = 0; i < l2; i++) C2a[i] = -Cn_2[i];
+            for (i64 k = 2; k <= m; k++) {
+                o_daxpy(l1, wk[k], Rn_1[m - k], C1a);
+                o_daxpy(l2, wk[k], Rn_2[m - k], C2a);
+            }
+            /* R2 = C2/(e2 - w0) (run_order.f90:54-58) */
+            double *R1 = Rn_1[m], *R2 = Rn_2[m];
+            for (i64 i = 0; i < l2; i++) R2[i] = C2a[i] / (oed2[i] - w0);
+            if (order != 2) {
+                /* solver (solver.f90:4-66) */
+                double *pR = zalloc(l1);
+                o_opt oR1, opR;
+                o_opt_view(&oR1, V, o, Z, Z, 1, 1, symR, R1);
+                o_opt_view(&opR, V, o, Z, Z, 1, 1, symR, pR);
+                for (i64 i = 0; i < l1; i++) C1a[i] = -C1a[i];
+                memcpy(pR, C1a, sizeof(double) * (size_t)l1);
+                o_diis dst;
+                o_diis_init(&dst, l1, p->diis_dim);
+                i64 iter = 0;
+                for (;;) {
+                    iter++;
+                    o_denomT1(R1, pR, I->eorb, V, o, symR);
+                    orth_r2l(R1, L, l1);
+                    double err = o_diis_step(&dst, iter, R1);
+                    orth_r2l(R1, L, l1);
+                    if (iter > 1 && fabs(err) < p->diis_max_err) break;
+                    if (iter > p->diis_cyc) break;
+                    memcpy(pR, C1a, sizeof(double) * (size_t)l1);
+                    o_daxpy(l1, -w0, R1, pR);
+                    rc = o_c1_r1iabj(&opR, &oR1, &v.iabj, 1.0);
+                    if (rc != O_OK) break;
+                }
+                sit += iter;
+                o_diis_free(&dst);
+                free(pR);
+            } else {
+                memset(R1, 0, sizeof(double) * (size_t)l1);
+            }
+        }
+        if (rc != O_OK) break;
+        /* calE_C (calE_C.f90:3-83): C^(n) = sum_k J^(k) R^(n-k) */
+        memset(C1a, 0, sizeof(double) * (size_t)l1);
+        memset(C2a, 0, sizeof(double) * (size_t)l2);
+        o_opt_view(&pR1, V, o, Z, Z, 1, 1, symR, Rn_1[order - 1]);
+        o_opt_view(&pR2, V, V, o, o, 0, 0, symR, Rn_2[order - 1]);
+        if (order != 1) rc = o_c1_r2abci(&C1, &pR2, &v.abci, 1.0);   /* calC1_VR2 */
+        if (rc == O_OK && order != 1) rc = o_c1_r2ijka(&C1, &pR2, &v.ijka, 1.0);
+        if (rc == O_OK && order != 3) {
+            if (order != 2) { /* calC2_VR1 */
+                rc = o_c2_r1ijka(&C2, &pR1, &v.ijka, 1.0);
+                if (rc == O_OK) rc = o_c2_r1abci(&C2, &pR1, &v.abci, 1.0);
+            }
+            if (rc == O_OK && order != 1) { /* calC2_VR2 */
+                rc = o_c2_r2Wmbej(&C2, &pR2, &v.iabj, 1.0);
+                if (rc == O_OK) rc = o_c2_r2Wmnij(&C2, &pR2, &v.ijkl, 1.0);
+                if (rc == O_OK) rc = o_c2_r2abcd(&C2, &pR2, &v.abcd, 1.0);
+            }
+        }
+        if (rc == O_OK && order == 2) {
+            /* calC_J2R (calC_JR.f90:4-52) with R^(0) */
+            o_opt_view(&pR1, V, o, Z, Z, 1, 1, symR, Rn_1[0]);
+            rc = o_c2_r1ijka(&C2, &pR1, &jwoo, 1.0);
+            if (rc == O_OK) rc = o_c1_r1iabj(&C1, &pR1, &jwvo, 1.0);
+            if (rc == O_OK) rc = o_c1_r1Fmi(&C1, &pR1, &jfoo, 1.0);
+            if (rc == O_OK) rc = o_c1_r1Fae(&C1, &pR1, &jfvv, 1.0);
+            /* calC_VTR (calC_VTR.f90:6-111) with T^(1) = (0, T2^(1)) */
+            o_opt tmp;
+            if (rc == O_OK) {
+                tmpa = zalloc(o_idsymsoc(symR, o, o, 0, o, o, 0));
+                o_opt_view(&tmp, o, o, o, o, 0, 0, symR, tmpa);
+                rc = o_Wmnij_r1ijka(&tmp, &pR1, &v.ijka, 1.0);
+                if (rc == O_OK) rc = o_c2_r2Wmnij(&C2, &T2, &tmp, 1.0);
+                free(tmpa);
+            }
+            if (rc == O_OK) {
+                tmpa = zalloc(o_idsymsoc(symR, V, o, 1, V, o, 1));
+                o_opt_view(&tmp, V, o, V, o, 1, 1, symR, tmpa);
+                rc = o_Wmbej_r1abci(&tmp, &pR1, &v.abci, 1.0);
+                if (rc == O_OK) rc = o_c2_r2Wmbej(&C2, &T2, &tmp, 1.0);
+                free(tmpa);
+            }
+            if (rc == O_OK) {
+                tmpa = zalloc(o_irpdso(symR, o, o, 1));
+                o_opt_view(&tmp, o, o, Z, Z, 1, 1, symR, tmpa);
+                rc = o_Fmi_r1ijka(&tmp, &pR1, &v.ijka, 1.0);
+                if (rc == O_OK) rc = o_c2_r2Fmi(&C2, &T2, &tmp, 1.0);
+                free(tmpa);
+            }
+            if (rc == O_OK) {
+                tmpa = zalloc(o_irpdso(symR, V, V, 1));
+                o_opt_view(&tmp, V, V, Z, Z, 1, 1, symR, tmpa);
+                rc = o_Fae_r1abci(&tmp, &pR1, &v.abci, 1.0);
+                if (rc == O_OK) rc = o_c2_r2Fae(&C2, &T2, &tmp, 1.0);
+                free(tmpa);
+            }
+        }
+        if (rc == O_OK && order == 3) {
+            /* calC_J3R (calC_JR.f90:56-106) with R^(0) */
+            o_opt_view(&pR1, V, o, Z, Z, 1, 1, symR, Rn_1[0]);
+            rc = o_c1_r1iabj(&C1, &pR1, &j3wvo, 1.0);
+            if (rc == O_OK) rc = o_c1_r1Fmi(&C1, &pR1, &j3foo, 1.0);
+            if (rc == O_OK) rc = o_c1_r1Fae(&C1, &pR1, &j3fvv, 1.0);
+        }
+        if (rc != O_OK) break;
+        wk[order] = o_ddot(l1, L, C1a);
+        memcpy(Cn_1, C1a, sizeof(double) * (size_t)l1);
+        memcpy(Cn_2, C2a, sizeof(double) * (size_t)l2);
+    }
+    w[0] = wk[1]; w[1] = wk[2]; w[2] = wk[3];
+    if (R2_1_out) memcpy(R2_1_out, Rn_2[1], sizeof(double) * (size_t)l2);
+    if (R1_2_out) memcpy(R1_2_out, Rn_1[2], sizeof(double) * (size_t)l1);
+    if (R2_2_out) memcpy(R2_2_out, Rn_2[2], sizeof(double) * (size_t)l2);
+    if (solver_iters) *solver_iters = sit;
+    for (int k = 0; k < 3; k++) { free(Rn_1[k]); free(Rn_2[k]); }
+    free(R0_1); free(Cn_1); free(Cn_2); free(C1a); free(C2a); free(oed2);
+    return rc;
+}
+
+/* ---------------- the whole pipeline (one "step" of the metric) --------- */
+int o_sfcpsd_pipeline(const o_system *s, const o_integrals *I, const o_params *p,
+                      double *omega_cis, double *w2, double *w3, i64 *nroots_out)
+{
+    const i64 *o = s->popo, *V = s->popv;
+    i64 nroot = 0, rlen = 0;
+    for (i64 sym = 1; sym <= s->nirrep; sym++) {
+        nroot += p->estate_sym[sym - 1];
+        rlen += p->estate_sym[sym - 1] * o_irpdso(sym, V, o, 1);
+    }
+    double *R = zalloc(rlen);
+    int rc = o_cis_run(s, I, p, omega_cis, R, NULL);
+    i64 l1 = o_irpdso(1, V, o, 1), l2 = o_idsymsoc(1, V, V, 0, o, o, 0);
+    double *T2_1 = zalloc(l2), *T1_2 = zalloc(l1), *T2_2 = zalloc(l2);
+    double E2, E3;
+    if (rc == O_OK) rc = o_cpsd_ground(s, I, p, T2_1, T1_2, T2_2, &E2, &E3, NULL);
+    o_jints J;
+    J.J2_Foo = zalloc(o_irpdso(1, o, o, 1));
+    J.J2_Fvv = zalloc(o_irpdso(1, V, V, 1));
+    J.J2_Wovvo = zalloc(o_idsymsoc(1, V, o, 1, V, o, 1));
+    J.J2_Wovoo = zalloc(o_idsymsoc(1, o, o, 0, o, V, 1));
+    J.J3_Foo = zalloc(o_irpdso(1, o, o, 1));
+    J.J3_Fvv = zalloc(o_irpdso(1, V, V, 1));
+    J.J3_Wovvo = zalloc(o_idsymsoc(1, V, o, 1, V, o, 1));
+    if (rc == O_OK) rc = o_calJ(s, I, T2_1, T1_2, T2_2, &J);
+    i64 k = 0, roff = 0;
+    for (i64 sym = 1; sym <= s->nirrep && rc == O_OK; sym++) {
+        i64 len = o_irpdso(sym, V, o, 1);
+        for (i64 r = 0; r < p->estate_sym[sym - 1] && rc == O_OK; r++) {
+            double w[3];
+            rc = o_eecpsd_root(s, I, p, T2_1, &J, sym, omega_cis[k], R + roff + r * len, w,
+                               NULL, NULL, NULL, NULL);
+            w2[k] = w[1];
+            w3[k] = w[2];
+            k++;
+        }
+        roff += len * p->estate_sym[sym - 1];
+    }
+    if (nroots_out) *nroots_out = nroot;
+    free(R); free(T2_1); free(T1_2); free(T2_2);
+    free(J.J2_Foo); free(J.J2_Fvv); free(J.J2_Wovvo); free(J.J2_Wovoo);
+    free(J.J3_Foo); free(J.J3_Fvv); free(J.J3_Wovvo);
+    return rc;
+}

@@ -1,0 +1,161 @@
+"""Seeded synthetic SF-CIS / SF-CPS(D) inputs.
+
+The reference builds its integrals with PySCF (src/pyscf2cc/py2cc.py:10) and
+xgetHF (src/getHF/main.f90:3); neither is available, so this module draws a
+synthetic high-spin open-shell reference:
+
+* nmo spatial orbitals, irreps assigned round-robin (MO k -> irrep k % nirrep + 1);
+  alpha-occupied for k < nocc_a, beta-occupied for k < nocc_b;
+* orbital energies occ ~ U[-1.5, -0.3] Eh and vir ~ U[0.1, 3.0] Eh, sorted,
+  drawn independently for alpha and beta (canonical, diagonal Fock);
+* (pq|rs) = sum_P L_pq^P L_rs^P, L ~ N(0, 0.05^2), naux = 4 nmo, symmetric in
+  pq; aux function P carries irrep P % nirrep + 1 and L_pq^P = 0 unless
+  irrep(p) x irrep(q) = irrep(P), so (pq|rs) vanishes wherever the irrep
+  product is not A1 and every symmetry-allowed block is populated;
+* Gamma(R_y) = A1, so a spin-free irrep equals the spatial irrep.
+
+The antisymmetrised spin-free DPD tensors are assembled by the C routine in
+csrc/synth.c.  Draw order (fixed): eps_a occ, eps_a vir, eps_b occ, eps_b vir, L.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from .dpd import Symmetry, ZORB, xor_dirprd
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_SYNTH_SO = os.path.join(_HERE, "_build", "libcpsd_synth.so")
+_lib = None
+
+
+def _load():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_SYNTH_SO):
+            raise RuntimeError(f"synthetic front end not built: {_SYNTH_SO} (run __graft_entry__.build())")
+        _lib = ctypes.CDLL(_SYNTH_SO)
+        _lib.cpsd_synth_build.restype = ctypes.c_int
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+class System:
+    """Orbital spaces, symmetry and integrals of one synthetic molecule."""
+
+    def __init__(self, nmo, nocc_a, nocc_b, nirrep, seed=0, naux=None, roots=None,
+                 spin_flip=1, skip_abcd=False):
+        self.nmo, self.nocc_a, self.nocc_b, self.nirrep = int(nmo), int(nocc_a), int(nocc_b), int(nirrep)
+        self.seed = int(seed)
+        self.naux = int(naux) if naux is not None else 4 * self.nmo
+        self.dirprd = xor_dirprd(self.nirrep)
+        self.sym = Symmetry(self.nirrep, self.dirprd)
+        self.symry = 1
+        self.spin_flip = int(spin_flip)
+        mo_irrep = np.array([k % self.nirrep + 1 for k in range(self.nmo)], dtype=np.int64)
+        self.mo_irrep = mo_irrep
+        self.popa = np.zeros(8, np.int64)
+        self.popb = np.zeros(8, np.int64)
+        self.vrta = np.zeros(8, np.int64)
+        self.vrtb = np.zeros(8, np.int64)
+        for k in range(self.nmo):
+            h = mo_irrep[k] - 1
+            if k < self.nocc_a:
+                self.popa[h] += 1
+            else:
+                self.vrta[h] += 1
+            if k < self.nocc_b:
+                self.popb[h] += 1
+            else:
+                self.vrtb[h] += 1
+        self.popo = self.popa + self.popb
+        self.popv = self.vrta + self.vrtb
+        rng = np.random.default_rng(self.seed)
+        ea = np.concatenate([np.sort(rng.uniform(-1.5, -0.3, self.nocc_a)),
+                             np.sort(rng.uniform(0.1, 3.0, self.nmo - self.nocc_a))])
+        eb = np.concatenate([np.sort(rng.uniform(-1.5, -0.3, self.nocc_b)),
+                             np.sort(rng.uniform(0.1, 3.0, self.nmo - self.nocc_b))])
+        self.eps_a, self.eps_b = ea, eb
+        L = rng.normal(0.0, 0.05, (self.naux, self.nmo, self.nmo))
+        L = np.triu(L) + np.transpose(np.triu(L, 1), (0, 2, 1))
+        aux_irrep = np.array([P % self.nirrep + 1 for P in range(self.naux)], dtype=np.int64)
+        ip = mo_irrep[:, None] - 1
+        iq = mo_irrep[None, :] - 1
+        pq_irrep = (ip ^ iq) + 1  # XOR-ordered abelian groups
+        mask = pq_irrep[None, :, :] == aux_irrep[:, None, None]
+        L = np.where(mask, L, 0.0)
+        self.L = np.ascontiguousarray(L)
+        self.aux_irrep = aux_irrep
+        # roots: dict irrep -> count (estate_sym)
+        self.estate_sym = np.zeros(8, np.int64)
+        if roots is not None:
+            if isinstance(roots, int):
+                self.estate_sym[0] = roots
+            else:
+                for h, n in dict(roots).items():
+                    self.estate_sym[int(h) - 1] = int(n)
+        self._build(skip_abcd)
+
+    # DPD lengths of the integral tensors (iop = 0 on antisymmetric pairs)
+    def lengths(self):
+        s, o, v = self.sym, self.popo, self.popv
+        return {
+            "ijkl": s.idsymsoc(1, o, o, 0, o, o, 0),
+            "ijka": s.idsymsoc(1, o, o, 0, o, v, 1),
+            "abij": s.idsymsoc(1, v, v, 0, o, o, 0),
+            "iabj": s.idsymsoc(1, v, o, 1, v, o, 1),
+            "abci": s.idsymsoc(1, v, v, 0, v, o, 1),
+            "abcd": s.idsymsoc(1, v, v, 0, v, v, 0),
+        }
+
+    def _build(self, skip_abcd):
+        lib = _load()
+        lens = self.lengths()
+        self.ints = {k: np.zeros(n, np.float64) for k, n in lens.items()}
+        if skip_abcd:
+            self.ints["abcd"] = None
+        self.eorb = np.zeros(int(self.popo.sum() + self.popv.sum()), np.float64)
+        popo = np.zeros(8, np.int64)
+        popv = np.zeros(8, np.int64)
+        rc = lib.cpsd_synth_build(
+            ctypes.c_int64(self.nmo), ctypes.c_int64(self.nirrep), _p(self.dirprd), _p(self.mo_irrep),
+            ctypes.c_int64(self.nocc_a), ctypes.c_int64(self.nocc_b), _p(self.eps_a), _p(self.eps_b),
+            ctypes.c_int64(self.naux), _p(self.aux_irrep), _p(self.L),
+            _p(popo), _p(popv), _p(self.eorb),
+            _p(self.ints["ijkl"]), _p(self.ints["ijka"]), _p(self.ints["abij"]), _p(self.ints["iabj"]),
+            _p(self.ints["abci"]), _p(self.ints["abcd"]))
+        if rc != 0:
+            raise RuntimeError(f"cpsd_synth_build failed: {rc}")
+        assert np.array_equal(popo, self.popo) and np.array_equal(popv, self.popv)
+
+    @property
+    def nroots(self):
+        return int(self.estate_sym.sum())
+
+    def r1_len(self, sym):
+        return self.sym.irpdso(sym, self.popv, self.popo, 1)
+
+    def r2_len(self, sym):
+        return self.sym.idsymsoc(sym, self.popv, self.popv, 0, self.popo, self.popo, 0)
+
+
+# named workloads (shapes of the benchmark configurations)
+CONFIGS = {
+    # plain FP64 SF-CIS + SF-CPS(D), C2v: nmo 48, nocc 5/3, 3 roots
+    "c2v_nmo48": dict(nmo=48, nocc_a=5, nocc_b=3, nirrep=4, roots=3),
+    # precision form, single molecule, D2h: nmo 200, nocc 10/8, 5 roots
+    "d2h_nmo200": dict(nmo=200, nocc_a=10, nocc_b=8, nirrep=8, roots=5),
+    # differentiation form shapes, C2v: nmo 120, nocc 8/6, 4 roots
+    "c2v_nmo120": dict(nmo=120, nocc_a=8, nocc_b=6, nirrep=4, roots=4),
+    # large EE run, D2h: nmo 400, nocc 20/18, 10 roots
+    "d2h_nmo400": dict(nmo=400, nocc_a=20, nocc_b=18, nirrep=8, roots=10),
+}
+
+
+def make(name, seed=0, **kw):
+    cfg = dict(CONFIGS[name])
+    cfg.update(kw)
+    return System(seed=seed, **cfg)

@@ -1,0 +1,137 @@
+"""Dense numpy SF-CIS / CPS(D) / EE-CPS(D-3) equations on small systems
+(test infrastructure): an independent check of the drivers' bookkeeping.
+
+Equations follow the reference's programs (src/EE-CIS.SF/calAR.f90,
+src/CPSd.SF/run1.f90, run2.f90, src/EE-CPSd.SF/run_order.f90, calE_C.f90,
+calJ.f90, calC_JR.f90, calC_VTR.f90, solver.f90) with the kernels' dense
+formulas from kernel_specs; linear solves are done exactly (numpy.linalg)
+instead of DIIS, which the iterative solvers converge to.
+"""
+import numpy as np
+
+import dense
+from kernel_specs import KERNELS
+
+
+def K(name, a, b, f=1.0):
+    return KERNELS[name][3](a, b, f)
+
+
+class DenseSystem:
+    def __init__(self, s):
+        self.s = s
+        g, O, V, eo, ev = dense.antisym_integrals(s)
+        self.eo, self.ev = eo, ev
+        self.ijkl = g[O, O, O, O]
+        self.ijka = g[O, O, O, V]
+        self.abij = g[V, V, O, O]
+        self.iabj = g[O, V, V, O].transpose(2, 0, 1, 3)  # (b,i,a,j)
+        self.abci = g[V, V, V, O]
+        self.abcd = g[V, V, V, V]
+        self.irr_o = dense.orbital_irreps(s.popo)
+        self.irr_v = dense.orbital_irreps(s.popv)
+        occ, vir = dense.spin_orbitals(s)
+        self.spin_o = np.array([x for _, x in occ])
+        self.spin_v = np.array([x for _, x in vir])
+        self.e1 = ev[:, None] - eo[None, :]
+        self.e2 = ev[:, None, None, None] + ev[None, :, None, None] - eo[None, None, :, None] - eo[None, None, None, :]
+
+    def mask1(self, symR):
+        sym = self.s.sym
+        return np.array([[sym.dp(a, i) == symR for i in self.irr_o] for a in self.irr_v])
+
+    def cis_matrix(self, symR, spin_flip=True):
+        m = self.mask1(symR)
+        if spin_flip:
+            m = m & (self.spin_v[:, None] == 1) & (self.spin_o[None, :] == 0)
+        idx = np.argwhere(m)
+        nv, no = self.e1.shape
+        Afull = np.einsum("fnai->aifn", self.iabj).reshape(nv * no, nv * no)
+        Afull = Afull + np.diag(self.e1.reshape(-1))
+        flat = idx[:, 0] * no + idx[:, 1]
+        return Afull[np.ix_(flat, flat)], idx
+
+    def ground(self):
+        T2_1 = -self.abij / self.e2
+        E2 = 0.25 * np.sum(T2_1 * self.abij)
+        C1 = K("c1_r2abci", T2_1, self.abci) + K("c1_r2ijka", T2_1, self.ijka)
+        C2 = (K("c2_r2Wmbej", T2_1, self.iabj) + K("c2_r2Wmnij", T2_1, self.ijkl)
+              + K("c2_r2abcd", T2_1, self.abcd))
+        T2_2 = -C2 / self.e2
+        E3 = 0.25 * np.sum(T2_2 * self.abij)
+        # T1^(2): -e T1 = C1 + V T1 on the totally symmetric (a,i) space
+        A, idx = self._sigma_matrix(1)
+        rhs = -C1[idx[:, 0], idx[:, 1]]
+        x = np.linalg.solve(A, rhs)
+        T1_2 = np.zeros_like(C1)
+        T1_2[idx[:, 0], idx[:, 1]] = x
+        return dict(T2_1=T2_1, T1_2=T1_2, T2_2=T2_2, E2=E2, E3=E3)
+
+    def _sigma_matrix(self, symR):
+        m = self.mask1(symR)
+        idx = np.argwhere(m)
+        nv, no = self.e1.shape
+        Afull = np.einsum("fnai->aifn", self.iabj).reshape(nv * no, nv * no) + np.diag(self.e1.reshape(-1))
+        flat = idx[:, 0] * no + idx[:, 1]
+        return Afull[np.ix_(flat, flat)], idx
+
+    def jints(self, g):
+        T2_1, T1_2, T2_2 = g["T2_1"], g["T1_2"], g["T2_2"]
+        J = {}
+        J["J2_Foo"] = K("Fmi_r2abij", T2_1, self.abij)
+        J["J2_Fvv"] = K("Fae_r2abij", T2_1, self.abij)
+        J["J2_Wovoo"] = K("Wkbij_r2ijka", T2_1, self.ijka) + K("Wkbij_r2abci", T2_1, self.abci)
+        J["J2_Wovvo"] = K("Wmbej_r2abij", T2_1, self.abij, 2.0)
+        J["J3_Foo"] = K("Fmi_r1ijka", T1_2, self.ijka) + K("Fmi_r2abij", T2_2, self.abij)
+        J["J3_Fvv"] = K("Fae_r1abci", T1_2, self.abci) + K("Fae_r2abij", T2_2, self.abij)
+        J["J3_Wovvo"] = (K("Wmbej_r1ijka", T1_2, self.ijka) + K("Wmbej_r1abci", T1_2, self.abci)
+                         + K("Wmbej_r2abij", T2_2, self.abij, 2.0))
+        return J
+
+    def root(self, g, J, symR, w0, L):
+        """L: dense (v,o) CIS vector; returns w^(1..3), R2^(1), R1^(2), R2^(2)."""
+        T2 = g["T2_1"]
+        # order 1: C^(1) = J^(1) R^(0): C2 only
+        C1_1 = np.zeros_like(L)
+        C2_1 = K("c2_r1ijka", L, self.ijka) + K("c2_r1abci", L, self.abci)
+        w1 = np.sum(L * C1_1)
+        # order 2
+        R2_1 = -C2_1 / (self.e2 - w0)
+        C1_2 = K("c1_r2abci", R2_1, self.abci) + K("c1_r2ijka", R2_1, self.ijka)
+        C2_2 = (K("c2_r2Wmbej", R2_1, self.iabj) + K("c2_r2Wmnij", R2_1, self.ijkl)
+                + K("c2_r2abcd", R2_1, self.abcd))
+        C2_2 = C2_2 + K("c2_r1ijka", L, J["J2_Wovoo"])
+        C1_2 = C1_2 + K("c1_r1iabj", L, J["J2_Wovvo"]) + K("c1_r1Fmi", L, J["J2_Foo"]) + K("c1_r1Fae", L, J["J2_Fvv"])
+        # calC_VTR with T^(1) = (0, T2^(1))
+        Wmn = K("Wmnij_r1ijka", L, self.ijka)
+        C2_2 = C2_2 + K("c2_r2Wmnij", T2, Wmn)
+        Wmb = K("Wmbej_r1abci", L, self.abci)
+        C2_2 = C2_2 + K("c2_r2Wmbej", T2, Wmb)
+        G = K("Fmi_r1ijka", L, self.ijka)
+        C2_2 = C2_2 + K("c2_r2Fmi", T2, G)
+        Gv = K("Fae_r1abci", L, self.abci)
+        C2_2 = C2_2 + K("c2_r2Fae", T2, Gv)
+        w2 = np.sum(L * C1_2)
+        # order 3
+        Ct1 = -C1_2 + w2 * L
+        Ct2 = -C2_2
+        R2_2 = Ct2 / (self.e2 - w0)
+        # fixed point of solver.f90: R1 = P[(C' - w0 R1 + V R1)/(-e)] with
+        # P = 1 - L L^T, i.e. (A - w0) R1 + c e*L = Ct1, L.R1 = 0
+        A, idx = self._sigma_matrix(symR)
+        l = L[idx[:, 0], idx[:, 1]]
+        el = self.e1[idx[:, 0], idx[:, 1]] * l
+        n = len(l)
+        M = np.zeros((n + 1, n + 1))
+        M[:n, :n] = A - w0 * np.eye(n)
+        M[:n, n] = el
+        M[n, :n] = l
+        rhs = np.zeros(n + 1)
+        rhs[:n] = Ct1[idx[:, 0], idx[:, 1]]
+        x = np.linalg.solve(M, rhs)[:n]
+        R1_2 = np.zeros_like(L)
+        R1_2[idx[:, 0], idx[:, 1]] = x
+        C1_3 = K("c1_r2abci", R2_2, self.abci) + K("c1_r2ijka", R2_2, self.ijka)
+        C1_3 = C1_3 + K("c1_r1iabj", L, J["J3_Wovvo"]) + K("c1_r1Fmi", L, J["J3_Foo"]) + K("c1_r1Fae", L, J["J3_Fvv"])
+        w3 = np.sum(L * C1_3)
+        return dict(w=np.array([w1, w2, w3]), R2_1=R2_1, R1_2=R1_2, R2_2=R2_2)

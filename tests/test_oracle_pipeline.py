@@ -1,0 +1,110 @@
+"""CPU oracle pipeline (SF-CIS Davidson, ground CPS(D), J^(2)/J^(3),
+EE-CPS(D-3) per root) against the dense numpy equations."""
+import numpy as np
+import pytest
+
+import dense
+import dense_pipeline as dp
+import oracle_ffi as of
+from cpsd_b200 import synth
+
+
+def small(nirrep, seed=5, roots=2):
+    return synth.System(nmo=14 if nirrep <= 2 else 16, nocc_a=3, nocc_b=1, nirrep=nirrep, seed=seed, roots=roots)
+
+
+def vo_dense(s, vec, symR):
+    z = np.array([1, 0, 0, 0, 0, 0, 0, 0])
+    return dense.dpd_to_dense(vec, s.sym, [s.popv, s.popo, z, z], (1, 1), symR)[:, :, 0, 0]
+
+
+def vvoo_dense(s, vec, symR):
+    return dense.dpd_to_dense(vec, s.sym, [s.popv, s.popv, s.popo, s.popo], (0, 0), symR)
+
+
+@pytest.mark.parametrize("lowest", [0, 1])
+@pytest.mark.parametrize("nirrep", [1, 2, 4])
+def test_cis_matches_dense_diagonalisation(nirrep, lowest):
+    s = small(nirrep)
+    orc = of.Oracle(s, lowest=lowest)
+    om, R, it = orc.cis()
+    ds = dp.DenseSystem(s)
+    A, idx = ds.cis_matrix(1, spin_flip=True)
+    ev = np.linalg.eigvalsh(0.5 * (A + A.T))
+    if lowest:
+        np.testing.assert_allclose(om, ev[:len(om)], atol=1e-9)
+    else:
+        # default root tracking (mod_davidson.f90:227-251) follows the
+        # eigenvector of largest overlap with each initial guess: every
+        # root is an eigenvalue, not necessarily one of the lowest
+        for w in om:
+            assert np.min(np.abs(ev - w)) < 1e-9
+    # Davidson self-test (src/lib_cc/mod_davidson.f90:525-542): |AR - wR|_inf < 1e-8
+    l1 = s.r1_len(1)
+    for k in range(len(om)):
+        r = vo_dense(s, R[k * l1:(k + 1) * l1], 1)
+        x = r[idx[:, 0], idx[:, 1]]
+        assert abs(np.linalg.norm(x) - 1) < 1e-10
+        assert np.max(np.abs(A @ x - om[k] * x)) < 1e-8
+
+
+@pytest.mark.parametrize("nirrep", [1, 4])
+def test_ground_matches_dense(nirrep):
+    s = small(nirrep)
+    g = of.Oracle(s).ground()
+    d = dp.DenseSystem(s).ground()
+    assert abs(g["E2"] - d["E2"]) < 1e-12
+    assert abs(g["E3"] - d["E3"]) < 1e-12
+    np.testing.assert_allclose(vvoo_dense(s, g["T2_1"], 1), d["T2_1"], atol=1e-13)
+    np.testing.assert_allclose(vvoo_dense(s, g["T2_2"], 1), d["T2_2"], atol=1e-13)
+    # T1^(2) from DIIS converged to 1e-7 (diis_max_err)
+    np.testing.assert_allclose(vo_dense(s, g["T1_2"], 1), d["T1_2"], atol=5e-7)
+
+
+@pytest.mark.parametrize("nirrep", [1, 2, 4])
+def test_eecpsd_roots_match_dense(nirrep):
+    s = small(nirrep)
+    orc = of.Oracle(s)
+    om, R, _ = orc.cis()
+    g = orc.ground()
+    J = orc.jints(g)
+    ds = dp.DenseSystem(s)
+    # feed the oracle's own T^(2) to the dense J^(3) so only the EE equations are compared
+    gd = ds.ground()
+    gd["T1_2"] = vo_dense(s, g["T1_2"], 1)
+    Jd = ds.jints(gd)
+    l1 = s.r1_len(1)
+    for k in range(len(om)):
+        L = R[k * l1:(k + 1) * l1]
+        r = orc.root(g, J, 1, om[k], L)
+        d = ds.root(gd, Jd, 1, om[k], vo_dense(s, L, 1))
+        assert r["w"][0] == 0.0
+        assert abs(r["w"][1] - d["w"][1]) < 1e-11, (r["w"], d["w"])
+        assert abs(r["w"][2] - d["w"][2]) < 1e-10, (r["w"], d["w"])
+        np.testing.assert_allclose(vvoo_dense(s, r["R2_1"], 1), d["R2_1"], atol=1e-12)
+        np.testing.assert_allclose(vvoo_dense(s, r["R2_2"], 1), d["R2_2"], atol=1e-11)
+        # R1^(2) from the DIIS solver (residual 1e-7); <L|R1^(2)> = 0
+        np.testing.assert_allclose(vo_dense(s, r["R1_2"], 1), d["R1_2"], atol=2e-6)
+        assert abs(np.dot(L, r["R1_2"])) < 1e-12
+
+
+def test_intermediates_match_dense():
+    s = small(4)
+    orc = of.Oracle(s)
+    g = orc.ground()
+    J = orc.jints(g)
+    ds = dp.DenseSystem(s)
+    gd = ds.ground()
+    gd["T1_2"] = vo_dense(s, g["T1_2"], 1)
+    Jd = ds.jints(gd)
+    z = np.array([1, 0, 0, 0, 0, 0, 0, 0])
+    o, v, sym = s.popo, s.popv, s.sym
+    lay = {"J2_Foo": ([o, o, z, z], (1, 1)), "J2_Fvv": ([v, v, z, z], (1, 1)),
+           "J2_Wovvo": ([v, o, v, o], (1, 1)), "J2_Wovoo": ([o, o, o, v], (0, 1)),
+           "J3_Foo": ([o, o, z, z], (1, 1)), "J3_Fvv": ([v, v, z, z], (1, 1)),
+           "J3_Wovvo": ([v, o, v, o], (1, 1))}
+    for k, (pops, iops) in lay.items():
+        D = Jd[k]
+        if D.ndim == 2:
+            D = D[:, :, None, None]
+        np.testing.assert_allclose(J[k], dense.dense_to_dpd(D, sym, pops, iops, 1), atol=1e-12, err_msg=k)
