@@ -1,0 +1,269 @@
+/*
+ * cpsd_b200 — C-ABI of the B200-native SF-CIS / SF-CPS(D-3) hot path.
+ *
+ * Drop-in for the reference's GPU path of libsrint / lib_cc
+ * (lishun-1208/revised-cluster-perturbation-single-double): every entry
+ * point takes DEVICE pointers (the reference's igpu=1 contract,
+ * src/libsrint/vv2v_dpd_444.f90:45-46), int64 integers (the reference is
+ * built with -i8, src/make.config:110), 1-based irreps and the DPD layout
+ * of src/libsrint/irpdso.f / isymoffso.f / idsymsoc.f.  Errors are returned
+ * as negative codes instead of the reference's STOP; cpsd_last_error()
+ * gives the message.  All work is queued on the stream set with
+ * cpsd_set_stream (default: the legacy default stream); entry points that
+ * return host scalars synchronise that stream.
+ */
+#ifndef CPSD_B200_H
+#define CPSD_B200_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CPSD_OK 0
+#define CPSD_EARG (-1)    /* invalid argument / index specification */
+#define CPSD_ELAYOUT (-2) /* packed pair not intact, population mismatch */
+#define CPSD_EMEM (-3)    /* device allocation failed */
+#define CPSD_ECUDA (-4)   /* CUDA runtime error */
+#define CPSD_ESTATE (-5)  /* library not initialised */
+
+/* ------------------------------------------------------------------ setup */
+/* Symmetry tables; replaces module mod_symm (src/lib_mod/mod_symm.f:1-9) as
+ * filled by readmodule (src/lib_cc/readmodule.f90:23-27).  dirprd is the
+ * column-major 8x8 DIRPRD table, dirprd[(j-1)*8+(i-1)] = DIRPRD(i,j). */
+int cpsd_init(int64_t nirrep, const int64_t *dirprd);
+/* cudaStream_t to queue work on (NULL = legacy default stream) */
+int cpsd_set_stream(void *stream);
+/* Caller-owned device scratch for expansions / split-K partials.  Without
+ * it the library allocates (cudaMalloc) its own and grows it on demand. */
+int cpsd_set_workspace(void *dev_ptr, size_t bytes);
+/* bytes of scratch the last operations needed (high-water mark) */
+size_t cpsd_workspace_high_water(void);
+const char *cpsd_last_error(void);
+/* number of kernels this library launched since cpsd_init / last reset */
+int64_t cpsd_launch_count(int reset);
+
+/* -------------------------------------------------------------- size math */
+/* irpdso (src/libsrint/irpdso.f:1-52) */
+int64_t cpsd_irpdso(int64_t sym, const int64_t *popp, const int64_t *popq, int64_t ioppq);
+/* idsymsoc (src/libsrint/idsymsoc.f:1-30) */
+int64_t cpsd_idsymsoc(int64_t irrepx, const int64_t *popp, const int64_t *popq, int64_t ioppq,
+                      const int64_t *popr, const int64_t *pops, int64_t ioprs);
+/* isymoffso (src/libsrint/isymoffso.f:1-54), 1-based */
+int64_t cpsd_isymoffso(int64_t irrepq1, int64_t irrep, const int64_t *popp, const int64_t *popq,
+                       int64_t iop);
+
+/* --------------------------------------------------------- DPD engines
+ * V3 = fact1 * (V1 (x) V2) + fact2 * V3 over symmetry-allowed elements,
+ * arbitrary 4-letter aliases.  fact2 = 0 overwrites V3 without reading it.
+ * Packed (iop 0/2) pairs must stay intact (same letters, order and iop in
+ * the partner operand), as the reference's dispatcher requires
+ * (src/libsrint/vv2v_dpd_444.f90:171-186). */
+
+/* vv2v_dpd_444 (src/libsrint/vv2v_dpd_444.f90:55-72) */
+int cpsd_vv2v_dpd_444(const double *v1, const int64_t *p1_1, const int64_t *p1_2, int64_t iop1_12,
+                      const int64_t *p1_3, const int64_t *p1_4, int64_t iop1_34, int64_t sym1,
+                      const char *type1,
+                      const double *v2, const int64_t *p2_1, const int64_t *p2_2, int64_t iop2_12,
+                      const int64_t *p2_3, const int64_t *p2_4, int64_t iop2_34, int64_t sym2,
+                      const char *type2,
+                      double *v3, const int64_t *p3_1, const int64_t *p3_2, int64_t iop3_12,
+                      const int64_t *p3_3, const int64_t *p3_4, int64_t iop3_34, int64_t sym3,
+                      const char *type3, double fact1, double fact2);
+/* vv2v_dpd_424 (src/libsrint/vv2v_dpd_424.f90:21-24): V2 is 2-index */
+int cpsd_vv2v_dpd_424(const double *v1, const int64_t *p1_1, const int64_t *p1_2, int64_t iop1_12,
+                      const int64_t *p1_3, const int64_t *p1_4, int64_t iop1_34, int64_t sym1,
+                      const char *type1,
+                      const double *v2, const int64_t *p2_1, const int64_t *p2_2, int64_t iop2_12,
+                      int64_t sym2, const char *type2,
+                      double *v3, const int64_t *p3_1, const int64_t *p3_2, int64_t iop3_12,
+                      const int64_t *p3_3, const int64_t *p3_4, int64_t iop3_34, int64_t sym3,
+                      const char *type3, double fact1, double fact2);
+/* vv2v_dpd_442 (src/libsrint/vv2v_dpd_442.f90:22-25): V3 is 2-index */
+int cpsd_vv2v_dpd_442(const double *v1, const int64_t *p1_1, const int64_t *p1_2, int64_t iop1_12,
+                      const int64_t *p1_3, const int64_t *p1_4, int64_t iop1_34, int64_t sym1,
+                      const char *type1,
+                      const double *v2, const int64_t *p2_1, const int64_t *p2_2, int64_t iop2_12,
+                      const int64_t *p2_3, const int64_t *p2_4, int64_t iop2_34, int64_t sym2,
+                      const char *type2,
+                      double *v3, const int64_t *p3_1, const int64_t *p3_2, int64_t iop3_12,
+                      int64_t sym3, const char *type3, double fact1, double fact2);
+/* vv2v_dpd_422 (src/libsrint/vv2v_dpd_422.f90:21): V2, V3 2-index */
+int cpsd_vv2v_dpd_422(const double *v1, const int64_t *p1_1, const int64_t *p1_2, int64_t iop1_12,
+                      const int64_t *p1_3, const int64_t *p1_4, int64_t iop1_34, int64_t sym1,
+                      const char *type1,
+                      const double *v2, const int64_t *p2_1, const int64_t *p2_2, int64_t iop2_12,
+                      int64_t sym2, const char *type2,
+                      double *v3, const int64_t *p3_1, const int64_t *p3_2, int64_t iop3_12,
+                      int64_t sym3, const char *type3, double fact1, double fact2);
+/* vv2v_dpd_222 (src/libsrint/vv2v_dpd_222.f90:19): all 2-index */
+int cpsd_vv2v_dpd_222(const double *v1, const int64_t *p1_1, const int64_t *p1_2, int64_t iop1_12,
+                      int64_t sym1, const char *type1,
+                      const double *v2, const int64_t *p2_1, const int64_t *p2_2, int64_t iop2_12,
+                      int64_t sym2, const char *type2,
+                      double *v3, const int64_t *p3_1, const int64_t *p3_2, int64_t iop3_12,
+                      int64_t sym3, const char *type3, double fact1, double fact2);
+
+/* Fortran-callable binding of the same engine (gfortran/nvfortran ABI:
+ * lower case + trailing underscore, every argument by reference, hidden
+ * character lengths last), so the reference's call sites
+ * (src/lib_cc/mod_contract.f90:104-107) link against it unchanged when
+ * igpu=1 and prec=8. */
+void vv2v_dpd_444_(const double *v1, const int64_t *p1_1, const int64_t *p1_2, const int64_t *iop1_12,
+                   const int64_t *p1_3, const int64_t *p1_4, const int64_t *iop1_34, const int64_t *sym1,
+                   const char *type1,
+                   const double *v2, const int64_t *p2_1, const int64_t *p2_2, const int64_t *iop2_12,
+                   const int64_t *p2_3, const int64_t *p2_4, const int64_t *iop2_34, const int64_t *sym2,
+                   const char *type2,
+                   double *v3, const int64_t *p3_1, const int64_t *p3_2, const int64_t *iop3_12,
+                   const int64_t *p3_3, const int64_t *p3_4, const int64_t *iop3_34, const int64_t *sym3,
+                   const char *type3, const double *fact1, const double *fact2,
+                   size_t len_type1, size_t len_type2, size_t len_type3);
+
+/* ------------------------------------------------- tensor descriptor
+ * POD mirror of type(opt) (src/lib_cc/mod_operator.f90:8-25): populations,
+ * iops, irrep, length (filled by cpsd_opt_init) and a device array. */
+typedef struct {
+    int64_t popp[8], popq[8], popr[8], pops[8];
+    int64_t ioppq, ioprs;
+    int64_t sym;
+    int64_t len;
+    double *arr;
+} cpsd_opt;
+
+/* init_opt (src/lib_cc/mod_operator.f90:70-115): fills len */
+int cpsd_opt_init(cpsd_opt *t, const int64_t *popp, const int64_t *popq, const int64_t *popr,
+                  const int64_t *pops, int64_t ioppq, int64_t ioprs, int64_t sym, double *dev_arr);
+
+/* layout transforms on cpsd_opt (device arrays), out described by its own
+ * cpsd_opt: iexpso (src/libsrint/iexpso.f90:24-120), icompso
+ * (src/libsrint/icompso.f:1-80; c = 1 keeps a pair), isymtrso
+ * (src/libsrint/isymtrso.f:1-351). */
+int cpsd_iexpso(const cpsd_opt *in, cpsd_opt *out, int64_t exppq, int64_t exprs);
+int cpsd_icompso(const cpsd_opt *in, cpsd_opt *out, int64_t cpq, int64_t crs);
+int cpsd_isymtrso(const cpsd_opt *in, cpsd_opt *out, int64_t swpq, int64_t swrs);
+
+/* mod_contract wrappers (src/lib_cc/mod_contract.f90:10-455):
+ * v3 += fact * P{v1 * v2}; anti 0/1/2/3 antisymmetrises none / 1st / 2nd /
+ * both pairs of v3.  2-index operands carry popr = pops = (1,0,...). */
+int cpsd_vv2v_444(const cpsd_opt *v1, const cpsd_opt *v2, cpsd_opt *v3, double fact,
+                  const char *t1, const char *t2, const char *t3, int64_t anti);
+int cpsd_vv2v_424(const cpsd_opt *v1, const cpsd_opt *v2, cpsd_opt *v3, double fact,
+                  const char *t1, const char *t2, const char *t3, int64_t anti);
+int cpsd_vv2v_442(const cpsd_opt *v1, const cpsd_opt *v2, cpsd_opt *v3, double fact,
+                  const char *t1, const char *t2, const char *t3);
+int cpsd_vv2v_422(const cpsd_opt *v1, const cpsd_opt *v2, cpsd_opt *v3, double fact,
+                  const char *t1, const char *t2, const char *t3);
+int cpsd_vv2v_222(const cpsd_opt *v1, const cpsd_opt *v2, cpsd_opt *v3, double fact,
+                  const char *t1, const char *t2, const char *t3);
+int cpsd_vv2v_224(const cpsd_opt *v1, const cpsd_opt *v2, cpsd_opt *v3, double fact,
+                  const char *t1, const char *t2, const char *t3, int64_t anti);
+
+/* ---------------------------------------- spin-free lib_cc kernels
+ * out += fact * kernel(a, b); each replaces the subroutine of the same name
+ * in src/lib_cc/<name>.f90 (plain spin-free variant). */
+#define CPSD_KERNEL(name) int cpsd_##name(cpsd_opt *out, const cpsd_opt *a, const cpsd_opt *b, double fact)
+CPSD_KERNEL(c1_r1iabj);  /* c1_r1iabj.f90:3   c(a,i) += r(f,n) V(fn,ai)        */
+CPSD_KERNEL(c1_r1Fae);   /* c1_r1Fae.f90:3    c(a,i) += r(e,i) F(a,e)          */
+CPSD_KERNEL(c1_r1Fmi);   /* c1_r1Fmi.f90:3    c(a,i) -= r(a,m) F(m,i)          */
+CPSD_KERNEL(c1_r2abci);  /* c1_r2abci.f90:3   c(a,i) += .5 r(fe,im) V(fe,am)   */
+CPSD_KERNEL(c1_r2ijka);  /* c1_r2ijka.f90:3   c(a,i) -= .5 r(ae,mn) V(mn,ie)   */
+CPSD_KERNEL(c2_r1abci);  /* c2_r1abci.f90:3   c(ab,ij) += P(ij) r(e,i) V(ab,ej) */
+CPSD_KERNEL(c2_r1ijka);  /* c2_r1ijka.f90:3   c(ab,ij) -= P(ab) r(a,m) V(ij,mb) */
+CPSD_KERNEL(c2_r2Wmbej); /* c2_r2Wmbej.f90:3  c(ab,ij) += P(ab|ij) r(ae,im) W(em,bj) */
+CPSD_KERNEL(c2_r2Wmnij); /* c2_r2Wmnij.f90:3  c(ab,ij) += .5 r(ab,mn) W(mn,ij) */
+CPSD_KERNEL(c2_r2abcd);  /* c2_r2abcd.f90:3   c(ab,ij) += .5 r(ef,ij) V(ab,ef) */
+CPSD_KERNEL(c2_r2Fae);   /* c2_r2Fae.f90:3    c(ab,ij) += P(ab) r(ae,ij) F(b,e) */
+CPSD_KERNEL(c2_r2Fmi);   /* c2_r2Fmi.f90:3    c(ab,ij) -= P(ij) r(ab,im) F(m,j) */
+CPSD_KERNEL(Fmi_r2abij); /* Fmi_r2abij.f90:3  F(m,i) += .5 r(ef,in) V(ef,mn)   */
+CPSD_KERNEL(Fae_r2abij); /* Fae_r2abij.f90:3  F(a,e) -= .5 r(af,mn) V(ef,mn)   */
+CPSD_KERNEL(Fmi_r1ijka); /* Fmi_r1ijka.f90:3  F(m,i) += r(e,n) V(mn,ie)        */
+CPSD_KERNEL(Fae_r1abci); /* Fae_r1abci.f90:3  F(a,e) += r(f,m) V(ef,am)        */
+CPSD_KERNEL(Wkbij_r2ijka); /* Wkbij_r2ijka.f90:3 W(ij,kb) += P(ij) V(kl,ic) r(bc,jl) */
+CPSD_KERNEL(Wkbij_r2abci); /* Wkbij_r2abci.f90:3 W(ij,kb) += .5 V(dc,bk) r(cd,ij)   */
+CPSD_KERNEL(Wmbej_r2abij); /* Wmbej_r2abij.f90:3 W(em,bj) += .5 r(bf,jn) V(fe,nm)   */
+CPSD_KERNEL(Wmbej_r1abci); /* Wmbej_r1abci.f90:3 W(em,bj) += r(f,j) V(fe,bm)        */
+CPSD_KERNEL(Wmbej_r1ijka); /* Wmbej_r1ijka.f90:3 W(em,bj) -= r(b,n) V(nm,je)        */
+CPSD_KERNEL(Wmnij_r1ijka); /* Wmnij_r1ijka.f90:3 W(mn,ij) += P(ij) r(e,j) V(mn,ie)  */
+#undef CPSD_KERNEL
+
+/* --------------------------------------------- planner introspection
+ * Host-only (no GPU needed; no counterpart in the reference): the tables
+ * the planner builds for a contraction / pair transform, for verification
+ * tools.  Layouts are TaskDev / SegDev / TileDev / PMBlockDev of
+ * csrc/runtime.hpp; pointers stay valid for the life of the process.
+ * op codes: 0 copy, 1 expand, 2 compress, 3 antisymmetrise,
+ * 4 antisymmetrise+compress, 5 swap. */
+int cpsd_debug_contract_plan(const cpsd_opt *v1, const char *t1, const cpsd_opt *v2, const char *t2,
+                             const cpsd_opt *v3, const char *t3, int64_t nb, int64_t sA, int64_t sB, int64_t sC,
+                             const void **tasks, int64_t *ntasks, const void **segs, int64_t *nsegs,
+                             const void **tiles, int64_t *ntiles);
+int cpsd_debug_pairmap_plan(const cpsd_opt *in, int64_t op0, int64_t op1, int64_t tgt0, int64_t tgt1,
+                            const void **blocks, int64_t *nblocks, const void **idx, const void **sgn,
+                            int64_t *nidx, int64_t *lterms, int64_t *rterms);
+
+/* -------------------------------------------------- molecular programs */
+typedef struct {
+    int64_t nirrep;
+    int64_t dirprd[64];
+    int64_t symry;
+    int64_t popa[8], popb[8], vrta[8], vrtb[8];
+} cpsd_system;
+
+/* spin-free integrals in DPD layout, iop 0 on antisymmetric pairs, device
+ * pointers (allocate_mem, src/EE-CPSd.SF/allocate_mem.f90:14-44) */
+typedef struct {
+    const double *ijkl, *ijka, *abij, *iabj, *abci, *abcd;
+    const double *eorb; /* spin-free orbital energies (src/getHF/resortEorb.f90) */
+} cpsd_integrals;
+
+typedef struct {
+    int64_t davidson_dim, davidson_cyc, davidson_conv, lowest; /* mod_common.f90:37-40 */
+    int64_t diis_dim, diis_cyc;                                 /* mod_common.f90:17-18 */
+    double diis_max_err;                                        /* mod_common.f90:20 */
+    int64_t spin_flip;  /* 0 none, 1 "ab", 2 "ba" (preDavidson.f90:64-95) */
+    int64_t open_shell; /* shell=open */
+    int64_t ex_mult;
+    int64_t estate_sym[8];
+    int64_t batch_roots; /* 1: the roots of one irrep share each contraction launch */
+} cpsd_params;
+
+void cpsd_params_default(cpsd_params *p);
+
+/* SF-CIS (src/EE-CIS.SF/run.f90:2-100): omega_host[k] and the unit-norm
+ * R1 of every requested root (irrep 1 first) into R_dev (device). */
+int cpsd_cis_run(const cpsd_system *s, const cpsd_integrals *I, const cpsd_params *p,
+                 double *omega_host, double *R_dev, int64_t *iterations);
+
+/* ground CPS(D) T^(1), T^(2) (src/CPSd.SF/run1.f90, run2.f90); device outputs */
+int cpsd_ground(const cpsd_system *s, const cpsd_integrals *I, const cpsd_params *p,
+                double *T2_1, double *T1_2, double *T2_2, double *E2_host, double *E3_host,
+                int64_t *diis_iters);
+
+/* J^(2) / J^(3) intermediates (src/EE-CPSd.SF/calJ.f90:6-228); device */
+typedef struct {
+    double *J2_Foo, *J2_Fvv, *J2_Wovvo, *J2_Wovoo;
+    double *J3_Foo, *J3_Fvv, *J3_Wovvo;
+} cpsd_jints;
+int cpsd_calJ(const cpsd_system *s, const cpsd_integrals *I, const double *T2_1,
+              const double *T1_2, const double *T2_2, cpsd_jints *J);
+
+/* EE-CPS(D-3) orders 1..3 (src/EE-CPSd.SF/run.f90:86-107, run_order.f90)
+ * for nroot roots of irrep symR with CIS energies w0_host[k] and CIS
+ * vectors L_dev (nroot x lenR1, device).  w_host[3k..3k+2] = w^(1..3).
+ * Optional device outputs (NULL to skip): R2_1, R1_2, R2_2 per root. */
+int cpsd_eecpsd_roots(const cpsd_system *s, const cpsd_integrals *I, const cpsd_params *p,
+                      const double *T2_1, const cpsd_jints *J, int64_t symR, int64_t nroot,
+                      const double *w0_host, const double *L_dev, double *w_host,
+                      double *R2_1, double *R1_2, double *R2_2, int64_t *solver_iters);
+
+/* The whole SF-CIS + SF-CPS(D-3) pipeline: one step of the roots/s metric.
+ * Integrals are device pointers; outputs on the host. */
+int cpsd_pipeline(const cpsd_system *s, const cpsd_integrals *I, const cpsd_params *p,
+                  double *omega_cis, double *w2, double *w3, int64_t *nroots);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,238 @@
+"""Python binding of libcpsd_b200 (the C-ABI in include/cpsd_b200.h).
+
+Mirrors the reference's call surface for the SF-CIS / SF-CPS(D-3) path:
+vv2v_dpd_444/424/442/422/222 (src/libsrint/vv2v_dpd_*.f90), the opt-level
+contraction wrappers (src/lib_cc/mod_contract.f90), the spin-free lib_cc
+kernels (src/lib_cc/<name>.f90) and the program drivers (EE-CIS.SF,
+CPSd.SF, EE-CPSd.SF).  Device memory comes from torch CUDA tensors; torch is
+plumbing only.  Every call raises CpsdError on a non-zero return code.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_build", "libcpsd_b200.so")
+I64 = ctypes.c_int64
+_lib = None
+
+
+class CpsdError(RuntimeError):
+    pass
+
+
+def lib():
+    """Load the CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise CpsdError(f"CUDA library missing: {LIB_PATH} (run __graft_entry__.build())")
+        _lib = ctypes.CDLL(LIB_PATH)
+        _lib.cpsd_last_error.restype = ctypes.c_char_p
+        _lib.cpsd_launch_count.restype = I64
+        _lib.cpsd_workspace_high_water.restype = ctypes.c_size_t
+        for f in ("cpsd_irpdso", "cpsd_idsymsoc", "cpsd_isymoffso"):
+            getattr(_lib, f).restype = I64
+    return _lib
+
+
+def check(rc, what=""):
+    if rc != 0:
+        msg = lib().cpsd_last_error().decode(errors="replace")
+        raise CpsdError(f"{what} failed with code {rc}: {msg}")
+    return rc
+
+
+class Opt(ctypes.Structure):
+    """POD mirror of type(opt) (src/lib_cc/mod_operator.f90:8-25)."""
+    _fields_ = [("popp", I64 * 8), ("popq", I64 * 8), ("popr", I64 * 8), ("pops", I64 * 8),
+                ("ioppq", I64), ("ioprs", I64), ("sym", I64), ("len", I64), ("arr", ctypes.c_void_p)]
+
+
+class System(ctypes.Structure):
+    _fields_ = [("nirrep", I64), ("dirprd", I64 * 64), ("symry", I64),
+                ("popa", I64 * 8), ("popb", I64 * 8), ("vrta", I64 * 8), ("vrtb", I64 * 8)]
+
+
+class Integrals(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_void_p) for k in ("ijkl", "ijka", "abij", "iabj", "abci", "abcd", "eorb")]
+
+
+class Params(ctypes.Structure):
+    _fields_ = [("davidson_dim", I64), ("davidson_cyc", I64), ("davidson_conv", I64), ("lowest", I64),
+                ("diis_dim", I64), ("diis_cyc", I64), ("diis_max_err", ctypes.c_double),
+                ("spin_flip", I64), ("open_shell", I64), ("ex_mult", I64), ("estate_sym", I64 * 8),
+                ("batch_roots", I64)]
+
+
+class Jints(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_void_p) for k in ("J2_Foo", "J2_Fvv", "J2_Wovvo", "J2_Wovoo",
+                                               "J3_Foo", "J3_Fvv", "J3_Wovvo")]
+
+
+def arr8(v):
+    return (I64 * 8)(*[int(x) for x in v])
+
+
+def dptr(t):
+    """device pointer of a torch CUDA tensor (or None)"""
+    if t is None:
+        return None
+    import torch
+    if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()):
+        raise CpsdError("expected a contiguous float64 CUDA tensor")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def init(nirrep, dirprd):
+    d = np.ascontiguousarray(dirprd, dtype=np.int64)
+    check(lib().cpsd_init(I64(nirrep), d.ctypes.data_as(ctypes.c_void_p)), "cpsd_init")
+
+
+def use_torch_stream():
+    import torch
+    check(lib().cpsd_set_stream(ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)), "cpsd_set_stream")
+
+
+def launch_count(reset=False):
+    return int(lib().cpsd_launch_count(1 if reset else 0))
+
+
+def opt(pops, iops, sym, t):
+    o = Opt()
+    check(lib().cpsd_opt_init(ctypes.byref(o), arr8(pops[0]), arr8(pops[1]), arr8(pops[2]), arr8(pops[3]),
+                              I64(iops[0]), I64(iops[1]), I64(sym), dptr(t)), "cpsd_opt_init")
+    return o
+
+
+def kernel(name, out, a, b, fact=1.0):
+    """cpsd_<name>(out, a, b, fact): one of the lib_cc kernels on Opt views."""
+    fn = getattr(lib(), "cpsd_" + name)
+    check(fn(ctypes.byref(out), ctypes.byref(a), ctypes.byref(b), ctypes.c_double(fact)), name)
+
+
+def vv2v_dpd_444(v1, d1, t1, v2, d2, t2, v3, d3, t3, f1, f2):
+    """vv2v_dpd_444 on device tensors; dK = (pops[4], iops[2], sym)."""
+    (p1, i1, s1), (p2, i2, s2), (p3, i3, s3) = d1, d2, d3
+    check(lib().cpsd_vv2v_dpd_444(
+        dptr(v1), arr8(p1[0]), arr8(p1[1]), I64(i1[0]), arr8(p1[2]), arr8(p1[3]), I64(i1[1]), I64(s1), t1.encode(),
+        dptr(v2), arr8(p2[0]), arr8(p2[1]), I64(i2[0]), arr8(p2[2]), arr8(p2[3]), I64(i2[1]), I64(s2), t2.encode(),
+        dptr(v3), arr8(p3[0]), arr8(p3[1]), I64(i3[0]), arr8(p3[2]), arr8(p3[3]), I64(i3[1]), I64(s3), t3.encode(),
+        ctypes.c_double(f1), ctypes.c_double(f2)), "vv2v_dpd_444")
+
+
+def make_system(s):
+    """System struct from a synth.System (or any object with the same fields)."""
+    o = System()
+    o.nirrep = s.nirrep
+    for i in range(64):
+        o.dirprd[i] = int(s.dirprd[i])
+    o.symry = s.symry
+    for k in range(8):
+        o.popa[k], o.popb[k], o.vrta[k], o.vrtb[k] = int(s.popa[k]), int(s.popb[k]), int(s.vrta[k]), int(s.vrtb[k])
+    return o
+
+
+def make_params(s, batch_roots=1, **kw):
+    p = Params()
+    lib().cpsd_params_default(ctypes.byref(p))
+    for h in range(8):
+        p.estate_sym[h] = int(s.estate_sym[h])
+    p.spin_flip = s.spin_flip
+    p.batch_roots = batch_roots
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+class DeviceIntegrals:
+    """The six spin-free integral tensors and Eorb resident in HBM."""
+
+    KEYS = ("ijkl", "ijka", "abij", "iabj", "abci", "abcd")
+
+    def __init__(self, s, device="cuda"):
+        import torch
+        self.t = {}
+        for k in self.KEYS:
+            a = s.ints[k]
+            self.t[k] = torch.from_numpy(a).to(device) if a is not None else None
+        self.t["eorb"] = torch.from_numpy(s.eorb).to(device)
+        self.struct = Integrals()
+        for k, v in self.t.items():
+            setattr(self.struct, k, v.data_ptr() if v is not None else None)
+
+    @property
+    def nbytes(self):
+        return sum(v.numel() * 8 for v in self.t.values() if v is not None)
+
+
+def cis_run(s, sysc, ints, par):
+    import torch
+    n = s.nroots
+    rlen = sum(int(s.estate_sym[h]) * s.r1_len(h + 1) for h in range(8))
+    om = np.zeros(max(n, 1))
+    R = torch.zeros(max(rlen, 1), dtype=torch.float64, device="cuda")
+    it = I64()
+    check(lib().cpsd_cis_run(ctypes.byref(sysc), ctypes.byref(ints.struct), ctypes.byref(par),
+                             om.ctypes.data_as(ctypes.c_void_p), dptr(R), ctypes.byref(it)), "cpsd_cis_run")
+    return om[:n], R[:rlen], it.value
+
+
+def ground(s, sysc, ints, par):
+    import torch
+    l1, l2 = s.r1_len(1), s.r2_len(1)
+    T2_1 = torch.zeros(l2, dtype=torch.float64, device="cuda")
+    T1_2 = torch.zeros(l1, dtype=torch.float64, device="cuda")
+    T2_2 = torch.zeros(l2, dtype=torch.float64, device="cuda")
+    E2, E3, it = ctypes.c_double(), ctypes.c_double(), I64()
+    check(lib().cpsd_ground(ctypes.byref(sysc), ctypes.byref(ints.struct), ctypes.byref(par), dptr(T2_1),
+                            dptr(T1_2), dptr(T2_2), ctypes.byref(E2), ctypes.byref(E3), ctypes.byref(it)),
+          "cpsd_ground")
+    return dict(T2_1=T2_1, T1_2=T1_2, T2_2=T2_2, E2=E2.value, E3=E3.value, iters=it.value)
+
+
+def calJ(s, sysc, ints, g):
+    import torch
+    sym, o, v = s.sym, s.popo, s.popv
+    sizes = {"J2_Foo": sym.irpdso(1, o, o, 1), "J2_Fvv": sym.irpdso(1, v, v, 1),
+             "J2_Wovvo": sym.idsymsoc(1, v, o, 1, v, o, 1), "J2_Wovoo": sym.idsymsoc(1, o, o, 0, o, v, 1),
+             "J3_Foo": sym.irpdso(1, o, o, 1), "J3_Fvv": sym.irpdso(1, v, v, 1),
+             "J3_Wovvo": sym.idsymsoc(1, v, o, 1, v, o, 1)}
+    J = {k: torch.zeros(n, dtype=torch.float64, device="cuda") for k, n in sizes.items()}
+    js = Jints()
+    for k, t in J.items():
+        setattr(js, k, t.data_ptr())
+    check(lib().cpsd_calJ(ctypes.byref(sysc), ctypes.byref(ints.struct), dptr(g["T2_1"]), dptr(g["T1_2"]),
+                          dptr(g["T2_2"]), ctypes.byref(js)), "cpsd_calJ")
+    return J, js
+
+
+def eecpsd_roots(s, sysc, ints, par, g, js, symR, w0, L, want_vectors=False):
+    import torch
+    nroot = len(w0)
+    l1, l2 = s.r1_len(symR), s.r2_len(symR)
+    w = np.zeros(3 * nroot)
+    w0a = np.ascontiguousarray(w0, dtype=np.float64)
+    outs = {}
+    if want_vectors:
+        outs = {"R2_1": torch.zeros(nroot * l2, dtype=torch.float64, device="cuda"),
+                "R1_2": torch.zeros(nroot * l1, dtype=torch.float64, device="cuda"),
+                "R2_2": torch.zeros(nroot * l2, dtype=torch.float64, device="cuda")}
+    it = I64()
+    check(lib().cpsd_eecpsd_roots(ctypes.byref(sysc), ctypes.byref(ints.struct), ctypes.byref(par),
+                                  dptr(g["T2_1"]), ctypes.byref(js), I64(symR), I64(nroot),
+                                  w0a.ctypes.data_as(ctypes.c_void_p), dptr(L), w.ctypes.data_as(ctypes.c_void_p),
+                                  dptr(outs.get("R2_1")), dptr(outs.get("R1_2")), dptr(outs.get("R2_2")),
+                                  ctypes.byref(it)), "cpsd_eecpsd_roots")
+    return w.reshape(nroot, 3), outs, it.value
+
+
+def pipeline(s, sysc, ints, par):
+    n = max(s.nroots, 1)
+    om, w2, w3 = np.zeros(n), np.zeros(n), np.zeros(n)
+    nr = I64()
+    check(lib().cpsd_pipeline(ctypes.byref(sysc), ctypes.byref(ints.struct), ctypes.byref(par),
+                              om.ctypes.data_as(ctypes.c_void_p), w2.ctypes.data_as(ctypes.c_void_p),
+                              w3.ctypes.data_as(ctypes.c_void_p), ctypes.byref(nr)), "cpsd_pipeline")
+    return om[:nr.value], w2[:nr.value], w3[:nr.value]

@@ -1,0 +1,690 @@
+// Program drivers on the device: SF-CIS (src/EE-CIS.SF/run.f90), ground
+// CPS(D) first/second order (src/CPSd.SF/run1.f90, run2.f90), the J^(2) /
+// J^(3) intermediates (src/EE-CPSd.SF/calJ.f90) and EE-CPS(D-3) orders 1-3
+// (src/EE-CPSd.SF/run.f90, run_order.f90, calV_C.f90, calE_C.f90,
+// calC_JR.f90, calC_VTR.f90, solver.f90).  The host keeps the reference's
+// control flow; every contraction, denominator, reduction, Davidson and
+// DIIS step runs on the device.  The reference's scratch files are device
+// buffers.  The roots of one irrep can share each contraction launch
+// (params.batch_roots), which streams every integral block once per launch
+// instead of once per root.
+#include <cmath>
+#include <cstddef>
+#include <cstring>
+#include <vector>
+
+#include "ops.hpp"
+#include "solvers.cuh"
+
+namespace cpsd {
+
+namespace {
+
+struct Sys {
+    i64 nirrep, symry;
+    i64 popa[8], popb[8], vrta[8], vrtb[8], popo[8], popv[8];
+};
+
+int make_sys(const cpsd_system *s, Sys *S) {
+    if (!s) return set_error(CPSD_EARG, "null system");
+    bool same = ctx().init && ctx().nirrep == s->nirrep;
+    for (int j = 0; j < s->nirrep && same; j++)
+        for (int i = 0; i < s->nirrep && same; i++)
+            if (ctx().dirprd[i][j] != s->dirprd[j * 8 + i]) same = false;
+    if (!same) CPSD_TRY(cpsd_init(s->nirrep, s->dirprd));
+    S->nirrep = s->nirrep;
+    S->symry = s->symry;
+    for (int r = 0; r < 8; r++) {
+        S->popa[r] = s->popa[r];
+        S->popb[r] = s->popb[r];
+        S->vrta[r] = s->vrta[r];
+        S->vrtb[r] = s->vrtb[r];
+    }
+    for (i64 r = 1; r <= 8; r++) {
+        if (r > s->nirrep) {
+            S->popo[r - 1] = S->popv[r - 1] = 0;
+            continue;
+        }
+        i64 rb = dp(r, s->symry);  // readmodule.f90:36-41
+        S->popo[r - 1] = s->popa[r - 1] + s->popb[rb - 1];
+        S->popv[r - 1] = s->vrta[r - 1] + s->vrtb[rb - 1];
+    }
+    return CPSD_OK;
+}
+
+struct Ints {
+    Ten ijkl, ijka, abij, iabj, abci, abcd;
+    const double *eorb;
+};
+Ints make_ints(const Sys &S, const cpsd_integrals *I) {
+    const i64 *o = S.popo, *v = S.popv;
+    Ints x;
+    x.ijkl = ten(o, o, o, o, 0, 0, 1, (double *)I->ijkl);
+    x.ijka = ten(o, o, o, v, 0, 1, 1, (double *)I->ijka);
+    x.abij = ten(v, v, o, o, 0, 0, 1, (double *)I->abij);
+    x.iabj = ten(v, o, v, o, 1, 1, 1, (double *)I->iabj);
+    x.abci = ten(v, v, v, o, 0, 1, 1, (double *)I->abci);
+    x.abcd = ten(v, v, v, v, 0, 0, 1, (double *)I->abcd);
+    x.eorb = I->eorb;
+    return x;
+}
+
+// pinned host mailbox for the few scalars the host control flow needs
+double *mailbox() {
+    static double *p = nullptr;
+    if (!p) cudaMallocHost(&p, 4096);
+    return p;
+}
+
+int read_back(void *host, const void *dev, size_t bytes) {
+    CPSD_TRY(cuda_check(cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, stream()), "read back"));
+    return cuda_check(cudaStreamSynchronize(stream()), "sync");
+}
+
+int zero(double *p, i64 n) { return launch_scale(p, n, 0.0); }
+
+// AR = e(a,i) R + V(fn,ai) R(fn): calAR (src/EE-CIS.SF/calAR.f90:6-34), batched
+int cis_sigma(const Sys &S, const Ints &I, i64 sym, const double *R, i64 sR, double *AR, i64 sAR, i64 nb) {
+    Desc d = make_desc(S.popv, S.popo, ZORB, ZORB, 1, 1, sym);
+    const EnergyPlan *ep;
+    CPSD_TRY(plan_energy(d, "vozz", &ep));
+    CPSD_TRY(launch_energy(ep, 4, I.eorb, R, AR, nullptr, nb, sR, sAR));
+    Ten r = ten(S.popv, S.popo, ZORB, ZORB, 1, 1, sym, (double *)R, sR);
+    Ten ar = ten(S.popv, S.popo, ZORB, ZORB, 1, 1, sym, AR, sAR);
+    return k_c1_r1iabj(ar, r, I.iabj, 1.0, nb);
+}
+
+// ---------------------------------------------------------------- guesses
+void get_lowest(const std::vector<double> &v, i64 nl, std::vector<i64> &low) {
+    i64 n = (i64)v.size();
+    low.resize(nl);
+    for (i64 i = 0; i < nl; i++) low[i] = i + 1;
+    for (i64 i = 0; i < nl - 1; i++)
+        for (i64 j = i + 1; j < nl; j++)
+            if (v[low[i] - 1] > v[low[j] - 1]) std::swap(low[i], low[j]);
+    for (i64 i = nl + 1; i <= n; i++) {
+        if (v[i - 1] < v[low[nl - 1] - 1]) {
+            i64 s = 1, e = nl;
+            for (;;) {
+                i64 mid = s + (e - s) / 2;
+                if (v[low[mid - 1] - 1] > v[i - 1]) e = mid;
+                else s = mid + 1;
+                if (s == e) break;
+            }
+            for (i64 j = 0; j <= nl - e - 1; j++) low[nl - j - 1] = low[nl - j - 2];
+            low[e - 1] = i;
+        }
+    }
+}
+
+struct PairIdx {
+    i64 ip, iq, p, q;
+};
+// storage-order pairs of a 2-index (p,q) iop 1 vector of irrep sym
+std::vector<PairIdx> pairs2(const i64 *pp, const i64 *pq, i64 sym) {
+    std::vector<PairIdx> v;
+    for (i64 iq = 1; iq <= ctx().nirrep; iq++) {
+        i64 ip = dp(iq, sym);
+        for (i64 q = 0; q < pq[iq - 1]; q++)
+            for (i64 p = 0; p < pp[ip - 1]; p++) v.push_back({ip, iq, p, q});
+    }
+    return v;
+}
+i64 putidx2(const Sys &S, i64 ia, i64 ii, i64 a, i64 i) {
+    i64 irr = dp(ia, ii);
+    return isymoffso(ii, irr, S.popv, S.popo, 1) - 1 + i * S.popv[ia - 1] + a;
+}
+
+// preDavidson1_ns (src/lib_cc/preDavidson.f90:6-515): nroot guess records
+int make_guess(const Sys &S, const std::vector<double> &eorb, const cpsd_params *p, i64 irrepex, i64 nroot,
+               std::vector<double> &rec) {
+    i64 n = S.nirrep;
+    // seperateEorb (src/lib_cc/seperateEorb.f90): alpha / beta occupied and
+    // virtual energies, each ordered by its own irrep
+    std::vector<double> Ea, Eb_o, Ea_v, Eb_v;
+    i64 o[9] = {0}, v[9] = {0};
+    for (i64 r = 0; r < n; r++) o[r + 1] = o[r] + S.popo[r];
+    v[0] = o[n];
+    for (i64 r = 0; r < n; r++) v[r + 1] = v[r] + S.popv[r];
+    for (i64 r = 1; r <= n; r++)
+        for (i64 k = 0; k < S.popa[r - 1]; k++) Ea.push_back(eorb[o[r - 1] + k]);
+    for (i64 rb = 1; rb <= n; rb++) {  // beta irrep rb sits in spin-free irrep r with r x symry = rb
+        i64 r = dp(rb, S.symry);
+        for (i64 k = 0; k < S.popb[rb - 1]; k++) Eb_o.push_back(eorb[o[r - 1] + S.popa[r - 1] + k]);
+    }
+    for (i64 r = 1; r <= n; r++)
+        for (i64 k = 0; k < S.vrta[r - 1]; k++) Ea_v.push_back(eorb[v[r - 1] + k]);
+    for (i64 rb = 1; rb <= n; rb++) {
+        i64 r = dp(rb, S.symry);
+        for (i64 k = 0; k < S.vrtb[rb - 1]; k++) Eb_v.push_back(eorb[v[r - 1] + S.vrta[r - 1] + k]);
+    }
+    // per-irrep offsets inside the alpha / beta arrays
+    auto offs = [&](const i64 *pop, i64 *off) {
+        off[0] = 0;
+        for (i64 r = 0; r < n; r++) off[r + 1] = off[r] + pop[r];
+    };
+    i64 oa[9], ob[9], va[9], vb[9];
+    offs(S.popa, oa);
+    offs(S.popb, ob);
+    offs(S.vrta, va);
+    offs(S.vrtb, vb);
+    i64 vlen = irpdso(irrepex, S.popv, S.popo, 1);
+    rec.assign((size_t)(nroot * (1 + vlen)), 0.0);
+    std::vector<i64> low;
+    // e(a,i) over (a in pop_a1 of E1, i in pop_i2 of E2) in (a,i) storage order
+    auto oed = [&](const std::vector<double> &Evir, const i64 *voff, const i64 *pa, const std::vector<double> &Eocc,
+                   const i64 *ooff, const i64 *pi, i64 sym) {
+        std::vector<double> e;
+        for (auto &pr : pairs2(pa, pi, sym)) e.push_back(Evir[voff[pr.ip - 1] + pr.p] - Eocc[ooff[pr.iq - 1] + pr.q]);
+        return e;
+    };
+    if (p->spin_flip == 1 || p->spin_flip == 2) {
+        bool ab = p->spin_flip == 1;
+        i64 ssym = dp(irrepex, S.symry);
+        std::vector<double> e = ab ? oed(Eb_v, vb, S.vrtb, Ea, oa, S.popa, ssym) : oed(Ea_v, va, S.vrta, Eb_o, ob, S.popb, ssym);
+        if ((i64)e.size() < nroot) return set_error(CPSD_EARG, "more roots than guesses");
+        get_lowest(e, nroot, low);
+        auto pl = ab ? pairs2(S.vrtb, S.popa, ssym) : pairs2(S.vrta, S.popb, ssym);
+        for (i64 k = 0; k < nroot; k++) {
+            rec[k * (1 + vlen)] = e[low[k] - 1];
+            PairIdx x = pl[low[k] - 1];
+            i64 ia = x.ip, ii = x.iq, a = x.p, i = x.q;
+            if (ab) {
+                ia = dp(ia, S.symry);
+                a += S.vrta[ia - 1];
+            } else {
+                ii = dp(ii, S.symry);
+                i += S.popa[ii - 1];
+            }
+            rec[k * (1 + vlen) + 1 + putidx2(S, ia, ii, a, i)] = 1.0;
+        }
+    } else if (p->open_shell) {
+        std::vector<double> e = oed(Ea_v, va, S.vrta, Ea, oa, S.popa, irrepex);
+        i64 n1 = (i64)e.size();
+        std::vector<double> e2 = oed(Eb_v, vb, S.vrtb, Eb_o, ob, S.popb, irrepex);
+        e.insert(e.end(), e2.begin(), e2.end());
+        if ((i64)e.size() < nroot) return set_error(CPSD_EARG, "more roots than guesses");
+        get_lowest(e, nroot, low);
+        auto pa = pairs2(S.vrta, S.popa, irrepex), pb = pairs2(S.vrtb, S.popb, irrepex);
+        for (i64 k = 0; k < nroot; k++) {
+            rec[k * (1 + vlen)] = e[low[k] - 1];
+            i64 ia, ii, a, i;
+            if (low[k] <= n1) {
+                PairIdx x = pa[low[k] - 1];
+                ia = x.ip; ii = x.iq; a = x.p; i = x.q;
+            } else {
+                PairIdx x = pb[low[k] - n1 - 1];
+                ia = dp(x.ip, S.symry); ii = dp(x.iq, S.symry);
+                a = x.p + S.vrta[ia - 1];
+                i = x.q + S.popa[ii - 1];
+            }
+            rec[k * (1 + vlen) + 1 + putidx2(S, ia, ii, a, i)] = 1.0;
+        }
+    } else {
+        std::vector<double> e = oed(Ea_v, va, S.vrta, Ea, oa, S.popa, irrepex);
+        if ((i64)e.size() < nroot) return set_error(CPSD_EARG, "more roots than guesses");
+        get_lowest(e, nroot, low);
+        auto pa = pairs2(S.vrta, S.popa, irrepex);
+        for (i64 k = 0; k < nroot; k++) {
+            rec[k * (1 + vlen)] = e[low[k] - 1];
+            PairIdx x = pa[low[k] - 1];
+            rec[k * (1 + vlen) + 1 + putidx2(S, x.ip, x.iq, x.p, x.q)] = 1.0 / std::sqrt(2.0);
+            i64 ib = dp(x.ip, S.symry), jb = dp(x.iq, S.symry);
+            double val = (p->ex_mult == 3) ? -1.0 / std::sqrt(2.0) : 1.0 / std::sqrt(2.0);
+            rec[k * (1 + vlen) + 1 + putidx2(S, ib, jb, S.vrta[ib - 1] + x.p, S.popa[jb - 1] + x.q)] = val;
+        }
+    }
+    return CPSD_OK;
+}
+
+// Davidson (src/lib_cc/mod_davidson.f90:40-561) for one irrep; fileEV holds
+// the guess records on entry and the roots on exit (device)
+int davidson(const Sys &S, const Ints &I, const cpsd_params *p, i64 sym, i64 nroot, double *fileEV,
+             i64 *iters, double *max_resid) {
+    ScratchScope sc;
+    const i64 n = irpdso(sym, S.popv, S.popo, 1);
+    const i64 D = p->davidson_dim;
+    if (D > DAV_MAXD) return set_error(CPSD_EARG, "davidson_dim above 32");
+    if (nroot >= D) return set_error(CPSD_EARG, "too many roots for davidson_dim");
+    DavBuffers b;
+    double *diag;
+    CPSD_TRY(scratch(n, &diag));
+    for (int k = 0; k < 2; k++) {
+        CPSD_TRY(scratch(D * n, &b.B[k]));
+        CPSD_TRY(scratch(D * n, &b.AB[k]));
+    }
+    CPSD_TRY(scratch(n, &b.w0));
+    CPSD_TRY(scratch(n, &b.w1));
+    b.diag = diag;
+    b.fileEV = fileEV;
+    Desc d = make_desc(S.popv, S.popo, ZORB, ZORB, 1, 1, sym);
+    const EnergyPlan *ep;
+    CPSD_TRY(plan_energy(d, "vozz", &ep));
+    CPSD_TRY(launch_energy(ep, 0, I.eorb, nullptr, diag));  // Eorb_diff1 (OED1)
+    DavState hs;
+    memset(&hs, 0, sizeof hs);
+    hs.D = (int)D;
+    hs.dimA = (int)n;
+    hs.nroot = (int)nroot;
+    hs.lowest = (int)p->lowest;
+    hs.maxcyc = (int)p->davidson_cyc;
+    hs.dimDel = (int)(D - nroot - 5);
+    hs.maxError = std::pow(10.0, -(double)p->davidson_conv);
+    DavState *st;
+    CPSD_TRY(arena().alloc(sizeof(DavState), (void **)&st));
+    CPSD_TRY(cuda_check(cudaMemcpyAsync(st, &hs, sizeof hs, cudaMemcpyHostToDevice, stream()), "dav state"));
+    // initDavidson: b_i = guess_i, Ab_i = A b_i
+    CPSD_TRY(cuda_check(cudaMemcpy2DAsync(b.B[0], n * sizeof(double), fileEV + 1, (n + 1) * sizeof(double),
+                                          n * sizeof(double), nroot, cudaMemcpyDeviceToDevice, stream()),
+                        "guess copy"));
+    CPSD_TRY(cis_sigma(S, I, sym, b.B[0], n, b.AB[0], n, nroot));
+    CPSD_TRY(dav_init_launch(st, b));
+    int *hdr = (int *)mailbox();
+    const size_t hbytes = offsetof(DavState, warn_imag);
+    for (;;) {
+        CPSD_TRY(dav_step_launch(st, b));
+        CPSD_TRY(read_back(hdr, st, hbytes));
+        const DavState *h = (const DavState *)hdr;
+        if (h->done) break;
+        if (h->nNew > 0)
+            CPSD_TRY(cis_sigma(S, I, sym, b.B[h->cur] + (i64)h->newpos * n, n, b.AB[h->cur] + (i64)h->newpos * n, n,
+                               h->nNew));
+        CPSD_TRY(dav_abar_launch(st, b));
+    }
+    if (iters) *iters = ((const DavState *)hdr)->iterations;
+    // eigen test of the converged roots (mod_davidson.f90:525-542)
+    CPSD_TRY(cis_sigma(S, I, sym, fileEV + 1, n + 1, b.AB[0], n, nroot));
+    CPSD_TRY(dav_final_launch(st, b));
+    double mr;
+    CPSD_TRY(read_back(&mr, &st->max_resid, sizeof(double)));
+    if (max_resid) *max_resid = mr;
+    return CPSD_OK;
+}
+
+// ----------------------------------------------------------------- DIIS
+struct Diis {
+    DiisState *st;
+    DiisBuffers b;
+    i64 len;
+};
+int diis_alloc(Diis *d, i64 len, i64 maxdim) {
+    if (maxdim > DIIS_MAXDIM) return set_error(CPSD_EARG, "diis_dim above 16");
+    d->len = len;
+    CPSD_TRY(arena().alloc(sizeof(DiisState), (void **)&d->st));
+    CPSD_TRY(scratch(len, &d->b.prev));
+    CPSD_TRY(scratch(len * maxdim, &d->b.err));
+    CPSD_TRY(scratch(len * maxdim, &d->b.amp));
+    DiisState h{(int)len, (int)maxdim, 1, 1, 1.0};
+    return cuda_check(cudaMemcpyAsync(d->st, &h, sizeof h, cudaMemcpyHostToDevice, stream()), "diis state");
+}
+
+}  // namespace
+}  // namespace cpsd
+
+using namespace cpsd;
+
+extern "C" {
+
+void cpsd_params_default(cpsd_params *p) {
+    memset(p, 0, sizeof *p);
+    p->davidson_dim = 20;
+    p->davidson_cyc = 50;
+    p->davidson_conv = 8;
+    p->lowest = 0;
+    p->diis_dim = 10;
+    p->diis_cyc = 50;
+    p->diis_max_err = 10.0e-8;
+    p->spin_flip = 1;
+    p->open_shell = 1;
+    p->ex_mult = 1;
+    p->batch_roots = 1;
+}
+
+int cpsd_cis_run(const cpsd_system *s, const cpsd_integrals *I, const cpsd_params *p, double *omega_host,
+                 double *R_dev, int64_t *iterations) {
+    Sys S;
+    CPSD_TRY(make_sys(s, &S));
+    Ints X = make_ints(S, I);
+    i64 ne = 0;
+    for (int r = 0; r < 8; r++) ne += S.popo[r] + S.popv[r];
+    std::vector<double> eorb((size_t)ne);
+    CPSD_TRY(read_back(eorb.data(), I->eorb, sizeof(double) * (size_t)ne));
+    i64 kroot = 0, roff = 0, itsum = 0;
+    for (i64 sym = 1; sym <= S.nirrep; sym++) {
+        i64 nroot = p->estate_sym[sym - 1];
+        if (nroot == 0) continue;
+        i64 n = irpdso(sym, S.popv, S.popo, 1);
+        std::vector<double> rec;
+        CPSD_TRY(make_guess(S, eorb, p, sym, nroot, rec));
+        ScratchScope sc;
+        double *fileEV;
+        CPSD_TRY(scratch((i64)rec.size(), &fileEV));
+        CPSD_TRY(cuda_check(cudaMemcpyAsync(fileEV, rec.data(), sizeof(double) * rec.size(), cudaMemcpyHostToDevice,
+                                            stream()),
+                            "guess upload"));
+        i64 it = 0;
+        double mr = 0;
+        CPSD_TRY(davidson(S, X, p, sym, nroot, fileEV, &it, &mr));
+        itsum += it;
+        CPSD_TRY(read_back(rec.data(), fileEV, sizeof(double) * rec.size()));
+        for (i64 k = 0; k < nroot; k++) omega_host[kroot + k] = rec[k * (n + 1)];
+        if (R_dev)
+            CPSD_TRY(cuda_check(cudaMemcpy2DAsync(R_dev + roff, n * sizeof(double), fileEV + 1, (n + 1) * sizeof(double),
+                                                  n * sizeof(double), nroot, cudaMemcpyDeviceToDevice, stream()),
+                                "R copy"));
+        kroot += nroot;
+        roff += n * nroot;
+    }
+    if (iterations) *iterations = itsum;
+    return cuda_check(cudaStreamSynchronize(stream()), "cis sync");
+}
+
+int cpsd_ground(const cpsd_system *s, const cpsd_integrals *I, const cpsd_params *p, double *T2_1, double *T1_2,
+                double *T2_2, double *E2_host, double *E3_host, int64_t *diis_iters) {
+    Sys S;
+    CPSD_TRY(make_sys(s, &S));
+    Ints X = make_ints(S, I);
+    const i64 *o = S.popo, *v = S.popv;
+    ScratchScope sc;
+    i64 l1 = irpdso(1, v, o, 1), l2 = idsymsoc(1, v, v, 0, o, o, 0);
+    double *c1, *c2, *r1, *dE;
+    CPSD_TRY(scratch(l1, &c1));
+    CPSD_TRY(scratch(l2, &c2));
+    CPSD_TRY(scratch(l1, &r1));
+    CPSD_TRY(scratch(2, &dE));
+    Desc d2 = make_desc(v, v, o, o, 0, 0, 1), d1 = make_desc(v, o, ZORB, ZORB, 1, 1, 1);
+    const EnergyPlan *e2, *e1;
+    CPSD_TRY(plan_energy(d2, "vvoo", &e2));
+    CPSD_TRY(plan_energy(d1, "vozz", &e1));
+    // run1 (src/CPSd.SF/run1.f90:20-36): T2^(1) = <ab||ij>/D, E^(2) = T2.abij
+    CPSD_TRY(launch_energy(e2, 2, X.eorb, I->abij, T2_1));
+    CPSD_TRY(launch_dot(T2_1, I->abij, l2, dE, true));
+    // run2 (src/CPSd.SF/run2.f90:8-95)
+    Ten t2 = ten(v, v, o, o, 0, 0, 1, T2_1), t1 = ten(v, o, ZORB, ZORB, 1, 1, 1, T1_2);
+    Ten C1 = ten(v, o, ZORB, ZORB, 1, 1, 1, c1), C2 = ten(v, v, o, o, 0, 0, 1, c2);
+    Ten R1 = ten(v, o, ZORB, ZORB, 1, 1, 1, r1);
+    CPSD_TRY(zero(c1, l1));
+    CPSD_TRY(zero(c2, l2));
+    CPSD_TRY(k_c1_r2abci(C1, t2, X.abci, 1.0));
+    CPSD_TRY(k_c1_r2ijka(C1, t2, X.ijka, 1.0));
+    CPSD_TRY(k_c2_r2Wmbej(C2, t2, X.iabj, 1.0));
+    CPSD_TRY(k_c2_r2Wmnij(C2, t2, X.ijkl, 1.0));
+    CPSD_TRY(k_c2_r2abcd(C2, t2, X.abcd, 1.0));
+    CPSD_TRY(launch_energy(e2, 2, X.eorb, c2, T2_2));
+    CPSD_TRY(launch_copy(r1, c1, l1));
+    Diis dd;
+    CPSD_TRY(diis_alloc(&dd, l1, p->diis_dim));
+    i64 iter = 0;
+    for (;;) {
+        iter++;
+        CPSD_TRY(launch_energy(e1, 3, X.eorb, r1, T1_2));
+        CPSD_TRY(diis_step_launch(dd.st, dd.b, (int)iter, T1_2));
+        double res;
+        CPSD_TRY(read_back(&res, &dd.st->res, sizeof res));
+        if (iter > 1 && std::fabs(res) < p->diis_max_err) break;
+        if (iter > p->diis_cyc) break;
+        CPSD_TRY(launch_copy(r1, c1, l1));
+        CPSD_TRY(k_c1_r1iabj(R1, t1, X.iabj, 1.0));
+    }
+    if (diis_iters) *diis_iters = iter;
+    CPSD_TRY(launch_dot(T2_2, I->abij, l2, dE + 1, true));
+    double h[2];
+    CPSD_TRY(read_back(h, dE, sizeof h));
+    if (E2_host) *E2_host = h[0];
+    if (E3_host) *E3_host = h[1];
+    return CPSD_OK;
+}
+
+int cpsd_calJ(const cpsd_system *s, const cpsd_integrals *I, const double *T2_1, const double *T1_2,
+              const double *T2_2, cpsd_jints *J) {
+    Sys S;
+    CPSD_TRY(make_sys(s, &S));
+    Ints X = make_ints(S, I);
+    const i64 *o = S.popo, *v = S.popv;
+    Ten t2a = ten(v, v, o, o, 0, 0, 1, (double *)T2_1), t1b = ten(v, o, ZORB, ZORB, 1, 1, 1, (double *)T1_2);
+    Ten t2b = ten(v, v, o, o, 0, 0, 1, (double *)T2_2);
+    Ten foo = ten(o, o, ZORB, ZORB, 1, 1, 1, J->J2_Foo), fvv = ten(v, v, ZORB, ZORB, 1, 1, 1, J->J2_Fvv);
+    Ten wvo = ten(v, o, v, o, 1, 1, 1, J->J2_Wovvo), woo = ten(o, o, o, v, 0, 1, 1, J->J2_Wovoo);
+    Ten foo3 = ten(o, o, ZORB, ZORB, 1, 1, 1, J->J3_Foo), fvv3 = ten(v, v, ZORB, ZORB, 1, 1, 1, J->J3_Fvv);
+    Ten wvo3 = ten(v, o, v, o, 1, 1, 1, J->J3_Wovvo);
+    for (Ten *t : {&foo, &fvv, &wvo, &woo, &foo3, &fvv3, &wvo3}) CPSD_TRY(zero(t->arr, t->len()));
+    // calJ2 (calJ.f90:6-99)
+    CPSD_TRY(k_Fmi_r2abij(foo, t2a, X.abij, 1.0));
+    CPSD_TRY(k_Fae_r2abij(fvv, t2a, X.abij, 1.0));
+    CPSD_TRY(k_Wkbij_r2ijka(woo, t2a, X.ijka, 1.0));
+    CPSD_TRY(k_Wkbij_r2abci(woo, t2a, X.abci, 1.0));
+    CPSD_TRY(k_Wmbej_r2abij(wvo, t2a, X.abij, 2.0));
+    // calJ3 (calJ.f90:104-228)
+    CPSD_TRY(k_Fmi_r1ijka(foo3, t1b, X.ijka, 1.0));
+    CPSD_TRY(k_Fmi_r2abij(foo3, t2b, X.abij, 1.0));
+    CPSD_TRY(k_Fae_r1abci(fvv3, t1b, X.abci, 1.0));
+    CPSD_TRY(k_Fae_r2abij(fvv3, t2b, X.abij, 1.0));
+    CPSD_TRY(k_Wmbej_r1ijka(wvo3, t1b, X.ijka, 1.0));
+    CPSD_TRY(k_Wmbej_r1abci(wvo3, t1b, X.abci, 1.0));
+    CPSD_TRY(k_Wmbej_r2abij(wvo3, t2b, X.abij, 2.0));
+    return cuda_check(cudaGetLastError(), "calJ");
+}
+
+// EE-CPS(D-3) for nb roots of irrep symR sharing every contraction launch
+static int ee_roots_batch(const Sys &S, const Ints &X, const cpsd_params *p, const double *T2_1,
+                          const cpsd_jints *J, i64 symR, i64 nb, const double *w0_host, const double *L,
+                          double *w_host, double *R2_1o, double *R1_2o, double *R2_2o, i64 *sit_out) {
+    const i64 *o = S.popo, *v = S.popv;
+    ScratchScope sc;
+    const i64 l1 = irpdso(symR, v, o, 1), l2 = idsymsoc(symR, v, v, 0, o, o, 0);
+    double *c1, *c2, *cn1, *cn2, *r21, *r12, *r22, *w0d, *wd;
+    CPSD_TRY(scratch(nb * l1, &c1));
+    CPSD_TRY(scratch(nb * l2, &c2));
+    CPSD_TRY(scratch(nb * l1, &cn1));
+    CPSD_TRY(scratch(nb * l2, &cn2));
+    CPSD_TRY(scratch(nb * l2, &r21));
+    CPSD_TRY(scratch(nb * l1, &r12));
+    CPSD_TRY(scratch(nb * l2, &r22));
+    CPSD_TRY(scratch(nb, &w0d));
+    CPSD_TRY(scratch(3 * nb, &wd));
+    CPSD_TRY(cuda_check(cudaMemcpyAsync(w0d, w0_host, sizeof(double) * nb, cudaMemcpyHostToDevice, stream()), "w0"));
+    Ten Lt = ten(v, o, ZORB, ZORB, 1, 1, symR, (double *)L, l1);
+    Ten C1 = ten(v, o, ZORB, ZORB, 1, 1, symR, c1, l1), C2 = ten(v, v, o, o, 0, 0, symR, c2, l2);
+    Ten R21 = ten(v, v, o, o, 0, 0, symR, r21, l2), R22 = ten(v, v, o, o, 0, 0, symR, r22, l2);
+    Ten T2 = ten(v, v, o, o, 0, 0, 1, (double *)T2_1);
+    Ten jfoo = ten(o, o, ZORB, ZORB, 1, 1, 1, J->J2_Foo), jfvv = ten(v, v, ZORB, ZORB, 1, 1, 1, J->J2_Fvv);
+    Ten jwvo = ten(v, o, v, o, 1, 1, 1, J->J2_Wovvo), jwoo = ten(o, o, o, v, 0, 1, 1, J->J2_Wovoo);
+    Ten j3foo = ten(o, o, ZORB, ZORB, 1, 1, 1, J->J3_Foo), j3fvv = ten(v, v, ZORB, ZORB, 1, 1, 1, J->J3_Fvv);
+    Ten j3wvo = ten(v, o, v, o, 1, 1, 1, J->J3_Wovvo);
+    Desc d2 = make_desc(v, v, o, o, 0, 0, symR), d1 = make_desc(v, o, ZORB, ZORB, 1, 1, symR);
+    const EnergyPlan *e2, *e1;
+    CPSD_TRY(plan_energy(d2, "vvoo", &e2));
+    CPSD_TRY(plan_energy(d1, "vozz", &e1));
+    auto energies = [&](int order) -> int {  // w^(n) = L . C1^(n), compensated sum
+        for (i64 r = 0; r < nb; r++)
+            CPSD_TRY(launch_dot(L + r * l1, c1 + r * l1, l1, wd + (order - 1) * nb + r, true));
+        return CPSD_OK;
+    };
+    // ---- order 1: C^(1) = J^(1) R^(0) (calE_C.f90:37-52): calC2_VR1
+    CPSD_TRY(zero(c1, nb * l1));
+    CPSD_TRY(zero(c2, nb * l2));
+    CPSD_TRY(k_c2_r1ijka(C2, Lt, X.ijka, 1.0, nb));
+    CPSD_TRY(k_c2_r1abci(C2, Lt, X.abci, 1.0, nb));
+    CPSD_TRY(energies(1));
+    CPSD_TRY(launch_copy(cn1, c1, nb * l1));
+    CPSD_TRY(launch_copy(cn2, c2, nb * l2));
+    // ---- order 2: R^(1) = (0, -C2^(1)/(e2 - w0)) (calV_C.f90, run_order.f90:54-66)
+    CPSD_TRY(launch_copy(r21, cn2, nb * l2));
+    CPSD_TRY(launch_scale(r21, nb * l2, -1.0));
+    CPSD_TRY(launch_energy(e2, 1, X.eorb, r21, r21, w0d, nb, l2, l2));
+    CPSD_TRY(zero(c1, nb * l1));
+    CPSD_TRY(zero(c2, nb * l2));
+    CPSD_TRY(k_c1_r2abci(C1, R21, X.abci, 1.0, nb));  // calC1_VR2
+    CPSD_TRY(k_c1_r2ijka(C1, R21, X.ijka, 1.0, nb));
+    CPSD_TRY(k_c2_r2Wmbej(C2, R21, X.iabj, 1.0, nb));  // calC2_VR2
+    CPSD_TRY(k_c2_r2Wmnij(C2, R21, X.ijkl, 1.0, nb));
+    CPSD_TRY(k_c2_r2abcd(C2, R21, X.abcd, 1.0, nb));
+    CPSD_TRY(k_c2_r1ijka(C2, Lt, jwoo, 1.0, nb));  // calC_J2R (calC_JR.f90:4-52)
+    CPSD_TRY(k_c1_r1iabj(C1, Lt, jwvo, 1.0, nb));
+    CPSD_TRY(k_c1_r1Fmi(C1, Lt, jfoo, 1.0, nb));
+    CPSD_TRY(k_c1_r1Fae(C1, Lt, jfvv, 1.0, nb));
+    {  // calC_VTR (calC_VTR.f90:6-111) with T^(1) = (0, T2^(1))
+        ScratchScope s2;
+        double *t;
+        Ten w = ten(o, o, o, o, 0, 0, symR, nullptr);
+        CPSD_TRY(scratch(nb * w.len(), &t));
+        w.arr = t;
+        w.bs = w.len();
+        CPSD_TRY(zero(t, nb * w.len()));
+        CPSD_TRY(k_Wmnij_r1ijka(w, Lt, X.ijka, 1.0, nb));
+        CPSD_TRY(k_c2_r2Wmnij(C2, T2, w, 1.0, nb));
+        Ten m = ten(v, o, v, o, 1, 1, symR, nullptr);
+        CPSD_TRY(scratch(nb * m.len(), &t));
+        m.arr = t;
+        m.bs = m.len();
+        CPSD_TRY(zero(t, nb * m.len()));
+        CPSD_TRY(k_Wmbej_r1abci(m, Lt, X.abci, 1.0, nb));
+        CPSD_TRY(k_c2_r2Wmbej(C2, T2, m, 1.0, nb));
+        Ten g = ten(o, o, ZORB, ZORB, 1, 1, symR, nullptr);
+        CPSD_TRY(scratch(nb * g.len(), &t));
+        g.arr = t;
+        g.bs = g.len();
+        CPSD_TRY(zero(t, nb * g.len()));
+        CPSD_TRY(k_Fmi_r1ijka(g, Lt, X.ijka, 1.0, nb));
+        CPSD_TRY(k_c2_r2Fmi(C2, T2, g, 1.0, nb));
+        Ten gv = ten(v, v, ZORB, ZORB, 1, 1, symR, nullptr);
+        CPSD_TRY(scratch(nb * gv.len(), &t));
+        gv.arr = t;
+        gv.bs = gv.len();
+        CPSD_TRY(zero(t, nb * gv.len()));
+        CPSD_TRY(k_Fae_r1abci(gv, Lt, X.abci, 1.0, nb));
+        CPSD_TRY(k_c2_r2Fae(C2, T2, gv, 1.0, nb));
+    }
+    CPSD_TRY(energies(2));
+    CPSD_TRY(launch_copy(cn1, c1, nb * l1));
+    CPSD_TRY(launch_copy(cn2, c2, nb * l2));
+    // ---- order 3: Ctilde^(2) = w^(2) R^(0) - C^(2)
+    CPSD_TRY(launch_scale(cn1, nb * l1, -1.0));
+    CPSD_TRY(launch_axpy_dev(l1, wd + nb, 1.0, L, cn1, nb, l1, l1));
+    CPSD_TRY(launch_copy(r22, cn2, nb * l2));
+    CPSD_TRY(launch_scale(r22, nb * l2, -1.0));
+    CPSD_TRY(launch_energy(e2, 1, X.eorb, r22, r22, w0d, nb, l2, l2));
+    // solver (solver.f90:4-66): (A - w0) R1 = Ctilde1, orthogonal to L, per root
+    i64 sit = 0;
+    for (i64 r = 0; r < nb; r++) {
+        ScratchScope s3;
+        double *cc = cn1 + r * l1, *R1 = r12 + r * l1, *pr;
+        CPSD_TRY(scratch(l1, &pr));
+        CPSD_TRY(launch_scale(cc, l1, -1.0));
+        CPSD_TRY(launch_copy(pr, cc, l1));
+        Diis dd;
+        CPSD_TRY(diis_alloc(&dd, l1, p->diis_dim));
+        Ten tR1 = ten(v, o, ZORB, ZORB, 1, 1, symR, R1), tpr = ten(v, o, ZORB, ZORB, 1, 1, symR, pr);
+        i64 iter = 0;
+        for (;;) {
+            iter++;
+            CPSD_TRY(launch_energy(e1, 3, X.eorb, pr, R1));
+            CPSD_TRY(orth_launch(R1, L + r * l1, l1));
+            CPSD_TRY(diis_step_launch(dd.st, dd.b, (int)iter, R1));
+            CPSD_TRY(orth_launch(R1, L + r * l1, l1));
+            double res;
+            CPSD_TRY(read_back(&res, &dd.st->res, sizeof res));
+            if (iter > 1 && std::fabs(res) < p->diis_max_err) break;
+            if (iter > p->diis_cyc) break;
+            CPSD_TRY(launch_copy(pr, cc, l1));
+            CPSD_TRY(launch_axpy(l1, -w0_host[r], R1, pr));
+            CPSD_TRY(k_c1_r1iabj(tpr, tR1, X.iabj, 1.0));
+        }
+        sit += iter;
+    }
+    // C^(3) = J^(1) R^(2) + J^(3) R^(0), C1 only (calE_C.f90:37-79)
+    CPSD_TRY(zero(c1, nb * l1));
+    CPSD_TRY(k_c1_r2abci(C1, R22, X.abci, 1.0, nb));
+    CPSD_TRY(k_c1_r2ijka(C1, R22, X.ijka, 1.0, nb));
+    CPSD_TRY(k_c1_r1iabj(C1, Lt, j3wvo, 1.0, nb));  // calC_J3R (calC_JR.f90:56-106)
+    CPSD_TRY(k_c1_r1Fmi(C1, Lt, j3foo, 1.0, nb));
+    CPSD_TRY(k_c1_r1Fae(C1, Lt, j3fvv, 1.0, nb));
+    CPSD_TRY(energies(3));
+    std::vector<double> wh((size_t)(3 * nb));
+    CPSD_TRY(read_back(wh.data(), wd, sizeof(double) * wh.size()));
+    for (i64 r = 0; r < nb; r++)
+        for (int k = 0; k < 3; k++) w_host[3 * r + k] = wh[k * nb + r];
+    if (R2_1o) CPSD_TRY(launch_copy(R2_1o, r21, nb * l2));
+    if (R1_2o) CPSD_TRY(launch_copy(R1_2o, r12, nb * l1));
+    if (R2_2o) CPSD_TRY(launch_copy(R2_2o, r22, nb * l2));
+    if (sit_out) *sit_out = sit;
+    return cuda_check(cudaStreamSynchronize(stream()), "ee sync");
+}
+
+int cpsd_eecpsd_roots(const cpsd_system *s, const cpsd_integrals *I, const cpsd_params *p, const double *T2_1,
+                      const cpsd_jints *J, int64_t symR, int64_t nroot, const double *w0_host, const double *L_dev,
+                      double *w_host, double *R2_1, double *R1_2, double *R2_2, int64_t *solver_iters) {
+    Sys S;
+    CPSD_TRY(make_sys(s, &S));
+    Ints X = make_ints(S, I);
+    if (nroot <= 0) return CPSD_OK;
+    const i64 l1 = irpdso(symR, S.popv, S.popo, 1), l2 = idsymsoc(symR, S.popv, S.popv, 0, S.popo, S.popo, 0);
+    if (p->batch_roots) {
+        i64 it = 0;
+        CPSD_TRY(ee_roots_batch(S, X, p, T2_1, J, symR, nroot, w0_host, L_dev, w_host, R2_1, R1_2, R2_2, &it));
+        if (solver_iters) *solver_iters = it;
+        return CPSD_OK;
+    }
+    i64 tot = 0;
+    for (i64 r = 0; r < nroot; r++) {
+        i64 it = 0;
+        CPSD_TRY(ee_roots_batch(S, X, p, T2_1, J, symR, 1, w0_host + r, L_dev + r * l1, w_host + 3 * r,
+                                R2_1 ? R2_1 + r * l2 : nullptr, R1_2 ? R1_2 + r * l1 : nullptr,
+                                R2_2 ? R2_2 + r * l2 : nullptr, &it));
+        tot += it;
+    }
+    if (solver_iters) *solver_iters = tot;
+    return CPSD_OK;
+}
+
+int cpsd_pipeline(const cpsd_system *s, const cpsd_integrals *I, const cpsd_params *p, double *omega_cis,
+                  double *w2, double *w3, int64_t *nroots) {
+    Sys S;
+    CPSD_TRY(make_sys(s, &S));
+    const i64 *o = S.popo, *v = S.popv;
+    i64 nroot = 0, rlen = 0;
+    for (i64 sym = 1; sym <= S.nirrep; sym++) {
+        nroot += p->estate_sym[sym - 1];
+        rlen += p->estate_sym[sym - 1] * irpdso(sym, v, o, 1);
+    }
+    ScratchScope sc;
+    double *R;
+    CPSD_TRY(scratch(rlen, &R));
+    CPSD_TRY(cpsd_cis_run(s, I, p, omega_cis, R, nullptr));
+    const i64 l1 = irpdso(1, v, o, 1), l2 = idsymsoc(1, v, v, 0, o, o, 0);
+    double *T2_1, *T1_2, *T2_2;
+    CPSD_TRY(scratch(l2, &T2_1));
+    CPSD_TRY(scratch(l1, &T1_2));
+    CPSD_TRY(scratch(l2, &T2_2));
+    double E2, E3;
+    CPSD_TRY(cpsd_ground(s, I, p, T2_1, T1_2, T2_2, &E2, &E3, nullptr));
+    cpsd_jints J;
+    CPSD_TRY(scratch(irpdso(1, o, o, 1), &J.J2_Foo));
+    CPSD_TRY(scratch(irpdso(1, v, v, 1), &J.J2_Fvv));
+    CPSD_TRY(scratch(idsymsoc(1, v, o, 1, v, o, 1), &J.J2_Wovvo));
+    CPSD_TRY(scratch(idsymsoc(1, o, o, 0, o, v, 1), &J.J2_Wovoo));
+    CPSD_TRY(scratch(irpdso(1, o, o, 1), &J.J3_Foo));
+    CPSD_TRY(scratch(irpdso(1, v, v, 1), &J.J3_Fvv));
+    CPSD_TRY(scratch(idsymsoc(1, v, o, 1, v, o, 1), &J.J3_Wovvo));
+    CPSD_TRY(cpsd_calJ(s, I, T2_1, T1_2, T2_2, &J));
+    i64 k = 0, roff = 0;
+    std::vector<double> w;
+    for (i64 sym = 1; sym <= S.nirrep; sym++) {
+        i64 nr = p->estate_sym[sym - 1];
+        if (nr == 0) continue;
+        i64 len = irpdso(sym, v, o, 1);
+        w.assign((size_t)(3 * nr), 0.0);
+        CPSD_TRY(cpsd_eecpsd_roots(s, I, p, T2_1, &J, sym, nr, omega_cis + k, R + roff, w.data(), nullptr, nullptr,
+                                   nullptr, nullptr));
+        for (i64 r = 0; r < nr; r++) {
+            w2[k + r] = w[3 * r + 1];
+            w3[k + r] = w[3 * r + 2];
+        }
+        k += nr;
+        roff += len * nr;
+    }
+    if (nroots) *nroots = nroot;
+    return CPSD_OK;
+}
+
+}  // extern "C"

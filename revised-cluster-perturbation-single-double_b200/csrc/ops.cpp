@@ -1,0 +1,564 @@
+// DPD engine entry points, layout transforms, the mod_contract wrappers and
+// the spin-free lib_cc kernels (device side: libcpsd_b200).
+#include "ops.hpp"
+
+#include <cstring>
+#include <string>
+
+namespace cpsd {
+
+Ten ten_of(const cpsd_opt *t) {
+    Ten x;
+    x.d = desc_of(t);
+    x.arr = t->arr;
+    return x;
+}
+
+Ten ten(const i64 *p0, const i64 *p1, const i64 *p2, const i64 *p3, i64 iop0, i64 iop1, i64 sym, double *arr,
+        i64 bs) {
+    Ten x;
+    x.d = make_desc(p0, p1, p2, p3, iop0, iop1, sym);
+    x.arr = arr;
+    x.bs = bs;
+    return x;
+}
+
+static int need_init() {
+    if (!ctx().init) return set_error(CPSD_ESTATE, "cpsd_init has not been called");
+    return CPSD_OK;
+}
+
+int engine(const Ten &v1, const char *t1, const Ten &v2, const char *t2, Ten &v3, const char *t3, double f1,
+           double f2, i64 nb) {
+    CPSD_TRY(need_init());
+    Batch b;
+    b.nb = nb;
+    if (nb > 1) {
+        b.strideA = v1.bs;
+        b.strideB = v2.bs;
+        b.strideC = v3.bs ? v3.bs : v3.len();
+    }
+    const ContractPlan *p;
+    CPSD_TRY(plan_contract(v1.d, t1, v2.d, t2, v3.d, t3, b, &p));
+    i64 l3 = v3.len();
+    if (f2 != 1.0) {
+        if (nb <= 1 || b.strideC == l3) CPSD_TRY(launch_scale(v3.arr, l3 * (nb > 1 ? nb : 1), f2));
+        else
+            for (i64 c = 0; c < nb; c++) CPSD_TRY(launch_scale(v3.arr + c * b.strideC, l3, f2));
+    }
+    return launch_contract(p, v1.arr, v2.arr, v3.arr, f1);
+}
+
+namespace {
+
+bool check_flat(const char *cur, const char pairs[][2], int n, int self) {
+    for (int i = 0; i < n; i++) {
+        if (i == self) continue;
+        if (pairs[i][0] == cur[0] && pairs[i][1] == cur[1]) return false;
+    }
+    return true;
+}
+
+// iexpso into scratch: expanded copy (batched when v is)
+int expand(const Ten &v, bool e0, bool e1, i64 nb, Ten *out) {
+    *out = v;
+    if (!e0 && !e1) return CPSD_OK;
+    const PairMapPlan *pm;
+    Desc d;
+    CPSD_TRY(plan_pairmap(v.d, e0 ? PAIR_EXPAND : PAIR_ID, e1 ? PAIR_EXPAND : PAIR_ID, 1, 1, &d, &pm));
+    i64 n = d.len(), copies = v.bs ? nb : 1;
+    double *buf;
+    CPSD_TRY(scratch(n * copies, &buf));
+    CPSD_TRY(launch_pairmap(pm, v.arr, buf, 1.0, 0.0, copies, v.bs, n));
+    out->d = d;
+    out->arr = buf;
+    out->bs = v.bs ? n : 0;
+    return CPSD_OK;
+}
+
+// v3 += P(X): antisymmetrise / compress pairs of the full-ish result X
+int finish(const Ten &X, Ten &v3, bool anti0, bool anti1, bool comp0, bool comp1, i64 nb) {
+    int op0 = anti0 ? (comp0 ? PAIR_ANTI_COMPRESS : PAIR_ANTI) : (comp0 ? PAIR_COMPRESS : PAIR_ID);
+    int op1 = anti1 ? (comp1 ? PAIR_ANTI_COMPRESS : PAIR_ANTI) : (comp1 ? PAIR_COMPRESS : PAIR_ID);
+    const PairMapPlan *pm;
+    Desc d;
+    CPSD_TRY(plan_pairmap(X.d, op0, op1, v3.d.iop[0], v3.d.iop[1], &d, &pm));
+    if (d.iop[0] != v3.d.iop[0] || d.iop[1] != v3.d.iop[1]) return set_error(CPSD_ELAYOUT, "result layout mismatch");
+    i64 s3 = nb > 1 ? (v3.bs ? v3.bs : v3.len()) : 0;
+    return launch_pairmap(pm, X.arr, v3.arr, 1.0, 1.0, nb, X.bs, s3);
+}
+
+void pad(const char *t, int n, const char *tail, char out[5]) {
+    for (int i = 0; i < 4; i++) out[i] = i < n ? t[i] : tail[i - n];
+    out[4] = 0;
+}
+
+}  // namespace
+
+// vv2v_444 (src/lib_cc/mod_contract.f90:10-162): v3 += fact * P1 P2 {v1 v2}
+int w444(const Ten &v1, const Ten &v2, Ten &v3, double fact, const char *t1, const char *t2, const char *t3,
+         i64 anti, i64 nb) {
+    if (anti < 0 || anti > 3) return set_error(CPSD_EARG, "vv2v_444: anti must be 0..3");
+    const char pair[6][2] = {{t1[0], t1[1]}, {t1[2], t1[3]}, {t2[0], t2[1]},
+                             {t2[2], t2[3]}, {t3[0], t3[1]}, {t3[2], t3[3]}};
+    i64 iop[6] = {v1.d.iop[0], v1.d.iop[1], v2.d.iop[0], v2.d.iop[1], v3.d.iop[0], v3.d.iop[1]};
+    bool iexp[6] = {};
+    for (int i = 0; i < 6; i++)
+        if (check_flat(pair[i], pair, 6, i) && iop[i] != 1) {
+            iexp[i] = true;
+            iop[i] = 1;
+        }
+    if (anti == 0 && (iexp[4] || iexp[5]))
+        return set_error(CPSD_ELAYOUT, "vv2v_444: packed result pair needs antisymmetrisation");
+    ScratchScope sc;
+    Ten e1, e2;
+    CPSD_TRY(expand(v1, iexp[0], iexp[1], nb, &e1));
+    CPSD_TRY(expand(v2, iexp[2], iexp[3], nb, &e2));
+    if (anti == 0) return engine(e1, t1, e2, t2, v3, t3, fact, 1.0, nb);
+    Ten X = v3;
+    X.d.iop[0] = iop[4];
+    X.d.iop[1] = iop[5];
+    i64 n = X.d.len();
+    CPSD_TRY(scratch(n * nb, &X.arr));
+    X.bs = nb > 1 ? n : 0;
+    CPSD_TRY(launch_scale(X.arr, n * nb, 0.0));
+    CPSD_TRY(engine(e1, t1, e2, t2, X, t3, fact, 1.0, nb));
+    return finish(X, v3, anti == 1 || anti == 3, anti == 2 || anti == 3, iexp[4], iexp[5], nb);
+}
+
+// vv2v_424 (src/lib_cc/mod_contract.f90:220-367)
+int w424(const Ten &v1, const Ten &v2, Ten &v3, double fact, const char *t1, const char *t2, const char *t3,
+         i64 anti, i64 nb) {
+    if (anti < 0 || anti > 2) return set_error(CPSD_EARG, "vv2v_424: anti must be 0..2");
+    const char pair[4][2] = {{t1[0], t1[1]}, {t1[2], t1[3]}, {t3[0], t3[1]}, {t3[2], t3[3]}};
+    i64 iop[4] = {v1.d.iop[0], v1.d.iop[1], v3.d.iop[0], v3.d.iop[1]};
+    bool iexp[4] = {};
+    for (int i = 0; i < 4; i++)
+        if (check_flat(pair[i], pair, 4, i) && iop[i] != 1) {
+            iexp[i] = true;
+            iop[i] = 1;
+        }
+    if ((anti != 1 && iexp[2]) || (anti != 2 && iexp[3]))
+        return set_error(CPSD_ELAYOUT, "vv2v_424: an expanded result pair must be antisymmetrised");
+    char n2[5];
+    pad(t2, 2, "..", n2);
+    ScratchScope sc;
+    Ten e1;
+    CPSD_TRY(expand(v1, iexp[0], iexp[1], nb, &e1));
+    if (anti == 0) return engine(e1, t1, v2, n2, v3, t3, fact, 1.0, nb);
+    Ten X = v3;
+    X.d.iop[0] = iop[2];
+    X.d.iop[1] = iop[3];
+    i64 n = X.d.len();
+    CPSD_TRY(scratch(n * nb, &X.arr));
+    X.bs = nb > 1 ? n : 0;
+    CPSD_TRY(launch_scale(X.arr, n * nb, 0.0));
+    CPSD_TRY(engine(e1, t1, v2, n2, X, t3, fact, 1.0, nb));
+    return finish(X, v3, anti == 1, anti == 2, iexp[2], iexp[3], nb);
+}
+
+// vv2v_442 (src/lib_cc/mod_contract.f90:369-455)
+int w442(const Ten &v1, const Ten &v2, Ten &v3, double fact, const char *t1, const char *t2, const char *t3,
+         i64 nb) {
+    const char pair[4][2] = {{t1[0], t1[1]}, {t1[2], t1[3]}, {t2[0], t2[1]}, {t2[2], t2[3]}};
+    i64 iop[4] = {v1.d.iop[0], v1.d.iop[1], v2.d.iop[0], v2.d.iop[1]};
+    bool iexp[4] = {};
+    for (int i = 0; i < 4; i++)
+        if (check_flat(pair[i], pair, 4, i) && iop[i] != 1) iexp[i] = true;
+    char n3[5];
+    pad(t3, 2, "..", n3);
+    ScratchScope sc;
+    Ten e1, e2;
+    CPSD_TRY(expand(v1, iexp[0], iexp[1], nb, &e1));
+    CPSD_TRY(expand(v2, iexp[2], iexp[3], nb, &e2));
+    return engine(e1, t1, e2, t2, v3, n3, fact, 1.0, nb);
+}
+
+// vv2v_422 (src/lib_cc/mod_contract.f90:184-200)
+int w422(const Ten &v1, const Ten &v2, Ten &v3, double fact, const char *t1, const char *t2, const char *t3,
+         i64 nb) {
+    char b[5], c[5];
+    pad(t2, 2, "+-", b);
+    pad(t3, 2, "+-", c);
+    return w444(v1, v2, v3, fact, t1, b, c, 0, nb);
+}
+
+// vv2v_222 (src/lib_cc/mod_contract.f90:166-182)
+int w222(const Ten &v1, const Ten &v2, Ten &v3, double fact, const char *t1, const char *t2, const char *t3,
+         i64 nb) {
+    char a[5], b[5], c[5];
+    pad(t1, 2, "=+", a);
+    pad(t2, 2, "=-", b);
+    pad(t3, 2, "+-", c);
+    return w444(v1, v2, v3, fact, a, b, c, 0, nb);
+}
+
+// vv2v_224 (src/lib_cc/mod_contract.f90:202-218)
+int w224(const Ten &v1, const Ten &v2, Ten &v3, double fact, const char *t1, const char *t2, const char *t3,
+         i64 anti, i64 nb) {
+    char a[5], b[5];
+    pad(t1, 2, "+-", a);
+    pad(t2, 2, "+-", b);
+    return w444(v1, v2, v3, fact, a, b, t3, anti, nb);
+}
+
+// ------------------------------------------------ lib_cc kernels (spin-free)
+int k_c1_r1iabj(Ten &c1, const Ten &r1, const Ten &V, double f, i64 nb) {
+    return w422(V, r1, c1, f, "fnai", "fn", "ai", nb);
+}
+int k_c1_r1Fae(Ten &c1, const Ten &r1, const Ten &F, double f, i64 nb) {
+    return w222(F, r1, c1, f, "ae", "ei", "ai", nb);
+}
+int k_c1_r1Fmi(Ten &c1, const Ten &r1, const Ten &F, double f, i64 nb) {
+    return w222(r1, F, c1, -f, "am", "mi", "ai", nb);
+}
+int k_c1_r2abci(Ten &c1, const Ten &r2, const Ten &V, double f, i64 nb) {
+    return w442(V, r2, c1, r2.d.iop[0] == 0 ? f : 0.5 * f, "feam", "feim", "ai", nb);
+}
+int k_c1_r2ijka(Ten &c1, const Ten &r2, const Ten &V, double f, i64 nb) {
+    return w442(r2, V, c1, r2.d.iop[1] == 0 ? -f : -0.5 * f, "aemn", "mnie", "ai", nb);
+}
+int k_c2_r1abci(Ten &c2, const Ten &r1, const Ten &V, double f, i64 nb) {
+    return w424(V, r1, c2, f, "abej", "ei", "abij", 2, nb);
+}
+int k_c2_r1ijka(Ten &c2, const Ten &r1, const Ten &V, double f, i64 nb) {
+    return w424(V, r1, c2, -f, "ijmb", "am", "abij", 1, nb);
+}
+int k_c2_r2Wmbej(Ten &c2, const Ten &r2, const Ten &W, double f, i64 nb) {
+    return w444(r2, W, c2, f, "aeim", "embj", "abij", 3, nb);
+}
+int k_c2_r2Wmnij(Ten &c2, const Ten &r2, const Ten &W, double f, i64 nb) {
+    return w444(r2, W, c2, r2.d.iop[0] == 0 ? f : 0.5 * f, "abmn", "mnij", "abij", 0, nb);
+}
+int k_c2_r2abcd(Ten &c2, const Ten &r2, const Ten &V, double f, i64 nb) {
+    return w444(V, r2, c2, r2.d.iop[0] == 1 ? 0.5 * f : f, "abef", "efij", "abij", 0, nb);
+}
+int k_c2_r2Fae(Ten &c2, const Ten &r2, const Ten &F, double f, i64 nb) {
+    return w424(r2, F, c2, f, "aeij", "be", "abij", 1, nb);
+}
+int k_c2_r2Fmi(Ten &c2, const Ten &r2, const Ten &F, double f, i64 nb) {
+    return w424(r2, F, c2, -f, "abim", "mj", "abij", 2, nb);
+}
+int k_Fmi_r2abij(Ten &F, const Ten &r2, const Ten &V, double f, i64 nb) {
+    return w442(V, r2, F, r2.d.iop[0] == 1 ? 0.5 * f : f, "efmn", "efin", "mi", nb);
+}
+int k_Fae_r2abij(Ten &F, const Ten &r2, const Ten &V, double f, i64 nb) {
+    return w442(r2, V, F, r2.d.iop[1] == 0 ? -f : -0.5 * f, "afmn", "efmn", "ae", nb);
+}
+int k_Fmi_r1ijka(Ten &F, const Ten &r1, const Ten &V, double f, i64 nb) {
+    return w422(V, r1, F, f, "mnie", "en", "mi", nb);
+}
+int k_Fae_r1abci(Ten &F, const Ten &r1, const Ten &V, double f, i64 nb) {
+    return w422(V, r1, F, f, "efam", "fm", "ae", nb);
+}
+int k_Wkbij_r2ijka(Ten &W, const Ten &r2, const Ten &V, double f, i64 nb) {
+    return w444(V, r2, W, f, "klic", "bcjl", "ijkb", 1, nb);
+}
+// Wkbij_r2abci.f90:3-43: tmp(ij,bk) = -.5 V(cd,bk) r(cd,ij); W(ij,kb) += tmp(ij,bk)
+int k_Wkbij_r2abci(Ten &W, const Ten &r2, const Ten &V, double f, i64 nb) {
+    ScratchScope sc;
+    Ten tmp = W;
+    std::swap(tmp.d.pop[2], tmp.d.pop[3]);
+    tmp.d.iop[1] = 1;
+    i64 n = tmp.d.len();
+    CPSD_TRY(scratch(n * nb, &tmp.arr));
+    tmp.bs = nb > 1 ? n : 0;
+    CPSD_TRY(launch_scale(tmp.arr, n * nb, 0.0));
+    CPSD_TRY(w444(r2, V, tmp, r2.d.iop[0] == 0 ? -f : -0.5 * f, "cdij", "cdbk", "ijbk", 0, nb));
+    const PairMapPlan *pm;
+    Desc d;
+    CPSD_TRY(plan_pairmap(tmp.d, PAIR_ID, PAIR_SWAP, 1, 1, &d, &pm));
+    i64 sw = nb > 1 ? (W.bs ? W.bs : W.len()) : 0;
+    return launch_pairmap(pm, tmp.arr, W.arr, 1.0, 1.0, nb, tmp.bs, sw);
+}
+int k_Wmbej_r2abij(Ten &W, const Ten &r2, const Ten &V, double f, i64 nb) {
+    return w444(V, r2, W, 0.5 * f, "fenm", "bfjn", "embj", 0, nb);
+}
+int k_Wmbej_r1abci(Ten &W, const Ten &r1, const Ten &V, double f, i64 nb) {
+    return w424(V, r1, W, f, "febm", "fj", "embj", 0, nb);
+}
+int k_Wmbej_r1ijka(Ten &W, const Ten &r1, const Ten &V, double f, i64 nb) {
+    return w424(V, r1, W, -f, "nmje", "bn", "embj", 0, nb);
+}
+int k_Wmnij_r1ijka(Ten &W, const Ten &r1, const Ten &V, double f, i64 nb) {
+    return w424(V, r1, W, f, "mnie", "ej", "mnij", 2, nb);
+}
+
+}  // namespace cpsd
+
+// =============================================================== C-ABI
+using namespace cpsd;
+
+extern "C" {
+
+int cpsd_init(int64_t nirrep, const int64_t *dirprd) {
+    if (nirrep < 1 || nirrep > 8 || !dirprd) return set_error(CPSD_EARG, "cpsd_init: nirrep must be 1..8");
+    Context &c = ctx();
+    c.nirrep = nirrep;
+    for (int j = 0; j < 8; j++)
+        for (int i = 0; i < 8; i++) c.dirprd[i][j] = dirprd[j * 8 + i];
+    for (int i = 1; i <= nirrep; i++)
+        for (int j = 1; j <= nirrep; j++)
+            if (c.dirprd[i - 1][j - 1] < 1 || c.dirprd[i - 1][j - 1] > nirrep)
+                return set_error(CPSD_EARG, "cpsd_init: invalid direct-product table");
+    c.init = true;
+    c.launches = 0;
+    return CPSD_OK;
+}
+
+int cpsd_set_stream(void *s) {
+    ctx().stream = (cudaStream_t)s;
+    return CPSD_OK;
+}
+
+int cpsd_set_workspace(void *p, size_t bytes) {
+    if (p) arena().set_external(p, bytes);
+    else arena().free_all();
+    return CPSD_OK;
+}
+
+size_t cpsd_workspace_high_water(void) { return arena().high_water; }
+
+const char *cpsd_last_error(void) { return last_error().c_str(); }
+
+int64_t cpsd_launch_count(int reset) {
+    int64_t n = ctx().launches;
+    if (reset) ctx().launches = 0;
+    return n;
+}
+
+int64_t cpsd_irpdso(int64_t sym, const int64_t *popp, const int64_t *popq, int64_t ioppq) {
+    return irpdso(sym, popp, popq, ioppq);
+}
+int64_t cpsd_idsymsoc(int64_t irrepx, const int64_t *popp, const int64_t *popq, int64_t ioppq, const int64_t *popr,
+                      const int64_t *pops, int64_t ioprs) {
+    return idsymsoc(irrepx, popp, popq, ioppq, popr, pops, ioprs);
+}
+int64_t cpsd_isymoffso(int64_t irrepq1, int64_t irrep, const int64_t *popp, const int64_t *popq, int64_t iop) {
+    return isymoffso(irrepq1, irrep, popp, popq, iop);
+}
+
+static void type4(const char *t, int n, char out[5]) {
+    for (int i = 0; i < 4; i++) out[i] = i < n ? t[i] : '.';
+    out[4] = 0;
+}
+
+int cpsd_vv2v_dpd_444(const double *v1, const int64_t *p1_1, const int64_t *p1_2, int64_t iop1_12,
+                      const int64_t *p1_3, const int64_t *p1_4, int64_t iop1_34, int64_t sym1, const char *type1,
+                      const double *v2, const int64_t *p2_1, const int64_t *p2_2, int64_t iop2_12,
+                      const int64_t *p2_3, const int64_t *p2_4, int64_t iop2_34, int64_t sym2, const char *type2,
+                      double *v3, const int64_t *p3_1, const int64_t *p3_2, int64_t iop3_12, const int64_t *p3_3,
+                      const int64_t *p3_4, int64_t iop3_34, int64_t sym3, const char *type3, double fact1,
+                      double fact2) {
+    Ten a = ten(p1_1, p1_2, p1_3, p1_4, iop1_12, iop1_34, sym1, (double *)v1);
+    Ten b = ten(p2_1, p2_2, p2_3, p2_4, iop2_12, iop2_34, sym2, (double *)v2);
+    Ten c = ten(p3_1, p3_2, p3_3, p3_4, iop3_12, iop3_34, sym3, v3);
+    char t1[5], t2[5], t3[5];
+    type4(type1, 4, t1);
+    type4(type2, 4, t2);
+    type4(type3, 4, t3);
+    return engine(a, t1, b, t2, c, t3, fact1, fact2);
+}
+
+int cpsd_vv2v_dpd_424(const double *v1, const int64_t *p1_1, const int64_t *p1_2, int64_t iop1_12,
+                      const int64_t *p1_3, const int64_t *p1_4, int64_t iop1_34, int64_t sym1, const char *type1,
+                      const double *v2, const int64_t *p2_1, const int64_t *p2_2, int64_t iop2_12, int64_t sym2,
+                      const char *type2, double *v3, const int64_t *p3_1, const int64_t *p3_2, int64_t iop3_12,
+                      const int64_t *p3_3, const int64_t *p3_4, int64_t iop3_34, int64_t sym3, const char *type3,
+                      double fact1, double fact2) {
+    Ten a = ten(p1_1, p1_2, p1_3, p1_4, iop1_12, iop1_34, sym1, (double *)v1);
+    Ten b = ten(p2_1, p2_2, ZORB, ZORB, iop2_12, 1, sym2, (double *)v2);
+    Ten c = ten(p3_1, p3_2, p3_3, p3_4, iop3_12, iop3_34, sym3, v3);
+    char t1[5], t2[5], t3[5];
+    type4(type1, 4, t1);
+    type4(type2, 2, t2);
+    type4(type3, 4, t3);
+    return engine(a, t1, b, t2, c, t3, fact1, fact2);
+}
+
+int cpsd_vv2v_dpd_442(const double *v1, const int64_t *p1_1, const int64_t *p1_2, int64_t iop1_12,
+                      const int64_t *p1_3, const int64_t *p1_4, int64_t iop1_34, int64_t sym1, const char *type1,
+                      const double *v2, const int64_t *p2_1, const int64_t *p2_2, int64_t iop2_12,
+                      const int64_t *p2_3, const int64_t *p2_4, int64_t iop2_34, int64_t sym2, const char *type2,
+                      double *v3, const int64_t *p3_1, const int64_t *p3_2, int64_t iop3_12, int64_t sym3,
+                      const char *type3, double fact1, double fact2) {
+    Ten a = ten(p1_1, p1_2, p1_3, p1_4, iop1_12, iop1_34, sym1, (double *)v1);
+    Ten b = ten(p2_1, p2_2, p2_3, p2_4, iop2_12, iop2_34, sym2, (double *)v2);
+    Ten c = ten(p3_1, p3_2, ZORB, ZORB, iop3_12, 1, sym3, v3);
+    char t1[5], t2[5], t3[5];
+    type4(type1, 4, t1);
+    type4(type2, 4, t2);
+    type4(type3, 2, t3);
+    return engine(a, t1, b, t2, c, t3, fact1, fact2);
+}
+
+int cpsd_vv2v_dpd_422(const double *v1, const int64_t *p1_1, const int64_t *p1_2, int64_t iop1_12,
+                      const int64_t *p1_3, const int64_t *p1_4, int64_t iop1_34, int64_t sym1, const char *type1,
+                      const double *v2, const int64_t *p2_1, const int64_t *p2_2, int64_t iop2_12, int64_t sym2,
+                      const char *type2, double *v3, const int64_t *p3_1, const int64_t *p3_2, int64_t iop3_12,
+                      int64_t sym3, const char *type3, double fact1, double fact2) {
+    Ten a = ten(p1_1, p1_2, p1_3, p1_4, iop1_12, iop1_34, sym1, (double *)v1);
+    Ten b = ten(p2_1, p2_2, ZORB, ZORB, iop2_12, 1, sym2, (double *)v2);
+    Ten c = ten(p3_1, p3_2, ZORB, ZORB, iop3_12, 1, sym3, v3);
+    char t1[5], t2[5], t3[5];
+    type4(type1, 4, t1);
+    type4(type2, 2, t2);
+    type4(type3, 2, t3);
+    return engine(a, t1, b, t2, c, t3, fact1, fact2);
+}
+
+int cpsd_vv2v_dpd_222(const double *v1, const int64_t *p1_1, const int64_t *p1_2, int64_t iop1_12, int64_t sym1,
+                      const char *type1, const double *v2, const int64_t *p2_1, const int64_t *p2_2,
+                      int64_t iop2_12, int64_t sym2, const char *type2, double *v3, const int64_t *p3_1,
+                      const int64_t *p3_2, int64_t iop3_12, int64_t sym3, const char *type3, double fact1,
+                      double fact2) {
+    Ten a = ten(p1_1, p1_2, ZORB, ZORB, iop1_12, 1, sym1, (double *)v1);
+    Ten b = ten(p2_1, p2_2, ZORB, ZORB, iop2_12, 1, sym2, (double *)v2);
+    Ten c = ten(p3_1, p3_2, ZORB, ZORB, iop3_12, 1, sym3, v3);
+    char t1[5], t2[5], t3[5];
+    type4(type1, 2, t1);
+    type4(type2, 2, t2);
+    type4(type3, 2, t3);
+    return engine(a, t1, b, t2, c, t3, fact1, fact2);
+}
+
+void vv2v_dpd_444_(const double *v1, const int64_t *p1_1, const int64_t *p1_2, const int64_t *iop1_12,
+                   const int64_t *p1_3, const int64_t *p1_4, const int64_t *iop1_34, const int64_t *sym1,
+                   const char *type1, const double *v2, const int64_t *p2_1, const int64_t *p2_2,
+                   const int64_t *iop2_12, const int64_t *p2_3, const int64_t *p2_4, const int64_t *iop2_34,
+                   const int64_t *sym2, const char *type2, double *v3, const int64_t *p3_1, const int64_t *p3_2,
+                   const int64_t *iop3_12, const int64_t *p3_3, const int64_t *p3_4, const int64_t *iop3_34,
+                   const int64_t *sym3, const char *type3, const double *fact1, const double *fact2,
+                   size_t len_type1, size_t len_type2, size_t len_type3) {
+    char t1[5], t2[5], t3[5];
+    type4(type1, len_type1 < 4 ? (int)len_type1 : 4, t1);
+    type4(type2, len_type2 < 4 ? (int)len_type2 : 4, t2);
+    type4(type3, len_type3 < 4 ? (int)len_type3 : 4, t3);
+    int rc = cpsd_vv2v_dpd_444(v1, p1_1, p1_2, *iop1_12, p1_3, p1_4, *iop1_34, *sym1, t1, v2, p2_1, p2_2, *iop2_12,
+                               p2_3, p2_4, *iop2_34, *sym2, t2, v3, p3_1, p3_2, *iop3_12, p3_3, p3_4, *iop3_34, *sym3,
+                               t3, *fact1, *fact2);
+    if (rc != CPSD_OK) fprintf(stderr, "vv2v_dpd_444: error %d\n", rc);
+}
+
+int cpsd_opt_init(cpsd_opt *t, const int64_t *popp, const int64_t *popq, const int64_t *popr, const int64_t *pops,
+                  int64_t ioppq, int64_t ioprs, int64_t sym, double *dev_arr) {
+    memcpy(t->popp, popp, sizeof t->popp);
+    memcpy(t->popq, popq, sizeof t->popq);
+    memcpy(t->popr, popr, sizeof t->popr);
+    memcpy(t->pops, pops, sizeof t->pops);
+    t->ioppq = ioppq;
+    t->ioprs = ioprs;
+    t->sym = sym;
+    t->len = idsymsoc(sym, popp, popq, ioppq, popr, pops, ioprs);
+    t->arr = dev_arr;
+    return CPSD_OK;
+}
+
+static int xform(const cpsd_opt *in, cpsd_opt *out, int op0, int op1, i64 t0, i64 t1) {
+    CPSD_TRY(need_init());
+    const PairMapPlan *pm;
+    Desc d;
+    CPSD_TRY(plan_pairmap(desc_of(in), op0, op1, t0, t1, &d, &pm));
+    Desc o = desc_of(out);
+    if (o.key() != d.key()) return set_error(CPSD_ELAYOUT, "output descriptor does not match the transform");
+    return launch_pairmap(pm, in->arr, out->arr, 1.0, 0.0);
+}
+int cpsd_iexpso(const cpsd_opt *in, cpsd_opt *out, int64_t e0, int64_t e1) {
+    return xform(in, out, e0 ? PAIR_EXPAND : PAIR_ID, e1 ? PAIR_EXPAND : PAIR_ID, 1, 1);
+}
+int cpsd_icompso(const cpsd_opt *in, cpsd_opt *out, int64_t c0, int64_t c1) {
+    return xform(in, out, c0 != 1 ? PAIR_COMPRESS : PAIR_ID, c1 != 1 ? PAIR_COMPRESS : PAIR_ID, c0, c1);
+}
+int cpsd_isymtrso(const cpsd_opt *in, cpsd_opt *out, int64_t s0, int64_t s1) {
+    return xform(in, out, s0 ? PAIR_SWAP : PAIR_ID, s1 ? PAIR_SWAP : PAIR_ID, 1, 1);
+}
+
+int cpsd_debug_contract_plan(const cpsd_opt *v1, const char *t1, const cpsd_opt *v2, const char *t2,
+                             const cpsd_opt *v3, const char *t3, int64_t nb, int64_t sA, int64_t sB, int64_t sC,
+                             const void **tasks, int64_t *ntasks, const void **segs, int64_t *nsegs,
+                             const void **tiles, int64_t *ntiles) {
+    CPSD_TRY(need_init());
+    Batch b;
+    b.nb = nb;
+    b.strideA = sA;
+    b.strideB = sB;
+    b.strideC = sC;
+    const ContractPlan *p;
+    CPSD_TRY(plan_contract(desc_of(v1), t1, desc_of(v2), t2, desc_of(v3), t3, b, &p));
+    *tasks = p->h_tasks.data();
+    *ntasks = (int64_t)p->h_tasks.size();
+    *segs = p->h_segs.data();
+    *nsegs = (int64_t)p->h_segs.size();
+    *tiles = p->h_tiles.data();
+    *ntiles = (int64_t)p->h_tiles.size();
+    return CPSD_OK;
+}
+
+int cpsd_debug_pairmap_plan(const cpsd_opt *in, int64_t op0, int64_t op1, int64_t tgt0, int64_t tgt1,
+                            const void **blocks, int64_t *nblocks, const void **idx, const void **sgn, int64_t *nidx,
+                            int64_t *lterms, int64_t *rterms) {
+    CPSD_TRY(need_init());
+    const PairMapPlan *p;
+    Desc d;
+    CPSD_TRY(plan_pairmap(desc_of(in), (int)op0, (int)op1, tgt0, tgt1, &d, &p));
+    *blocks = p->h_blocks.data();
+    *nblocks = (int64_t)p->h_blocks.size();
+    *idx = p->h_idx.data();
+    *sgn = p->h_sgn.data();
+    *nidx = (int64_t)p->h_idx.size();
+    *lterms = p->lterms;
+    *rterms = p->rterms;
+    return CPSD_OK;
+}
+
+#define WRAP4(nm, fn)                                                                                           \
+    int cpsd_##nm(const cpsd_opt *v1, const cpsd_opt *v2, cpsd_opt *v3, double fact, const char *t1,              \
+                  const char *t2, const char *t3, int64_t anti) {                                                \
+        CPSD_TRY(need_init());                                                                                   \
+        Ten a = ten_of(v1), b = ten_of(v2), c = ten_of(v3);                                                      \
+        return fn(a, b, c, fact, t1, t2, t3, anti);                                                              \
+    }
+#define WRAP3(nm, fn)                                                                                            \
+    int cpsd_##nm(const cpsd_opt *v1, const cpsd_opt *v2, cpsd_opt *v3, double fact, const char *t1,              \
+                  const char *t2, const char *t3) {                                                              \
+        CPSD_TRY(need_init());                                                                                   \
+        Ten a = ten_of(v1), b = ten_of(v2), c = ten_of(v3);                                                      \
+        return fn(a, b, c, fact, t1, t2, t3);                                                                    \
+    }
+WRAP4(vv2v_444, w444)
+WRAP4(vv2v_424, w424)
+WRAP4(vv2v_224, w224)
+WRAP3(vv2v_442, w442)
+WRAP3(vv2v_422, w422)
+WRAP3(vv2v_222, w222)
+
+#define KER(nm)                                                                                                  \
+    int cpsd_##nm(cpsd_opt *out, const cpsd_opt *a, const cpsd_opt *b, double fact) {                            \
+        CPSD_TRY(need_init());                                                                                   \
+        Ten o = ten_of(out), x = ten_of(a), y = ten_of(b);                                                       \
+        return k_##nm(o, x, y, fact);                                                                            \
+    }
+KER(c1_r1iabj)
+KER(c1_r1Fae)
+KER(c1_r1Fmi)
+KER(c1_r2abci)
+KER(c1_r2ijka)
+KER(c2_r1abci)
+KER(c2_r1ijka)
+KER(c2_r2Wmbej)
+KER(c2_r2Wmnij)
+KER(c2_r2abcd)
+KER(c2_r2Fae)
+KER(c2_r2Fmi)
+KER(Fmi_r2abij)
+KER(Fae_r2abij)
+KER(Fmi_r1ijka)
+KER(Fae_r1abci)
+KER(Wkbij_r2ijka)
+KER(Wkbij_r2abci)
+KER(Wmbej_r2abij)
+KER(Wmbej_r1abci)
+KER(Wmbej_r1ijka)
+KER(Wmnij_r1ijka)
+
+}  // extern "C"

@@ -1,0 +1,64 @@
+// Internal tensor operations of libcpsd_b200 (mod_contract wrappers and the
+// spin-free lib_cc kernels) with optional batching over independent
+// copies (the roots of one irrep): a Ten with bs != 0 is a stack of nb
+// tensors bs elements apart; the output of a batched call is always
+// stacked.
+#pragma once
+#include "runtime.hpp"
+
+namespace cpsd {
+
+struct Ten {
+    Desc d;
+    double *arr = nullptr;
+    i64 bs = 0;  // batch stride in elements (0 = one tensor shared by the batch)
+    i64 len() const { return d.len(); }
+};
+Ten ten_of(const cpsd_opt *t);
+Ten ten(const i64 *p0, const i64 *p1, const i64 *p2, const i64 *p3, i64 iop0, i64 iop1, i64 sym, double *arr,
+        i64 bs = 0);
+
+// V3 = f1 * V1 (x) V2 + f2 * V3 (the vv2v_dpd engines)
+int engine(const Ten &v1, const char *t1, const Ten &v2, const char *t2, Ten &v3, const char *t3, double f1,
+           double f2, i64 nb = 1);
+
+int w444(const Ten &v1, const Ten &v2, Ten &v3, double fact, const char *t1, const char *t2, const char *t3,
+         i64 anti, i64 nb = 1);
+int w424(const Ten &v1, const Ten &v2, Ten &v3, double fact, const char *t1, const char *t2, const char *t3,
+         i64 anti, i64 nb = 1);
+int w442(const Ten &v1, const Ten &v2, Ten &v3, double fact, const char *t1, const char *t2, const char *t3,
+         i64 nb = 1);
+int w422(const Ten &v1, const Ten &v2, Ten &v3, double fact, const char *t1, const char *t2, const char *t3,
+         i64 nb = 1);
+int w222(const Ten &v1, const Ten &v2, Ten &v3, double fact, const char *t1, const char *t2, const char *t3,
+         i64 nb = 1);
+int w224(const Ten &v1, const Ten &v2, Ten &v3, double fact, const char *t1, const char *t2, const char *t3,
+         i64 anti, i64 nb = 1);
+
+// lib_cc kernels: out += f * kernel(a, b)
+#define CPSD_IK(name) int k_##name(Ten &out, const Ten &a, const Ten &b, double f, i64 nb = 1)
+CPSD_IK(c1_r1iabj);
+CPSD_IK(c1_r1Fae);
+CPSD_IK(c1_r1Fmi);
+CPSD_IK(c1_r2abci);
+CPSD_IK(c1_r2ijka);
+CPSD_IK(c2_r1abci);
+CPSD_IK(c2_r1ijka);
+CPSD_IK(c2_r2Wmbej);
+CPSD_IK(c2_r2Wmnij);
+CPSD_IK(c2_r2abcd);
+CPSD_IK(c2_r2Fae);
+CPSD_IK(c2_r2Fmi);
+CPSD_IK(Fmi_r2abij);
+CPSD_IK(Fae_r2abij);
+CPSD_IK(Fmi_r1ijka);
+CPSD_IK(Fae_r1abci);
+CPSD_IK(Wkbij_r2ijka);
+CPSD_IK(Wkbij_r2abci);
+CPSD_IK(Wmbej_r2abij);
+CPSD_IK(Wmbej_r1abci);
+CPSD_IK(Wmbej_r1ijka);
+CPSD_IK(Wmnij_r1ijka);
+#undef CPSD_IK
+
+}  // namespace cpsd

@@ -1,0 +1,549 @@
+// Device-resident Davidson (src/lib_cc/mod_davidson.f90:40-728) and DIIS
+// (src/libsrint/dosodiis2_d.f:1-119, dodiis.f, minv.f) for the small CIS /
+// R1 spaces: one CTA owns the whole subspace logic, so an iteration costs
+// one step launch + the batched sigma contraction + one Ritz-matrix update.
+#include "solvers.cuh"
+
+namespace cpsd {
+
+namespace {
+constexpr int DT = 512;  // threads of the single-CTA solver kernels
+
+__device__ double block_sum(double v, double *sh) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) sh[w] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double r = 0.0;
+        for (int i = 0; i < DT / 32; i++) r += sh[i];
+        sh[DT / 32] = r;
+    }
+    __syncthreads();
+    double r = sh[DT / 32];
+    __syncthreads();
+    return r;
+}
+
+__device__ double block_dot(const double *x, const double *y, int n, double *sh) {
+    double a = 0.0;
+    for (int k = threadIdx.x; k < n; k += DT) a = fma(x[k], y[k], a);
+    return block_sum(a, sh);
+}
+
+// value of the first element of largest magnitude (BLAS idamax semantics)
+__device__ double block_amax(const double *x, int n, double *sh, int *shi) {
+    double best = -1.0;
+    int bi = 0x7fffffff;
+    for (int k = threadIdx.x; k < n; k += DT) {
+        double a = fabs(x[k]);
+        if (a > best) {
+            best = a;
+            bi = k;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        double ob = __shfl_down_sync(0xffffffffu, best, o);
+        int oi = __shfl_down_sync(0xffffffffu, bi, o);
+        if (ob > best || (ob == best && oi < bi)) {
+            best = ob;
+            bi = oi;
+        }
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) {
+        sh[w] = best;
+        shi[w] = bi;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double b = -1.0;
+        int ii = 0x7fffffff;
+        for (int i = 0; i < DT / 32; i++)
+            if (sh[i] > b || (sh[i] == b && shi[i] < ii)) {
+                b = sh[i];
+                ii = shi[i];
+            }
+        shi[DT / 32] = ii;
+    }
+    __syncthreads();
+    int idx = shi[DT / 32];
+    __syncthreads();
+    return (idx < n) ? x[idx] : 0.0;
+}
+
+// cyclic Jacobi on a symmetric n x n matrix S (row-major, ld DAV_MAXD) by
+// one warp; eigenvectors accumulate in V (columns)
+__device__ void warp_jacobi(double *S, double *V, int n) {
+    const int lane = threadIdx.x & 31;
+    for (int k = 0; k < n; k++) V[lane * DAV_MAXD + k] = (lane < n) ? (lane == k ? 1.0 : 0.0) : 0.0;
+    __syncwarp();
+    for (int sweep = 0; sweep < 60; sweep++) {
+        double off = 0.0, tot = 0.0;
+        for (int i = lane; i < n; i += 32)
+            for (int j = 0; j < n; j++) {
+                double v = S[i * DAV_MAXD + j];
+                tot += v * v;
+                if (i != j) off += v * v;
+            }
+        for (int o = 16; o > 0; o >>= 1) {
+            off += __shfl_xor_sync(0xffffffffu, off, o);
+            tot += __shfl_xor_sync(0xffffffffu, tot, o);
+        }
+        if (off <= 1e-34 * tot || off == 0.0) break;
+        for (int p = 0; p < n - 1; p++)
+            for (int q = p + 1; q < n; q++) {
+                double apq = S[p * DAV_MAXD + q];
+                if (apq == 0.0) continue;
+                double app = S[p * DAV_MAXD + p], aqq = S[q * DAV_MAXD + q];
+                double tau = (aqq - app) / (2.0 * apq);
+                double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+                double c = 1.0 / sqrt(1.0 + t * t), s = t * c;
+                __syncwarp();
+                if (lane < n) {  // S <- S J
+                    double skp = S[lane * DAV_MAXD + p], skq = S[lane * DAV_MAXD + q];
+                    S[lane * DAV_MAXD + p] = c * skp - s * skq;
+                    S[lane * DAV_MAXD + q] = s * skp + c * skq;
+                    double vkp = V[lane * DAV_MAXD + p], vkq = V[lane * DAV_MAXD + q];
+                    V[lane * DAV_MAXD + p] = c * vkp - s * vkq;
+                    V[lane * DAV_MAXD + q] = s * vkp + c * vkq;
+                }
+                __syncwarp();
+                if (lane < n) {  // S <- J^T S
+                    double spk = S[p * DAV_MAXD + lane], sqk = S[q * DAV_MAXD + lane];
+                    S[p * DAV_MAXD + lane] = c * spk - s * sqk;
+                    S[q * DAV_MAXD + lane] = s * spk + c * sqk;
+                }
+                __syncwarp();
+            }
+    }
+}
+
+// Schmidt_2D (mod_davidson.f90:642-680) on columns of length len
+__device__ void schmidt_2d(const double *in, double *out, int len, int dim) {
+    for (int i = 0; i < len * dim; i++) out[i] = in[i];
+    for (int i = 1; i < dim; i++) {
+        for (int j = 0; j < i; j++) {
+            double ov = 0.0;
+            for (int k = 0; k < len; k++) ov += out[j * len + k] * out[i * len + k];
+            for (int k = 0; k < len; k++) out[i * len + k] += -ov * out[j * len + k];
+        }
+        double nrm = 0.0;
+        for (int k = 0; k < len; k++) nrm += out[i * len + k] * out[i * len + k];
+        nrm = sqrt(nrm);
+        for (int k = 0; k < len; k++) out[i * len + k] *= 1.0 / nrm;
+    }
+}
+
+__global__ void __launch_bounds__(DT) k_dav_init(DavState *st, DavBuffers b) {
+    __shared__ double sh[DT / 32 + 1];
+    DavState &s = *st;
+    const int n = s.dimA, D = s.D, nr = s.nroot;
+    for (int i = 0; i < nr; i++)
+        for (int j = 0; j < nr; j++) {
+            double v = block_dot(b.fileEV + (size_t)j * (n + 1) + 1, b.AB[0] + (size_t)i * n, n, sh);
+            if (threadIdx.x == 0) s.Abar[j + i * D] = v;
+        }
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < nr; i++) {
+            s.eigenVal[i] = b.fileEV[(size_t)i * (n + 1)];
+            for (int k = 0; k < D; k++) s.vecNeed[k + i * D] = (k == i) ? 1.0 : 0.0;
+        }
+        s.iterations = 1;
+        s.dimIter = nr;
+        s.dimFree = D - nr;
+        s.dim_exceed = 0;
+        s.cur = 0;
+        s.done = 0;
+        s.converged = 0;
+    }
+}
+
+__global__ void __launch_bounds__(DT) k_dav_step(DavState *st, DavBuffers b) {
+    __shared__ double S[DAV_MAXD * DAV_MAXD], V[DAV_MAXD * DAV_MAXD];
+    __shared__ double sh[DT / 32 + 1];
+    __shared__ int shi[DT / 32 + 1];
+    DavState &s = *st;
+    const int tid = threadIdx.x;
+    const int D = s.D, n = s.dimA, nroot = s.nroot;
+    if (s.done) return;
+    if (s.iterations > s.maxcyc) {
+        if (tid == 0) s.done = 1;
+        return;
+    }
+    int dimIter = s.dimIter, cur = s.cur, dimFree = s.dimFree;
+    const int dim_exceed = s.dim_exceed;
+    // ---- step 3: eigenpairs of the (symmetrised) Ritz matrix
+    for (int e = tid; e < DAV_MAXD * DAV_MAXD; e += DT) {
+        int i = e / DAV_MAXD, j = e % DAV_MAXD;
+        S[e] = (i < dimIter && j < dimIter) ? 0.5 * (s.Abar[i + j * D] + s.Abar[j + i * D]) : 0.0;
+    }
+    __syncthreads();
+    if (tid < 32) warp_jacobi(S, V, dimIter);
+    __syncthreads();
+    if (tid == 0) {
+        for (int k = 0; k < dimIter; k++) {
+            s.valR[k] = S[k * DAV_MAXD + k];
+            for (int i = 0; i < D; i++) s.vecR[i + k * D] = (i < dimIter) ? V[i * DAV_MAXD + k] : 0.0;
+        }
+        // sort (mod_davidson.f90:620-640)
+        int *low = s.lowestE;
+        for (int i = 0; i < dimIter; i++) low[i] = i + 1;
+        for (int i = 0; i < dimIter - 1; i++)
+            for (int j = i + 1; j < dimIter; j++)
+                if (s.valR[low[j] - 1] < s.valR[low[i] - 1]) {
+                    int t = low[j];
+                    low[j] = low[i];
+                    low[i] = t;
+                }
+        if (!s.lowest) {  // root tracking by largest component (mod_davidson.f90:227-251)
+            for (int iroot = 1; iroot <= nroot; iroot++) {
+                double t1 = 0.0;
+                int i = 1;
+                for (int j = 1; j <= dimIter; j++) {
+                    double t2 = fabs(s.vecR[(iroot - 1) + (low[j - 1] - 1) * D]);
+                    if (t2 > t1) {
+                        t1 = t2;
+                        i = j;
+                    }
+                }
+                int idx = low[i - 1];
+                for (int j = 1; j <= i - iroot; j++) low[i - j] = low[i - j - 1];
+                low[iroot - 1] = idx;
+            }
+        }
+        for (int ir = 0; ir < nroot; ir++) {
+            for (int k = 0; k < D; k++) s.vecNeed[k + ir * D] = s.vecR[k + (low[ir] - 1) * D];
+            s.eigenVal[ir] = s.valR[low[ir] - 1];
+        }
+    }
+    __syncthreads();
+    // ---- collapse when the subspace was full (mod_davidson.f90:266-325)
+    if (dim_exceed) {
+        const int nd = s.ndimIter;
+        if (tid == 0) {
+            for (int i = 0; i < nd; i++)
+                for (int k = 0; k < dimIter; k++) s.oldE[k + i * dimIter] = s.vecR[k + (s.lowestE[i] - 1) * D];
+            schmidt_2d(s.oldE, s.newE, dimIter, nd);
+        }
+        __syncthreads();
+        const int nw = 1 - cur;
+        for (int ir = 0; ir < nd; ir++)
+            for (int k = tid; k < n; k += DT) {
+                double a = 0.0, c = 0.0;
+                for (int i = 0; i < dimIter; i++) {
+                    double t = s.newE[i + ir * dimIter];
+                    a += t * b.AB[cur][(size_t)i * n + k];
+                    c += t * b.B[cur][(size_t)i * n + k];
+                }
+                b.AB[nw][(size_t)ir * n + k] = a;
+                b.B[nw][(size_t)ir * n + k] = c;
+            }
+        __syncthreads();
+        cur = nw;
+        dimFree = s.ndimFree;
+        dimIter = nd;
+        for (int i = 0; i < dimIter; i++)
+            for (int j = 0; j < dimIter; j++) {
+                double v = block_dot(b.AB[cur] + (size_t)i * n, b.B[cur] + (size_t)j * n, n, sh);
+                if (tid == 0) s.Abar[j + i * D] = v;
+            }
+    }
+    // ---- steps 4-6 per root
+    int nNew = 0, nconv = 0;
+    for (int ir = 0; ir < nroot; ir++) {
+        if (tid == 0) s.conv[ir] = 0;
+        for (int k = tid; k < n; k += DT) {
+            double a = 0.0, c = 0.0;
+            if (dim_exceed) {
+                a = b.AB[cur][(size_t)ir * n + k];
+                c = b.B[cur][(size_t)ir * n + k];
+            } else {
+                for (int i = 0; i < dimIter; i++) {
+                    double t = s.vecNeed[i + ir * D];
+                    a += t * b.AB[cur][(size_t)i * n + k];
+                    c += t * b.B[cur][(size_t)i * n + k];
+                }
+            }
+            b.w0[k] = a;
+            b.w1[k] = c;
+        }
+        __syncthreads();
+        double t = sqrt(block_dot(b.w1, b.w1, n, sh));
+        const double ev = s.eigenVal[ir];
+        for (int k = tid; k < n; k += DT) {
+            double q = b.w1[k], aq = b.w0[k];
+            if (fabs(t - 1.0) > 1.0e-10) {
+                q *= 1.0 / t;
+                aq *= 1.0 / t;
+            }
+            b.fileEV[(size_t)ir * (n + 1) + 1 + k] = q;
+            b.w1[k] = q;
+            b.w0[k] = aq - ev * q;
+        }
+        if (tid == 0) b.fileEV[(size_t)ir * (n + 1)] = ev;
+        __syncthreads();
+        double em = block_amax(b.w0, n, sh, shi);
+        if (fabs(em) < s.maxError) {
+            if (tid == 0) s.conv[ir] = 1;
+            nconv++;
+            continue;
+        }
+        if (dimFree == 0) continue;
+        for (int k = tid; k < n; k += DT) {
+            double d = ev - b.diag[k];
+            if (fabs(d) < 1.0e-4) d = (d < 0.0) ? -1.0e-4 : 1.0e-4;
+            b.w1[k] = b.w0[k] / d;
+        }
+        __syncthreads();
+        // SchmidtS (mod_davidson.f90:682-727)
+        double nrm = sqrt(block_dot(b.w1, b.w1, n, sh));
+        for (int k = tid; k < n; k += DT) b.w1[k] *= 1.0 / nrm;
+        __syncthreads();
+        for (int i = 0; i < dimIter + nNew; i++) {
+            double ov = block_dot(b.B[cur] + (size_t)i * n, b.w1, n, sh);
+            for (int k = tid; k < n; k += DT) b.w1[k] += -ov * b.B[cur][(size_t)i * n + k];
+            __syncthreads();
+        }
+        nrm = sqrt(block_dot(b.w1, b.w1, n, sh));
+        if (nrm < 1.0e-6) continue;
+        const int pos = dimIter + nNew;
+        for (int k = tid; k < n; k += DT) b.B[cur][(size_t)pos * n + k] = b.w1[k] * (1.0 / nrm);
+        __syncthreads();
+        dimFree--;
+        nNew++;
+    }
+    if (tid == 0) {
+        s.cur = cur;
+        s.dimIter = dimIter;
+        s.dimFree = dimFree;
+        s.newpos = dimIter;
+        s.nNew = nNew;
+        if (nconv == nroot) {
+            s.done = 1;
+            s.converged = 1;
+        } else {
+            s.dim_exceed = 0;
+            if (dimFree == 0) {
+                s.dim_exceed = 1;
+                s.ndimIter = D - s.dimDel;
+                if (s.ndimIter < nroot) {
+                    s.ndimIter = nroot;
+                    s.ndimFree = D - s.ndimIter;
+                } else {
+                    s.ndimFree = s.dimDel;
+                }
+            }
+        }
+    }
+}
+
+// Ritz-matrix update with the new vectors (mod_davidson.f90:460-496)
+__global__ void __launch_bounds__(DT) k_dav_abar(DavState *st, DavBuffers b) {
+    __shared__ double sh[DT / 32 + 1];
+    DavState &s = *st;
+    if (s.done) return;
+    const int n = s.dimA, D = s.D, dimIter = s.dimIter, nNew = s.nNew, cur = s.cur;
+    const double *B = b.B[cur], *AB = b.AB[cur];
+    for (int j = 0; j < dimIter; j++)
+        for (int i = dimIter; i < dimIter + nNew; i++) {
+            double v = block_dot(B + (size_t)i * n, AB + (size_t)j * n, n, sh);
+            if (threadIdx.x == 0) s.Abar[i + j * D] = v;
+        }
+    for (int j = dimIter; j < dimIter + nNew; j++)
+        for (int i = 0; i < dimIter + nNew; i++) {
+            double v = block_dot(B + (size_t)i * n, AB + (size_t)j * n, n, sh);
+            if (threadIdx.x == 0) s.Abar[i + j * D] = v;
+        }
+    if (threadIdx.x == 0) {
+        s.dimIter = dimIter + nNew;
+        s.iterations++;
+    }
+}
+
+// eigen test of the final roots (mod_davidson.f90:525-542): AR in w-buffer
+__global__ void __launch_bounds__(DT) k_dav_final(DavState *st, DavBuffers b, const double *AR) {
+    __shared__ double sh[DT / 32 + 1];
+    __shared__ int shi[DT / 32 + 1];
+    DavState &s = *st;
+    const int n = s.dimA;
+    double worst = 0.0;
+    for (int ir = 0; ir < s.nroot; ir++) {
+        const double *R = b.fileEV + (size_t)ir * (n + 1);
+        double w = R[0];
+        for (int k = threadIdx.x; k < n; k += DT) b.w0[k] = AR[(size_t)ir * n + k] - w * R[1 + k];
+        __syncthreads();
+        double e = fabs(block_amax(b.w0, n, sh, shi));
+        if (e > worst) worst = e;
+    }
+    if (threadIdx.x == 0) s.max_resid = worst;
+}
+
+// ------------------------------------------------------------------- DIIS
+// LINPACK dgefa / dgesl (as MINV, src/libsrint/minv.f, calls them)
+__device__ void dgefa(double *a, int lda, int n, int *ipvt) {
+    for (int k = 0; k < n - 1; k++) {
+        int l = k;
+        double m = -1.0;
+        for (int i = k; i < n; i++)
+            if (fabs(a[i + k * lda]) > m) {
+                m = fabs(a[i + k * lda]);
+                l = i;
+            }
+        ipvt[k] = l;
+        if (a[l + k * lda] == 0.0) continue;
+        if (l != k) {
+            double t = a[l + k * lda];
+            a[l + k * lda] = a[k + k * lda];
+            a[k + k * lda] = t;
+        }
+        double t = -1.0 / a[k + k * lda];
+        for (int i = k + 1; i < n; i++) a[i + k * lda] *= t;
+        for (int j = k + 1; j < n; j++) {
+            double tj = a[l + j * lda];
+            if (l != k) {
+                a[l + j * lda] = a[k + j * lda];
+                a[k + j * lda] = tj;
+            }
+            for (int i = k + 1; i < n; i++) a[i + j * lda] += tj * a[i + k * lda];
+        }
+    }
+    ipvt[n - 1] = n - 1;
+}
+__device__ void dgesl(const double *a, int lda, int n, const int *ipvt, double *bv) {
+    for (int k = 0; k < n - 1; k++) {
+        int l = ipvt[k];
+        double t = bv[l];
+        if (l != k) {
+            bv[l] = bv[k];
+            bv[k] = t;
+        }
+        for (int i = k + 1; i < n; i++) bv[i] += t * a[i + k * lda];
+    }
+    for (int kb = 0; kb < n; kb++) {
+        int k = n - 1 - kb;
+        bv[k] /= a[k + k * lda];
+        double t = -bv[k];
+        for (int i = 0; i < k; i++) bv[i] += t * a[i + k * lda];
+    }
+}
+
+__global__ void __launch_bounds__(DT) k_diis(DiisState *st, DiisBuffers b, int iter, double *vec) {
+    __shared__ double sh[DT / 32 + 1];
+    __shared__ int shi[DT / 32 + 1];
+    __shared__ double Bm[DIIS_MAXDIM * DIIS_MAXDIM];
+    __shared__ double coef[DIIS_MAXDIM + 1];
+    DiisState &s = *st;
+    const int len = s.len, maxdim = s.maxdim, tid = threadIdx.x;
+    if (iter == 1) {
+        for (int k = tid; k < len; k += DT) b.prev[k] = vec[k];
+        if (tid == 0) {
+            s.idimr = 1;
+            s.ndimr = 1;
+            s.res = 1.0;
+        }
+        return;
+    }
+    const int id = s.idimr - 1;
+    for (int k = tid; k < len; k += DT) {
+        double p = b.prev[k];
+        b.amp[(size_t)id * len + k] = p;
+        double e = vec[k] - p;
+        vec[k] = e;
+        b.err[(size_t)id * len + k] = e;
+    }
+    __syncthreads();
+    const int nd = s.ndimr;
+    for (int i = 0; i < nd; i++)
+        for (int j = 0; j <= i; j++) {
+            double x = block_dot(b.err + (size_t)i * len, b.err + (size_t)j * len, len, sh);
+            if (tid == 0) {
+                Bm[i + j * DIIS_MAXDIM] = x;
+                Bm[j + i * DIIS_MAXDIM] = x;
+            }
+        }
+    __syncthreads();
+    if (tid == 0) {  // dodiis (src/libsrint/dodiis.f): bordered system with -1e-4
+        const int n1 = nd + 1;
+        double aug[(DIIS_MAXDIM + 1) * (DIIS_MAXDIM + 1)];
+        double rhs[DIIS_MAXDIM + 1];
+        int ipvt[DIIS_MAXDIM + 1];
+        for (int e = 0; e < n1 * n1; e++) aug[e] = 0.0;
+        for (int j = 0; j < nd; j++)
+            for (int i = 0; i < nd; i++) aug[(i + 1) + (j + 1) * n1] = Bm[i + j * DIIS_MAXDIM];
+        for (int i = 1; i <= nd; i++) {
+            aug[i] = -1.0e-4;
+            aug[i * n1] = -1.0e-4;
+        }
+        rhs[0] = -1.0e-4;
+        for (int i = 1; i <= nd; i++) rhs[i] = 0.0;
+        dgefa(aug, n1, n1, ipvt);
+        dgesl(aug, n1, n1, ipvt, rhs);
+        for (int i = 0; i < nd; i++) coef[i] = rhs[i + 1];
+    }
+    __syncthreads();
+    for (int k = tid; k < len; k += DT) {
+        double v = 0.0;
+        for (int i = 0; i < nd; i++) v += coef[i] * b.err[(size_t)i * len + k];
+        vec[k] = v;
+    }
+    __syncthreads();
+    double res = block_amax(vec, len, sh, shi);
+    for (int k = tid; k < len; k += DT) {
+        double v = vec[k];
+        for (int i = 0; i < nd; i++) v += coef[i] * b.amp[(size_t)i * len + k];
+        vec[k] = v;
+        b.prev[k] = v;
+    }
+    if (tid == 0) {
+        s.res = res;
+        s.ndimr = (nd + 1 < maxdim) ? nd + 1 : maxdim;
+        s.idimr = s.idimr + 1;
+        if (s.idimr > maxdim) s.idimr = 1;
+    }
+}
+
+__global__ void __launch_bounds__(DT) k_orth(double *R, const double *L, int n) {
+    __shared__ double sh[DT / 32 + 1];
+    double nrm = sqrt(block_dot(L, L, n, sh));
+    double dot = block_dot(L, R, n, sh);
+    double f = -dot / nrm;
+    for (int k = threadIdx.x; k < n; k += DT) R[k] += f * L[k];
+}
+}  // namespace
+
+int dav_init_launch(DavState *st, const DavBuffers &b) {
+    k_dav_init<<<1, DT, 0, stream()>>>(st, b);
+    count_launch();
+    return cuda_check(cudaGetLastError(), "k_dav_init");
+}
+int dav_step_launch(DavState *st, const DavBuffers &b) {
+    k_dav_step<<<1, DT, 0, stream()>>>(st, b);
+    count_launch();
+    return cuda_check(cudaGetLastError(), "k_dav_step");
+}
+int dav_abar_launch(DavState *st, const DavBuffers &b) {
+    k_dav_abar<<<1, DT, 0, stream()>>>(st, b);
+    count_launch();
+    return cuda_check(cudaGetLastError(), "k_dav_abar");
+}
+int dav_final_launch(DavState *st, const DavBuffers &b) {
+    // AR of the final roots was written to b.AB[0] by the caller
+    k_dav_final<<<1, DT, 0, stream()>>>(st, b, b.AB[0]);
+    count_launch();
+    return cuda_check(cudaGetLastError(), "k_dav_final");
+}
+int diis_step_launch(DiisState *st, const DiisBuffers &b, int iter, double *vec) {
+    k_diis<<<1, DT, 0, stream()>>>(st, b, iter, vec);
+    count_launch();
+    return cuda_check(cudaGetLastError(), "k_diis");
+}
+int orth_launch(double *R, const double *L, i64 n) {
+    k_orth<<<1, DT, 0, stream()>>>(R, L, (int)n);
+    count_launch();
+    return cuda_check(cudaGetLastError(), "k_orth");
+}
+
+}  // namespace cpsd

@@ -1,0 +1,52 @@
+// Device state of the Davidson eigensolver and the DIIS extrapolator.
+#pragma once
+#include "runtime.hpp"
+
+namespace cpsd {
+
+constexpr int DAV_MAXD = 32;  // davidson_dim limit (reference default 20)
+
+// Everything the reference keeps in local variables / scratch files
+// (src/lib_cc/mod_davidson.f90:40-560), resident on the device.
+struct DavState {
+    int D, dimA, nroot, lowest, maxcyc;
+    int dimIter, dimFree, dim_exceed, ndimIter, ndimFree, dimDel;
+    int iterations, cur, nNew, newpos, done, converged;
+    int warn_imag;
+    double maxError, max_resid;
+    int conv[DAV_MAXD];
+    int lowestE[DAV_MAXD];
+    double eigenVal[DAV_MAXD];
+    double valR[DAV_MAXD];
+    double Abar[DAV_MAXD * DAV_MAXD];
+    double vecR[DAV_MAXD * DAV_MAXD];
+    double vecNeed[DAV_MAXD * DAV_MAXD];
+    double oldE[DAV_MAXD * DAV_MAXD];
+    double newE[DAV_MAXD * DAV_MAXD];
+};
+
+struct DavBuffers {
+    double *B[2], *AB[2];  // basis and sigma "files", D x dimA each
+    const double *diag;    // OED1 of the irrep
+    double *fileEV;        // nroot records (w, R)
+    double *w0, *w1;       // work vectors
+};
+
+int dav_init_launch(DavState *st, const DavBuffers &b);      // Abar of the guesses
+int dav_step_launch(DavState *st, const DavBuffers &b);
+int dav_abar_launch(DavState *st, const DavBuffers &b);
+int dav_final_launch(DavState *st, const DavBuffers &b);     // eigen test residual
+
+constexpr int DIIS_MAXDIM = 16;
+struct DiisState {
+    int len, maxdim, ndimr, idimr;
+    double res;
+};
+struct DiisBuffers {
+    double *prev, *err, *amp;  // len, maxdim*len, maxdim*len
+};
+int diis_step_launch(DiisState *st, const DiisBuffers &b, int iter, double *vec);
+// R -= (<L|R>/||L||) L  (orthogonalR2L, src/EE-CPSd.SF/orthogonalR2L.f90:5-34)
+int orth_launch(double *R, const double *L, i64 n);
+
+}  // namespace cpsd

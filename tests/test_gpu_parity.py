@@ -1,0 +1,213 @@
+"""GPU (libcpsd_b200 through the C-ABI) against the CPU oracle on the same
+seeded inputs.  FP64 throughout: contractions to 1e-12 absolute on O(1)
+data, excitation energies and (D) corrections to 1e-9 Eh; vectors from
+iterative solvers are compared up to sign and to their convergence
+thresholds (Davidson residual 1e-8, DIIS 1e-7)."""
+import numpy as np
+import pytest
+
+import kernel_specs as ks
+import oracle_ffi as of
+from cpsd_b200 import api, synth
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+TOL_E = 1e-9
+
+
+def dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def host(t):
+    torch.cuda.synchronize()
+    return t.cpu().numpy()
+
+
+def small(nirrep, roots=2, seed=5, nmo=None):
+    return synth.System(nmo=nmo or (14 if nirrep <= 2 else 16), nocc_a=3, nocc_b=1, nirrep=nirrep, seed=seed,
+                        roots=roots)
+
+
+@pytest.fixture(autouse=True)
+def _stream():
+    api.use_torch_stream()
+    yield
+
+
+@pytest.mark.parametrize("nirrep", [1, 4, 8])
+def test_engine_matches_oracle(nirrep):
+    s = synth.System(nmo=24, nocc_a=4, nocc_b=2, nirrep=nirrep, seed=nirrep)
+    api.init(s.nirrep, s.dirprd)
+    of.set_symmetry(s.nirrep, s.dirprd)
+    sym, o, v = s.sym, s.popo, s.popv
+    rng = np.random.default_rng(0)
+    s2 = 2 if nirrep > 1 else 1
+    z = np.array([1, 0, 0, 0, 0, 0, 0, 0])
+    cases = [
+        ("aeim", [v, v, o, o], (1, 1), s2, "embj", [v, o, v, o], (1, 1), 1, "abij", [v, v, o, o], (1, 1), s2),
+        ("abef", [v, v, v, v], (0, 0), 1, "efij", [v, v, o, o], (0, 0), s2, "abij", [v, v, o, o], (0, 0), s2),
+        ("mbie", [o, v, o, v], (1, 1), 1, "ajme", [v, o, o, v], (1, 1), s2, "abij", [v, v, o, o], (1, 1), s2),
+        ("ijmb", [o, o, o, v], (0, 1), 1, "am..", [v, o, z, z], (1, 1), s2, "abij", [v, v, o, o], (1, 0), s2),
+    ]
+    for (t1, p1, i1, y1, t2, p2, i2, y2, t3, p3, i3, y3) in cases:
+        a = rng.standard_normal(sym.idsymsoc(y1, p1[0], p1[1], i1[0], p1[2], p1[3], i1[1]))
+        b = rng.standard_normal(sym.idsymsoc(y2, p2[0], p2[1], i2[0], p2[2], p2[3], i2[1]))
+        c = rng.standard_normal(sym.idsymsoc(y3, p3[0], p3[1], i3[0], p3[2], p3[3], i3[1]))
+        for f2 in (1.0, 0.0, 0.5):
+            ref = c.copy() if f2 != 0.0 else np.full_like(c, 999.0)
+            rc = of.vv2v_dpd(a, of.desc(p1, i1, y1), t1, b, of.desc(p2, i2, y2), t2, ref, of.desc(p3, i3, y3), t3,
+                             0.7, f2)
+            assert rc == 0
+            out = dev(c if f2 != 0.0 else np.full_like(c, 999.0))
+            api.vv2v_dpd_444(dev(a), (p1, i1, y1), t1, dev(b), (p2, i2, y2), t2, out, (p3, i3, y3), t3, 0.7, f2)
+            np.testing.assert_allclose(host(out), ref, rtol=0, atol=1e-12, err_msg=f"{t1}*{t2}->{t3} f2={f2}")
+
+
+@pytest.mark.parametrize("nirrep", [1, 4])
+@pytest.mark.parametrize("name", sorted(ks.KERNELS))
+def test_kernel_matches_oracle(name, nirrep):
+    rng = np.random.default_rng(abs(hash(name)) % 1000 + nirrep)
+    s = small(nirrep)
+    api.init(s.nirrep, s.dirprd)
+    of.set_symmetry(s.nirrep, s.dirprd)
+    sym = s.sym
+    lo, la, lb = ks.KERNELS[name][:3]
+    symR = 2 if nirrep > 1 else 1
+    syms = {"a": symR, "b": 1}
+    if name.startswith("c2_r2"):
+        syms = {"a": 1, "b": symR}
+    so = sym.dp(syms["a"], syms["b"])
+    po, io = ks.pops_of(lo, s.popo, s.popv)
+    pa, ia = ks.pops_of(la, s.popo, s.popv)
+    pb, ib = ks.pops_of(lb, s.popo, s.popv)
+    va = rng.standard_normal(sym.idsymsoc(syms["a"], pa[0], pa[1], ia[0], pa[2], pa[3], ia[1]))
+    vb = rng.standard_normal(sym.idsymsoc(syms["b"], pb[0], pb[1], ib[0], pb[2], pb[3], ib[1]))
+    vo = rng.standard_normal(sym.idsymsoc(so, po[0], po[1], io[0], po[2], po[3], io[1]))
+    ref = vo.copy()
+    rc = of.call_kernel(name, of.opt(po, io, so, ref), of.opt(pa, ia, syms["a"], va), of.opt(pb, ib, syms["b"], vb),
+                        0.8)
+    assert rc == 0
+    ta, tb, to = dev(va), dev(vb), dev(vo)
+    api.kernel(name, api.opt(po, io, so, to), api.opt(pa, ia, syms["a"], ta), api.opt(pb, ib, syms["b"], tb), 0.8)
+    np.testing.assert_allclose(host(to), ref, rtol=0, atol=1e-12, err_msg=name)
+
+
+def _run_both(s, batch_roots=1, **kw):
+    api.init(s.nirrep, s.dirprd)
+    ints = api.DeviceIntegrals(s)
+    return ints, api.make_system(s), api.make_params(s, batch_roots=batch_roots, **kw), of.Oracle(s, **kw)
+
+
+@pytest.mark.parametrize("nirrep", [1, 2, 4])
+def test_cis_matches_oracle(nirrep):
+    s = small(nirrep, roots=3)
+    ints, sc, par, orc = _run_both(s)
+    om, R, it = api.cis_run(s, sc, ints, par)
+    oom, oR, oit = orc.cis()
+    np.testing.assert_allclose(om, oom, rtol=0, atol=1e-10)
+    l1 = s.r1_len(1)
+    Rg = host(R)
+    for k in range(len(om)):
+        a, b = Rg[k * l1:(k + 1) * l1], oR[k * l1:(k + 1) * l1]
+        sgn = np.sign(np.dot(a, b))
+        np.testing.assert_allclose(sgn * a, b, rtol=0, atol=1e-7)
+
+
+@pytest.mark.parametrize("nirrep", [1, 4])
+def test_ground_and_intermediates_match_oracle(nirrep):
+    s = small(nirrep)
+    ints, sc, par, orc = _run_both(s)
+    g = api.ground(s, sc, ints, par)
+    og = orc.ground()
+    assert abs(g["E2"] - og["E2"]) < 1e-11 and abs(g["E3"] - og["E3"]) < 1e-11
+    np.testing.assert_allclose(host(g["T2_1"]), og["T2_1"], rtol=0, atol=1e-13)
+    np.testing.assert_allclose(host(g["T2_2"]), og["T2_2"], rtol=0, atol=1e-12)
+    np.testing.assert_allclose(host(g["T1_2"]), og["T1_2"], rtol=0, atol=1e-9)
+    assert g["iters"] == og["iters"]
+    J, js = api.calJ(s, sc, ints, g)
+    oJ = orc.jints(og)
+    for k in oJ:
+        np.testing.assert_allclose(host(J[k]), oJ[k], rtol=0, atol=1e-9, err_msg=k)
+
+
+@pytest.mark.parametrize("batch", [0, 1])
+@pytest.mark.parametrize("nirrep", [1, 4])
+def test_eecpsd_roots_match_oracle(nirrep, batch):
+    s = small(nirrep, roots=3)
+    ints, sc, par, orc = _run_both(s, batch_roots=batch)
+    om, R, _ = api.cis_run(s, sc, ints, par)
+    g = api.ground(s, sc, ints, par)
+    J, js = api.calJ(s, sc, ints, g)
+    w, outs, it = api.eecpsd_roots(s, sc, ints, par, g, js, 1, om, R, want_vectors=True)
+    og = orc.ground()
+    oJ = orc.jints(og)
+    oom, oR, _ = orc.cis()
+    l1, l2 = s.r1_len(1), s.r2_len(1)
+    Rg = host(R)
+    for k in range(len(om)):
+        L = Rg[k * l1:(k + 1) * l1]
+        r = orc.root(og, oJ, 1, om[k], L)
+        np.testing.assert_allclose(w[k], r["w"], rtol=0, atol=TOL_E)
+        np.testing.assert_allclose(host(outs["R2_1"])[k * l2:(k + 1) * l2], r["R2_1"], rtol=0, atol=1e-11)
+        np.testing.assert_allclose(host(outs["R2_2"])[k * l2:(k + 1) * l2], r["R2_2"], rtol=0, atol=1e-10)
+        np.testing.assert_allclose(host(outs["R1_2"])[k * l1:(k + 1) * l1], r["R1_2"], rtol=0, atol=1e-6)
+        assert abs(np.dot(L, host(outs["R1_2"])[k * l1:(k + 1) * l1])) < 1e-10
+
+
+@pytest.mark.parametrize("batch", [0, 1])
+def test_pipeline_c2v_nmo48(batch):
+    """The plain-FP64 configuration (C2v, nmo 48, nocc 5/3, 3 roots)."""
+    s = synth.make("c2v_nmo48")
+    ints, sc, par, orc = _run_both(s, batch_roots=batch)
+    om, w2, w3 = api.pipeline(s, sc, ints, par)
+    oom, ow2, ow3 = orc.pipeline()
+    np.testing.assert_allclose(om, oom, rtol=0, atol=TOL_E)
+    np.testing.assert_allclose(w2, ow2, rtol=0, atol=TOL_E)
+    np.testing.assert_allclose(w3, ow3, rtol=0, atol=TOL_E)
+
+
+def test_full_size_d2h_nmo200_properties():
+    """The precision-form shapes (D2h, nmo 200, nocc 10/8, 5 roots): checks
+    that need no full-size oracle run — Davidson eigen residual, batched vs
+    per-root identity, <L|R1^(2)> = 0 — plus one root of the oracle on the
+    same inputs."""
+    s = synth.make("d2h_nmo200")
+    api.init(s.nirrep, s.dirprd)
+    ints = api.DeviceIntegrals(s)
+    sc = api.make_system(s)
+    par1 = api.make_params(s, batch_roots=1)
+    om, R, it = api.cis_run(s, sc, ints, par1)
+    l1 = s.r1_len(1)
+    # eigen residual with the library's own sigma: AR = e(a,i) R + V R
+    Rg = R.view(len(om), l1)
+    z = np.array([1, 0, 0, 0, 0, 0, 0, 0])
+    for k in range(len(om)):
+        AR = torch.zeros(l1, dtype=torch.float64, device="cuda")
+        api.kernel("c1_r1iabj", api.opt([s.popv, s.popo, z, z], (1, 1), 1, AR),
+                   api.opt([s.popv, s.popo, z, z], (1, 1), 1, Rg[k].contiguous()),
+                   api.opt([s.popv, s.popo, s.popv, s.popo], (1, 1), 1, ints.t["iabj"]), 1.0)
+        oed = np.zeros(l1)
+        of.set_symmetry(s.nirrep, s.dirprd)
+        of.lib().o_eorb_diff1(of.ptr(oed), of.ptr(s.eorb), of.arr8(s.popv), of.arr8(s.popo), of.I64(1))
+        r = host(Rg[k])
+        res = host(AR) + oed * r - om[k] * r
+        assert np.max(np.abs(res)) < 1e-8
+        assert abs(np.linalg.norm(r) - 1.0) < 1e-10
+    g = api.ground(s, sc, ints, par1)
+    J, js = api.calJ(s, sc, ints, g)
+    wb, ob, _ = api.eecpsd_roots(s, sc, ints, par1, g, js, 1, om, R, want_vectors=True)
+    par0 = api.make_params(s, batch_roots=0)
+    wu, ou, _ = api.eecpsd_roots(s, sc, ints, par0, g, js, 1, om, R, want_vectors=False)
+    np.testing.assert_allclose(wb, wu, rtol=0, atol=1e-12)
+    R12 = host(ob["R1_2"]).reshape(len(om), l1)
+    for k in range(len(om)):
+        assert abs(np.dot(host(Rg[k]), R12[k])) < 1e-10
+    assert np.all(np.isfinite(wb))
+    # oracle on the first root (same integrals / CIS vector / ground T)
+    orc = of.Oracle(s, nthreads=8)
+    og = dict(T2_1=host(g["T2_1"]), T1_2=host(g["T1_2"]), T2_2=host(g["T2_2"]))
+    oJ = {k: host(v) for k, v in J.items()}
+    r = orc.root(og, oJ, 1, om[0], host(Rg[0]))
+    np.testing.assert_allclose(wb[0], r["w"], rtol=0, atol=TOL_E)
