@@ -1,0 +1,315 @@
+#!/usr/bin/env python
+"""Benchmark: SF-CIS + SF-CPS(D-3) roots per second on B200.
+
+One step = the whole pipeline of the workload: SF-CIS Davidson (residual
+1e-8) for every requested root, ground CPS(D) T^(1)/T^(2), the J^(2)/J^(3)
+intermediates and EE-CPS(D-3) orders 1-3 for every root, with the integrals
+resident in HBM.  Default workload: D2h, nmo 200, nocc 10/8, 5 spin-flip
+roots, FP64 throughout (synthetic seeded integrals, see synth.py).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--config NAME]
+  python bench.py --impl reference ...   (CPU restatement on the host cores)
+
+Multi-GPU: one process per GPU (torchrun); every rank runs an independent
+replica of the workload (replicas only: the path has no exchange step);
+value = roots of all ranks / max-over-ranks device time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+METRIC = "SF-CPS(D) roots/sec: mixed+batched vs FP64 GPU at ≤1 µEh; contraction TFLOP/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="d2h_nmo200")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-threads", type=int, default=0)
+    return ap.parse_args()
+
+
+def workload_desc(s, name):
+    return (f"{name}: SF-CIS (spin-flip a->b, Davidson residual 1e-8) + ground CPS(D) + J2/J3 + "
+            f"EE-CPS(D-3) orders 1-3; {['C1','Cs','','C2v','','','','D2h'][s.nirrep-1] or s.nirrep} "
+            f"nirrep={s.nirrep}, nmo={s.nmo}, nocc {s.nocc_a}/{s.nocc_b}, o={int(s.popo.sum())}, "
+            f"v={int(s.popv.sum())}, roots={s.nroots}, FP64")
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.f = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(gpu_index), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                smax = float(r[2])
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        busy = [x for x in sm if smax and x > 0.5 * smax] or sm
+        return {"sm_mhz": float(np.median(busy)) if busy else None, "sm_max_mhz": smax,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def measured_fp64_peak(torch):
+    """cuBLAS DGEMM throughput on this GPU (TFLOP/s), the FP64 roofline."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def cpu_reference_sample(name, threads, steps=1, warmup=0):
+    """The CPU restatement (oracle) on a bounded sample of the workload: one
+    root's full chain (CIS for it, ground, J, EE orders 1-3) timed per stage;
+    the workload's roots/s is extrapolated from the stage times:
+    nroot / (T_cis * nroot + T_ground + T_J + nroot * T_root)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import conftest  # noqa: F401  (registers the package)
+    import oracle_ffi as of
+    from cpsd_b200 import synth
+    s = synth.make(name)
+    nroot = s.nroots
+    s.estate_sym[:] = 0
+    s.estate_sym[0] = 1
+    orc = of.Oracle(s, nthreads=threads)
+    small = synth.make("c2v_nmo48")
+    for _ in range(warmup):
+        of.Oracle(small, nthreads=threads).pipeline()
+    samples = []
+    for _ in range(max(steps, 1)):
+        t0 = time.perf_counter()
+        om, R, _ = orc.cis()
+        t1 = time.perf_counter()
+        g = orc.ground()
+        t2 = time.perf_counter()
+        J = orc.jints(g)
+        t3 = time.perf_counter()
+        orc.root(g, J, 1, om[0], R[:s.r1_len(1)])
+        t4 = time.perf_counter()
+        samples.append((t1 - t0, t2 - t1, t3 - t2, t4 - t3))
+    tc, tg, tj, tr = np.mean(np.array(samples), axis=0)
+    t_all = tc * nroot + tg + tj + tr * nroot
+    return nroot / t_all, dict(t_cis_per_root=tc, t_ground=tg, t_J=tj, t_root=tr, sample_wall=sum(samples[-1]))
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    threads = args.cpu_threads or os.cpu_count() or 1
+    t0 = time.time()
+    v, info = cpu_reference_sample(args.config, threads, steps=args.steps, warmup=args.warmup)
+    from cpsd_b200 import synth  # noqa
+    line = {
+        "metric": METRIC, "value": v, "unit": "roots/s", "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * info["sample_wall"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "config": {"workload": args.config, "note": "CPU restatement of the reference's FP64 path "
+                   "(the Fortran reference cannot be built here: no Fortran compiler)"},
+        "cpu_baseline": {"value": v, "unit": "roots/s", "cores": threads, "kind": "port",
+                         "sample": "one root's chain (CIS, ground CPS(D), J2/J3, EE orders 1-3) per step, "
+                                   "stage times extrapolated to all roots of the workload",
+                         "stage_seconds": {k: round(x, 4) for k, x in info.items()}},
+        "e2e": {"value": v, "unit": "roots/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "wall_s": round(time.time() - t0, 1),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    import __graft_entry__ as ge
+    ge.load_package()
+    from cpsd_b200 import api, synth
+
+    torch.cuda.set_device(local_rank)
+    s = synth.make(args.config)
+    api.init(s.nirrep, s.dirprd)
+    api.use_torch_stream()
+    ints = api.DeviceIntegrals(s)
+    sysc = api.make_system(s)
+    par = api.make_params(s, batch_roots=1)
+    stream = torch.cuda.current_stream()
+
+    def step():
+        return api.pipeline(s, sysc, ints, par)
+
+    for _ in range(args.warmup):
+        out = step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(local_rank)
+    api.launch_count(True)
+    api.flop_count(True)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        out = step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ck = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    launches = api.launch_count(True)
+    flops = api.flop_count(True)
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * s.nroots * args.steps / (ms_max / 1e3)
+    om, w2, w3 = out
+
+    # roofline of the dominant kernel (the grouped FP64 contraction), timed
+    # with CUDA events around each of its launches in one extra step
+    import ctypes
+    lib = api.lib()
+    lib.cpsd_contract_timing(1)
+    lib.cpsd_contract_time(None, None, None, 1)
+    step()
+    c_ms, c_n, c_fl = ctypes.c_double(), ctypes.c_int64(), ctypes.c_double()
+    lib.cpsd_contract_time(ctypes.byref(c_ms), ctypes.byref(c_n), ctypes.byref(c_fl), 1)
+    lib.cpsd_contract_timing(0)
+    fp64_peak = measured_fp64_peak(torch)
+    achieved = c_fl.value / (c_ms.value / 1e3) / 1e12 if c_ms.value > 0 else 0.0
+    step_total_ms = ms_max / args.steps
+
+    # end to end through the public API with host buffers: H2D of every
+    # integral tensor from pinned memory, the pipeline, results back on the host
+    e2e = None
+    if not args.no_e2e:
+        host = {k: torch.from_numpy(s.ints[k]).pin_memory() for k in api.DeviceIntegrals.KEYS
+                if s.ints[k] is not None}
+        host["eorb"] = torch.from_numpy(s.eorb).pin_memory()
+        h2d = sum(v.numel() * 8 for v in host.values())
+        d2h = 3 * s.nroots * 8
+        torch.cuda.synchronize()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(args.steps):
+            for k, v in host.items():
+                ints.t[k].copy_(v, non_blocking=True)
+            step()
+        f1.record(stream)
+        torch.cuda.synchronize()
+        t2 = torch.tensor([f0.elapsed_time(f1)], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(t2, op=dist.ReduceOp.MAX)
+        e2e = {"value": world * s.nroots * args.steps / (float(t2.item()) / 1e3), "unit": "roots/s",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = args.cpu_threads or os.cpu_count() or 1
+        v, info = cpu_reference_sample(args.config, threads, steps=1)
+        cpu = {"value": v, "unit": "roots/s", "cores": threads, "kind": "port",
+               "sample": "one root's chain (CIS, ground CPS(D), J2/J3, EE orders 1-3), stage times "
+                         "extrapolated to all roots of the workload",
+               "stage_seconds": {k: round(x, 4) for k, x in info.items()}}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "roots/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_total_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator, synth.py)",
+            "config": {"workload": workload_desc(s, args.config), "inputs": "resident in HBM, "
+                       f"{ints.nbytes / 1e9:.2f} GB of integrals (larger than L2)",
+                       "parallelism": f"replicas x{world}", "roots_batched": True},
+            "roofline": {"bound": "tensor", "kernel": "k_contract (grouped FP64 DPD contraction)",
+                         "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                         "frac": achieved / fp64_peak if fp64_peak else None, "traffic": None,
+                         "peak_source": "measured cuBLAS DGEMM 8192^3 on this GPU (MEASURED_PEAKS.json has no FP64 "
+                                        "figure)", "share_of_step": c_ms.value / step_total_ms,
+                         "launches_per_step": c_n.value},
+            "contraction_tflops": flops / (ms_max / 1e3) / 1e12,
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": ck,
+            "results": {"omega_cis": [float(x) for x in om], "w2": [float(x) for x in w2],
+                        "w3": [float(x) for x in w3]},
+        }
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if world > 1 and rank != 0:
+            return
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -43,6 +43,14 @@ size_t cpsd_workspace_high_water(void);
 const char *cpsd_last_error(void);
 /* number of kernels this library launched since cpsd_init / last reset */
 int64_t cpsd_launch_count(int reset);
+/* useful contraction flops (2*M*N*K over the irrep blocks) issued since
+ * the last reset */
+double cpsd_flop_count(int reset);
+/* CUDA-event timing of every contraction-kernel launch on its stream
+ * (off by default); cpsd_contract_time synchronises the recorded events
+ * and returns total milliseconds, launches and useful flops. */
+int cpsd_contract_timing(int enable);
+int cpsd_contract_time(double *ms, int64_t *launches, double *flops, int reset);
 
 /* -------------------------------------------------------------- size math */
 /* irpdso (src/libsrint/irpdso.f:1-52) */

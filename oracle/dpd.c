@@ -3,6 +3,7 @@
  * and the layout transforms iexpso / icompso / isymtrso.
  */
 #include "cpsd_oracle.h"
+#include "oracle_internal.h"
 #include <stdlib.h>
 #include <string.h>
 
@@ -138,55 +139,60 @@ i64 o_elem_offset(const o_desc *d, const i64 irr[4], const i64 idx[4], int *sign
     return base + pr * nleft + pl;
 }
 
-/* Generic element loop over every (irreps, indices) of the FULL index space
- * of descriptor `dout` (iop ignored: all p,q / r,s), calling f for each
- * element that dout stores in canonical order. */
-typedef void (*elem_fn)(const i64 irr[4], const i64 idx[4], i64 off_out, void *ctx);
-
-static void foreach_stored(const o_desc *dout, elem_fn f, void *ctx)
+static i64 block_base(const o_desc *d, i64 R)
 {
-    i64 n = g_nirrep;
-    i64 irr[4], idx[4];
-    for (irr[0] = 1; irr[0] <= n; irr[0]++)
-        for (irr[1] = 1; irr[1] <= n; irr[1]++)
-            for (irr[2] = 1; irr[2] <= n; irr[2]++) {
-                irr[3] = o_dirprd(o_dirprd(o_dirprd(irr[0], irr[1]), irr[2]), dout->sym);
-                if (dout->iop[0] != 1 && irr[0] > irr[1]) continue;
-                if (dout->iop[1] != 1 && irr[2] > irr[3]) continue;
-                for (idx[3] = 0; idx[3] < dout->pop[3][irr[3] - 1]; idx[3]++)
-                    for (idx[2] = 0; idx[2] < dout->pop[2][irr[2] - 1]; idx[2]++) {
-                        if (dout->iop[1] == 0 && irr[2] == irr[3] && idx[2] >= idx[3]) continue;
-                        if (dout->iop[1] == 2 && irr[2] == irr[3] && idx[2] > idx[3]) continue;
-                        for (idx[1] = 0; idx[1] < dout->pop[1][irr[1] - 1]; idx[1]++)
-                            for (idx[0] = 0; idx[0] < dout->pop[0][irr[0] - 1]; idx[0]++) {
-                                if (dout->iop[0] == 0 && irr[0] == irr[1] && idx[0] >= idx[1]) continue;
-                                if (dout->iop[0] == 2 && irr[0] == irr[1] && idx[0] > idx[1]) continue;
-                                int s;
-                                i64 o = o_elem_offset(dout, irr, idx, &s);
-                                if (o >= 0) f(irr, idx, o, ctx);
-                            }
-                    }
-            }
+    i64 b = 0;
+    for (i64 r = 1; r < R; r++)
+        b += o_irpdso(o_dirprd(r, d->sym), d->pop[0], d->pop[1], d->iop[0]) *
+             o_irpdso(r, d->pop[2], d->pop[3], d->iop[1]);
+    return b;
 }
 
-typedef struct {
-    const double *in;
-    double *out;
-    const o_desc *din;
-    int swpq, swrs;
-} xform_ctx;
-
-/* out(element) = in(same element, maybe pair-swapped) with the packed sign */
-static void copy_elem(const i64 irr[4], const i64 idx[4], i64 off_out, void *vctx)
+/* For every stored pair of `dout`'s pair k in the pair space of irrep X:
+ * the offset of the same (possibly swapped) pair in `din` and its sign. */
+static void pair_map(const o_desc *din, const o_desc *dout, int k, i64 X, int swap, o_pairs *pl,
+                     i64 **off, double **sgn)
 {
-    xform_ctx *c = (xform_ctx *)vctx;
-    i64 ir[4] = {irr[0], irr[1], irr[2], irr[3]};
-    i64 ix[4] = {idx[0], idx[1], idx[2], idx[3]};
-    if (c->swpq) { i64 t = ir[0]; ir[0] = ir[1]; ir[1] = t; t = ix[0]; ix[0] = ix[1]; ix[1] = t; }
-    if (c->swrs) { i64 t = ir[2]; ir[2] = ir[3]; ir[3] = t; t = ix[2]; ix[2] = ix[3]; ix[3] = t; }
-    int s;
-    i64 o = o_elem_offset(c->din, ir, ix, &s);
-    c->out[off_out] = (o < 0) ? 0.0 : s * c->in[o];
+    o_pairs_build(pl, dout->pop[2 * k], dout->pop[2 * k + 1], dout->iop[k], X);
+    *off = (i64 *)malloc(sizeof(i64) * (size_t)(pl->n + 1));
+    *sgn = (double *)malloc(sizeof(double) * (size_t)(pl->n + 1));
+    for (i64 e = 0; e < pl->n; e++) {
+        i64 ip = pl->ip[e], p = pl->p[e], iq = pl->iq[e], q = pl->q[e];
+        if (swap) { i64 t = ip; ip = iq; iq = t; t = p; p = q; q = t; }
+        int s = 1;
+        (*off)[e] = pair_offset(din->pop[2 * k], din->pop[2 * k + 1], din->iop[k], ip, p, iq, q, &s);
+        (*sgn)[e] = s;
+    }
+}
+
+/* out(element) = sign * in(same element, pairs possibly swapped); zero for
+ * structurally vanishing elements (p == q of a p<q pair).  Works block by
+ * block on separable per-pair maps. */
+static void xform(const double *in, double *out, const o_desc *din, const o_desc *dout, int swpq, int swrs)
+{
+    for (i64 R = 1; R <= g_nirrep; R++) {
+        i64 L = o_dirprd(R, dout->sym);
+        o_pairs pl, pr;
+        i64 *lo, *ro;
+        double *ls, *rs;
+        pair_map(din, dout, 0, L, swpq, &pl, &lo, &ls);
+        pair_map(din, dout, 1, R, swrs, &pr, &ro, &rs);
+        i64 ob = block_base(dout, R), ib = block_base(din, R);
+        i64 nlo = pl.n, nli = o_irpdso(L, din->pop[0], din->pop[1], din->iop[0]);
+#pragma omp parallel for schedule(static)
+        for (i64 r = 0; r < pr.n; r++) {
+            double *o = out + ob + r * nlo;
+            if (ro[r] < 0) {
+                for (i64 l = 0; l < nlo; l++) o[l] = 0.0;
+                continue;
+            }
+            const double *x = in + ib + ro[r] * nli;
+            for (i64 l = 0; l < nlo; l++) o[l] = (lo[l] < 0) ? 0.0 : rs[r] * ls[l] * x[lo[l]];
+        }
+        free(lo); free(ls); free(ro); free(rs);
+        o_pairs_free(&pl);
+        o_pairs_free(&pr);
+    }
 }
 
 /* iexpso (src/libsrint/iexpso.f90:24-120, exp_pq: out(q,p) = -in(p<q),
@@ -196,8 +202,7 @@ int o_iexpso(const double *in, double *out, const o_desc *din, i64 exppq, i64 ex
     o_desc dout = *din;
     if (exppq) dout.iop[0] = 1;
     if (exprs) dout.iop[1] = 1;
-    xform_ctx c = {in, out, din, 0, 0};
-    foreach_stored(&dout, copy_elem, &c);
+    xform(in, out, din, &dout, 0, 0);
     return O_OK;
 }
 
@@ -210,8 +215,7 @@ int o_icompso(const double *in, double *out, const o_desc *din, i64 cpq, i64 crs
     o_desc dout = *din;
     if (cpq != 1) dout.iop[0] = cpq;
     if (crs != 1) dout.iop[1] = crs;
-    xform_ctx c = {in, out, din, 0, 0};
-    foreach_stored(&dout, copy_elem, &c);
+    xform(in, out, din, &dout, 0, 0);
     return O_OK;
 }
 
@@ -230,7 +234,6 @@ int o_isymtrso(const double *in, double *out, const o_desc *din, i64 swpq, i64 s
         memcpy(dout.pop[2], din->pop[3], sizeof(dout.pop[0]));
         memcpy(dout.pop[3], din->pop[2], sizeof(dout.pop[0]));
     }
-    xform_ctx c = {in, out, din, (int)swpq, (int)swrs};
-    foreach_stored(&dout, copy_elem, &c);
+    xform(in, out, din, &dout, (int)swpq, (int)swrs);
     return O_OK;
 }

@@ -31,6 +31,7 @@ def lib():
         _lib = ctypes.CDLL(LIB_PATH)
         _lib.cpsd_last_error.restype = ctypes.c_char_p
         _lib.cpsd_launch_count.restype = I64
+        _lib.cpsd_flop_count.restype = ctypes.c_double
         _lib.cpsd_workspace_high_water.restype = ctypes.c_size_t
         for f in ("cpsd_irpdso", "cpsd_idsymsoc", "cpsd_isymoffso"):
             getattr(_lib, f).restype = I64
@@ -99,6 +100,11 @@ def launch_count(reset=False):
     return int(lib().cpsd_launch_count(1 if reset else 0))
 
 
+def flop_count(reset=False):
+    """useful contraction flops issued since the last reset"""
+    return float(lib().cpsd_flop_count(1 if reset else 0))
+
+
 def opt(pops, iops, sym, t):
     o = Opt()
     check(lib().cpsd_opt_init(ctypes.byref(o), arr8(pops[0]), arr8(pops[1]), arr8(pops[2]), arr8(pops[3]),
@@ -141,7 +147,7 @@ def make_params(s, batch_roots=1, **kw):
         p.estate_sym[h] = int(s.estate_sym[h])
     p.spin_flip = s.spin_flip
     p.batch_roots = batch_roots
-    for k, v in kw.items():
+    for k, v in {**getattr(s, 'run_opts', {}), **kw}.items():
         setattr(p, k, v)
     return p
 

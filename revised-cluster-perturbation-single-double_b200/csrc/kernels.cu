@@ -8,6 +8,7 @@
 //  * BLAS-1          scale, axpy, copy, deterministic (optionally
 //                    compensated) dot product.
 #include <cstdio>
+#include <vector>
 
 #include "runtime.hpp"
 
@@ -301,14 +302,73 @@ int grid_for(i64 n, int threads = 256) {
 }
 }  // namespace
 
+// optional CUDA-event timing of every k_contract launch (on its stream)
+namespace {
+struct Timing {
+    bool on = false;
+    std::vector<cudaEvent_t> pool;
+    size_t used = 0;
+    std::vector<double> flops;
+};
+Timing &timing() {
+    static Timing t;
+    return t;
+}
+}  // namespace
+
+int contract_timing(int enable) {
+    timing().on = enable != 0;
+    return CPSD_OK;
+}
+
+int contract_time(double *ms, int64_t *launches, double *flops, int reset) {
+    Timing &t = timing();
+    double tot = 0.0, fl = 0.0;
+    for (size_t i = 0; i + 1 < t.used; i += 2) {
+        CPSD_TRY(cuda_check(cudaEventSynchronize(t.pool[i + 1]), "event sync"));
+        float x = 0.f;
+        CPSD_TRY(cuda_check(cudaEventElapsedTime(&x, t.pool[i], t.pool[i + 1]), "event time"));
+        tot += x;
+        fl += t.flops[i / 2];
+    }
+    if (ms) *ms = tot;
+    if (launches) *launches = (int64_t)(t.used / 2);
+    if (flops) *flops = fl;
+    if (reset) {
+        t.used = 0;
+        t.flops.clear();
+    }
+    return CPSD_OK;
+}
+
+static int timing_event(cudaEvent_t *e) {
+    Timing &t = timing();
+    if (t.used == t.pool.size()) {
+        cudaEvent_t ev;
+        CPSD_TRY(cuda_check(cudaEventCreate(&ev), "event create"));
+        t.pool.push_back(ev);
+    }
+    *e = t.pool[t.used++];
+    return CPSD_OK;
+}
+
 int launch_contract(const ContractPlan *p, const double *A, const double *B, double *C, double alpha) {
     if (p->empty) return CPSD_OK;
     CPSD_TRY(const_cast<ContractPlan *>(p)->upload());
     double *part = nullptr;
     ScratchScope scope;
     if (p->nparts > 0) CPSD_TRY(scratch(p->nparts * BM * BN, &part));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (timing().on) {
+        CPSD_TRY(timing_event(&e0));
+        CPSD_TRY(timing_event(&e1));
+        timing().flops.push_back(p->flops);
+        CPSD_TRY(cuda_check(cudaEventRecord(e0, stream()), "event record"));
+    }
     k_contract<<<p->ntiles, NT, 0, stream()>>>(A, B, C, p->d_tasks, p->d_segs, p->d_tiles, alpha, part);
     count_launch();
+    ctx().flops += p->flops;
+    if (e1) CPSD_TRY(cuda_check(cudaEventRecord(e1, stream()), "event record"));
     if (p->nreduce > 0) {
         k_splitk_reduce<<<p->nreduce, NT, 0, stream()>>>(p->d_reduce, p->d_tasks, part, C, alpha);
         count_launch();

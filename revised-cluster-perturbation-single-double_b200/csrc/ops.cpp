@@ -327,6 +327,18 @@ int64_t cpsd_launch_count(int reset) {
     return n;
 }
 
+int cpsd_contract_timing(int enable) { return contract_timing(enable); }
+
+int cpsd_contract_time(double *ms, int64_t *launches, double *flops, int reset) {
+    return contract_time(ms, launches, flops, reset);
+}
+
+double cpsd_flop_count(int reset) {
+    double f = ctx().flops;
+    if (reset) ctx().flops = 0;
+    return f;
+}
+
 int64_t cpsd_irpdso(int64_t sym, const int64_t *popp, const int64_t *popq, int64_t ioppq) {
     return irpdso(sym, popp, popq, ioppq);
 }

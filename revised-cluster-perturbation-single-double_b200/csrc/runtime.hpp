@@ -31,6 +31,7 @@ struct Context {
     i64 dirprd[8][8] = {};  // [i-1][j-1]
     cudaStream_t stream = nullptr;
     int64_t launches = 0;
+    double flops = 0;  // useful contraction flops issued (2 M N K per block)
 };
 Context &ctx();
 inline i64 dp(i64 a, i64 b) { return ctx().dirprd[a - 1][b - 1]; }
@@ -167,6 +168,8 @@ int plan_pairmap(const Desc &din, int op0, int op1, i64 target_iop0, i64 target_
 
 // ------------------------------------------------------------- launches
 int launch_contract(const ContractPlan *p, const double *A, const double *B, double *C, double alpha);
+int contract_timing(int enable);
+int contract_time(double *ms, int64_t *launches, double *flops, int reset);
 int launch_pairmap(const PairMapPlan *p, const double *in, double *out, double alpha, double beta, i64 nb = 1,
                    i64 in_stride = 0, i64 out_stride = 0);
 int launch_scale(double *x, i64 n, double beta);                  // x *= beta (beta 0: zero fill)

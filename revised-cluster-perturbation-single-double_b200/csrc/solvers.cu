@@ -80,24 +80,25 @@ __device__ void warp_jacobi(double *S, double *V, int n) {
     const int lane = threadIdx.x & 31;
     for (int k = 0; k < n; k++) V[lane * DAV_MAXD + k] = (lane < n) ? (lane == k ? 1.0 : 0.0) : 0.0;
     __syncwarp();
-    for (int sweep = 0; sweep < 60; sweep++) {
-        double off = 0.0, tot = 0.0;
-        for (int i = lane; i < n; i += 32)
-            for (int j = 0; j < n; j++) {
-                double v = S[i * DAV_MAXD + j];
-                tot += v * v;
-                if (i != j) off += v * v;
-            }
-        for (int o = 16; o > 0; o >>= 1) {
-            off += __shfl_xor_sync(0xffffffffu, off, o);
-            tot += __shfl_xor_sync(0xffffffffu, tot, o);
-        }
-        if (off <= 1e-34 * tot || off == 0.0) break;
+    // classic cyclic Jacobi (Golub & Van Loan, Alg. 8.5.3): an element below
+    // eps * sqrt(|a_pp a_qq|) is negligible and set to zero; a sweep without
+    // rotations ends the iteration
+    for (int sweep = 0; sweep < 50; sweep++) {
+        int rotated = 0;
         for (int p = 0; p < n - 1; p++)
             for (int q = p + 1; q < n; q++) {
                 double apq = S[p * DAV_MAXD + q];
-                if (apq == 0.0) continue;
                 double app = S[p * DAV_MAXD + p], aqq = S[q * DAV_MAXD + q];
+                if (fabs(apq) <= 1.0e-17 * sqrt(fabs(app) * fabs(aqq)) || apq == 0.0) {
+                    __syncwarp();
+                    if (lane == 0) {
+                        S[p * DAV_MAXD + q] = 0.0;
+                        S[q * DAV_MAXD + p] = 0.0;
+                    }
+                    __syncwarp();
+                    continue;
+                }
+                rotated = 1;
                 double tau = (aqq - app) / (2.0 * apq);
                 double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
                 double c = 1.0 / sqrt(1.0 + t * t), s = t * c;
@@ -118,6 +119,7 @@ __device__ void warp_jacobi(double *S, double *V, int n) {
                 }
                 __syncwarp();
             }
+        if (!rotated) break;
     }
 }
 

@@ -147,7 +147,7 @@ def make_params(s, nthreads=1, **kw):
         p.estate_sym[h] = int(s.estate_sym[h])
     p.spin_flip = s.spin_flip
     p.nthreads = nthreads
-    for k, v in kw.items():
+    for k, v in {**getattr(s, 'run_opts', {}), **kw}.items():
         setattr(p, k, v)
     return p
 
