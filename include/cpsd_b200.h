@@ -206,7 +206,10 @@ CPSD_KERNEL(Wmnij_r1ijka); /* Wmnij_r1ijka.f90:3 W(mn,ij) += P(ij) r(e,j) V(mn,i
 int cpsd_debug_contract_plan(const cpsd_opt *v1, const char *t1, const cpsd_opt *v2, const char *t2,
                              const cpsd_opt *v3, const char *t3, int64_t nb, int64_t sA, int64_t sB, int64_t sC,
                              const void **tasks, int64_t *ntasks, const void **segs, int64_t *nsegs,
-                             const void **tiles, int64_t *ntiles);
+                             const void **tiles, int64_t *ntiles, int64_t *tile_bm, int64_t *tile_bn);
+/* per-launch records of the contraction timing buffer: milliseconds,
+ * useful flops and (tasks, segments, tiles, tile shape) */
+int cpsd_contract_records(double *ms, double *flops, int64_t *shape, int64_t maxrec, int64_t *nrec);
 int cpsd_debug_pairmap_plan(const cpsd_opt *in, int64_t op0, int64_t op1, int64_t tgt0, int64_t tgt1,
                             const void **blocks, int64_t *nblocks, const void **idx, const void **sgn,
                             int64_t *nidx, int64_t *lterms, int64_t *rterms);

@@ -1,0 +1,363 @@
+// The grouped DPD contraction kernel (sm_100a, FP64).
+//
+// One launch executes every irrep block of a contraction: each CTA owns a
+// BM x BN tile of one output block (task) and walks the K segments of that
+// task (the irrep assignments of the contracted indices), gathering A / B
+// tiles through the planner's stride tables (packed pairs are composite
+// indices) into padded shared memory and multiplying them on the FP64
+// tensor pipe with mma.sync.m8n8k4.f64 (tcgen05 has no FP64 kind).  The
+// next K stage is fetched into registers while the current one is
+// multiplied.  Split-K tiles write partial sums that k_splitk_reduce adds
+// in a fixed order, so results are deterministic.
+#include <array>
+#include <vector>
+
+#include "runtime.hpp"
+
+namespace cpsd {
+
+namespace {
+constexpr int NT = 256, BK = 16, PAD = 4;
+
+__device__ __forceinline__ i64 decode1(i64 x, int n, const i64 *ext, const i64 *st) {
+    i64 off = 0;
+    for (int u = 0; u < n; u++) {
+        i64 e = ext[u];
+        i64 q = x / e;
+        off += (x - q * e) * st[u];
+        x = q;
+    }
+    return off;
+}
+
+__device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(c[0]), "+d"(c[1])
+                 : "d"(a), "d"(b));
+}
+
+template <int BM, int BN>
+constexpr int smem_bytes() {
+    return (int)sizeof(double) * 2 * BK * ((BM + PAD) + (BN + PAD));
+}
+
+template <int BM, int BN, int WM, int WN>
+__global__ void __launch_bounds__(NT, 2) k_contract(const double *__restrict__ A, const double *__restrict__ B,
+                                                    double *__restrict__ C, const TaskDev *__restrict__ tasks,
+                                                    const SegDev *__restrict__ segs, const TileDev *__restrict__ tiles,
+                                                    double alpha, double *__restrict__ partial) {
+    static_assert(WM * WN == NT / 32, "8 warps");
+    constexpr int WTM = BM / WM, WTN = BN / WN, MI = WTM / 8, NI = WTN / 8;
+    constexpr int LA = BM * BK / NT, LB = BN * BK / NT;
+    static_assert(LA >= 1 && LB >= 1 && BM + BN <= NT, "tile shape");
+    extern __shared__ double dsm[];
+    double(*As)[BK][BM + PAD] = reinterpret_cast<double(*)[BK][BM + PAD]>(dsm);
+    double(*Bs)[BK][BN + PAD] = reinterpret_cast<double(*)[BK][BN + PAD]>(dsm + 2 * BK * (BM + PAD));
+    __shared__ i64 offM[BM], offN[BN], offKA[2][BK], offKB[2][BK];
+    __shared__ TaskDev tk;
+    __shared__ SegDev sg;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = warp % WM, wn = warp / WM;
+    const TileDev tl = tiles[blockIdx.x];
+    if (tid == 0) tk = tasks[tl.task];
+    __syncthreads();
+    const i64 m0 = (i64)tl.mt * BM, n0 = (i64)tl.nt * BN;
+    double acc[MI][NI][2];
+#pragma unroll
+    for (int i = 0; i < MI; i++)
+#pragma unroll
+        for (int j = 0; j < NI; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
+    double ra[LA], rb[LB];
+
+    for (int si = 0; si < tk.nseg; si++) {
+        __syncthreads();
+        if (tid == 0) sg = segs[tk.seg0 + si];
+        __syncthreads();
+        i64 kb = tl.k_lo - sg.kstart, ke = tl.k_hi - sg.kstart;
+        if (kb < 0) kb = 0;
+        if (ke > sg.K) ke = sg.K;
+        if (kb >= ke) continue;
+        if (tid < BM) {
+            i64 m = m0 + tid;
+            offM[tid] = (m < tk.M) ? sg.baseA + decode1(m, tk.nm, tk.mExt, sg.mSA) : -1;
+        } else if (tid < BM + BN) {
+            i64 n = n0 + tid - BM;
+            offN[tid - BM] = (n < tk.N) ? sg.baseB + decode1(n, tk.nn, tk.nExt, sg.nSB) : -1;
+        }
+        const int nst = (int)((ke - kb + BK - 1) / BK);
+        auto decodeK = [&](int s, int buf) {
+            if (tid < BK) {
+                i64 k = kb + (i64)s * BK + tid;
+                if (k < ke) {
+                    i64 a = 0, b = 0, x = k;
+                    for (int u = 0; u < sg.nk; u++) {
+                        i64 e = sg.kExt[u], q = x / e, r = x - q * e;
+                        a += r * sg.kSA[u];
+                        b += r * sg.kSB[u];
+                        x = q;
+                    }
+                    offKA[buf][tid] = a;
+                    offKB[buf][tid] = b;
+                } else {
+                    offKA[buf][tid] = -1;
+                    offKB[buf][tid] = -1;
+                }
+            }
+        };
+        auto loadRegs = [&](int buf) {
+#pragma unroll
+            for (int i = 0; i < LA; i++) {
+                int e = tid + i * NT, m, k;
+                if (sg.aMfast) {
+                    m = e % BM;
+                    k = e / BM;
+                } else {
+                    k = e % BK;
+                    m = e / BK;
+                }
+                i64 om = offM[m], ok = offKA[buf][k];
+                ra[i] = (om >= 0 && ok >= 0) ? __ldg(A + om + ok) : 0.0;
+            }
+#pragma unroll
+            for (int i = 0; i < LB; i++) {
+                int e = tid + i * NT, n, k;
+                if (sg.bKfast) {
+                    k = e % BK;
+                    n = e / BK;
+                } else {
+                    n = e % BN;
+                    k = e / BN;
+                }
+                i64 on = offN[n], ok = offKB[buf][k];
+                rb[i] = (on >= 0 && ok >= 0) ? __ldg(B + on + ok) : 0.0;
+            }
+        };
+        auto storeRegs = [&](int buf) {
+#pragma unroll
+            for (int i = 0; i < LA; i++) {
+                int e = tid + i * NT;
+                if (sg.aMfast) As[buf][e / BM][e % BM] = ra[i];
+                else As[buf][e % BK][e / BK] = ra[i];
+            }
+#pragma unroll
+            for (int i = 0; i < LB; i++) {
+                int e = tid + i * NT;
+                if (sg.bKfast) Bs[buf][e % BK][e / BK] = rb[i];
+                else Bs[buf][e / BN][e % BN] = rb[i];
+            }
+        };
+        decodeK(0, 0);
+        __syncthreads();
+        loadRegs(0);
+        for (int s = 0; s < nst; s++) {
+            const int buf = s & 1;
+            storeRegs(buf);
+            if (s + 1 < nst) decodeK(s + 1, buf ^ 1);
+            __syncthreads();
+            if (s + 1 < nst) loadRegs(buf ^ 1);
+#pragma unroll
+            for (int kk = 0; kk < BK / 4; kk++) {
+                const int kr = kk * 4 + (lane & 3);
+                double a[MI], b[NI];
+#pragma unroll
+                for (int i = 0; i < MI; i++) a[i] = As[buf][kr][wm * WTM + i * 8 + (lane >> 2)];
+#pragma unroll
+                for (int j = 0; j < NI; j++) b[j] = Bs[buf][kr][wn * WTN + j * 8 + (lane >> 2)];
+#pragma unroll
+                for (int i = 0; i < MI; i++)
+#pragma unroll
+                    for (int j = 0; j < NI; j++) dmma(acc[i][j], a[i], b[j]);
+            }
+        }
+    }
+    __syncthreads();
+    const int rl = lane >> 2, cl = 2 * (lane & 3);
+    if (tl.part >= 0) {
+        double *P = partial + (size_t)tl.part * (BM * BN);
+#pragma unroll
+        for (int i = 0; i < MI; i++)
+#pragma unroll
+            for (int j = 0; j < NI; j++) {
+                int r = wm * WTM + i * 8 + rl, c = wn * WTN + j * 8 + cl;
+                P[r * BN + c] = acc[i][j][0];
+                P[r * BN + c + 1] = acc[i][j][1];
+            }
+        return;
+    }
+    if (tid < BM) {
+        i64 m = m0 + tid;
+        offM[tid] = (m < tk.M) ? tk.baseC + decode1(m, tk.nm, tk.mExt, tk.mSC) : -1;
+    } else if (tid < BM + BN) {
+        i64 n = n0 + tid - BM;
+        offN[tid - BM] = (n < tk.N) ? decode1(n, tk.nn, tk.nExt, tk.nSC) : -1;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < MI; i++) {
+        i64 om = offM[wm * WTM + i * 8 + rl];
+        if (om < 0) continue;
+#pragma unroll
+        for (int j = 0; j < NI; j++)
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                i64 on = offN[wn * WTN + j * 8 + cl + h];
+                if (on < 0) continue;
+                C[om + on] += alpha * acc[i][j][h];
+            }
+    }
+}
+
+// sum the split-K partial tiles of one output tile in a fixed order
+__global__ void __launch_bounds__(NT) k_splitk_reduce(const int *__restrict__ red, const TaskDev *__restrict__ tasks,
+                                                      const double *__restrict__ partial, double *__restrict__ C,
+                                                      double alpha, int bm, int bn) {
+    const int *r = red + 5 * blockIdx.x;
+    const TaskDev &tk = tasks[r[0]];
+    const i64 m0 = (i64)r[1] * bm, n0 = (i64)r[2] * bn;
+    const i64 p0 = r[3];
+    const int ns = r[4];
+    __shared__ i64 offM[128], offN[128];
+    int tid = threadIdx.x;
+    if (tid < bm) {
+        i64 m = m0 + tid;
+        offM[tid] = (m < tk.M) ? decode1(m, tk.nm, tk.mExt, tk.mSC) : -1;
+    }
+    if (tid < bn) {
+        i64 n = n0 + tid;
+        offN[tid] = (n < tk.N) ? decode1(n, tk.nn, tk.nExt, tk.nSC) : -1;
+    }
+    __syncthreads();
+    for (int e = tid; e < bm * bn; e += NT) {
+        int mi = e / bn, ni = e % bn;
+        i64 om = offM[mi], on = offN[ni];
+        if (om < 0 || on < 0) continue;
+        double s = 0.0;
+        for (int q = 0; q < ns; q++) s += partial[(size_t)(p0 + q) * (bm * bn) + e];
+        C[tk.baseC + om + on] += alpha * s;
+    }
+}
+
+// optional CUDA-event timing of every contraction launch (on its stream)
+struct Timing {
+    bool on = false;
+    std::vector<cudaEvent_t> pool;
+    size_t used = 0;
+    std::vector<double> flops;
+    std::vector<std::array<int64_t, 4>> shape;  // tasks, segments, tiles, tile config
+};
+Timing &timing() {
+    static Timing t;
+    return t;
+}
+int timing_event(cudaEvent_t *e) {
+    Timing &t = timing();
+    if (t.used == t.pool.size()) {
+        cudaEvent_t ev;
+        CPSD_TRY(cuda_check(cudaEventCreate(&ev), "event create"));
+        t.pool.push_back(ev);
+    }
+    *e = t.pool[t.used++];
+    return CPSD_OK;
+}
+}  // namespace
+
+const int TILE_BM[4] = {128, 128, 64, 64};
+const int TILE_BN[4] = {64, 32, 128, 64};
+
+int contract_timing(int enable) {
+    timing().on = enable != 0;
+    return CPSD_OK;
+}
+
+int contract_records(double *ms, double *flops, int64_t *shape, int64_t maxrec, int64_t *nrec) {
+    Timing &t = timing();
+    int64_t n = 0;
+    for (size_t i = 0; i + 1 < t.used && n < maxrec; i += 2, n++) {
+        CPSD_TRY(cuda_check(cudaEventSynchronize(t.pool[i + 1]), "event sync"));
+        float x = 0.f;
+        CPSD_TRY(cuda_check(cudaEventElapsedTime(&x, t.pool[i], t.pool[i + 1]), "event time"));
+        ms[n] = x;
+        flops[n] = t.flops[i / 2];
+        for (int k = 0; k < 4; k++) shape[4 * n + k] = t.shape[i / 2][k];
+    }
+    *nrec = n;
+    return CPSD_OK;
+}
+
+int contract_time(double *ms, int64_t *launches, double *flops, int reset) {
+    Timing &t = timing();
+    double tot = 0.0, fl = 0.0;
+    for (size_t i = 0; i + 1 < t.used; i += 2) {
+        CPSD_TRY(cuda_check(cudaEventSynchronize(t.pool[i + 1]), "event sync"));
+        float x = 0.f;
+        CPSD_TRY(cuda_check(cudaEventElapsedTime(&x, t.pool[i], t.pool[i + 1]), "event time"));
+        tot += x;
+        fl += t.flops[i / 2];
+    }
+    if (ms) *ms = tot;
+    if (launches) *launches = (int64_t)(t.used / 2);
+    if (flops) *flops = fl;
+    if (reset) {
+        t.used = 0;
+        t.flops.clear();
+        t.shape.clear();
+    }
+    return CPSD_OK;
+}
+
+int launch_contract(const ContractPlan *p, const double *A, const double *B, double *C, double alpha) {
+    if (p->empty) return CPSD_OK;
+    CPSD_TRY(const_cast<ContractPlan *>(p)->upload());
+    const int bm = TILE_BM[p->cfg], bn = TILE_BN[p->cfg];
+    double *part = nullptr;
+    ScratchScope scope;
+    if (p->nparts > 0) CPSD_TRY(scratch(p->nparts * bm * bn, &part));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (timing().on) {
+        CPSD_TRY(timing_event(&e0));
+        CPSD_TRY(timing_event(&e1));
+        timing().flops.push_back(p->flops);
+        timing().shape.push_back({p->ntasks, p->nsegs, p->ntiles, p->cfg});
+        CPSD_TRY(cuda_check(cudaEventRecord(e0, stream()), "event record"));
+    }
+    static bool attr_set = false;
+    if (!attr_set) {
+        CPSD_TRY(cuda_check(cudaFuncSetAttribute(k_contract<128, 64, 4, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 smem_bytes<128, 64>()), "smem attr"));
+        CPSD_TRY(cuda_check(cudaFuncSetAttribute(k_contract<128, 32, 4, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 smem_bytes<128, 32>()), "smem attr"));
+        CPSD_TRY(cuda_check(cudaFuncSetAttribute(k_contract<64, 128, 2, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 smem_bytes<64, 128>()), "smem attr"));
+        CPSD_TRY(cuda_check(cudaFuncSetAttribute(k_contract<64, 64, 2, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 smem_bytes<64, 64>()), "smem attr"));
+        attr_set = true;
+    }
+    switch (p->cfg) {
+    case 0:
+        k_contract<128, 64, 4, 2><<<p->ntiles, NT, smem_bytes<128, 64>(), stream()>>>(
+            A, B, C, p->d_tasks, p->d_segs, p->d_tiles, alpha, part);
+        break;
+    case 1:
+        k_contract<128, 32, 4, 2><<<p->ntiles, NT, smem_bytes<128, 32>(), stream()>>>(
+            A, B, C, p->d_tasks, p->d_segs, p->d_tiles, alpha, part);
+        break;
+    case 2:
+        k_contract<64, 128, 2, 4><<<p->ntiles, NT, smem_bytes<64, 128>(), stream()>>>(
+            A, B, C, p->d_tasks, p->d_segs, p->d_tiles, alpha, part);
+        break;
+    default:
+        k_contract<64, 64, 2, 4><<<p->ntiles, NT, smem_bytes<64, 64>(), stream()>>>(
+            A, B, C, p->d_tasks, p->d_segs, p->d_tiles, alpha, part);
+        break;
+    }
+    count_launch();
+    ctx().flops += p->flops;
+    if (e1) CPSD_TRY(cuda_check(cudaEventRecord(e1, stream()), "event record"));
+    if (p->nreduce > 0) {
+        k_splitk_reduce<<<p->nreduce, NT, 0, stream()>>>(p->d_reduce, p->d_tasks, part, C, alpha, bm, bn);
+        count_launch();
+    }
+    return cuda_check(cudaGetLastError(), "k_contract");
+}
+
+}  // namespace cpsd

@@ -488,7 +488,7 @@ int cpsd_isymtrso(const cpsd_opt *in, cpsd_opt *out, int64_t s0, int64_t s1) {
 int cpsd_debug_contract_plan(const cpsd_opt *v1, const char *t1, const cpsd_opt *v2, const char *t2,
                              const cpsd_opt *v3, const char *t3, int64_t nb, int64_t sA, int64_t sB, int64_t sC,
                              const void **tasks, int64_t *ntasks, const void **segs, int64_t *nsegs,
-                             const void **tiles, int64_t *ntiles) {
+                             const void **tiles, int64_t *ntiles, int64_t *tile_bm, int64_t *tile_bn) {
     CPSD_TRY(need_init());
     Batch b;
     b.nb = nb;
@@ -503,7 +503,13 @@ int cpsd_debug_contract_plan(const cpsd_opt *v1, const char *t1, const cpsd_opt 
     *nsegs = (int64_t)p->h_segs.size();
     *tiles = p->h_tiles.data();
     *ntiles = (int64_t)p->h_tiles.size();
+    *tile_bm = TILE_BM[p->cfg];
+    *tile_bn = TILE_BN[p->cfg];
     return CPSD_OK;
+}
+
+int cpsd_contract_records(double *ms, double *flops, int64_t *shape, int64_t maxrec, int64_t *nrec) {
+    return contract_records(ms, flops, shape, maxrec, nrec);
 }
 
 int cpsd_debug_pairmap_plan(const cpsd_opt *in, int64_t op0, int64_t op1, int64_t tgt0, int64_t tgt1,

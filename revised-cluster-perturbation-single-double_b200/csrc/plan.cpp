@@ -61,8 +61,6 @@ void geom(const Desc &d, const i64 irr[4], i64 *base, i64 st[4], i64 *nleft) {
     *nleft = nl;
 }
 
-constexpr int TBM = 64, TBN = 64;  // tile shape of the contraction kernel
-
 }  // namespace
 
 int ContractPlan::upload() {
@@ -354,6 +352,25 @@ int plan_contract(const Desc &d1, const char *t1, const Desc &d2, const char *t2
         }
         i = j;
     }
+    // tile shape: the one with the least estimated time, counting the padded
+    // tensor-pipe work (FP64 ~35 TFLOP/s) and the operand re-reads (~6 TB/s)
+    int cfg = 0;
+    double best = 1e300;
+    for (int c = 0; c < 4; c++) {
+        double fl = 0, by = 0;
+        for (auto &tk : tasks) {
+            double mt = (double)((tk.M + TILE_BM[c] - 1) / TILE_BM[c]), nt = (double)((tk.N + TILE_BN[c] - 1) / TILE_BN[c]);
+            fl += 2.0 * mt * TILE_BM[c] * nt * TILE_BN[c] * (double)tk.Ktot;
+            by += 8.0 * (double)tk.Ktot * ((double)tk.M * nt + (double)tk.N * mt);
+        }
+        double t = fl / 35e12 + by / 6e12;
+        if (t < best * 0.999) {
+            best = t;
+            cfg = c;
+        }
+    }
+    const i64 TBM = TILE_BM[cfg], TBN = TILE_BN[cfg];
+    plan->cfg = cfg;
     // tiles, with split-K so that small outputs with long K still fill the GPU
     std::vector<TileDev> tiles;
     std::vector<int> red;

@@ -117,8 +117,13 @@ struct TileDev {
     i64 part;            // partial slot (split-K) or -1
 };
 
+// tile shapes of the contraction kernel: BM x BN = 128x64, 128x32, 64x128, 64x64
+extern const int TILE_BM[4];
+extern const int TILE_BN[4];
+
 struct ContractPlan {
     bool empty = true;
+    int cfg = 0;  // tile shape (index into TILE_BM / TILE_BN)
     int ntasks = 0, nsegs = 0, ntiles = 0;
     i64 nparts = 0;      // split-K partial tiles
     // host tables (kept for introspection) and their device copies,
@@ -170,6 +175,7 @@ int plan_pairmap(const Desc &din, int op0, int op1, i64 target_iop0, i64 target_
 int launch_contract(const ContractPlan *p, const double *A, const double *B, double *C, double alpha);
 int contract_timing(int enable);
 int contract_time(double *ms, int64_t *launches, double *flops, int reset);
+int contract_records(double *ms, double *flops, int64_t *shape, int64_t maxrec, int64_t *nrec);
 int launch_pairmap(const PairMapPlan *p, const double *in, double *out, double alpha, double beta, i64 nb = 1,
                    i64 in_stride = 0, i64 out_stride = 0);
 int launch_scale(double *x, i64 n, double beta);                  // x *= beta (beta 0: zero fill)

@@ -53,18 +53,20 @@ def decode(x, ext, st):
 def get_plan(o1, t1, o2, t2, o3, t3, nb=1, sA=0, sB=0, sC=0):
     P = [ctypes.c_void_p() for _ in range(3)]
     N = [I64() for _ in range(3)]
+    bm, bn = I64(), I64()
     rc = api.lib().cpsd_debug_contract_plan(ctypes.byref(o1), t1.encode(), ctypes.byref(o2), t2.encode(),
                                             ctypes.byref(o3), t3.encode(), I64(nb), I64(sA), I64(sB), I64(sC),
                                             ctypes.byref(P[0]), ctypes.byref(N[0]), ctypes.byref(P[1]),
-                                            ctypes.byref(N[1]), ctypes.byref(P[2]), ctypes.byref(N[2]))
+                                            ctypes.byref(N[1]), ctypes.byref(P[2]), ctypes.byref(N[2]),
+                                            ctypes.byref(bm), ctypes.byref(bn))
     api.check(rc, "plan")
     tasks = (TaskDev * N[0].value).from_address(P[0].value) if N[0].value else []
     segs = (SegDev * N[1].value).from_address(P[1].value) if N[1].value else []
     tiles = (TileDev * N[2].value).from_address(P[2].value) if N[2].value else []
-    return tasks, segs, tiles
+    return tasks, segs, tiles, (bm.value, bn.value)
 
 
-def emulate(tasks, segs, tiles, A, B, C, alpha):
+def emulate(tasks, segs, tiles, A, B, C, alpha, tile=(64, 64)):
     """C += alpha * contraction, exactly as k_contract indexes; bounds-checked."""
     C = C.copy()
     for ti, tk in enumerate(tasks):
@@ -96,9 +98,10 @@ def emulate(tasks, segs, tiles, A, B, C, alpha):
     cover = {}
     for t in tiles:
         cover.setdefault((t.task, t.mt, t.nt), []).append((t.k_lo, t.k_hi))
+    bm, bn = tile
     for ti, tk in enumerate(tasks):
-        for a in range((tk.M + 63) // 64):
-            for b in range((tk.N + 63) // 64):
+        for a in range((tk.M + bm - 1) // bm):
+            for b in range((tk.N + bn - 1) // bn):
                 r = sorted(cover.pop((ti, a, b)))
                 assert r[0][0] == 0 and r[-1][1] == tk.Ktot
                 for (x0, x1), (y0, y1) in zip(r, r[1:]):
@@ -207,9 +210,10 @@ def test_kernel_engine_plans(name, nirrep, nb):
     for o, p, i, y in ((o1, p1, j1, y1), (o2, p2, j2, y2), (o3, po, j3, so)):
         api.check(api.lib().cpsd_opt_init(ctypes.byref(o), api.arr8(p[0]), api.arr8(p[1]), api.arr8(p[2]),
                                            api.arr8(p[3]), I64(i[0]), I64(i[1]), I64(y), None), "opt")
-    tasks, segs, tiles = get_plan(o1, e1, o2, e2, o3, e3, nb, l1 if n1 > 1 else 0, l2 if n2 > 1 else 0,
-                                  l3 if nb > 1 else 0)
-    out = emulate(tasks, segs, tiles, A, B, C, 0.9)
+    tasks, segs, tiles, tile = get_plan(o1, e1, o2, e2, o3, e3, nb, l1 if n1 > 1 else 0, l2 if n2 > 1 else 0,
+                                        l3 if nb > 1 else 0)
+    assert tile in ((128, 64), (128, 32), (64, 128), (64, 64))
+    out = emulate(tasks, segs, tiles, A, B, C, 0.9, tile)
     for c in range(nb):
         ref = C[c * l3:(c + 1) * l3].copy()
         Ac = A[c * l1:(c + 1) * l1] if n1 > 1 else A
