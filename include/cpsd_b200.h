@@ -113,6 +113,30 @@ int cpsd_vv2v_dpd_222(const double *v1, const int64_t *p1_1, const int64_t *p1_2
                       double *v3, const int64_t *p3_1, const int64_t *p3_2, int64_t iop3_12,
                       int64_t sym3, const char *type3, double fact1, double fact2);
 
+/* No counterpart in the reference.  cpsd_vv2v_dpd_444 with the same
+ * arguments and results, for callers that may not allocate device memory
+ * during the call (all of HBM handed to their own pool, or no cudaMalloc /
+ * cudaFree stalls allowed in a time-critical loop): the contraction's plan
+ * tables and split-K partial tiles live in a fixed region compiled into
+ * the library, CPSD_NOALLOC_SCRATCH_BYTES (32 MiB) per device, instead of
+ * cudaMalloc'ed memory.  A contraction that needs more is rejected with
+ * CPSD_EARG before any work is queued.  Nothing in the region has to start
+ * at zero.  The region is shared by all calls on a device: calls queued on
+ * one stream are ordered, calls that overlap in time (other streams, other
+ * host threads) race.  The first call on each device does the set-up
+ * (region address, kernel attributes); make it before any stream capture
+ * begins. */
+#define CPSD_NOALLOC_SCRATCH_BYTES (32u << 20)
+int cpsd_vv2v_dpd_444_noalloc(const double *v1, const int64_t *p1_1, const int64_t *p1_2, int64_t iop1_12,
+                              const int64_t *p1_3, const int64_t *p1_4, int64_t iop1_34, int64_t sym1,
+                              const char *type1,
+                              const double *v2, const int64_t *p2_1, const int64_t *p2_2, int64_t iop2_12,
+                              const int64_t *p2_3, const int64_t *p2_4, int64_t iop2_34, int64_t sym2,
+                              const char *type2,
+                              double *v3, const int64_t *p3_1, const int64_t *p3_2, int64_t iop3_12,
+                              const int64_t *p3_3, const int64_t *p3_4, int64_t iop3_34, int64_t sym3,
+                              const char *type3, double fact1, double fact2);
+
 /* Fortran-callable binding of the same engine (gfortran/nvfortran ABI:
  * lower case + trailing underscore, every argument by reference, hidden
  * character lengths last), so the reference's call sites

@@ -128,6 +128,17 @@ def vv2v_dpd_444(v1, d1, t1, v2, d2, t2, v3, d3, t3, f1, f2):
         ctypes.c_double(f1), ctypes.c_double(f2)), "vv2v_dpd_444")
 
 
+def vv2v_dpd_444_noalloc(v1, d1, t1, v2, d2, t2, v3, d3, t3, f1, f2):
+    """vv2v_dpd_444 through the entry point that allocates no device memory
+    (tables and split-K partials in the library's fixed 32 MiB region)."""
+    (p1, i1, s1), (p2, i2, s2), (p3, i3, s3) = d1, d2, d3
+    check(lib().cpsd_vv2v_dpd_444_noalloc(
+        dptr(v1), arr8(p1[0]), arr8(p1[1]), I64(i1[0]), arr8(p1[2]), arr8(p1[3]), I64(i1[1]), I64(s1), t1.encode(),
+        dptr(v2), arr8(p2[0]), arr8(p2[1]), I64(i2[0]), arr8(p2[2]), arr8(p2[3]), I64(i2[1]), I64(s2), t2.encode(),
+        dptr(v3), arr8(p3[0]), arr8(p3[1]), I64(i3[0]), arr8(p3[2]), arr8(p3[3]), I64(i3[1]), I64(s3), t3.encode(),
+        ctypes.c_double(f1), ctypes.c_double(f2)), "vv2v_dpd_444_noalloc")
+
+
 def make_system(s):
     """System struct from a synth.System (or any object with the same fields)."""
     o = System()

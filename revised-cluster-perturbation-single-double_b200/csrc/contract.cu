@@ -360,4 +360,111 @@ int launch_contract(const ContractPlan *p, const double *A, const double *B, dou
     return cuda_check(cudaGetLastError(), "k_contract");
 }
 
+// ------------------------------------------- contraction without allocation
+// Some callers may not allocate device memory while they run a contraction:
+// a host program that hands (nearly) all of HBM to its own pool at start-up
+// sees cudaMalloc fail, and cudaMalloc / cudaFree can stall the device in
+// the middle of a time-critical loop.  For them, launch_contract_noalloc
+// keeps the plan tables and the split-K partial tiles in one fixed region
+// compiled into this library instead of the cudaMalloc'ed plan copies and
+// the scratch arena launch_contract uses.  Limits and rules:
+//  - the region holds CPSD_NOALLOC_SCRATCH_BYTES; a contraction whose
+//    tables plus partial tiles need more is rejected (CPSD_EARG) before any
+//    work is queued;
+//  - nothing in the region has to start at zero: every word a call reads
+//    was written earlier in the same call (tables copied in, partial tiles
+//    stored in full before the reduce reads them);
+//  - there is one region per device, so two calls whose work overlaps in
+//    time (different streams, or host threads) race on it; calls queued on
+//    one stream are ordered and safe;
+//  - the first call on each device does the set-up (symbol address of the
+//    region, kernel attributes); make that first call before any stream
+//    capture begins.
+namespace {
+__device__ __align__(256) unsigned char g_noalloc_scratch[CPSD_NOALLOC_SCRATCH_BYTES];
+
+constexpr int NOALLOC_MAXDEV = 64;
+unsigned char *g_noalloc_base[NOALLOC_MAXDEV];  // per device ordinal; null until set up
+
+int noalloc_setup(unsigned char **base) {
+    int dev = 0;
+    CPSD_TRY(cuda_check(cudaGetDevice(&dev), "cudaGetDevice"));
+    if (dev < 0 || dev >= NOALLOC_MAXDEV) return set_error(CPSD_EARG, "device ordinal beyond 63");
+    if (!g_noalloc_base[dev]) {
+        void *p = nullptr;
+        CPSD_TRY(cuda_check(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress(noalloc scratch)"));
+        CPSD_TRY(cuda_check(cudaFuncSetAttribute(k_contract<128, 64, 4, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 smem_bytes<128, 64>()), "smem attr"));
+        CPSD_TRY(cuda_check(cudaFuncSetAttribute(k_contract<128, 32, 4, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 smem_bytes<128, 32>()), "smem attr"));
+        CPSD_TRY(cuda_check(cudaFuncSetAttribute(k_contract<64, 128, 2, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 smem_bytes<64, 128>()), "smem attr"));
+        CPSD_TRY(cuda_check(cudaFuncSetAttribute(k_contract<64, 64, 2, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 smem_bytes<64, 64>()), "smem attr"));
+        g_noalloc_base[dev] = (unsigned char *)p;
+    }
+    *base = g_noalloc_base[dev];
+    return CPSD_OK;
+}
+
+size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+}  // namespace
+
+size_t contract_noalloc_bytes(const ContractPlan *p) {
+    if (p->empty) return 0;
+    const size_t tile = (size_t)TILE_BM[p->cfg] * TILE_BN[p->cfg] * sizeof(double);
+    return align256(p->h_tasks.size() * sizeof(TaskDev)) + align256(p->h_segs.size() * sizeof(SegDev)) +
+           align256(p->h_tiles.size() * sizeof(TileDev)) + align256(p->h_reduce.size() * sizeof(int)) +
+           align256((size_t)p->nparts * tile);
+}
+
+int launch_contract_noalloc(const ContractPlan *p, const double *A, const double *B, double *C, double alpha) {
+    if (p->empty) return CPSD_OK;
+    const size_t need = contract_noalloc_bytes(p);
+    if (need > (size_t)CPSD_NOALLOC_SCRATCH_BYTES)
+        return set_error(CPSD_EARG, "contraction needs " + std::to_string(need) +
+                                        " bytes of scratch; the no-allocation entry point holds at most " +
+                                        std::to_string((size_t)CPSD_NOALLOC_SCRATCH_BYTES));
+    unsigned char *base = nullptr;
+    CPSD_TRY(noalloc_setup(&base));
+    size_t off = 0;
+    auto place = [&](const void *src, size_t bytes, void **dst) -> int {
+        *dst = base + off;
+        off += align256(bytes);
+        if (bytes == 0) return CPSD_OK;
+        return cuda_check(cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, stream()), "copy plan tables");
+    };
+    void *d_tasks, *d_segs, *d_tiles, *d_reduce;
+    CPSD_TRY(place(p->h_tasks.data(), p->h_tasks.size() * sizeof(TaskDev), &d_tasks));
+    CPSD_TRY(place(p->h_segs.data(), p->h_segs.size() * sizeof(SegDev), &d_segs));
+    CPSD_TRY(place(p->h_tiles.data(), p->h_tiles.size() * sizeof(TileDev), &d_tiles));
+    CPSD_TRY(place(p->h_reduce.data(), p->h_reduce.size() * sizeof(int), &d_reduce));
+    double *part = p->nparts > 0 ? (double *)(base + off) : nullptr;
+    const TaskDev *tk = (const TaskDev *)d_tasks;
+    const SegDev *sg = (const SegDev *)d_segs;
+    const TileDev *tl = (const TileDev *)d_tiles;
+    const int bm = TILE_BM[p->cfg], bn = TILE_BN[p->cfg];
+    switch (p->cfg) {
+    case 0:
+        k_contract<128, 64, 4, 2><<<p->ntiles, NT, smem_bytes<128, 64>(), stream()>>>(A, B, C, tk, sg, tl, alpha, part);
+        break;
+    case 1:
+        k_contract<128, 32, 4, 2><<<p->ntiles, NT, smem_bytes<128, 32>(), stream()>>>(A, B, C, tk, sg, tl, alpha, part);
+        break;
+    case 2:
+        k_contract<64, 128, 2, 4><<<p->ntiles, NT, smem_bytes<64, 128>(), stream()>>>(A, B, C, tk, sg, tl, alpha, part);
+        break;
+    default:
+        k_contract<64, 64, 2, 4><<<p->ntiles, NT, smem_bytes<64, 64>(), stream()>>>(A, B, C, tk, sg, tl, alpha, part);
+        break;
+    }
+    count_launch();
+    ctx().flops += p->flops;
+    if (p->nreduce > 0) {
+        k_splitk_reduce<<<p->nreduce, NT, 0, stream()>>>((const int *)d_reduce, tk, part, C, alpha, bm, bn);
+        count_launch();
+    }
+    return cuda_check(cudaGetLastError(), "k_contract (no allocation)");
+}
+
 }  // namespace cpsd

@@ -372,6 +372,35 @@ int cpsd_vv2v_dpd_444(const double *v1, const int64_t *p1_1, const int64_t *p1_2
     return engine(a, t1, b, t2, c, t3, fact1, fact2);
 }
 
+// engine() for callers that may not allocate device memory: same plan and
+// kernels, tables and partial tiles in the library's fixed region; the
+// size check comes before V3 is scaled so a rejected call changes nothing
+int cpsd_vv2v_dpd_444_noalloc(const double *v1, const int64_t *p1_1, const int64_t *p1_2, int64_t iop1_12,
+                              const int64_t *p1_3, const int64_t *p1_4, int64_t iop1_34, int64_t sym1,
+                              const char *type1, const double *v2, const int64_t *p2_1, const int64_t *p2_2,
+                              int64_t iop2_12, const int64_t *p2_3, const int64_t *p2_4, int64_t iop2_34,
+                              int64_t sym2, const char *type2, double *v3, const int64_t *p3_1,
+                              const int64_t *p3_2, int64_t iop3_12, const int64_t *p3_3, const int64_t *p3_4,
+                              int64_t iop3_34, int64_t sym3, const char *type3, double fact1, double fact2) {
+    CPSD_TRY(need_init());
+    Ten a = ten(p1_1, p1_2, p1_3, p1_4, iop1_12, iop1_34, sym1, (double *)v1);
+    Ten b = ten(p2_1, p2_2, p2_3, p2_4, iop2_12, iop2_34, sym2, (double *)v2);
+    Ten c = ten(p3_1, p3_2, p3_3, p3_4, iop3_12, iop3_34, sym3, v3);
+    char t1[5], t2[5], t3[5];
+    type4(type1, 4, t1);
+    type4(type2, 4, t2);
+    type4(type3, 4, t3);
+    const ContractPlan *p;
+    CPSD_TRY(plan_contract(a.d, t1, b.d, t2, c.d, t3, Batch{}, &p));
+    size_t need = contract_noalloc_bytes(p);
+    if (need > (size_t)CPSD_NOALLOC_SCRATCH_BYTES)
+        return set_error(CPSD_EARG, "contraction needs " + std::to_string(need) +
+                                        " bytes of scratch; the no-allocation entry point holds at most " +
+                                        std::to_string((size_t)CPSD_NOALLOC_SCRATCH_BYTES));
+    if (fact2 != 1.0) CPSD_TRY(launch_scale(c.arr, c.len(), fact2));
+    return launch_contract_noalloc(p, a.arr, b.arr, c.arr, fact1);
+}
+
 int cpsd_vv2v_dpd_424(const double *v1, const int64_t *p1_1, const int64_t *p1_2, int64_t iop1_12,
                       const int64_t *p1_3, const int64_t *p1_4, int64_t iop1_34, int64_t sym1, const char *type1,
                       const double *v2, const int64_t *p2_1, const int64_t *p2_2, int64_t iop2_12, int64_t sym2,

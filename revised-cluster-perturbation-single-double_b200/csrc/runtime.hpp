@@ -173,6 +173,10 @@ int plan_pairmap(const Desc &din, int op0, int op1, i64 target_iop0, i64 target_
 
 // ------------------------------------------------------------- launches
 int launch_contract(const ContractPlan *p, const double *A, const double *B, double *C, double alpha);
+// same contraction with its tables and partial tiles in the library's fixed
+// device region (no allocation); bytes of that region a plan needs
+int launch_contract_noalloc(const ContractPlan *p, const double *A, const double *B, double *C, double alpha);
+size_t contract_noalloc_bytes(const ContractPlan *p);
 int contract_timing(int enable);
 int contract_time(double *ms, int64_t *launches, double *flops, int reset);
 int contract_records(double *ms, double *flops, int64_t *shape, int64_t maxrec, int64_t *nrec);
