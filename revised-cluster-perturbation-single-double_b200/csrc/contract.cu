@@ -207,34 +207,34 @@ __global__ void __launch_bounds__(NT, 2) k_contract(const double *__restrict__ A
     }
 }
 
-// sum the split-K partial tiles of one output tile in a fixed order
+// Sum the split-K partial tiles of the output tiles in a fixed order.  One
+// thread per tile element: block b covers elements [NT*(b % chunks), +NT)
+// of reduce group b / chunks (chunks = bm*bn / NT), with four independent
+// partial sums so that the loads of several partial tiles are in flight.
 __global__ void __launch_bounds__(NT) k_splitk_reduce(const int *__restrict__ red, const TaskDev *__restrict__ tasks,
                                                       const double *__restrict__ partial, double *__restrict__ C,
                                                       double alpha, int bm, int bn) {
-    const int *r = red + 5 * blockIdx.x;
+    const int chunks = bm * bn / NT;
+    const int *r = red + 5 * (blockIdx.x / chunks);
+    const int e = (blockIdx.x % chunks) * NT + threadIdx.x;
     const TaskDev &tk = tasks[r[0]];
-    const i64 m0 = (i64)r[1] * bm, n0 = (i64)r[2] * bn;
+    const i64 m = (i64)r[1] * bm + e / bn, n = (i64)r[2] * bn + e % bn;
+    if (m >= tk.M || n >= tk.N) return;
     const i64 p0 = r[3];
     const int ns = r[4];
-    __shared__ i64 offM[128], offN[128];
-    int tid = threadIdx.x;
-    if (tid < bm) {
-        i64 m = m0 + tid;
-        offM[tid] = (m < tk.M) ? decode1(m, tk.nm, tk.mExt, tk.mSC) : -1;
+    const size_t ts = (size_t)bm * bn;
+    const double *P = partial + (size_t)p0 * ts + e;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    int q = 0;
+    for (; q + 4 <= ns; q += 4) {
+        s0 += P[(size_t)q * ts];
+        s1 += P[(size_t)(q + 1) * ts];
+        s2 += P[(size_t)(q + 2) * ts];
+        s3 += P[(size_t)(q + 3) * ts];
     }
-    if (tid < bn) {
-        i64 n = n0 + tid;
-        offN[tid] = (n < tk.N) ? decode1(n, tk.nn, tk.nExt, tk.nSC) : -1;
-    }
-    __syncthreads();
-    for (int e = tid; e < bm * bn; e += NT) {
-        int mi = e / bn, ni = e % bn;
-        i64 om = offM[mi], on = offN[ni];
-        if (om < 0 || on < 0) continue;
-        double s = 0.0;
-        for (int q = 0; q < ns; q++) s += partial[(size_t)(p0 + q) * (bm * bn) + e];
-        C[tk.baseC + om + on] += alpha * s;
-    }
+    for (; q < ns; q++) s0 += P[(size_t)q * ts];
+    const double s = (s0 + s1) + (s2 + s3);
+    C[tk.baseC + decode1(m, tk.nm, tk.mExt, tk.mSC) + decode1(n, tk.nn, tk.nExt, tk.nSC)] += alpha * s;
 }
 
 // optional CUDA-event timing of every contraction launch (on its stream)
@@ -354,7 +354,8 @@ int launch_contract(const ContractPlan *p, const double *A, const double *B, dou
     ctx().flops += p->flops;
     if (e1) CPSD_TRY(cuda_check(cudaEventRecord(e1, stream()), "event record"));
     if (p->nreduce > 0) {
-        k_splitk_reduce<<<p->nreduce, NT, 0, stream()>>>(p->d_reduce, p->d_tasks, part, C, alpha, bm, bn);
+        k_splitk_reduce<<<p->nreduce * (bm * bn / NT), NT, 0, stream()>>>(p->d_reduce, p->d_tasks, part, C, alpha,
+                                                                          bm, bn);
         count_launch();
     }
     return cuda_check(cudaGetLastError(), "k_contract");
@@ -461,7 +462,8 @@ int launch_contract_noalloc(const ContractPlan *p, const double *A, const double
     count_launch();
     ctx().flops += p->flops;
     if (p->nreduce > 0) {
-        k_splitk_reduce<<<p->nreduce, NT, 0, stream()>>>((const int *)d_reduce, tk, part, C, alpha, bm, bn);
+        k_splitk_reduce<<<p->nreduce * (bm * bn / NT), NT, 0, stream()>>>((const int *)d_reduce, tk, part, C, alpha,
+                                                                          bm, bn);
         count_launch();
     }
     return cuda_check(cudaGetLastError(), "k_contract (no allocation)");

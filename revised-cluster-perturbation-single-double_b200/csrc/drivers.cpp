@@ -69,6 +69,15 @@ Ints make_ints(const Sys &S, const cpsd_integrals *I) {
     return x;
 }
 
+// a program does not write its integrals: expanded copies of them are kept
+// for the whole run (ConstOperands)
+struct IntegralScope {
+    const double *a[6];
+    ConstOperands scope;
+    explicit IntegralScope(const cpsd_integrals *I)
+        : a{I->ijkl, I->ijka, I->abij, I->iabj, I->abci, I->abcd}, scope(a, 6) {}
+};
+
 // pinned host mailbox for the few scalars the host control flow needs
 double *mailbox() {
     static double *p = nullptr;
@@ -345,6 +354,7 @@ int cpsd_cis_run(const cpsd_system *s, const cpsd_integrals *I, const cpsd_param
     Sys S;
     CPSD_TRY(make_sys(s, &S));
     Ints X = make_ints(S, I);
+    IntegralScope keep(I);
     i64 ne = 0;
     for (int r = 0; r < 8; r++) ne += S.popo[r] + S.popv[r];
     std::vector<double> eorb((size_t)ne);
@@ -384,6 +394,7 @@ int cpsd_ground(const cpsd_system *s, const cpsd_integrals *I, const cpsd_params
     Sys S;
     CPSD_TRY(make_sys(s, &S));
     Ints X = make_ints(S, I);
+    IntegralScope keep(I);
     const i64 *o = S.popo, *v = S.popv;
     ScratchScope sc;
     i64 l1 = irpdso(1, v, o, 1), l2 = idsymsoc(1, v, v, 0, o, o, 0);
@@ -440,6 +451,7 @@ int cpsd_calJ(const cpsd_system *s, const cpsd_integrals *I, const double *T2_1,
     Sys S;
     CPSD_TRY(make_sys(s, &S));
     Ints X = make_ints(S, I);
+    IntegralScope keep(I);
     const i64 *o = S.popo, *v = S.popv;
     Ten t2a = ten(v, v, o, o, 0, 0, 1, (double *)T2_1), t1b = ten(v, o, ZORB, ZORB, 1, 1, 1, (double *)T1_2);
     Ten t2b = ten(v, v, o, o, 0, 0, 1, (double *)T2_2);
@@ -618,6 +630,7 @@ int cpsd_eecpsd_roots(const cpsd_system *s, const cpsd_integrals *I, const cpsd_
     CPSD_TRY(make_sys(s, &S));
     Ints X = make_ints(S, I);
     if (nroot <= 0) return CPSD_OK;
+    IntegralScope keep(I);
     const i64 l1 = irpdso(symR, S.popv, S.popo, 1), l2 = idsymsoc(symR, S.popv, S.popv, 0, S.popo, S.popo, 0);
     if (p->batch_roots) {
         i64 it = 0;
@@ -641,6 +654,7 @@ int cpsd_pipeline(const cpsd_system *s, const cpsd_integrals *I, const cpsd_para
                   double *w2, double *w3, int64_t *nroots) {
     Sys S;
     CPSD_TRY(make_sys(s, &S));
+    IntegralScope keep(I);
     const i64 *o = S.popo, *v = S.popv;
     i64 nroot = 0, rlen = 0;
     for (i64 sym = 1; sym <= S.nirrep; sym++) {

@@ -18,6 +18,16 @@ Ten ten_of(const cpsd_opt *t);
 Ten ten(const i64 *p0, const i64 *p1, const i64 *p2, const i64 *p3, i64 iop0, i64 iop1, i64 sym, double *arr,
         i64 bs = 0);
 
+// Scope during which the given device arrays (a program's integrals) are
+// not written: expanded copies made of them are kept and reused until the
+// outermost scope ends.
+struct ConstOperands {
+    ConstOperands(const double *const *arrs, int n);
+    ~ConstOperands();
+    ConstOperands(const ConstOperands &) = delete;
+    ConstOperands &operator=(const ConstOperands &) = delete;
+};
+
 // V3 = f1 * V1 (x) V2 + f2 * V3 (the vv2v_dpd engines)
 int engine(const Ten &v1, const char *t1, const Ten &v2, const char *t2, Ten &v3, const char *t3, double f1,
            double f2, i64 nb = 1);

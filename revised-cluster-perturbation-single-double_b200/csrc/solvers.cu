@@ -74,80 +74,128 @@ __device__ double block_amax(const double *x, int n, double *sh, int *shi) {
     return (idx < n) ? x[idx] : 0.0;
 }
 
-// cyclic Jacobi on a symmetric n x n matrix S (row-major, ld DAV_MAXD) by
-// one warp; eigenvectors accumulate in V (columns)
-__device__ void warp_jacobi(double *S, double *V, int n) {
+// dot product of two length-n vectors by one warp (result in every lane)
+__device__ double warp_dot(const double *x, const double *y, int n) {
     const int lane = threadIdx.x & 31;
-    for (int k = 0; k < n; k++) V[lane * DAV_MAXD + k] = (lane < n) ? (lane == k ? 1.0 : 0.0) : 0.0;
-    __syncwarp();
-    // classic cyclic Jacobi (Golub & Van Loan, Alg. 8.5.3): an element below
-    // eps * sqrt(|a_pp a_qq|) is negligible and set to zero; a sweep without
-    // rotations ends the iteration
-    for (int sweep = 0; sweep < 50; sweep++) {
-        int rotated = 0;
-        for (int p = 0; p < n - 1; p++)
-            for (int q = p + 1; q < n; q++) {
-                double apq = S[p * DAV_MAXD + q];
-                double app = S[p * DAV_MAXD + p], aqq = S[q * DAV_MAXD + q];
-                if (fabs(apq) <= 1.0e-17 * sqrt(fabs(app) * fabs(aqq)) || apq == 0.0) {
-                    __syncwarp();
-                    if (lane == 0) {
-                        S[p * DAV_MAXD + q] = 0.0;
-                        S[q * DAV_MAXD + p] = 0.0;
-                    }
-                    __syncwarp();
-                    continue;
-                }
-                rotated = 1;
-                double tau = (aqq - app) / (2.0 * apq);
-                double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
-                double c = 1.0 / sqrt(1.0 + t * t), s = t * c;
-                __syncwarp();
-                if (lane < n) {  // S <- S J
-                    double skp = S[lane * DAV_MAXD + p], skq = S[lane * DAV_MAXD + q];
-                    S[lane * DAV_MAXD + p] = c * skp - s * skq;
-                    S[lane * DAV_MAXD + q] = s * skp + c * skq;
-                    double vkp = V[lane * DAV_MAXD + p], vkq = V[lane * DAV_MAXD + q];
-                    V[lane * DAV_MAXD + p] = c * vkp - s * vkq;
-                    V[lane * DAV_MAXD + q] = s * vkp + c * vkq;
-                }
-                __syncwarp();
-                if (lane < n) {  // S <- J^T S
-                    double spk = S[p * DAV_MAXD + lane], sqk = S[q * DAV_MAXD + lane];
-                    S[p * DAV_MAXD + lane] = c * spk - s * sqk;
-                    S[q * DAV_MAXD + lane] = s * spk + c * sqk;
-                }
-                __syncwarp();
-            }
-        if (!rotated) break;
-    }
+    double a = 0.0;
+    for (int k = lane; k < n; k += 32) a = fma(x[k], y[k], a);
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    return a;
 }
 
-// Schmidt_2D (mod_davidson.f90:642-680) on columns of length len
-__device__ void schmidt_2d(const double *in, double *out, int len, int dim) {
-    for (int i = 0; i < len * dim; i++) out[i] = in[i];
-    for (int i = 1; i < dim; i++) {
-        for (int j = 0; j < i; j++) {
-            double ov = 0.0;
-            for (int k = 0; k < len; k++) ov += out[j * len + k] * out[i * len + k];
-            for (int k = 0; k < len; k++) out[i * len + k] += -ov * out[j * len + k];
+// Cyclic Jacobi on the symmetric n x n matrix S (row-major, ld DAV_MAXD,
+// zero outside n x n) by the whole block; eigenvectors accumulate in the
+// columns of V.  Classic threshold (Golub & Van Loan, Alg. 8.5.3): an
+// element below 1e-17 sqrt(|a_pp a_qq|) is negligible and set to zero; a
+// sweep without rotations ends the iteration.  The n(n-1)/2 rotations of a
+// sweep run as n-1 rounds of n/2 disjoint rotations (round-robin pairing,
+// n padded to even), each round one parallel update of S and V.
+__device__ void block_jacobi(double *S, double *V, int n) {
+    __shared__ double cs[DAV_MAXD], sn[DAV_MAXD];
+    __shared__ int pp[DAV_MAXD / 2], qq[DAV_MAXD / 2];
+    __shared__ int rotated;
+    const int tid = threadIdx.x;
+    const int m = (n + 1) & ~1, half = m / 2;
+    for (int e = tid; e < DAV_MAXD * DAV_MAXD; e += DT) {
+        int i = e / DAV_MAXD, j = e % DAV_MAXD;
+        V[e] = (i == j && i < m) ? 1.0 : 0.0;
+    }
+    for (int sweep = 0; sweep < 50 && m > 1; sweep++) {
+        if (tid == 0) rotated = 0;
+        __syncthreads();
+        for (int r = 0; r < m - 1; r++) {
+            if (tid < half) {  // pair k of round r: (m-1, r) and (r+k, r-k) mod m-1
+                int a, b;
+                if (tid == 0) {
+                    a = r;
+                    b = m - 1;
+                } else {
+                    a = (r + tid) % (m - 1);
+                    b = (r - tid + (m - 1)) % (m - 1);
+                }
+                int p = min(a, b), q = max(a, b);
+                double apq = S[p * DAV_MAXD + q];
+                double app = S[p * DAV_MAXD + p], aqq = S[q * DAV_MAXD + q];
+                double c = 1.0, s = 0.0;
+                if (!(fabs(apq) <= 1.0e-17 * sqrt(fabs(app) * fabs(aqq)) || apq == 0.0)) {
+                    double tau = (aqq - app) / (2.0 * apq);
+                    double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+                    c = 1.0 / sqrt(1.0 + t * t);
+                    s = t * c;
+                    rotated = 1;
+                }
+                pp[tid] = p;
+                qq[tid] = q;
+                cs[tid] = c;
+                sn[tid] = s;
+            }
+            __syncthreads();
+            // S <- J^T S J on the 2x2 blocks of (pair k rows, pair l columns)
+            for (int idx = tid; idx < half * half; idx += DT) {
+                const int k = idx / half, l = idx % half;
+                const int pk = pp[k], qk = qq[k], pl = pp[l], ql = qq[l];
+                const double ck = cs[k], sk = sn[k], cl = cs[l], sl = sn[l];
+                double b00 = S[pk * DAV_MAXD + pl], b01 = S[pk * DAV_MAXD + ql];
+                double b10 = S[qk * DAV_MAXD + pl], b11 = S[qk * DAV_MAXD + ql];
+                double t00 = cl * b00 - sl * b01, t01 = sl * b00 + cl * b01;
+                double t10 = cl * b10 - sl * b11, t11 = sl * b10 + cl * b11;
+                double n00 = ck * t00 - sk * t10, n01 = ck * t01 - sk * t11;
+                double n10 = sk * t00 + ck * t10, n11 = sk * t01 + ck * t11;
+                if (k == l) n01 = n10 = 0.0;  // annihilated (or negligible) element
+                S[pk * DAV_MAXD + pl] = n00;
+                S[pk * DAV_MAXD + ql] = n01;
+                S[qk * DAV_MAXD + pl] = n10;
+                S[qk * DAV_MAXD + ql] = n11;
+            }
+            // V <- V J
+            for (int idx = tid; idx < m * half; idx += DT) {
+                const int i = idx / half, l = idx % half;
+                const int pl = pp[l], ql = qq[l];
+                const double cl = cs[l], sl = sn[l];
+                double vp = V[i * DAV_MAXD + pl], vq = V[i * DAV_MAXD + ql];
+                V[i * DAV_MAXD + pl] = cl * vp - sl * vq;
+                V[i * DAV_MAXD + ql] = sl * vp + cl * vq;
+            }
+            __syncthreads();
         }
-        double nrm = 0.0;
-        for (int k = 0; k < len; k++) nrm += out[i * len + k] * out[i * len + k];
+        if (!rotated) break;
+        __syncthreads();
+    }
+    __syncthreads();
+}
+
+// Schmidt_2D (mod_davidson.f90:642-680) on the dim columns (length len <= 32)
+// of `in`, by one warp: lane k holds row k; modified Gram-Schmidt in the
+// reference's order
+__device__ void warp_schmidt_2d(const double *in, double *out, int len, int dim) {
+    const int lane = threadIdx.x & 31;
+    for (int i = 0; i < dim; i++)
+        if (lane < len) out[i * len + lane] = in[i * len + lane];
+    __syncwarp();
+    for (int i = 1; i < dim; i++) {
+        double x = (lane < len) ? out[i * len + lane] : 0.0;
+        for (int j = 0; j < i; j++) {
+            double y = (lane < len) ? out[j * len + lane] : 0.0;
+            double ov = x * y;
+            for (int o = 16; o > 0; o >>= 1) ov += __shfl_xor_sync(0xffffffffu, ov, o);
+            x += -ov * y;
+        }
+        double nrm = x * x;
+        for (int o = 16; o > 0; o >>= 1) nrm += __shfl_xor_sync(0xffffffffu, nrm, o);
         nrm = sqrt(nrm);
-        for (int k = 0; k < len; k++) out[i * len + k] *= 1.0 / nrm;
+        if (lane < len) out[i * len + lane] = x * (1.0 / nrm);
+        __syncwarp();
     }
 }
 
 __global__ void __launch_bounds__(DT) k_dav_init(DavState *st, DavBuffers b) {
-    __shared__ double sh[DT / 32 + 1];
     DavState &s = *st;
     const int n = s.dimA, D = s.D, nr = s.nroot;
-    for (int i = 0; i < nr; i++)
-        for (int j = 0; j < nr; j++) {
-            double v = block_dot(b.fileEV + (size_t)j * (n + 1) + 1, b.AB[0] + (size_t)i * n, n, sh);
-            if (threadIdx.x == 0) s.Abar[j + i * D] = v;
-        }
+    for (int e = threadIdx.x >> 5; e < nr * nr; e += DT / 32) {
+        const int i = e / nr, j = e % nr;
+        double v = warp_dot(b.fileEV + (size_t)j * (n + 1) + 1, b.AB[0] + (size_t)i * n, n);
+        if ((threadIdx.x & 31) == 0) s.Abar[j + i * D] = v;
+    }
     if (threadIdx.x == 0) {
         for (int i = 0; i < nr; i++) {
             s.eigenVal[i] = b.fileEV[(size_t)i * (n + 1)];
@@ -164,7 +212,7 @@ __global__ void __launch_bounds__(DT) k_dav_init(DavState *st, DavBuffers b) {
 }
 
 __global__ void __launch_bounds__(DT) k_dav_step(DavState *st, DavBuffers b) {
-    __shared__ double S[DAV_MAXD * DAV_MAXD], V[DAV_MAXD * DAV_MAXD];
+    __shared__ double S[DAV_MAXD * DAV_MAXD], V[DAV_MAXD * DAV_MAXD], ovl[DAV_MAXD];
     __shared__ double sh[DT / 32 + 1];
     __shared__ int shi[DT / 32 + 1];
     DavState &s = *st;
@@ -183,13 +231,14 @@ __global__ void __launch_bounds__(DT) k_dav_step(DavState *st, DavBuffers b) {
         S[e] = (i < dimIter && j < dimIter) ? 0.5 * (s.Abar[i + j * D] + s.Abar[j + i * D]) : 0.0;
     }
     __syncthreads();
-    if (tid < 32) warp_jacobi(S, V, dimIter);
+    block_jacobi(S, V, dimIter);
+    for (int e = tid; e < D * dimIter; e += DT) {
+        int i = e % D, k = e / D;
+        s.vecR[i + k * D] = (i < dimIter) ? V[i * DAV_MAXD + k] : 0.0;
+    }
     __syncthreads();
     if (tid == 0) {
-        for (int k = 0; k < dimIter; k++) {
-            s.valR[k] = S[k * DAV_MAXD + k];
-            for (int i = 0; i < D; i++) s.vecR[i + k * D] = (i < dimIter) ? V[i * DAV_MAXD + k] : 0.0;
-        }
+        for (int k = 0; k < dimIter; k++) s.valR[k] = S[k * DAV_MAXD + k];
         // sort (mod_davidson.f90:620-640)
         int *low = s.lowestE;
         for (int i = 0; i < dimIter; i++) low[i] = i + 1;
@@ -225,11 +274,12 @@ __global__ void __launch_bounds__(DT) k_dav_step(DavState *st, DavBuffers b) {
     // ---- collapse when the subspace was full (mod_davidson.f90:266-325)
     if (dim_exceed) {
         const int nd = s.ndimIter;
-        if (tid == 0) {
-            for (int i = 0; i < nd; i++)
-                for (int k = 0; k < dimIter; k++) s.oldE[k + i * dimIter] = s.vecR[k + (s.lowestE[i] - 1) * D];
-            schmidt_2d(s.oldE, s.newE, dimIter, nd);
+        for (int e = tid; e < nd * dimIter; e += DT) {
+            int k = e % dimIter, i = e / dimIter;
+            s.oldE[k + i * dimIter] = s.vecR[k + (s.lowestE[i] - 1) * D];
         }
+        __syncthreads();
+        if (tid < 32) warp_schmidt_2d(s.oldE, s.newE, dimIter, nd);
         __syncthreads();
         const int nw = 1 - cur;
         for (int ir = 0; ir < nd; ir++)
@@ -247,11 +297,12 @@ __global__ void __launch_bounds__(DT) k_dav_step(DavState *st, DavBuffers b) {
         cur = nw;
         dimFree = s.ndimFree;
         dimIter = nd;
-        for (int i = 0; i < dimIter; i++)
-            for (int j = 0; j < dimIter; j++) {
-                double v = block_dot(b.AB[cur] + (size_t)i * n, b.B[cur] + (size_t)j * n, n, sh);
-                if (tid == 0) s.Abar[j + i * D] = v;
-            }
+        for (int e = tid >> 5; e < dimIter * dimIter; e += DT / 32) {
+            const int i = e / dimIter, j = e % dimIter;
+            double v = warp_dot(b.AB[cur] + (size_t)i * n, b.B[cur] + (size_t)j * n, n);
+            if ((tid & 31) == 0) s.Abar[j + i * D] = v;
+        }
+        __syncthreads();
     }
     // ---- steps 4-6 per root
     int nNew = 0, nconv = 0;
@@ -304,9 +355,21 @@ __global__ void __launch_bounds__(DT) k_dav_step(DavState *st, DavBuffers b) {
         double nrm = sqrt(block_dot(b.w1, b.w1, n, sh));
         for (int k = tid; k < n; k += DT) b.w1[k] *= 1.0 / nrm;
         __syncthreads();
-        for (int i = 0; i < dimIter + nNew; i++) {
-            double ov = block_dot(b.B[cur] + (size_t)i * n, b.w1, n, sh);
-            for (int k = tid; k < n; k += DT) b.w1[k] += -ov * b.B[cur][(size_t)i * n + k];
+        // projections on the basis: classical Gram-Schmidt applied twice
+        // (same result as the reference's sequential projections to
+        // rounding, with all overlaps of a pass computed at once)
+        const int nb = dimIter + nNew;
+        for (int pass = 0; pass < 2; pass++) {
+            for (int i = tid >> 5; i < nb; i += DT / 32) {
+                double v = warp_dot(b.B[cur] + (size_t)i * n, b.w1, n);
+                if ((tid & 31) == 0) ovl[i] = v;
+            }
+            __syncthreads();
+            for (int k = tid; k < n; k += DT) {
+                double x = b.w1[k];
+                for (int i = 0; i < nb; i++) x += -ovl[i] * b.B[cur][(size_t)i * n + k];
+                b.w1[k] = x;
+            }
             __syncthreads();
         }
         nrm = sqrt(block_dot(b.w1, b.w1, n, sh));
@@ -344,21 +407,25 @@ __global__ void __launch_bounds__(DT) k_dav_step(DavState *st, DavBuffers b) {
 
 // Ritz-matrix update with the new vectors (mod_davidson.f90:460-496)
 __global__ void __launch_bounds__(DT) k_dav_abar(DavState *st, DavBuffers b) {
-    __shared__ double sh[DT / 32 + 1];
     DavState &s = *st;
     if (s.done) return;
     const int n = s.dimA, D = s.D, dimIter = s.dimIter, nNew = s.nNew, cur = s.cur;
     const double *B = b.B[cur], *AB = b.AB[cur];
-    for (int j = 0; j < dimIter; j++)
-        for (int i = dimIter; i < dimIter + nNew; i++) {
-            double v = block_dot(B + (size_t)i * n, AB + (size_t)j * n, n, sh);
-            if (threadIdx.x == 0) s.Abar[i + j * D] = v;
+    // new rows (i >= dimIter, j < dimIter) then new columns (j >= dimIter)
+    const int nrow = nNew * dimIter, tot = nrow + nNew * (dimIter + nNew);
+    for (int e = threadIdx.x >> 5; e < tot; e += DT / 32) {
+        int i, j;
+        if (e < nrow) {
+            j = e / nNew;
+            i = dimIter + e % nNew;
+        } else {
+            j = dimIter + (e - nrow) / (dimIter + nNew);
+            i = (e - nrow) % (dimIter + nNew);
         }
-    for (int j = dimIter; j < dimIter + nNew; j++)
-        for (int i = 0; i < dimIter + nNew; i++) {
-            double v = block_dot(B + (size_t)i * n, AB + (size_t)j * n, n, sh);
-            if (threadIdx.x == 0) s.Abar[i + j * D] = v;
-        }
+        double v = warp_dot(B + (size_t)i * n, AB + (size_t)j * n, n);
+        if ((threadIdx.x & 31) == 0) s.Abar[i + j * D] = v;
+    }
+    __syncthreads();
     if (threadIdx.x == 0) {
         s.dimIter = dimIter + nNew;
         s.iterations++;
@@ -458,14 +525,17 @@ __global__ void __launch_bounds__(DT) k_diis(DiisState *st, DiisBuffers b, int i
     }
     __syncthreads();
     const int nd = s.ndimr;
-    for (int i = 0; i < nd; i++)
-        for (int j = 0; j <= i; j++) {
-            double x = block_dot(b.err + (size_t)i * len, b.err + (size_t)j * len, len, sh);
-            if (tid == 0) {
-                Bm[i + j * DIIS_MAXDIM] = x;
-                Bm[j + i * DIIS_MAXDIM] = x;
-            }
+    // only the row of the error vector stored now changes; the others are
+    // kept in the state from earlier steps
+    for (int j = tid >> 5; j < nd; j += DT / 32) {
+        double x = warp_dot(b.err + (size_t)id * len, b.err + (size_t)j * len, len);
+        if ((tid & 31) == 0) {
+            s.Bm[id + j * DIIS_MAXDIM] = x;
+            s.Bm[j + id * DIIS_MAXDIM] = x;
         }
+    }
+    __syncthreads();
+    for (int e = tid; e < DIIS_MAXDIM * DIIS_MAXDIM; e += DT) Bm[e] = s.Bm[e];
     __syncthreads();
     if (tid == 0) {  // dodiis (src/libsrint/dodiis.f): bordered system with -1e-4
         const int n1 = nd + 1;

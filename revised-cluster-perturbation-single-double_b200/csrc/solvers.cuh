@@ -41,6 +41,7 @@ constexpr int DIIS_MAXDIM = 16;
 struct DiisState {
     int len, maxdim, ndimr, idimr;
     double res;
+    double Bm[DIIS_MAXDIM * DIIS_MAXDIM];  // error-vector overlaps of the stored steps
 };
 struct DiisBuffers {
     double *prev, *err, *amp;  // len, maxdim*len, maxdim*len
