@@ -47,20 +47,6 @@ struct Unit {
     int cls;      // 0 M, 1 N, 2 K
 };
 
-// block geometry of a tensor for the four slot irreps
-void geom(const Desc &d, const i64 irr[4], i64 *base, i64 st[4], i64 *nleft) {
-    i64 L = dp(irr[0], irr[1]), R = dp(irr[2], irr[3]);
-    i64 nl = d.nleft(L);
-    i64 lsub = isymoffso(irr[1], L, d.pop[0], d.pop[1], d.iop[0]) - 1;
-    i64 rsub = isymoffso(irr[3], R, d.pop[2], d.pop[3], d.iop[1]) - 1;
-    *base = d.block_base(R) + rsub * nl + lsub;
-    st[0] = 1;
-    st[1] = d.pop[0][irr[0] - 1];
-    st[2] = nl;
-    st[3] = nl * d.pop[2][irr[2] - 1];
-    *nleft = nl;
-}
-
 }  // namespace
 
 int ContractPlan::upload() {
@@ -145,6 +131,11 @@ int plan_contract(const Desc &d1, const char *t1, const Desc &d2, const char *t2
         if (memcmp(D[ta]->pop[where[k][ta]], D[tb]->pop[where[k][tb]], sizeof(D[0]->pop[0])) != 0)
             return set_error(CPSD_ELAYOUT, std::string("orbital populations of index '") + letters[k] + "' differ");
     }
+    // Units: a pair whose two letters stay together (same order, same iop)
+    // in both tensors that carry it is one composite index running over all
+    // pairs of its pair irrep, in the DPD order (the reference's direct-GEMM
+    // fast path); packed pairs must be intact; every other letter is its
+    // own unit.
     Unit U[8];
     int nu = 0;
     int lunit[6];
@@ -152,9 +143,11 @@ int plan_contract(const Desc &d1, const char *t1, const Desc &d2, const char *t2
     for (int t = 0; t < 3; t++)
         for (int p = 0; p < 2; p++) {
             i64 iop = D[t]->iop[p];
-            if (iop == 1) continue;
             int a = lslot[t][2 * p], b = lslot[t][2 * p + 1];
-            if (a < 0 || b < 0) return set_error(CPSD_ELAYOUT, "packed pair with a dummy index");
+            if (a < 0 || b < 0) {
+                if (iop != 1) return set_error(CPSD_ELAYOUT, "packed pair with a dummy index");
+                continue;
+            }
             if (lunit[a] >= 0 && lunit[a] == lunit[b] && U[lunit[a]].nlet == 2) continue;
             bool ok = false;
             for (int u = 0; u < 3; u++) {
@@ -162,9 +155,11 @@ int plan_contract(const Desc &d1, const char *t1, const Desc &d2, const char *t2
                 for (int q = 0; q < 2; q++)
                     if (lslot[u][2 * q] == a && lslot[u][2 * q + 1] == b && D[u]->iop[q] == iop) ok = true;
             }
-            if (!ok)
+            if (!ok) {
+                if (iop == 1) continue;
                 return set_error(CPSD_ELAYOUT, std::string("packed pair not intact (expand to iop=1 first): ") + t1 +
                                                    "*" + t2 + "->" + t3);
+            }
             U[nu] = Unit{2, {a, b}, (int)iop, {}, {}, 0};
             lunit[a] = lunit[b] = nu++;
         }
@@ -215,39 +210,48 @@ int plan_contract(const Desc &d1, const char *t1, const Desc &d2, const char *t2
     };
     std::vector<Seg> segs;
     i64 nir = ctx().nirrep;
-    i64 lir[6];
-    // letters of each tensor for pruning: a tensor can be checked once all its letters are set
-    int last_let[3] = {-1, -1, -1};
+    i64 uir[8];  // irrep of each unit: letter irrep, or pair irrep of a pair unit
+    // units of each tensor for pruning: a tensor can be checked once all its units are set
+    int last_u[3] = {-1, -1, -1};
     for (int t = 0; t < 3; t++)
-        for (int s = 0; s < 4; s++) last_let[t] = std::max(last_let[t], lslot[t][s]);
-    std::vector<int> stack;
+        for (int u = 0; u < nu; u++)
+            if (U[u].in[t]) last_u[t] = u;
     std::function<void(int)> rec = [&](int k) {
-        if (k == nlet) {
-            i64 sirr[3][4];
-            for (int t = 0; t < 3; t++)
-                for (int s = 0; s < 4; s++) {
-                    sirr[t][s] = lslot[t][s] < 0 ? 1 : lir[lslot[t][s]];
-                    if (D[t]->pop[s][sirr[t][s] - 1] == 0) return;
-                }
+        if (k == nu) {
             Seg sg;
             for (int u = 0; u < nu; u++) {
                 if (U[u].nlet == 2) {
-                    i64 ia = lir[U[u].let[0]], ib = lir[U[u].let[1]];
-                    if (ia > ib) return;
                     int t0 = U[u].in[0] ? 0 : 1;
                     int p = U[u].slot[t0];
-                    i64 na = D[t0]->pop[2 * p][ia - 1], nb = D[t0]->pop[2 * p + 1][ib - 1];
-                    sg.ext[u] = (ia < ib) ? na * nb : (U[u].iop == 0 ? na * (na - 1) / 2 : na * (na + 1) / 2);
-                    if (sg.ext[u] == 0) return;
+                    sg.ext[u] = (p == 0) ? D[t0]->nleft(uir[u]) : D[t0]->nright(uir[u]);
                 } else {
                     int kk = U[u].let[0];
                     int t0 = where[kk][0] >= 0 ? 0 : 1;
-                    sg.ext[u] = D[t0]->pop[where[kk][t0]][lir[kk] - 1];
+                    sg.ext[u] = D[t0]->pop[where[kk][t0]][uir[u] - 1];
                 }
+                if (sg.ext[u] == 0) return;
             }
             for (int t = 0; t < 3; t++) {
-                i64 st4[4], nl;
-                geom(*D[t], sirr[t], &sg.base[t], st4, &nl);
+                const Desc &d = *D[t];
+                i64 PI[2], sub[2], h[4];
+                bool whole[2];
+                for (int p = 0; p < 2; p++) {
+                    int a = lslot[t][2 * p], b = lslot[t][2 * p + 1];
+                    whole[p] = a >= 0 && b >= 0 && lunit[a] == lunit[b] && U[lunit[a]].nlet == 2;
+                    if (whole[p]) {
+                        PI[p] = uir[lunit[a]];
+                        sub[p] = 0;
+                        h[2 * p] = h[2 * p + 1] = 1;
+                    } else {
+                        h[2 * p] = a < 0 ? 1 : uir[lunit[a]];
+                        h[2 * p + 1] = b < 0 ? 1 : uir[lunit[b]];
+                        PI[p] = dp(h[2 * p], h[2 * p + 1]);
+                        sub[p] = isymoffso(h[2 * p + 1], PI[p], d.pop[2 * p], d.pop[2 * p + 1], d.iop[p]) - 1;
+                    }
+                }
+                const i64 nl = d.nleft(PI[0]);
+                sg.base[t] = d.block_base(PI[1]) + sub[1] * nl + sub[0];
+                const i64 st4[4] = {1, whole[0] ? 0 : d.pop[0][h[0] - 1], nl, whole[1] ? 0 : nl * d.pop[2][h[2] - 1]};
                 for (int u = 0; u < nu; u++) {
                     if (!U[u].in[t]) {
                         sg.st[t][u] = 0;
@@ -257,18 +261,19 @@ int plan_contract(const Desc &d1, const char *t1, const Desc &d2, const char *t2
                 }
             }
             sg.okey.clear();
-            for (int kk = 0; kk < nlet; kk++)
-                if (U[lunit[kk]].cls != 2) sg.okey += (char)('0' + lir[kk]);
+            for (int u = 0; u < nu; u++)
+                if (U[u].cls != 2) sg.okey += (char)('0' + uir[u]);
             segs.push_back(sg);
             return;
         }
-        for (i64 h = 1; h <= nir; h++) {
-            lir[k] = h;
+        for (i64 hh = 1; hh <= nir; hh++) {
+            uir[k] = hh;
             bool ok = true;
             for (int t = 0; t < 3 && ok; t++) {
-                if (last_let[t] != k) continue;
+                if (last_u[t] != k) continue;
                 i64 prod = 1;
-                for (int s = 0; s < 4; s++) prod = dp(prod, lslot[t][s] < 0 ? 1 : lir[lslot[t][s]]);
+                for (int u = 0; u < nu; u++)
+                    if (U[u].in[t]) prod = dp(prod, uir[u]);
                 if (prod != D[t]->sym) ok = false;
             }
             if (ok) rec(k + 1);
@@ -276,7 +281,7 @@ int plan_contract(const Desc &d1, const char *t1, const Desc &d2, const char *t2
     };
     // tensors whose letters are all dummies must still match their irrep
     for (int t = 0; t < 3; t++)
-        if (last_let[t] < 0 && D[t]->sym != 1) {
+        if (last_u[t] < 0 && D[t]->sym != 1) {
             *out = nullptr;
             return set_error(CPSD_EARG, "scalar tensor with non-totally-symmetric irrep");
         }
