@@ -51,6 +51,16 @@ double cpsd_flop_count(int reset);
  * and returns total milliseconds, launches and useful flops. */
 int cpsd_contract_timing(int enable);
 int cpsd_contract_time(double *ms, int64_t *launches, double *flops, int reset);
+/* Sliced-integer tensor-core contractions (no counterpart in the
+ * reference): contractions of at least min_gflop useful GFLOP whose irrep
+ * blocks regroup into dense GEMMs run on the int8 tensor cores with every
+ * FP64 operand split into `digits` signed 7-bit digits under a power-of-two
+ * scale per row / column, exact int32 sums and an FP64 epilogue; the error
+ * per element is below (digits+1) K 128^-digits max|a_row| max|b_col|.
+ * digits = 0 (default) keeps the FP64 tensor-pipe path everywhere.
+ * cpsd_mixed_error returns 1 if a wait in that path ever timed out. */
+int cpsd_set_mixed(int digits, double min_gflop);
+int cpsd_mixed_error(int reset);
 
 /* -------------------------------------------------------------- size math */
 /* irpdso (src/libsrint/irpdso.f:1-52) */
@@ -234,6 +244,16 @@ int cpsd_debug_contract_plan(const cpsd_opt *v1, const char *t1, const cpsd_opt 
 /* per-launch records of the contraction timing buffer: milliseconds,
  * useful flops and (tasks, segments, tiles, tile shape) */
 int cpsd_contract_records(double *ms, double *flops, int64_t *shape, int64_t maxrec, int64_t *nrec);
+/* tables of the sliced-integer plan of a contraction (layouts OzGroup,
+ * OzTile, OzSliceJob of csrc/ozaki.cuh): tables[0..12] = groups, tiles,
+ * A jobs, B jobs, A row / K offsets, B row / K offsets, C row / column
+ * offsets, M / N / K combination ids, sizes[0..12] their counts;
+ * sizes[13..19] = A digit bytes, B digit bytes, A / B exponents, K stages
+ * per launch, most K stages, B tile width.  tables[0] = NULL when the
+ * contraction does not regroup into dense GEMMs. */
+int cpsd_debug_ozaki_plan(const cpsd_opt *v1, const char *t1, const cpsd_opt *v2, const char *t2,
+                          const cpsd_opt *v3, const char *t3, int64_t nb, int64_t sA, int64_t sB, int64_t sC,
+                          int digits, const void **tables, int64_t *sizes);
 int cpsd_debug_pairmap_plan(const cpsd_opt *in, int64_t op0, int64_t op1, int64_t tgt0, int64_t tgt1,
                             const void **blocks, int64_t *nblocks, const void **idx, const void **sgn,
                             int64_t *nidx, int64_t *lterms, int64_t *rterms);

@@ -105,6 +105,20 @@ def flop_count(reset=False):
     return float(lib().cpsd_flop_count(1 if reset else 0))
 
 
+def set_mixed(digits, min_gflop=1.0):
+    """int8-digit tensor-core contractions with `digits` 7-bit digits per
+    FP64 value for contractions of at least min_gflop GFLOP (0 = off)"""
+    check(lib().cpsd_set_mixed(ctypes.c_int(digits), ctypes.c_double(min_gflop)), "cpsd_set_mixed")
+
+
+def mixed_error(reset=True):
+    """1 if a bounded wait of the digit path timed out since the last reset"""
+    rc = lib().cpsd_mixed_error(ctypes.c_int(1 if reset else 0))
+    if rc < 0:
+        check(rc, "cpsd_mixed_error")
+    return rc
+
+
 def opt(pops, iops, sym, t):
     o = Opt()
     check(lib().cpsd_opt_init(ctypes.byref(o), arr8(pops[0]), arr8(pops[1]), arr8(pops[2]), arr8(pops[3]),

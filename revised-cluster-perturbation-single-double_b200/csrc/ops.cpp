@@ -2,6 +2,10 @@
 // the spin-free lib_cc kernels (device side: libcpsd_b200).
 #include "ops.hpp"
 
+#include <algorithm>
+
+#include "ozaki.cuh"
+
 #include <cstring>
 #include <string>
 
@@ -28,6 +32,10 @@ static int need_init() {
     return CPSD_OK;
 }
 
+namespace {
+int launch_ozaki(const OzPlan *oz, const double *A, const double *B, double *C, double alpha);
+}
+
 int engine(const Ten &v1, const char *t1, const Ten &v2, const char *t2, Ten &v3, const char *t3, double f1,
            double f2, i64 nb) {
     CPSD_TRY(need_init());
@@ -40,11 +48,18 @@ int engine(const Ten &v1, const char *t1, const Ten &v2, const char *t2, Ten &v3
     }
     const ContractPlan *p;
     CPSD_TRY(plan_contract(v1.d, t1, v2.d, t2, v3.d, t3, b, &p));
+    const OzPlan *oz = nullptr;
+    if (ctx().oz_digits > 0 && !p->empty && p->flops >= ctx().oz_min_flops)
+        CPSD_TRY(plan_ozaki(p, ctx().oz_digits, &oz));
     i64 l3 = v3.len();
     if (f2 != 1.0) {
         if (nb <= 1 || b.strideC == l3) CPSD_TRY(launch_scale(v3.arr, l3 * (nb > 1 ? nb : 1), f2));
         else
             for (i64 c = 0; c < nb; c++) CPSD_TRY(launch_scale(v3.arr + c * b.strideC, l3, f2));
+    }
+    if (oz) {
+        ctx().flops += p->flops;
+        return launch_ozaki(oz, v1.arr, v2.arr, v3.arr, f1);
     }
     return launch_contract(p, v1.arr, v2.arr, v3.arr, f1);
 }
@@ -70,14 +85,84 @@ struct ExpEntry {
     Desc d;
     double *buf;
 };
+// digit tiles (and their exponents) made of a constant operand
+struct DigEntry {
+    const double *src;
+    uint64_t hash;
+    int8_t *dig;
+    int *expo;
+};
 struct ConstOps {
     int depth = 0;
     std::vector<const double *> arrs;
     std::vector<ExpEntry> exp;
+    std::vector<DigEntry> dig;
 };
 ConstOps &const_ops() {
     static ConstOps c;
     return c;
+}
+
+bool is_const_operand(const double *a) {
+    ConstOps &c = const_ops();
+    if (c.depth == 0 || arena().external) return false;
+    for (const double *x : c.arrs)
+        if (x == a) return true;
+    return false;
+}
+
+int oz_error_word(int **err) {
+    if (!ctx().oz_err) {
+        CPSD_TRY(cuda_check(cudaMalloc(&ctx().oz_err, sizeof(int)), "cudaMalloc(error word)"));
+        CPSD_TRY(cuda_check(cudaMemset(ctx().oz_err, 0, sizeof(int)), "clear error word"));
+    }
+    *err = ctx().oz_err;
+    return CPSD_OK;
+}
+
+// digit tiles of one operand: kept for the program run when the operand is
+// constant, otherwise made in scratch (released with the caller's scope)
+int digits_of(const OzPlan *oz, bool sideA, const double *src, int8_t **dig, int **expo) {
+    const uint64_t h = sideA ? oz->ahash : oz->bhash;
+    const i64 bytes = sideA ? oz->adig : oz->bdig, ne = sideA ? oz->nea : oz->neb;
+    const OzSideDev &sd = sideA ? oz->adev : oz->bdev;
+    const int rt = sideA ? 128 : oz->BN;
+    if (is_const_operand(src)) {
+        ConstOps &c = const_ops();
+        for (const DigEntry &e : c.dig)
+            if (e.src == src && e.hash == h) {
+                *dig = e.dig;
+                *expo = e.expo;
+                return CPSD_OK;
+            }
+        int8_t *d = nullptr;
+        int *x = nullptr;
+        if (cudaMalloc(&d, (size_t)std::max<i64>(bytes, 16)) == cudaSuccess &&
+            cudaMalloc(&x, sizeof(int) * (size_t)std::max<i64>(ne, 1)) == cudaSuccess) {
+            c.dig.push_back({src, h, d, x});
+            *dig = d;
+            *expo = x;
+            return oz_slice(oz->S, rt, sd, src, d, x);
+        }
+        cudaGetLastError();
+        if (d) cudaFree(d);  // no room to keep them: make them in scratch
+    }
+    CPSD_TRY(scratch(bytes, dig));
+    CPSD_TRY(scratch(ne, expo));
+    return oz_slice(oz->S, rt, sd, src, *dig, *expo);
+}
+
+int launch_ozaki(const OzPlan *oz, const double *A, const double *B, double *C, double alpha) {
+    CPSD_TRY(const_cast<OzPlan *>(oz)->upload());
+    ScratchScope sc;
+    int8_t *ad, *bd;
+    int *ea, *eb, *err;
+    CPSD_TRY(oz_error_word(&err));
+    CPSD_TRY(digits_of(oz, true, A, &ad, &ea));
+    CPSD_TRY(digits_of(oz, false, B, &bd, &eb));
+    for (int kt0 = 0; kt0 < oz->kt_max; kt0 += oz->kt_chunk)
+        CPSD_TRY(oz_gemm(oz->S, oz->dev, ad, bd, ea, eb, C, alpha, kt0, kt0 + oz->kt_chunk, err));
+    return CPSD_OK;
 }
 
 int expand_cached(const Ten &v, bool e0, bool e1, Ten *out, bool *done) {
@@ -105,6 +190,7 @@ int expand_cached(const Ten &v, bool e0, bool e1, Ten *out, bool *done) {
         return CPSD_OK;  // no room to keep it: expand into scratch as usual
     }
     c.exp.push_back({v.arr, key, d, buf});
+    c.arrs.push_back(buf);  // derived from a constant operand: constant too
     CPSD_TRY(launch_pairmap(pm, v.arr, buf, 1.0, 0.0, 1, 0, d.len()));
     *out = v;
     out->d = d;
@@ -161,7 +247,12 @@ ConstOperands::~ConstOperands() {
     ConstOps &c = const_ops();
     if (--c.depth > 0) return;
     for (ExpEntry &e : c.exp) cudaFree(e.buf);  // waits for the kernels that read them
+    for (DigEntry &e : c.dig) {
+        cudaFree(e.dig);
+        cudaFree(e.expo);
+    }
     c.exp.clear();
+    c.dig.clear();
     c.arrs.clear();
 }
 
@@ -409,6 +500,22 @@ double cpsd_flop_count(int reset) {
     return f;
 }
 
+int cpsd_set_mixed(int digits, double min_gflop) {
+    if (digits != 0 && (digits < 3 || digits > 7)) return set_error(CPSD_EARG, "digits must be 0 or 3..7");
+    if (!(min_gflop >= 0.0)) return set_error(CPSD_EARG, "min_gflop must be >= 0");
+    ctx().oz_digits = digits;
+    ctx().oz_min_flops = min_gflop * 1e9;
+    return CPSD_OK;
+}
+
+int cpsd_mixed_error(int reset) {
+    if (!ctx().oz_err) return 0;
+    int h = 0;
+    CPSD_TRY(cuda_check(cudaMemcpy(&h, ctx().oz_err, sizeof h, cudaMemcpyDeviceToHost), "read error word"));
+    if (reset && h) CPSD_TRY(cuda_check(cudaMemset(ctx().oz_err, 0, sizeof(int)), "clear error word"));
+    return h;
+}
+
 int64_t cpsd_irpdso(int64_t sym, const int64_t *popp, const int64_t *popq, int64_t ioppq) {
     return irpdso(sym, popp, popq, ioppq);
 }
@@ -609,6 +716,48 @@ int cpsd_debug_contract_plan(const cpsd_opt *v1, const char *t1, const cpsd_opt 
 
 int cpsd_contract_records(double *ms, double *flops, int64_t *shape, int64_t maxrec, int64_t *nrec) {
     return contract_records(ms, flops, shape, maxrec, nrec);
+}
+
+int cpsd_debug_ozaki_plan(const cpsd_opt *v1, const char *t1, const cpsd_opt *v2, const char *t2,
+                          const cpsd_opt *v3, const char *t3, int64_t nb, int64_t sA, int64_t sB, int64_t sC,
+                          int digits, const void **tables, int64_t *sizes) {
+    CPSD_TRY(need_init());
+    if (digits < 3 || digits > 7) return set_error(CPSD_EARG, "digits must be 3..7");
+    Batch b;
+    b.nb = nb;
+    b.strideA = sA;
+    b.strideB = sB;
+    b.strideC = sC;
+    const ContractPlan *p;
+    CPSD_TRY(plan_contract(desc_of(v1), t1, desc_of(v2), t2, desc_of(v3), t3, b, &p));
+    const OzPlan *oz = nullptr;
+    if (!p->empty) CPSD_TRY(plan_ozaki(p, digits, &oz));
+    for (int i = 0; i < 20; i++) {
+        tables[i] = nullptr;
+        sizes[i] = 0;
+    }
+    if (!oz) return CPSD_OK;
+    const void *t[13] = {oz->groups.data(), oz->tiles.data(), oz->ajobs.data(), oz->bjobs.data(),
+                         oz->aroff.data(),  oz->akoff.data(), oz->broff.data(), oz->bkoff.data(),
+                         oz->crow.data(),   oz->ccol.data(),  oz->mcombo.data(), oz->ncombo.data(),
+                         oz->kcombo.data()};
+    const int64_t n[13] = {(int64_t)oz->groups.size(), (int64_t)oz->tiles.size(), (int64_t)oz->ajobs.size(),
+                           (int64_t)oz->bjobs.size(),  (int64_t)oz->aroff.size(), (int64_t)oz->akoff.size(),
+                           (int64_t)oz->broff.size(),  (int64_t)oz->bkoff.size(), (int64_t)oz->crow.size(),
+                           (int64_t)oz->ccol.size(),   (int64_t)oz->mcombo.size(), (int64_t)oz->ncombo.size(),
+                           (int64_t)oz->kcombo.size()};
+    for (int i = 0; i < 13; i++) {
+        tables[i] = t[i];
+        sizes[i] = n[i];
+    }
+    sizes[13] = oz->adig;
+    sizes[14] = oz->bdig;
+    sizes[15] = oz->nea;
+    sizes[16] = oz->neb;
+    sizes[17] = oz->kt_chunk;
+    sizes[18] = oz->kt_max;
+    sizes[19] = oz->BN;
+    return CPSD_OK;
 }
 
 int cpsd_debug_pairmap_plan(const cpsd_opt *in, int64_t op0, int64_t op1, int64_t tgt0, int64_t tgt1,

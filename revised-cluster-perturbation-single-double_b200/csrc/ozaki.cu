@@ -1,0 +1,411 @@
+// Sliced-integer contraction on the 5th-generation tensor cores (sm_100a).
+//
+// A FP64 contraction C += alpha * A B is evaluated as an exact integer sum:
+// every row of A (column of B) is scaled by a power of two 2^e so that its
+// largest element is below 1 in magnitude, and each scaled value y is cut
+// into S signed 7-bit digits q_t = trunc(128^(t+1) y - ...), so that
+// a = 2^e sum_t q_t 128^-(t+1) up to 2^e 128^-S (Ozaki, Ogita, Oishi & Rump,
+// "Error-free transformations of matrix multiplication by using fast
+// routines of matrix multiplication", 2012; the integer form of Ootomo,
+// Ozaki & Yokota 2024).  The digit products q_t(A) q_u(B) with t + u <= S - 1
+// are summed exactly in int32 by tcgen05.mma kind::i8, one TMEM accumulator
+// per diagonal d = t + u, and the epilogue combines the diagonals in FP64:
+// C += alpha 2^(e_a + e_b) sum_d acc_d 128^-(d+2).  The truncation error is
+// below (S + 1) K 128^-S max|a_row| max|b_col| per element.
+//
+// Operands are first gathered from their DPD layout into the digit tiles
+// (k_oz_slice): per 128 (A) or BN (B) rows and 64 contracted indices, S
+// canonical K-major tiles (8 x 16-byte core matrices, no swizzle) stored
+// contiguously, so one bulk copy (cp.async.bulk) moves a whole pipeline
+// stage.  One CTA computes one 128 x BN output tile (k_oz_gemm): a producer
+// warp streams the stages through an mbarrier ring, one thread issues the
+// MMAs, four warps read the accumulators back (tcgen05.ld) and scatter the
+// FP64 result through the output offset tables.  Every wait is bounded: on
+// a timeout the kernel records it in an error word and drains.
+#include <cstdint>
+
+#include "ozaki.cuh"
+
+namespace cpsd {
+
+namespace {
+
+constexpr int OZ_BK = 64;             // contracted indices per stage (bytes of a digit row)
+constexpr int OZ_THREADS = 192;       // 4 epilogue warps, 1 producer warp, 1 MMA warp
+constexpr uint32_t OZ_SPIN = 1u << 20;  // poll limit of every mbarrier wait
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// bounded wait for the phase with the given parity; false on timeout
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+    const uint32_t a = smem_u32(bar);
+    for (uint32_t i = 0; i < OZ_SPIN; i++) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// K-major canonical layout without swizzle: core matrices of 8 rows x 16
+// bytes (128 contiguous bytes), LBO = next core matrix along K, SBO = next
+// group of 8 rows
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr & 0x3FFFF) >> 4);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t)1 << 46;  // descriptor version of sm_100
+    return d;                // base offset 0, layout type 0 (no swizzle)
+}
+
+// instruction descriptor of kind::i8: s8 x s8 -> s32, both K-major, M = 128
+__host__ __device__ constexpr uint32_t umma_idesc_i8(int n) {
+    return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                        uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0)
+        : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, int32_t (&v)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+template <int S, int BN>
+struct OzCfg {
+    static constexpr int A_STAGE = S * 128 * OZ_BK;  // bytes of the A digit tiles of one stage
+    static constexpr int B_STAGE = S * BN * OZ_BK;
+    static constexpr int STAGE = A_STAGE + B_STAGE;
+    static constexpr int NST = (200 * 1024) / STAGE >= 4 ? 4 : (200 * 1024) / STAGE;
+    static constexpr int SMEM = NST * STAGE + 1024;
+    static constexpr int NCOL_RAW = S * BN;
+    static constexpr int NCOL = NCOL_RAW <= 32 ? 32 : NCOL_RAW <= 64 ? 64 : NCOL_RAW <= 128 ? 128 : NCOL_RAW <= 256 ? 256 : 512;
+    static_assert(NST >= 2, "at least two pipeline stages");
+    static_assert(NCOL_RAW <= 512, "accumulators exceed TMEM");
+};
+
+// One output tile per CTA: 128 rows (TMEM lanes) x BN columns, S diagonal
+// accumulators side by side in TMEM columns.
+template <int S, int BN>
+__global__ void __launch_bounds__(OZ_THREADS, 1)
+    k_oz_gemm(const OzTile *__restrict__ tiles, const OzGroup *__restrict__ groups, const int8_t *__restrict__ Adig,
+              const int8_t *__restrict__ Bdig, const int *__restrict__ ea, const int *__restrict__ eb,
+              const i64 *__restrict__ crow, const i64 *__restrict__ ccol, const int *__restrict__ mcombo,
+              const int *__restrict__ ncombo, double *__restrict__ C, double alpha, int kt0, int kt1,
+              int *__restrict__ err) {
+    using Cf = OzCfg<S, BN>;
+    extern __shared__ __align__(1024) unsigned char oz_smem[];
+    unsigned char *stages = (unsigned char *)(((uintptr_t)oz_smem + 1023) & ~(uintptr_t)1023);
+    __shared__ __align__(8) uint64_t full[Cf::NST], empty[Cf::NST], done;
+    __shared__ uint32_t tmem_base_sh;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const OzTile tl = tiles[blockIdx.x];
+    const OzGroup g = groups[tl.g];
+    const int KT = g.KT;
+    const int kb = kt0, ke = kt1 < KT ? kt1 : KT;
+    const int nk = ke > kb ? ke - kb : 0;  // groups with fewer K stages add nothing in later chunks
+
+    if (warp == 5) {  // TMEM columns for the S accumulators
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_sh)),
+                     "r"(Cf::NCOL)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        for (int s = 0; s < Cf::NST; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(&done, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_base_sh;
+    bool ok = true;
+
+    if (warp == 4) {
+        if (lane == 0) {  // producer
+            const int8_t *Ab = Adig + g.aoff + (size_t)tl.mt * KT * Cf::A_STAGE;
+            const int8_t *Bb = Bdig + g.boff + (size_t)tl.nt * KT * Cf::B_STAGE;
+            for (int i = 0; i < nk; i++) {
+                const int s = i % Cf::NST, u = i / Cf::NST;
+                if (u > 0 && !mbar_wait(&empty[s], (u - 1) & 1)) {
+                    ok = false;
+                    break;
+                }
+                unsigned char *sa = stages + (size_t)s * Cf::STAGE;
+                mbar_expect_tx(&full[s], Cf::STAGE);
+                bulk_g2s(sa, Ab + (size_t)(kb + i) * Cf::A_STAGE, Cf::A_STAGE, &full[s]);
+                bulk_g2s(sa + Cf::A_STAGE, Bb + (size_t)(kb + i) * Cf::B_STAGE, Cf::B_STAGE, &full[s]);
+            }
+        }
+    } else if (warp == 5) {
+        if (lane == 0) {  // MMA issuer
+            constexpr uint32_t idesc = umma_idesc_i8(BN);
+            bool init[S];
+#pragma unroll
+            for (int d = 0; d < S; d++) init[d] = false;
+            for (int i = 0; i < nk; i++) {
+                const int s = i % Cf::NST, u = i / Cf::NST;
+                if (!mbar_wait(&full[s], u & 1)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t sa = smem_u32(stages + (size_t)s * Cf::STAGE), sb = sa + Cf::A_STAGE;
+#pragma unroll
+                for (int t = 0; t < S; t++)
+#pragma unroll
+                    for (int v = 0; v < S - t; v++) {
+                        const int d = t + v;
+#pragma unroll
+                        for (int kk = 0; kk < OZ_BK / 32; kk++) {
+                            uint64_t ad = umma_desc(sa + t * 128 * OZ_BK + kk * 256, 128, 8 * OZ_BK);
+                            uint64_t bd = umma_desc(sb + v * BN * OZ_BK + kk * 256, 128, 8 * OZ_BK);
+                            umma_i8(tmem + (uint32_t)(d * BN), ad, bd, idesc, init[d] ? 1u : 0u);
+                            init[d] = true;
+                        }
+                    }
+                umma_commit(&empty[s]);  // frees the stage once these MMAs are done
+            }
+            umma_commit(&done);
+        }
+    } else {  // epilogue: warp w reads TMEM lanes 32w..32w+31 = tile rows
+        // one lane waits so that the warp stays converged for tcgen05.ld
+        int fin_l = 0;
+        if (lane == 0) fin_l = mbar_wait(&done, 0) ? 1 : 0;
+        const bool fin = __shfl_sync(0xffffffffu, fin_l, 0) != 0;
+        tc_fence_after();
+        const int r = warp * 32 + lane;
+        const i64 m = (i64)tl.mt * 128 + r;
+        const bool rowok = fin && m < g.M;
+        const int mc = rowok ? mcombo[g.moff + m] : 0;
+        const int e_a = rowok ? ea[g.eaoff + m] : 0;
+        const i64 *crow_m = crow + g.crowoff + (rowok ? m : 0) * g.nL;
+        for (int c0 = 0; c0 < BN; c0 += 16) {
+            double acc[16];
+#pragma unroll
+            for (int j = 0; j < 16; j++) acc[j] = 0.0;
+            double w = 1.0 / 16384.0;  // 128^-(d+2), d = 0
+#pragma unroll
+            for (int d = 0; d < S; d++) {
+                int32_t v[16];
+                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(d * BN + c0), v);
+#pragma unroll
+                for (int j = 0; j < 16; j++) acc[j] += (double)v[j] * w;
+                w *= 1.0 / 128.0;
+            }
+            if (!rowok || nk == 0) continue;
+#pragma unroll
+            for (int j = 0; j < 16; j++) {
+                const i64 n = (i64)tl.nt * BN + c0 + j;
+                if (n >= g.N) break;
+                const int nc = ncombo[g.noff + n];
+                const i64 addr = crow_m[nc] + ccol[g.ccoloff + n * g.nI + mc];
+                C[addr] += alpha * ldexp(acc[j], e_a + eb[g.eboff + n]);
+            }
+        }
+        if (!fin) ok = false;
+    }
+    if (!ok) atomicExch(err, 1);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 5) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Cf::NCOL) : "memory");
+    }
+}
+
+// Digit tiles of one operand side.  Block b handles slicing job b (one row
+// tile of one group): the rows' scale exponents (pass 1 over all contracted
+// indices) and the S digit tiles of every K stage (pass 2).  Element (r, k)
+// of the group lives at src[roff[r * nJ + kcombo[k]] + koff[k * nI +
+// rcombo[r]]] (row r of irrep combination rcombo[r], contracted index k of
+// combination kcombo[k]); rows and columns beyond the group's extents are
+// written as zero digits.
+template <int S, int RT>
+__global__ void __launch_bounds__(256) k_oz_slice(const OzSliceJob *__restrict__ jobs, const double *__restrict__ src,
+                                                  const i64 *__restrict__ roff, const i64 *__restrict__ koff,
+                                                  const int *__restrict__ rcombo, const int *__restrict__ kcombo,
+                                                  int8_t *__restrict__ dig, int *__restrict__ expo) {
+    const OzSliceJob jb = jobs[blockIdx.x];
+    __shared__ int rmax[RT];
+    const int tid = threadIdx.x;
+    for (int r = tid; r < RT; r += 256) rmax[r] = -100000;
+    __syncthreads();
+    constexpr int UNITS = RT * (OZ_BK / 16);  // (row, 16 contracted indices) per stage
+    const i64 r0 = (i64)jb.rt * RT;
+    // pass 1: exponent of the row maximum (|x| < 2^e)
+    for (int kt = 0; kt < jb.KT; kt++)
+        for (int u = tid; u < UNITS; u += 256) {
+            const int r = u % RT, k16 = u / RT;
+            const i64 row = r0 + r;
+            if (row >= jb.R) continue;
+            const i64 *ro = roff + jb.roff + row * jb.nJ;
+            const int rc = rcombo[jb.rcoff + row];
+            int e = -100000;
+            for (int q = 0; q < 16; q++) {
+                const i64 k = (i64)kt * OZ_BK + k16 * 16 + q;
+                if (k >= jb.K) break;
+                double x = src[ro[kcombo[jb.kcoff + k]] + koff[jb.koff + k * jb.nI + rc]];
+                if (x != 0.0) {
+                    int ex;
+                    frexp(x, &ex);
+                    e = max(e, ex);
+                }
+            }
+            if (e > -100000) atomicMax(&rmax[r], e);
+        }
+    __syncthreads();
+    for (int r = tid; r < RT; r += 256) {
+        const i64 row = r0 + r;
+        if (rmax[r] == -100000) rmax[r] = 0;
+        if (row < jb.R) expo[jb.eoff + row] = rmax[r];
+    }
+    __syncthreads();
+    // pass 2: digits, written as 16-byte rows of the core matrices
+    for (int kt = 0; kt < jb.KT; kt++) {
+        int8_t *tile = dig + jb.doff + ((size_t)jb.rt * jb.KT + kt) * (size_t)(S * RT * OZ_BK);
+        for (int u = tid; u < UNITS; u += 256) {
+            const int r = u % RT, k16 = u / RT;
+            const i64 row = r0 + r;
+            uint32_t w[S][4];
+#pragma unroll
+            for (int t = 0; t < S; t++) w[t][0] = w[t][1] = w[t][2] = w[t][3] = 0u;
+            if (row < jb.R) {
+                const i64 *ro = roff + jb.roff + row * jb.nJ;
+                const int rc = rcombo[jb.rcoff + row];
+                const double sc = ldexp(1.0, -rmax[r]);
+                for (int q = 0; q < 16; q++) {
+                    const i64 k = (i64)kt * OZ_BK + k16 * 16 + q;
+                    if (k >= jb.K) break;
+                    double y = src[ro[kcombo[jb.kcoff + k]] + koff[jb.koff + k * jb.nI + rc]] * sc;
+#pragma unroll
+                    for (int t = 0; t < S; t++) {
+                        y *= 128.0;
+                        const double qd = trunc(y);
+                        y -= qd;
+                        w[t][q >> 2] |= ((uint32_t)(uint8_t)(int8_t)(int)qd) << (8 * (q & 3));
+                    }
+                }
+            }
+            const size_t off = (size_t)(r >> 3) * (8 * OZ_BK) + (size_t)k16 * 128 + (size_t)(r & 7) * 16;
+#pragma unroll
+            for (int t = 0; t < S; t++)
+                *reinterpret_cast<uint4 *>(tile + (size_t)t * RT * OZ_BK + off) =
+                    make_uint4(w[t][0], w[t][1], w[t][2], w[t][3]);
+        }
+    }
+}
+
+template <int S, int BN>
+int oz_gemm_launch(const OzDevPlan &p, const int8_t *Adig, const int8_t *Bdig, const int *ea, const int *eb,
+                   double *C, double alpha, int kt0, int kt1, int *err) {
+    using Cf = OzCfg<S, BN>;
+    static bool attr = false;
+    if (!attr) {
+        CPSD_TRY(cuda_check(cudaFuncSetAttribute(k_oz_gemm<S, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cf::SMEM),
+                            "oz smem attr"));
+        attr = true;
+    }
+    k_oz_gemm<S, BN><<<p.ntiles, OZ_THREADS, Cf::SMEM, stream()>>>(p.tiles, p.groups, Adig, Bdig, ea, eb, p.crow,
+                                                                   p.ccol, p.mcombo, p.ncombo, C, alpha, kt0, kt1,
+                                                                   err);
+    count_launch();
+    return cuda_check(cudaGetLastError(), "k_oz_gemm");
+}
+
+template <int S, int RT>
+int oz_slice_launch(const OzSideDev &sd, const double *src, int8_t *dig, int *expo) {
+    if (sd.njobs == 0) return CPSD_OK;
+    k_oz_slice<S, RT><<<sd.njobs, 256, 0, stream()>>>(sd.jobs, src, sd.roff, sd.koff, sd.rcombo, sd.kcombo, dig, expo);
+    count_launch();
+    return cuda_check(cudaGetLastError(), "k_oz_slice");
+}
+
+}  // namespace
+
+int oz_slice(int S, int rows_per_tile, const OzSideDev &sd, const double *src, int8_t *dig, int *expo) {
+#define OZ_SL(s)                                                                    \
+    case s:                                                                         \
+        return rows_per_tile == 128 ? oz_slice_launch<s, 128>(sd, src, dig, expo)  \
+                                    : oz_slice_launch<s, 64>(sd, src, dig, expo);
+    switch (S) {
+        OZ_SL(3)
+        OZ_SL(4)
+        OZ_SL(5)
+        OZ_SL(6)
+        OZ_SL(7)
+    default:
+        return set_error(CPSD_EARG, "digit count must be 3..7");
+    }
+#undef OZ_SL
+}
+
+int oz_gemm(int S, const OzDevPlan &p, const int8_t *Adig, const int8_t *Bdig, const int *ea, const int *eb,
+            double *C, double alpha, int kt0, int kt1, int *err) {
+    switch (S) {
+    case 3:
+        return oz_gemm_launch<3, 128>(p, Adig, Bdig, ea, eb, C, alpha, kt0, kt1, err);
+    case 4:
+        return oz_gemm_launch<4, 128>(p, Adig, Bdig, ea, eb, C, alpha, kt0, kt1, err);
+    case 5:
+        return oz_gemm_launch<5, 64>(p, Adig, Bdig, ea, eb, C, alpha, kt0, kt1, err);
+    case 6:
+        return oz_gemm_launch<6, 64>(p, Adig, Bdig, ea, eb, C, alpha, kt0, kt1, err);
+    case 7:
+        return oz_gemm_launch<7, 64>(p, Adig, Bdig, ea, eb, C, alpha, kt0, kt1, err);
+    default:
+        return set_error(CPSD_EARG, "digit count must be 3..7");
+    }
+}
+
+int oz_tile_n(int S) { return S <= 4 ? 128 : 64; }
+
+}  // namespace cpsd

@@ -203,7 +203,7 @@ int plan_contract(const Desc &d1, const char *t1, const Desc &d2, const char *t2
 
     // enumerate irrep assignments (depth-first with symmetry pruning)
     struct Seg {
-        std::string okey;
+        std::string okey, mkey, nkey, kkey;
         i64 ext[8];
         i64 base[3];
         i64 st[3][8];
@@ -261,8 +261,11 @@ int plan_contract(const Desc &d1, const char *t1, const Desc &d2, const char *t2
                 }
             }
             sg.okey.clear();
-            for (int u = 0; u < nu; u++)
-                if (U[u].cls != 2) sg.okey += (char)('0' + uir[u]);
+            for (int u = 0; u < nu; u++) {
+                const char c = (char)('0' + uir[u]);
+                if (U[u].cls != 2) sg.okey += c;
+                (U[u].cls == 0 ? sg.mkey : U[u].cls == 1 ? sg.nkey : sg.kkey) += c;
+            }
             segs.push_back(sg);
             return;
         }
@@ -347,13 +350,17 @@ int plan_contract(const Desc &d1, const char *t1, const Desc &d2, const char *t2
             sd.kstart = tk.Ktot;
             tk.Ktot += sd.K;
             dsegs.push_back(sd);
+            plan->seg_kkey.push_back(s.kkey);
         }
         tk.nseg = (int)dsegs.size() - tk.seg0;
         if (tk.M > 0 && tk.N > 0 && tk.nseg > 0) {
             tasks.push_back(tk);
+            plan->task_mkey.push_back(s0.mkey);
+            plan->task_nkey.push_back(s0.nkey);
             plan->flops += 2.0 * (double)tk.M * (double)tk.N * (double)tk.Ktot;
         } else {
             dsegs.resize(tk.seg0);
+            plan->seg_kkey.resize(tk.seg0);
         }
         i = j;
     }

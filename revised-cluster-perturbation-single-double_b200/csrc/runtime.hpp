@@ -32,6 +32,12 @@ struct Context {
     cudaStream_t stream = nullptr;
     int64_t launches = 0;
     double flops = 0;  // useful contraction flops issued (2 M N K per block)
+    // sliced-integer (int8 digit) tensor-core path: digits per operand
+    // element (0 = FP64 DMMA everywhere) and the smallest contraction, in
+    // flops, that takes it; error word of its bounded waits
+    int oz_digits = 0;
+    double oz_min_flops = 1e9;
+    int *oz_err = nullptr;
 };
 Context &ctx();
 inline i64 dp(i64 a, i64 b) { return ctx().dirprd[a - 1][b - 1]; }
@@ -139,6 +145,9 @@ struct ContractPlan {
     int *d_reduce = nullptr;  // (task, mt, nt, part0, nsplit) groups for split-K
     int nreduce = 0;
     double flops = 0;    // 2*sum M*N*K
+    // irreps of the M / N units of each task and of the K units of each
+    // segment (one character per unit), for regrouping into dense GEMMs
+    std::vector<std::string> task_mkey, task_nkey, seg_kkey;
     int upload();
 };
 // A batched operand / result: `nb` copies with the given element stride
