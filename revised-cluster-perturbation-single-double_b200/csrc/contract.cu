@@ -269,6 +269,22 @@ int contract_timing(int enable) {
     return CPSD_OK;
 }
 
+int timing_begin(double flops, int64_t a, int64_t b, int64_t c, int64_t kind, cudaEvent_t *end) {
+    *end = nullptr;
+    if (!timing().on) return CPSD_OK;
+    cudaEvent_t e0;
+    CPSD_TRY(timing_event(&e0));
+    CPSD_TRY(timing_event(end));
+    timing().flops.push_back(flops);
+    timing().shape.push_back({a, b, c, kind});
+    return cuda_check(cudaEventRecord(e0, stream()), "event record");
+}
+
+int timing_end(cudaEvent_t end) {
+    if (!end) return CPSD_OK;
+    return cuda_check(cudaEventRecord(end, stream()), "event record");
+}
+
 int contract_records(double *ms, double *flops, int64_t *shape, int64_t maxrec, int64_t *nrec) {
     Timing &t = timing();
     int64_t n = 0;

@@ -48,9 +48,14 @@ int engine(const Ten &v1, const char *t1, const Ten &v2, const char *t2, Ten &v3
     }
     const ContractPlan *p;
     CPSD_TRY(plan_contract(v1.d, t1, v2.d, t2, v3.d, t3, b, &p));
+    // digit tensor-core path for large contractions whose dense regrouping
+    // wastes at most half of the padded tiles and has K of at least 256
+    // (min_gflop = 0 routes every contraction that regroups)
     const OzPlan *oz = nullptr;
-    if (ctx().oz_digits > 0 && !p->empty && p->flops >= ctx().oz_min_flops)
+    if (ctx().oz_digits > 0 && !p->empty && p->flops >= ctx().oz_min_flops) {
         CPSD_TRY(plan_ozaki(p, ctx().oz_digits, &oz));
+        if (oz && ctx().oz_min_flops > 0 && (oz->pad_eff < 0.5 || oz->kmin < 256)) oz = nullptr;
+    }
     i64 l3 = v3.len();
     if (f2 != 1.0) {
         if (nb <= 1 || b.strideC == l3) CPSD_TRY(launch_scale(v3.arr, l3 * (nb > 1 ? nb : 1), f2));
@@ -84,6 +89,7 @@ struct ExpEntry {
     std::string key;
     Desc d;
     double *buf;
+    size_t bytes;
 };
 // digit tiles (and their exponents) made of a constant operand
 struct DigEntry {
@@ -91,6 +97,7 @@ struct DigEntry {
     uint64_t hash;
     int8_t *dig;
     int *expo;
+    size_t dbytes, ebytes;
 };
 struct ConstOps {
     int depth = 0;
@@ -101,6 +108,42 @@ struct ConstOps {
 ConstOps &const_ops() {
     static ConstOps c;
     return c;
+}
+
+// Device buffers of the constant-operand copies are kept after a program
+// run and reused by the next one (the same workload asks for the same
+// sizes), so that runs do not pay cudaMalloc / cudaFree of gigabytes.
+struct PoolBuf {
+    void *p;
+    size_t bytes;
+};
+std::vector<PoolBuf> &pool_free() {
+    static std::vector<PoolBuf> v;
+    return v;
+}
+void *pool_get(size_t bytes) {
+    auto &f = pool_free();
+    int best = -1;
+    for (int i = 0; i < (int)f.size(); i++)
+        if (f[i].bytes >= bytes && f[i].bytes <= 2 * bytes + (1u << 20) &&
+            (best < 0 || f[i].bytes < f[best].bytes))
+            best = i;
+    if (best >= 0) {
+        void *p = f[best].p;
+        f.erase(f.begin() + best);
+        return p;
+    }
+    void *p = nullptr;
+    if (cudaMalloc(&p, bytes) == cudaSuccess) return p;
+    cudaGetLastError();
+    for (PoolBuf &b : f) cudaFree(b.p);  // out of memory: give back the idle buffers and retry
+    f.clear();
+    if (cudaMalloc(&p, bytes) == cudaSuccess) return p;
+    cudaGetLastError();
+    return nullptr;
+}
+void pool_put(void *p, size_t bytes) {
+    if (p) pool_free().push_back({p, bytes});
 }
 
 bool is_const_operand(const double *a) {
@@ -120,13 +163,19 @@ int oz_error_word(int **err) {
     return CPSD_OK;
 }
 
+int slice_timed(const OzPlan *oz, bool sideA, const double *src, int8_t *dig, int *expo) {
+    cudaEvent_t end;
+    const i64 rows = sideA ? oz->nea : oz->neb, bytes = sideA ? oz->adig : oz->bdig;
+    CPSD_TRY(timing_begin(0.0, rows, bytes, (i64)oz->groups.size(), sideA ? 10 : 11, &end));
+    CPSD_TRY(oz_slice(oz->S, sideA ? 128 : oz->BN, sideA ? oz->adev : oz->bdev, src, dig, expo));
+    return timing_end(end);
+}
+
 // digit tiles of one operand: kept for the program run when the operand is
 // constant, otherwise made in scratch (released with the caller's scope)
 int digits_of(const OzPlan *oz, bool sideA, const double *src, int8_t **dig, int **expo) {
     const uint64_t h = sideA ? oz->ahash : oz->bhash;
     const i64 bytes = sideA ? oz->adig : oz->bdig, ne = sideA ? oz->nea : oz->neb;
-    const OzSideDev &sd = sideA ? oz->adev : oz->bdev;
-    const int rt = sideA ? 128 : oz->BN;
     if (is_const_operand(src)) {
         ConstOps &c = const_ops();
         for (const DigEntry &e : c.dig)
@@ -135,21 +184,20 @@ int digits_of(const OzPlan *oz, bool sideA, const double *src, int8_t **dig, int
                 *expo = e.expo;
                 return CPSD_OK;
             }
-        int8_t *d = nullptr;
-        int *x = nullptr;
-        if (cudaMalloc(&d, (size_t)std::max<i64>(bytes, 16)) == cudaSuccess &&
-            cudaMalloc(&x, sizeof(int) * (size_t)std::max<i64>(ne, 1)) == cudaSuccess) {
-            c.dig.push_back({src, h, d, x});
+        const size_t db = (size_t)std::max<i64>(bytes, 16), eb = sizeof(int) * (size_t)std::max<i64>(ne, 1);
+        int8_t *d = (int8_t *)pool_get(db);
+        int *x = d ? (int *)pool_get(eb) : nullptr;
+        if (d && x) {
+            c.dig.push_back({src, h, d, x, db, eb});
             *dig = d;
             *expo = x;
-            return oz_slice(oz->S, rt, sd, src, d, x);
+            return slice_timed(oz, sideA, src, d, x);
         }
-        cudaGetLastError();
-        if (d) cudaFree(d);  // no room to keep them: make them in scratch
+        pool_put(d, db);  // no room to keep them: make them in scratch
     }
     CPSD_TRY(scratch(bytes, dig));
     CPSD_TRY(scratch(ne, expo));
-    return oz_slice(oz->S, rt, sd, src, *dig, *expo);
+    return slice_timed(oz, sideA, src, *dig, *expo);
 }
 
 int launch_ozaki(const OzPlan *oz, const double *A, const double *B, double *C, double alpha) {
@@ -160,9 +208,11 @@ int launch_ozaki(const OzPlan *oz, const double *A, const double *B, double *C, 
     CPSD_TRY(oz_error_word(&err));
     CPSD_TRY(digits_of(oz, true, A, &ad, &ea));
     CPSD_TRY(digits_of(oz, false, B, &bd, &eb));
+    cudaEvent_t end;
+    CPSD_TRY(timing_begin(oz->flops, (i64)oz->groups.size(), 0, (i64)oz->tiles.size(), 12, &end));
     for (int kt0 = 0; kt0 < oz->kt_max; kt0 += oz->kt_chunk)
         CPSD_TRY(oz_gemm(oz->S, oz->dev, ad, bd, ea, eb, C, alpha, kt0, kt0 + oz->kt_chunk, err));
-    return CPSD_OK;
+    return timing_end(end);
 }
 
 int expand_cached(const Ten &v, bool e0, bool e1, Ten *out, bool *done) {
@@ -184,12 +234,10 @@ int expand_cached(const Ten &v, bool e0, bool e1, Ten *out, bool *done) {
     const PairMapPlan *pm;
     Desc d;
     CPSD_TRY(plan_pairmap(v.d, e0 ? PAIR_EXPAND : PAIR_ID, e1 ? PAIR_EXPAND : PAIR_ID, 1, 1, &d, &pm));
-    double *buf = nullptr;
-    if (cudaMalloc(&buf, sizeof(double) * (size_t)std::max<i64>(d.len(), 1)) != cudaSuccess) {
-        cudaGetLastError();
-        return CPSD_OK;  // no room to keep it: expand into scratch as usual
-    }
-    c.exp.push_back({v.arr, key, d, buf});
+    const size_t bytes = sizeof(double) * (size_t)std::max<i64>(d.len(), 1);
+    double *buf = (double *)pool_get(bytes);
+    if (!buf) return CPSD_OK;  // no room to keep it: expand into scratch as usual
+    c.exp.push_back({v.arr, key, d, buf, bytes});
     c.arrs.push_back(buf);  // derived from a constant operand: constant too
     CPSD_TRY(launch_pairmap(pm, v.arr, buf, 1.0, 0.0, 1, 0, d.len()));
     *out = v;
@@ -246,10 +294,13 @@ ConstOperands::ConstOperands(const double *const *arrs, int n) {
 ConstOperands::~ConstOperands() {
     ConstOps &c = const_ops();
     if (--c.depth > 0) return;
-    for (ExpEntry &e : c.exp) cudaFree(e.buf);  // waits for the kernels that read them
+    // the buffers go back to the pool once the kernels that read them are
+    // done (the next user may run on another stream)
+    if (!c.exp.empty() || !c.dig.empty()) cudaStreamSynchronize(stream());
+    for (ExpEntry &e : c.exp) pool_put(e.buf, e.bytes);
     for (DigEntry &e : c.dig) {
-        cudaFree(e.dig);
-        cudaFree(e.expo);
+        pool_put(e.dig, e.dbytes);
+        pool_put(e.expo, e.ebytes);
     }
     c.exp.clear();
     c.dig.clear();

@@ -33,6 +33,11 @@ namespace {
 constexpr int OZ_BK = 64;             // contracted indices per stage (bytes of a digit row)
 constexpr int OZ_THREADS = 192;       // 4 epilogue warps, 1 producer warp, 1 MMA warp
 constexpr uint32_t OZ_SPIN = 1u << 20;  // poll limit of every mbarrier wait
+constexpr int OZ_EXPO_NONE = (int)0x80808080;  // byte-filled "no element yet" (all-zero row)
+
+// scale exponent of a row / column; an all-zero one has zero digits, any
+// exponent does
+__device__ __forceinline__ int oz_expo(int e) { return e == OZ_EXPO_NONE ? 0 : e; }
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
     return (uint32_t)__cvta_generic_to_shared(p);
@@ -226,7 +231,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
         const i64 m = (i64)tl.mt * 128 + r;
         const bool rowok = fin && m < g.M;
         const int mc = rowok ? mcombo[g.moff + m] : 0;
-        const int e_a = rowok ? ea[g.eaoff + m] : 0;
+        const int e_a = rowok ? oz_expo(ea[g.eaoff + m]) : 0;
         const i64 *crow_m = crow + g.crowoff + (rowok ? m : 0) * g.nL;
         for (int c0 = 0; c0 < BN; c0 += 16) {
             double acc[16];
@@ -248,7 +253,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                 if (n >= g.N) break;
                 const int nc = ncombo[g.noff + n];
                 const i64 addr = crow_m[nc] + ccol[g.ccoloff + n * g.nI + mc];
-                C[addr] += alpha * ldexp(acc[j], e_a + eb[g.eboff + n]);
+                C[addr] += alpha * ldexp(acc[j], e_a + oz_expo(eb[g.eboff + n]));
             }
         }
         if (!fin) ok = false;
@@ -262,55 +267,84 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
     }
 }
 
-// Digit tiles of one operand side.  Block b handles slicing job b (one row
-// tile of one group): the rows' scale exponents (pass 1 over all contracted
-// indices) and the S digit tiles of every K stage (pass 2).  Element (r, k)
-// of the group lives at src[roff[r * nJ + kcombo[k]] + koff[k * nI +
-// rcombo[r]]] (row r of irrep combination rcombo[r], contracted index k of
-// combination kcombo[k]); rows and columns beyond the group's extents are
-// written as zero digits.
-template <int S, int RT>
-__global__ void __launch_bounds__(256) k_oz_slice(const OzSliceJob *__restrict__ jobs, const double *__restrict__ src,
-                                                  const i64 *__restrict__ roff, const i64 *__restrict__ koff,
-                                                  const int *__restrict__ rcombo, const int *__restrict__ kcombo,
-                                                  int8_t *__restrict__ dig, int *__restrict__ expo) {
+// Digit tiles of one operand side, in two fully parallel passes over the
+// slicing jobs (one row tile of one group each).  Element (r, k) of a group
+// lives at src[roff[r * nJ + kcombo[k]] + koff[k * nI + rcombo[r]]] (row r
+// of irrep combination rcombo[r], contracted index k of combination
+// kcombo[k]).
+constexpr int OZ_EXPO_CHUNK = 16;  // K stages per block of the exponent pass
+
+// the elements k0 .. k0+15 of one row (zero beyond K), all loads in flight
+__device__ __forceinline__ void oz_load16(double (&x)[16], const OzSliceJob &jb, const double *__restrict__ src,
+                                          const i64 *__restrict__ roff, const i64 *__restrict__ koff,
+                                          const int *__restrict__ kcombo, i64 row, int rc, i64 k0) {
+    const i64 *ro = roff + jb.roff + row * jb.nJ;
+    i64 addr[16];
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+        const i64 k = k0 + q;
+        addr[q] = k < jb.K ? ro[kcombo[jb.kcoff + k]] + koff[jb.koff + k * jb.nI + rc] : -1;
+    }
+#pragma unroll
+    for (int q = 0; q < 16; q++) x[q] = addr[q] >= 0 ? __ldg(src + addr[q]) : 0.0;
+}
+
+// pass 1: exponent e of every row maximum (|x| < 2^e) over chunks of
+// OZ_EXPO_CHUNK stages (grid.y), merged with atomicMax into expo, which
+// holds OZ_EXPO_NONE on entry
+template <int RT>
+__global__ void __launch_bounds__(256) k_oz_expo(const OzSliceJob *__restrict__ jobs, const double *__restrict__ src,
+                                                 const i64 *__restrict__ roff, const i64 *__restrict__ koff,
+                                                 const int *__restrict__ rcombo, const int *__restrict__ kcombo,
+                                                 int *__restrict__ expo) {
     const OzSliceJob jb = jobs[blockIdx.x];
+    const int kt0 = blockIdx.y * OZ_EXPO_CHUNK;
+    if (kt0 >= jb.KT) return;
+    const int kt1 = min(jb.KT, kt0 + OZ_EXPO_CHUNK);
     __shared__ int rmax[RT];
     const int tid = threadIdx.x;
-    for (int r = tid; r < RT; r += 256) rmax[r] = -100000;
+    for (int r = tid; r < RT; r += 256) rmax[r] = OZ_EXPO_NONE;
     __syncthreads();
     constexpr int UNITS = RT * (OZ_BK / 16);  // (row, 16 contracted indices) per stage
     const i64 r0 = (i64)jb.rt * RT;
-    // pass 1: exponent of the row maximum (|x| < 2^e)
-    for (int kt = 0; kt < jb.KT; kt++)
+    for (int kt = kt0; kt < kt1; kt++)
         for (int u = tid; u < UNITS; u += 256) {
             const int r = u % RT, k16 = u / RT;
             const i64 row = r0 + r;
             if (row >= jb.R) continue;
-            const i64 *ro = roff + jb.roff + row * jb.nJ;
-            const int rc = rcombo[jb.rcoff + row];
-            int e = -100000;
-            for (int q = 0; q < 16; q++) {
-                const i64 k = (i64)kt * OZ_BK + k16 * 16 + q;
-                if (k >= jb.K) break;
-                double x = src[ro[kcombo[jb.kcoff + k]] + koff[jb.koff + k * jb.nI + rc]];
-                if (x != 0.0) {
-                    int ex;
-                    frexp(x, &ex);
-                    e = max(e, ex);
-                }
+            double x[16];
+            oz_load16(x, jb, src, roff, koff, kcombo, row, rcombo[jb.rcoff + row], (i64)kt * OZ_BK + k16 * 16);
+            double amax = 0.0;
+#pragma unroll
+            for (int q = 0; q < 16; q++) amax = fmax(amax, fabs(x[q]));
+            if (amax != 0.0) {
+                int ex;
+                frexp(amax, &ex);
+                atomicMax(&rmax[r], ex);
             }
-            if (e > -100000) atomicMax(&rmax[r], e);
         }
     __syncthreads();
     for (int r = tid; r < RT; r += 256) {
         const i64 row = r0 + r;
-        if (rmax[r] == -100000) rmax[r] = 0;
-        if (row < jb.R) expo[jb.eoff + row] = rmax[r];
+        if (row < jb.R && rmax[r] != OZ_EXPO_NONE) atomicMax(&expo[jb.eoff + row], rmax[r]);
     }
-    __syncthreads();
-    // pass 2: digits, written as 16-byte rows of the core matrices
-    for (int kt = 0; kt < jb.KT; kt++) {
+}
+
+// pass 2: the S digit tiles of stage blockIdx.y, written as 16-byte rows of
+// the core matrices; rows and columns beyond the group's extents get zero
+// digits
+template <int S, int RT>
+__global__ void __launch_bounds__(256) k_oz_slice(const OzSliceJob *__restrict__ jobs, const double *__restrict__ src,
+                                                  const i64 *__restrict__ roff, const i64 *__restrict__ koff,
+                                                  const int *__restrict__ rcombo, const int *__restrict__ kcombo,
+                                                  int8_t *__restrict__ dig, const int *__restrict__ expo) {
+    const OzSliceJob jb = jobs[blockIdx.x];
+    const int kt = blockIdx.y;
+    if (kt >= jb.KT) return;
+    const int tid = threadIdx.x;
+    constexpr int UNITS = RT * (OZ_BK / 16);
+    const i64 r0 = (i64)jb.rt * RT;
+    {
         int8_t *tile = dig + jb.doff + ((size_t)jb.rt * jb.KT + kt) * (size_t)(S * RT * OZ_BK);
         for (int u = tid; u < UNITS; u += 256) {
             const int r = u % RT, k16 = u / RT;
@@ -319,13 +353,12 @@ __global__ void __launch_bounds__(256) k_oz_slice(const OzSliceJob *__restrict__
 #pragma unroll
             for (int t = 0; t < S; t++) w[t][0] = w[t][1] = w[t][2] = w[t][3] = 0u;
             if (row < jb.R) {
-                const i64 *ro = roff + jb.roff + row * jb.nJ;
-                const int rc = rcombo[jb.rcoff + row];
-                const double sc = ldexp(1.0, -rmax[r]);
+                double x[16];
+                oz_load16(x, jb, src, roff, koff, kcombo, row, rcombo[jb.rcoff + row], (i64)kt * OZ_BK + k16 * 16);
+                const double sc = ldexp(1.0, -oz_expo(expo[jb.eoff + row]));
+#pragma unroll
                 for (int q = 0; q < 16; q++) {
-                    const i64 k = (i64)kt * OZ_BK + k16 * 16 + q;
-                    if (k >= jb.K) break;
-                    double y = src[ro[kcombo[jb.kcoff + k]] + koff[jb.koff + k * jb.nI + rc]] * sc;
+                    double y = x[q] * sc;
 #pragma unroll
                     for (int t = 0; t < S; t++) {
                         y *= 128.0;
@@ -364,8 +397,11 @@ int oz_gemm_launch(const OzDevPlan &p, const int8_t *Adig, const int8_t *Bdig, c
 template <int S, int RT>
 int oz_slice_launch(const OzSideDev &sd, const double *src, int8_t *dig, int *expo) {
     if (sd.njobs == 0) return CPSD_OK;
-    k_oz_slice<S, RT><<<sd.njobs, 256, 0, stream()>>>(sd.jobs, src, sd.roff, sd.koff, sd.rcombo, sd.kcombo, dig, expo);
-    count_launch();
+    CPSD_TRY(cuda_check(cudaMemsetAsync(expo, 0x80, sizeof(int) * (size_t)sd.nexpo, stream()), "clear exponents"));
+    const dim3 ge(sd.njobs, (sd.kt_max + OZ_EXPO_CHUNK - 1) / OZ_EXPO_CHUNK), gd(sd.njobs, sd.kt_max);
+    k_oz_expo<RT><<<ge, 256, 0, stream()>>>(sd.jobs, src, sd.roff, sd.koff, sd.rcombo, sd.kcombo, expo);
+    k_oz_slice<S, RT><<<gd, 256, 0, stream()>>>(sd.jobs, src, sd.roff, sd.koff, sd.rcombo, sd.kcombo, dig, expo);
+    count_launch(2);
     return cuda_check(cudaGetLastError(), "k_oz_slice");
 }
 

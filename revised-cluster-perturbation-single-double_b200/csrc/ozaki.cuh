@@ -30,6 +30,8 @@ struct OzSliceJob {
 struct OzSideDev {
     const OzSliceJob *jobs = nullptr;
     int njobs = 0;
+    int kt_max = 0;  // most K stages of a job
+    i64 nexpo = 0;   // exponents of this side
     const i64 *roff = nullptr, *koff = nullptr;
     const int *rcombo = nullptr, *kcombo = nullptr;
 };
@@ -55,6 +57,9 @@ struct OzPlan {
     i64 nea = 0, neb = 0;        // row / column exponents
     int kt_chunk = 0;            // K stages per launch (keeps the int32 sums exact)
     int kt_max = 0;              // largest K stage count of the groups
+    double flops = 0;            // useful FP64-equivalent flops (2 M N K)
+    double pad_eff = 0;          // useful / padded tile work
+    i64 kmin = 0;                // shortest contracted length of a group
     uint64_t ahash = 0, bhash = 0;  // layout signatures of the A / B digits
     // device copies (uploaded at the first launch)
     bool uploaded = false;

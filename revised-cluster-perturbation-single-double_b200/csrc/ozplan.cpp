@@ -67,6 +67,10 @@ int OzPlan::upload() {
     CPSD_TRY(upload_vec(aroff, &adev.roff));
     CPSD_TRY(upload_vec(akoff, &adev.koff));
     adev.njobs = (int)ajobs.size();
+    adev.kt_max = kt_max;
+    adev.nexpo = nea;
+    bdev.kt_max = kt_max;
+    bdev.nexpo = neb;
     adev.rcombo = dev.mcombo;
     adev.kcombo = kc;
     CPSD_TRY(upload_vec(bjobs, &bdev.jobs));
@@ -92,6 +96,7 @@ int plan_ozaki(const ContractPlan *cp, int S, const OzPlan **out) {
     OzPlan &p = *P;
     p.S = S;
     p.BN = oz_tile_n(S);
+    p.flops = cp->flops;
     const int BN = p.BN;
     bool ok = !cp->empty && cp->task_mkey.size() == cp->h_tasks.size() && cp->seg_kkey.size() == cp->h_segs.size();
     // group the tasks by their (sorted) list of contracted combinations
@@ -138,6 +143,7 @@ int plan_ozaki(const ContractPlan *cp, int S, const OzPlan **out) {
     }
     const i64 kmax = (i64)(2147483647ll / ((i64)S * 127 * 127));
     p.kt_chunk = (int)std::max<i64>(1, kmax / 64);
+    double padded = 0.0;
     for (auto &G : grps) {
         const int nI = (int)G.mkeys.size(), nL = (int)G.nkeys.size(), nJ = (int)G.kkeys.size();
         // segment of task t for contracted combination j
@@ -227,8 +233,11 @@ int plan_ozaki(const ContractPlan *cp, int S, const OzPlan **out) {
         p.nea += Mpad;
         p.neb += Npad;
         p.kt_max = std::max(p.kt_max, og.KT);
+        p.kmin = p.groups.empty() ? og.K : std::min(p.kmin, og.K);
+        padded += 2.0 * (double)Mpad * (double)Npad * (double)Kpad;
         p.groups.push_back(og);
     }
+    p.pad_eff = padded > 0 ? p.flops / padded : 0.0;
     // signatures of the digit layouts: equal signatures read the same
     // elements of the source into the same digits
     uint64_t h = 1469598103934665603ull;
