@@ -591,9 +591,8 @@ static int ee_roots_batch(const Sys &S, const Ints &X, const cpsd_params *p, con
         for (;;) {
             iter++;
             CPSD_TRY(launch_energy(e1, 3, X.eorb, pr, R1));
-            CPSD_TRY(orth_launch(R1, L + r * l1, l1));
-            CPSD_TRY(diis_step_launch(dd.st, dd.b, (int)iter, R1));
-            CPSD_TRY(orth_launch(R1, L + r * l1, l1));
+            // orthogonalR2L, dosodiis2_d, orthogonalR2L in one launch
+            CPSD_TRY(diis_step_launch(dd.st, dd.b, (int)iter, R1, L + r * l1));
             double res;
             CPSD_TRY(read_back(&res, &dd.st->res, sizeof res));
             if (iter > 1 && std::fabs(res) < p->diis_max_err) break;

@@ -49,12 +49,12 @@ int engine(const Ten &v1, const char *t1, const Ten &v2, const char *t2, Ten &v3
     const ContractPlan *p;
     CPSD_TRY(plan_contract(v1.d, t1, v2.d, t2, v3.d, t3, b, &p));
     // digit tensor-core path for large contractions whose dense regrouping
-    // wastes at most half of the padded tiles and has K of at least 256
+    // uses at least a quarter of the padded tiles and has K of at least 256
     // (min_gflop = 0 routes every contraction that regroups)
     const OzPlan *oz = nullptr;
     if (ctx().oz_digits > 0 && !p->empty && p->flops >= ctx().oz_min_flops) {
         CPSD_TRY(plan_ozaki(p, ctx().oz_digits, &oz));
-        if (oz && ctx().oz_min_flops > 0 && (oz->pad_eff < 0.5 || oz->kmin < 256)) oz = nullptr;
+        if (oz && ctx().oz_min_flops > 0 && (oz->pad_eff < 0.25 || oz->kmin < 256)) oz = nullptr;
     }
     i64 l3 = v3.len();
     if (f2 != 1.0) {

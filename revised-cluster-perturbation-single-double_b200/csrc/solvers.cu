@@ -451,61 +451,92 @@ __global__ void __launch_bounds__(DT) k_dav_final(DavState *st, DavBuffers b, co
 }
 
 // ------------------------------------------------------------------- DIIS
-// LINPACK dgefa / dgesl (as MINV, src/libsrint/minv.f, calls them)
-__device__ void dgefa(double *a, int lda, int n, int *ipvt) {
+// LINPACK dgefa / dgesl (as MINV, src/libsrint/minv.f, calls them) by one
+// warp on a matrix in shared memory (n <= 32): lane i owns row i.  Pivot =
+// first row of largest magnitude; every element sees the same operations in
+// the same order as the sequential LINPACK loops.
+__device__ void warp_dgefa(double *a, int lda, int n, int *ipvt) {
+    const int i = threadIdx.x & 31;
     for (int k = 0; k < n - 1; k++) {
-        int l = k;
-        double m = -1.0;
-        for (int i = k; i < n; i++)
-            if (fabs(a[i + k * lda]) > m) {
-                m = fabs(a[i + k * lda]);
-                l = i;
+        double m = (i >= k && i < n) ? fabs(a[i + k * lda]) : -1.0;
+        int l = (i >= k && i < n) ? i : 0x7fffffff;
+        for (int o = 16; o > 0; o >>= 1) {
+            double om = __shfl_xor_sync(0xffffffffu, m, o);
+            int ol = __shfl_xor_sync(0xffffffffu, l, o);
+            if (om > m || (om == m && ol < l)) {
+                m = om;
+                l = ol;
             }
-        ipvt[k] = l;
+        }
+        if (i == 0) ipvt[k] = l;
+        __syncwarp();
         if (a[l + k * lda] == 0.0) continue;
-        if (l != k) {
-            double t = a[l + k * lda];
-            a[l + k * lda] = a[k + k * lda];
-            a[k + k * lda] = t;
+        if (l != k && i >= k && i < n) {  // swap rows l and k in columns >= k (lane i: column i)
+            double t = a[l + i * lda];
+            a[l + i * lda] = a[k + i * lda];
+            a[k + i * lda] = t;
         }
-        double t = -1.0 / a[k + k * lda];
-        for (int i = k + 1; i < n; i++) a[i + k * lda] *= t;
-        for (int j = k + 1; j < n; j++) {
-            double tj = a[l + j * lda];
-            if (l != k) {
-                a[l + j * lda] = a[k + j * lda];
-                a[k + j * lda] = tj;
-            }
-            for (int i = k + 1; i < n; i++) a[i + j * lda] += tj * a[i + k * lda];
+        __syncwarp();
+        const double t = -1.0 / a[k + k * lda];
+        if (i > k && i < n) {
+            double aik = a[i + k * lda] * t;
+            a[i + k * lda] = aik;
+            for (int j = k + 1; j < n; j++) a[i + j * lda] += a[k + j * lda] * aik;
         }
+        __syncwarp();
     }
-    ipvt[n - 1] = n - 1;
+    if (i == 0) ipvt[n - 1] = n - 1;
+    __syncwarp();
 }
-__device__ void dgesl(const double *a, int lda, int n, const int *ipvt, double *bv) {
+__device__ void warp_dgesl(const double *a, int lda, int n, const int *ipvt, double *bv) {
+    const int i = threadIdx.x & 31;
     for (int k = 0; k < n - 1; k++) {
-        int l = ipvt[k];
-        double t = bv[l];
-        if (l != k) {
+        const int l = ipvt[k];
+        const double t = bv[l];
+        __syncwarp();
+        if (i == 0 && l != k) {
             bv[l] = bv[k];
             bv[k] = t;
         }
-        for (int i = k + 1; i < n; i++) bv[i] += t * a[i + k * lda];
+        __syncwarp();
+        if (i > k && i < n) bv[i] += t * a[i + k * lda];
+        __syncwarp();
     }
     for (int kb = 0; kb < n; kb++) {
-        int k = n - 1 - kb;
-        bv[k] /= a[k + k * lda];
-        double t = -bv[k];
-        for (int i = 0; i < k; i++) bv[i] += t * a[i + k * lda];
+        const int k = n - 1 - kb;
+        if (i == 0) bv[k] /= a[k + k * lda];
+        __syncwarp();
+        const double t = -bv[k];
+        if (i < k) bv[i] += t * a[i + k * lda];
+        __syncwarp();
     }
 }
 
-__global__ void __launch_bounds__(DT) k_diis(DiisState *st, DiisBuffers b, int iter, double *vec) {
+// R -= (<L|R> / ||L||) L, the reference's orthogonalR2L (L is normalised,
+// so it divides by the norm)
+__device__ void block_orth(double *R, const double *L, int n, double *sh) {
+    double nrm = sqrt(block_dot(L, L, n, sh));
+    double dot = block_dot(L, R, n, sh);
+    double f = -dot / nrm;
+    for (int k = threadIdx.x; k < n; k += DT) R[k] += f * L[k];
+    __syncthreads();
+}
+
+__device__ void diis_extrapolate(DiisState &s, const DiisBuffers &b, double *vec, double *sh, int *shi, double *Bm,
+                                 double *coef, double *aug, double *rhs, int *ipvt);
+
+// One DIIS step (dosodiis2_d) on vec; with L, vec is first and last made
+// orthogonal to L (the solver's orthogonalR2L calls around it)
+__global__ void __launch_bounds__(DT) k_diis(DiisState *st, DiisBuffers b, int iter, double *vec, const double *L) {
     __shared__ double sh[DT / 32 + 1];
     __shared__ int shi[DT / 32 + 1];
     __shared__ double Bm[DIIS_MAXDIM * DIIS_MAXDIM];
     __shared__ double coef[DIIS_MAXDIM + 1];
+    __shared__ double aug[(DIIS_MAXDIM + 1) * (DIIS_MAXDIM + 1)], rhs[DIIS_MAXDIM + 1];
+    __shared__ int ipvt[DIIS_MAXDIM + 1];
     DiisState &s = *st;
-    const int len = s.len, maxdim = s.maxdim, tid = threadIdx.x;
+    const int len = s.len, tid = threadIdx.x;
+    if (L) block_orth(vec, L, len, sh);
     if (iter == 1) {
         for (int k = tid; k < len; k += DT) b.prev[k] = vec[k];
         if (tid == 0) {
@@ -513,8 +544,18 @@ __global__ void __launch_bounds__(DT) k_diis(DiisState *st, DiisBuffers b, int i
             s.ndimr = 1;
             s.res = 1.0;
         }
-        return;
+    } else {
+        diis_extrapolate(s, b, vec, sh, shi, Bm, coef, aug, rhs, ipvt);
     }
+    if (L) {
+        __syncthreads();
+        block_orth(vec, L, len, sh);
+    }
+}
+
+__device__ void diis_extrapolate(DiisState &s, const DiisBuffers &b, double *vec, double *sh, int *shi, double *Bm,
+                                 double *coef, double *aug, double *rhs, int *ipvt) {
+    const int len = s.len, maxdim = s.maxdim, tid = threadIdx.x;
     const int id = s.idimr - 1;
     for (int k = tid; k < len; k += DT) {
         double p = b.prev[k];
@@ -537,23 +578,19 @@ __global__ void __launch_bounds__(DT) k_diis(DiisState *st, DiisBuffers b, int i
     __syncthreads();
     for (int e = tid; e < DIIS_MAXDIM * DIIS_MAXDIM; e += DT) Bm[e] = s.Bm[e];
     __syncthreads();
-    if (tid == 0) {  // dodiis (src/libsrint/dodiis.f): bordered system with -1e-4
+    if (tid < 32) {  // dodiis (src/libsrint/dodiis.f): bordered system with -1e-4
         const int n1 = nd + 1;
-        double aug[(DIIS_MAXDIM + 1) * (DIIS_MAXDIM + 1)];
-        double rhs[DIIS_MAXDIM + 1];
-        int ipvt[DIIS_MAXDIM + 1];
-        for (int e = 0; e < n1 * n1; e++) aug[e] = 0.0;
-        for (int j = 0; j < nd; j++)
-            for (int i = 0; i < nd; i++) aug[(i + 1) + (j + 1) * n1] = Bm[i + j * DIIS_MAXDIM];
-        for (int i = 1; i <= nd; i++) {
-            aug[i] = -1.0e-4;
-            aug[i * n1] = -1.0e-4;
+        for (int e = tid; e < n1 * n1; e += 32) {
+            const int i = e % n1, j = e / n1;
+            aug[e] = (i == 0 && j == 0) ? 0.0
+                     : (i == 0 || j == 0) ? -1.0e-4
+                                          : Bm[(i - 1) + (j - 1) * DIIS_MAXDIM];
         }
-        rhs[0] = -1.0e-4;
-        for (int i = 1; i <= nd; i++) rhs[i] = 0.0;
-        dgefa(aug, n1, n1, ipvt);
-        dgesl(aug, n1, n1, ipvt, rhs);
-        for (int i = 0; i < nd; i++) coef[i] = rhs[i + 1];
+        if (tid < n1) rhs[tid] = (tid == 0) ? -1.0e-4 : 0.0;
+        __syncwarp();
+        warp_dgefa(aug, n1, n1, ipvt);
+        warp_dgesl(aug, n1, n1, ipvt, rhs);
+        if (tid < nd) coef[tid] = rhs[tid + 1];
     }
     __syncthreads();
     for (int k = tid; k < len; k += DT) {
@@ -607,8 +644,8 @@ int dav_final_launch(DavState *st, const DavBuffers &b) {
     count_launch();
     return cuda_check(cudaGetLastError(), "k_dav_final");
 }
-int diis_step_launch(DiisState *st, const DiisBuffers &b, int iter, double *vec) {
-    k_diis<<<1, DT, 0, stream()>>>(st, b, iter, vec);
+int diis_step_launch(DiisState *st, const DiisBuffers &b, int iter, double *vec, const double *L) {
+    k_diis<<<1, DT, 0, stream()>>>(st, b, iter, vec, L);
     count_launch();
     return cuda_check(cudaGetLastError(), "k_diis");
 }

@@ -46,7 +46,9 @@ struct DiisState {
 struct DiisBuffers {
     double *prev, *err, *amp;  // len, maxdim*len, maxdim*len
 };
-int diis_step_launch(DiisState *st, const DiisBuffers &b, int iter, double *vec);
+// one DIIS step on vec; with L (not null) vec is made orthogonal to L before
+// and after it (orthogonalR2L around dosodiis2_d in the reference's solver)
+int diis_step_launch(DiisState *st, const DiisBuffers &b, int iter, double *vec, const double *L = nullptr);
 // R -= (<L|R>/||L||) L  (orthogonalR2L, src/EE-CPSd.SF/orthogonalR2L.f90:5-34)
 int orth_launch(double *R, const double *L, i64 n);
 
