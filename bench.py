@@ -5,9 +5,13 @@ One step = the whole pipeline of the workload: SF-CIS Davidson (residual
 1e-8) for every requested root, ground CPS(D) T^(1)/T^(2), the J^(2)/J^(3)
 intermediates and EE-CPS(D-3) orders 1-3 for every root, with the integrals
 resident in HBM.  Default workload: D2h, nmo 200, nocc 10/8, 5 spin-flip
-roots, FP64 throughout (synthetic seeded integrals, see synth.py).
+roots (synthetic seeded integrals, see synth.py).  The headline value is
+the mixed mode (contractions of at least 1 GFLOP on the int8 tensor cores
+with --digits 7-bit digits per FP64 value, exact integer sums, FP64
+everywhere else); the plain FP64 path is timed beside it (fp64_path) and
+the largest deviation of any energy from it is reported.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--config NAME]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--config NAME] [--digits D]
   python bench.py --impl reference ...   (CPU restatement on the host cores)
 
 Multi-GPU: one process per GPU (torchrun); every rank runs an independent
@@ -39,6 +43,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-threads", type=int, default=0)
+    ap.add_argument("--digits", type=int, default=5,
+                    help="7-bit digits per FP64 value on the int8 tensor cores (0 = FP64 path only)")
     return ap.parse_args()
 
 
@@ -170,6 +176,46 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def measured_int8_peak(torch):
+    """cuBLASLt int8 GEMM (torch._int_mm, 8192^3) on this GPU in TOPS, the
+    roofline of the int8-digit contraction kernel; None if unavailable."""
+    try:
+        n = 8192
+        a = torch.randint(-127, 128, (n, n), dtype=torch.int8, device="cuda")
+        b = torch.randint(-127, 128, (n, n), dtype=torch.int8, device="cuda")
+        for _ in range(2):
+            torch._int_mm(a, b)
+        torch.cuda.synchronize()
+        best = 1e30
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch._int_mm(a, b)
+            e1.record()
+            e1.synchronize()
+            best = min(best, e0.elapsed_time(e1) / 1e3)
+        del a, b
+        torch.cuda.empty_cache()
+        return 2.0 * n ** 3 / best / 1e12
+    except Exception:
+        return None
+
+
+def contraction_records(api):
+    """per-launch (ms, flops, kind) of the contraction timing buffer"""
+    import ctypes
+    lib = api.lib()
+    n = 16384
+    ms = np.zeros(n)
+    fl = np.zeros(n)
+    sh = np.zeros(4 * n, np.int64)
+    nr = ctypes.c_int64()
+    lib.cpsd_contract_records(ms.ctypes.data_as(ctypes.c_void_p), fl.ctypes.data_as(ctypes.c_void_p),
+                              sh.ctypes.data_as(ctypes.c_void_p), ctypes.c_int64(n), ctypes.byref(nr))
+    k = nr.value
+    return ms[:k], fl[:k], sh[:4 * k].reshape(k, 4)[:, 3]
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -185,58 +231,95 @@ def run_ours(args, rank, world, local_rank):
     sysc = api.make_system(s)
     par = api.make_params(s, batch_roots=1)
     stream = torch.cuda.current_stream()
+    digits = args.digits
 
     def step():
         return api.pipeline(s, sysc, ints, par)
 
-    for _ in range(args.warmup):
-        out = step()
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    clocks = ClockSampler(local_rank)
-    api.launch_count(True)
-    api.flop_count(True)
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        out = step()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    ck = clocks.stop()
-    ms = e0.elapsed_time(e1)
-    launches = api.launch_count(True)
-    flops = api.flop_count(True)
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = world * s.nroots * args.steps / (ms_max / 1e3)
-    om, w2, w3 = out
+    def timed(mode_digits):
+        api.set_mixed(mode_digits, 1.0)
+        for _ in range(args.warmup):
+            out = step()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        api.launch_count(True)
+        api.flop_count(True)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            out = step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        ms = e0.elapsed_time(e1)
+        launches = api.launch_count(True)
+        flops = api.flop_count(True)
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item()), out, launches, flops
 
-    # roofline of the dominant kernel (the grouped FP64 contraction), timed
-    # with CUDA events around each of its launches in one extra step
-    import ctypes
+    clocks = ClockSampler(local_rank)
+    ms64, out64, launches64, flops64 = timed(0)
+    if digits:
+        ms_max, out, launches, flops = timed(digits)
+    else:
+        ms_max, out, launches, flops = ms64, out64, launches64, flops64
+    ck = clocks.stop()
+    err = api.mixed_error() if digits else 0
+    value = world * s.nroots * args.steps / (ms_max / 1e3)
+    value64 = world * s.nroots * args.steps / (ms64 / 1e3)
+    dev_fp64 = max(float(np.max(np.abs(np.asarray(a) - np.asarray(b)))) for a, b in zip(out, out64))
+    om, w2, w3 = out
+    step_ms = ms_max / args.steps
+
+    # per-launch CUDA-event timing of every contraction launch in one extra
+    # step of the headline mode: roofline of the digit GEMM (int8 tensor
+    # cores) and of the FP64 tensor-pipe kernel
     lib = api.lib()
     lib.cpsd_contract_timing(1)
     lib.cpsd_contract_time(None, None, None, 1)
     step()
-    c_ms, c_n, c_fl = ctypes.c_double(), ctypes.c_int64(), ctypes.c_double()
-    lib.cpsd_contract_time(ctypes.byref(c_ms), ctypes.byref(c_n), ctypes.byref(c_fl), 1)
+    torch.cuda.synchronize()
+    rms, rfl, rkind = contraction_records(api)
+    lib.cpsd_contract_time(None, None, None, 1)
     lib.cpsd_contract_timing(0)
+    api.set_mixed(0)
     fp64_peak = measured_fp64_peak(torch)
-    achieved = c_fl.value / (c_ms.value / 1e3) / 1e12 if c_ms.value > 0 else 0.0
-    step_total_ms = ms_max / args.steps
+    pairs = digits * (digits + 1) // 2 if digits else 0
+    roof = None
+    if digits:
+        int8_peak = measured_int8_peak(torch)
+        sel = rkind == 12
+        g_ms, g_fl = float(rms[sel].sum()), float(rfl[sel].sum())
+        ach = g_fl * pairs / (g_ms / 1e3) / 1e12 if g_ms > 0 else 0.0
+        roof = {"bound": "tensor", "kernel": f"k_oz_gemm (tcgen05 kind::i8, {digits} digits, {pairs} digit products)",
+                "achieved": ach, "peak": int8_peak, "unit": "TOPS (int8)",
+                "frac": ach / int8_peak if int8_peak else None, "traffic": None,
+                "peak_source": "measured cuBLASLt int8 GEMM 8192^3 (torch._int_mm) on this GPU",
+                "fp64_equivalent_tflops": g_fl / (g_ms / 1e3) / 1e12 if g_ms > 0 else 0.0,
+                "share_of_step": g_ms / step_ms, "launches_per_step": int(sel.sum())}
+    sel = rkind < 10
+    d_ms, d_fl = float(rms[sel].sum()), float(rfl[sel].sum())
+    roof64 = {"bound": "tensor", "kernel": "k_contract (FP64 mma.sync m8n8k4 grouped contraction)",
+              "achieved": d_fl / (d_ms / 1e3) / 1e12 if d_ms > 0 else 0.0, "peak": fp64_peak, "unit": "TFLOP/s",
+              "frac": (d_fl / (d_ms / 1e3) / 1e12) / fp64_peak if d_ms > 0 and fp64_peak else None,
+              "traffic": None, "peak_source": "measured cuBLAS DGEMM 8192^3 on this GPU",
+              "share_of_step": d_ms / step_ms, "launches_per_step": int(sel.sum())}
+    shares = {lab: round(float(rms[m].sum()) / step_ms, 4) for lab, m in
+              (("digit_gemm", rkind == 12), ("digit_slicing", (rkind == 10) | (rkind == 11)),
+               ("fp64_tiles", rkind < 10), ("narrow", rkind >= 20))}
 
     # end to end through the public API with host buffers: H2D of every
     # integral tensor from pinned memory, the pipeline, results back on the host
     e2e = None
     if not args.no_e2e:
+        api.set_mixed(digits, 1.0)
         host = {k: torch.from_numpy(s.ints[k]).pin_memory() for k in api.DeviceIntegrals.KEYS
                 if s.ints[k] is not None}
         host["eorb"] = torch.from_numpy(s.eorb).pin_memory()
@@ -256,6 +339,7 @@ def run_ours(args, rank, world, local_rank):
             dist.all_reduce(t2, op=dist.ReduceOp.MAX)
         e2e = {"value": world * s.nroots * args.steps / (float(t2.item()) / 1e3), "unit": "roots/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
+        api.set_mixed(0)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -266,21 +350,25 @@ def run_ours(args, rank, world, local_rank):
                          "extrapolated to all roots of the workload",
                "stage_seconds": {k: round(x, 4) for k, x in info.items()}}
     if rank == 0:
+        mode = (f"mixed: contractions >= 1 GFLOP on the int8 tensor cores with {digits} 7-bit digits per FP64 "
+                f"value (exact int32 sums, FP64 epilogue); everything else FP64" if digits else "FP64")
         line = {
             "metric": METRIC, "value": value, "unit": "roots/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": step_total_ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator, synth.py)",
+            "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64 (int8 digits)" if digits else "f64",
+            "data": "synthetic (seeded generator, synth.py)",
             "config": {"workload": workload_desc(s, args.config), "inputs": "resident in HBM, "
                        f"{ints.nbytes / 1e9:.2f} GB of integrals (larger than L2)",
-                       "parallelism": f"replicas x{world}", "roots_batched": True},
-            "roofline": {"bound": "tensor", "kernel": "k_contract (grouped FP64 DPD contraction)",
-                         "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
-                         "frac": achieved / fp64_peak if fp64_peak else None, "traffic": None,
-                         "peak_source": "measured cuBLAS DGEMM 8192^3 on this GPU (MEASURED_PEAKS.json has no FP64 "
-                                        "figure)", "share_of_step": c_ms.value / step_total_ms,
-                         "launches_per_step": c_n.value},
+                       "parallelism": f"replicas x{world}", "roots_batched": True, "mode": mode},
+            "max_abs_dev_vs_fp64_eh": dev_fp64,
+            "fp64_path": {"value": value64, "unit": "roots/s", "ms_per_step": ms64 / args.steps,
+                          "gpu_launches": launches64, "contraction_tflops": flops64 / (ms64 / 1e3) / 1e12},
+            "roofline": roof or roof64,
+            "roofline_fp64_tiles": roof64,
+            "contraction_shares_of_step": shares,
             "contraction_tflops": flops / (ms_max / 1e3) / 1e12,
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": ck,
+            "digit_path_timeouts": err,
             "results": {"omega_cis": [float(x) for x in om], "w2": [float(x) for x in w2],
                         "w3": [float(x) for x in w3]},
         }

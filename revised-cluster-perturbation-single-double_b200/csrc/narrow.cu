@@ -1,0 +1,329 @@
+// Narrow-output contractions (FP64): CIS / solver sigma vectors, one-index
+// intermediates and the other contractions whose output block has at most
+// 16 columns (or rows), where tensor-core tiles would be mostly padding.
+//
+// Short contracted range: one thread per output row, the few columns in
+// registers, the column operand read as warp-uniform broadcasts.  Long
+// contracted range: one warp per 4 rows x 8 columns, lanes striding over K
+// (loads along the contiguous K of both operands), a 31-shuffle transpose
+// reduction of the 32 sums, and a K split with a fixed-order reduce when
+// there are too few rows to fill the GPU.  Both use the planner's task /
+// segment tables of the grouped contraction, so every layout that the
+// tensor-core path handles is handled here too.
+#include <algorithm>
+#include <map>
+#include <memory>
+
+#include "narrow.cuh"
+
+namespace cpsd {
+
+namespace {
+
+constexpr int NW = 4;  // warps per CTA
+
+__device__ __forceinline__ i64 ndecode(i64 x, int n, const i64 *ext, const i64 *st) {
+    i64 off = 0;
+    for (int u = 0; u < n; u++) {
+        i64 e = ext[u];
+        i64 q = x / e;
+        off += (x - q * e) * st[u];
+        x = q;
+    }
+    return off;
+}
+
+__device__ __forceinline__ void kdecode(i64 k, const SegDev &sg, const i64 *kx, const i64 *ky, i64 *ox, i64 *oy) {
+    if (sg.nk == 1) {
+        *ox = k * kx[0];
+        *oy = k * ky[0];
+        return;
+    }
+    i64 a = 0, b = 0;
+    for (int u = 0; u < sg.nk; u++) {
+        i64 e = sg.kExt[u], q = k / e, r = k - q * e;
+        a += r * kx[u];
+        b += r * ky[u];
+        k = q;
+    }
+    *ox = a;
+    *oy = b;
+}
+
+// row / column views of a task and segment: rows run over the M side
+// (first operand), or over the N side when SWAP
+template <bool SWAP>
+struct View {
+    const TaskDev &tk;
+    __device__ View(const TaskDev &t) : tk(t) {}
+    __device__ i64 R() const { return SWAP ? tk.N : tk.M; }
+    __device__ i64 CN() const { return SWAP ? tk.M : tk.N; }
+    __device__ i64 xrow(const SegDev &sg, i64 r) const {
+        return SWAP ? sg.baseB + ndecode(r, tk.nn, tk.nExt, sg.nSB) : sg.baseA + ndecode(r, tk.nm, tk.mExt, sg.mSA);
+    }
+    __device__ i64 ycol(const SegDev &sg, i64 c) const {
+        return SWAP ? sg.baseA + ndecode(c, tk.nm, tk.mExt, sg.mSA) : sg.baseB + ndecode(c, tk.nn, tk.nExt, sg.nSB);
+    }
+    __device__ i64 crow(i64 r) const {
+        return SWAP ? ndecode(r, tk.nn, tk.nExt, tk.nSC) : ndecode(r, tk.nm, tk.mExt, tk.mSC);
+    }
+    __device__ i64 ccol(i64 c) const {
+        return SWAP ? ndecode(c, tk.nm, tk.mExt, tk.mSC) : ndecode(c, tk.nn, tk.nExt, tk.nSC);
+    }
+    __device__ const i64 *kx(const SegDev &sg) const { return SWAP ? sg.kSB : sg.kSA; }
+    __device__ const i64 *ky(const SegDev &sg) const { return SWAP ? sg.kSA : sg.kSB; }
+};
+
+// short K: thread = row, 8 columns in registers
+template <bool SWAP>
+__global__ void __launch_bounds__(NW * 32) k_narrow_rows(const TaskDev *__restrict__ tasks,
+                                                         const SegDev *__restrict__ segs,
+                                                         const NarrowItem *__restrict__ items, int nitems,
+                                                         const double *__restrict__ A, const double *__restrict__ B,
+                                                         double *__restrict__ C, double alpha) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int it = blockIdx.x * NW + warp;
+    if (it >= nitems) return;
+    const NarrowItem item = items[it];
+    const TaskDev &tk = tasks[item.task];
+    const View<SWAP> v(tk);
+    const double *X = SWAP ? B : A, *Y = SWAP ? A : B;
+    const i64 r = item.r0 + lane;
+    const bool rok = r < v.R();
+    const int ncol = (int)min((i64)NARROW_COLS, v.CN() - item.c0);
+    double acc[NARROW_COLS];
+#pragma unroll
+    for (int c = 0; c < NARROW_COLS; c++) acc[c] = 0.0;
+    for (int si = 0; si < tk.nseg; si++) {
+        const SegDev &sg = segs[tk.seg0 + si];
+        const i64 ox = rok ? v.xrow(sg, r) : 0;
+        i64 oy[NARROW_COLS];
+#pragma unroll
+        for (int c = 0; c < NARROW_COLS; c++) oy[c] = c < ncol ? v.ycol(sg, item.c0 + c) : 0;
+        const i64 *kx = v.kx(sg), *ky = v.ky(sg);
+#pragma unroll 4
+        for (i64 k = 0; k < sg.K; k++) {
+            i64 fx, fy;
+            kdecode(k, sg, kx, ky, &fx, &fy);
+            const double x = rok ? __ldg(X + ox + fx) : 0.0;
+#pragma unroll
+            for (int c = 0; c < NARROW_COLS; c++)
+                if (c < ncol) acc[c] = fma(x, __ldg(Y + oy[c] + fy), acc[c]);
+        }
+    }
+    if (!rok) return;
+    const i64 oc = tk.baseC + v.crow(r);
+#pragma unroll
+    for (int c = 0; c < NARROW_COLS; c++)
+        if (c < ncol) C[oc + v.ccol(item.c0 + c)] += alpha * acc[c];
+}
+
+// 32 values per lane -> lane l holds the warp total of value l
+__device__ __forceinline__ double transpose_reduce(double (&v)[32]) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int s = 16; s >= 1; s >>= 1) {
+        const bool up = (lane & s) != 0;
+#pragma unroll
+        for (int j = 0; j < s; j++) {
+            const double send = up ? v[j] : v[j + s];
+            const double recv = __shfl_xor_sync(0xffffffffu, send, s);
+            v[j] = (up ? v[j + s] : v[j]) + recv;
+        }
+    }
+    return v[0];
+}
+
+// long K: warp = 4 rows x 8 columns over the K range of the item
+template <bool SWAP>
+__global__ void __launch_bounds__(NW * 32) k_narrow_k(const TaskDev *__restrict__ tasks,
+                                                      const SegDev *__restrict__ segs,
+                                                      const NarrowItem *__restrict__ items, int nitems,
+                                                      const double *__restrict__ A, const double *__restrict__ B,
+                                                      double *__restrict__ C, double alpha,
+                                                      double *__restrict__ partial) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int it = blockIdx.x * NW + warp;
+    if (it >= nitems) return;
+    const NarrowItem item = items[it];
+    const TaskDev &tk = tasks[item.task];
+    const View<SWAP> v(tk);
+    const double *X = SWAP ? B : A, *Y = SWAP ? A : B;
+    const int nrow = (int)min((i64)NARROW_ROWS, v.R() - item.r0);
+    const int ncol = (int)min((i64)NARROW_COLS, v.CN() - item.c0);
+    double acc[32];
+#pragma unroll
+    for (int j = 0; j < 32; j++) acc[j] = 0.0;
+    for (int si = 0; si < tk.nseg; si++) {
+        const SegDev &sg = segs[tk.seg0 + si];
+        i64 kb = item.k0 - sg.kstart, ke = item.k1 - sg.kstart;
+        if (kb < 0) kb = 0;
+        if (ke > sg.K) ke = sg.K;
+        if (kb >= ke) continue;
+        i64 ox[NARROW_ROWS], oy[NARROW_COLS];
+#pragma unroll
+        for (int i = 0; i < NARROW_ROWS; i++) ox[i] = i < nrow ? v.xrow(sg, item.r0 + i) : 0;
+#pragma unroll
+        for (int c = 0; c < NARROW_COLS; c++) oy[c] = c < ncol ? v.ycol(sg, item.c0 + c) : 0;
+        const i64 *kx = v.kx(sg), *ky = v.ky(sg);
+#pragma unroll 2
+        for (i64 k = kb + lane; k < ke; k += 32) {
+            i64 fx, fy;
+            kdecode(k, sg, kx, ky, &fx, &fy);
+            double x[NARROW_ROWS], y[NARROW_COLS];
+#pragma unroll
+            for (int i = 0; i < NARROW_ROWS; i++) x[i] = i < nrow ? __ldg(X + ox[i] + fx) : 0.0;
+#pragma unroll
+            for (int c = 0; c < NARROW_COLS; c++) y[c] = c < ncol ? __ldg(Y + oy[c] + fy) : 0.0;
+#pragma unroll
+            for (int i = 0; i < NARROW_ROWS; i++)
+#pragma unroll
+                for (int c = 0; c < NARROW_COLS; c++) acc[i * NARROW_COLS + c] = fma(x[i], y[c], acc[i * NARROW_COLS + c]);
+        }
+    }
+    const double s = transpose_reduce(acc);
+    if (item.part >= 0) {
+        partial[item.part * 32 + lane] = s;
+        return;
+    }
+    const int i = lane / NARROW_COLS, c = lane % NARROW_COLS;
+    if (i < nrow && c < ncol) C[tk.baseC + v.crow(item.r0 + i) + v.ccol(item.c0 + c)] += alpha * s;
+}
+
+// split items of one output block, summed in K order
+template <bool SWAP>
+__global__ void __launch_bounds__(NW * 32) k_narrow_reduce(const TaskDev *__restrict__ tasks,
+                                                           const NarrowRed *__restrict__ reds, int nreds,
+                                                           const double *__restrict__ partial,
+                                                           double *__restrict__ C, double alpha) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int it = blockIdx.x * NW + warp;
+    if (it >= nreds) return;
+    const NarrowRed rd = reds[it];
+    const TaskDev &tk = tasks[rd.task];
+    const View<SWAP> v(tk);
+    double s = 0.0;
+    for (int q = 0; q < rd.nparts; q++) s += partial[(rd.part0 + q) * 32 + lane];
+    const int i = lane / NARROW_COLS, c = lane % NARROW_COLS;
+    if (rd.r0 + i < v.R() && rd.c0 + c < v.CN())
+        C[tk.baseC + v.crow(rd.r0 + i) + v.ccol(rd.c0 + c)] += alpha * s;
+}
+
+template <class T>
+int upload_vec(const std::vector<T> &v, T **d) {
+    *d = nullptr;
+    if (v.empty()) return CPSD_OK;
+    CPSD_TRY(cuda_check(cudaMalloc(d, sizeof(T) * v.size()), "cudaMalloc(narrow plan)"));
+    return cuda_check(cudaMemcpy(*d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice), "upload narrow plan");
+}
+
+}  // namespace
+
+int NarrowPlan::upload() {
+    if (uploaded) return CPSD_OK;
+    CPSD_TRY(upload_vec(items, &d_items));
+    CPSD_TRY(upload_vec(reds, &d_reds));
+    uploaded = true;
+    return CPSD_OK;
+}
+
+int plan_narrow(const ContractPlan *cp, const NarrowPlan **out) {
+    static std::map<const ContractPlan *, std::unique_ptr<NarrowPlan>> cache;
+    *out = nullptr;
+    auto it = cache.find(cp);
+    if (it != cache.end()) {
+        *out = it->second.get();
+        return CPSD_OK;
+    }
+    i64 maxM = 0, maxN = 0, maxK = 0;
+    for (const TaskDev &tk : cp->h_tasks) {
+        maxM = std::max(maxM, tk.M);
+        maxN = std::max(maxN, tk.N);
+        maxK = std::max(maxK, tk.Ktot);
+    }
+    std::unique_ptr<NarrowPlan> P;
+    bool ok = !cp->empty && (maxN <= 16 || maxM <= 16);
+    const bool swap = !(maxN <= 16), longk = maxK > 96;
+    if (ok) {  // the loads must be coalesced: along K (lanes over K) or along the rows
+        const TaskDev &t0 = cp->h_tasks[0];
+        const SegDev &s0 = cp->h_segs[t0.seg0];
+        const i64 kst = swap ? s0.kSB[0] : s0.kSA[0];
+        const i64 rst = swap ? s0.nSB[0] : s0.mSA[0];
+        const int nr = swap ? t0.nn : t0.nm;
+        ok = longk ? (s0.nk > 0 && kst == 1) : (nr > 0 && rst == 1);
+    }
+    if (ok) {
+        P = std::make_unique<NarrowPlan>();
+        NarrowPlan &p = *P;
+        p.swap = swap;
+        p.longk = longk;
+        auto R = [&](const TaskDev &t) { return p.swap ? t.N : t.M; };
+        auto CN = [&](const TaskDev &t) { return p.swap ? t.M : t.N; };
+        if (!p.longk) {
+            for (int ti = 0; ti < (int)cp->h_tasks.size(); ti++) {
+                const TaskDev &t = cp->h_tasks[ti];
+                for (i64 c0 = 0; c0 < CN(t); c0 += NARROW_COLS)
+                    for (i64 r0 = 0; r0 < R(t); r0 += 32) p.items.push_back(NarrowItem{ti, (int)c0, r0, 0, t.Ktot, -1});
+            }
+        } else {
+            i64 base = 0;
+            for (const TaskDev &t : cp->h_tasks)
+                base += ((R(t) + NARROW_ROWS - 1) / NARROW_ROWS) * ((CN(t) + NARROW_COLS - 1) / NARROW_COLS);
+            const i64 want = std::max<i64>(1, (8192 + base - 1) / base);
+            for (int ti = 0; ti < (int)cp->h_tasks.size(); ti++) {
+                const TaskDev &t = cp->h_tasks[ti];
+                const i64 ns = std::max<i64>(1, std::min<i64>(want, t.Ktot / 256));
+                for (i64 c0 = 0; c0 < CN(t); c0 += NARROW_COLS)
+                    for (i64 r0 = 0; r0 < R(t); r0 += NARROW_ROWS) {
+                        if (ns > 1) p.reds.push_back(NarrowRed{ti, (int)c0, (int)ns, 0, r0, p.nparts});
+                        for (i64 q = 0; q < ns; q++)
+                            p.items.push_back(NarrowItem{ti, (int)c0, r0, t.Ktot * q / ns, t.Ktot * (q + 1) / ns,
+                                                         ns > 1 ? p.nparts + q : -1});
+                        if (ns > 1) p.nparts += ns;
+                    }
+            }
+        }
+        *out = P.get();
+    }
+    cache[cp] = std::move(P);
+    return CPSD_OK;
+}
+
+int launch_narrow(const ContractPlan *cp, const NarrowPlan *np, const double *A, const double *B, double *C,
+                  double alpha) {
+    CPSD_TRY(const_cast<ContractPlan *>(cp)->upload());
+    CPSD_TRY(const_cast<NarrowPlan *>(np)->upload());
+    const int ni = (int)np->items.size(), nr = (int)np->reds.size();
+    if (ni == 0) return CPSD_OK;
+    cudaEvent_t end;
+    CPSD_TRY(timing_begin(cp->flops, cp->ntasks, ni, np->nparts, 20 + (np->longk ? 1 : 0), &end));
+    const int grid = (ni + NW - 1) / NW;
+    if (!np->longk) {
+        if (np->swap)
+            k_narrow_rows<true><<<grid, NW * 32, 0, stream()>>>(cp->d_tasks, cp->d_segs, np->d_items, ni, A, B, C, alpha);
+        else
+            k_narrow_rows<false><<<grid, NW * 32, 0, stream()>>>(cp->d_tasks, cp->d_segs, np->d_items, ni, A, B, C, alpha);
+        count_launch();
+    } else {
+        ScratchScope sc;
+        double *part = nullptr;
+        if (np->nparts > 0) CPSD_TRY(scratch(np->nparts * 32, &part));
+        if (np->swap)
+            k_narrow_k<true><<<grid, NW * 32, 0, stream()>>>(cp->d_tasks, cp->d_segs, np->d_items, ni, A, B, C, alpha, part);
+        else
+            k_narrow_k<false><<<grid, NW * 32, 0, stream()>>>(cp->d_tasks, cp->d_segs, np->d_items, ni, A, B, C, alpha, part);
+        count_launch();
+        if (nr > 0) {
+            const int rg = (nr + NW - 1) / NW;
+            if (np->swap)
+                k_narrow_reduce<true><<<rg, NW * 32, 0, stream()>>>(cp->d_tasks, np->d_reds, nr, part, C, alpha);
+            else
+                k_narrow_reduce<false><<<rg, NW * 32, 0, stream()>>>(cp->d_tasks, np->d_reds, nr, part, C, alpha);
+            count_launch();
+        }
+    }
+    CPSD_TRY(cuda_check(cudaGetLastError(), "k_narrow"));
+    return timing_end(end);
+}
+
+}  // namespace cpsd

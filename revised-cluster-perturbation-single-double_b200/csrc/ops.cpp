@@ -4,6 +4,7 @@
 
 #include <algorithm>
 
+#include "narrow.cuh"
 #include "ozaki.cuh"
 
 #include <cstring>
@@ -65,6 +66,13 @@ int engine(const Ten &v1, const char *t1, const Ten &v2, const char *t2, Ten &v3
     if (oz) {
         ctx().flops += p->flops;
         return launch_ozaki(oz, v1.arr, v2.arr, v3.arr, f1);
+    }
+    // at most 16 output columns (or rows): streaming kernels instead of tiles
+    const NarrowPlan *np = nullptr;
+    if (!p->empty) CPSD_TRY(plan_narrow(p, &np));
+    if (np) {
+        ctx().flops += p->flops;
+        return launch_narrow(p, np, v1.arr, v2.arr, v3.arr, f1);
     }
     return launch_contract(p, v1.arr, v2.arr, v3.arr, f1);
 }
@@ -767,6 +775,30 @@ int cpsd_debug_contract_plan(const cpsd_opt *v1, const char *t1, const cpsd_opt 
 
 int cpsd_contract_records(double *ms, double *flops, int64_t *shape, int64_t maxrec, int64_t *nrec) {
     return contract_records(ms, flops, shape, maxrec, nrec);
+}
+
+int cpsd_debug_narrow_plan(const cpsd_opt *v1, const char *t1, const cpsd_opt *v2, const char *t2,
+                           const cpsd_opt *v3, const char *t3, int64_t nb, int64_t sA, int64_t sB, int64_t sC,
+                           const void **items, int64_t *nitems, const void **reds, int64_t *nreds, int64_t *flags) {
+    CPSD_TRY(need_init());
+    Batch b;
+    b.nb = nb;
+    b.strideA = sA;
+    b.strideB = sB;
+    b.strideC = sC;
+    const ContractPlan *p;
+    CPSD_TRY(plan_contract(desc_of(v1), t1, desc_of(v2), t2, desc_of(v3), t3, b, &p));
+    const NarrowPlan *np = nullptr;
+    if (!p->empty) CPSD_TRY(plan_narrow(p, &np));
+    *items = np ? np->items.data() : nullptr;
+    *nitems = np ? (int64_t)np->items.size() : 0;
+    *reds = np ? np->reds.data() : nullptr;
+    *nreds = np ? (int64_t)np->reds.size() : 0;
+    flags[0] = np ? 1 : 0;
+    flags[1] = np && np->swap ? 1 : 0;
+    flags[2] = np && np->longk ? 1 : 0;
+    flags[3] = np ? np->nparts : 0;
+    return CPSD_OK;
 }
 
 int cpsd_debug_ozaki_plan(const cpsd_opt *v1, const char *t1, const cpsd_opt *v2, const char *t2,
