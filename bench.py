@@ -45,6 +45,10 @@ def parse():
     ap.add_argument("--cpu-threads", type=int, default=0)
     ap.add_argument("--digits", type=int, default=5,
                     help="7-bit digits per FP64 value on the int8 tensor cores (0 = FP64 path only)")
+    ap.add_argument("--no-fp64-path", action="store_true", help="skip timing the plain FP64 path beside the headline")
+    ap.add_argument("--case-nmo", type=int, default=100)
+    ap.add_argument("--case", default="", choices=["", "ladder"],
+                    help="time one contraction on its own (kernel profiling) instead of the pipeline")
     return ap.parse_args()
 
 
@@ -265,10 +269,11 @@ def run_ours(args, rank, world, local_rank):
         return float(t.item()), out, launches, flops
 
     clocks = ClockSampler(local_rank)
-    ms64, out64, launches64, flops64 = timed(0)
     if digits:
         ms_max, out, launches, flops = timed(digits)
+        ms64, out64, launches64, flops64 = (ms_max, out, launches, flops) if args.no_fp64_path else timed(0)
     else:
+        ms64, out64, launches64, flops64 = timed(0)
         ms_max, out, launches, flops = ms64, out64, launches64, flops64
     ck = clocks.stop()
     err = api.mixed_error() if digits else 0
@@ -375,8 +380,57 @@ def run_ours(args, rank, world, local_rank):
         print(json.dumps(line), flush=True)
 
 
+def run_case(args):
+    """One contraction of the pipeline on its own, for kernel profiling:
+    'ladder' = the particle-particle ladder V(ab,ef) T(ef,ij) -> C(ab,ij)
+    (c2_r2abcd's engine call) on one irrep, nmo 100, nocc 10/8 (v = 182,
+    16471 packed pairs: 2.2 GB of integrals), random data; --digits 0 runs
+    the FP64 tensor-pipe kernel, otherwise the int8-digit kernels."""
+    import torch
+    import __graft_entry__ as ge
+    ge.load_package()
+    from cpsd_b200 import api
+    from cpsd_b200.dpd import Symmetry, xor_dirprd
+    nmo, na, nb_ = args.case_nmo, 10, 8
+    o = np.array([na + nb_, 0, 0, 0, 0, 0, 0, 0])
+    v = np.array([2 * nmo - na - nb_, 0, 0, 0, 0, 0, 0, 0])
+    sym = Symmetry(1, xor_dirprd(1))
+    api.init(1, xor_dirprd(1))
+    api.use_torch_stream()
+    api.set_mixed(args.digits, 0.0)
+    la = sym.idsymsoc(1, v, v, 0, v, v, 0)
+    lt = sym.idsymsoc(1, v, v, 0, o, o, 0)
+    g = torch.Generator(device="cuda").manual_seed(0)
+    A = torch.randn(la, dtype=torch.float64, device="cuda", generator=g) * 0.05
+    T = torch.randn(lt, dtype=torch.float64, device="cuda", generator=g) * 0.01
+    C = torch.zeros(lt, dtype=torch.float64, device="cuda")
+    d4 = ([v, v, v, v], (0, 0), 1)
+    dt = ([v, v, o, o], (0, 0), 1)
+
+    def step():
+        api.vv2v_dpd_444(A, d4, "abef", T, dt, "efij", C, dt, "abij", 1.0, 0.0)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    fl = 2.0 * float(np.sqrt(la)) ** 2 * (lt / np.sqrt(la))  # 2 M N K with M = K = pairs
+    print(json.dumps({"case": args.case, "digits": args.digits, "ms_per_call": ms, "fp64_equivalent_tflops":
+                      fl / (ms / 1e3) / 1e12, "M": int(round(np.sqrt(la))), "N": int(round(lt / np.sqrt(la)))}),
+          flush=True)
+
+
 def main():
     args = parse()
+    if args.case:
+        run_case(args)
+        return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
