@@ -478,6 +478,95 @@ int cpsd_calJ(const cpsd_system *s, const cpsd_integrals *I, const double *T2_1,
 }
 
 // EE-CPS(D-3) for nb roots of irrep symR sharing every contraction launch
+// mapped host memory through which device-driven loops report progress
+static int mapped_mailbox(int **host, int **dev) {
+    static int *h = nullptr, *d = nullptr;
+    if (!h) {
+        CPSD_TRY(cuda_check(cudaHostAlloc((void **)&h, 4096, cudaHostAllocMapped), "cudaHostAlloc(mapped)"));
+        CPSD_TRY(cuda_check(cudaHostGetDevicePointer((void **)&d, h, 0), "mapped pointer"));
+    }
+    *host = h;
+    *dev = d;
+    return CPSD_OK;
+}
+
+// The solver of solver.f90:4-66 for nb roots of irrep symR at once: cc holds
+// -Ctilde1 (nb x l1), L the CIS vectors, w0d the CIS energies (device);
+// R1 receives the solutions, *sit the summed step counts.  Each step is one
+// k_solver_step launch (every root's update, denominator, orthogonalR2L /
+// dosodiis2_d / orthogonalR2L and its own convergence test) and one batched
+// sigma V(fn,ai) R1(fn); the host never waits on a step's result, it stays
+// at most two steps ahead and stops once every root reports convergence.
+static int solve_r1(const Sys &S, const Ints &X, const cpsd_params *p, i64 symR, i64 nb, i64 l1,
+                    const EnergyPlan *e1, const double *cc, const double *L, const double *w0d, double *R1,
+                    i64 *sit) {
+    const i64 *o = S.popo, *v = S.popv;
+    const int md = (int)p->diis_dim;
+    if (md > DIIS_MAXDIM) return set_error(CPSD_EARG, "diis_dim above 16");
+    if (nb > 1000) return set_error(CPSD_EARG, "more than 1000 roots in one irrep");
+    ScratchScope sc;
+    double *pr, *sg, *den, *prev, *err, *amp;
+    CPSD_TRY(scratch(nb * l1, &pr));
+    CPSD_TRY(scratch(nb * l1, &sg));
+    CPSD_TRY(scratch(l1, &den));
+    CPSD_TRY(scratch(nb * l1, &prev));
+    CPSD_TRY(scratch(nb * md * l1, &err));
+    CPSD_TRY(scratch(nb * md * l1, &amp));
+    SolverState *ss;
+    DiisState *ds;
+    CPSD_TRY(arena().alloc(sizeof(SolverState) * nb, (void **)&ss));
+    CPSD_TRY(arena().alloc(sizeof(DiisState) * nb, (void **)&ds));
+    std::vector<SolverState> hss((size_t)nb, SolverState{0, 1, 0, 0, 0.0});
+    std::vector<DiisState> hds((size_t)nb, DiisState{(int)l1, md, 1, 1, 1.0, {}});
+    CPSD_TRY(cuda_check(cudaMemcpyAsync(ss, hss.data(), sizeof(SolverState) * nb, cudaMemcpyHostToDevice, stream()),
+                        "solver state"));
+    CPSD_TRY(cuda_check(cudaMemcpyAsync(ds, hds.data(), sizeof(DiisState) * nb, cudaMemcpyHostToDevice, stream()),
+                        "diis state"));
+    CPSD_TRY(launch_energy(e1, 5, X.eorb, nullptr, den));
+    CPSD_TRY(launch_copy(pr, cc, nb * l1));
+    SolverArgs a;
+    a.len = (int)l1;
+    a.nb = (int)nb;
+    a.cyc = (int)p->diis_cyc;
+    a.tol = p->diis_max_err;
+    a.ss = ss;
+    a.ds = ds;
+    a.db.prev = prev;
+    a.db.err = err;
+    a.db.amp = amp;
+    a.sprev = l1;
+    a.serr = md * l1;
+    a.pr = pr;
+    a.R1 = R1;
+    a.cc = cc;
+    a.S = sg;
+    a.den = den;
+    a.L = L;
+    a.w0 = w0d;
+    int *mb, *mb_dev;
+    CPSD_TRY(mapped_mailbox(&mb, &mb_dev));
+    for (i64 r = 0; r < nb; r++) mb[r] = 1;
+    a.mailbox = mb_dev;
+    static cudaEvent_t ev[4] = {};
+    if (!ev[0])
+        for (auto &e : ev) CPSD_TRY(cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event"));
+    Ten tS = ten(v, o, ZORB, ZORB, 1, 1, symR, sg, nb > 1 ? l1 : 0);
+    Ten tR = ten(v, o, ZORB, ZORB, 1, 1, symR, R1, nb > 1 ? l1 : 0);
+    for (i64 it = 1; it <= p->diis_cyc + 1; it++) {
+        CPSD_TRY(solver_step_launch(a));
+        CPSD_TRY(cuda_check(cudaEventRecord(ev[it % 4], stream()), "event record"));
+        bool any = false;
+        for (i64 r = 0; r < nb; r++) any |= ((volatile int *)mb)[r] != 0;
+        if (!any) break;
+        CPSD_TRY(zero(sg, nb * l1));
+        CPSD_TRY(k_c1_r1iabj(tS, tR, X.iabj, 1.0, nb));
+        if (it >= 3) CPSD_TRY(cuda_check(cudaEventSynchronize(ev[(it - 2) % 4]), "event sync"));
+    }
+    CPSD_TRY(read_back(hss.data(), ss, sizeof(SolverState) * nb));
+    for (const SolverState &h : hss) *sit += h.iter;
+    return CPSD_OK;
+}
+
 static int ee_roots_batch(const Sys &S, const Ints &X, const cpsd_params *p, const double *T2_1,
                           const cpsd_jints *J, i64 symR, i64 nb, const double *w0_host, const double *L,
                           double *w_host, double *R2_1o, double *R1_2o, double *R2_2o, i64 *sit_out) {
@@ -576,33 +665,12 @@ static int ee_roots_batch(const Sys &S, const Ints &X, const cpsd_params *p, con
     CPSD_TRY(launch_copy(r22, cn2, nb * l2));
     CPSD_TRY(launch_scale(r22, nb * l2, -1.0));
     CPSD_TRY(launch_energy(e2, 1, X.eorb, r22, r22, w0d, nb, l2, l2));
-    // solver (solver.f90:4-66): (A - w0) R1 = Ctilde1, orthogonal to L, per root
+    // solver (solver.f90:4-66): (A - w0) R1 = Ctilde1, orthogonal to L, all
+    // roots at once and driven on the device (each root stops on its own
+    // convergence test); the sigma of every step is one batched launch
     i64 sit = 0;
-    for (i64 r = 0; r < nb; r++) {
-        ScratchScope s3;
-        double *cc = cn1 + r * l1, *R1 = r12 + r * l1, *pr;
-        CPSD_TRY(scratch(l1, &pr));
-        CPSD_TRY(launch_scale(cc, l1, -1.0));
-        CPSD_TRY(launch_copy(pr, cc, l1));
-        Diis dd;
-        CPSD_TRY(diis_alloc(&dd, l1, p->diis_dim));
-        Ten tR1 = ten(v, o, ZORB, ZORB, 1, 1, symR, R1), tpr = ten(v, o, ZORB, ZORB, 1, 1, symR, pr);
-        i64 iter = 0;
-        for (;;) {
-            iter++;
-            CPSD_TRY(launch_energy(e1, 3, X.eorb, pr, R1));
-            // orthogonalR2L, dosodiis2_d, orthogonalR2L in one launch
-            CPSD_TRY(diis_step_launch(dd.st, dd.b, (int)iter, R1, L + r * l1));
-            double res;
-            CPSD_TRY(read_back(&res, &dd.st->res, sizeof res));
-            if (iter > 1 && std::fabs(res) < p->diis_max_err) break;
-            if (iter > p->diis_cyc) break;
-            CPSD_TRY(launch_copy(pr, cc, l1));
-            CPSD_TRY(launch_axpy(l1, -w0_host[r], R1, pr));
-            CPSD_TRY(k_c1_r1iabj(tpr, tR1, X.iabj, 1.0));
-        }
-        sit += iter;
-    }
+    CPSD_TRY(launch_scale(cn1, nb * l1, -1.0));
+    CPSD_TRY(solve_r1(S, X, p, symR, nb, l1, e1, cn1, L, w0d, r12, &sit));
     // C^(3) = J^(1) R^(2) + J^(3) R^(0), C1 only (calE_C.f90:37-79)
     CPSD_TRY(zero(c1, nb * l1));
     CPSD_TRY(k_c1_r2abci(C1, R22, X.abci, 1.0, nb));

@@ -61,7 +61,8 @@ __global__ void k_energy(const i64 *__restrict__ blk, int nblocks, i64 n, const 
             double ea = eorb[ia], ei = eorb[ib];
             if (mode == 0) v = ea - ei;
             else if (mode == 3) v = in[e] / (ei - ea);
-            else v = (ea - ei) * in[e];  // mode 4
+            else if (mode == 5) v = ei - ea;  // the divisor of mode 3
+            else v = (ea - ei) * in[e];       // mode 4
         } else {
             double ea = eorb[ia], eb = eorb[ib], ei = eorb[ii], ej = eorb[ij];
             if (mode == 0) v = ea + eb - ei - ej;

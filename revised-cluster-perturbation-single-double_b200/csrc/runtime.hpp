@@ -221,6 +221,7 @@ int plan_energy(const Desc &d, const char *kinds, const EnergyPlan **out);
 // mode 2: out = in / (ei+ej-ea-eb)             (denomT2, denomT.f90:175)
 // mode 3: out = in / (ei-ea)                   (denomT1, denomT.f90:82)
 // mode 4: out = e(a,i) * in                    (calAR vdmul, calAR.f90:29)
+// mode 5: out = ei-ea                          (the mode-3 divisor, 2-index)
 int launch_energy(const EnergyPlan *p, int mode, const double *eorb, const double *in, double *out,
                   const double *w0_dev = nullptr, i64 nb = 1, i64 in_stride = 0, i64 out_stride = 0);
 // y_c += sgn * a_dev[c] * x_c for nb copies

@@ -553,6 +553,55 @@ __global__ void __launch_bounds__(DT) k_diis(DiisState *st, DiisBuffers b, int i
     }
 }
 
+// one step of the device-driven solver for root blockIdx.x (see solvers.cuh)
+__global__ void __launch_bounds__(DT) k_solver_step(SolverArgs a) {
+    __shared__ double sh[DT / 32 + 1];
+    __shared__ int shi[DT / 32 + 1];
+    __shared__ double Bm[DIIS_MAXDIM * DIIS_MAXDIM];
+    __shared__ double coef[DIIS_MAXDIM + 1];
+    __shared__ double aug[(DIIS_MAXDIM + 1) * (DIIS_MAXDIM + 1)], rhs[DIIS_MAXDIM + 1];
+    __shared__ int ipvt[DIIS_MAXDIM + 1];
+    const int r = blockIdx.x, tid = threadIdx.x, len = a.len;
+    SolverState &ss = a.ss[r];
+    if (!ss.active) return;
+    const int iter = ss.iter + 1;
+    double *pr = a.pr + (size_t)r * len, *R1 = a.R1 + (size_t)r * len;
+    const double *cc = a.cc + (size_t)r * len, *S = a.S + (size_t)r * len, *L = a.L + (size_t)r * len;
+    if (iter > 1) {  // pr = cc; pr += (-w0) R1; pr += sigma  (the reference's three updates, in order)
+        const double mw0 = -a.w0[r];
+        for (int k = tid; k < len; k += DT) pr[k] = fma(mw0, R1[k], cc[k]) + S[k];
+        __syncthreads();
+    }
+    for (int k = tid; k < len; k += DT) R1[k] = pr[k] / a.den[k];
+    __syncthreads();
+    DiisState &ds = a.ds[r];
+    DiisBuffers b;
+    b.prev = a.db.prev + (size_t)r * a.sprev;
+    b.err = a.db.err + (size_t)r * a.serr;
+    b.amp = a.db.amp + (size_t)r * a.serr;
+    block_orth(R1, L, len, sh);
+    if (iter == 1) {
+        for (int k = tid; k < len; k += DT) b.prev[k] = R1[k];
+        if (tid == 0) {
+            ds.idimr = 1;
+            ds.ndimr = 1;
+            ds.res = 1.0;
+        }
+    } else {
+        diis_extrapolate(ds, b, R1, sh, shi, Bm, coef, aug, rhs, ipvt);
+    }
+    __syncthreads();
+    block_orth(R1, L, len, sh);
+    if (tid == 0) {
+        const double res = ds.res;
+        ss.iter = iter;
+        ss.res = res;
+        if ((iter > 1 && fabs(res) < a.tol) || iter > a.cyc) ss.active = 0;
+        a.mailbox[r] = ss.active;
+        __threadfence_system();
+    }
+}
+
 __device__ void diis_extrapolate(DiisState &s, const DiisBuffers &b, double *vec, double *sh, int *shi, double *Bm,
                                  double *coef, double *aug, double *rhs, int *ipvt) {
     const int len = s.len, maxdim = s.maxdim, tid = threadIdx.x;
@@ -648,6 +697,12 @@ int diis_step_launch(DiisState *st, const DiisBuffers &b, int iter, double *vec,
     k_diis<<<1, DT, 0, stream()>>>(st, b, iter, vec, L);
     count_launch();
     return cuda_check(cudaGetLastError(), "k_diis");
+}
+int solver_step_launch(const SolverArgs &a) {
+    if (a.nb <= 0) return CPSD_OK;
+    k_solver_step<<<a.nb, DT, 0, stream()>>>(a);
+    count_launch();
+    return cuda_check(cudaGetLastError(), "k_solver_step");
 }
 int orth_launch(double *R, const double *L, i64 n) {
     k_orth<<<1, DT, 0, stream()>>>(R, L, (int)n);

@@ -52,4 +52,29 @@ int diis_step_launch(DiisState *st, const DiisBuffers &b, int iter, double *vec,
 // R -= (<L|R>/||L||) L  (orthogonalR2L, src/EE-CPSd.SF/orthogonalR2L.f90:5-34)
 int orth_launch(double *R, const double *L, i64 n);
 
+// Device-driven solver steps (solver.f90:4-66) for nb independent roots:
+// one CTA per root and step does
+//   pr = cc - w0 R1 + S      (S = the sigma of the previous step's R1; from step 2)
+//   R1 = pr / (ei - ea);  orthogonalR2L; dosodiis2_d; orthogonalR2L
+// and stops the root (active = 0) once |DIIS residual| < tol after step 1 or
+// after step cyc + 1, exactly where the reference's loop exits.  The host
+// keeps launching steps without reading anything back; mailbox (mapped host
+// memory) tells it when every root has stopped.
+struct SolverState {
+    int iter, active, pad0, pad1;
+    double res;
+};
+struct SolverArgs {
+    int len = 0, nb = 0, cyc = 0;
+    double tol = 0;
+    SolverState *ss = nullptr;      // nb
+    DiisState *ds = nullptr;        // nb
+    DiisBuffers db{};               // root r at db.prev + r * sprev, db.err / db.amp + r * serr
+    i64 sprev = 0, serr = 0;
+    double *pr = nullptr, *R1 = nullptr;  // nb x len
+    const double *cc = nullptr, *S = nullptr, *den = nullptr, *L = nullptr, *w0 = nullptr;
+    int *mailbox = nullptr;         // nb (device view of mapped host memory)
+};
+int solver_step_launch(const SolverArgs &a);
+
 }  // namespace cpsd
