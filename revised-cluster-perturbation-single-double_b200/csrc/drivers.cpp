@@ -310,23 +310,6 @@ int davidson(const Sys &S, const Ints &I, const cpsd_params *p, i64 sym, i64 nro
     return CPSD_OK;
 }
 
-// ----------------------------------------------------------------- DIIS
-struct Diis {
-    DiisState *st;
-    DiisBuffers b;
-    i64 len;
-};
-int diis_alloc(Diis *d, i64 len, i64 maxdim) {
-    if (maxdim > DIIS_MAXDIM) return set_error(CPSD_EARG, "diis_dim above 16");
-    d->len = len;
-    CPSD_TRY(arena().alloc(sizeof(DiisState), (void **)&d->st));
-    CPSD_TRY(scratch(len, &d->b.prev));
-    CPSD_TRY(scratch(len * maxdim, &d->b.err));
-    CPSD_TRY(scratch(len * maxdim, &d->b.amp));
-    DiisState h{(int)len, (int)maxdim, 1, 1, 1.0};
-    return cuda_check(cudaMemcpyAsync(d->st, &h, sizeof h, cudaMemcpyHostToDevice, stream()), "diis state");
-}
-
 }  // namespace
 }  // namespace cpsd
 
@@ -389,6 +372,10 @@ int cpsd_cis_run(const cpsd_system *s, const cpsd_integrals *I, const cpsd_param
     return cuda_check(cudaStreamSynchronize(stream()), "cis sync");
 }
 
+static int solve_r1(const Sys &S, const Ints &X, const cpsd_params *p, i64 symR, i64 nb, i64 l1,
+                    const EnergyPlan *e1, const double *cc, const double *L, const double *w0d, double *R1,
+                    i64 *sit);
+
 int cpsd_ground(const cpsd_system *s, const cpsd_integrals *I, const cpsd_params *p, double *T2_1, double *T1_2,
                 double *T2_2, double *E2_host, double *E3_host, int64_t *diis_iters) {
     Sys S;
@@ -398,10 +385,9 @@ int cpsd_ground(const cpsd_system *s, const cpsd_integrals *I, const cpsd_params
     const i64 *o = S.popo, *v = S.popv;
     ScratchScope sc;
     i64 l1 = irpdso(1, v, o, 1), l2 = idsymsoc(1, v, v, 0, o, o, 0);
-    double *c1, *c2, *r1, *dE;
+    double *c1, *c2, *dE;
     CPSD_TRY(scratch(l1, &c1));
     CPSD_TRY(scratch(l2, &c2));
-    CPSD_TRY(scratch(l1, &r1));
     CPSD_TRY(scratch(2, &dE));
     Desc d2 = make_desc(v, v, o, o, 0, 0, 1), d1 = make_desc(v, o, ZORB, ZORB, 1, 1, 1);
     const EnergyPlan *e2, *e1;
@@ -411,9 +397,8 @@ int cpsd_ground(const cpsd_system *s, const cpsd_integrals *I, const cpsd_params
     CPSD_TRY(launch_energy(e2, 2, X.eorb, I->abij, T2_1));
     CPSD_TRY(launch_dot(T2_1, I->abij, l2, dE, true));
     // run2 (src/CPSd.SF/run2.f90:8-95)
-    Ten t2 = ten(v, v, o, o, 0, 0, 1, T2_1), t1 = ten(v, o, ZORB, ZORB, 1, 1, 1, T1_2);
+    Ten t2 = ten(v, v, o, o, 0, 0, 1, T2_1);
     Ten C1 = ten(v, o, ZORB, ZORB, 1, 1, 1, c1), C2 = ten(v, v, o, o, 0, 0, 1, c2);
-    Ten R1 = ten(v, o, ZORB, ZORB, 1, 1, 1, r1);
     CPSD_TRY(zero(c1, l1));
     CPSD_TRY(zero(c2, l2));
     CPSD_TRY(k_c1_r2abci(C1, t2, X.abci, 1.0));
@@ -422,21 +407,10 @@ int cpsd_ground(const cpsd_system *s, const cpsd_integrals *I, const cpsd_params
     CPSD_TRY(k_c2_r2Wmnij(C2, t2, X.ijkl, 1.0));
     CPSD_TRY(k_c2_r2abcd(C2, t2, X.abcd, 1.0));
     CPSD_TRY(launch_energy(e2, 2, X.eorb, c2, T2_2));
-    CPSD_TRY(launch_copy(r1, c1, l1));
-    Diis dd;
-    CPSD_TRY(diis_alloc(&dd, l1, p->diis_dim));
+    // the T1^(2) DIIS loop (run2.f90): T1 = (C1 + V T1) / (ei - ea), driven on
+    // the device like the EE solver (no orthogonalisation, no w0 term)
     i64 iter = 0;
-    for (;;) {
-        iter++;
-        CPSD_TRY(launch_energy(e1, 3, X.eorb, r1, T1_2));
-        CPSD_TRY(diis_step_launch(dd.st, dd.b, (int)iter, T1_2));
-        double res;
-        CPSD_TRY(read_back(&res, &dd.st->res, sizeof res));
-        if (iter > 1 && std::fabs(res) < p->diis_max_err) break;
-        if (iter > p->diis_cyc) break;
-        CPSD_TRY(launch_copy(r1, c1, l1));
-        CPSD_TRY(k_c1_r1iabj(R1, t1, X.iabj, 1.0));
-    }
+    CPSD_TRY(solve_r1(S, X, p, 1, 1, l1, e1, c1, nullptr, nullptr, T1_2, &iter));
     if (diis_iters) *diis_iters = iter;
     CPSD_TRY(launch_dot(T2_2, I->abij, l2, dE + 1, true));
     double h[2];

@@ -525,34 +525,6 @@ __device__ void block_orth(double *R, const double *L, int n, double *sh) {
 __device__ void diis_extrapolate(DiisState &s, const DiisBuffers &b, double *vec, double *sh, int *shi, double *Bm,
                                  double *coef, double *aug, double *rhs, int *ipvt);
 
-// One DIIS step (dosodiis2_d) on vec; with L, vec is first and last made
-// orthogonal to L (the solver's orthogonalR2L calls around it)
-__global__ void __launch_bounds__(DT) k_diis(DiisState *st, DiisBuffers b, int iter, double *vec, const double *L) {
-    __shared__ double sh[DT / 32 + 1];
-    __shared__ int shi[DT / 32 + 1];
-    __shared__ double Bm[DIIS_MAXDIM * DIIS_MAXDIM];
-    __shared__ double coef[DIIS_MAXDIM + 1];
-    __shared__ double aug[(DIIS_MAXDIM + 1) * (DIIS_MAXDIM + 1)], rhs[DIIS_MAXDIM + 1];
-    __shared__ int ipvt[DIIS_MAXDIM + 1];
-    DiisState &s = *st;
-    const int len = s.len, tid = threadIdx.x;
-    if (L) block_orth(vec, L, len, sh);
-    if (iter == 1) {
-        for (int k = tid; k < len; k += DT) b.prev[k] = vec[k];
-        if (tid == 0) {
-            s.idimr = 1;
-            s.ndimr = 1;
-            s.res = 1.0;
-        }
-    } else {
-        diis_extrapolate(s, b, vec, sh, shi, Bm, coef, aug, rhs, ipvt);
-    }
-    if (L) {
-        __syncthreads();
-        block_orth(vec, L, len, sh);
-    }
-}
-
 // one step of the device-driven solver for root blockIdx.x (see solvers.cuh)
 __global__ void __launch_bounds__(DT) k_solver_step(SolverArgs a) {
     __shared__ double sh[DT / 32 + 1];
@@ -566,10 +538,15 @@ __global__ void __launch_bounds__(DT) k_solver_step(SolverArgs a) {
     if (!ss.active) return;
     const int iter = ss.iter + 1;
     double *pr = a.pr + (size_t)r * len, *R1 = a.R1 + (size_t)r * len;
-    const double *cc = a.cc + (size_t)r * len, *S = a.S + (size_t)r * len, *L = a.L + (size_t)r * len;
-    if (iter > 1) {  // pr = cc; pr += (-w0) R1; pr += sigma  (the reference's three updates, in order)
-        const double mw0 = -a.w0[r];
-        for (int k = tid; k < len; k += DT) pr[k] = fma(mw0, R1[k], cc[k]) + S[k];
+    const double *cc = a.cc + (size_t)r * len, *S = a.S + (size_t)r * len;
+    const double *L = a.L ? a.L + (size_t)r * len : nullptr;
+    if (iter > 1) {  // pr = cc; pr += (-w0) R1; pr += sigma  (the reference's updates, in order)
+        if (a.w0) {
+            const double mw0 = -a.w0[r];
+            for (int k = tid; k < len; k += DT) pr[k] = fma(mw0, R1[k], cc[k]) + S[k];
+        } else {
+            for (int k = tid; k < len; k += DT) pr[k] = cc[k] + S[k];
+        }
         __syncthreads();
     }
     for (int k = tid; k < len; k += DT) R1[k] = pr[k] / a.den[k];
@@ -579,7 +556,7 @@ __global__ void __launch_bounds__(DT) k_solver_step(SolverArgs a) {
     b.prev = a.db.prev + (size_t)r * a.sprev;
     b.err = a.db.err + (size_t)r * a.serr;
     b.amp = a.db.amp + (size_t)r * a.serr;
-    block_orth(R1, L, len, sh);
+    if (L) block_orth(R1, L, len, sh);
     if (iter == 1) {
         for (int k = tid; k < len; k += DT) b.prev[k] = R1[k];
         if (tid == 0) {
@@ -591,7 +568,7 @@ __global__ void __launch_bounds__(DT) k_solver_step(SolverArgs a) {
         diis_extrapolate(ds, b, R1, sh, shi, Bm, coef, aug, rhs, ipvt);
     }
     __syncthreads();
-    block_orth(R1, L, len, sh);
+    if (L) block_orth(R1, L, len, sh);
     if (tid == 0) {
         const double res = ds.res;
         ss.iter = iter;
@@ -663,13 +640,6 @@ __device__ void diis_extrapolate(DiisState &s, const DiisBuffers &b, double *vec
     }
 }
 
-__global__ void __launch_bounds__(DT) k_orth(double *R, const double *L, int n) {
-    __shared__ double sh[DT / 32 + 1];
-    double nrm = sqrt(block_dot(L, L, n, sh));
-    double dot = block_dot(L, R, n, sh);
-    double f = -dot / nrm;
-    for (int k = threadIdx.x; k < n; k += DT) R[k] += f * L[k];
-}
 }  // namespace
 
 int dav_init_launch(DavState *st, const DavBuffers &b) {
@@ -693,21 +663,11 @@ int dav_final_launch(DavState *st, const DavBuffers &b) {
     count_launch();
     return cuda_check(cudaGetLastError(), "k_dav_final");
 }
-int diis_step_launch(DiisState *st, const DiisBuffers &b, int iter, double *vec, const double *L) {
-    k_diis<<<1, DT, 0, stream()>>>(st, b, iter, vec, L);
-    count_launch();
-    return cuda_check(cudaGetLastError(), "k_diis");
-}
 int solver_step_launch(const SolverArgs &a) {
     if (a.nb <= 0) return CPSD_OK;
     k_solver_step<<<a.nb, DT, 0, stream()>>>(a);
     count_launch();
     return cuda_check(cudaGetLastError(), "k_solver_step");
-}
-int orth_launch(double *R, const double *L, i64 n) {
-    k_orth<<<1, DT, 0, stream()>>>(R, L, (int)n);
-    count_launch();
-    return cuda_check(cudaGetLastError(), "k_orth");
 }
 
 }  // namespace cpsd

@@ -46,16 +46,13 @@ struct DiisState {
 struct DiisBuffers {
     double *prev, *err, *amp;  // len, maxdim*len, maxdim*len
 };
-// one DIIS step on vec; with L (not null) vec is made orthogonal to L before
-// and after it (orthogonalR2L around dosodiis2_d in the reference's solver)
-int diis_step_launch(DiisState *st, const DiisBuffers &b, int iter, double *vec, const double *L = nullptr);
-// R -= (<L|R>/||L||) L  (orthogonalR2L, src/EE-CPSd.SF/orthogonalR2L.f90:5-34)
-int orth_launch(double *R, const double *L, i64 n);
-
-// Device-driven solver steps (solver.f90:4-66) for nb independent roots:
-// one CTA per root and step does
+// Device-driven solver steps for nb independent roots: the EE solver
+// (solver.f90:4-66) and, without L and w0, the ground T1^(2) DIIS loop
+// (run2.f90).  One CTA per root and step does
 //   pr = cc - w0 R1 + S      (S = the sigma of the previous step's R1; from step 2)
-//   R1 = pr / (ei - ea);  orthogonalR2L; dosodiis2_d; orthogonalR2L
+//   R1 = pr / (ei - ea);  orthogonalR2L; dosodiis2_d (LINPACK solve of the
+//   bordered -1e-4 system, dodiis.f / minv.f); orthogonalR2L
+// (orthogonalR2L: R -= (<L|R>/||L||) L, orthogonalR2L.f90:5-34)
 // and stops the root (active = 0) once |DIIS residual| < tol after step 1 or
 // after step cyc + 1, exactly where the reference's loop exits.  The host
 // keeps launching steps without reading anything back; mailbox (mapped host
