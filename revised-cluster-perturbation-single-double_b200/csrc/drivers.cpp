@@ -90,6 +90,38 @@ int read_back(void *host, const void *dev, size_t bytes) {
     return cuda_check(cudaStreamSynchronize(stream()), "sync");
 }
 
+// mapped host memory through which device-driven loops report progress
+int mapped_mailbox(int **host, int **dev) {
+    static int *h = nullptr, *d = nullptr;
+    if (!h) {
+        CPSD_TRY(cuda_check(cudaHostAlloc((void **)&h, 4096, cudaHostAllocMapped), "cudaHostAlloc(mapped)"));
+        CPSD_TRY(cuda_check(cudaHostGetDevicePointer((void **)&d, h, 0), "mapped pointer"));
+    }
+    *host = h;
+    *dev = d;
+    return CPSD_OK;
+}
+
+// Device-driven loops stay at most two steps ahead of the device: before
+// queueing step it the host waits for the end of step it - 2.
+struct StepThrottle {
+    cudaEvent_t ev[4] = {};
+    int init() {
+        for (auto &e : ev)
+            if (!e) CPSD_TRY(cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event"));
+        return CPSD_OK;
+    }
+    int mark(i64 it) { return cuda_check(cudaEventRecord(ev[it % 4], stream()), "event record"); }
+    int wait(i64 it) {
+        if (it < 3) return CPSD_OK;
+        return cuda_check(cudaEventSynchronize(ev[(it - 2) % 4]), "event sync");
+    }
+};
+StepThrottle &throttle() {
+    static StepThrottle t;
+    return t;
+}
+
 int zero(double *p, i64 n) { return launch_scale(p, n, 0.0); }
 
 // AR = e(a,i) R + V(fn,ai) R(fn): calAR (src/EE-CIS.SF/calAR.f90:6-34), batched
@@ -288,18 +320,28 @@ int davidson(const Sys &S, const Ints &I, const cpsd_params *p, i64 sym, i64 nro
                         "guess copy"));
     CPSD_TRY(cis_sigma(S, I, sym, b.B[0], n, b.AB[0], n, nroot));
     CPSD_TRY(dav_init_launch(st, b));
+    // device-driven iterations: every step stages its new vectors (zero
+    // padded to nroot), one sigma launch of fixed size, the Ritz update puts
+    // the sigma vectors in place; the host only watches the mailbox
+    CPSD_TRY(scratch(nroot * n, &b.W));
+    CPSD_TRY(scratch(nroot * n, &b.AW));
+    int *mb, *mb_dev;
+    CPSD_TRY(mapped_mailbox(&mb, &mb_dev));
+    mb[0] = 1;
+    b.mailbox = mb_dev;
+    StepThrottle &th = throttle();
+    CPSD_TRY(th.init());
+    for (i64 it = 1; it <= p->davidson_cyc + 2; it++) {
+        CPSD_TRY(dav_step_launch(st, b));
+        CPSD_TRY(th.mark(it));
+        if (((volatile int *)mb)[0] == 0) break;
+        CPSD_TRY(cis_sigma(S, I, sym, b.W, n, b.AW, n, nroot));
+        CPSD_TRY(dav_abar_launch(st, b));
+        CPSD_TRY(th.wait(it));
+    }
     int *hdr = (int *)mailbox();
     const size_t hbytes = offsetof(DavState, warn_imag);
-    for (;;) {
-        CPSD_TRY(dav_step_launch(st, b));
-        CPSD_TRY(read_back(hdr, st, hbytes));
-        const DavState *h = (const DavState *)hdr;
-        if (h->done) break;
-        if (h->nNew > 0)
-            CPSD_TRY(cis_sigma(S, I, sym, b.B[h->cur] + (i64)h->newpos * n, n, b.AB[h->cur] + (i64)h->newpos * n, n,
-                               h->nNew));
-        CPSD_TRY(dav_abar_launch(st, b));
-    }
+    CPSD_TRY(read_back(hdr, st, hbytes));
     if (iters) *iters = ((const DavState *)hdr)->iterations;
     // eigen test of the converged roots (mod_davidson.f90:525-542)
     CPSD_TRY(cis_sigma(S, I, sym, fileEV + 1, n + 1, b.AB[0], n, nroot));
@@ -452,18 +494,6 @@ int cpsd_calJ(const cpsd_system *s, const cpsd_integrals *I, const double *T2_1,
 }
 
 // EE-CPS(D-3) for nb roots of irrep symR sharing every contraction launch
-// mapped host memory through which device-driven loops report progress
-static int mapped_mailbox(int **host, int **dev) {
-    static int *h = nullptr, *d = nullptr;
-    if (!h) {
-        CPSD_TRY(cuda_check(cudaHostAlloc((void **)&h, 4096, cudaHostAllocMapped), "cudaHostAlloc(mapped)"));
-        CPSD_TRY(cuda_check(cudaHostGetDevicePointer((void **)&d, h, 0), "mapped pointer"));
-    }
-    *host = h;
-    *dev = d;
-    return CPSD_OK;
-}
-
 // The solver of solver.f90:4-66 for nb roots of irrep symR at once: cc holds
 // -Ctilde1 (nb x l1), L the CIS vectors, w0d the CIS energies (device);
 // R1 receives the solutions, *sit the summed step counts.  Each step is one
@@ -521,20 +551,19 @@ static int solve_r1(const Sys &S, const Ints &X, const cpsd_params *p, i64 symR,
     CPSD_TRY(mapped_mailbox(&mb, &mb_dev));
     for (i64 r = 0; r < nb; r++) mb[r] = 1;
     a.mailbox = mb_dev;
-    static cudaEvent_t ev[4] = {};
-    if (!ev[0])
-        for (auto &e : ev) CPSD_TRY(cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event"));
+    StepThrottle &th = throttle();
+    CPSD_TRY(th.init());
     Ten tS = ten(v, o, ZORB, ZORB, 1, 1, symR, sg, nb > 1 ? l1 : 0);
     Ten tR = ten(v, o, ZORB, ZORB, 1, 1, symR, R1, nb > 1 ? l1 : 0);
     for (i64 it = 1; it <= p->diis_cyc + 1; it++) {
         CPSD_TRY(solver_step_launch(a));
-        CPSD_TRY(cuda_check(cudaEventRecord(ev[it % 4], stream()), "event record"));
+        CPSD_TRY(th.mark(it));
         bool any = false;
         for (i64 r = 0; r < nb; r++) any |= ((volatile int *)mb)[r] != 0;
         if (!any) break;
         CPSD_TRY(zero(sg, nb * l1));
         CPSD_TRY(k_c1_r1iabj(tS, tR, X.iabj, 1.0, nb));
-        if (it >= 3) CPSD_TRY(cuda_check(cudaEventSynchronize(ev[(it - 2) % 4]), "event sync"));
+        CPSD_TRY(th.wait(it));
     }
     CPSD_TRY(read_back(hss.data(), ss, sizeof(SolverState) * nb));
     for (const SolverState &h : hss) *sit += h.iter;

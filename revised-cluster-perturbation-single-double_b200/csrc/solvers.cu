@@ -220,7 +220,13 @@ __global__ void __launch_bounds__(DT) k_dav_step(DavState *st, DavBuffers b) {
     const int D = s.D, n = s.dimA, nroot = s.nroot;
     if (s.done) return;
     if (s.iterations > s.maxcyc) {
-        if (tid == 0) s.done = 1;
+        if (tid == 0) {
+            s.done = 1;
+            if (b.mailbox) {
+                b.mailbox[0] = 0;
+                __threadfence_system();
+            }
+        }
         return;
     }
     int dimIter = s.dimIter, cur = s.cur, dimFree = s.dimFree;
@@ -402,14 +408,31 @@ __global__ void __launch_bounds__(DT) k_dav_step(DavState *st, DavBuffers b) {
                 }
             }
         }
+        if (b.mailbox) {
+            b.mailbox[0] = s.done ? 0 : 1;
+            __threadfence_system();
+        }
     }
+    // staged copies of the new basis vectors (zero beyond nNew) for a sigma
+    // launch whose size does not depend on nNew
+    if (b.W)
+        for (int q = 0; q < nroot; q++)
+            for (int k = tid; k < n; k += DT)
+                b.W[(size_t)q * n + k] = q < nNew ? b.B[cur][(size_t)(dimIter + q) * n + k] : 0.0;
 }
 
-// Ritz-matrix update with the new vectors (mod_davidson.f90:460-496)
+// Ritz-matrix update with the new vectors (mod_davidson.f90:460-496); with
+// staged sigma vectors, AW[0..nNew) are first put in place in AB
 __global__ void __launch_bounds__(DT) k_dav_abar(DavState *st, DavBuffers b) {
     DavState &s = *st;
     if (s.done) return;
     const int n = s.dimA, D = s.D, dimIter = s.dimIter, nNew = s.nNew, cur = s.cur;
+    if (b.AW) {
+        for (int q = 0; q < nNew; q++)
+            for (int k = threadIdx.x; k < n; k += DT)
+                b.AB[cur][(size_t)(dimIter + q) * n + k] = b.AW[(size_t)q * n + k];
+        __syncthreads();
+    }
     const double *B = b.B[cur], *AB = b.AB[cur];
     // new rows (i >= dimIter, j < dimIter) then new columns (j >= dimIter)
     const int nrow = nNew * dimIter, tot = nrow + nNew * (dimIter + nNew);

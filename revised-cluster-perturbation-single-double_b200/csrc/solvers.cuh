@@ -30,6 +30,11 @@ struct DavBuffers {
     const double *diag;    // OED1 of the irrep
     double *fileEV;        // nroot records (w, R)
     double *w0, *w1;       // work vectors
+    // device-driven loop: the step stages its new vectors in W (nroot x dimA,
+    // zero beyond nNew), the sigma of W goes to AW and the Ritz update moves
+    // it in place; mailbox[0] (mapped host memory) = 1 while iterating
+    double *W = nullptr, *AW = nullptr;
+    int *mailbox = nullptr;
 };
 
 int dav_init_launch(DavState *st, const DavBuffers &b);      // Abar of the guesses
