@@ -318,7 +318,9 @@ def run_ours(args, rank, world, local_rank):
               "share_of_step": d_ms / step_ms, "launches_per_step": int(sel.sum())}
     shares = {lab: round(float(rms[m].sum()) / step_ms, 4) for lab, m in
               (("digit_gemm", rkind == 12), ("digit_slicing", (rkind == 10) | (rkind == 11)),
-               ("fp64_tiles", rkind < 10), ("narrow", rkind >= 20))}
+               ("fp64_tiles", rkind < 10), ("narrow", (rkind >= 20) & (rkind < 30)),
+               ("davidson", (rkind == 30) | (rkind == 31)), ("diis_solver", rkind == 32),
+               ("pair_transforms", rkind == 40))}
 
     # end to end through the public API with host buffers: H2D of every
     # integral tensor from pinned memory, the pipeline, results back on the host

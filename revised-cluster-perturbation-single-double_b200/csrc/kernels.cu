@@ -19,8 +19,12 @@ __global__ void k_pairmap(const PMBlockDev *__restrict__ blocks, int nblocks, i6
         i64 cpy = g / total, e = g - cpy * total;
         const double *in = in0 + cpy * sin;
         double *out = out0 + cpy * sout;
-        int b = 0;
-        while (b + 1 < nblocks && blocks[b + 1].start <= e) b++;
+        int b = 0, hi = nblocks - 1;  // last block starting at or before e
+        while (b < hi) {
+            const int mid = (b + hi + 1) >> 1;
+            if (blocks[mid].start <= e) b = mid;
+            else hi = mid - 1;
+        }
         const PMBlockDev &B = blocks[b];
         i64 loc = e - B.start;
         i64 r = loc / B.nlo, l = loc - r * B.nlo;
@@ -49,8 +53,12 @@ __global__ void k_energy(const i64 *__restrict__ blk, int nblocks, i64 n, const 
         const double *in = in0 ? in0 + cpy * sin : nullptr;
         double *out = out0 + cpy * sout;
         double w0 = w0v ? w0v[cpy] : 0.0;
-        int b = 0;
-        while (b + 1 < nblocks && blk[5 * (b + 1)] <= e) b++;
+        int b = 0, hi = nblocks - 1;  // last block starting at or before e
+        while (b < hi) {
+            const int mid = (b + hi + 1) >> 1;
+            if (blk[5 * mid] <= e) b = mid;
+            else hi = mid - 1;
+        }
         const i64 *B = blk + 5 * b;
         i64 loc = e - B[0];
         i64 r = loc / B[1], l = loc - r * B[1];
@@ -135,11 +143,14 @@ int launch_pairmap(const PairMapPlan *p, const double *in, double *out, double a
                    i64 in_stride, i64 out_stride) {
     if (p->total == 0 || nb <= 0) return CPSD_OK;
     CPSD_TRY(const_cast<PairMapPlan *>(p)->upload());
+    cudaEvent_t end;
+    CPSD_TRY(timing_begin(0.0, p->total, nb, p->lterms * p->rterms, 40, &end));
     k_pairmap<<<grid_for(p->total * nb), 256, 0, stream()>>>(p->d_blocks, p->nblocks, p->total, p->d_idx, p->d_sgn,
                                                              p->lterms, p->rterms, in, out, alpha, beta, nb,
                                                              in_stride, out_stride);
     count_launch();
-    return cuda_check(cudaGetLastError(), "k_pairmap");
+    CPSD_TRY(cuda_check(cudaGetLastError(), "k_pairmap"));
+    return timing_end(end);
 }
 
 int launch_scale(double *x, i64 n, double beta) {

@@ -671,14 +671,20 @@ int dav_init_launch(DavState *st, const DavBuffers &b) {
     return cuda_check(cudaGetLastError(), "k_dav_init");
 }
 int dav_step_launch(DavState *st, const DavBuffers &b) {
+    cudaEvent_t end;
+    CPSD_TRY(timing_begin(0.0, 0, 0, 0, 30, &end));
     k_dav_step<<<1, DT, 0, stream()>>>(st, b);
     count_launch();
-    return cuda_check(cudaGetLastError(), "k_dav_step");
+    CPSD_TRY(cuda_check(cudaGetLastError(), "k_dav_step"));
+    return timing_end(end);
 }
 int dav_abar_launch(DavState *st, const DavBuffers &b) {
+    cudaEvent_t end;
+    CPSD_TRY(timing_begin(0.0, 0, 0, 0, 31, &end));
     k_dav_abar<<<1, DT, 0, stream()>>>(st, b);
     count_launch();
-    return cuda_check(cudaGetLastError(), "k_dav_abar");
+    CPSD_TRY(cuda_check(cudaGetLastError(), "k_dav_abar"));
+    return timing_end(end);
 }
 int dav_final_launch(DavState *st, const DavBuffers &b) {
     // AR of the final roots was written to b.AB[0] by the caller
@@ -688,9 +694,12 @@ int dav_final_launch(DavState *st, const DavBuffers &b) {
 }
 int solver_step_launch(const SolverArgs &a) {
     if (a.nb <= 0) return CPSD_OK;
+    cudaEvent_t end;
+    CPSD_TRY(timing_begin(0.0, a.nb, 0, 0, 32, &end));
     k_solver_step<<<a.nb, DT, 0, stream()>>>(a);
     count_launch();
-    return cuda_check(cudaGetLastError(), "k_solver_step");
+    CPSD_TRY(cuda_check(cudaGetLastError(), "k_solver_step"));
+    return timing_end(end);
 }
 
 }  // namespace cpsd
