@@ -325,6 +325,34 @@ int cpsd_eecpsd_roots(const cpsd_system *s, const cpsd_integrals *I, const cpsd_
 int cpsd_pipeline(const cpsd_system *s, const cpsd_integrals *I, const cpsd_params *p,
                   double *omega_cis, double *w2, double *w3, int64_t *nroots);
 
+/* -------------------------------------------- SF-CIS(D) energy gradient
+ * No counterpart in the reference (it has no derivative code).
+ *
+ * cpsd_cisd_energies: the SF-CIS roots of irrep symR (Davidson as in
+ * cpsd_cis_run, roots requested only in symR) and their second-order
+ * corrections w^(2) (src/EE-CPSd.SF/run_order.f90 order 2, the same terms
+ * as cpsd_eecpsd_roots).  w0_host[k], w2_host[k] per root; the unit CIS
+ * vectors go to L_dev (nroot x lenR1, device).  ijkl and abcd are not read.
+ *
+ * cpsd_cisd_gradient: ADDS to G the gradient of
+ *     sum_k g0_host[k] w0_k + g2_host[k] w2_k
+ * with respect to the DPD integral tensors (same layouts as cpsd_integrals)
+ * and Eorb, at the roots w0_host / L_dev of cpsd_cisd_energies.  The doubles
+ * amplitudes are recomputed; the CIS vector response is one Z-vector solve
+ * by the solver of solver.f90 (p->diis_dim / diis_cyc / diis_max_err; its
+ * tolerance bounds the gradient's accuracy).  ijkl and abcd do not enter
+ * w0 / w^(2): G->ijkl and G->abcd are not written and may be NULL.
+ * Contractions run in FP64 whatever cpsd_set_mixed selected. */
+typedef struct {
+    double *ijkl, *ijka, *abij, *iabj, *abci, *abcd;
+    double *eorb;
+} cpsd_integral_grads;
+int cpsd_cisd_energies(const cpsd_system *s, const cpsd_integrals *I, const cpsd_params *p,
+                       int64_t symR, int64_t nroot, double *w0_host, double *w2_host, double *L_dev);
+int cpsd_cisd_gradient(const cpsd_system *s, const cpsd_integrals *I, const cpsd_params *p,
+                       int64_t symR, int64_t nroot, const double *w0_host, const double *L_dev,
+                       const double *g0_host, const double *g2_host, cpsd_integral_grads *G);
+
 #ifdef __cplusplus
 }
 #endif

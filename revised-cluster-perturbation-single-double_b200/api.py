@@ -267,3 +267,45 @@ def pipeline(s, sysc, ints, par):
                               om.ctypes.data_as(ctypes.c_void_p), w2.ctypes.data_as(ctypes.c_void_p),
                               w3.ctypes.data_as(ctypes.c_void_p), ctypes.byref(nr)), "cpsd_pipeline")
     return om[:nr.value], w2[:nr.value], w3[:nr.value]
+
+
+class IntegralGrads(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_void_p) for k in ("ijkl", "ijka", "abij", "iabj", "abci", "abcd", "eorb")]
+
+
+def integrals_struct(t):
+    """Integrals struct from a dict of float64 CUDA tensors (missing keys: NULL)."""
+    st = Integrals()
+    for k in ("ijkl", "ijka", "abij", "iabj", "abci", "abcd", "eorb"):
+        v = t.get(k)
+        p = dptr(v)
+        setattr(st, k, p.value if p is not None else None)
+    return st
+
+
+def cisd_energies(s, sysc, ints_struct, par, symR, nroot):
+    """SF-CIS roots of irrep symR and their w^(2): (w0, w2, L) with L the
+    unit CIS vectors (nroot x lenR1, CUDA)."""
+    import torch
+    l1 = s.r1_len(symR)
+    L = torch.zeros(nroot * l1, dtype=torch.float64, device="cuda")
+    w0, w2 = np.zeros(nroot), np.zeros(nroot)
+    check(lib().cpsd_cisd_energies(ctypes.byref(sysc), ctypes.byref(ints_struct), ctypes.byref(par), I64(symR),
+                                   I64(nroot), w0.ctypes.data_as(ctypes.c_void_p),
+                                   w2.ctypes.data_as(ctypes.c_void_p), dptr(L)), "cpsd_cisd_energies")
+    return w0, w2, L
+
+
+def cisd_gradient(sysc, ints_struct, par, symR, w0, L, g0, g2, grads):
+    """Adds d(sum g0 w0 + g2 w2) to grads (dict of CUDA tensors: ijka, abij,
+    iabj, abci, eorb)."""
+    w0 = np.ascontiguousarray(w0, dtype=np.float64)
+    g0 = np.ascontiguousarray(g0, dtype=np.float64)
+    g2 = np.ascontiguousarray(g2, dtype=np.float64)
+    G = IntegralGrads()
+    for k in ("ijka", "abij", "iabj", "abci", "eorb"):
+        setattr(G, k, dptr(grads[k]).value)
+    check(lib().cpsd_cisd_gradient(ctypes.byref(sysc), ctypes.byref(ints_struct), ctypes.byref(par), I64(symR),
+                                   I64(len(w0)), w0.ctypes.data_as(ctypes.c_void_p), dptr(L),
+                                   g0.ctypes.data_as(ctypes.c_void_p), g2.ctypes.data_as(ctypes.c_void_p),
+                                   ctypes.byref(G)), "cpsd_cisd_gradient")

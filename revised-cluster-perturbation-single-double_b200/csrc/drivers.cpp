@@ -13,17 +13,10 @@
 #include <cstring>
 #include <vector>
 
-#include "ops.hpp"
+#include "drivers.hpp"
 #include "solvers.cuh"
 
 namespace cpsd {
-
-namespace {
-
-struct Sys {
-    i64 nirrep, symry;
-    i64 popa[8], popb[8], vrta[8], vrtb[8], popo[8], popv[8];
-};
 
 int make_sys(const cpsd_system *s, Sys *S) {
     if (!s) return set_error(CPSD_EARG, "null system");
@@ -52,10 +45,6 @@ int make_sys(const cpsd_system *s, Sys *S) {
     return CPSD_OK;
 }
 
-struct Ints {
-    Ten ijkl, ijka, abij, iabj, abci, abcd;
-    const double *eorb;
-};
 Ints make_ints(const Sys &S, const cpsd_integrals *I) {
     const i64 *o = S.popo, *v = S.popv;
     Ints x;
@@ -69,16 +58,6 @@ Ints make_ints(const Sys &S, const cpsd_integrals *I) {
     return x;
 }
 
-// a program does not write its integrals: expanded copies of them are kept
-// for the whole run (ConstOperands)
-struct IntegralScope {
-    const double *a[6];
-    ConstOperands scope;
-    explicit IntegralScope(const cpsd_integrals *I)
-        : a{I->ijkl, I->ijka, I->abij, I->iabj, I->abci, I->abcd}, scope(a, 6) {}
-};
-
-// pinned host mailbox for the few scalars the host control flow needs
 double *mailbox() {
     static double *p = nullptr;
     if (!p) cudaMallocHost(&p, 4096);
@@ -89,6 +68,8 @@ int read_back(void *host, const void *dev, size_t bytes) {
     CPSD_TRY(cuda_check(cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, stream()), "read back"));
     return cuda_check(cudaStreamSynchronize(stream()), "sync");
 }
+
+namespace {
 
 // mapped host memory through which device-driven loops report progress
 int mapped_mailbox(int **host, int **dev) {
@@ -414,10 +395,6 @@ int cpsd_cis_run(const cpsd_system *s, const cpsd_integrals *I, const cpsd_param
     return cuda_check(cudaStreamSynchronize(stream()), "cis sync");
 }
 
-static int solve_r1(const Sys &S, const Ints &X, const cpsd_params *p, i64 symR, i64 nb, i64 l1,
-                    const EnergyPlan *e1, const double *cc, const double *L, const double *w0d, double *R1,
-                    i64 *sit);
-
 int cpsd_ground(const cpsd_system *s, const cpsd_integrals *I, const cpsd_params *p, double *T2_1, double *T1_2,
                 double *T2_2, double *E2_host, double *E3_host, int64_t *diis_iters) {
     Sys S;
@@ -493,7 +470,10 @@ int cpsd_calJ(const cpsd_system *s, const cpsd_integrals *I, const double *T2_1,
     return cuda_check(cudaGetLastError(), "calJ");
 }
 
-// EE-CPS(D-3) for nb roots of irrep symR sharing every contraction launch
+}  // extern "C"
+
+namespace cpsd {
+
 // The solver of solver.f90:4-66 for nb roots of irrep symR at once: cc holds
 // -Ctilde1 (nb x l1), L the CIS vectors, w0d the CIS energies (device);
 // R1 receives the solutions, *sit the summed step counts.  Each step is one
@@ -501,9 +481,8 @@ int cpsd_calJ(const cpsd_system *s, const cpsd_integrals *I, const double *T2_1,
 // dosodiis2_d / orthogonalR2L and its own convergence test) and one batched
 // sigma V(fn,ai) R1(fn); the host never waits on a step's result, it stays
 // at most two steps ahead and stops once every root reports convergence.
-static int solve_r1(const Sys &S, const Ints &X, const cpsd_params *p, i64 symR, i64 nb, i64 l1,
-                    const EnergyPlan *e1, const double *cc, const double *L, const double *w0d, double *R1,
-                    i64 *sit) {
+int solve_r1(const Sys &S, const Ints &X, const cpsd_params *p, i64 symR, i64 nb, i64 l1, const EnergyPlan *e1,
+             const double *cc, const double *L, const double *w0d, double *R1, i64 *sit) {
     const i64 *o = S.popo, *v = S.popv;
     const int md = (int)p->diis_dim;
     if (md > DIIS_MAXDIM) return set_error(CPSD_EARG, "diis_dim above 16");
@@ -570,6 +549,7 @@ static int solve_r1(const Sys &S, const Ints &X, const cpsd_params *p, i64 symR,
     return CPSD_OK;
 }
 
+// EE-CPS(D-3) for nb roots of irrep symR sharing every contraction launch
 static int ee_roots_batch(const Sys &S, const Ints &X, const cpsd_params *p, const double *T2_1,
                           const cpsd_jints *J, i64 symR, i64 nb, const double *w0_host, const double *L,
                           double *w_host, double *R2_1o, double *R1_2o, double *R2_2o, i64 *sit_out) {
@@ -692,6 +672,10 @@ static int ee_roots_batch(const Sys &S, const Ints &X, const cpsd_params *p, con
     if (sit_out) *sit_out = sit;
     return cuda_check(cudaStreamSynchronize(stream()), "ee sync");
 }
+
+}  // namespace cpsd
+
+extern "C" {
 
 int cpsd_eecpsd_roots(const cpsd_system *s, const cpsd_integrals *I, const cpsd_params *p, const double *T2_1,
                       const cpsd_jints *J, int64_t symR, int64_t nroot, const double *w0_host, const double *L_dev,

@@ -3,6 +3,7 @@
 //               antisymmetrise / swap of index pairs);
 //  * k_energy   orbital-energy differences and denominators;
 //  * BLAS-1     scale, axpy, deterministic (optionally compensated) dot.
+#include <algorithm>
 #include <cstdio>
 
 #include "runtime.hpp"
@@ -78,6 +79,56 @@ __global__ void k_energy(const i64 *__restrict__ blk, int nblocks, i64 n, const 
             else v = in[e] / (ei + ej - ea - eb);  // mode 2
         }
         out[e] = v;
+    }
+}
+
+// Adjoint of the orbital-energy differences: with weights w = alpha x y on
+// the elements of a DPD tensor, the derivative of sum_e w(e) e(pq,rs) with
+// e(ab,ij) = ea+eb-ei-ej (e(a,i) = ea-ei) is, per orbital, the signed sum of
+// the weights of the elements that carry it.  Per-pair sums first (rows:
+// thread per left pair, columns: warp per right pair), then one signed
+// atomic per pair orbital.
+__global__ void k_energy_rows(const i64 *__restrict__ blk, const double *__restrict__ x,
+                              const double *__restrict__ y, double alpha, double *__restrict__ rsum) {
+    const i64 *B = blk + 5 * blockIdx.y;
+    for (i64 l = (i64)blockIdx.x * blockDim.x + threadIdx.x; l < B[1]; l += (i64)gridDim.x * blockDim.x) {
+        double acc = 0.0;
+        for (i64 r = 0; r < B[2]; r++) {
+            const i64 e = B[0] + r * B[1] + l;
+            acc += y ? x[e] * y[e] : x[e];
+        }
+        rsum[B[3] + l] = alpha * acc;
+    }
+}
+
+__global__ void k_energy_cols(const i64 *__restrict__ blk, const double *__restrict__ x,
+                              const double *__restrict__ y, double alpha, double *__restrict__ csum) {
+    const i64 *B = blk + 5 * blockIdx.y;
+    const int lane = threadIdx.x & 31;
+    const i64 nw = (i64)gridDim.x * (blockDim.x >> 5);
+    for (i64 r = (i64)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < B[2]; r += nw) {
+        double acc = 0.0;
+        for (i64 l = lane; l < B[1]; l += 32) {
+            const i64 e = B[0] + r * B[1] + l;
+            acc += y ? x[e] * y[e] : x[e];
+        }
+        for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) csum[B[4] + r] = alpha * acc;
+    }
+}
+
+// orbital k receives +sum for a virtual, -sum for an occupied orbital
+// (Eorb holds the occupied orbitals first: index < nocc)
+__global__ void k_energy_scatter(const i64 *__restrict__ lidx, i64 nl, const i64 *__restrict__ ridx, i64 nr,
+                                 const double *__restrict__ rsum, const double *__restrict__ csum, i64 nocc,
+                                 double *__restrict__ gorb) {
+    for (i64 k = (i64)blockIdx.x * blockDim.x + threadIdx.x; k < nl + nr; k += (i64)gridDim.x * blockDim.x) {
+        const bool left = k < nl;
+        const i64 q = left ? k : k - nl;
+        const double v = left ? rsum[q] : csum[q];
+        const i64 *ix = left ? lidx + 2 * q : ridx + 2 * q;
+        for (int t = 0; t < 2; t++)
+            if (ix[t] >= 0) atomicAdd(gorb + ix[t], ix[t] < nocc ? -v : v);
     }
 }
 
@@ -199,6 +250,31 @@ int launch_energy(const EnergyPlan *p, int mode, const double *eorb, const doubl
                                                         mode, in, out, w0_dev, nb, in_stride, out_stride);
     count_launch();
     return cuda_check(cudaGetLastError(), "k_energy");
+}
+
+int launch_energy_adjoint(const EnergyPlan *p, const double *x, const double *y, double alpha, i64 nocc,
+                          double *gorb) {
+    if (p->n == 0) return CPSD_OK;
+    CPSD_TRY(const_cast<EnergyPlan *>(p)->upload());
+    const i64 nl = (i64)p->h_lidx.size() / 2, nr = (i64)p->h_ridx.size() / 2;
+    i64 maxl = 1, maxr = 1;
+    for (int b = 0; b < p->nblocks; b++) {
+        maxl = std::max(maxl, p->h_blk[5 * b + 1]);
+        maxr = std::max(maxr, p->h_blk[5 * b + 2]);
+    }
+    ScratchScope sc;
+    double *rsum, *csum;
+    CPSD_TRY(scratch(nl, &rsum));
+    CPSD_TRY(scratch(nr, &csum));
+    dim3 gr((unsigned)std::min<i64>((maxl + 255) / 256, 148), (unsigned)p->nblocks);
+    dim3 gc((unsigned)std::min<i64>((maxr + 7) / 8, 296), (unsigned)p->nblocks);
+    k_energy_rows<<<gr, 256, 0, stream()>>>(p->d_blk, x, y, alpha, rsum);
+    k_energy_cols<<<gc, 256, 0, stream()>>>(p->d_blk, x, y, alpha, csum);
+    k_energy_scatter<<<grid_for(nl + nr), 256, 0, stream()>>>(p->d_lidx, nl, p->d_ridx, nr, rsum, csum, nocc, gorb);
+    count_launch();
+    count_launch();
+    count_launch();
+    return cuda_check(cudaGetLastError(), "k_energy adjoint");
 }
 
 }  // namespace cpsd

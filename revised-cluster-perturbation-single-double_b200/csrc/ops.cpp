@@ -422,6 +422,71 @@ int w224(const Ten &v1, const Ten &v2, Ten &v3, double fact, const char *t1, con
     return w444(v1, v2, v3, fact, a, b, t3, anti, nb);
 }
 
+// Vector-Jacobian product of the vv2v_444 form v3 += fact * P{v1 v2}: G +=
+// d<Y, v3> / d(operand `which`) (0: v1, 1: v2), the other operand fixed.
+// Every wrapper above is this form with padded specs (422 / 222 / 224 pad
+// with "+-" / "=+" / "=-", 424 / 442 pad the 2-index operand / result with
+// ".."), so one routine reverses them all.  The forward chain expand ->
+// contract -> antisymmetrise / compress is run backwards with each step
+// replaced by its adjoint: antisymmetrise-and-compress by expansion (the
+// cotangent of a packed p<q element goes to (p,q) and, negated, to (q,p)),
+// antisymmetrise by itself, the contraction by the contraction of Y with
+// the other operand onto the operand's letters, and the operand's
+// expansion by antisymmetrise-and-compress.  One copy (nb = 1).
+int vjp444(const Ten &v1, const Ten &v2, const Ten &Y, Ten &G, int which, double fact, const char *t1,
+           const char *t2, const char *t3, i64 anti) {
+    if (anti < 0 || anti > 3) return set_error(CPSD_EARG, "vjp444: anti must be 0..3");
+    if (which != 0 && which != 1) return set_error(CPSD_EARG, "vjp444: operand must be 0 or 1");
+    const char pair[6][2] = {{t1[0], t1[1]}, {t1[2], t1[3]}, {t2[0], t2[1]},
+                             {t2[2], t2[3]}, {t3[0], t3[1]}, {t3[2], t3[3]}};
+    const i64 iop[6] = {v1.d.iop[0], v1.d.iop[1], v2.d.iop[0], v2.d.iop[1], Y.d.iop[0], Y.d.iop[1]};
+    bool iexp[6] = {};
+    for (int i = 0; i < 6; i++)
+        if (check_flat(pair[i], pair, 6, i) && iop[i] != 1) {
+            if (iop[i] != 0) return set_error(CPSD_ELAYOUT, "vjp444: only antisymmetric (iop 0) pairs expand");
+            iexp[i] = true;
+        }
+    const bool a0 = anti == 1 || anti == 3, a1 = anti == 2 || anti == 3;
+    if ((!a0 && iexp[4]) || (!a1 && iexp[5]))
+        return set_error(CPSD_ELAYOUT, "vjp444: packed result pair needs antisymmetrisation");
+    ScratchScope sc;
+    // cotangent of the contraction result: adjoint of finish()
+    Ten X = Y;
+    X.bs = 0;
+    if (anti != 0) {
+        const int op0 = a0 ? (iexp[4] ? PAIR_EXPAND : PAIR_ANTI) : PAIR_ID;
+        const int op1 = a1 ? (iexp[5] ? PAIR_EXPAND : PAIR_ANTI) : PAIR_ID;
+        const PairMapPlan *pm;
+        Desc d;
+        CPSD_TRY(plan_pairmap(Y.d, op0, op1, 1, 1, &d, &pm));
+        X.d = d;
+        CPSD_TRY(scratch(d.len(), &X.arr));
+        CPSD_TRY(launch_pairmap(pm, Y.arr, X.arr, 1.0, 0.0));
+    }
+    const Ten &other = which == 0 ? v2 : v1;
+    const char *ts = which == 0 ? t1 : t2, *to = which == 0 ? t2 : t1;
+    const bool *ex_s = iexp + 2 * which, *ex_o = iexp + 2 * (1 - which);
+    Ten eo;
+    CPSD_TRY(expand(other, ex_o[0], ex_o[1], 1, &eo));
+    if (!ex_s[0] && !ex_s[1]) return engine(X, t3, eo, to, G, ts, fact, 1.0);
+    // the operand's packed pairs were expanded: contract into the full
+    // layout, then antisymmetrise-and-compress into G
+    Ten E = G;
+    E.bs = 0;
+    if (ex_s[0]) E.d.iop[0] = 1;
+    if (ex_s[1]) E.d.iop[1] = 1;
+    const i64 n = E.d.len();
+    CPSD_TRY(scratch(n, &E.arr));
+    CPSD_TRY(launch_scale(E.arr, n, 0.0));
+    CPSD_TRY(engine(X, t3, eo, to, E, ts, fact, 1.0));
+    const PairMapPlan *pm;
+    Desc d;
+    CPSD_TRY(plan_pairmap(E.d, ex_s[0] ? PAIR_ANTI_COMPRESS : PAIR_ID, ex_s[1] ? PAIR_ANTI_COMPRESS : PAIR_ID,
+                          G.d.iop[0], G.d.iop[1], &d, &pm));
+    if (d.iop[0] != G.d.iop[0] || d.iop[1] != G.d.iop[1]) return set_error(CPSD_ELAYOUT, "vjp444: layout mismatch");
+    return launch_pairmap(pm, E.arr, G.arr, 1.0, 1.0);
+}
+
 // ------------------------------------------------ lib_cc kernels (spin-free)
 int k_c1_r1iabj(Ten &c1, const Ten &r1, const Ten &V, double f, i64 nb) {
     return w422(V, r1, c1, f, "fnai", "fn", "ai", nb);
@@ -502,6 +567,42 @@ int k_Wmbej_r1ijka(Ten &W, const Ten &r1, const Ten &V, double f, i64 nb) {
 }
 int k_Wmnij_r1ijka(Ten &W, const Ten &r1, const Ten &V, double f, i64 nb) {
     return w424(V, r1, W, f, "mnie", "ej", "mnij", 2, nb);
+}
+
+// ------------------------------------------ adjoints of the lib_cc kernels
+// vjp_<name>(a, b, Y, G, which, f): G += d<Y, out>/da (which 0) or /db
+// (which 1) of out += f * <name>(a, b), with the operand order, specs and
+// factors of the forward kernels above (a 2-index operand or result padded
+// the way its wrapper pads it).
+int vjp_c1_r1iabj(const Ten &r1, const Ten &V, const Ten &Y, Ten &G, int which, double f) {
+    return vjp444(V, r1, Y, G, 1 - which, f, "fnai", "fn+-", "ai+-", 0);
+}
+int vjp_c1_r1Fae(const Ten &r1, const Ten &F, const Ten &Y, Ten &G, int which, double f) {
+    return vjp444(F, r1, Y, G, 1 - which, f, "ae=+", "ei=-", "ai+-", 0);
+}
+int vjp_c1_r1Fmi(const Ten &r1, const Ten &F, const Ten &Y, Ten &G, int which, double f) {
+    return vjp444(r1, F, Y, G, which, -f, "am=+", "mi=-", "ai+-", 0);
+}
+int vjp_c1_r2abci(const Ten &r2, const Ten &V, const Ten &Y, Ten &G, int which, double f) {
+    return vjp444(V, r2, Y, G, 1 - which, r2.d.iop[0] == 0 ? f : 0.5 * f, "feam", "feim", "ai..", 0);
+}
+int vjp_c1_r2ijka(const Ten &r2, const Ten &V, const Ten &Y, Ten &G, int which, double f) {
+    return vjp444(r2, V, Y, G, which, r2.d.iop[1] == 0 ? -f : -0.5 * f, "aemn", "mnie", "ai..", 0);
+}
+int vjp_c2_r1abci(const Ten &r1, const Ten &V, const Ten &Y, Ten &G, int which, double f) {
+    return vjp444(V, r1, Y, G, 1 - which, f, "abej", "ei..", "abij", 2);
+}
+int vjp_c2_r1ijka(const Ten &r1, const Ten &V, const Ten &Y, Ten &G, int which, double f) {
+    return vjp444(V, r1, Y, G, 1 - which, -f, "ijmb", "am..", "abij", 1);
+}
+int vjp_Fmi_r2abij(const Ten &r2, const Ten &V, const Ten &Y, Ten &G, int which, double f) {
+    return vjp444(V, r2, Y, G, 1 - which, r2.d.iop[0] == 1 ? 0.5 * f : f, "efmn", "efin", "mi..", 0);
+}
+int vjp_Fae_r2abij(const Ten &r2, const Ten &V, const Ten &Y, Ten &G, int which, double f) {
+    return vjp444(r2, V, Y, G, which, r2.d.iop[1] == 0 ? -f : -0.5 * f, "afmn", "efmn", "ae..", 0);
+}
+int vjp_Wmbej_r2abij(const Ten &r2, const Ten &V, const Ten &Y, Ten &G, int which, double f) {
+    return vjp444(V, r2, Y, G, 1 - which, 0.5 * f, "fenm", "bfjn", "embj", 0);
 }
 
 }  // namespace cpsd

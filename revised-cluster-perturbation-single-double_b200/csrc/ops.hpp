@@ -71,4 +71,24 @@ CPSD_IK(Wmbej_r1ijka);
 CPSD_IK(Wmnij_r1ijka);
 #undef CPSD_IK
 
+// Vector-Jacobian product of the vv2v_444 form v3 += fact * P{v1 v2}:
+// G += d<Y, v3>/d(v1) (which 0) or d(v2) (which 1); Y has v3's layout, G
+// the operand's.  One copy (no batch).
+int vjp444(const Ten &v1, const Ten &v2, const Ten &Y, Ten &G, int which, double fact, const char *t1,
+           const char *t2, const char *t3, i64 anti);
+// adjoints of the kernels on the SF-CIS(D) energy path: G += d<Y, out>/da
+// (which 0) or d<Y, out>/db (which 1) of out += f * kernel(a, b)
+#define CPSD_VJP(name) int vjp_##name(const Ten &a, const Ten &b, const Ten &Y, Ten &G, int which, double f)
+CPSD_VJP(c1_r1iabj);
+CPSD_VJP(c1_r1Fae);
+CPSD_VJP(c1_r1Fmi);
+CPSD_VJP(c1_r2abci);
+CPSD_VJP(c1_r2ijka);
+CPSD_VJP(c2_r1abci);
+CPSD_VJP(c2_r1ijka);
+CPSD_VJP(Fmi_r2abij);
+CPSD_VJP(Fae_r2abij);
+CPSD_VJP(Wmbej_r2abij);
+#undef CPSD_VJP
+
 }  // namespace cpsd

@@ -226,6 +226,10 @@ int plan_energy(const Desc &d, const char *kinds, const EnergyPlan **out);
 // mode 5: out = ei-ea                          (the mode-3 divisor, 2-index)
 int launch_energy(const EnergyPlan *p, int mode, const double *eorb, const double *in, double *out,
                   const double *w0_dev = nullptr, i64 nb = 1, i64 in_stride = 0, i64 out_stride = 0);
+// gorb[k] += d/d eorb[k] of sum_e alpha x(e) y(e) e(pq,rs) (y null: y = 1),
+// e(pq,rs) the plan's orbital-energy difference; nocc = occupied orbitals
+int launch_energy_adjoint(const EnergyPlan *p, const double *x, const double *y, double alpha, i64 nocc,
+                          double *gorb);
 // y_c += sgn * a_dev[c] * x_c for nb copies
 int launch_axpy_dev(i64 n, const double *a_dev, double sgn, const double *x, double *y, i64 nb = 1, i64 sx = 0,
                     i64 sy = 0);

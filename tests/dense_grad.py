@@ -1,0 +1,167 @@
+"""FP64 reference gradient of the SF-CIS(D) energies (test infrastructure).
+
+The energies w0 (SF-CIS) and w^(2) (order 2 of src/EE-CPSd.SF/run_order.f90)
+are restated densely in torch (float64, CPU) from the packed DPD integral
+vectors and Eorb, and differentiated by torch autograd; no hand-written
+adjoint is involved.  The packed -> dense expansion is an index scatter with
+the pair signs of the DPD layout (tests/dense.py), so autograd returns the
+gradient with respect to the packed storage the library differentiates.
+
+The CIS vector is the converged right eigenvector of A(ai,fn) = e(a,i) d +
+V(fn,ai) on the irrep's (a,i) space, obtained by shifted inverse iteration
+started from a converged root (unrolled, so autograd differentiates the
+eigenvector itself, also for perturbations that make A non-symmetric); w0 is
+its Rayleigh quotient, which agrees with the eigenvalue to first order.
+The dense kernel formulas are those of tests/kernel_specs.py.
+"""
+import numpy as np
+import torch
+
+import dense
+
+T = torch.float64
+
+
+def _pq(X):
+    return X - X.permute(1, 0, 2, 3)
+
+
+def _rs(X):
+    return X - X.permute(0, 1, 3, 2)
+
+
+class DenseCisd:
+    """Dense w0 / w^(2) of the roots of irrep symR of a synth.System."""
+
+    LAYOUTS = {  # tensor -> (pop letters, iops)
+        "ijka": ("ooov", (0, 1)),
+        "abij": ("vvoo", (0, 0)),
+        "iabj": ("vovo", (1, 1)),
+        "abci": ("vvvo", (0, 1)),
+    }
+
+    def __init__(self, s, symR):
+        self.s, self.symR = s, symR
+        sym = s.sym
+        self.no, self.nv = int(s.popo.sum()), int(s.popv.sum())
+        pm = {"o": s.popo, "v": s.popv}
+        self.maps = {}
+        for k, (letters, iops) in self.LAYOUTS.items():
+            pops = [pm[c] for c in letters]
+            rows, total = dense.dpd_index_lists(sym, pops, iops, 1)
+            self.maps[k] = (torch.from_numpy(rows), total, iops, tuple(int(np.sum(p)) for p in pops))
+        z = np.array([1, 0, 0, 0, 0, 0, 0, 0], np.int64)
+        rows, self.l1 = dense.dpd_index_lists(sym, [s.popv, s.popo, z, z], (1, 1), symR)
+        self.r1_rows = torch.from_numpy(rows)
+        irr_o, irr_v = dense.orbital_irreps(s.popo), dense.orbital_irreps(s.popv)
+        mask = np.array([[sym.dp(a, i) == symR for i in irr_o] for a in irr_v])
+        self.idx = torch.from_numpy(np.argwhere(mask))
+
+    def to_dense(self, key, vec):
+        rows, total, iops, shape = self.maps[key]
+        assert vec.numel() == total
+        o, a, b, c, d = rows.T
+        x = vec[o]
+        D = torch.zeros(shape, dtype=T)
+        D = D.index_put((a, b, c, d), x, accumulate=True)
+        if iops[0] == 0:
+            D = D.index_put((b, a, c, d), -x, accumulate=True)
+        if iops[1] == 0:
+            D = D.index_put((a, b, d, c), -x, accumulate=True)
+        if iops[0] == 0 and iops[1] == 0:
+            D = D.index_put((b, a, d, c), x, accumulate=True)
+        return D
+
+    def r1_to_dense(self, vec):
+        o, a, b = self.r1_rows.T[:3]
+        return torch.zeros((self.nv, self.no), dtype=T).index_put((a, b), vec[o], accumulate=True)
+
+    def r1_to_dpd(self, M):
+        o, a, b = self.r1_rows.T[:3]
+        out = torch.zeros(self.l1, dtype=T)
+        out[o] = M[a, b]
+        return out
+
+    def energies(self, ints, eorb, L0, w0_start, iters=4, shift=1e-7):
+        """ints: dict of packed torch vectors; eorb: torch vector; L0: packed
+        converged CIS vector (start of the inverse iteration); returns
+        (w0, w2, L packed)."""
+        ijka = self.to_dense("ijka", ints["ijka"])
+        abij = self.to_dense("abij", ints["abij"])
+        iabj = self.to_dense("iabj", ints["iabj"])
+        abci = self.to_dense("abci", ints["abci"])
+        eo, ev = eorb[:self.no], eorb[self.no:]
+        e1 = ev[:, None] - eo[None, :]
+        e2 = ev[:, None, None, None] + ev[None, :, None, None] - eo[None, None, :, None] - eo[None, None, None, :]
+        # CIS: A(ai,fn) = V(fn,ai) + e(a,i) on the (a,i) pairs of irrep symR
+        a, i = self.idx[:, 0], self.idx[:, 1]
+        A = iabj[:, :, a, i][a, i].T + torch.diag(e1[a, i])  # rows (ai), columns (fn)
+        x = self.r1_to_dense(torch.as_tensor(L0, dtype=T))[a, i]
+        x = x / torch.linalg.norm(x)
+        sig = float(w0_start) + shift
+        M = A - sig * torch.eye(len(a), dtype=T)
+        for _ in range(iters):
+            x = torch.linalg.solve(M, x)
+            x = x / torch.linalg.norm(x)
+        if float(torch.dot(x.detach(), self.r1_to_dense(torch.as_tensor(L0, dtype=T))[a, i])) < 0:
+            x = -x
+        w0 = torch.dot(x, A @ x)
+        L = torch.zeros((self.nv, self.no), dtype=T).index_put((a, i), x)
+        # T2^(1) and J^(2) (run1.f90, calJ.f90)
+        T2 = -abij / e2
+        Foo = 0.5 * torch.einsum("efin,efmn->mi", T2, abij)
+        Fvv = -0.5 * torch.einsum("afmn,efmn->ae", T2, abij)
+        Wvo = torch.einsum("bfjn,fenm->embj", T2, abij)
+        # order 1 / 2 of run_order.f90
+        C2 = -_pq(torch.einsum("ijmb,am->abij", ijka, L)) + _rs(torch.einsum("abej,ei->abij", abci, L))
+        R2 = -C2 / (e2 - w0)
+        C1 = (0.5 * torch.einsum("feam,feim->ai", abci, R2) - 0.5 * torch.einsum("aemn,mnie->ai", R2, ijka)
+              + torch.einsum("fn,fnai->ai", L, Wvo) + torch.einsum("ae,ei->ai", Fvv, L)
+              - torch.einsum("am,mi->ai", L, Foo))
+        w2 = torch.sum(L * C1)
+        return w0, w2, self.r1_to_dpd(L.detach())
+
+    def gradient(self, s, L0, w0_start, g0, g2):
+        """d(g0 w0 + g2 w2) / d(ijka, abij, iabj, abci, eorb) as numpy vectors."""
+        leaves = {k: torch.tensor(s.ints[k], dtype=T, requires_grad=True) for k in self.LAYOUTS}
+        eorb = torch.tensor(s.eorb, dtype=T, requires_grad=True)
+        w0, w2, _ = self.energies(leaves, eorb, L0, w0_start)
+        E = g0 * w0 + g2 * w2
+        grads = torch.autograd.grad(E, [leaves[k] for k in self.LAYOUTS] + [eorb])
+        out = {k: g.numpy() for k, g in zip(self.LAYOUTS, grads[:4])}
+        out["eorb"] = grads[4].numpy()
+        return out, float(w0.detach()), float(w2.detach())
+
+
+def perturbed(s, h, dL, deps_a, deps_b):
+    """Integrals and Eorb of s with the generator's inputs moved by h along
+    (dL, deps_a, deps_b); restores s afterwards."""
+    L0, ea0, eb0 = s.L, s.eps_a, s.eps_b
+    try:
+        s.L = np.ascontiguousarray(L0 + h * dL)
+        s.eps_a, s.eps_b = ea0 + h * deps_a, eb0 + h * deps_b
+        s._build(s.ints["abcd"] is None)
+        return {k: (None if v is None else v.copy()) for k, v in s.ints.items()}, s.eorb.copy()
+    finally:
+        s.L, s.eps_a, s.eps_b = L0, ea0, eb0
+        s._build(s.ints["abcd"] is None)
+
+
+def random_direction(s, rng):
+    """A generator-input direction that keeps the integrals' symmetry: L'
+    symmetric in pq with the aux-irrep mask of synth.System; orbital-energy
+    moves small enough to keep the orbital order."""
+    dL = rng.normal(0.0, 0.05, s.L.shape)
+    dL = np.triu(dL) + np.transpose(np.triu(dL, 1), (0, 2, 1))
+    dL = np.where(s.L != 0, dL, 0.0)
+    return dL, rng.normal(0.0, 0.1, s.eps_a.shape), rng.normal(0.0, 0.1, s.eps_b.shape)
+
+
+def direction_in_dpd(s, h, dL, dea, deb):
+    """The integral / Eorb direction of a generator-input direction, by
+    central difference (exact for the quadratic integrals and linear Eorb)."""
+    ip, ep = perturbed(s, h, dL, dea, deb)
+    im, em = perturbed(s, -h, dL, dea, deb)
+    d = {k: (ip[k] - im[k]) / (2 * h) for k in DenseCisd.LAYOUTS}
+    d["eorb"] = (ep - em) / (2 * h)
+    return d, (ip, ep), (im, em)
