@@ -47,7 +47,8 @@ def parse():
                     help="7-bit digits per FP64 value on the int8 tensor cores (0 = FP64 path only)")
     ap.add_argument("--no-fp64-path", action="store_true", help="skip timing the plain FP64 path beside the headline")
     ap.add_argument("--case-nmo", type=int, default=100)
-    ap.add_argument("--case", default="", choices=["", "ladder"],
+    ap.add_argument("--directions", type=int, default=200, help="finite-difference directions of --case grad")
+    ap.add_argument("--case", default="", choices=["", "ladder", "grad"],
                     help="time one contraction on its own (kernel profiling) instead of the pipeline")
     return ap.parse_args()
 
@@ -428,8 +429,92 @@ def run_case(args):
           flush=True)
 
 
+def run_grad(args):
+    """Differentiation form: C2v, nmo 120, nocc 8/6, 4 roots of irrep 1.
+    Times the SF-CIS(D) energies (cpsd_cisd_energies: Davidson to 1e-12 and
+    w^(2)) and one adjoint gradient per root (cpsd_cisd_gradient, FP64),
+    then checks every root's gradient against central finite differences of
+    the device energies (step 1e-5) along --directions seeded integral-
+    perturbation directions (DPD images of moves of the generator's (pq|rs)
+    factor and orbital energies)."""
+    import torch
+    import __graft_entry__ as ge
+    ge.load_package()
+    from cpsd_b200 import api, synth
+    keys = ("ijka", "abij", "iabj", "abci", "eorb")
+    s = synth.make("c2v_nmo120", skip_abcd=True)
+    symR, nroot = 1, int(s.estate_sym[0])
+    api.use_torch_stream()
+    t = {k: torch.from_numpy(s.ints[k] if k != "eorb" else s.eorb).cuda() for k in keys}
+    par = api.make_params(s, davidson_conv=12, davidson_cyc=100, diis_max_err=1e-12, diis_cyc=200)
+    sysc = api.make_system(s)
+    st = api.integrals_struct(t)
+
+    def forward(tt=None):
+        return api.cisd_energies(s, sysc, api.integrals_struct(tt) if tt else st, par, symR, nroot)
+
+    def backward(w0, L):
+        out = []
+        for r in range(nroot):
+            g = np.zeros(nroot)
+            g[r] = 1.0
+            G = {k: torch.zeros_like(v) for k, v in t.items()}
+            api.cisd_gradient(sysc, st, par, symR, w0, L, g, g, G)
+            out.append(G)
+        return out
+
+    def timed(fn, n):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(n):
+            res = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / n, res
+
+    for _ in range(args.warmup):
+        w0, w2, L = forward()
+        backward(w0, L)
+    f_ms, (w0, w2, L) = timed(forward, args.steps)
+    b_ms, Gs = timed(lambda: backward(w0, L), args.steps)
+    rng = np.random.default_rng(0)
+    h = 1e-5
+    rel, absn, fds = [], [], []
+    t0 = time.time()
+    for _ in range(args.directions):
+        d = s.integral_direction(*s.input_direction(rng))
+        dt = {k: torch.from_numpy(d[k]).cuda() for k in keys}
+        E = []
+        for sg in (1.0, -1.0):
+            a, b, _ = forward({k: t[k] + sg * h * dt[k] for k in keys})
+            E.append(a + b)
+        fd = (E[0] - E[1]) / (2 * h)
+        for r in range(nroot):
+            pred = sum(float(torch.dot(Gs[r][k], dt[k])) for k in keys)
+            rel.append(abs(pred - fd[r]) / abs(fd[r]))
+            absn.append(abs(pred - fd[r]))
+            fds.append(abs(fd[r]))
+    rel, absn = np.array(rel), np.array(absn)
+    print(json.dumps({
+        "case": "grad", "workload": "c2v_nmo120", "config": (f"c2v_nmo120: SF-CIS (Davidson residual 1e-12) + w^(2) and d(w0 + w2)/d(ijka, abij, iabj, "
+                   f"abci, Eorb) per root; C2v nirrep={s.nirrep}, nmo={s.nmo}, nocc {s.nocc_a}/{s.nocc_b}, "
+                   f"o={int(s.popo.sum())}, v={int(s.popv.sum())}"), "roots": nroot,
+        "dtype": "f64", "data": "synthetic (seeded generator)",
+        "forward_ms": f_ms, "backward_ms_all_roots": b_ms, "backward_ms_per_root": b_ms / nroot,
+        "w0": [float(x) for x in w0], "w2": [float(x) for x in w2],
+        "fd": {"directions": args.directions, "step": h, "checks": int(rel.size),
+               "max_rel_err": float(rel.max()), "median_rel_err": float(np.median(rel)),
+               "max_abs_err": float(absn.max()), "median_abs_derivative": float(np.median(fds)),
+               "within_1e-6": int((rel < 1e-6).sum()), "seconds": time.time() - t0},
+    }), flush=True)
+
+
 def main():
     args = parse()
+    if args.case == "grad":
+        run_grad(args)
+        return
     if args.case:
         run_case(args)
         return

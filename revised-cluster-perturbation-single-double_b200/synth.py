@@ -133,6 +133,37 @@ class System:
             raise RuntimeError(f"cpsd_synth_build failed: {rc}")
         assert np.array_equal(popo, self.popo) and np.array_equal(popv, self.popv)
 
+    def input_direction(self, rng):
+        """Seeded direction in the generator's inputs that keeps the
+        integrals' structure: L' symmetric in pq under the aux-irrep mask of
+        L, and orbital-energy moves for eps_a / eps_b."""
+        dL = rng.normal(0.0, 0.05, self.L.shape)
+        dL = np.triu(dL) + np.transpose(np.triu(dL, 1), (0, 2, 1))
+        dL = np.where(self.L != 0, dL, 0.0)
+        return dL, rng.normal(0.0, 0.1, self.eps_a.shape), rng.normal(0.0, 0.1, self.eps_b.shape)
+
+    def integral_direction(self, dL, deps_a, deps_b):
+        """The direction in the DPD integrals and Eorb of a generator-input
+        direction: the integrals are quadratic in L, so with the symmetric
+        bilinear form B, ints(L + L') - ints(L - L') = 4 B(L, L') exactly;
+        Eorb is linear in the orbital energies.  Returns {name: array}
+        (abcd None when it is not built)."""
+        L0, ea0, eb0 = self.L, self.eps_a, self.eps_b
+        out = []
+        try:
+            for sgn in (1.0, -1.0):
+                self.L = np.ascontiguousarray(L0 + sgn * dL)
+                self.eps_a, self.eps_b = ea0 + sgn * deps_a, eb0 + sgn * deps_b
+                self._build(self.ints["abcd"] is None)
+                out.append(({k: (None if v is None else v.copy()) for k, v in self.ints.items()}, self.eorb.copy()))
+        finally:
+            self.L, self.eps_a, self.eps_b = L0, ea0, eb0
+            self._build(self.ints["abcd"] is None)
+        (ip, ep), (im, em) = out
+        d = {k: (None if ip[k] is None else 0.5 * (ip[k] - im[k])) for k in ip}
+        d["eorb"] = 0.5 * (ep - em)
+        return d
+
     @property
     def nroots(self):
         return int(self.estate_sym.sum())

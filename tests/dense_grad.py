@@ -133,35 +133,8 @@ class DenseCisd:
         return out, float(w0.detach()), float(w2.detach())
 
 
-def perturbed(s, h, dL, deps_a, deps_b):
-    """Integrals and Eorb of s with the generator's inputs moved by h along
-    (dL, deps_a, deps_b); restores s afterwards."""
-    L0, ea0, eb0 = s.L, s.eps_a, s.eps_b
-    try:
-        s.L = np.ascontiguousarray(L0 + h * dL)
-        s.eps_a, s.eps_b = ea0 + h * deps_a, eb0 + h * deps_b
-        s._build(s.ints["abcd"] is None)
-        return {k: (None if v is None else v.copy()) for k, v in s.ints.items()}, s.eorb.copy()
-    finally:
-        s.L, s.eps_a, s.eps_b = L0, ea0, eb0
-        s._build(s.ints["abcd"] is None)
 
-
-def random_direction(s, rng):
-    """A generator-input direction that keeps the integrals' symmetry: L'
-    symmetric in pq with the aux-irrep mask of synth.System; orbital-energy
-    moves small enough to keep the orbital order."""
-    dL = rng.normal(0.0, 0.05, s.L.shape)
-    dL = np.triu(dL) + np.transpose(np.triu(dL, 1), (0, 2, 1))
-    dL = np.where(s.L != 0, dL, 0.0)
-    return dL, rng.normal(0.0, 0.1, s.eps_a.shape), rng.normal(0.0, 0.1, s.eps_b.shape)
-
-
-def direction_in_dpd(s, h, dL, dea, deb):
-    """The integral / Eorb direction of a generator-input direction, by
-    central difference (exact for the quadratic integrals and linear Eorb)."""
-    ip, ep = perturbed(s, h, dL, dea, deb)
-    im, em = perturbed(s, -h, dL, dea, deb)
-    d = {k: (ip[k] - im[k]) / (2 * h) for k in DenseCisd.LAYOUTS}
-    d["eorb"] = (ep - em) / (2 * h)
-    return d, (ip, ep), (im, em)
+def shifted(s, d, h):
+    """integrals and Eorb of s moved by h along the DPD direction d"""
+    ints = {k: (None if v is None else v + h * d[k]) if k in d else v for k, v in s.ints.items()}
+    return ints, s.eorb + h * d["eorb"]

@@ -103,10 +103,9 @@ def test_gradient_fd_c2v_nmo120():
         Gs.append(gradient(s, symR, w0, L, t, par, g, g))
     worst = 0.0
     for _ in range(3):
-        dL, dea, deb = dg.random_direction(s, rng)
-        d, (ip, ep), (im, em) = dg.direction_in_dpd(s, h, dL, dea, deb)
+        d = s.integral_direction(*s.input_direction(rng))
         vals = []
-        for ints, eo in ((ip, ep), (im, em)):
+        for ints, eo in (dg.shifted(s, d, h), dg.shifted(s, d, -h)):
             saved = s.ints, s.eorb
             s.ints, s.eorb = ints, eo
             try:
