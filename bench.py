@@ -48,7 +48,9 @@ def parse():
     ap.add_argument("--no-fp64-path", action="store_true", help="skip timing the plain FP64 path beside the headline")
     ap.add_argument("--case-nmo", type=int, default=100)
     ap.add_argument("--directions", type=int, default=200, help="finite-difference directions of --case grad")
-    ap.add_argument("--case", default="", choices=["", "ladder", "grad"],
+    ap.add_argument("--workers", type=int, default=8, help="concurrent molecules of --case batch")
+    ap.add_argument("--wave-gb", type=float, default=140.0, help="device-memory budget of one --case batch wave")
+    ap.add_argument("--case", default="", choices=["", "ladder", "grad", "batch"],
                     help="time one contraction on its own (kernel profiling) instead of the pipeline")
     return ap.parse_args()
 
@@ -288,6 +290,7 @@ def run_ours(args, rank, world, local_rank):
     # step of the headline mode: roofline of the digit GEMM (int8 tensor
     # cores) and of the FP64 tensor-pipe kernel
     lib = api.lib()
+    api.set_mixed(digits, 1.0)
     lib.cpsd_contract_timing(1)
     lib.cpsd_contract_time(None, None, None, 1)
     step()
@@ -510,10 +513,108 @@ def run_grad(args):
     }), flush=True)
 
 
+def run_batch(args):
+    """Batching workload: synth.batch_draw() - 64 independent molecules,
+    nmo ~ U{60..240}, nocc_alpha ~ U{4..12}, nocc_beta = nocc_alpha - 2,
+    nirrep from {1, 2, 4, 8}, 4-8 roots each (392 roots), lowest-root
+    Davidson.  Their abcd + abci integrals alone take 846 GB in FP64, more
+    than four B200s hold, so the molecules run in waves whose estimated
+    footprint (integrals, cached digit tiles, scratch) fits in --wave-gb:
+    each wave's integrals are built on the device (synth.device_integrals),
+    then the wave runs as one cpsd_pipeline_batch on --workers streams in
+    the mixed mode and in plain FP64, each timed with CUDA events with the
+    wave's inputs resident.  value = all roots / summed mixed wave times;
+    the FP64 figure and the largest energy deviation between the two modes
+    are reported beside it."""
+    import gc
+    import torch
+    import __graft_entry__ as ge
+    ge.load_package()
+    from cpsd_b200 import api, synth
+    t_start = time.time()
+    draws = synth.batch_draw()
+    mols = [synth.System(**d, host_ints=False, run_opts={"lowest": 1}) for d in draws]
+    api.use_torch_stream()
+    stream = torch.cuda.current_stream()
+
+    def need(s):
+        L = s.lengths()
+        ints = 8.0 * sum(L.values())
+        digits = 0.7 * 8.0 * (L["abcd"] + L["abci"])  # digit tiles of the cached integrals
+        scratch = 8.0 * s.nroots * 14 * s.r2_len(1)
+        return ints + digits + scratch + 1.5e9
+
+    order = sorted(range(len(mols)), key=lambda i: -need(mols[i]))
+    budget = args.wave_gb * 1e9
+    waves, cur, tot = [], [], 0.0
+    for i in order:
+        if cur and tot + need(mols[i]) > budget:
+            waves.append(cur)
+            cur, tot = [], 0.0
+        cur.append(i)
+        tot += need(mols[i])
+    waves.append(cur)
+    res = {0: [None] * len(mols), args.digits: [None] * len(mols)}
+    times = {0: 0.0, args.digits: 0.0}
+    gen_s, launches = 0.0, {0: 0, args.digits: 0}
+    for w in waves:
+        g0 = time.time()
+        tens = [synth.device_integrals(mols[i]) for i in w]
+        torch.cuda.synchronize()
+        gen_s += time.time() - g0
+        ints = [api.DeviceIntegrals.from_tensors(t) for t in tens]
+        pars = [api.make_params(mols[i]) for i in w]
+        for mode in (args.digits, 0):
+            api.set_mixed(mode, 1.0)
+            for _ in range(args.warmup):
+                api.pipeline_batch([mols[i] for i in w], ints, pars, nworkers=args.workers)
+            torch.cuda.synchronize()
+            api.launch_count(True)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(args.steps):
+                out = api.pipeline_batch([mols[i] for i in w], ints, pars, nworkers=args.workers)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times[mode] += e0.elapsed_time(e1) / args.steps / 1e3
+            launches[mode] += api.launch_count(True) // max(args.steps, 1)
+            for i, o in zip(w, out):
+                res[mode][i] = o
+        api.set_mixed(0)
+        del ints, tens, out
+        gc.collect()
+        torch.cuda.empty_cache()
+        api.release_device_cache()
+    nroots = sum(s.nroots for s in mols)
+    dev = max(float(np.max(np.abs(np.asarray(a) - np.asarray(b))))
+              for i in range(len(mols)) for a, b in zip(res[args.digits][i], res[0][i]))
+    print(json.dumps({
+        "case": "batch", "metric": METRIC, "unit": "roots/s", "dtype": "f64 (int8 digits)",
+        "data": "synthetic (seeded generator, synth.batch_draw)",
+        "config": {"workload": "batching form: 64 independent molecules, nmo ~U{60..240}, nocc_a ~U{4..12}, "
+                               "nocc_b = nocc_a - 2, nirrep from {1,2,4,8}, 4-8 roots each (lowest roots)",
+                   "molecules": len(mols), "roots": nroots, "waves": [len(w) for w in waves],
+                   "wave_budget_gb": args.wave_gb, "workers": args.workers,
+                   "abcd_abci_fp64_gb": round(sum(8.0 * (s.lengths()["abcd"] + s.lengths()["abci"])
+                                                  for s in mols) / 1e9, 1),
+                   "mode": f"mixed: contractions >= 1 GFLOP on the int8 tensor cores with {args.digits} digits"},
+        "value": nroots / times[args.digits], "ms_total": 1e3 * times[args.digits],
+        "fp64_path": {"value": nroots / times[0], "ms_total": 1e3 * times[0], "gpu_launches": launches[0]},
+        "mixed_over_fp64": times[0] / times[args.digits],
+        "max_abs_dev_vs_fp64_eh": dev, "gpu_launches": launches[args.digits],
+        "steps": args.steps, "warmup": args.warmup, "device_generation_s": gen_s,
+        "wall_s": time.time() - t_start,
+        "roots_per_molecule": [[float(x) for x in res[args.digits][i][0]] for i in range(len(mols))][:3],
+    }), flush=True)
+
+
 def main():
     args = parse()
     if args.case == "grad":
         run_grad(args)
+        return
+    if args.case == "batch":
+        run_batch(args)
         return
     if args.case:
         run_case(args)

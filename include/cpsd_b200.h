@@ -325,6 +325,26 @@ int cpsd_eecpsd_roots(const cpsd_system *s, const cpsd_integrals *I, const cpsd_
 int cpsd_pipeline(const cpsd_system *s, const cpsd_integrals *I, const cpsd_params *p,
                   double *omega_cis, double *w2, double *w3, int64_t *nroots);
 
+/* Independent molecules in one call (no counterpart in the reference, which
+ * runs one molecule per program invocation): cpsd_pipeline of molecule m
+ * with s[m], I[m], p[m] (each with its own nirrep / populations), run by
+ * nworkers (1..64) persistent host threads, each with its own CUDA stream
+ * and library state, largest molecules first; the batch starts after the
+ * work queued so far on the calling thread's stream and the call returns
+ * when every molecule is done.  Roots go to omega_cis / w2 / w3 in molecule
+ * order (molecule m's roots start after those of molecules 0..m-1);
+ * *nroots = their total.  The mixed-precision setting of the calling thread
+ * applies to every molecule.  The first failing molecule's error is
+ * returned (the remaining ones are not started). */
+int cpsd_pipeline_batch(int64_t nmol, const cpsd_system *s, const cpsd_integrals *I, const cpsd_params *p,
+                        int64_t nworkers, double *omega_cis, double *w2, double *w3, int64_t *nroots);
+
+/* Gives back device memory the library keeps between calls: the idle
+ * buffers of its constant-operand copies and the calling thread's scratch
+ * arena now, the batch workers' arenas at their next job.  Later calls
+ * allocate again as needed. */
+int cpsd_release_device_cache(void);
+
 /* -------------------------------------------- SF-CIS(D) energy gradient
  * No counterpart in the reference (it has no derivative code).
  *

@@ -193,6 +193,17 @@ class DeviceIntegrals:
         for k, v in self.t.items():
             setattr(self.struct, k, v.data_ptr() if v is not None else None)
 
+    @classmethod
+    def from_tensors(cls, t):
+        """wrap a dict of device tensors (ijkl ... abcd, eorb; missing: NULL)"""
+        self = cls.__new__(cls)
+        self.t = {k: t.get(k) for k in cls.KEYS}
+        self.t["eorb"] = t["eorb"]
+        self.struct = Integrals()
+        for k, v in self.t.items():
+            setattr(self.struct, k, v.data_ptr() if v is not None else None)
+        return self
+
     @property
     def nbytes(self):
         return sum(v.numel() * 8 for v in self.t.values() if v is not None)
@@ -309,3 +320,30 @@ def cisd_gradient(sysc, ints_struct, par, symR, w0, L, g0, g2, grads):
                                    I64(len(w0)), w0.ctypes.data_as(ctypes.c_void_p), dptr(L),
                                    g0.ctypes.data_as(ctypes.c_void_p), g2.ctypes.data_as(ctypes.c_void_p),
                                    ctypes.byref(G)), "cpsd_cisd_gradient")
+
+
+def pipeline_batch(systems, ints_list, params, nworkers=4):
+    """cpsd_pipeline_batch over independent molecules: systems (synth.System
+    or compatible), their DeviceIntegrals and Params; returns per-molecule
+    (omega_cis, w2, w3) lists."""
+    n = len(systems)
+    S = (System * n)(*[make_system(s) for s in systems])
+    I = (Integrals * n)(*[d.struct for d in ints_list])
+    P = (Params * n)(*params)
+    counts = [int(sum(p.estate_sym[h] for h in range(8))) for p in params]
+    tot = max(sum(counts), 1)
+    om, w2, w3 = np.zeros(tot), np.zeros(tot), np.zeros(tot)
+    nr = I64()
+    check(lib().cpsd_pipeline_batch(I64(n), S, I, P, I64(nworkers), om.ctypes.data_as(ctypes.c_void_p),
+                                    w2.ctypes.data_as(ctypes.c_void_p), w3.ctypes.data_as(ctypes.c_void_p),
+                                    ctypes.byref(nr)), "cpsd_pipeline_batch")
+    out, k = [], 0
+    for c in counts:
+        out.append((om[k:k + c], w2[k:k + c], w3[k:k + c]))
+        k += c
+    return out
+
+
+def release_device_cache():
+    """cpsd_release_device_cache: free the library's idle device buffers."""
+    check(lib().cpsd_release_device_cache(), "cpsd_release_device_cache")

@@ -9,6 +9,7 @@
 // next K stage is fetched into registers while the current one is
 // multiplied.  Split-K tiles write partial sums that k_splitk_reduce adds
 // in a fixed order, so results are deterministic.
+#include <atomic>
 #include <array>
 #include <vector>
 
@@ -246,7 +247,7 @@ struct Timing {
     std::vector<std::array<int64_t, 4>> shape;  // tasks, segments, tiles, tile config
 };
 Timing &timing() {
-    static Timing t;
+    thread_local Timing t;
     return t;
 }
 int timing_event(cudaEvent_t *e) {
@@ -337,7 +338,7 @@ int launch_contract(const ContractPlan *p, const double *A, const double *B, dou
         timing().shape.push_back({p->ntasks, p->nsegs, p->ntiles, p->cfg});
         CPSD_TRY(cuda_check(cudaEventRecord(e0, stream()), "event record"));
     }
-    static bool attr_set = false;
+    static std::atomic<bool> attr_set{false};
     if (!attr_set) {
         CPSD_TRY(cuda_check(cudaFuncSetAttribute(k_contract<128, 64, 4, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                  smem_bytes<128, 64>()), "smem attr"));

@@ -8,6 +8,7 @@
 // buffers.  The roots of one irrep can share each contraction launch
 // (params.batch_roots), which streams every integral block once per launch
 // instead of once per root.
+#include <algorithm>
 #include <cmath>
 #include <cstddef>
 #include <cstring>
@@ -59,7 +60,7 @@ Ints make_ints(const Sys &S, const cpsd_integrals *I) {
 }
 
 double *mailbox() {
-    static double *p = nullptr;
+    thread_local double *p = nullptr;
     if (!p) cudaMallocHost(&p, 4096);
     return p;
 }
@@ -73,7 +74,7 @@ namespace {
 
 // mapped host memory through which device-driven loops report progress
 int mapped_mailbox(int **host, int **dev) {
-    static int *h = nullptr, *d = nullptr;
+    thread_local int *h = nullptr, *d = nullptr;
     if (!h) {
         CPSD_TRY(cuda_check(cudaHostAlloc((void **)&h, 4096, cudaHostAllocMapped), "cudaHostAlloc(mapped)"));
         CPSD_TRY(cuda_check(cudaHostGetDevicePointer((void **)&d, h, 0), "mapped pointer"));
@@ -99,7 +100,7 @@ struct StepThrottle {
     }
 };
 StepThrottle &throttle() {
-    static StepThrottle t;
+    thread_local StepThrottle t;
     return t;
 }
 
@@ -686,16 +687,23 @@ int cpsd_eecpsd_roots(const cpsd_system *s, const cpsd_integrals *I, const cpsd_
     if (nroot <= 0) return CPSD_OK;
     IntegralScope keep(I);
     const i64 l1 = irpdso(symR, S.popv, S.popo, 1), l2 = idsymsoc(symR, S.popv, S.popv, 0, S.popo, S.popo, 0);
+    // roots per launch: all of them (batch_roots) unless their scratch
+    // (about 12 R2-sized and 8 R1-sized vectors and one (vo|vo) intermediate
+    // per root) does not fit in the memory left next to the integrals
+    i64 chunk = 1;
     if (p->batch_roots) {
-        i64 it = 0;
-        CPSD_TRY(ee_roots_batch(S, X, p, T2_1, J, symR, nroot, w0_host, L_dev, w_host, R2_1, R1_2, R2_2, &it));
-        if (solver_iters) *solver_iters = it;
-        return CPSD_OK;
+        const double per_root =
+            8.0 * (12.0 * (double)l2 + 8.0 * (double)l1 + 2.0 * (double)idsymsoc(symR, S.popv, S.popo, 1, S.popv, S.popo, 1));
+        size_t fr = 0, tot_mem = 0;
+        CPSD_TRY(cuda_check(cudaMemGetInfo(&fr, &tot_mem), "cudaMemGetInfo"));
+        const double avail = (double)fr + (double)arena().spare() + (double)pool_idle_bytes();
+        chunk = std::max<i64>(1, std::min<i64>(nroot, (i64)(0.7 * ctx().mem_share * avail / per_root)));
     }
     i64 tot = 0;
-    for (i64 r = 0; r < nroot; r++) {
+    for (i64 r = 0; r < nroot; r += chunk) {
+        const i64 nb = std::min(chunk, nroot - r);
         i64 it = 0;
-        CPSD_TRY(ee_roots_batch(S, X, p, T2_1, J, symR, 1, w0_host + r, L_dev + r * l1, w_host + 3 * r,
+        CPSD_TRY(ee_roots_batch(S, X, p, T2_1, J, symR, nb, w0_host + r, L_dev + r * l1, w_host + 3 * r,
                                 R2_1 ? R2_1 + r * l2 : nullptr, R1_2 ? R1_2 + r * l1 : nullptr,
                                 R2_2 ? R2_2 + r * l2 : nullptr, &it));
         tot += it;

@@ -214,7 +214,8 @@ int upload_vec(const std::vector<T> &v, T **d) {
     *d = nullptr;
     if (v.empty()) return CPSD_OK;
     CPSD_TRY(cuda_check(cudaMalloc(d, sizeof(T) * v.size()), "cudaMalloc(narrow plan)"));
-    return cuda_check(cudaMemcpy(*d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice), "upload narrow plan");
+    return cuda_check(cudaMemcpyAsync(*d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, stream()),
+                      "upload narrow plan");
 }
 
 }  // namespace
@@ -228,7 +229,7 @@ int NarrowPlan::upload() {
 }
 
 int plan_narrow(const ContractPlan *cp, const NarrowPlan **out) {
-    static std::map<const ContractPlan *, std::unique_ptr<NarrowPlan>> cache;
+    thread_local std::map<const ContractPlan *, std::unique_ptr<NarrowPlan>> cache;
     *out = nullptr;
     auto it = cache.find(cp);
     if (it != cache.end()) {

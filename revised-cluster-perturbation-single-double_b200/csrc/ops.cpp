@@ -8,6 +8,7 @@
 #include "ozaki.cuh"
 
 #include <cstring>
+#include <mutex>
 #include <string>
 
 namespace cpsd {
@@ -114,7 +115,7 @@ struct ConstOps {
     std::vector<DigEntry> dig;
 };
 ConstOps &const_ops() {
-    static ConstOps c;
+    thread_local ConstOps c;
     return c;
 }
 
@@ -125,11 +126,19 @@ struct PoolBuf {
     void *p;
     size_t bytes;
 };
+// The pool is shared by all host threads (concurrent molecules of a batch):
+// an idle buffer may serve any of them, and a thread short of memory gives
+// back every idle buffer.
 std::vector<PoolBuf> &pool_free() {
     static std::vector<PoolBuf> v;
     return v;
 }
+std::mutex &pool_mutex() {
+    static std::mutex m;
+    return m;
+}
 void *pool_get(size_t bytes) {
+    std::lock_guard<std::mutex> lock(pool_mutex());
     auto &f = pool_free();
     int best = -1;
     for (int i = 0; i < (int)f.size(); i++)
@@ -151,8 +160,27 @@ void *pool_get(size_t bytes) {
     return nullptr;
 }
 void pool_put(void *p, size_t bytes) {
-    if (p) pool_free().push_back({p, bytes});
+    if (!p) return;
+    std::lock_guard<std::mutex> lock(pool_mutex());
+    pool_free().push_back({p, bytes});
 }
+
+}  // namespace
+
+size_t pool_idle_bytes() {
+    std::lock_guard<std::mutex> lock(pool_mutex());
+    size_t t = 0;
+    for (const PoolBuf &b : pool_free()) t += b.bytes;
+    return t;
+}
+
+void pool_release_idle() {
+    std::lock_guard<std::mutex> lock(pool_mutex());
+    for (PoolBuf &b : pool_free()) cudaFree(b.p);
+    pool_free().clear();
+}
+
+namespace {
 
 bool is_const_operand(const double *a) {
     ConstOps &c = const_ops();
@@ -165,7 +193,7 @@ bool is_const_operand(const double *a) {
 int oz_error_word(int **err) {
     if (!ctx().oz_err) {
         CPSD_TRY(cuda_check(cudaMalloc(&ctx().oz_err, sizeof(int)), "cudaMalloc(error word)"));
-        CPSD_TRY(cuda_check(cudaMemset(ctx().oz_err, 0, sizeof(int)), "clear error word"));
+        CPSD_TRY(cuda_check(cudaMemsetAsync(ctx().oz_err, 0, sizeof(int), stream()), "clear error word"));
     }
     *err = ctx().oz_err;
     return CPSD_OK;
@@ -623,11 +651,13 @@ int cpsd_init(int64_t nirrep, const int64_t *dirprd) {
             if (c.dirprd[i - 1][j - 1] < 1 || c.dirprd[i - 1][j - 1] > nirrep)
                 return set_error(CPSD_EARG, "cpsd_init: invalid direct-product table");
     c.init = true;
-    c.launches = 0;
     return CPSD_OK;
 }
 
 int cpsd_set_stream(void *s) {
+    // plan tables are uploaded on the stream in use when a plan is first
+    // launched; finish those copies before kernels on another stream read them
+    if (ctx().stream != (cudaStream_t)s) CPSD_TRY(cuda_check(cudaStreamSynchronize(ctx().stream), "sync"));
     ctx().stream = (cudaStream_t)s;
     return CPSD_OK;
 }
@@ -671,8 +701,10 @@ int cpsd_set_mixed(int digits, double min_gflop) {
 int cpsd_mixed_error(int reset) {
     if (!ctx().oz_err) return 0;
     int h = 0;
-    CPSD_TRY(cuda_check(cudaMemcpy(&h, ctx().oz_err, sizeof h, cudaMemcpyDeviceToHost), "read error word"));
-    if (reset && h) CPSD_TRY(cuda_check(cudaMemset(ctx().oz_err, 0, sizeof(int)), "clear error word"));
+    CPSD_TRY(cuda_check(cudaMemcpyAsync(&h, ctx().oz_err, sizeof h, cudaMemcpyDeviceToHost, stream()), "read error word"));
+    CPSD_TRY(cuda_check(cudaStreamSynchronize(stream()), "sync"));
+    if (reset && h)
+        CPSD_TRY(cuda_check(cudaMemsetAsync(ctx().oz_err, 0, sizeof(int), stream()), "clear error word"));
     return h;
 }
 

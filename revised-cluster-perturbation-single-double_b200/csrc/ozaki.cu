@@ -22,6 +22,7 @@
 // MMAs, four warps read the accumulators back (tcgen05.ld) and scatter the
 // FP64 result through the output offset tables.  Every wait is bounded: on
 // a timeout the kernel records it in an error word and drains.
+#include <atomic>
 #include <cstdint>
 
 #include "ozaki.cuh"
@@ -355,10 +356,13 @@ __global__ void __launch_bounds__(256) k_oz_slice(const OzSliceJob *__restrict__
             if (row < jb.R) {
                 double x[16];
                 oz_load16(x, jb, src, roff, koff, kcombo, row, rcombo[jb.rcoff + row], (i64)kt * OZ_BK + k16 * 16);
-                const double sc = ldexp(1.0, -oz_expo(expo[jb.eoff + row]));
+                // 2^-e in two finite factors: a row whose largest element is
+                // below 2^-1022 has e < -1021 and 2^-e alone would overflow
+                const int e = oz_expo(expo[jb.eoff + row]);
+                const double sc1 = ldexp(1.0, -(e / 2)), sc2 = ldexp(1.0, -(e - e / 2));
 #pragma unroll
                 for (int q = 0; q < 16; q++) {
-                    double y = x[q] * sc;
+                    double y = x[q] * sc1 * sc2;
 #pragma unroll
                     for (int t = 0; t < S; t++) {
                         y *= 128.0;
@@ -381,7 +385,7 @@ template <int S, int BN>
 int oz_gemm_launch(const OzDevPlan &p, const int8_t *Adig, const int8_t *Bdig, const int *ea, const int *eb,
                    double *C, double alpha, int kt0, int kt1, int *err) {
     using Cf = OzCfg<S, BN>;
-    static bool attr = false;
+    static std::atomic<bool> attr{false};
     if (!attr) {
         CPSD_TRY(cuda_check(cudaFuncSetAttribute(k_oz_gemm<S, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cf::SMEM),
                             "oz smem attr"));

@@ -45,7 +45,8 @@ int upload_vec(const std::vector<T> &v, const T **d) {
     T *p = nullptr;
     CPSD_TRY(cuda_check(cudaMalloc(&p, sizeof(T) * v.size()), "cudaMalloc(digit plan)"));
     *d = p;
-    return cuda_check(cudaMemcpy(p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice), "upload digit plan");
+    return cuda_check(cudaMemcpyAsync(p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, stream()),
+                      "upload digit plan");
 }
 
 i64 roundup(i64 x, i64 m) { return (x + m - 1) / m * m; }
@@ -84,7 +85,7 @@ int OzPlan::upload() {
 }
 
 int plan_ozaki(const ContractPlan *cp, int S, const OzPlan **out) {
-    static std::map<std::pair<const ContractPlan *, int>, std::unique_ptr<OzPlan>> cache;
+    thread_local std::map<std::pair<const ContractPlan *, int>, std::unique_ptr<OzPlan>> cache;
     *out = nullptr;
     auto key = std::make_pair(cp, S);
     auto it = cache.find(key);

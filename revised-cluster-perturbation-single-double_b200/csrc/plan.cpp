@@ -28,7 +28,11 @@ int upload(const std::vector<T> &v, T **d) {
     *d = nullptr;
     if (v.empty()) return CPSD_OK;
     CPSD_TRY(cuda_check(cudaMalloc(d, sizeof(T) * v.size()), "cudaMalloc(plan)"));
-    return cuda_check(cudaMemcpy(*d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice), "upload plan");
+    // on the library stream: the kernels that read the tables are queued
+    // behind the copy on the same stream (a legacy-stream cudaMemcpy from
+    // pageable memory may still be in flight when it returns)
+    return cuda_check(cudaMemcpyAsync(*d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, stream()),
+                      "upload plan");
 }
 
 bool is_zorb(const i64 *p) {
@@ -77,7 +81,7 @@ int EnergyPlan::upload() {
 
 int plan_contract(const Desc &d1, const char *t1, const Desc &d2, const char *t2, const Desc &d3,
                   const char *t3, const Batch &batch, const ContractPlan **out) {
-    static std::map<std::string, std::unique_ptr<ContractPlan>> cache;
+    thread_local std::map<std::string, std::unique_ptr<ContractPlan>> cache;
     std::string key = d1.key() + t1 + d2.key() + t2 + d3.key() + t3 + "#" + std::to_string(batch.nb) + "," +
                       std::to_string(batch.strideA) + "," + std::to_string(batch.strideB) + "," +
                       std::to_string(batch.strideC) + "#" + std::to_string(ctx().nirrep);
@@ -478,7 +482,7 @@ i64 pair_off(const i64 *pp, const i64 *pq, i64 iop, i64 ip, i64 p, i64 iq, i64 q
 // PAIR_ANTI_COMPRESS (packed out = in(p,q)-in(q,p)), PAIR_SWAP (out(q,p)=in(p,q))
 int plan_pairmap(const Desc &din, int op0, int op1, i64 target_iop0, i64 target_iop1, Desc *dout_ret,
                  const PairMapPlan **out) {
-    static std::map<std::string, std::unique_ptr<PairMapPlan>> cache;
+    thread_local std::map<std::string, std::unique_ptr<PairMapPlan>> cache;
     Desc dout = din;
     int ops[2] = {op0, op1};
     i64 tgt[2] = {target_iop0, target_iop1};
@@ -572,7 +576,7 @@ int plan_pairmap(const Desc &din, int op0, int op1, i64 target_iop0, i64 target_
 
 // ----------------------------------------------------------- energies
 int plan_energy(const Desc &d, const char *kinds, const EnergyPlan **out) {
-    static std::map<std::string, std::unique_ptr<EnergyPlan>> cache;
+    thread_local std::map<std::string, std::unique_ptr<EnergyPlan>> cache;
     std::string key = d.key() + kinds + "#" + std::to_string(ctx().nirrep);
     auto it = cache.find(key);
     if (it != cache.end()) {

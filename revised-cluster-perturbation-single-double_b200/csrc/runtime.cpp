@@ -1,6 +1,7 @@
 // Context, errors, scratch arena and DPD size math of libcpsd_b200.
 #include "runtime.hpp"
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 
@@ -23,7 +24,7 @@ int cuda_check(cudaError_t e, const char *what) {
 }
 
 Context &ctx() {
-    static Context c;
+    thread_local Context c;
     return c;
 }
 
@@ -100,7 +101,7 @@ Desc desc_of(const cpsd_opt *t) {
 
 // ------------------------------------------------------------------ arena
 Arena &arena() {
-    static Arena a;
+    thread_local Arena a;
     return a;
 }
 
@@ -135,7 +136,8 @@ int Arena::alloc(size_t bytes, void **out) {
     }
     if (external)
         return set_error(CPSD_EMEM, "workspace too small: need " + std::to_string(bytes) + " more bytes");
-    size_t sz = bytes * 2;
+    // room for what follows: up to 1 GiB beyond the request (256 MiB at least)
+    size_t sz = bytes + std::min(bytes, (size_t)1 << 30);
     if (sz < ((size_t)256 << 20)) sz = (size_t)256 << 20;
     void *p = nullptr;
     if (cudaMalloc(&p, sz) != cudaSuccess) {
@@ -143,7 +145,11 @@ int Arena::alloc(size_t bytes, void **out) {
         sz = bytes;
         if (cudaMalloc(&p, sz) != cudaSuccess) {
             cudaGetLastError();
-            return set_error(CPSD_EMEM, "cudaMalloc of scratch failed (" + std::to_string(bytes) + " bytes)");
+            pool_release_idle();  // idle cached copies of earlier runs give way to scratch
+            if (cudaMalloc(&p, sz) != cudaSuccess) {
+                cudaGetLastError();
+                return set_error(CPSD_EMEM, "cudaMalloc of scratch failed (" + std::to_string(bytes) + " bytes)");
+            }
         }
     }
     chunks.push_back({(char *)p, sz, true});

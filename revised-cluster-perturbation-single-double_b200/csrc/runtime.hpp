@@ -38,6 +38,9 @@ struct Context {
     int oz_digits = 0;
     double oz_min_flops = 1e9;
     int *oz_err = nullptr;
+    // fraction of the free device memory this thread may plan its scratch
+    // for (molecules running side by side share it)
+    double mem_share = 1.0;
 };
 Context &ctx();
 inline i64 dp(i64 a, i64 b) { return ctx().dirprd[a - 1][b - 1]; }
@@ -90,8 +93,18 @@ struct Arena {
     }
     void set_external(void *p, size_t bytes);
     void free_all();
+    // bytes of the owned chunks not in use (reusable without cudaMalloc)
+    size_t spare() const {
+        size_t t = 0;
+        for (const Chunk &c : chunks) t += c.size;
+        return t > in_use ? t - in_use : 0;
+    }
 };
 Arena &arena();
+// frees the idle buffers of the device-buffer pool (constant-operand copies
+// kept between program runs)
+void pool_release_idle();
+size_t pool_idle_bytes();
 struct ScratchScope {
     Arena::Mark m;
     ScratchScope() : m(arena().mark()) {}

@@ -47,7 +47,7 @@ class System:
     """Orbital spaces, symmetry and integrals of one synthetic molecule."""
 
     def __init__(self, nmo, nocc_a, nocc_b, nirrep, seed=0, naux=None, roots=None,
-                 spin_flip=1, skip_abcd=False, run_opts=None):
+                 spin_flip=1, skip_abcd=False, run_opts=None, host_ints=True):
         self.nmo, self.nocc_a, self.nocc_b, self.nirrep = int(nmo), int(nocc_a), int(nocc_b), int(nirrep)
         # program keywords of this workload (CCSOINP keys of mod_common.f90)
         self.run_opts = dict(run_opts or {})
@@ -99,7 +99,7 @@ class System:
             else:
                 for h, n in dict(roots).items():
                     self.estate_sym[int(h) - 1] = int(n)
-        self._build(skip_abcd)
+        self._build(skip_abcd, host_ints)
 
     # DPD lengths of the integral tensors (iop = 0 on antisymmetric pairs)
     def lengths(self):
@@ -113,10 +113,10 @@ class System:
             "abcd": s.idsymsoc(1, v, v, 0, v, v, 0),
         }
 
-    def _build(self, skip_abcd):
+    def _build(self, skip_abcd, host_ints=True):
         lib = _load()
         lens = self.lengths()
-        self.ints = {k: np.zeros(n, np.float64) for k, n in lens.items()}
+        self.ints = {k: np.zeros(n, np.float64) if host_ints else None for k, n in lens.items()}
         if skip_abcd:
             self.ints["abcd"] = None
         self.eorb = np.zeros(int(self.popo.sum() + self.popv.sum()), np.float64)
@@ -175,6 +175,41 @@ class System:
         return self.sym.idsymsoc(sym, self.popv, self.popv, 0, self.popo, self.popo, 0)
 
 
+_SYNTH_DEV_SO = os.path.join(_HERE, "_build", "libcpsd_synth_dev.so")
+_dev_lib = None
+
+
+def device_integrals(s, keys=("ijkl", "ijka", "abij", "iabj", "abci", "abcd"), stream=None):
+    """The integral tensors of s built on the current CUDA device (float64
+    torch tensors; same values as the host build up to the summation order of
+    the (pq|rs) dot products) plus Eorb; for molecules whose integrals are
+    too large to assemble on the host (csrc/synth_dev.cu)."""
+    global _dev_lib
+    import torch
+    if _dev_lib is None:
+        if not os.path.exists(_SYNTH_DEV_SO):
+            raise RuntimeError(f"device generator not built: {_SYNTH_DEV_SO} (run __graft_entry__.build())")
+        _dev_lib = ctypes.CDLL(_SYNTH_DEV_SO)
+        _dev_lib.cpsd_synth_build_device.restype = ctypes.c_int
+    lens = s.lengths()
+    out = {k: torch.empty(lens[k], dtype=torch.float64, device="cuda") for k in keys}
+    L = torch.from_numpy(s.L).cuda()
+    st = stream if stream is not None else torch.cuda.current_stream()
+
+    def ptr(k):
+        return ctypes.c_void_p(out[k].data_ptr()) if k in out else None
+
+    rc = _dev_lib.cpsd_synth_build_device(
+        ctypes.c_int64(s.nmo), ctypes.c_int64(s.nirrep), _p(s.dirprd), _p(s.mo_irrep), ctypes.c_int64(s.nocc_a),
+        ctypes.c_int64(s.nocc_b), ctypes.c_int64(s.naux), _p(s.aux_irrep), ctypes.c_void_p(L.data_ptr()),
+        ptr("ijkl"), ptr("ijka"), ptr("abij"), ptr("iabj"), ptr("abci"), ptr("abcd"), ctypes.c_void_p(st.cuda_stream))
+    del L
+    if rc != 0:
+        raise RuntimeError(f"cpsd_synth_build_device failed: {rc}")
+    out["eorb"] = torch.from_numpy(s.eorb).cuda()
+    return out
+
+
 # named workloads (shapes of the benchmark configurations).  With these
 # random integrals the spin-flip CIS spectrum at nmo >= 200 has roots below
 # the guess energies, where the reference's default root tracking
@@ -191,6 +226,22 @@ CONFIGS = {
     # large EE run, D2h: nmo 400, nocc 20/18, 10 roots
     "d2h_nmo400": dict(nmo=400, nocc_a=20, nocc_b=18, nirrep=8, roots=10, run_opts={"lowest": 1}),
 }
+
+
+def batch_draw(n=64, seed=0):
+    """Shapes of the batching workload: n independent molecules with
+    nmo ~ U{60..240}, nocc_alpha ~ U{4..12}, nocc_beta = nocc_alpha - 2,
+    irrep count from {1, 2, 4, 8} and 4-8 roots (irrep 1) each; molecule k
+    uses generator seed 1000 + k."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        nmo = int(rng.integers(60, 241))
+        na = int(rng.integers(4, 13))
+        nirrep = int(rng.choice([1, 2, 4, 8]))
+        roots = int(rng.integers(4, 9))
+        out.append(dict(nmo=nmo, nocc_a=na, nocc_b=na - 2, nirrep=nirrep, roots=roots, seed=1000 + k))
+    return out
 
 
 def make(name, seed=0, **kw):
