@@ -555,6 +555,7 @@ def run_batch(args):
         tot += need(mols[i])
     waves.append(cur)
     res = {0: [None] * len(mols), args.digits: [None] * len(mols)}
+    wave_ms = []
     times = {0: 0.0, args.digits: 0.0}
     gen_s, launches = 0.0, {0: 0, args.digits: 0}
     for w in waves:
@@ -577,6 +578,7 @@ def run_batch(args):
             e1.record(stream)
             torch.cuda.synchronize()
             times[mode] += e0.elapsed_time(e1) / args.steps / 1e3
+            wave_ms.append(round(e0.elapsed_time(e1) / args.steps, 1))
             launches[mode] += api.launch_count(True) // max(args.steps, 1)
             for i, o in zip(w, out):
                 res[mode][i] = o
@@ -586,8 +588,15 @@ def run_batch(args):
         torch.cuda.empty_cache()
         api.release_device_cache()
     nroots = sum(s.nroots for s in mols)
-    dev = max(float(np.max(np.abs(np.asarray(a) - np.asarray(b))))
-              for i in range(len(mols)) for a, b in zip(res[args.digits][i], res[0][i]))
+    per = []
+    for i, s in enumerate(mols):
+        d = [float(np.max(np.abs(np.asarray(a) - np.asarray(b)))) for a, b in zip(res[args.digits][i], res[0][i])]
+        mag = [float(np.max(np.abs(np.asarray(b)))) for b in res[0][i]]
+        per.append({"molecule": i, "nmo": s.nmo, "nirrep": s.nirrep, "nocc_a": s.nocc_a, "roots": s.nroots,
+                    "dev_omega_w2_w3": d, "max_abs_omega_w2_w3": mag})
+    dev = max(max(p["dev_omega_w2_w3"]) for p in per)
+    rel = max(max(x / max(m, 1e-30) for x, m in zip(p["dev_omega_w2_w3"], p["max_abs_omega_w2_w3"])) for p in per)
+    worst = sorted(per, key=lambda p: -max(p["dev_omega_w2_w3"]))[:5]
     print(json.dumps({
         "case": "batch", "metric": METRIC, "unit": "roots/s", "dtype": "f64 (int8 digits)",
         "data": "synthetic (seeded generator, synth.batch_draw)",
@@ -601,7 +610,9 @@ def run_batch(args):
         "value": nroots / times[args.digits], "ms_total": 1e3 * times[args.digits],
         "fp64_path": {"value": nroots / times[0], "ms_total": 1e3 * times[0], "gpu_launches": launches[0]},
         "mixed_over_fp64": times[0] / times[args.digits],
-        "max_abs_dev_vs_fp64_eh": dev, "gpu_launches": launches[args.digits],
+        "max_abs_dev_vs_fp64_eh": dev, "max_rel_dev_vs_fp64": rel, "worst_molecules": worst,
+        "gpu_launches": launches[args.digits],
+        "wave_ms_mixed_fp64": [wave_ms[k:k + 2] for k in range(0, len(wave_ms), 2)],
         "steps": args.steps, "warmup": args.warmup, "device_generation_s": gen_s,
         "wall_s": time.time() - t_start,
         "roots_per_molecule": [[float(x) for x in res[args.digits][i][0]] for i in range(len(mols))][:3],

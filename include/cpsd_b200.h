@@ -341,8 +341,8 @@ int cpsd_pipeline_batch(int64_t nmol, const cpsd_system *s, const cpsd_integrals
 
 /* Gives back device memory the library keeps between calls: the idle
  * buffers of its constant-operand copies and the calling thread's scratch
- * arena now, the batch workers' arenas at their next job.  Later calls
- * allocate again as needed. */
+ * arena (batch workers free theirs at the end of every batch).  Later
+ * calls allocate again as needed. */
 int cpsd_release_device_cache(void);
 
 /* -------------------------------------------- SF-CIS(D) energy gradient

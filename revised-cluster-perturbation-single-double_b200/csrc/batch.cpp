@@ -64,13 +64,6 @@ Workers &workers() {
     return *w;
 }
 
-// cpsd_release_device_cache bumps the epoch; a worker frees its scratch
-// arena at its next job when the epoch moved since its last release
-std::atomic<int64_t> &trim_epoch() {
-    static std::atomic<int64_t> e{0};
-    return e;
-}
-
 // work estimate of a molecule: the particle-particle ladder, v^4 o^2 / nirrep
 double weight(const cpsd_system *s) {
     double o = 0, v = 0;
@@ -125,11 +118,6 @@ int cpsd_pipeline_batch(int64_t nmol, const cpsd_system *s, const cpsd_integrals
     const int64_t njobs = std::min<int64_t>(nworkers, nmol);
     for (int64_t j = 0; j < njobs; j++) {
         W.submit([&] {
-            thread_local int64_t trimmed = 0;
-            if (trimmed != trim_epoch().load()) {
-                trimmed = trim_epoch().load();
-                arena().free_all();
-            }
             Context &c = ctx();
             c.oz_digits = digits;
             c.oz_min_flops = min_flops;
@@ -144,6 +132,9 @@ int cpsd_pipeline_batch(int64_t nmol, const cpsd_system *s, const cpsd_integrals
                                    w3 + off[(size_t)m], &nr);
                 if (rc != CPSD_OK) next.store(nmol);  // stop handing out molecules
             }
+            // an idle worker keeps no scratch: the next batch may run its
+            // largest molecules on other workers
+            if (!arena().external) arena().free_all();
             std::lock_guard<std::mutex> lock(dm);
             if (rc != CPSD_OK && first_rc == CPSD_OK) {
                 first_rc = rc;
@@ -170,7 +161,6 @@ int cpsd_release_device_cache(void) {
     CPSD_TRY(cuda_check(cudaStreamSynchronize(stream()), "sync"));
     pool_release_idle();
     if (!arena().external) arena().free_all();
-    trim_epoch().fetch_add(1);
     return CPSD_OK;
 }
 

@@ -36,11 +36,24 @@ static int need_init() {
 
 namespace {
 int launch_ozaki(const OzPlan *oz, const double *A, const double *B, double *C, double alpha);
+void op_enter();
+void op_leave();
+// One outermost operation (an engine, wrapper or kernel call): the cached
+// constant-operand copies handed to it stay in place until it returns,
+// whatever it allocates meanwhile; copies of earlier operations may be
+// evicted when memory runs out.
+struct OpScope {
+    OpScope() { op_enter(); }
+    ~OpScope() { op_leave(); }
+    OpScope(const OpScope &) = delete;
+    OpScope &operator=(const OpScope &) = delete;
+};
 }
 
 int engine(const Ten &v1, const char *t1, const Ten &v2, const char *t2, Ten &v3, const char *t3, double f1,
            double f2, i64 nb) {
     CPSD_TRY(need_init());
+    OpScope op;
     Batch b;
     b.nb = nb;
     if (nb > 1) {
@@ -99,6 +112,7 @@ struct ExpEntry {
     Desc d;
     double *buf;
     size_t bytes;
+    int64_t used;  // operation (epoch) that was last handed this copy
 };
 // digit tiles (and their exponents) made of a constant operand
 struct DigEntry {
@@ -107,17 +121,26 @@ struct DigEntry {
     int8_t *dig;
     int *expo;
     size_t dbytes, ebytes;
+    int64_t used;
 };
 struct ConstOps {
     int depth = 0;
     std::vector<const double *> arrs;
     std::vector<ExpEntry> exp;
     std::vector<DigEntry> dig;
+    int64_t epoch = 0;  // outermost operations so far
+    int op_depth = 0;
 };
 ConstOps &const_ops() {
     thread_local ConstOps c;
     return c;
 }
+
+void op_enter() {
+    ConstOps &c = const_ops();
+    if (c.op_depth++ == 0) c.epoch++;
+}
+void op_leave() { const_ops().op_depth--; }
 
 // Device buffers of the constant-operand copies are kept after a program
 // run and reused by the next one (the same workload asks for the same
@@ -155,6 +178,7 @@ void *pool_get(size_t bytes) {
     cudaGetLastError();
     for (PoolBuf &b : f) cudaFree(b.p);  // out of memory: give back the idle buffers and retry
     f.clear();
+    arena().trim();  // and this thread's unused scratch chunks
     if (cudaMalloc(&p, bytes) == cudaSuccess) return p;
     cudaGetLastError();
     return nullptr;
@@ -190,6 +214,50 @@ bool is_const_operand(const double *a) {
     return false;
 }
 
+// Cached copies give way when device memory runs out: every copy the
+// running program keeps, except those handed to the operation in progress
+// and those made of `keep` (the operand being requested), goes back to the
+// pool once the stream has finished the kernels that read it, and the idle
+// pool is freed.  Returns false when there was nothing to evict.
+bool evict_const_except(const double *keep) {
+    ConstOps &c = const_ops();
+    auto kept_e = [&](const ExpEntry &e) { return e.used == c.epoch || e.src == keep || e.buf == keep; };
+    auto kept_d = [&](const DigEntry &e) { return e.used == c.epoch || e.src == keep; };
+    std::vector<ExpEntry> ke;
+    std::vector<DigEntry> kd;
+    std::vector<const double *> dropped;
+    for (const ExpEntry &e : c.exp)
+        if (kept_e(e)) ke.push_back(e);
+        else dropped.push_back(e.buf);
+    for (const DigEntry &e : c.dig)
+        if (kept_d(e)) kd.push_back(e);
+    if (ke.size() == c.exp.size() && kd.size() == c.dig.size()) return false;
+    cudaStreamSynchronize(stream());
+    for (const ExpEntry &e : c.exp)
+        if (!kept_e(e)) pool_put(e.buf, e.bytes);
+    for (const DigEntry &e : c.dig)
+        if (!kept_d(e)) {
+            pool_put(e.dig, e.dbytes);
+            pool_put(e.expo, e.ebytes);
+        }
+    c.exp.swap(ke);
+    c.dig.swap(kd);
+    // an evicted expanded copy is no longer a constant operand
+    c.arrs.erase(std::remove_if(c.arrs.begin(), c.arrs.end(),
+                                [&](const double *x) {
+                                    return std::find(dropped.begin(), dropped.end(), x) != dropped.end();
+                                }),
+                 c.arrs.end());
+    pool_release_idle();
+    return true;
+}
+
+}  // namespace
+
+bool evict_cached_copies() { return evict_const_except(nullptr); }
+
+namespace {
+
 int oz_error_word(int **err) {
     if (!ctx().oz_err) {
         CPSD_TRY(cuda_check(cudaMalloc(&ctx().oz_err, sizeof(int)), "cudaMalloc(error word)"));
@@ -214,8 +282,9 @@ int digits_of(const OzPlan *oz, bool sideA, const double *src, int8_t **dig, int
     const i64 bytes = sideA ? oz->adig : oz->bdig, ne = sideA ? oz->nea : oz->neb;
     if (is_const_operand(src)) {
         ConstOps &c = const_ops();
-        for (const DigEntry &e : c.dig)
+        for (DigEntry &e : c.dig)
             if (e.src == src && e.hash == h) {
+                e.used = c.epoch;
                 *dig = e.dig;
                 *expo = e.expo;
                 return CPSD_OK;
@@ -223,8 +292,16 @@ int digits_of(const OzPlan *oz, bool sideA, const double *src, int8_t **dig, int
         const size_t db = (size_t)std::max<i64>(bytes, 16), eb = sizeof(int) * (size_t)std::max<i64>(ne, 1);
         int8_t *d = (int8_t *)pool_get(db);
         int *x = d ? (int *)pool_get(eb) : nullptr;
+        if (!(d && x)) {
+            pool_put(d, db);
+            d = nullptr;
+            if (evict_const_except(src)) {
+                d = (int8_t *)pool_get(db);
+                x = d ? (int *)pool_get(eb) : nullptr;
+            }
+        }
         if (d && x) {
-            c.dig.push_back({src, h, d, x, db, eb});
+            c.dig.push_back({src, h, d, x, db, eb, c.epoch});
             *dig = d;
             *expo = x;
             return slice_timed(oz, sideA, src, d, x);
@@ -259,8 +336,9 @@ int expand_cached(const Ten &v, bool e0, bool e1, Ten *out, bool *done) {
     for (const double *a : c.arrs) is_const |= (a == v.arr);
     if (!is_const) return CPSD_OK;
     std::string key = v.d.key() + (e0 ? "E" : "-") + (e1 ? "E" : "-");
-    for (const ExpEntry &e : c.exp)
+    for (ExpEntry &e : c.exp)
         if (e.src == v.arr && e.key == key) {
+            e.used = c.epoch;
             *out = v;
             out->d = e.d;
             out->arr = e.buf;
@@ -272,8 +350,9 @@ int expand_cached(const Ten &v, bool e0, bool e1, Ten *out, bool *done) {
     CPSD_TRY(plan_pairmap(v.d, e0 ? PAIR_EXPAND : PAIR_ID, e1 ? PAIR_EXPAND : PAIR_ID, 1, 1, &d, &pm));
     const size_t bytes = sizeof(double) * (size_t)std::max<i64>(d.len(), 1);
     double *buf = (double *)pool_get(bytes);
+    if (!buf && evict_const_except(v.arr)) buf = (double *)pool_get(bytes);
     if (!buf) return CPSD_OK;  // no room to keep it: expand into scratch as usual
-    c.exp.push_back({v.arr, key, d, buf, bytes});
+    c.exp.push_back({v.arr, key, d, buf, bytes, c.epoch});
     c.arrs.push_back(buf);  // derived from a constant operand: constant too
     CPSD_TRY(launch_pairmap(pm, v.arr, buf, 1.0, 0.0, 1, 0, d.len()));
     *out = v;
@@ -346,6 +425,7 @@ ConstOperands::~ConstOperands() {
 // vv2v_444 (src/lib_cc/mod_contract.f90:10-162): v3 += fact * P1 P2 {v1 v2}
 int w444(const Ten &v1, const Ten &v2, Ten &v3, double fact, const char *t1, const char *t2, const char *t3,
          i64 anti, i64 nb) {
+    OpScope op;
     if (anti < 0 || anti > 3) return set_error(CPSD_EARG, "vv2v_444: anti must be 0..3");
     const char pair[6][2] = {{t1[0], t1[1]}, {t1[2], t1[3]}, {t2[0], t2[1]},
                              {t2[2], t2[3]}, {t3[0], t3[1]}, {t3[2], t3[3]}};
@@ -377,6 +457,7 @@ int w444(const Ten &v1, const Ten &v2, Ten &v3, double fact, const char *t1, con
 // vv2v_424 (src/lib_cc/mod_contract.f90:220-367)
 int w424(const Ten &v1, const Ten &v2, Ten &v3, double fact, const char *t1, const char *t2, const char *t3,
          i64 anti, i64 nb) {
+    OpScope op;
     if (anti < 0 || anti > 2) return set_error(CPSD_EARG, "vv2v_424: anti must be 0..2");
     const char pair[4][2] = {{t1[0], t1[1]}, {t1[2], t1[3]}, {t3[0], t3[1]}, {t3[2], t3[3]}};
     i64 iop[4] = {v1.d.iop[0], v1.d.iop[1], v3.d.iop[0], v3.d.iop[1]};
@@ -408,6 +489,7 @@ int w424(const Ten &v1, const Ten &v2, Ten &v3, double fact, const char *t1, con
 // vv2v_442 (src/lib_cc/mod_contract.f90:369-455)
 int w442(const Ten &v1, const Ten &v2, Ten &v3, double fact, const char *t1, const char *t2, const char *t3,
          i64 nb) {
+    OpScope op;
     const char pair[4][2] = {{t1[0], t1[1]}, {t1[2], t1[3]}, {t2[0], t2[1]}, {t2[2], t2[3]}};
     i64 iop[4] = {v1.d.iop[0], v1.d.iop[1], v2.d.iop[0], v2.d.iop[1]};
     bool iexp[4] = {};
@@ -463,6 +545,7 @@ int w224(const Ten &v1, const Ten &v2, Ten &v3, double fact, const char *t1, con
 // expansion by antisymmetrise-and-compress.  One copy (nb = 1).
 int vjp444(const Ten &v1, const Ten &v2, const Ten &Y, Ten &G, int which, double fact, const char *t1,
            const char *t2, const char *t3, i64 anti) {
+    OpScope op;
     if (anti < 0 || anti > 3) return set_error(CPSD_EARG, "vjp444: anti must be 0..3");
     if (which != 0 && which != 1) return set_error(CPSD_EARG, "vjp444: operand must be 0 or 1");
     const char pair[6][2] = {{t1[0], t1[1]}, {t1[2], t1[3]}, {t2[0], t2[1]},
@@ -569,6 +652,7 @@ int k_Wkbij_r2ijka(Ten &W, const Ten &r2, const Ten &V, double f, i64 nb) {
 }
 // Wkbij_r2abci.f90:3-43: tmp(ij,bk) = -.5 V(cd,bk) r(cd,ij); W(ij,kb) += tmp(ij,bk)
 int k_Wkbij_r2abci(Ten &W, const Ten &r2, const Ten &V, double f, i64 nb) {
+    OpScope op;
     ScratchScope sc;
     Ten tmp = W;
     std::swap(tmp.d.pop[2], tmp.d.pop[3]);

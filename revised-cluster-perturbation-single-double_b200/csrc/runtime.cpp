@@ -119,6 +119,13 @@ void Arena::free_all() {
     external = false;
 }
 
+void Arena::trim() {
+    while (chunks.size() > cur_chunk + 1 && chunks.back().owned) {
+        cudaFree(chunks.back().base);
+        chunks.pop_back();
+    }
+}
+
 int Arena::alloc(size_t bytes, void **out) {
     bytes = (bytes + 255) & ~(size_t)255;
     while (cur_chunk < chunks.size()) {
@@ -148,7 +155,12 @@ int Arena::alloc(size_t bytes, void **out) {
             pool_release_idle();  // idle cached copies of earlier runs give way to scratch
             if (cudaMalloc(&p, sz) != cudaSuccess) {
                 cudaGetLastError();
-                return set_error(CPSD_EMEM, "cudaMalloc of scratch failed (" + std::to_string(bytes) + " bytes)");
+                // then the copies this run keeps for later operations
+                if (!evict_cached_copies() || cudaMalloc(&p, sz) != cudaSuccess) {
+                    cudaGetLastError();
+                    return set_error(CPSD_EMEM,
+                                     "cudaMalloc of scratch failed (" + std::to_string(bytes) + " bytes)");
+                }
             }
         }
     }

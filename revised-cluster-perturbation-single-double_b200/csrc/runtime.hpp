@@ -93,6 +93,9 @@ struct Arena {
     }
     void set_external(void *p, size_t bytes);
     void free_all();
+    // frees the owned chunks past the allocation frontier (nothing there is
+    // allocated; cudaFree waits for kernels still reading released scratch)
+    void trim();
     // bytes of the owned chunks not in use (reusable without cudaMalloc)
     size_t spare() const {
         size_t t = 0;
@@ -104,6 +107,9 @@ Arena &arena();
 // frees the idle buffers of the device-buffer pool (constant-operand copies
 // kept between program runs)
 void pool_release_idle();
+// frees the constant-operand copies a program keeps that the operation in
+// progress was not handed (false: nothing to free)
+bool evict_cached_copies();
 size_t pool_idle_bytes();
 struct ScratchScope {
     Arena::Mark m;
