@@ -556,7 +556,6 @@ def run_batch(args):
     waves.append(cur)
     res = {0: [None] * len(mols), args.digits: [None] * len(mols)}
     wave_ms = []
-    wave_ms = []
     times = {0: 0.0, args.digits: 0.0}
     gen_s, launches = 0.0, {0: 0, args.digits: 0}
     for w in waves:
@@ -579,7 +578,6 @@ def run_batch(args):
             e1.record(stream)
             torch.cuda.synchronize()
             times[mode] += e0.elapsed_time(e1) / args.steps / 1e3
-            wave_ms.append(round(e0.elapsed_time(e1) / args.steps, 1))
             wave_ms.append(round(e0.elapsed_time(e1) / args.steps, 1))
             launches[mode] += api.launch_count(True) // max(args.steps, 1)
             for i, o in zip(w, out):
@@ -614,7 +612,6 @@ def run_batch(args):
         "mixed_over_fp64": times[0] / times[args.digits],
         "max_abs_dev_vs_fp64_eh": dev, "max_rel_dev_vs_fp64": rel, "worst_molecules": worst,
         "gpu_launches": launches[args.digits],
-        "wave_ms_mixed_fp64": [wave_ms[k:k + 2] for k in range(0, len(wave_ms), 2)],
         "wave_ms_mixed_fp64": [wave_ms[k:k + 2] for k in range(0, len(wave_ms), 2)],
         "steps": args.steps, "warmup": args.warmup, "device_generation_s": gen_s,
         "wall_s": time.time() - t_start,

@@ -10,6 +10,7 @@
 // there are too few rows to fill the GPU.  Both use the planner's task /
 // segment tables of the grouped contraction, so every layout that the
 // tensor-core path handles is handled here too.
+#include <mutex>
 #include <algorithm>
 #include <map>
 #include <memory>
@@ -221,15 +222,21 @@ int upload_vec(const std::vector<T> &v, T **d) {
 }  // namespace
 
 int NarrowPlan::upload() {
-    if (uploaded) return CPSD_OK;
+    if (uploaded.load(std::memory_order_acquire)) return CPSD_OK;
+    std::lock_guard<std::mutex> lock(upload_mutex());
+    if (uploaded.load(std::memory_order_relaxed)) return CPSD_OK;
     CPSD_TRY(upload_vec(items, &d_items));
     CPSD_TRY(upload_vec(reds, &d_reds));
-    uploaded = true;
+    // the tables may next be read by kernels on another thread's stream
+    CPSD_TRY(cuda_check(cudaStreamSynchronize(stream()), "plan upload"));
+    uploaded.store(true, std::memory_order_release);
     return CPSD_OK;
 }
 
 int plan_narrow(const ContractPlan *cp, const NarrowPlan **out) {
-    thread_local std::map<const ContractPlan *, std::unique_ptr<NarrowPlan>> cache;
+    static std::mutex m;
+    std::lock_guard<std::mutex> lock(m);
+    static std::map<const ContractPlan *, std::unique_ptr<NarrowPlan>> cache;
     *out = nullptr;
     auto it = cache.find(cp);
     if (it != cache.end()) {

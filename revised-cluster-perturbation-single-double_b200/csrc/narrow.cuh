@@ -3,6 +3,7 @@
 // CIS and of the R1 solver, one-index intermediates.  Tensor-core tiles would
 // be mostly padding there; these kernels stream the wide operand once.
 #pragma once
+#include <atomic>
 #include "runtime.hpp"
 
 namespace cpsd {
@@ -29,7 +30,7 @@ struct NarrowPlan {
     std::vector<NarrowItem> items;
     std::vector<NarrowRed> reds;
     i64 nparts = 0;
-    bool uploaded = false;
+    std::atomic<bool> uploaded{false};
     NarrowItem *d_items = nullptr;
     NarrowRed *d_reds = nullptr;
     int upload();

@@ -1,6 +1,7 @@
 // Sliced-integer (int8 digit) contraction on tcgen05: device tables and
 // launchers.  See ozaki.cu for the method.
 #pragma once
+#include <atomic>
 #include "runtime.hpp"
 
 namespace cpsd {
@@ -62,7 +63,7 @@ struct OzPlan {
     i64 kmin = 0;                // shortest contracted length of a group
     uint64_t ahash = 0, bhash = 0;  // layout signatures of the A / B digits
     // device copies (uploaded at the first launch)
-    bool uploaded = false;
+    std::atomic<bool> uploaded{false};
     OzDevPlan dev;
     OzSideDev adev, bdev;
     int upload();

@@ -10,6 +10,7 @@
 // and strides depend on the irreps of letters of both indices), hence the
 // per-combination tables: element (r, k) of A_g is at
 // roff[r][kcombo(k)] + koff[k][rcombo(r)], and C likewise.
+#include <mutex>
 #include <algorithm>
 #include <map>
 #include <memory>
@@ -54,7 +55,9 @@ i64 roundup(i64 x, i64 m) { return (x + m - 1) / m * m; }
 }  // namespace
 
 int OzPlan::upload() {
-    if (uploaded) return CPSD_OK;
+    if (uploaded.load(std::memory_order_acquire)) return CPSD_OK;
+    std::lock_guard<std::mutex> lock(upload_mutex());
+    if (uploaded.load(std::memory_order_relaxed)) return CPSD_OK;
     CPSD_TRY(upload_vec(tiles, &dev.tiles));
     CPSD_TRY(upload_vec(groups, &dev.groups));
     CPSD_TRY(upload_vec(crow, &dev.crow));
@@ -80,12 +83,16 @@ int OzPlan::upload() {
     bdev.njobs = (int)bjobs.size();
     bdev.rcombo = dev.ncombo;
     bdev.kcombo = kc;
-    uploaded = true;
+    // the tables may next be read by kernels on another thread's stream
+    CPSD_TRY(cuda_check(cudaStreamSynchronize(stream()), "plan upload"));
+    uploaded.store(true, std::memory_order_release);
     return CPSD_OK;
 }
 
 int plan_ozaki(const ContractPlan *cp, int S, const OzPlan **out) {
-    thread_local std::map<std::pair<const ContractPlan *, int>, std::unique_ptr<OzPlan>> cache;
+    static std::mutex m;
+    std::lock_guard<std::mutex> lock(m);
+    static std::map<std::pair<const ContractPlan *, int>, std::unique_ptr<OzPlan>> cache;
     *out = nullptr;
     auto key = std::make_pair(cp, S);
     auto it = cache.find(key);

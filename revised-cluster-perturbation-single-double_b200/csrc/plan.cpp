@@ -10,6 +10,7 @@
 // and iop in both operands) is one composite index, which reproduces the
 // reference's fast path, and every other letter is addressed by stride,
 // which reproduces its fallback.
+#include <mutex>
 #include <algorithm>
 #include <cstring>
 #include <functional>
@@ -54,34 +55,48 @@ struct Unit {
 }  // namespace
 
 int ContractPlan::upload() {
-    if (uploaded) return CPSD_OK;
+    if (uploaded.load(std::memory_order_acquire)) return CPSD_OK;
+    std::lock_guard<std::mutex> lock(upload_mutex());
+    if (uploaded.load(std::memory_order_relaxed)) return CPSD_OK;
     CPSD_TRY(cpsd::upload(h_tasks, &d_tasks));
     CPSD_TRY(cpsd::upload(h_segs, &d_segs));
     CPSD_TRY(cpsd::upload(h_tiles, &d_tiles));
     CPSD_TRY(cpsd::upload(h_reduce, &d_reduce));
-    uploaded = true;
+    // the tables may next be read by kernels on another thread's stream
+    CPSD_TRY(cuda_check(cudaStreamSynchronize(stream()), "plan upload"));
+    uploaded.store(true, std::memory_order_release);
     return CPSD_OK;
 }
 int PairMapPlan::upload() {
-    if (uploaded) return CPSD_OK;
+    if (uploaded.load(std::memory_order_acquire)) return CPSD_OK;
+    std::lock_guard<std::mutex> lock(upload_mutex());
+    if (uploaded.load(std::memory_order_relaxed)) return CPSD_OK;
     CPSD_TRY(cpsd::upload(h_blocks, &d_blocks));
     CPSD_TRY(cpsd::upload(h_idx, &d_idx));
     CPSD_TRY(cpsd::upload(h_sgn, &d_sgn));
-    uploaded = true;
+    // the tables may next be read by kernels on another thread's stream
+    CPSD_TRY(cuda_check(cudaStreamSynchronize(stream()), "plan upload"));
+    uploaded.store(true, std::memory_order_release);
     return CPSD_OK;
 }
 int EnergyPlan::upload() {
-    if (uploaded) return CPSD_OK;
+    if (uploaded.load(std::memory_order_acquire)) return CPSD_OK;
+    std::lock_guard<std::mutex> lock(upload_mutex());
+    if (uploaded.load(std::memory_order_relaxed)) return CPSD_OK;
     CPSD_TRY(cpsd::upload(h_blk, &d_blk));
     CPSD_TRY(cpsd::upload(h_lidx, &d_lidx));
     CPSD_TRY(cpsd::upload(h_ridx, &d_ridx));
-    uploaded = true;
+    // the tables may next be read by kernels on another thread's stream
+    CPSD_TRY(cuda_check(cudaStreamSynchronize(stream()), "plan upload"));
+    uploaded.store(true, std::memory_order_release);
     return CPSD_OK;
 }
 
 int plan_contract(const Desc &d1, const char *t1, const Desc &d2, const char *t2, const Desc &d3,
                   const char *t3, const Batch &batch, const ContractPlan **out) {
-    thread_local std::map<std::string, std::unique_ptr<ContractPlan>> cache;
+    static std::mutex m;
+    std::lock_guard<std::mutex> lock(m);
+    static std::map<std::string, std::unique_ptr<ContractPlan>> cache;
     std::string key = d1.key() + t1 + d2.key() + t2 + d3.key() + t3 + "#" + std::to_string(batch.nb) + "," +
                       std::to_string(batch.strideA) + "," + std::to_string(batch.strideB) + "," +
                       std::to_string(batch.strideC) + "#" + std::to_string(ctx().nirrep);
@@ -482,7 +497,9 @@ i64 pair_off(const i64 *pp, const i64 *pq, i64 iop, i64 ip, i64 p, i64 iq, i64 q
 // PAIR_ANTI_COMPRESS (packed out = in(p,q)-in(q,p)), PAIR_SWAP (out(q,p)=in(p,q))
 int plan_pairmap(const Desc &din, int op0, int op1, i64 target_iop0, i64 target_iop1, Desc *dout_ret,
                  const PairMapPlan **out) {
-    thread_local std::map<std::string, std::unique_ptr<PairMapPlan>> cache;
+    static std::mutex m;
+    std::lock_guard<std::mutex> lock(m);
+    static std::map<std::string, std::unique_ptr<PairMapPlan>> cache;
     Desc dout = din;
     int ops[2] = {op0, op1};
     i64 tgt[2] = {target_iop0, target_iop1};
@@ -576,7 +593,9 @@ int plan_pairmap(const Desc &din, int op0, int op1, i64 target_iop0, i64 target_
 
 // ----------------------------------------------------------- energies
 int plan_energy(const Desc &d, const char *kinds, const EnergyPlan **out) {
-    thread_local std::map<std::string, std::unique_ptr<EnergyPlan>> cache;
+    static std::mutex m;
+    std::lock_guard<std::mutex> lock(m);
+    static std::map<std::string, std::unique_ptr<EnergyPlan>> cache;
     std::string key = d.key() + kinds + "#" + std::to_string(ctx().nirrep);
     auto it = cache.find(key);
     if (it != cache.end()) {

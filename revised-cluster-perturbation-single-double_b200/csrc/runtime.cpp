@@ -99,6 +99,11 @@ Desc desc_of(const cpsd_opt *t) {
     return make_desc(t->popp, t->popq, t->popr, t->pops, t->ioppq, t->ioprs, t->sym);
 }
 
+std::mutex &upload_mutex() {
+    static std::mutex m;
+    return m;
+}
+
 // ------------------------------------------------------------------ arena
 Arena &arena() {
     thread_local Arena a;

@@ -1,6 +1,8 @@
 // Internal runtime of libcpsd_b200: symmetry context, device scratch arena,
 // DPD descriptors and the execution plans built by the host planner.
 #pragma once
+#include <mutex>
+#include <atomic>
 #include <cstddef>
 #include <cstdint>
 #include <string>
@@ -104,6 +106,9 @@ struct Arena {
     }
 };
 Arena &arena();
+// serialises the first upload of each cached plan's device tables (plans
+// are shared by all host threads)
+std::mutex &upload_mutex();
 // frees the idle buffers of the device-buffer pool (constant-operand copies
 // kept between program runs)
 void pool_release_idle();
@@ -157,7 +162,7 @@ struct ContractPlan {
     std::vector<SegDev> h_segs;
     std::vector<TileDev> h_tiles;
     std::vector<int> h_reduce;
-    bool uploaded = false;
+    std::atomic<bool> uploaded{false};
     TaskDev *d_tasks = nullptr;
     SegDev *d_segs = nullptr;
     TileDev *d_tiles = nullptr;
@@ -189,7 +194,7 @@ struct PairMapPlan {
     std::vector<PMBlockDev> h_blocks;
     std::vector<long long> h_idx;
     std::vector<double> h_sgn;
-    bool uploaded = false;
+    std::atomic<bool> uploaded{false};
     PMBlockDev *d_blocks = nullptr;
     long long *d_idx = nullptr;  // index maps (terms interleaved)
     double *d_sgn = nullptr;
@@ -228,7 +233,7 @@ struct EnergyPlan {
     i64 n = 0;
     int nblocks = 0;
     std::vector<i64> h_blk, h_lidx, h_ridx;
-    bool uploaded = false;
+    std::atomic<bool> uploaded{false};
     i64 *d_blk = nullptr;      // per block: base, nl, nr, lpair offset, rpair offset
     i64 *d_lidx = nullptr;     // per left pair: eorb index of p, q (-1 = none)
     i64 *d_ridx = nullptr;     // per right pair: eorb index of r, s (-1 = none)
