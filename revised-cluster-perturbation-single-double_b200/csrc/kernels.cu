@@ -12,36 +12,78 @@ namespace cpsd {
 
 namespace {
 
-__global__ void k_pairmap(const PMBlockDev *__restrict__ blocks, int nblocks, i64 total,
-                          const long long *__restrict__ idx, const double *__restrict__ sgn, int lt, int rt,
-                          const double *__restrict__ in0, double *__restrict__ out0, double alpha, double beta,
-                          i64 nb, i64 sin, i64 sout) {
-    for (i64 g = (i64)blockIdx.x * blockDim.x + threadIdx.x; g < total * nb; g += (i64)gridDim.x * blockDim.x) {
-        i64 cpy = g / total, e = g - cpy * total;
+// Each CTA covers PM_TILE consecutive output elements of one copy: thread t
+// handles e0 + t + PM_T j (j < PM_PER), so the stores of a warp stay
+// coalesced; the block, column r and row l of its first element come from
+// one search and one division, the later ones by stepping l (a division
+// again only at a block boundary or in blocks narrower than PM_T rows).
+constexpr int PM_T = 256, PM_PER = 8, PM_TILE = PM_T * PM_PER;
+
+__device__ __forceinline__ int pm_block(const PMBlockDev *__restrict__ blocks, int nblocks, i64 e) {
+    int b = 0, hi = nblocks - 1;  // last block starting at or before e
+    while (b < hi) {
+        const int mid = (b + hi + 1) >> 1;
+        if (blocks[mid].start <= e) b = mid;
+        else hi = mid - 1;
+    }
+    return b;
+}
+
+__global__ void __launch_bounds__(PM_T) k_pairmap(const PMBlockDev *__restrict__ blocks, int nblocks, i64 total,
+                                                  const long long *__restrict__ idx, const double *__restrict__ sgn,
+                                                  int lt, int rt, const double *__restrict__ in0,
+                                                  double *__restrict__ out0, double alpha, double beta, i64 nb,
+                                                  i64 sin, i64 sout) {
+    const i64 tiles = (total + PM_TILE - 1) / PM_TILE;
+    for (i64 tile = blockIdx.x; tile < tiles * nb; tile += gridDim.x) {
+        const i64 cpy = tile / tiles;
+        const i64 e0 = (tile - cpy * tiles) * PM_TILE + threadIdx.x;
+        if (e0 >= total) continue;
         const double *in = in0 + cpy * sin;
         double *out = out0 + cpy * sout;
-        int b = 0, hi = nblocks - 1;  // last block starting at or before e
-        while (b < hi) {
-            const int mid = (b + hi + 1) >> 1;
-            if (blocks[mid].start <= e) b = mid;
-            else hi = mid - 1;
-        }
-        const PMBlockDev &B = blocks[b];
-        i64 loc = e - B.start;
-        i64 r = loc / B.nlo, l = loc - r * B.nlo;
-        double v = 0.0;
-        for (int tr = 0; tr < rt; tr++) {
-            i64 ri = idx[B.rmap + r * rt + tr];
-            if (ri < 0) continue;
-            double sr = sgn[B.rmap + r * rt + tr];
-            for (int tq = 0; tq < lt; tq++) {
-                i64 li = idx[B.lmap + l * lt + tq];
-                if (li < 0) continue;
-                v += sr * sgn[B.lmap + l * lt + tq] * in[B.inBase + ri * B.nli + li];
+        int b = pm_block(blocks, nblocks, e0);
+        PMBlockDev B = blocks[b];
+        i64 next = b + 1 < nblocks ? blocks[b + 1].start : total;
+        i64 r = (e0 - B.start) / B.nlo, l = (e0 - B.start) - r * B.nlo;
+        for (int j = 0; j < PM_PER; j++) {
+            const i64 e = e0 + (i64)j * PM_T;
+            if (e >= total) break;
+            if (j > 0) {
+                if (e >= next) {
+                    while (e >= next) {
+                        b++;
+                        next = b + 1 < nblocks ? blocks[b + 1].start : total;
+                    }
+                    B = blocks[b];
+                    r = (e - B.start) / B.nlo;
+                    l = (e - B.start) - r * B.nlo;
+                } else {
+                    l += PM_T;
+                    if (l >= B.nlo) {
+                        if (B.nlo >= PM_T) {
+                            l -= B.nlo;
+                            r++;
+                        } else {
+                            r = (e - B.start) / B.nlo;
+                            l = (e - B.start) - r * B.nlo;
+                        }
+                    }
+                }
             }
+            double v = 0.0;
+            for (int tr = 0; tr < rt; tr++) {
+                const i64 ri = idx[B.rmap + r * rt + tr];
+                if (ri < 0) continue;
+                const double sr = sgn[B.rmap + r * rt + tr];
+                for (int tq = 0; tq < lt; tq++) {
+                    const i64 li = idx[B.lmap + l * lt + tq];
+                    if (li < 0) continue;
+                    v += sr * sgn[B.lmap + l * lt + tq] * in[B.inBase + ri * B.nli + li];
+                }
+            }
+            const i64 o = B.outBase + r * B.nlo + l;
+            out[o] = (beta == 0.0) ? alpha * v : beta * out[o] + alpha * v;
         }
-        i64 o = B.outBase + r * B.nlo + l;
-        out[o] = (beta == 0.0) ? alpha * v : beta * out[o] + alpha * v;
     }
 }
 
@@ -196,7 +238,9 @@ int launch_pairmap(const PairMapPlan *p, const double *in, double *out, double a
     CPSD_TRY(const_cast<PairMapPlan *>(p)->upload());
     cudaEvent_t end;
     CPSD_TRY(timing_begin(0.0, p->total, nb, p->lterms * p->rterms, 40, &end));
-    k_pairmap<<<grid_for(p->total * nb), 256, 0, stream()>>>(p->d_blocks, p->nblocks, p->total, p->d_idx, p->d_sgn,
+    const i64 tiles = (p->total + PM_TILE - 1) / PM_TILE * nb;
+    k_pairmap<<<(unsigned)std::min<i64>(tiles, 148 * 16), PM_T, 0, stream()>>>(p->d_blocks, p->nblocks, p->total,
+                                                                              p->d_idx, p->d_sgn,
                                                              p->lterms, p->rterms, in, out, alpha, beta, nb,
                                                              in_stride, out_stride);
     count_launch();
