@@ -21,14 +21,16 @@ namespace {
 constexpr int NT = 256, BK = 16, PAD = 4;
 
 __device__ __forceinline__ i64 decode1(i64 x, int n, const i64 *ext, const i64 *st) {
+    // the last unit takes the remaining quotient whole (x < its extent), so
+    // it needs no division; the others divide in 32 bits when both fit
     i64 off = 0;
-    for (int u = 0; u < n; u++) {
-        i64 e = ext[u];
-        i64 q = x / e;
+    for (int u = 0; u < n - 1; u++) {
+        const i64 e = ext[u];
+        const i64 q = (x <= 0x7fffffffLL && e <= 0x7fffffffLL) ? (i64)((unsigned)x / (unsigned)e) : x / e;
         off += (x - q * e) * st[u];
         x = q;
     }
-    return off;
+    return n > 0 ? off + x * st[n - 1] : off;
 }
 
 __device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
@@ -91,11 +93,18 @@ __global__ void __launch_bounds__(NT, 2) k_contract(const double *__restrict__ A
                 i64 k = kb + (i64)s * BK + tid;
                 if (k < ke) {
                     i64 a = 0, b = 0, x = k;
-                    for (int u = 0; u < sg.nk; u++) {
-                        i64 e = sg.kExt[u], q = x / e, r = x - q * e;
+                    for (int u = 0; u < sg.nk - 1; u++) {
+                        const i64 e = sg.kExt[u];
+                        const i64 q = (x <= 0x7fffffffLL && e <= 0x7fffffffLL) ? (i64)((unsigned)x / (unsigned)e)
+                                                                               : x / e;
+                        const i64 r = x - q * e;
                         a += r * sg.kSA[u];
                         b += r * sg.kSB[u];
                         x = q;
+                    }
+                    if (sg.nk > 0) {  // the last unit takes the remaining quotient
+                        a += x * sg.kSA[sg.nk - 1];
+                        b += x * sg.kSB[sg.nk - 1];
                     }
                     offKA[buf][tid] = a;
                     offKB[buf][tid] = b;

@@ -694,10 +694,23 @@ int cpsd_eecpsd_roots(const cpsd_system *s, const cpsd_integrals *I, const cpsd_
     if (p->batch_roots) {
         const double per_root =
             8.0 * (12.0 * (double)l2 + 8.0 * (double)l1 + 2.0 * (double)idsymsoc(symR, S.popv, S.popo, 1, S.popv, S.popo, 1));
-        size_t fr = 0, tot_mem = 0;
-        CPSD_TRY(cuda_check(cudaMemGetInfo(&fr, &tot_mem), "cudaMemGetInfo"));
-        const double avail = (double)fr + (double)arena().spare() + (double)pool_idle_bytes();
-        chunk = std::max<i64>(1, std::min<i64>(nroot, (i64)(0.7 * ctx().mem_share * avail / per_root)));
+        // the free-memory query only when the roots' scratch is a sizeable
+        // part of the device (it is a driver round trip)
+        thread_local size_t dev_total = 0;
+        if (!dev_total) {
+            int dev = 0;
+            CPSD_TRY(cuda_check(cudaGetDevice(&dev), "cudaGetDevice"));
+            cudaDeviceProp prop;
+            CPSD_TRY(cuda_check(cudaGetDeviceProperties(&prop, dev), "cudaGetDeviceProperties"));
+            dev_total = prop.totalGlobalMem;
+        }
+        chunk = nroot;
+        if (per_root * (double)nroot > 0.05 * ctx().mem_share * (double)dev_total) {
+            size_t fr = 0, tot_mem = 0;
+            CPSD_TRY(cuda_check(cudaMemGetInfo(&fr, &tot_mem), "cudaMemGetInfo"));
+            const double avail = (double)fr + (double)arena().spare() + (double)pool_idle_bytes();
+            chunk = std::max<i64>(1, std::min<i64>(nroot, (i64)(0.7 * ctx().mem_share * avail / per_root)));
+        }
     }
     i64 tot = 0;
     for (i64 r = 0; r < nroot; r += chunk) {

@@ -24,14 +24,16 @@ namespace {
 constexpr int NW = 4;  // warps per CTA
 
 __device__ __forceinline__ i64 ndecode(i64 x, int n, const i64 *ext, const i64 *st) {
+    // the last unit takes the remaining quotient whole (x < its extent), so
+    // it needs no division; the others divide in 32 bits when both fit
     i64 off = 0;
-    for (int u = 0; u < n; u++) {
-        i64 e = ext[u];
-        i64 q = x / e;
+    for (int u = 0; u < n - 1; u++) {
+        const i64 e = ext[u];
+        const i64 q = (x <= 0x7fffffffLL && e <= 0x7fffffffLL) ? (i64)((unsigned)x / (unsigned)e) : x / e;
         off += (x - q * e) * st[u];
         x = q;
     }
-    return off;
+    return n > 0 ? off + x * st[n - 1] : off;
 }
 
 __device__ __forceinline__ void kdecode(i64 k, const SegDev &sg, const i64 *kx, const i64 *ky, i64 *ox, i64 *oy) {
@@ -40,15 +42,22 @@ __device__ __forceinline__ void kdecode(i64 k, const SegDev &sg, const i64 *kx, 
         *oy = k * ky[0];
         return;
     }
+    if (sg.nk == 0) {  // no contracted unit: K = 1
+        *ox = 0;
+        *oy = 0;
+        return;
+    }
     i64 a = 0, b = 0;
-    for (int u = 0; u < sg.nk; u++) {
-        i64 e = sg.kExt[u], q = k / e, r = k - q * e;
+    for (int u = 0; u < sg.nk - 1; u++) {
+        const i64 e = sg.kExt[u];
+        const i64 q = (k <= 0x7fffffffLL && e <= 0x7fffffffLL) ? (i64)((unsigned)k / (unsigned)e) : k / e;
+        const i64 r = k - q * e;
         a += r * kx[u];
         b += r * ky[u];
         k = q;
     }
-    *ox = a;
-    *oy = b;
+    *ox = a + k * kx[sg.nk - 1];
+    *oy = b + k * ky[sg.nk - 1];
 }
 
 // row / column views of a task and segment: rows run over the M side
