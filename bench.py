@@ -105,6 +105,16 @@ class ClockSampler:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
+def hbm_peak_gbs():
+    """measured HBM copy bandwidth of this pool (MEASURED_PEAKS.json), else
+    the pool's earlier measurement of 6650 GB/s"""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"])
+    except (OSError, KeyError, ValueError):
+        return 6650.0
+
+
 def measured_fp64_peak(torch):
     """cuBLAS DGEMM throughput on this GPU (TFLOP/s), the FP64 roofline."""
     n = 8192
@@ -220,7 +230,7 @@ def contraction_records(api):
     lib.cpsd_contract_records(ms.ctypes.data_as(ctypes.c_void_p), fl.ctypes.data_as(ctypes.c_void_p),
                               sh.ctypes.data_as(ctypes.c_void_p), ctypes.c_int64(n), ctypes.byref(nr))
     k = nr.value
-    return ms[:k], fl[:k], sh[:4 * k].reshape(k, 4)[:, 3]
+    return ms[:k], fl[:k], sh[:4 * k].reshape(k, 4)[:, 3], sh[:4 * k].reshape(k, 4)[:, :3]
 
 
 def run_ours(args, rank, world, local_rank):
@@ -295,7 +305,7 @@ def run_ours(args, rank, world, local_rank):
     lib.cpsd_contract_time(None, None, None, 1)
     step()
     torch.cuda.synchronize()
-    rms, rfl, rkind = contraction_records(api)
+    rms, rfl, rkind, rshape = contraction_records(api)
     lib.cpsd_contract_time(None, None, None, 1)
     lib.cpsd_contract_timing(0)
     api.set_mixed(0)
@@ -307,12 +317,25 @@ def run_ours(args, rank, world, local_rank):
         sel = rkind == 12
         g_ms, g_fl = float(rms[sel].sum()), float(rfl[sel].sum())
         ach = g_fl * pairs / (g_ms / 1e3) / 1e12 if g_ms > 0 else 0.0
+        # per launch the slower of its int8 ops at the measured int8 peak and
+        # its digit-tile bytes at the measured HBM bandwidth: launches with
+        # few output columns stream their digit tiles once and are HBM-bound
+        hbm = hbm_peak_gbs()
+        att_ms = 0.0
+        for f_, b_ in zip(rfl[sel], rshape[sel][:, 1]):
+            t_tensor = f_ * pairs / (int8_peak * 1e12) if int8_peak else 0.0
+            t_hbm = float(b_) / (hbm * 1e9) if hbm else 0.0
+            att_ms += 1e3 * max(t_tensor, t_hbm)
         roof = {"bound": "tensor", "kernel": f"k_oz_gemm (tcgen05 kind::i8, {digits} digits, {pairs} digit products)",
                 "achieved": ach, "peak": int8_peak, "unit": "TOPS (int8)",
                 "frac": ach / int8_peak if int8_peak else None, "traffic": None,
                 "peak_source": "measured cuBLASLt int8 GEMM 8192^3 (torch._int_mm) on this GPU",
                 "fp64_equivalent_tflops": g_fl / (g_ms / 1e3) / 1e12 if g_ms > 0 else 0.0,
-                "share_of_step": g_ms / step_ms, "launches_per_step": int(sel.sum())}
+                "share_of_step": g_ms / step_ms, "launches_per_step": int(sel.sum()),
+                "digit_tile_bytes_per_step": int(rshape[sel][:, 1].sum()),
+                "attainable_ms": att_ms, "frac_of_attainable": att_ms / g_ms if g_ms > 0 else None,
+                "attainable_note": "per launch max(int8 ops / measured int8 peak, digit-tile bytes / measured "
+                                   "HBM copy bandwidth of MEASURED_PEAKS.json)"}
     sel = rkind < 10
     d_ms, d_fl = float(rms[sel].sum()), float(rfl[sel].sum())
     roof64 = {"bound": "tensor", "kernel": "k_contract (FP64 mma.sync m8n8k4 grouped contraction)",

@@ -322,7 +322,8 @@ int launch_ozaki(const OzPlan *oz, const double *A, const double *B, double *C, 
     CPSD_TRY(digits_of(oz, true, A, &ad, &ea));
     CPSD_TRY(digits_of(oz, false, B, &bd, &eb));
     cudaEvent_t end;
-    CPSD_TRY(timing_begin(oz->flops, (i64)oz->groups.size(), 0, (i64)oz->tiles.size(), 12, &end));
+    // record: groups, bytes of the digit tiles the launch streams, tiles
+    CPSD_TRY(timing_begin(oz->flops, (i64)oz->groups.size(), oz->adig + oz->bdig, (i64)oz->tiles.size(), 12, &end));
     for (int kt0 = 0; kt0 < oz->kt_max; kt0 += oz->kt_chunk)
         CPSD_TRY(oz_gemm(oz->S, oz->dev, ad, bd, ea, eb, C, alpha, kt0, kt0 + oz->kt_chunk, err));
     return timing_end(end);

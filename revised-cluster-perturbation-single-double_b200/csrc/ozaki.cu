@@ -248,13 +248,33 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                 w *= 1.0 / 128.0;
             }
             if (!rowok || nk == 0) continue;
+            // 8 columns at a time: all their index loads, then all their C
+            // loads, then the stores, so that the latencies of a group
+            // overlap instead of chaining output after output (every output
+            // address is written once, and C never aliases the tables)
+            const i64 nbase = (i64)tl.nt * BN + c0;
 #pragma unroll
-            for (int j = 0; j < 16; j++) {
-                const i64 n = (i64)tl.nt * BN + c0 + j;
-                if (n >= g.N) break;
-                const int nc = ncombo[g.noff + n];
-                const i64 addr = crow_m[nc] + ccol[g.ccoloff + n * g.nI + mc];
-                C[addr] += alpha * ldexp(acc[j], e_a + oz_expo(eb[g.eboff + n]));
+            for (int h = 0; h < 16; h += 8) {
+                const int nj = (int)min((i64)8, g.N - (nbase + h));
+                if (nj <= 0) break;
+                int nc[8], ex[8];
+#pragma unroll
+                for (int j = 0; j < 8; j++)
+                    if (j < nj) {
+                        nc[j] = ncombo[g.noff + nbase + h + j];
+                        ex[j] = eb[g.eboff + nbase + h + j];
+                    }
+                i64 addr[8];
+#pragma unroll
+                for (int j = 0; j < 8; j++)
+                    if (j < nj) addr[j] = crow_m[nc[j]] + ccol[g.ccoloff + (nbase + h + j) * g.nI + mc];
+                double cv[8];
+#pragma unroll
+                for (int j = 0; j < 8; j++)
+                    if (j < nj) cv[j] = C[addr[j]];
+#pragma unroll
+                for (int j = 0; j < 8; j++)
+                    if (j < nj) C[addr[j]] = cv[j] + alpha * ldexp(acc[h + j], e_a + oz_expo(ex[j]));
             }
         }
         if (!fin) ok = false;
