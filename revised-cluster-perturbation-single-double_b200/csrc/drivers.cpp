@@ -276,8 +276,8 @@ int davidson(const Sys &S, const Ints &I, const cpsd_params *p, i64 sym, i64 nro
         CPSD_TRY(scratch(D * n, &b.B[k]));
         CPSD_TRY(scratch(D * n, &b.AB[k]));
     }
-    CPSD_TRY(scratch(n, &b.w0));
-    CPSD_TRY(scratch(n, &b.w1));
+    CPSD_TRY(scratch(nroot * n, &b.w0));  // one slice per root
+    CPSD_TRY(scratch(nroot * n, &b.w1));
     b.diag = diag;
     b.fileEV = fileEV;
     Desc d = make_desc(S.popv, S.popo, ZORB, ZORB, 1, 1, sym);

@@ -74,6 +74,68 @@ __device__ double block_amax(const double *x, int n, double *sh, int *shi) {
     return (idx < n) ? x[idx] : 0.0;
 }
 
+// out[r] = x_r . y_r for the nr vector pairs x_r = x + r n, y_r = y + r n,
+// each summed in block_dot's order (strided per-thread sums, warp
+// shuffle-down, warp totals in warp order), with two barriers for all r
+__device__ void block_dots(const double *x, const double *y, int n, int nr, double *red, double *out) {
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    for (int r = 0; r < nr; r++) {
+        double a = 0.0;
+        for (int k = threadIdx.x; k < n; k += DT) a = fma(x[(size_t)r * n + k], y[(size_t)r * n + k], a);
+        for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+        if (l == 0) red[r * (DT / 32) + w] = a;
+    }
+    __syncthreads();
+    if (threadIdx.x < nr) {
+        double s = 0.0;
+        for (int i = 0; i < DT / 32; i++) s += red[threadIdx.x * (DT / 32) + i];
+        out[threadIdx.x] = s;
+    }
+    __syncthreads();
+}
+
+// out[r] = block_amax of x_r = x + r n for r < nr (value of the first
+// element of largest magnitude), with two barriers for all r
+__device__ void block_amaxs(const double *x, int n, int nr, double *redv, int *redi, double *out) {
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    for (int r = 0; r < nr; r++) {
+        double best = -1.0;
+        int bi = 0x7fffffff;
+        for (int k = threadIdx.x; k < n; k += DT) {
+            const double a = fabs(x[(size_t)r * n + k]);
+            if (a > best) {
+                best = a;
+                bi = k;
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ob = __shfl_down_sync(0xffffffffu, best, o);
+            const int oi = __shfl_down_sync(0xffffffffu, bi, o);
+            if (ob > best || (ob == best && oi < bi)) {
+                best = ob;
+                bi = oi;
+            }
+        }
+        if (l == 0) {
+            redv[r * (DT / 32) + w] = best;
+            redi[r * (DT / 32) + w] = bi;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < nr) {
+        const int r = threadIdx.x;
+        double bv = -1.0;
+        int ii = 0x7fffffff;
+        for (int i = 0; i < DT / 32; i++)
+            if (redv[r * (DT / 32) + i] > bv || (redv[r * (DT / 32) + i] == bv && redi[r * (DT / 32) + i] < ii)) {
+                bv = redv[r * (DT / 32) + i];
+                ii = redi[r * (DT / 32) + i];
+            }
+        out[r] = (ii < n) ? x[(size_t)r * n + ii] : 0.0;
+    }
+    __syncthreads();
+}
+
 // dot product of two length-n vectors by one warp (result in every lane)
 __device__ double warp_dot(const double *x, const double *y, int n) {
     const int lane = threadIdx.x & 31;
@@ -214,7 +276,6 @@ __global__ void __launch_bounds__(DT) k_dav_init(DavState *st, DavBuffers b) {
 __global__ void __launch_bounds__(DT) k_dav_step(DavState *st, DavBuffers b) {
     __shared__ double S[DAV_MAXD * DAV_MAXD], V[DAV_MAXD * DAV_MAXD], ovl[DAV_MAXD];
     __shared__ double sh[DT / 32 + 1];
-    __shared__ int shi[DT / 32 + 1];
     DavState &s = *st;
     const int tid = threadIdx.x;
     const int D = s.D, n = s.dimA, nroot = s.nroot;
@@ -310,78 +371,94 @@ __global__ void __launch_bounds__(DT) k_dav_step(DavState *st, DavBuffers b) {
         }
         __syncthreads();
     }
-    // ---- steps 4-6 per root
+    // ---- steps 4-6.  The Ritz vector, residual, convergence test and
+    // preconditioned vector of a root depend only on the subspace before this
+    // step (the new vectors go to positions >= dimIter), so they are formed
+    // for all roots at once in per-root slices of w0 / w1 (each reduction
+    // summed in block_dot / block_amax order); only the Schmidt projections
+    // and the insertion of the new vectors run root after root.
+    __shared__ double rd[DAV_MAXD * (DT / 32)], rv[DAV_MAXD];
+    __shared__ int ri[DAV_MAXD * (DT / 32)], cvd[DAV_MAXD];
+    double *const W0 = b.w0, *const W1 = b.w1;
+    for (int e = tid; e < nroot * n; e += DT) {
+        const int ir = e / n, k = e - ir * n;
+        double a = 0.0, c = 0.0;
+        if (dim_exceed) {
+            a = b.AB[cur][(size_t)ir * n + k];
+            c = b.B[cur][(size_t)ir * n + k];
+        } else {
+            for (int i = 0; i < dimIter; i++) {
+                double t = s.vecNeed[i + ir * D];
+                a += t * b.AB[cur][(size_t)i * n + k];
+                c += t * b.B[cur][(size_t)i * n + k];
+            }
+        }
+        W0[(size_t)ir * n + k] = a;
+        W1[(size_t)ir * n + k] = c;
+    }
+    __syncthreads();
+    block_dots(W1, W1, n, nroot, rd, rv);
+    for (int e = tid; e < nroot * n; e += DT) {
+        const int ir = e / n, k = e - ir * n;
+        const double t = sqrt(rv[ir]), ev = s.eigenVal[ir];
+        double q = W1[(size_t)ir * n + k], aq = W0[(size_t)ir * n + k];
+        if (fabs(t - 1.0) > 1.0e-10) {
+            q *= 1.0 / t;
+            aq *= 1.0 / t;
+        }
+        b.fileEV[(size_t)ir * (n + 1) + 1 + k] = q;
+        W1[(size_t)ir * n + k] = q;
+        W0[(size_t)ir * n + k] = aq - ev * q;
+    }
+    if (tid < nroot) b.fileEV[(size_t)tid * (n + 1)] = s.eigenVal[tid];
+    __syncthreads();
+    block_amaxs(W0, n, nroot, rd, ri, rv);
+    if (tid < nroot) {
+        cvd[tid] = fabs(rv[tid]) < s.maxError ? 1 : 0;
+        s.conv[tid] = cvd[tid];
+    }
+    __syncthreads();
     int nNew = 0, nconv = 0;
+    for (int ir = 0; ir < nroot; ir++) nconv += cvd[ir];
+    for (int e = tid; e < nroot * n; e += DT) {
+        const int ir = e / n, k = e - ir * n;
+        if (cvd[ir]) continue;
+        double d = s.eigenVal[ir] - b.diag[k];
+        if (fabs(d) < 1.0e-4) d = (d < 0.0) ? -1.0e-4 : 1.0e-4;
+        W1[(size_t)ir * n + k] = W0[(size_t)ir * n + k] / d;
+    }
+    __syncthreads();
+    // SchmidtS (mod_davidson.f90:682-727): normalise, then project
+    block_dots(W1, W1, n, nroot, rd, rv);
+    for (int e = tid; e < nroot * n; e += DT) {
+        const int ir = e / n, k = e - ir * n;
+        if (!cvd[ir]) W1[(size_t)ir * n + k] *= 1.0 / sqrt(rv[ir]);
+    }
+    __syncthreads();
     for (int ir = 0; ir < nroot; ir++) {
-        if (tid == 0) s.conv[ir] = 0;
-        for (int k = tid; k < n; k += DT) {
-            double a = 0.0, c = 0.0;
-            if (dim_exceed) {
-                a = b.AB[cur][(size_t)ir * n + k];
-                c = b.B[cur][(size_t)ir * n + k];
-            } else {
-                for (int i = 0; i < dimIter; i++) {
-                    double t = s.vecNeed[i + ir * D];
-                    a += t * b.AB[cur][(size_t)i * n + k];
-                    c += t * b.B[cur][(size_t)i * n + k];
-                }
-            }
-            b.w0[k] = a;
-            b.w1[k] = c;
-        }
-        __syncthreads();
-        double t = sqrt(block_dot(b.w1, b.w1, n, sh));
-        const double ev = s.eigenVal[ir];
-        for (int k = tid; k < n; k += DT) {
-            double q = b.w1[k], aq = b.w0[k];
-            if (fabs(t - 1.0) > 1.0e-10) {
-                q *= 1.0 / t;
-                aq *= 1.0 / t;
-            }
-            b.fileEV[(size_t)ir * (n + 1) + 1 + k] = q;
-            b.w1[k] = q;
-            b.w0[k] = aq - ev * q;
-        }
-        if (tid == 0) b.fileEV[(size_t)ir * (n + 1)] = ev;
-        __syncthreads();
-        double em = block_amax(b.w0, n, sh, shi);
-        if (fabs(em) < s.maxError) {
-            if (tid == 0) s.conv[ir] = 1;
-            nconv++;
-            continue;
-        }
-        if (dimFree == 0) continue;
-        for (int k = tid; k < n; k += DT) {
-            double d = ev - b.diag[k];
-            if (fabs(d) < 1.0e-4) d = (d < 0.0) ? -1.0e-4 : 1.0e-4;
-            b.w1[k] = b.w0[k] / d;
-        }
-        __syncthreads();
-        // SchmidtS (mod_davidson.f90:682-727)
-        double nrm = sqrt(block_dot(b.w1, b.w1, n, sh));
-        for (int k = tid; k < n; k += DT) b.w1[k] *= 1.0 / nrm;
-        __syncthreads();
+        if (cvd[ir] || dimFree == 0) continue;
+        double *const w1 = W1 + (size_t)ir * n;
         // projections on the basis: classical Gram-Schmidt applied twice
         // (same result as the reference's sequential projections to
         // rounding, with all overlaps of a pass computed at once)
         const int nb = dimIter + nNew;
         for (int pass = 0; pass < 2; pass++) {
             for (int i = tid >> 5; i < nb; i += DT / 32) {
-                double v = warp_dot(b.B[cur] + (size_t)i * n, b.w1, n);
+                double v = warp_dot(b.B[cur] + (size_t)i * n, w1, n);
                 if ((tid & 31) == 0) ovl[i] = v;
             }
             __syncthreads();
             for (int k = tid; k < n; k += DT) {
-                double x = b.w1[k];
+                double x = w1[k];
                 for (int i = 0; i < nb; i++) x += -ovl[i] * b.B[cur][(size_t)i * n + k];
-                b.w1[k] = x;
+                w1[k] = x;
             }
             __syncthreads();
         }
-        nrm = sqrt(block_dot(b.w1, b.w1, n, sh));
+        const double nrm = sqrt(block_dot(w1, w1, n, sh));
         if (nrm < 1.0e-6) continue;
         const int pos = dimIter + nNew;
-        for (int k = tid; k < n; k += DT) b.B[cur][(size_t)pos * n + k] = b.w1[k] * (1.0 / nrm);
+        for (int k = tid; k < n; k += DT) b.B[cur][(size_t)pos * n + k] = w1[k] * (1.0 / nrm);
         __syncthreads();
         dimFree--;
         nNew++;

@@ -29,7 +29,7 @@ struct DavBuffers {
     double *B[2], *AB[2];  // basis and sigma "files", D x dimA each
     const double *diag;    // OED1 of the irrep
     double *fileEV;        // nroot records (w, R)
-    double *w0, *w1;       // work vectors
+    double *w0, *w1;       // work vectors, nroot x dimA (one slice per root)
     // device-driven loop: the step stages its new vectors in W (nroot x dimA,
     // zero beyond nNew), the sigma of W goes to AW and the Ritz update moves
     // it in place; mailbox[0] (mapped host memory) = 1 while iterating
