@@ -256,8 +256,10 @@ int cpsd_debug_narrow_plan(const cpsd_opt *v1, const char *t1, const cpsd_opt *v
  * A jobs, B jobs, A row / K offsets, B row / K offsets, C row / column
  * offsets, M / N / K combination ids, sizes[0..12] their counts;
  * sizes[13..19] = A digit bytes, B digit bytes, A / B exponents, K stages
- * per launch, most K stages, B tile width.  tables[0] = NULL when the
- * contraction does not regroup into dense GEMMs. */
+ * per launch, most K stages, B tile width; tables[20..21] = the A / B
+ * OzStage tables (affine K stages), sizes[20..21] their counts.  Both
+ * arrays hold 22 entries.  tables[0] = NULL when the contraction does not
+ * regroup into dense GEMMs. */
 int cpsd_debug_ozaki_plan(const cpsd_opt *v1, const char *t1, const cpsd_opt *v2, const char *t2,
                           const cpsd_opt *v3, const char *t3, int64_t nb, int64_t sA, int64_t sB, int64_t sC,
                           int digits, const void **tables, int64_t *sizes);

@@ -1033,7 +1033,7 @@ int cpsd_debug_ozaki_plan(const cpsd_opt *v1, const char *t1, const cpsd_opt *v2
     CPSD_TRY(plan_contract(desc_of(v1), t1, desc_of(v2), t2, desc_of(v3), t3, b, &p));
     const OzPlan *oz = nullptr;
     if (!p->empty) CPSD_TRY(plan_ozaki(p, digits, &oz));
-    for (int i = 0; i < 20; i++) {
+    for (int i = 0; i < 22; i++) {
         tables[i] = nullptr;
         sizes[i] = 0;
     }
@@ -1058,6 +1058,10 @@ int cpsd_debug_ozaki_plan(const cpsd_opt *v1, const char *t1, const cpsd_opt *v2
     sizes[17] = oz->kt_chunk;
     sizes[18] = oz->kt_max;
     sizes[19] = oz->BN;
+    tables[20] = oz->astage.data();
+    sizes[20] = (int64_t)oz->astage.size();
+    tables[21] = oz->bstage.data();
+    sizes[21] = (int64_t)oz->bstage.size();
     return CPSD_OK;
 }
 

@@ -292,13 +292,53 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
 // slicing jobs (one row tile of one group each).  Element (r, k) of a group
 // lives at src[roff[r * nJ + kcombo[k]] + koff[k * nI + rcombo[r]]] (row r
 // of irrep combination rcombo[r], contracted index k of combination
-// kcombo[k]).
-constexpr int OZ_EXPO_CHUNK = 16;  // K stages per block of the exponent pass
+// kcombo[k]); on an affine job and stage (OzSliceJob) the address is a base
+// plus row and column steps, with no table read per element.  Thread t of a
+// block always handles row t mod RT of its tile, 16 contracted indices (one
+// 16-byte row of a core matrix) at a time; a warp covers 32 consecutive
+// rows, so for a fixed index its loads are one contiguous run when the rows
+// are.
+constexpr int OZ_EXPO_CHUNK = 16;  // most K stages per block of the exponent pass
 
-// the elements k0 .. k0+15 of one row (zero beyond K), all loads in flight
-__device__ __forceinline__ void oz_load16(double (&x)[16], const OzSliceJob &jb, const double *__restrict__ src,
-                                          const i64 *__restrict__ roff, const i64 *__restrict__ koff,
-                                          const int *__restrict__ kcombo, i64 row, int rc, i64 k0) {
+// gather of one K stage of a job: base and column step when the stage is
+// affine for the job
+struct OzStageAddr {
+    bool fast;
+    i64 base, sk;
+};
+__device__ __forceinline__ OzStageAddr oz_stage_addr(const OzSliceJob &jb, const OzStage *__restrict__ stage,
+                                                     const i64 *__restrict__ roff, int kt, i64 r0) {
+    OzStageAddr a{false, 0, 0};
+    if (jb.affine) {
+        const OzStage st = stage[jb.soff + (i64)kt * jb.nI + jb.rc];
+        if (st.ok) {
+            a.fast = true;
+            a.base = roff[jb.roff + r0 * jb.nJ + st.j] + st.ko0;
+            a.sk = st.sk;
+        }
+    }
+    return a;
+}
+
+// elements kst + kk .. kst + kk + 15 of one row (zero beyond K; kst = first
+// index of the stage), all loads in flight
+__device__ __forceinline__ void oz_load16(double (&x)[16], const OzSliceJob &jb, const OzStageAddr &sa,
+                                          const double *__restrict__ src, const i64 *__restrict__ roff,
+                                          const i64 *__restrict__ koff, const int *__restrict__ rcombo,
+                                          const int *__restrict__ kcombo, i64 row, i64 r0, i64 kst, int kk) {
+    const i64 k0 = kst + kk;
+    if (sa.fast) {
+        const double *p = src + (sa.base + (row - r0) * jb.sr + (i64)kk * sa.sk);
+        if (k0 + 16 <= jb.K) {
+#pragma unroll
+            for (int q = 0; q < 16; q++) x[q] = __ldg(p + (i64)q * sa.sk);
+        } else {
+#pragma unroll
+            for (int q = 0; q < 16; q++) x[q] = k0 + q < jb.K ? __ldg(p + (i64)q * sa.sk) : 0.0;
+        }
+        return;
+    }
+    const int rc = rcombo[jb.rcoff + row];
     const i64 *ro = roff + jb.roff + row * jb.nJ;
     i64 addr[16];
 #pragma unroll
@@ -310,94 +350,104 @@ __device__ __forceinline__ void oz_load16(double (&x)[16], const OzSliceJob &jb,
     for (int q = 0; q < 16; q++) x[q] = addr[q] >= 0 ? __ldg(src + addr[q]) : 0.0;
 }
 
-// pass 1: exponent e of every row maximum (|x| < 2^e) over chunks of
-// OZ_EXPO_CHUNK stages (grid.y), merged with atomicMax into expo, which
-// holds OZ_EXPO_NONE on entry
+// pass 1: exponent e of every row maximum (|x| < 2^e) over `chunk` stages
+// (grid.y), merged with atomicMax into expo, which holds OZ_EXPO_NONE on
+// entry.  Each thread keeps the running maximum of its row in a register.
 template <int RT>
-__global__ void __launch_bounds__(256) k_oz_expo(const OzSliceJob *__restrict__ jobs, const double *__restrict__ src,
+__global__ void __launch_bounds__(256) k_oz_expo(const OzSliceJob *__restrict__ jobs,
+                                                 const OzStage *__restrict__ stage, const double *__restrict__ src,
                                                  const i64 *__restrict__ roff, const i64 *__restrict__ koff,
                                                  const int *__restrict__ rcombo, const int *__restrict__ kcombo,
-                                                 int *__restrict__ expo) {
+                                                 int chunk, int *__restrict__ expo) {
     const OzSliceJob jb = jobs[blockIdx.x];
-    const int kt0 = blockIdx.y * OZ_EXPO_CHUNK;
+    const int kt0 = blockIdx.y * chunk;
     if (kt0 >= jb.KT) return;
-    const int kt1 = min(jb.KT, kt0 + OZ_EXPO_CHUNK);
+    const int kt1 = min(jb.KT, kt0 + chunk);
+    constexpr int PER = 256 / RT;              // threads per row
+    constexpr int NU = (OZ_BK / 16) / PER;     // 16-index units of a thread per stage
     __shared__ int rmax[RT];
-    const int tid = threadIdx.x;
-    for (int r = tid; r < RT; r += 256) rmax[r] = OZ_EXPO_NONE;
+    const int tid = threadIdx.x, r = tid % RT;
+    for (int i = tid; i < RT; i += 256) rmax[i] = OZ_EXPO_NONE;
     __syncthreads();
-    constexpr int UNITS = RT * (OZ_BK / 16);  // (row, 16 contracted indices) per stage
-    const i64 r0 = (i64)jb.rt * RT;
-    for (int kt = kt0; kt < kt1; kt++)
-        for (int u = tid; u < UNITS; u += 256) {
-            const int r = u % RT, k16 = u / RT;
-            const i64 row = r0 + r;
-            if (row >= jb.R) continue;
-            double x[16];
-            oz_load16(x, jb, src, roff, koff, kcombo, row, rcombo[jb.rcoff + row], (i64)kt * OZ_BK + k16 * 16);
-            double amax = 0.0;
+    const i64 r0 = (i64)jb.rt * RT, row = r0 + r;
+    double amax = 0.0;
+    if (row < jb.R)
+        for (int kt = kt0; kt < kt1; kt++) {
+            const OzStageAddr sa = oz_stage_addr(jb, stage, roff, kt, r0);
+            double x[NU][16];
 #pragma unroll
-            for (int q = 0; q < 16; q++) amax = fmax(amax, fabs(x[q]));
-            if (amax != 0.0) {
-                int ex;
-                frexp(amax, &ex);
-                atomicMax(&rmax[r], ex);
-            }
+            for (int u = 0; u < NU; u++)
+                oz_load16(x[u], jb, sa, src, roff, koff, rcombo, kcombo, row, r0, (i64)kt * OZ_BK,
+                          (tid / RT + u * PER) * 16);
+#pragma unroll
+            for (int u = 0; u < NU; u++)
+#pragma unroll
+                for (int q = 0; q < 16; q++) amax = fmax(amax, fabs(x[u][q]));
         }
-    __syncthreads();
-    for (int r = tid; r < RT; r += 256) {
-        const i64 row = r0 + r;
-        if (row < jb.R && rmax[r] != OZ_EXPO_NONE) atomicMax(&expo[jb.eoff + row], rmax[r]);
+    if (amax != 0.0) {
+        int ex;
+        frexp(amax, &ex);
+        atomicMax(&rmax[r], ex);
     }
+    __syncthreads();
+    for (int i = tid; i < RT; i += 256)
+        if (r0 + i < jb.R && rmax[i] != OZ_EXPO_NONE) atomicMax(&expo[jb.eoff + r0 + i], rmax[i]);
 }
 
 // pass 2: the S digit tiles of stage blockIdx.y, written as 16-byte rows of
 // the core matrices; rows and columns beyond the group's extents get zero
 // digits
 template <int S, int RT>
-__global__ void __launch_bounds__(256) k_oz_slice(const OzSliceJob *__restrict__ jobs, const double *__restrict__ src,
+__global__ void __launch_bounds__(256) k_oz_slice(const OzSliceJob *__restrict__ jobs,
+                                                  const OzStage *__restrict__ stage, const double *__restrict__ src,
                                                   const i64 *__restrict__ roff, const i64 *__restrict__ koff,
                                                   const int *__restrict__ rcombo, const int *__restrict__ kcombo,
                                                   int8_t *__restrict__ dig, const int *__restrict__ expo) {
     const OzSliceJob jb = jobs[blockIdx.x];
     const int kt = blockIdx.y;
     if (kt >= jb.KT) return;
-    const int tid = threadIdx.x;
-    constexpr int UNITS = RT * (OZ_BK / 16);
-    const i64 r0 = (i64)jb.rt * RT;
-    {
-        int8_t *tile = dig + jb.doff + ((size_t)jb.rt * jb.KT + kt) * (size_t)(S * RT * OZ_BK);
-        for (int u = tid; u < UNITS; u += 256) {
-            const int r = u % RT, k16 = u / RT;
-            const i64 row = r0 + r;
-            uint32_t w[S][4];
+    constexpr int PER = 256 / RT, NU = (OZ_BK / 16) / PER;
+    const int tid = threadIdx.x, r = tid % RT;
+    const i64 r0 = (i64)jb.rt * RT, row = r0 + r;
+    int8_t *tile = dig + jb.doff + ((size_t)jb.rt * jb.KT + kt) * (size_t)(S * RT * OZ_BK);
+    uint32_t w[NU][S][4];
 #pragma unroll
-            for (int t = 0; t < S; t++) w[t][0] = w[t][1] = w[t][2] = w[t][3] = 0u;
-            if (row < jb.R) {
-                double x[16];
-                oz_load16(x, jb, src, roff, koff, kcombo, row, rcombo[jb.rcoff + row], (i64)kt * OZ_BK + k16 * 16);
-                // 2^-e in two finite factors: a row whose largest element is
-                // below 2^-1022 has e < -1021 and 2^-e alone would overflow
-                const int e = oz_expo(expo[jb.eoff + row]);
-                const double sc1 = ldexp(1.0, -(e / 2)), sc2 = ldexp(1.0, -(e - e / 2));
+    for (int u = 0; u < NU; u++)
 #pragma unroll
-                for (int q = 0; q < 16; q++) {
-                    double y = x[q] * sc1 * sc2;
+        for (int t = 0; t < S; t++) w[u][t][0] = w[u][t][1] = w[u][t][2] = w[u][t][3] = 0u;
+    if (row < jb.R) {
+        const OzStageAddr sa = oz_stage_addr(jb, stage, roff, kt, r0);
+        double x[NU][16];
 #pragma unroll
-                    for (int t = 0; t < S; t++) {
-                        y *= 128.0;
-                        const double qd = trunc(y);
-                        y -= qd;
-                        w[t][q >> 2] |= ((uint32_t)(uint8_t)(int8_t)(int)qd) << (8 * (q & 3));
-                    }
+        for (int u = 0; u < NU; u++)
+            oz_load16(x[u], jb, sa, src, roff, koff, rcombo, kcombo, row, r0, (i64)kt * OZ_BK,
+                      (tid / RT + u * PER) * 16);
+        // 2^-e in two finite factors: a row whose largest element is below
+        // 2^-1022 has e < -1021 and 2^-e alone would overflow
+        const int e = oz_expo(expo[jb.eoff + row]);
+        const double sc1 = ldexp(1.0, -(e / 2)), sc2 = ldexp(1.0, -(e - e / 2));
+#pragma unroll
+        for (int u = 0; u < NU; u++)
+#pragma unroll
+            for (int q = 0; q < 16; q++) {
+                double y = x[u][q] * sc1 * sc2;
+#pragma unroll
+                for (int t = 0; t < S; t++) {
+                    y *= 128.0;
+                    const double qd = trunc(y);
+                    y -= qd;
+                    w[u][t][q >> 2] |= ((uint32_t)(uint8_t)(int8_t)(int)qd) << (8 * (q & 3));
                 }
             }
-            const size_t off = (size_t)(r >> 3) * (8 * OZ_BK) + (size_t)k16 * 128 + (size_t)(r & 7) * 16;
+    }
 #pragma unroll
-            for (int t = 0; t < S; t++)
-                *reinterpret_cast<uint4 *>(tile + (size_t)t * RT * OZ_BK + off) =
-                    make_uint4(w[t][0], w[t][1], w[t][2], w[t][3]);
-        }
+    for (int u = 0; u < NU; u++) {
+        const int k16 = tid / RT + u * PER;
+        const size_t off = (size_t)(r >> 3) * (8 * OZ_BK) + (size_t)k16 * 128 + (size_t)(r & 7) * 16;
+#pragma unroll
+        for (int t = 0; t < S; t++)
+            *reinterpret_cast<uint4 *>(tile + (size_t)t * RT * OZ_BK + off) =
+                make_uint4(w[u][t][0], w[u][t][1], w[u][t][2], w[u][t][3]);
     }
 }
 
@@ -422,9 +472,21 @@ template <int S, int RT>
 int oz_slice_launch(const OzSideDev &sd, const double *src, int8_t *dig, int *expo) {
     if (sd.njobs == 0) return CPSD_OK;
     CPSD_TRY(cuda_check(cudaMemsetAsync(expo, 0x80, sizeof(int) * (size_t)sd.nexpo, stream()), "clear exponents"));
-    const dim3 ge(sd.njobs, (sd.kt_max + OZ_EXPO_CHUNK - 1) / OZ_EXPO_CHUNK), gd(sd.njobs, sd.kt_max);
-    k_oz_expo<RT><<<ge, 256, 0, stream()>>>(sd.jobs, src, sd.roff, sd.koff, sd.rcombo, sd.kcombo, expo);
-    k_oz_slice<S, RT><<<gd, 256, 0, stream()>>>(sd.jobs, src, sd.roff, sd.koff, sd.rcombo, sd.kcombo, dig, expo);
+    // stages per exponent block: up to OZ_EXPO_CHUNK, fewer while the grid
+    // would not give every SM four blocks
+    static const int sms = [] {
+        int d = 0, n = 148;
+        if (cudaGetDevice(&d) != cudaSuccess || cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, d) != cudaSuccess)
+            n = 148;
+        return n;
+    }();
+    int chunk = OZ_EXPO_CHUNK;
+    while (chunk > 1 && (i64)sd.njobs * ((sd.kt_max + chunk - 1) / chunk) < 4 * (i64)sms) chunk /= 2;
+    const dim3 ge(sd.njobs, (sd.kt_max + chunk - 1) / chunk), gd(sd.njobs, sd.kt_max);
+    k_oz_expo<RT><<<ge, 256, 0, stream()>>>(sd.jobs, sd.stage, src, sd.roff, sd.koff, sd.rcombo, sd.kcombo, chunk,
+                                            expo);
+    k_oz_slice<S, RT><<<gd, 256, 0, stream()>>>(sd.jobs, sd.stage, src, sd.roff, sd.koff, sd.rcombo, sd.kcombo, dig,
+                                                expo);
     count_launch(2);
     return cuda_check(cudaGetLastError(), "k_oz_slice");
 }

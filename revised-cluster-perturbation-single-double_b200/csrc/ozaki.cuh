@@ -21,11 +21,22 @@ struct OzGroup {
 struct OzTile {
     int g, mt, nt, pad;
 };
-// slicing work item: one row tile of one group of one operand side
+// slicing work item: one row tile of one group of one operand side.  When
+// every row of the tile has the same row combination rc and the row offsets
+// step by sr for every contracted combination (affine = 1), and a K stage
+// lies in one contracted combination j with column offsets stepping by sk
+// (the OzStage of (stage, rc)), element (r0 + dr, k0 + dk) of the tile is at
+// roff[r0][j] + ko0 + dr sr + dk sk: the gather needs no per-element table.
 struct OzSliceJob {
     i64 R, K;
     int KT, rt, nJ, nI;
     i64 roff, koff, rcoff, kcoff, eoff, doff;
+    int affine, rc;
+    i64 sr, soff;  // row stride; offset of the group's OzStage table (KT x nI)
+};
+struct OzStage {
+    i64 ko0, sk;  // column offset of the stage's first index, column stride
+    int j, ok;    // contracted combination; 1 when the stage is affine
 };
 
 struct OzSideDev {
@@ -35,6 +46,7 @@ struct OzSideDev {
     i64 nexpo = 0;   // exponents of this side
     const i64 *roff = nullptr, *koff = nullptr;
     const int *rcombo = nullptr, *kcombo = nullptr;
+    const OzStage *stage = nullptr;
 };
 struct OzDevPlan {
     const OzTile *tiles = nullptr;
@@ -52,6 +64,7 @@ struct OzPlan {
     std::vector<OzGroup> groups;
     std::vector<OzTile> tiles;
     std::vector<OzSliceJob> ajobs, bjobs;
+    std::vector<OzStage> astage, bstage;
     std::vector<i64> aroff, akoff, broff, bkoff, crow, ccol;
     std::vector<int> mcombo, ncombo, kcombo;
     i64 adig = 0, bdig = 0;      // bytes of the A / B digit tiles

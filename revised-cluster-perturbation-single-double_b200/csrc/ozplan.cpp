@@ -83,6 +83,8 @@ int OzPlan::upload() {
     bdev.njobs = (int)bjobs.size();
     bdev.rcombo = dev.ncombo;
     bdev.kcombo = kc;
+    CPSD_TRY(upload_vec(astage, &adev.stage));
+    CPSD_TRY(upload_vec(bstage, &bdev.stage));
     // the tables may next be read by kernels on another thread's stream
     CPSD_TRY(cuda_check(cudaStreamSynchronize(stream()), "plan upload"));
     uploaded.store(true, std::memory_order_release);
@@ -227,12 +229,53 @@ int plan_ozaki(const ContractPlan *cp, int S, const OzPlan **out) {
                 for (i64 nl = 0; nl < tk.N; nl++)
                     p.ccol[og.ccoloff + (nstart[l] + nl) * nI + i] = decode(nl, tk.nn, tk.nExt, tk.nSC);
             }
-        for (i64 rt = 0; rt < Mpad / 128; rt++)
-            p.ajobs.push_back(OzSliceJob{og.M, og.K, og.KT, (int)rt, nJ, nI, aroff0, akoff0, og.moff, kcoff, og.eaoff,
-                                         og.aoff});
-        for (i64 rt = 0; rt < Npad / BN; rt++)
-            p.bjobs.push_back(OzSliceJob{og.N, og.K, og.KT, (int)rt, nJ, nL, broff0, bkoff0, og.noff, kcoff, og.eboff,
-                                         og.boff});
+        // affine descriptors of the K stages (per row combination) and of the
+        // row tiles: most tiles of a large group sit inside one DPD block,
+        // whose offsets step by constant strides
+        auto stage_table = [&](const std::vector<i64> &koff, i64 koff0, int nrc, std::vector<OzStage> &out) {
+            const i64 soff = (i64)out.size();
+            out.resize(soff + (i64)og.KT * nrc);
+            for (int kt = 0; kt < og.KT; kt++) {
+                const i64 k0 = (i64)kt * 64, k1 = std::min<i64>(og.K, k0 + 64);
+                const int j = p.kcombo[kcoff + k0];
+                for (int rc = 0; rc < nrc; rc++) {
+                    OzStage &st = out[soff + (i64)kt * nrc + rc];
+                    st = OzStage{koff[koff0 + k0 * nrc + rc], 0, j, 1};
+                    if (k1 - k0 > 1) st.sk = koff[koff0 + (k0 + 1) * nrc + rc] - st.ko0;
+                    for (i64 k = k0; k < k1 && st.ok; k++)
+                        if (p.kcombo[kcoff + k] != j || koff[koff0 + k * nrc + rc] != st.ko0 + (k - k0) * st.sk)
+                            st.ok = 0;
+                }
+            }
+            return soff;
+        };
+        auto job_affine = [](OzSliceJob &jb, const std::vector<i64> &roff, const std::vector<int> &combo, int RT) {
+            const i64 r0 = (i64)jb.rt * RT, r1 = std::min<i64>(jb.R, r0 + RT);
+            jb.rc = combo[jb.rcoff + r0];
+            const i64 *ro = roff.data() + jb.roff;
+            const i64 sr = r1 - r0 > 1 ? ro[(r0 + 1) * jb.nJ] - ro[r0 * jb.nJ] : 0;
+            for (i64 r = r0; r < r1; r++) {
+                if (combo[jb.rcoff + r] != jb.rc) return;
+                for (int j = 0; j < jb.nJ; j++)
+                    if (ro[r * jb.nJ + j] != ro[r0 * jb.nJ + j] + (r - r0) * sr) return;
+            }
+            jb.affine = 1;
+            jb.sr = sr;
+        };
+        const i64 asoff = og.K > 0 ? stage_table(p.akoff, akoff0, nI, p.astage) : 0;
+        const i64 bsoff = og.K > 0 ? stage_table(p.bkoff, bkoff0, nL, p.bstage) : 0;
+        for (i64 rt = 0; rt < Mpad / 128; rt++) {
+            OzSliceJob jb{og.M, og.K, og.KT, (int)rt, nJ, nI, aroff0, akoff0, og.moff, kcoff, og.eaoff, og.aoff};
+            jb.soff = asoff;
+            if (og.K > 0) job_affine(jb, p.aroff, p.mcombo, 128);
+            p.ajobs.push_back(jb);
+        }
+        for (i64 rt = 0; rt < Npad / BN; rt++) {
+            OzSliceJob jb{og.N, og.K, og.KT, (int)rt, nJ, nL, broff0, bkoff0, og.noff, kcoff, og.eboff, og.boff};
+            jb.soff = bsoff;
+            if (og.K > 0) job_affine(jb, p.broff, p.ncombo, BN);
+            p.bjobs.push_back(jb);
+        }
         for (i64 mt = 0; mt < Mpad / 128; mt++)
             for (i64 nt = 0; nt < Npad / BN; nt++)
                 p.tiles.push_back(OzTile{(int)p.groups.size(), (int)mt, (int)nt, 0});

@@ -34,18 +34,23 @@ class OzTile(ctypes.Structure):
 
 class OzSliceJob(ctypes.Structure):
     _fields_ = [("R", I64), ("K", I64)] + [(k, ctypes.c_int) for k in ("KT", "rt", "nJ", "nI")] + \
-               [(k, I64) for k in ("roff", "koff", "rcoff", "kcoff", "eoff", "doff")]
+               [(k, I64) for k in ("roff", "koff", "rcoff", "kcoff", "eoff", "doff")] + \
+               [("affine", ctypes.c_int), ("rc", ctypes.c_int), ("sr", I64), ("soff", I64)]
+
+
+class OzStage(ctypes.Structure):
+    _fields_ = [("ko0", I64), ("sk", I64), ("j", ctypes.c_int), ("ok", ctypes.c_int)]
 
 
 def get_oz_plan(o1, t1, o2, t2, o3, t3, nb, sA, sB, sC, digits):
-    tabs = (ctypes.c_void_p * 20)()
-    sizes = (I64 * 20)()
+    tabs = (ctypes.c_void_p * 22)()
+    sizes = (I64 * 22)()
     api.check(api.lib().cpsd_debug_ozaki_plan(ctypes.byref(o1), t1.encode(), ctypes.byref(o2), t2.encode(),
                                               ctypes.byref(o3), t3.encode(), I64(nb), I64(sA), I64(sB), I64(sC),
                                               ctypes.c_int(digits), tabs, sizes), "ozaki plan")
     if not tabs[0]:
         return None
-    n = [sizes[i] for i in range(20)]
+    n = [sizes[i] for i in range(22)]
 
     def arr(i, ct):
         return np.ctypeslib.as_array((ct * n[i]).from_address(tabs[i])).copy() if n[i] else np.zeros(0, np.int64)
@@ -56,7 +61,9 @@ def get_oz_plan(o1, t1, o2, t2, o3, t3, nb, sA, sB, sC, digits):
                 aroff=arr(4, I64), akoff=arr(5, I64), broff=arr(6, I64), bkoff=arr(7, I64), crow=arr(8, I64),
                 ccol=arr(9, I64), mcombo=arr(10, ctypes.c_int), ncombo=arr(11, ctypes.c_int),
                 kcombo=arr(12, ctypes.c_int), adig=n[13], bdig=n[14], nea=n[15], neb=n[16], kt_chunk=n[17],
-                kt_max=n[18], BN=n[19])
+                kt_max=n[18], BN=n[19],
+                astage=list((OzStage * n[20]).from_address(tabs[20])) if n[20] else [],
+                bstage=list((OzStage * n[21]).from_address(tabs[21])) if n[21] else [])
 
 
 def digits_of(X, S):
@@ -76,12 +83,34 @@ def digits_of(X, S):
     return e, q
 
 
-def side(plan, jobs, roff, koff, rcombo, src, S, RT, total_bytes, nexp):
+def check_affine(plan, jb, stage, roff, koff, rcombo, RT):
+    """the kernels' affine gather of an affine job and stage (base + row and
+    column steps) must read exactly the table address of every element"""
+    r0, r1 = jb.rt * RT, min(jb.R, (jb.rt + 1) * RT)
+    r = np.arange(r0, r1)[:, None]
+    assert (rcombo[jb.rcoff + r] == jb.rc).all()
+    n_fast = 0
+    for kt in range(jb.KT):
+        st = stage[jb.soff + kt * jb.nI + jb.rc]
+        if not st.ok:
+            continue
+        n_fast += 1
+        k = np.arange(kt * BK, min(jb.K, (kt + 1) * BK))[None, :]
+        kc = plan["kcombo"][jb.kcoff + k]
+        idx = roff[jb.roff + r * jb.nJ + kc] + koff[jb.koff + k * jb.nI + jb.rc]
+        fast = roff[jb.roff + r0 * jb.nJ + st.j] + st.ko0 + (r - r0) * jb.sr + (k - kt * BK) * st.sk
+        assert (fast == idx).all(), "affine gather differs from the tables"
+    return n_fast
+
+
+def side(plan, jobs, roff, koff, rcombo, src, S, RT, total_bytes, nexp, stage=None):
     """gather one operand side per group (bounds-checked) -> {doff: (e, digits)}"""
     out = {}
     for jb in jobs:
         assert jb.doff + (jb.rt * jb.KT + jb.KT) * S * RT * BK <= total_bytes
         assert jb.eoff + min(jb.R, (jb.rt + 1) * RT) <= nexp
+        if stage is not None and jb.affine:
+            check_affine(plan, jb, stage, roff, koff, rcombo, RT)
         if jb.rt:
             continue
         R, K = jb.R, jb.K
@@ -99,9 +128,9 @@ def emulate(plan, A, B, C, alpha, S):
     C = C.copy()
     BN = plan["BN"]
     adig = side(plan, plan["ajobs"], plan["aroff"], plan["akoff"], plan["mcombo"], A, S, 128, plan["adig"],
-                plan["nea"])
+                plan["nea"], plan["astage"])
     bdig = side(plan, plan["bjobs"], plan["broff"], plan["bkoff"], plan["ncombo"], B, S, BN, plan["bdig"],
-                plan["neb"])
+                plan["neb"], plan["bstage"])
     for t in plan["tiles"]:
         g = plan["groups"][t.g]
         assert g.aoff + (t.mt * g.KT + g.KT) * S * 128 * BK <= plan["adig"]
@@ -175,6 +204,15 @@ def test_kernel_ozaki_plans(name, nirrep, nb, digits):
                        l3 if nb > 1 else 0, digits)
     if plan is None:
         pytest.skip("contraction does not regroup into dense GEMMs")
+    if name == "c2_r2abcd":
+        # the particle-particle ladder streams the largest operand, (ab|cd):
+        # every row tile and K stage of that side must take the table-free
+        # gather (the amplitude side's tiles may straddle batch copies)
+        big = max(((plan["ajobs"], plan["astage"]), (plan["bjobs"], plan["bstage"])),
+                  key=lambda js: sum(jb.R * jb.K for jb in js[0] if jb.rt == 0))
+        jobs, stage = big
+        assert all(jb.affine for jb in jobs)
+        assert all(stage[jb.soff + kt * jb.nI + jb.rc].ok for jb in jobs for kt in range(jb.KT))
     out = emulate(plan, A, B, C, 0.9, digits)
     kmax = max(g.K for g in plan["groups"])
     bound = (digits + 1) * kmax * 128.0 ** -digits * np.abs(A).max() * np.abs(B).max() * 0.9 * 4 + 1e-12
