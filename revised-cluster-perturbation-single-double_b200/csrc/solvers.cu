@@ -299,43 +299,53 @@ __global__ void __launch_bounds__(DT) k_dav_step(DavState *st, DavBuffers b) {
     }
     __syncthreads();
     block_jacobi(S, V, dimIter);
+    // eigenvalues, their order and the chosen roots, worked out in shared
+    // memory (vecR(i, k) = V[i][k] for i < dimIter, zero below) and then
+    // published to the state
+    __shared__ double vR[DAV_MAXD];
+    __shared__ int lw[DAV_MAXD];
     for (int e = tid; e < D * dimIter; e += DT) {
         int i = e % D, k = e / D;
         s.vecR[i + k * D] = (i < dimIter) ? V[i * DAV_MAXD + k] : 0.0;
     }
+    if (tid < dimIter) vR[tid] = S[tid * DAV_MAXD + tid];
     __syncthreads();
     if (tid == 0) {
-        for (int k = 0; k < dimIter; k++) s.valR[k] = S[k * DAV_MAXD + k];
         // sort (mod_davidson.f90:620-640)
-        int *low = s.lowestE;
-        for (int i = 0; i < dimIter; i++) low[i] = i + 1;
+        for (int i = 0; i < dimIter; i++) lw[i] = i + 1;
         for (int i = 0; i < dimIter - 1; i++)
             for (int j = i + 1; j < dimIter; j++)
-                if (s.valR[low[j] - 1] < s.valR[low[i] - 1]) {
-                    int t = low[j];
-                    low[j] = low[i];
-                    low[i] = t;
+                if (vR[lw[j] - 1] < vR[lw[i] - 1]) {
+                    int t = lw[j];
+                    lw[j] = lw[i];
+                    lw[i] = t;
                 }
         if (!s.lowest) {  // root tracking by largest component (mod_davidson.f90:227-251)
             for (int iroot = 1; iroot <= nroot; iroot++) {
                 double t1 = 0.0;
                 int i = 1;
                 for (int j = 1; j <= dimIter; j++) {
-                    double t2 = fabs(s.vecR[(iroot - 1) + (low[j - 1] - 1) * D]);
+                    double t2 = fabs(V[(iroot - 1) * DAV_MAXD + (lw[j - 1] - 1)]);
                     if (t2 > t1) {
                         t1 = t2;
                         i = j;
                     }
                 }
-                int idx = low[i - 1];
-                for (int j = 1; j <= i - iroot; j++) low[i - j] = low[i - j - 1];
-                low[iroot - 1] = idx;
+                int idx = lw[i - 1];
+                for (int j = 1; j <= i - iroot; j++) lw[i - j] = lw[i - j - 1];
+                lw[iroot - 1] = idx;
             }
         }
-        for (int ir = 0; ir < nroot; ir++) {
-            for (int k = 0; k < D; k++) s.vecNeed[k + ir * D] = s.vecR[k + (low[ir] - 1) * D];
-            s.eigenVal[ir] = s.valR[low[ir] - 1];
-        }
+    }
+    __syncthreads();
+    if (tid < dimIter) {
+        s.valR[tid] = vR[tid];
+        s.lowestE[tid] = lw[tid];
+    }
+    if (tid < nroot) s.eigenVal[tid] = vR[lw[tid] - 1];
+    for (int e = tid; e < nroot * D; e += DT) {
+        const int ir = e / D, k = e % D;
+        s.vecNeed[k + ir * D] = (k < dimIter) ? V[k * DAV_MAXD + (lw[ir] - 1)] : 0.0;
     }
     __syncthreads();
     // ---- collapse when the subspace was full (mod_davidson.f90:266-325)
