@@ -428,10 +428,14 @@ int o_davidson(double *fileEV, const double *diagA, i64 dimA, i64 nroot, i64 ist
         }
         dv_sort(dimIter, valR, lowestE);
         if (!p->lowest) {
+            /* largest component over the positions not yet given to a root
+             * (the reference searches j = 1..dimIter and can give one
+             * eigenvector to two roots, which makes its collapse divide by
+             * zero; identical wherever it assigns distinct vectors) */
             for (i64 iroot = 1; iroot <= nroot; iroot++) {
                 double t1 = 0.0;
-                i64 i = 1;
-                for (i64 j = 1; j <= dimIter; j++) {
+                i64 i = iroot;
+                for (i64 j = iroot; j <= dimIter; j++) {
                     double t2 = fabs(vecR[(iroot - 1) + (lowestE[j - 1] - 1) * D]);
                     if (t2 > t1) { t1 = t2; i = j; }
                 }

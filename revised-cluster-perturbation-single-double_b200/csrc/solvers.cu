@@ -140,6 +140,7 @@ __device__ void block_amaxs(const double *x, int n, int nr, double *redv, int *r
 __device__ double warp_dot(const double *x, const double *y, int n) {
     const int lane = threadIdx.x & 31;
     double a = 0.0;
+#pragma unroll 4
     for (int k = lane; k < n; k += 32) a = fma(x[k], y[k], a);
     for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
     return a;
@@ -151,7 +152,12 @@ __device__ double warp_dot(const double *x, const double *y, int n) {
 // element below 1e-17 sqrt(|a_pp a_qq|) is negligible and set to zero; a
 // sweep without rotations ends the iteration.  The n(n-1)/2 rotations of a
 // sweep run as n-1 rounds of n/2 disjoint rotations (round-robin pairing,
-// n padded to even), each round one parallel update of S and V.
+// n padded to even), each round one parallel update of S and V.  The
+// rotation of a pair is
+//   t = sgn(d b) |b| / (|d| + hypot(d, b)),  d = a_qq - a_pp, b = 2 a_pq,
+//   c = 1 / sqrt(1 + t^2),  s = t c
+// (the smaller root of t^2 + 2 tau t - 1 = 0, tau = d / b, written with one
+// division), evaluated next to the threshold test.
 __device__ void block_jacobi(double *S, double *V, int n) {
     __shared__ double cs[DAV_MAXD], sn[DAV_MAXD];
     __shared__ int pp[DAV_MAXD / 2], qq[DAV_MAXD / 2];
@@ -178,12 +184,14 @@ __device__ void block_jacobi(double *S, double *V, int n) {
                 int p = min(a, b), q = max(a, b);
                 double apq = S[p * DAV_MAXD + q];
                 double app = S[p * DAV_MAXD + p], aqq = S[q * DAV_MAXD + q];
+                const double d = aqq - app, b2 = 2.0 * apq;
+                double t = fabs(b2) / (fabs(d) + hypot(d, b2));
+                if (d != 0.0 && ((d > 0.0) != (b2 > 0.0))) t = -t;
+                const double ct = rsqrt(1.0 + t * t);
                 double c = 1.0, s = 0.0;
                 if (!(fabs(apq) <= 1.0e-17 * sqrt(fabs(app) * fabs(aqq)) || apq == 0.0)) {
-                    double tau = (aqq - app) / (2.0 * apq);
-                    double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
-                    c = 1.0 / sqrt(1.0 + t * t);
-                    s = t * c;
+                    c = ct;
+                    s = t * ct;
                     rotated = 1;
                 }
                 pp[tid] = p;
@@ -320,11 +328,17 @@ __global__ void __launch_bounds__(DT) k_dav_step(DavState *st, DavBuffers b) {
                     lw[j] = lw[i];
                     lw[i] = t;
                 }
-        if (!s.lowest) {  // root tracking by largest component (mod_davidson.f90:227-251)
+        // root tracking by largest component (mod_davidson.f90:227-251),
+        // searched over the positions not yet given to a root: the
+        // reference also searches the assigned ones and, when one of them
+        // wins, gives one eigenvector to two roots, whose collapse then
+        // orthonormalises a repeated vector (division by zero); wherever the
+        // reference assigns distinct vectors the choice is the same
+        if (!s.lowest) {
             for (int iroot = 1; iroot <= nroot; iroot++) {
                 double t1 = 0.0;
-                int i = 1;
-                for (int j = 1; j <= dimIter; j++) {
+                int i = iroot;
+                for (int j = iroot; j <= dimIter; j++) {
                     double t2 = fabs(V[(iroot - 1) * DAV_MAXD + (lw[j - 1] - 1)]);
                     if (t2 > t1) {
                         t1 = t2;
@@ -390,21 +404,44 @@ __global__ void __launch_bounds__(DT) k_dav_step(DavState *st, DavBuffers b) {
     __shared__ double rd[DAV_MAXD * (DT / 32)], rv[DAV_MAXD];
     __shared__ int ri[DAV_MAXD * (DT / 32)], cvd[DAV_MAXD];
     double *const W0 = b.w0, *const W1 = b.w1;
-    for (int e = tid; e < nroot * n; e += DT) {
-        const int ir = e / n, k = e - ir * n;
-        double a = 0.0, c = 0.0;
-        if (dim_exceed) {
-            a = b.AB[cur][(size_t)ir * n + k];
-            c = b.B[cur][(size_t)ir * n + k];
-        } else {
-            for (int i = 0; i < dimIter; i++) {
-                double t = s.vecNeed[i + ir * D];
-                a += t * b.AB[cur][(size_t)i * n + k];
-                c += t * b.B[cur][(size_t)i * n + k];
+    if (dim_exceed) {
+        for (int e = tid; e < nroot * n; e += DT) {
+            const int ir = e / n, k = e - ir * n;
+            W0[(size_t)ir * n + k] = b.AB[cur][(size_t)ir * n + k];
+            W1[(size_t)ir * n + k] = b.B[cur][(size_t)ir * n + k];
+        }
+    } else {
+        // one pass over the basis serves RB roots: element k of every basis
+        // vector is loaded once and summed into each root in basis order
+        // (coefficient vecNeed(i, root) = V[i][lw[root] - 1])
+        constexpr int RB = 8;
+        for (int r0 = 0; r0 < nroot; r0 += RB) {
+            const int nr = min(RB, nroot - r0);
+            int col[RB];
+#pragma unroll
+            for (int q = 0; q < RB; q++) col[q] = q < nr ? lw[r0 + q] - 1 : 0;
+            for (int k = tid; k < n; k += DT) {
+                double a[RB], c[RB];
+#pragma unroll
+                for (int q = 0; q < RB; q++) a[q] = c[q] = 0.0;
+#pragma unroll 4
+                for (int i = 0; i < dimIter; i++) {
+                    const double x = b.AB[cur][(size_t)i * n + k], y = b.B[cur][(size_t)i * n + k];
+#pragma unroll
+                    for (int q = 0; q < RB; q++) {
+                        const double t = V[i * DAV_MAXD + col[q]];
+                        a[q] += t * x;
+                        c[q] += t * y;
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < RB; q++)
+                    if (q < nr) {
+                        W0[(size_t)(r0 + q) * n + k] = a[q];
+                        W1[(size_t)(r0 + q) * n + k] = c[q];
+                    }
             }
         }
-        W0[(size_t)ir * n + k] = a;
-        W1[(size_t)ir * n + k] = c;
     }
     __syncthreads();
     block_dots(W1, W1, n, nroot, rd, rv);
@@ -460,6 +497,7 @@ __global__ void __launch_bounds__(DT) k_dav_step(DavState *st, DavBuffers b) {
             __syncthreads();
             for (int k = tid; k < n; k += DT) {
                 double x = w1[k];
+#pragma unroll 8
                 for (int i = 0; i < nb; i++) x += -ovl[i] * b.B[cur][(size_t)i * n + k];
                 w1[k] = x;
             }

@@ -114,3 +114,29 @@ def test_pipeline_digits_match_oracle(digits, tol):
     np.testing.assert_allclose(om, oom, rtol=0, atol=tol)
     np.testing.assert_allclose(w2, ow2, rtol=0, atol=tol)
     np.testing.assert_allclose(w3, ow3, rtol=0, atol=tol)
+
+
+@pytest.mark.parametrize("digits,tol", [(7, 1e-10), (5, 1e-7)])
+def test_all_digit_routing_follows_fp64_roots(digits, tol):
+    """Ten small molecules of the batching draw (one of them C1, nmo 45, 7
+    roots, max-overlap root tracking) with every regrouping contraction on
+    the digit path: same roots as FP64 and no NaN.  Root tracking that could
+    give one eigenvector to two roots made the collapse of that C1 molecule
+    divide by zero."""
+    import test_gpu_batch as tb
+    mols = tb.molecules(10, 42)
+    out = {}
+    for mode in (0, digits):
+        res = []
+        for s in mols:
+            api.init(s.nirrep, s.dirprd)
+            d, p = api.DeviceIntegrals(s), api.make_params(s)
+            api.set_mixed(mode, 0.0 if mode else 1.0)
+            try:
+                res.append(api.pipeline(s, api.make_system(s), d, p)[0])
+            finally:
+                api.set_mixed(0)
+        out[mode] = res
+    for a, b in zip(out[digits], out[0]):
+        assert not np.isnan(a).any()
+        np.testing.assert_allclose(a, b, rtol=0, atol=tol)
