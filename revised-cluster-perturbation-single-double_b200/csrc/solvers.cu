@@ -153,6 +153,9 @@ __device__ double warp_dot(const double *x, const double *y, int n) {
 // sweep without rotations ends the iteration.  The n(n-1)/2 rotations of a
 // sweep run as n-1 rounds of n/2 disjoint rotations (round-robin pairing,
 // n padded to even), each round one parallel update of S and V.  The
+// iteration ends at the first round whose matrix has no element above the
+// threshold: the rounds left of that sweep and the sweep without rotations
+// would change no diagonal element and no column of V.  The
 // rotation of a pair is
 //   t = sgn(d b) |b| / (|d| + hypot(d, b)),  d = a_qq - a_pp, b = 2 a_pq,
 //   c = 1 / sqrt(1 + t^2),  s = t c
@@ -161,17 +164,27 @@ __device__ double warp_dot(const double *x, const double *y, int n) {
 __device__ void block_jacobi(double *S, double *V, int n) {
     __shared__ double cs[DAV_MAXD], sn[DAV_MAXD];
     __shared__ int pp[DAV_MAXD / 2], qq[DAV_MAXD / 2];
-    __shared__ int rotated;
     const int tid = threadIdx.x;
     const int m = (n + 1) & ~1, half = m / 2;
     for (int e = tid; e < DAV_MAXD * DAV_MAXD; e += DT) {
         int i = e / DAV_MAXD, j = e % DAV_MAXD;
         V[e] = (i == j && i < m) ? 1.0 : 0.0;
     }
-    for (int sweep = 0; sweep < 50 && m > 1; sweep++) {
-        if (tid == 0) rotated = 0;
-        __syncthreads();
+    __syncthreads();
+    bool done = m <= 1;
+    for (int sweep = 0; sweep < 50 && !done; sweep++) {
         for (int r = 0; r < m - 1; r++) {
+            // does any element of the matrix still call for a rotation?
+            // (asked by warps 1.., beside warp 0's rotation parameters)
+            bool above = false;
+            for (int e = tid - 32; e >= 0 && e < n * n; e += DT - 32) {
+                const int p = e / n, q = e - p * n;
+                if (p < q) {
+                    const double apq = S[p * DAV_MAXD + q];
+                    above |= !(fabs(apq) <= 1.0e-17 * sqrt(fabs(S[p * DAV_MAXD + p]) * fabs(S[q * DAV_MAXD + q])) ||
+                               apq == 0.0);
+                }
+            }
             if (tid < half) {  // pair k of round r: (m-1, r) and (r+k, r-k) mod m-1
                 int a, b;
                 if (tid == 0) {
@@ -192,16 +205,19 @@ __device__ void block_jacobi(double *S, double *V, int n) {
                 if (!(fabs(apq) <= 1.0e-17 * sqrt(fabs(app) * fabs(aqq)) || apq == 0.0)) {
                     c = ct;
                     s = t * ct;
-                    rotated = 1;
                 }
                 pp[tid] = p;
                 qq[tid] = q;
                 cs[tid] = c;
                 sn[tid] = s;
             }
-            __syncthreads();
+            if (!__syncthreads_or(above)) {
+                done = true;
+                break;
+            }
             // S <- J^T S J on the 2x2 blocks of (pair k rows, pair l columns)
-            for (int idx = tid; idx < half * half; idx += DT) {
+            // by the first half of the block, V <- V J by the second
+            for (int idx = tid; tid < DT / 2 && idx < half * half; idx += DT / 2) {
                 const int k = idx / half, l = idx % half;
                 const int pk = pp[k], qk = qq[k], pl = pp[l], ql = qq[l];
                 const double ck = cs[k], sk = sn[k], cl = cs[l], sl = sn[l];
@@ -217,8 +233,7 @@ __device__ void block_jacobi(double *S, double *V, int n) {
                 S[qk * DAV_MAXD + pl] = n10;
                 S[qk * DAV_MAXD + ql] = n11;
             }
-            // V <- V J
-            for (int idx = tid; idx < m * half; idx += DT) {
+            for (int idx = tid - DT / 2; idx >= 0 && idx < m * half; idx += DT / 2) {
                 const int i = idx / half, l = idx % half;
                 const int pl = pp[l], ql = qq[l];
                 const double cl = cs[l], sl = sn[l];
@@ -228,8 +243,6 @@ __device__ void block_jacobi(double *S, double *V, int n) {
             }
             __syncthreads();
         }
-        if (!rotated) break;
-        __syncthreads();
     }
     __syncthreads();
 }
