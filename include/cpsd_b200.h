@@ -323,9 +323,16 @@ int cpsd_eecpsd_roots(const cpsd_system *s, const cpsd_integrals *I, const cpsd_
                       double *R2_1, double *R1_2, double *R2_2, int64_t *solver_iters);
 
 /* The whole SF-CIS + SF-CPS(D-3) pipeline: one step of the roots/s metric.
- * Integrals are device pointers; outputs on the host. */
+ * Integrals are device pointers; outputs on the host.  By default the
+ * SF-CIS Davidson and the ground state + J^(2)/J^(3) run at once on two
+ * library worker threads (own streams), then the excited orders; results
+ * equal the sequential order's.  The sequential order is used inside
+ * cpsd_pipeline_batch workers and while per-launch timing is on. */
 int cpsd_pipeline(const cpsd_system *s, const cpsd_integrals *I, const cpsd_params *p,
                   double *omega_cis, double *w2, double *w3, int64_t *nroots);
+/* on = 0: run the pipeline's phases one after the other on the caller's
+ * stream (default 1: SF-CIS beside the ground state) */
+int cpsd_set_phase_overlap(int on);
 
 /* Independent molecules in one call (no counterpart in the reference, which
  * runs one molecule per program invocation): cpsd_pipeline of molecule m

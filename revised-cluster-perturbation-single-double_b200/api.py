@@ -322,6 +322,12 @@ def cisd_gradient(sysc, ints_struct, par, symR, w0, L, g0, g2, grads):
                                    ctypes.byref(G)), "cpsd_cisd_gradient")
 
 
+def set_phase_overlap(on=True):
+    """SF-CIS beside the ground state on two library worker streams (True,
+    the default) or all phases in order on the caller's stream"""
+    check(lib().cpsd_set_phase_overlap(1 if on else 0), "cpsd_set_phase_overlap")
+
+
 def pipeline_batch(systems, ints_list, params, nworkers=4):
     """cpsd_pipeline_batch over independent molecules: systems (synth.System
     or compatible), their DeviceIntegrals and Params; returns per-molecule

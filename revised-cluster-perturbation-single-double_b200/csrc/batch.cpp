@@ -36,6 +36,7 @@ struct Workers {
         for (; nthreads < n; nthreads++) std::thread([this, device] { run(device); }).detach();
     }
     void run(int device) {
+        in_pool_worker() = true;
         cudaSetDevice(device);
         cudaStream_t s = nullptr;
         cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
@@ -75,6 +76,20 @@ double weight(const cpsd_system *s) {
 }
 
 }  // namespace
+
+bool &in_pool_worker() {
+    thread_local bool w = false;
+    return w;
+}
+
+void pool_submit(int nthreads, std::function<void()> job) {
+    int device = 0;
+    cudaGetDevice(&device);
+    Workers &W = workers();
+    W.ensure(nthreads, device);
+    W.submit(std::move(job));
+}
+
 }  // namespace cpsd
 
 using namespace cpsd;

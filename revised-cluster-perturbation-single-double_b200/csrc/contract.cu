@@ -278,6 +278,7 @@ int contract_timing(int enable) {
     timing().on = enable != 0;
     return CPSD_OK;
 }
+bool contract_timing_on() { return timing().on; }
 
 int timing_begin(double flops, int64_t a, int64_t b, int64_t c, int64_t kind, cudaEvent_t *end) {
     *end = nullptr;

@@ -9,7 +9,12 @@
 // (params.batch_roots), which streams every integral block once per launch
 // instead of once per root.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <condition_variable>
+#include <functional>
+#include <mutex>
+#include <string>
 #include <cstddef>
 #include <cstring>
 #include <vector>
@@ -676,6 +681,113 @@ static int ee_roots_batch(const Sys &S, const Ints &X, const cpsd_params *p, con
 
 }  // namespace cpsd
 
+namespace cpsd {
+namespace {
+
+std::atomic<bool> g_phase_overlap{true};
+
+// The SF-CIS Davidson (A) and the ground state + J^(2)/J^(3) (B) need
+// nothing from each other: they run at once on two pool workers, each on
+// its own stream, so A's latency-bound steps (one-CTA Davidson kernels,
+// small sigma contractions) fill the gaps of B's bandwidth-bound ones.  B's
+// worker then waits for A on the host and runs the excited-state orders (C)
+// with the constant-operand copies (the digits of (ab|cd) above all) kept
+// from the ground state.  The caller's stream waits for C's last work; the
+// caller's scratch holds every buffer the phases exchange.
+int overlapped_phases(const cpsd_integrals *I, const std::function<int()> &A, const std::function<int()> &B,
+                      const std::function<int()> &C) {
+    struct Shared {
+        std::mutex m;
+        std::condition_variable cv;
+        bool a_done = false;
+        int finished = 0, rc_a = CPSD_OK, rc_b = CPSD_OK;
+        std::string msg_a, msg_b;
+        int64_t launches = 0;
+        double flops = 0;
+    } d;
+    cudaEvent_t ready, end;
+    CPSD_TRY(cuda_check(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming), "event"));
+    CPSD_TRY(cuda_check(cudaEventCreateWithFlags(&end, cudaEventDisableTiming), "event"));
+    CPSD_TRY(cuda_check(cudaEventRecord(ready, stream()), "event record"));
+    const int digits = ctx().oz_digits;
+    const double min_flops = ctx().oz_min_flops, share = 0.5 * ctx().mem_share;
+    auto setup = [&] {
+        Context &c = ctx();
+        c.oz_digits = digits;
+        c.oz_min_flops = min_flops;
+        c.mem_share = share;
+        return cuda_check(cudaStreamWaitEvent(c.stream, ready, 0), "stream wait");
+    };
+    pool_submit(2, [&] {
+        // A runs on a stream of the highest priority: its short kernels are
+        // scheduled as soon as an SM frees up instead of queueing behind
+        // B's long bandwidth-bound grids
+        thread_local cudaStream_t hi = nullptr;
+        int rc = CPSD_OK;
+        if (!hi) {
+            int lo = 0, top = 0;
+            rc = cuda_check(cudaDeviceGetStreamPriorityRange(&lo, &top), "stream priorities");
+            if (rc == CPSD_OK)
+                rc = cuda_check(cudaStreamCreateWithPriority(&hi, cudaStreamNonBlocking, top), "stream create");
+        }
+        const cudaStream_t own = ctx().stream;
+        if (rc == CPSD_OK) ctx().stream = hi;
+        const int64_t l0 = ctx().launches;
+        const double f0 = ctx().flops;
+        if (rc == CPSD_OK) rc = setup();
+        if (rc == CPSD_OK) rc = A();
+        ctx().stream = own;
+        std::lock_guard<std::mutex> lock(d.m);
+        d.rc_a = rc;
+        if (rc != CPSD_OK) d.msg_a = last_error();
+        d.launches += ctx().launches - l0;
+        d.flops += ctx().flops - f0;
+        d.a_done = true;
+        d.finished++;
+        d.cv.notify_all();
+    });
+    pool_submit(2, [&] {
+        const int64_t l0 = ctx().launches;
+        const double f0 = ctx().flops;
+        int rc = setup();
+        {
+            IntegralScope keep(I);
+            if (rc == CPSD_OK) rc = B();
+            bool a_ok;
+            {
+                std::unique_lock<std::mutex> lock(d.m);
+                d.cv.wait(lock, [&] { return d.a_done; });
+                a_ok = d.rc_a == CPSD_OK;
+            }
+            if (rc == CPSD_OK && a_ok) rc = C();
+            if (rc == CPSD_OK) rc = cuda_check(cudaEventRecord(end, ctx().stream), "event record");
+        }
+        std::lock_guard<std::mutex> lock(d.m);
+        d.rc_b = rc;
+        if (rc != CPSD_OK) d.msg_b = last_error();
+        d.launches += ctx().launches - l0;
+        d.flops += ctx().flops - f0;
+        d.finished++;
+        d.cv.notify_all();
+    });
+    {
+        std::unique_lock<std::mutex> lock(d.m);
+        d.cv.wait(lock, [&] { return d.finished == 2; });
+    }
+    int rc = CPSD_OK;
+    if (d.rc_a == CPSD_OK && d.rc_b == CPSD_OK) rc = cuda_check(cudaStreamWaitEvent(stream(), end, 0), "stream wait");
+    cudaEventDestroy(ready);
+    cudaEventDestroy(end);
+    ctx().launches += d.launches;
+    ctx().flops += d.flops;
+    if (d.rc_a != CPSD_OK) return set_error(d.rc_a, "pipeline (SF-CIS): " + d.msg_a);
+    if (d.rc_b != CPSD_OK) return set_error(d.rc_b, "pipeline (ground / excited orders): " + d.msg_b);
+    return rc;
+}
+
+}  // namespace
+}  // namespace cpsd
+
 extern "C" {
 
 int cpsd_eecpsd_roots(const cpsd_system *s, const cpsd_integrals *I, const cpsd_params *p, const double *T2_1,
@@ -739,14 +851,11 @@ int cpsd_pipeline(const cpsd_system *s, const cpsd_integrals *I, const cpsd_para
     ScratchScope sc;
     double *R;
     CPSD_TRY(scratch(rlen, &R));
-    CPSD_TRY(cpsd_cis_run(s, I, p, omega_cis, R, nullptr));
     const i64 l1 = irpdso(1, v, o, 1), l2 = idsymsoc(1, v, v, 0, o, o, 0);
     double *T2_1, *T1_2, *T2_2;
     CPSD_TRY(scratch(l2, &T2_1));
     CPSD_TRY(scratch(l1, &T1_2));
     CPSD_TRY(scratch(l2, &T2_2));
-    double E2, E3;
-    CPSD_TRY(cpsd_ground(s, I, p, T2_1, T1_2, T2_2, &E2, &E3, nullptr));
     cpsd_jints J;
     CPSD_TRY(scratch(irpdso(1, o, o, 1), &J.J2_Foo));
     CPSD_TRY(scratch(irpdso(1, v, v, 1), &J.J2_Fvv));
@@ -755,24 +864,44 @@ int cpsd_pipeline(const cpsd_system *s, const cpsd_integrals *I, const cpsd_para
     CPSD_TRY(scratch(irpdso(1, o, o, 1), &J.J3_Foo));
     CPSD_TRY(scratch(irpdso(1, v, v, 1), &J.J3_Fvv));
     CPSD_TRY(scratch(idsymsoc(1, v, o, 1, v, o, 1), &J.J3_Wovvo));
-    CPSD_TRY(cpsd_calJ(s, I, T2_1, T1_2, T2_2, &J));
-    i64 k = 0, roff = 0;
-    std::vector<double> w;
-    for (i64 sym = 1; sym <= S.nirrep; sym++) {
-        i64 nr = p->estate_sym[sym - 1];
-        if (nr == 0) continue;
-        i64 len = irpdso(sym, v, o, 1);
-        w.assign((size_t)(3 * nr), 0.0);
-        CPSD_TRY(cpsd_eecpsd_roots(s, I, p, T2_1, &J, sym, nr, omega_cis + k, R + roff, w.data(), nullptr, nullptr,
-                                   nullptr, nullptr));
-        for (i64 r = 0; r < nr; r++) {
-            w2[k + r] = w[3 * r + 1];
-            w3[k + r] = w[3 * r + 2];
+    double E2, E3;
+    auto cis = [&]() -> int { return cpsd_cis_run(s, I, p, omega_cis, R, nullptr); };
+    auto ground = [&]() -> int {
+        CPSD_TRY(cpsd_ground(s, I, p, T2_1, T1_2, T2_2, &E2, &E3, nullptr));
+        return cpsd_calJ(s, I, T2_1, T1_2, T2_2, &J);
+    };
+    auto excited = [&]() -> int {
+        i64 k = 0, roff = 0;
+        std::vector<double> w;
+        for (i64 sym = 1; sym <= S.nirrep; sym++) {
+            i64 nr = p->estate_sym[sym - 1];
+            if (nr == 0) continue;
+            i64 len = irpdso(sym, v, o, 1);
+            w.assign((size_t)(3 * nr), 0.0);
+            CPSD_TRY(cpsd_eecpsd_roots(s, I, p, T2_1, &J, sym, nr, omega_cis + k, R + roff, w.data(), nullptr,
+                                       nullptr, nullptr, nullptr));
+            for (i64 r = 0; r < nr; r++) {
+                w2[k + r] = w[3 * r + 1];
+                w3[k + r] = w[3 * r + 2];
+            }
+            k += nr;
+            roff += len * nr;
         }
-        k += nr;
-        roff += len * nr;
+        return CPSD_OK;
+    };
+    if (g_phase_overlap.load() && !in_pool_worker() && !contract_timing_on()) {
+        CPSD_TRY(overlapped_phases(I, cis, ground, excited));
+    } else {
+        CPSD_TRY(cis());
+        CPSD_TRY(ground());
+        CPSD_TRY(excited());
     }
     if (nroots) *nroots = nroot;
+    return CPSD_OK;
+}
+
+int cpsd_set_phase_overlap(int on) {
+    g_phase_overlap.store(on != 0);
     return CPSD_OK;
 }
 

@@ -2,6 +2,8 @@
 // gradient program (gradient.cpp): the orbital spaces of a system, the DPD
 // views of its integrals and the device solver of solver.f90.
 #pragma once
+#include <functional>
+
 #include "ops.hpp"
 
 namespace cpsd {
@@ -42,5 +44,11 @@ int read_back(void *host, const void *dev, size_t bytes);
 // (A - w0) R1 = -cc with L.R1 = 0.  *sit receives the summed step counts.
 int solve_r1(const Sys &S, const Ints &X, const cpsd_params *p, i64 symR, i64 nb, i64 l1, const EnergyPlan *e1,
              const double *cc, const double *L, const double *w0d, double *R1, i64 *sit);
+
+// Host worker threads (batch.cpp), each with its own non-blocking stream
+// and library context, started on demand up to nthreads; in_pool_worker()
+// is true on them.
+void pool_submit(int nthreads, std::function<void()> job);
+bool &in_pool_worker();
 
 }  // namespace cpsd

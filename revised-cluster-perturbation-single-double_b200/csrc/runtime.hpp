@@ -218,6 +218,7 @@ size_t contract_noalloc_bytes(const ContractPlan *p);
 int timing_begin(double flops, int64_t a, int64_t b, int64_t c, int64_t kind, cudaEvent_t *end);
 int timing_end(cudaEvent_t end);
 int contract_timing(int enable);
+bool contract_timing_on();  // per-launch timing of this thread is on
 int contract_time(double *ms, int64_t *launches, double *flops, int reset);
 int contract_records(double *ms, double *flops, int64_t *shape, int64_t maxrec, int64_t *nrec);
 int launch_pairmap(const PairMapPlan *p, const double *in, double *out, double alpha, double beta, i64 nb = 1,
