@@ -327,7 +327,8 @@ int cpsd_eecpsd_roots(const cpsd_system *s, const cpsd_integrals *I, const cpsd_
  * SF-CIS Davidson and the ground state + J^(2)/J^(3) run at once on two
  * library worker threads (own streams), then the excited orders; results
  * equal the sequential order's.  The sequential order is used inside
- * cpsd_pipeline_batch workers and while per-launch timing is on. */
+ * cpsd_pipeline_batch workers, while per-launch timing is on and when the
+ * integrals take a fifth of the device memory or more. */
 int cpsd_pipeline(const cpsd_system *s, const cpsd_integrals *I, const cpsd_params *p,
                   double *omega_cis, double *w2, double *w3, int64_t *nroots);
 /* on = 0: run the pipeline's phases one after the other on the caller's

@@ -711,6 +711,12 @@ int overlapped_phases(const cpsd_integrals *I, const std::function<int()> &A, co
     CPSD_TRY(cuda_check(cudaEventRecord(ready, stream()), "event record"));
     const int digits = ctx().oz_digits;
     const double min_flops = ctx().oz_min_flops, share = 0.5 * ctx().mem_share;
+    // a worker keeps its scratch chunks for the next pipeline unless they
+    // are large: memory the caller's thread may need next (its own scratch
+    // or cached copies) cannot be taken back from another thread's arena
+    auto keep_small = [] {
+        if (!arena().external && arena().spare() > ((size_t)8 << 30)) arena().free_all();
+    };
     auto setup = [&] {
         Context &c = ctx();
         c.oz_digits = digits;
@@ -736,6 +742,7 @@ int overlapped_phases(const cpsd_integrals *I, const std::function<int()> &A, co
         const double f0 = ctx().flops;
         if (rc == CPSD_OK) rc = setup();
         if (rc == CPSD_OK) rc = A();
+        keep_small();
         ctx().stream = own;
         std::lock_guard<std::mutex> lock(d.m);
         d.rc_a = rc;
@@ -762,6 +769,7 @@ int overlapped_phases(const cpsd_integrals *I, const std::function<int()> &A, co
             if (rc == CPSD_OK && a_ok) rc = C();
             if (rc == CPSD_OK) rc = cuda_check(cudaEventRecord(end, ctx().stream), "event record");
         }
+        keep_small();
         std::lock_guard<std::mutex> lock(d.m);
         d.rc_b = rc;
         if (rc != CPSD_OK) d.msg_b = last_error();
@@ -889,7 +897,18 @@ int cpsd_pipeline(const cpsd_system *s, const cpsd_integrals *I, const cpsd_para
         }
         return CPSD_OK;
     };
-    if (g_phase_overlap.load() && !in_pool_worker() && !contract_timing_on()) {
+    // side by side only while the integrals take under a fifth of the device:
+    // beyond that the two phases' cached operand copies and scratch no
+    // longer fit together and the run would evict and rebuild them
+    bool small = false;
+    {
+        const Ints X = make_ints(S, I);
+        const double ib = 8.0 * (double)(X.ijkl.len() + X.ijka.len() + X.abij.len() + X.iabj.len() + X.abci.len() +
+                                         X.abcd.len());
+        size_t fr = 0, tot = 0;
+        small = cudaMemGetInfo(&fr, &tot) == cudaSuccess && ib < 0.2 * (double)tot;
+    }
+    if (small && g_phase_overlap.load() && !in_pool_worker() && !contract_timing_on()) {
         CPSD_TRY(overlapped_phases(I, cis, ground, excited));
     } else {
         CPSD_TRY(cis());
