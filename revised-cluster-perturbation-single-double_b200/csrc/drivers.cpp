@@ -712,10 +712,15 @@ int overlapped_phases(const cpsd_integrals *I, const std::function<int()> &A, co
     const int digits = ctx().oz_digits;
     const double min_flops = ctx().oz_min_flops, share = 0.5 * ctx().mem_share;
     // a worker keeps its scratch chunks for the next pipeline unless they
-    // are large: memory the caller's thread may need next (its own scratch
-    // or cached copies) cannot be taken back from another thread's arena
+    // take over a quarter of the device: memory the caller's thread may need
+    // next (its own scratch or cached copies) cannot be taken back from
+    // another thread's arena
+    static const size_t dev_total = [] {
+        size_t f = 0, t = 0;
+        return cudaMemGetInfo(&f, &t) == cudaSuccess ? t : (size_t)0;
+    }();
     auto keep_small = [] {
-        if (!arena().external && arena().spare() > ((size_t)8 << 30)) arena().free_all();
+        if (!arena().external && dev_total > 0 && arena().spare() > dev_total / 4) arena().free_all();
     };
     auto setup = [&] {
         Context &c = ctx();
@@ -905,8 +910,11 @@ int cpsd_pipeline(const cpsd_system *s, const cpsd_integrals *I, const cpsd_para
         const Ints X = make_ints(S, I);
         const double ib = 8.0 * (double)(X.ijkl.len() + X.ijka.len() + X.abij.len() + X.iabj.len() + X.abci.len() +
                                          X.abcd.len());
-        size_t fr = 0, tot = 0;
-        small = cudaMemGetInfo(&fr, &tot) == cudaSuccess && ib < 0.2 * (double)tot;
+        static const size_t tot = [] {
+            size_t f = 0, t = 0;
+            return cudaMemGetInfo(&f, &t) == cudaSuccess ? t : (size_t)0;
+        }();
+        small = ib < 0.2 * (double)tot;
     }
     if (small && g_phase_overlap.load() && !in_pool_worker() && !contract_timing_on()) {
         CPSD_TRY(overlapped_phases(I, cis, ground, excited));

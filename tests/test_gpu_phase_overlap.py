@@ -49,3 +49,19 @@ def test_overlap_reports_phase_errors():
     good = api.make_params(s, batch_roots=1)
     om, w2, w3 = api.pipeline(s, sc, ints, good)
     assert len(om) == s.nroots and np.isfinite(w3).all()
+
+
+def test_overlap_reports_ground_phase_errors():
+    """A failure in the ground-state phase (its DIIS solver rejects the
+    subspace size) while SF-CIS succeeds beside it."""
+    s = synth.make("c2v_nmo48")
+    api.init(s.nirrep, s.dirprd)
+    ints = api.DeviceIntegrals(s)
+    sc = api.make_system(s)
+    bad = api.make_params(s, batch_roots=1)
+    bad.diis_dim = 20  # above the device DIIS limit of 16
+    api.set_phase_overlap(True)
+    with pytest.raises(api.CpsdError, match="ground"):
+        api.pipeline(s, sc, ints, bad)
+    om, w2, w3 = api.pipeline(s, sc, ints, api.make_params(s, batch_roots=1))
+    assert np.isfinite(w3).all()
