@@ -84,7 +84,11 @@ struct View {
     __device__ const i64 *ky(const SegDev &sg) const { return SWAP ? sg.kSA : sg.kSB; }
 };
 
-// short K: thread = row, 8 columns in registers
+// short K: thread = row, 8 columns in registers.  The contracted indices
+// go in chunks of 32: lane l decodes index k0 + l once and loads its 8
+// second-operand values into the warp's shared buffer, then every lane runs
+// the 32 indices with its own first-operand loads in flight (same sums, in
+// the same order, as one index at a time).
 template <bool SWAP>
 __global__ void __launch_bounds__(NW * 32) k_narrow_rows(const TaskDev *__restrict__ tasks,
                                                          const SegDev *__restrict__ segs,
@@ -104,6 +108,8 @@ __global__ void __launch_bounds__(NW * 32) k_narrow_rows(const TaskDev *__restri
     double acc[NARROW_COLS];
 #pragma unroll
     for (int c = 0; c < NARROW_COLS; c++) acc[c] = 0.0;
+    __shared__ i64 fxs[NW][32];
+    __shared__ double ys[NW][NARROW_COLS][32];
     for (int si = 0; si < tk.nseg; si++) {
         const SegDev &sg = segs[tk.seg0 + si];
         const i64 ox = rok ? v.xrow(sg, r) : 0;
@@ -111,14 +117,24 @@ __global__ void __launch_bounds__(NW * 32) k_narrow_rows(const TaskDev *__restri
 #pragma unroll
         for (int c = 0; c < NARROW_COLS; c++) oy[c] = c < ncol ? v.ycol(sg, item.c0 + c) : 0;
         const i64 *kx = v.kx(sg), *ky = v.ky(sg);
-#pragma unroll 4
-        for (i64 k = 0; k < sg.K; k++) {
-            i64 fx, fy;
-            kdecode(k, sg, kx, ky, &fx, &fy);
-            const double x = rok ? __ldg(X + ox + fx) : 0.0;
+        for (i64 k0 = 0; k0 < sg.K; k0 += 32) {
+            const int nk = (int)min((i64)32, sg.K - k0);
+            __syncwarp();
+            if (lane < nk) {
+                i64 fx, fy;
+                kdecode(k0 + lane, sg, kx, ky, &fx, &fy);
+                fxs[warp][lane] = fx;
 #pragma unroll
-            for (int c = 0; c < NARROW_COLS; c++)
-                if (c < ncol) acc[c] = fma(x, __ldg(Y + oy[c] + fy), acc[c]);
+                for (int c = 0; c < NARROW_COLS; c++) ys[warp][c][lane] = c < ncol ? __ldg(Y + oy[c] + fy) : 0.0;
+            }
+            __syncwarp();
+#pragma unroll 8
+            for (int j = 0; j < nk; j++) {
+                const double x = rok ? __ldg(X + ox + fxs[warp][j]) : 0.0;
+#pragma unroll
+                for (int c = 0; c < NARROW_COLS; c++)
+                    if (c < ncol) acc[c] = fma(x, ys[warp][c][j], acc[c]);
+            }
         }
     }
     if (!rok) return;
