@@ -676,8 +676,35 @@ __device__ void warp_dgesl(const double *a, int lda, int n, const int *ipvt, dou
 // R -= (<L|R> / ||L||) L, the reference's orthogonalR2L (L is normalised,
 // so it divides by the norm)
 __device__ void block_orth(double *R, const double *L, int n, double *sh) {
-    double nrm = sqrt(block_dot(L, L, n, sh));
-    double dot = block_dot(L, R, n, sh);
+    // L.L and L.R in one pass and one reduction, each summed in
+    // block_dot's order (strided per-thread sums, shuffle-down, warp totals
+    // in warp order)
+    __shared__ double red[2][DT / 32];
+    double aa = 0.0, ab = 0.0;
+    for (int k = threadIdx.x; k < n; k += DT) {
+        const double l = L[k];
+        aa = fma(l, l, aa);
+        ab = fma(l, R[k], ab);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        aa += __shfl_down_sync(0xffffffffu, aa, o);
+        ab += __shfl_down_sync(0xffffffffu, ab, o);
+    }
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+        red[0][w] = aa;
+        red[1][w] = ab;
+    }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+        double t = 0.0;
+        for (int i = 0; i < DT / 32; i++) t += red[threadIdx.x][i];
+        sh[threadIdx.x] = t;
+    }
+    __syncthreads();
+    double nrm = sqrt(sh[0]);
+    double dot = sh[1];
+    __syncthreads();
     double f = -dot / nrm;
     for (int k = threadIdx.x; k < n; k += DT) R[k] += f * L[k];
     __syncthreads();
