@@ -729,7 +729,15 @@ int overlapped_phases(const cpsd_integrals *I, const std::function<int()> &A, co
         c.mem_share = share;
         return cuda_check(cudaStreamWaitEvent(c.stream, ready, 0), "stream wait");
     };
-    pool_submit(2, [&] {
+    // every pipeline in this section holds two workers (its ground-state
+    // worker waits for its SF-CIS one), so the pool keeps two per caller:
+    // with fewer, concurrent callers' waiting workers could take them all
+    static std::atomic<int> callers{0};
+    const int held = ++callers;
+    struct Leave {
+        ~Leave() { callers--; }
+    } leave;
+    pool_submit(2 * held, [&] {
         // A runs on a stream of the highest priority: its short kernels are
         // scheduled as soon as an SM frees up instead of queueing behind
         // B's long bandwidth-bound grids
@@ -758,7 +766,7 @@ int overlapped_phases(const cpsd_integrals *I, const std::function<int()> &A, co
         d.finished++;
         d.cv.notify_all();
     });
-    pool_submit(2, [&] {
+    pool_submit(2 * held, [&] {
         const int64_t l0 = ctx().launches;
         const double f0 = ctx().flops;
         int rc = setup();

@@ -65,3 +65,37 @@ def test_overlap_reports_ground_phase_errors():
         api.pipeline(s, sc, ints, bad)
     om, w2, w3 = api.pipeline(s, sc, ints, api.make_params(s, batch_roots=1))
     assert np.isfinite(w3).all()
+
+
+def test_concurrent_callers_do_not_starve_the_workers():
+    """Three host threads run overlapped pipelines at once (ctypes releases
+    the GIL): each pipeline holds two library workers, its ground-state one
+    waiting for its SF-CIS one, so the pool must grow with the callers; the
+    energies equal the same pipelines run alone."""
+    import threading
+    names = ["c2v_nmo48", "c2v_nmo48", "c2v_nmo48"]
+    mols = [synth.make(n, seed=k) for k, n in enumerate(names)]
+    api.init(mols[0].nirrep, mols[0].dirprd)
+    api.set_mixed(0)  # the callers' threads start in the library's default (FP64) mode
+    ints = [api.DeviceIntegrals(s) for s in mols]
+    api.set_phase_overlap(True)
+    alone = [api.pipeline(s, api.make_system(s), d, api.make_params(s, batch_roots=1)) for s, d in zip(mols, ints)]
+    out, errs = [None] * len(mols), []
+
+    def run(k):
+        try:
+            s = mols[k]
+            out[k] = api.pipeline(s, api.make_system(s), ints[k], api.make_params(s, batch_roots=1))
+        except Exception as e:  # reported below
+            errs.append(repr(e))
+
+    th = [threading.Thread(target=run, args=(k,), daemon=True) for k in range(len(mols))]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join(timeout=300)
+    assert not any(t.is_alive() for t in th), "pipelines did not finish"
+    assert not errs, errs
+    for a, b in zip(out, alone):
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)
