@@ -730,8 +730,10 @@ int overlapped_phases(const cpsd_integrals *I, const std::function<int()> &A, co
         return cuda_check(cudaStreamWaitEvent(c.stream, ready, 0), "stream wait");
     };
     // every pipeline in this section holds two workers (its ground-state
-    // worker waits for its SF-CIS one), so the pool keeps two per caller:
-    // with fewer, concurrent callers' waiting workers could take them all
+    // worker waits for its SF-CIS one), so the pool keeps two per caller and
+    // concurrent callers' phases run side by side instead of queueing (the
+    // queue is first in, first out and SF-CIS is queued first, so a waiting
+    // worker never holds up the phase it waits for)
     static std::atomic<int> callers{0};
     const int held = ++callers;
     struct Leave {
