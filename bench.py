@@ -4,12 +4,16 @@
 One step = the whole pipeline of the workload: SF-CIS Davidson (residual
 1e-8) for every requested root, ground CPS(D) T^(1)/T^(2), the J^(2)/J^(3)
 intermediates and EE-CPS(D-3) orders 1-3 for every root, with the integrals
-resident in HBM.  Default workload: D2h, nmo 200, nocc 10/8, 5 spin-flip
-roots (synthetic seeded integrals, see synth.py).  The headline value is
-the mixed mode (contractions of at least 1 GFLOP on the int8 tensor cores
-with --digits 7-bit digits per FP64 value, exact integer sums, FP64
-everywhere else); the plain FP64 path is timed beside it (fp64_path) and
-the largest deviation of any energy from it is reported.
+resident in HBM.  Default workload: the large run, D2h, nmo 400, nocc
+20/18, 10 spin-flip roots (93.5 GB of synthetic seeded integrals built on
+the device, see synth.py); --config d2h_nmo200 gives the precision-form
+workload (D2h, nmo 200, nocc 10/8, 5 roots).  The headline value is the
+mixed mode (contractions of at least 1 GFLOP on the int8 tensor cores with
+--digits 7-bit digits per FP64 value, exact integer sums, FP64 everywhere
+else; 6 digits on d2h_nmo400, 5 elsewhere unless given); the plain FP64
+path is timed beside it (fp64_path), every root's deviation from it is
+reported, and the line fails its gate (gate.pass = false, exit status 3)
+when any excitation energy, w^(2) or w^(3) is more than 1 micro-Eh away.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--config NAME] [--digits D]
   python bench.py --impl reference ...   (CPU restatement on the host cores)
@@ -31,6 +35,14 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 METRIC = "SF-CPS(D) roots/sec: mixed+batched vs FP64 GPU at ≤1 µEh; contraction TFLOP/s"
+# digits per workload that keep every energy within the 1 micro-Eh gate:
+# the synthetic nmo-400 system has |w^(3)| up to 1.5e3 Eh, where 5 digits
+# leave 1.6e-5 Eh and 6 digits 1.6e-7 Eh
+DEFAULT_DIGITS = {"d2h_nmo400": 6}
+GATE_EH = 1e-6
+# integrals above this size are built on the device (the host build is too
+# slow) and the CPU baseline gets them by a copy from there
+DEVICE_BUILD_BYTES = 16e9
 
 
 def parse():
@@ -39,12 +51,16 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="d2h_nmo200")
+    ap.add_argument("--config", default="d2h_nmo400")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-threads", type=int, default=0)
-    ap.add_argument("--digits", type=int, default=5,
-                    help="7-bit digits per FP64 value on the int8 tensor cores (0 = FP64 path only)")
+    ap.add_argument("--digits", type=int, default=-1,
+                    help="7-bit digits per FP64 value on the int8 tensor cores (0 = FP64 path only; "
+                         "default 6 on d2h_nmo400, 5 elsewhere)")
+    ap.add_argument("--cpu-samples", type=int, default=1,
+                    help="samples of the CPU baseline (one root's chain each) after one warm-up pass")
+    ap.add_argument("--cpu-worker", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--no-fp64-path", action="store_true", help="skip timing the plain FP64 path beside the headline")
     ap.add_argument("--no-phase-overlap", action="store_true",
                     help="run the pipeline's phases one after the other (SF-CIS is otherwise beside the ground state)")
@@ -54,7 +70,10 @@ def parse():
     ap.add_argument("--wave-gb", type=float, default=140.0, help="device-memory budget of one --case batch wave")
     ap.add_argument("--case", default="", choices=["", "ladder", "grad", "batch"],
                     help="time one contraction on its own (kernel profiling) instead of the pipeline")
-    return ap.parse_args()
+    a = ap.parse_args()
+    if a.digits < 0:
+        a.digits = DEFAULT_DIGITS.get(a.config, 5)
+    return a
 
 
 def workload_desc(s, name):
@@ -138,25 +157,63 @@ def measured_fp64_peak(torch):
     return 2.0 * n ** 3 / best / 1e12
 
 
-def cpu_reference_sample(name, threads, steps=1, warmup=0):
-    """The CPU restatement (oracle) on a bounded sample of the workload: one
-    root's full chain (CIS for it, ground, J, EE orders 1-3) timed per stage;
-    the workload's roots/s is extrapolated from the stage times:
-    nroot / (T_cis * nroot + T_ground + T_J + nroot * T_root)."""
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def is_big(name):
+    """integrals too large for the host build: built on the device"""
+    from cpsd_b200 import synth
+    return synth.config_integral_bytes(name) > DEVICE_BUILD_BYTES
+
+
+def big_workload(name):
+    """(built on the device?, synth.System; host integrals only when not)"""
+    from cpsd_b200 import synth
+    big = is_big(name)
+    return big, synth.make(name, host_ints=not big)
+
+
+def cpu_worker(args):
+    """The CPU restatement (oracle) on a bounded sample of the workload, in
+    a process of its own (both arms run this same function the same way):
+    one warm-up pass (the c2v_nmo48 pipeline: thread pool, BLAS, first
+    touch), then --cpu-samples samples of one root's whole chain (CIS
+    Davidson for that root, ground CPS(D), J2/J3, EE orders 1-3), each
+    stage timed; the workload's roots/s is extrapolated from the mean stage
+    times as nroot / (T_cis nroot + T_ground + T_J + T_root nroot).  Large
+    workloads' integrals are built on the GPU and copied to host memory
+    before anything is timed (input generation only: the timed work is the
+    oracle on the host cores).  Prints one JSON line."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import conftest  # noqa: F401  (registers the package)
     import oracle_ffi as of
     from cpsd_b200 import synth
-    s = synth.make(name)
+    threads = args.cpu_threads or os.cpu_count() or 1
+    t_start = time.time()
+    of.Oracle(synth.make("c2v_nmo48"), nthreads=threads).pipeline()
+    big, s = big_workload(args.config)
+    if big:
+        import torch
+        d = synth.device_integrals(s)
+        for k in api_keys():
+            s.ints[k] = d[k].cpu().numpy()
+            d[k] = None
+        del d
+        torch.cuda.empty_cache()
     nroot = s.nroots
     s.estate_sym[:] = 0
     s.estate_sym[0] = 1
     orc = of.Oracle(s, nthreads=threads)
-    small = synth.make("c2v_nmo48")
-    for _ in range(warmup):
-        of.Oracle(small, nthreads=threads).pipeline()
     samples = []
-    for _ in range(max(steps, 1)):
+    for _ in range(max(args.cpu_samples, 1)):
         t0 = time.perf_counter()
         om, R, _ = orc.cis()
         t1 = time.perf_counter()
@@ -168,8 +225,39 @@ def cpu_reference_sample(name, threads, steps=1, warmup=0):
         t4 = time.perf_counter()
         samples.append((t1 - t0, t2 - t1, t3 - t2, t4 - t3))
     tc, tg, tj, tr = np.mean(np.array(samples), axis=0)
-    t_all = tc * nroot + tg + tj + tr * nroot
-    return nroot / t_all, dict(t_cis_per_root=tc, t_ground=tg, t_J=tj, t_root=tr, sample_wall=sum(samples[-1]))
+    v = nroot / (tc * nroot + tg + tj + tr * nroot)
+    print(json.dumps({"value": v, "threads": threads, "samples": len(samples), "nroot": nroot,
+                      "stage_seconds": dict(t_cis_per_root=tc, t_ground=tg, t_J=tj, t_root=tr),
+                      "sample_wall_s": float(np.mean([sum(x) for x in samples])),
+                      "worker_wall_s": time.time() - t_start}), flush=True)
+
+
+def api_keys():
+    return ("ijkl", "ijka", "abij", "iabj", "abci", "abcd")
+
+
+def cpu_baseline(config, threads, samples):
+    """CPU baseline by cpu_worker in a fresh process: the same protocol,
+    process state and sample count for the GPU arm's cpu_baseline leg and
+    the reference arm.  Returns the cpu_baseline object (or None with the
+    reason on failure)."""
+    cmd = [sys.executable, os.path.join(ROOT, "bench.py"), "--cpu-worker", "--config", config,
+           "--cpu-threads", str(threads), "--cpu-samples", str(samples)]
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK")}
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=3600, env=env, cwd=ROOT)
+    lines = [ln for ln in r.stdout.strip().splitlines() if ln.startswith("{")]
+    if r.returncode != 0 or not lines:
+        return None, f"cpu worker failed (rc {r.returncode}): {r.stderr.strip()[-300:]}"
+    w = json.loads(lines[-1])
+    big = is_big(config)
+    return {"value": w["value"], "unit": "roots/s", "cores": w["threads"], "cpu_model": cpu_model(),
+            "kind": "port",
+            "sample": (f"one root's chain (CIS Davidson for it, ground CPS(D), J2/J3, EE orders 1-3) of "
+                       f"{config}, {w['samples']} sample(s) after one warm-up pass (c2v_nmo48 pipeline) in a "
+                       f"fresh process; stage times extrapolated to the workload's {w['nroot']} roots" +
+                       ("; integrals built on the GPU and copied to host memory before timing" if big else "")),
+            "stage_seconds": {k: round(x, 4) for k, x in w["stage_seconds"].items()},
+            "sample_wall_s": round(w["sample_wall_s"], 2)}, None
 
 
 def run_reference(args, rank, world):
@@ -177,18 +265,18 @@ def run_reference(args, rank, world):
         return
     threads = args.cpu_threads or os.cpu_count() or 1
     t0 = time.time()
-    v, info = cpu_reference_sample(args.config, threads, steps=args.steps, warmup=args.warmup)
-    from cpsd_b200 import synth  # noqa
+    cpu, why = cpu_baseline(args.config, threads, args.cpu_samples)
+    if cpu is None:
+        print(json.dumps({"impl": "reference", "unavailable": why}), flush=True)
+        return
+    v = cpu["value"]
     line = {
         "metric": METRIC, "value": v, "unit": "roots/s", "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * info["sample_wall"], "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": 1e3 * cpu["sample_wall_s"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
         "config": {"workload": args.config, "note": "CPU restatement of the reference's FP64 path "
-                   "(the Fortran reference cannot be built here: no Fortran compiler)"},
-        "cpu_baseline": {"value": v, "unit": "roots/s", "cores": threads, "kind": "port",
-                         "sample": "one root's chain (CIS, ground CPS(D), J2/J3, EE orders 1-3) per step, "
-                                   "stage times extrapolated to all roots of the workload",
-                         "stage_seconds": {k: round(x, 4) for k, x in info.items()}},
+                   "(the Fortran reference cannot be built: no Fortran compiler here or on the GPU box)"},
+        "cpu_baseline": cpu,
         "e2e": {"value": v, "unit": "roots/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "wall_s": round(time.time() - t0, 1),
     }
@@ -243,11 +331,14 @@ def run_ours(args, rank, world, local_rank):
     from cpsd_b200 import api, synth
 
     torch.cuda.set_device(local_rank)
-    s = synth.make(args.config)
+    big, s = big_workload(args.config)
     api.init(s.nirrep, s.dirprd)
     api.use_torch_stream()
     api.set_phase_overlap(not args.no_phase_overlap)
-    ints = api.DeviceIntegrals(s)
+    if big:  # built on the device (same values as the host build up to summation order)
+        ints = api.DeviceIntegrals.from_tensors(synth.device_integrals(s))
+    else:
+        ints = api.DeviceIntegrals(s)
     sysc = api.make_system(s)
     par = api.make_params(s, batch_roots=1)
     stream = torch.cuda.current_stream()
@@ -296,8 +387,13 @@ def run_ours(args, rank, world, local_rank):
     value = world * s.nroots * args.steps / (ms_max / 1e3)
     value64 = world * s.nroots * args.steps / (ms64 / 1e3)
     dev_fp64 = max(float(np.max(np.abs(np.asarray(a) - np.asarray(b)))) for a, b in zip(out, out64))
+    per_root_dev = np.max(np.abs(np.asarray(out) - np.asarray(out64)), axis=0)  # over (w0, w2, w3)
+    gate = {"bound_eh": GATE_EH, "max_abs_dev_eh": dev_fp64, "pass": bool(dev_fp64 <= GATE_EH),
+            "against": "the plain FP64 GPU path on the same inputs (itself tested against the oracle: "
+                       "1e-9 Eh per root at d2h_nmo200)"}
     om, w2, w3 = out
     step_ms = ms_max / args.steps
+    int_gb = ints.nbytes / 1e9
 
     # per-launch CUDA-event timing of every contraction launch in one extra
     # step of the headline mode: roofline of the digit GEMM (int8 tensor
@@ -329,9 +425,20 @@ def run_ours(args, rank, world, local_rank):
             t_tensor = f_ * pairs / (int8_peak * 1e12) if int8_peak else 0.0
             t_hbm = float(b_) / (hbm * 1e9) if hbm else 0.0
             att_ms += 1e3 * max(t_tensor, t_hbm)
+        # DRAM traffic per launch: the algorithmic bytes (digit tiles once,
+        # C read and written per K chunk) times the traffic / algorithmic
+        # ratio ncu measured on this kernel (1.03 on the nmo-80 ladder,
+        # profiles/k_oz_gemm_ladder_nmo80.md); traffic grows with the tiles
+        alg = rshape[sel][:, 1].astype(float) + rshape[sel][:, 2].astype(float)
+        nsel = max(int(sel.sum()), 1)
         roof = {"bound": "tensor", "kernel": f"k_oz_gemm (tcgen05 kind::i8, {digits} digits, {pairs} digit products)",
                 "achieved": ach, "peak": int8_peak, "unit": "TOPS (int8)",
-                "frac": ach / int8_peak if int8_peak else None, "traffic": None,
+                "frac": ach / int8_peak if int8_peak else None,
+                "traffic": 1.03 * float(alg.sum()) / nsel,
+                "traffic_note": "bytes per launch: algorithmic bytes (digit tiles + C read/write) x 1.03, the "
+                                "dram__bytes_read+write / algorithmic ratio of the ncu capture of this kernel "
+                                "(nmo-80 ladder, profiles/k_oz_gemm_ladder_nmo80.md)",
+                "algorithmic_bytes_per_launch": float(alg.sum()) / nsel,
                 "peak_source": "measured cuBLASLt int8 GEMM 8192^3 (torch._int_mm) on this GPU",
                 "fp64_equivalent_tflops": g_fl / (g_ms / 1e3) / 1e12 if g_ms > 0 else 0.0,
                 "share_of_step": g_ms / step_ms, "launches_per_step": int(sel.sum()),
@@ -353,39 +460,59 @@ def run_ours(args, rank, world, local_rank):
                ("pair_transforms", rkind == 40))}
 
     # end to end through the public API with host buffers: H2D of every
-    # integral tensor from pinned memory, the pipeline, results back on the host
+    # integral tensor from pinned memory, the pipeline, results back on the
+    # host (the pipeline returns its energies on the host)
     e2e = None
     if not args.no_e2e:
-        api.set_mixed(digits, 1.0)
-        host = {k: torch.from_numpy(s.ints[k]).pin_memory() for k in api.DeviceIntegrals.KEYS
-                if s.ints[k] is not None}
-        host["eorb"] = torch.from_numpy(s.eorb).pin_memory()
-        h2d = sum(v.numel() * 8 for v in host.values())
-        d2h = 3 * s.nroots * 8
-        torch.cuda.synchronize()
-        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        f0.record(stream)
-        for _ in range(args.steps):
-            for k, v in host.items():
-                ints.t[k].copy_(v, non_blocking=True)
-            step()
-        f1.record(stream)
-        torch.cuda.synchronize()
-        t2 = torch.tensor([f0.elapsed_time(f1)], dtype=torch.float64, device="cuda")
-        if world > 1:
-            dist.all_reduce(t2, op=dist.ReduceOp.MAX)
-        e2e = {"value": world * s.nroots * args.steps / (float(t2.item()) / 1e3), "unit": "roots/s",
-               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
-        api.set_mixed(0)
+        import psutil
+        nloc = int(os.environ.get("LOCAL_WORLD_SIZE", "1"))
+        need = float(ints.nbytes)
+        avail = float(psutil.virtual_memory().available)
+        if need * nloc > 0.8 * avail:
+            e2e = {"value": None, "unit": "roots/s", "skipped": f"pinned host copies of {need / 1e9:.1f} GB per rank "
+                   f"x {nloc} ranks exceed the host memory available ({avail / 1e9:.0f} GB)"}
+        else:
+            api.set_mixed(digits, 1.0)
+            host = {}
+            for k, t in ints.t.items():
+                if t is not None:
+                    h = torch.empty(t.numel(), dtype=torch.float64, pin_memory=True)
+                    h.copy_(t)
+                    host[k] = h
+            h2d = sum(v.numel() * 8 for v in host.values())
+            d2h = 3 * s.nroots * 8
+            e2e_steps = min(args.steps, 5) if big else args.steps
+            torch.cuda.synchronize()
+            f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            f0.record(stream)
+            for _ in range(e2e_steps):
+                for k, v in host.items():
+                    ints.t[k].copy_(v, non_blocking=True)
+                step()
+            f1.record(stream)
+            torch.cuda.synchronize()
+            t2 = torch.tensor([f0.elapsed_time(f1)], dtype=torch.float64, device="cuda")
+            if world > 1:
+                dist.all_reduce(t2, op=dist.ReduceOp.MAX)
+            e2e = {"value": world * s.nroots * e2e_steps / (float(t2.item()) / 1e3), "unit": "roots/s",
+                   "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "steps": e2e_steps,
+                   "note": "every step copies all integral tensors from pinned host memory, runs cpsd_pipeline "
+                           "and reads the energies back"}
+            api.set_mixed(0)
+            del host
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = args.cpu_threads or os.cpu_count() or 1
-        v, info = cpu_reference_sample(args.config, threads, steps=1)
-        cpu = {"value": v, "unit": "roots/s", "cores": threads, "kind": "port",
-               "sample": "one root's chain (CIS, ground CPS(D), J2/J3, EE orders 1-3), stage times "
-                         "extrapolated to all roots of the workload",
-               "stage_seconds": {k: round(x, 4) for k, x in info.items()}}
+        if big:  # the worker builds the integrals on the GPU: give the memory back first
+            import gc
+            del ints
+            gc.collect()
+            api.release_device_cache()
+            torch.cuda.empty_cache()
+        cpu, why = cpu_baseline(args.config, threads, args.cpu_samples)
+        if cpu is None:
+            cpu = {"value": None, "unit": "roots/s", "unavailable": why}
     if rank == 0:
         mode = (f"mixed: contractions >= 1 GFLOP on the int8 tensor cores with {digits} 7-bit digits per FP64 "
                 f"value (exact int32 sums, FP64 epilogue); everything else FP64" if digits else "FP64")
@@ -395,11 +522,13 @@ def run_ours(args, rank, world, local_rank):
             "vs_baseline": None, "dtype": "f64 (int8 digits)" if digits else "f64",
             "data": "synthetic (seeded generator, synth.py)",
             "config": {"workload": workload_desc(s, args.config), "inputs": "resident in HBM, "
-                       f"{ints.nbytes / 1e9:.2f} GB of integrals (larger than L2)",
+                       f"{int_gb:.2f} GB of integrals (larger than L2)" + (", built on the device" if big else ""),
                        "parallelism": f"replicas x{world}", "roots_batched": True, "mode": mode,
                        "phases": "SF-CIS in order with the ground state" if args.no_phase_overlap else
                        "SF-CIS beside the ground state + J2/J3 (two worker streams), then the excited orders"},
             "max_abs_dev_vs_fp64_eh": dev_fp64,
+            "per_root_dev_vs_fp64_eh": [float(x) for x in per_root_dev],
+            "gate": gate,
             "fp64_path": {"value": value64, "unit": "roots/s", "ms_per_step": ms64 / args.steps,
                           "gpu_launches": launches64, "contraction_tflops": flops64 / (ms64 / 1e3) / 1e12},
             "roofline": roof or roof64,
@@ -412,6 +541,8 @@ def run_ours(args, rank, world, local_rank):
                         "w3": [float(x) for x in w3]},
         }
         print(json.dumps(line), flush=True)
+    if not gate["pass"]:
+        sys.exit(3)
 
 
 def run_case(args):
@@ -649,6 +780,11 @@ def run_batch(args):
 
 def main():
     args = parse()
+    if args.cpu_worker:
+        import __graft_entry__ as ge
+        ge.load_package()
+        cpu_worker(args)
+        return
     if args.case == "grad":
         run_grad(args)
         return
@@ -664,6 +800,8 @@ def main():
     if args.impl == "reference":
         if world > 1 and rank != 0:
             return
+        import __graft_entry__ as ge
+        ge.load_package()
         run_reference(args, rank, world)
         return
     if world > 1:

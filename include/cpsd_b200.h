@@ -27,6 +27,8 @@ extern "C" {
 #define CPSD_EMEM (-3)    /* device allocation failed */
 #define CPSD_ECUDA (-4)   /* CUDA runtime error */
 #define CPSD_ESTATE (-5)  /* library not initialised */
+#define CPSD_ENUM (-6)    /* numerical failure: an eigen-solve did not converge */
+#define CPSD_ETIMEOUT (-7) /* a bounded device wait (int8-digit path) timed out; results invalid */
 
 /* ------------------------------------------------------------------ setup */
 /* Symmetry tables; replaces module mod_symm (src/lib_mod/mod_symm.f:1-9) as
@@ -58,9 +60,21 @@ int cpsd_contract_time(double *ms, int64_t *launches, double *flops, int reset);
  * scale per row / column, exact int32 sums and an FP64 epilogue; the error
  * per element is below (digits+1) K 128^-digits max|a_row| max|b_col|.
  * digits = 0 (default) keeps the FP64 tensor-pipe path everywhere.
- * cpsd_mixed_error returns 1 if a wait in that path ever timed out. */
+ * cpsd_mixed_error returns 1 if a wait in that path timed out since the
+ * last reset; cpsd_cis_run, cpsd_ground, cpsd_eecpsd_roots and so
+ * cpsd_pipeline / cpsd_pipeline_batch check it themselves and return
+ * CPSD_ETIMEOUT instead of results. */
 int cpsd_set_mixed(int digits, double min_gflop);
 int cpsd_mixed_error(int reset);
+/* Davidson subspace problem (src/lib_cc/mod_davidson.f90:185-219, dgeev on
+ * the Ritz matrix Abar): a step whose Abar is symmetric to 1e-12 of its
+ * largest element takes the parallel Jacobi on the symmetric part (same
+ * eigenpairs to rounding); any other takes the general Hessenberg + Francis
+ * QR solve.  Counts, for the calling thread since the last reset, of steps
+ * that took the general solve and of Ritz values with an imaginary part
+ * above 1e-10 (the reference prints a warning for each; their real parts
+ * are used, as there). */
+int cpsd_davidson_stats(int64_t *nonsym_steps, int64_t *imag_warnings, int reset);
 
 /* -------------------------------------------------------------- size math */
 /* irpdso (src/libsrint/irpdso.f:1-52) */
@@ -123,19 +137,35 @@ int cpsd_vv2v_dpd_222(const double *v1, const int64_t *p1_1, const int64_t *p1_2
                       double *v3, const int64_t *p3_1, const int64_t *p3_2, int64_t iop3_12,
                       int64_t sym3, const char *type3, double fact1, double fact2);
 
-/* No counterpart in the reference.  cpsd_vv2v_dpd_444 with the same
- * arguments and results, for callers that may not allocate device memory
+/* vv2v_dpd_224 (src/libsrint/vv2v_dpd_224.f90:16-19): V1, V2 2-index, V3
+ * 4-index (the outer product V3(pqrs) += fact1 V1(pq) V2(rs)) */
+int cpsd_vv2v_dpd_224(const double *v1, const int64_t *p1_1, const int64_t *p1_2, int64_t iop1_12,
+                      int64_t sym1, const char *type1,
+                      const double *v2, const int64_t *p2_1, const int64_t *p2_2, int64_t iop2_12,
+                      int64_t sym2, const char *type2,
+                      double *v3, const int64_t *p3_1, const int64_t *p3_2, int64_t iop3_12,
+                      const int64_t *p3_3, const int64_t *p3_4, int64_t iop3_34, int64_t sym3,
+                      const char *type3, double fact1, double fact2);
+
+/* No counterpart in the reference.  cpsd_vv2v_dpd_444's contraction with
+ * the same arguments, for callers that may not allocate device memory
  * during the call (all of HBM handed to their own pool, or no cudaMalloc /
  * cudaFree stalls allowed in a time-critical loop): the contraction's plan
  * tables and split-K partial tiles live in a fixed region compiled into
  * the library, CPSD_NOALLOC_SCRATCH_BYTES (32 MiB) per device, instead of
- * cudaMalloc'ed memory.  A contraction that needs more is rejected with
- * CPSD_EARG before any work is queued.  Nothing in the region has to start
- * at zero.  The region is shared by all calls on a device: calls queued on
- * one stream are ordered, calls that overlap in time (other streams, other
- * host threads) race.  The first call on each device does the set-up
- * (region address, kernel attributes); make it before any stream capture
- * begins. */
+ * cudaMalloc'ed memory.  It always runs the FP64 tile kernel (k_contract),
+ * whatever cpsd_set_mixed selected and whether or not cpsd_vv2v_dpd_444
+ * would take its narrow-output kernels: results equal cpsd_vv2v_dpd_444's
+ * in FP64 mode to rounding, and differ from its mixed-mode results by that
+ * mode's digit error.  A contraction that needs more than the region is
+ * rejected with CPSD_EARG before any work is queued.  Nothing in the
+ * region has to start at zero.  The region is shared by all calls on a
+ * device: calls queued on one stream are ordered, calls that overlap in
+ * time (other streams, other host threads) race.  The plan tables are
+ * copied from pageable host memory, which CUDA starts only after the work
+ * queued earlier on the stream: a call can block the host until then.  The
+ * first call on each device does the set-up (region address, kernel
+ * attributes); make it before any stream capture begins. */
 #define CPSD_NOALLOC_SCRATCH_BYTES (32u << 20)
 int cpsd_vv2v_dpd_444_noalloc(const double *v1, const int64_t *p1_1, const int64_t *p1_2, int64_t iop1_12,
                               const int64_t *p1_3, const int64_t *p1_4, int64_t iop1_34, int64_t sym1,
@@ -151,7 +181,11 @@ int cpsd_vv2v_dpd_444_noalloc(const double *v1, const int64_t *p1_1, const int64
  * lower case + trailing underscore, every argument by reference, hidden
  * character lengths last), so the reference's call sites
  * (src/lib_cc/mod_contract.f90:104-107) link against it unchanged when
- * igpu=1 and prec=8. */
+ * igpu=1 and prec=8.  Like the reference's dispatcher, which STOPs on a
+ * failed check (src/libsrint/vv2v_dpd_444.f90:150-200), it prints the
+ * error and ends the program (exit status 1) when the call fails.
+ * vv2v_dpd_444_ierr_ (no counterpart in the reference) takes one more
+ * integer, ierr, after fact2 and returns the code there instead. */
 void vv2v_dpd_444_(const double *v1, const int64_t *p1_1, const int64_t *p1_2, const int64_t *iop1_12,
                    const int64_t *p1_3, const int64_t *p1_4, const int64_t *iop1_34, const int64_t *sym1,
                    const char *type1,
@@ -162,6 +196,16 @@ void vv2v_dpd_444_(const double *v1, const int64_t *p1_1, const int64_t *p1_2, c
                    const int64_t *p3_3, const int64_t *p3_4, const int64_t *iop3_34, const int64_t *sym3,
                    const char *type3, const double *fact1, const double *fact2,
                    size_t len_type1, size_t len_type2, size_t len_type3);
+void vv2v_dpd_444_ierr_(const double *v1, const int64_t *p1_1, const int64_t *p1_2, const int64_t *iop1_12,
+                        const int64_t *p1_3, const int64_t *p1_4, const int64_t *iop1_34, const int64_t *sym1,
+                        const char *type1,
+                        const double *v2, const int64_t *p2_1, const int64_t *p2_2, const int64_t *iop2_12,
+                        const int64_t *p2_3, const int64_t *p2_4, const int64_t *iop2_34, const int64_t *sym2,
+                        const char *type2,
+                        double *v3, const int64_t *p3_1, const int64_t *p3_2, const int64_t *iop3_12,
+                        const int64_t *p3_3, const int64_t *p3_4, const int64_t *iop3_34, const int64_t *sym3,
+                        const char *type3, const double *fact1, const double *fact2, int64_t *ierr,
+                        size_t len_type1, size_t len_type2, size_t len_type3);
 
 /* ------------------------------------------------- tensor descriptor
  * POD mirror of type(opt) (src/lib_cc/mod_operator.f90:8-25): populations,
@@ -263,6 +307,12 @@ int cpsd_debug_narrow_plan(const cpsd_opt *v1, const char *t1, const cpsd_opt *v
 int cpsd_debug_ozaki_plan(const cpsd_opt *v1, const char *t1, const cpsd_opt *v2, const char *t2,
                           const cpsd_opt *v3, const char *t3, int64_t nb, int64_t sA, int64_t sB, int64_t sC,
                           int digits, const void **tables, int64_t *sizes);
+/* the Davidson step's general eigen-solve (one warp, n <= 32) on the
+ * row-major n x n host matrix A: eigenvalues wr / wi and row-major V whose
+ * columns are dgeev's right eigenvectors (a complex pair k, k+1 with
+ * wi[k] > 0: real and imaginary parts; unit norm, largest component real);
+ * *sweeps = QR sweeps or -1 when the iteration did not converge */
+int cpsd_debug_geev(const double *A_host, int64_t n, double *wr, double *wi, double *V_host, int64_t *sweeps);
 int cpsd_debug_pairmap_plan(const cpsd_opt *in, int64_t op0, int64_t op1, int64_t tgt0, int64_t tgt1,
                             const void **blocks, int64_t *nblocks, const void **idx, const void **sgn,
                             int64_t *nidx, int64_t *lterms, int64_t *rterms);

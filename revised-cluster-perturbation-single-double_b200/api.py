@@ -119,6 +119,50 @@ def mixed_error(reset=True):
     return rc
 
 
+def contract_records(maxrec=16384):
+    """Per-launch records of the contraction timing buffer (timing must
+    have been on, see contract_timing): milliseconds, useful flops, kind
+    (0-3 FP64 tile shapes, 10/11 digit slicing, 12 digit GEMM, 20/21 narrow,
+    30/31 Davidson, 32 solver, 40 pair transform) and size triple."""
+    ms, fl = np.zeros(maxrec), np.zeros(maxrec)
+    sh = np.zeros(4 * maxrec, np.int64)
+    nr = I64()
+    check(lib().cpsd_contract_records(ms.ctypes.data_as(ctypes.c_void_p), fl.ctypes.data_as(ctypes.c_void_p),
+                                      sh.ctypes.data_as(ctypes.c_void_p), I64(maxrec), ctypes.byref(nr)),
+          "cpsd_contract_records")
+    k = nr.value
+    shape = sh[:4 * k].reshape(k, 4)
+    return ms[:k], fl[:k], shape[:, 3], shape[:, :3]
+
+
+def contract_timing(on=True, reset=True):
+    """per-launch CUDA-event timing of the library's kernels on/off"""
+    check(lib().cpsd_contract_timing(ctypes.c_int(1 if on else 0)), "cpsd_contract_timing")
+    if reset:
+        check(lib().cpsd_contract_time(None, None, None, ctypes.c_int(1)), "cpsd_contract_time")
+
+
+def davidson_stats(reset=True):
+    """(steps that solved the general non-symmetric Ritz problem, complex Ritz
+    values met) on this thread since the last reset"""
+    a, b = I64(), I64()
+    check(lib().cpsd_davidson_stats(ctypes.byref(a), ctypes.byref(b), 1 if reset else 0), "cpsd_davidson_stats")
+    return a.value, b.value
+
+
+def geev(A):
+    """The Davidson step's general eigen-solve on a host matrix (n <= 32):
+    (wr, wi, V, sweeps) with dgeev's eigenvector columns in V."""
+    A = np.ascontiguousarray(A, dtype=np.float64)
+    n = A.shape[0]
+    wr, wi, V = np.zeros(n), np.zeros(n), np.zeros((n, n))
+    sw = I64()
+    check(lib().cpsd_debug_geev(A.ctypes.data_as(ctypes.c_void_p), I64(n), wr.ctypes.data_as(ctypes.c_void_p),
+                                wi.ctypes.data_as(ctypes.c_void_p), V.ctypes.data_as(ctypes.c_void_p),
+                                ctypes.byref(sw)), "cpsd_debug_geev")
+    return wr, wi, V, sw.value
+
+
 def opt(pops, iops, sym, t):
     o = Opt()
     check(lib().cpsd_opt_init(ctypes.byref(o), arr8(pops[0]), arr8(pops[1]), arr8(pops[2]), arr8(pops[3]),

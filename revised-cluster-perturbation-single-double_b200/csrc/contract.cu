@@ -408,18 +408,30 @@ int launch_contract(const ContractPlan *p, const double *A, const double *B, dou
 //    one stream are ordered and safe;
 //  - the first call on each device does the set-up (symbol address of the
 //    region, kernel attributes); make that first call before any stream
-//    capture begins.
+//    capture begins;
+//  - the plan tables are copied from the plan's pageable host vectors
+//    (pinned staging would itself be an allocation); CUDA lets such a copy
+//    start only after the work queued earlier on the stream, so a call can
+//    block the host until then.
 namespace {
 __device__ __align__(256) unsigned char g_noalloc_scratch[CPSD_NOALLOC_SCRATCH_BYTES];
 
 constexpr int NOALLOC_MAXDEV = 64;
-unsigned char *g_noalloc_base[NOALLOC_MAXDEV];  // per device ordinal; null until set up
+// region address per device ordinal (null until set up); the set-up runs
+// under a lock so that two host threads' first calls do not race on it
+std::atomic<unsigned char *> g_noalloc_base[NOALLOC_MAXDEV];
+std::mutex g_noalloc_setup_mutex;
 
 int noalloc_setup(unsigned char **base) {
     int dev = 0;
     CPSD_TRY(cuda_check(cudaGetDevice(&dev), "cudaGetDevice"));
     if (dev < 0 || dev >= NOALLOC_MAXDEV) return set_error(CPSD_EARG, "device ordinal beyond 63");
-    if (!g_noalloc_base[dev]) {
+    if (!g_noalloc_base[dev].load()) {
+        std::lock_guard<std::mutex> lock(g_noalloc_setup_mutex);
+        if (g_noalloc_base[dev].load()) {
+            *base = g_noalloc_base[dev].load();
+            return CPSD_OK;
+        }
         void *p = nullptr;
         CPSD_TRY(cuda_check(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress(noalloc scratch)"));
         CPSD_TRY(cuda_check(cudaFuncSetAttribute(k_contract<128, 64, 4, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -430,9 +442,9 @@ int noalloc_setup(unsigned char **base) {
                                                  smem_bytes<64, 128>()), "smem attr"));
         CPSD_TRY(cuda_check(cudaFuncSetAttribute(k_contract<64, 64, 2, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                  smem_bytes<64, 64>()), "smem attr"));
-        g_noalloc_base[dev] = (unsigned char *)p;
+        g_noalloc_base[dev].store((unsigned char *)p);
     }
-    *base = g_noalloc_base[dev];
+    *base = g_noalloc_base[dev].load();
     return CPSD_OK;
 }
 
@@ -473,6 +485,14 @@ int launch_contract_noalloc(const ContractPlan *p, const double *A, const double
     const SegDev *sg = (const SegDev *)d_segs;
     const TileDev *tl = (const TileDev *)d_tiles;
     const int bm = TILE_BM[p->cfg], bn = TILE_BN[p->cfg];
+    cudaEvent_t e0 = nullptr, e1 = nullptr;  // timing records, as launch_contract keeps them
+    if (timing().on) {
+        CPSD_TRY(timing_event(&e0));
+        CPSD_TRY(timing_event(&e1));
+        timing().flops.push_back(p->flops);
+        timing().shape.push_back({p->ntasks, p->nsegs, p->ntiles, p->cfg});
+        CPSD_TRY(cuda_check(cudaEventRecord(e0, stream()), "event record"));
+    }
     switch (p->cfg) {
     case 0:
         k_contract<128, 64, 4, 2><<<p->ntiles, NT, smem_bytes<128, 64>(), stream()>>>(A, B, C, tk, sg, tl, alpha, part);
@@ -489,6 +509,7 @@ int launch_contract_noalloc(const ContractPlan *p, const double *A, const double
     }
     count_launch();
     ctx().flops += p->flops;
+    if (e1) CPSD_TRY(cuda_check(cudaEventRecord(e1, stream()), "event record"));
     if (p->nreduce > 0) {
         k_splitk_reduce<<<p->nreduce * (bm * bn / NT), NT, 0, stream()>>>((const int *)d_reduce, tk, part, C, alpha,
                                                                           bm, bn);

@@ -327,9 +327,13 @@ int davidson(const Sys &S, const Ints &I, const cpsd_params *p, i64 sym, i64 nro
         CPSD_TRY(th.wait(it));
     }
     int *hdr = (int *)mailbox();
-    const size_t hbytes = offsetof(DavState, warn_imag);
+    const size_t hbytes = offsetof(DavState, maxError);
     CPSD_TRY(read_back(hdr, st, hbytes));
-    if (iters) *iters = ((const DavState *)hdr)->iterations;
+    const DavState *hst = (const DavState *)hdr;
+    if (iters) *iters = hst->iterations;
+    ctx().dav_nonsym_steps += hst->nonsym_steps;
+    ctx().dav_imag_warnings += hst->warn_imag;
+    if (hst->eig_fail) return set_error(CPSD_ENUM, "Davidson: QR iteration on the Ritz matrix did not converge");
     // eigen test of the converged roots (mod_davidson.f90:525-542)
     CPSD_TRY(cis_sigma(S, I, sym, fileEV + 1, n + 1, b.AB[0], n, nroot));
     CPSD_TRY(dav_final_launch(st, b));
@@ -398,7 +402,8 @@ int cpsd_cis_run(const cpsd_system *s, const cpsd_integrals *I, const cpsd_param
         roff += n * nroot;
     }
     if (iterations) *iterations = itsum;
-    return cuda_check(cudaStreamSynchronize(stream()), "cis sync");
+    CPSD_TRY(cuda_check(cudaStreamSynchronize(stream()), "cis sync"));
+    return digit_error_check();
 }
 
 int cpsd_ground(const cpsd_system *s, const cpsd_integrals *I, const cpsd_params *p, double *T2_1, double *T1_2,
@@ -442,7 +447,7 @@ int cpsd_ground(const cpsd_system *s, const cpsd_integrals *I, const cpsd_params
     CPSD_TRY(read_back(h, dE, sizeof h));
     if (E2_host) *E2_host = h[0];
     if (E3_host) *E3_host = h[1];
-    return CPSD_OK;
+    return digit_error_check();
 }
 
 int cpsd_calJ(const cpsd_system *s, const cpsd_integrals *I, const double *T2_1, const double *T1_2,
@@ -857,7 +862,8 @@ int cpsd_eecpsd_roots(const cpsd_system *s, const cpsd_integrals *I, const cpsd_
         tot += it;
     }
     if (solver_iters) *solver_iters = tot;
-    return CPSD_OK;
+    // the J^(2) / J^(3) contractions of this thread are covered here too
+    return digit_error_check();
 }
 
 int cpsd_pipeline(const cpsd_system *s, const cpsd_integrals *I, const cpsd_params *p, double *omega_cis,

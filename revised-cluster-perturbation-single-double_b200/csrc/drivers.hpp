@@ -45,6 +45,10 @@ int read_back(void *host, const void *dev, size_t bytes);
 int solve_r1(const Sys &S, const Ints &X, const cpsd_params *p, i64 symR, i64 nb, i64 l1, const EnergyPlan *e1,
              const double *cc, const double *L, const double *w0d, double *R1, i64 *sit);
 
+// CPSD_ETIMEOUT (word cleared) if a bounded wait of the int8-digit path
+// timed out on this thread since the last check; synchronises the stream
+int digit_error_check();
+
 // Host worker threads (batch.cpp), each with its own non-blocking stream
 // and library context, started on demand up to nthreads; in_pool_worker()
 // is true on them.

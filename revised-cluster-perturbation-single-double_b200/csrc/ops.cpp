@@ -4,8 +4,10 @@
 
 #include <algorithm>
 
+#include "drivers.hpp"
 #include "narrow.cuh"
 #include "ozaki.cuh"
+#include "solvers.cuh"
 
 #include <cstring>
 #include <mutex>
@@ -258,6 +260,23 @@ bool evict_cached_copies() { return evict_const_except(nullptr); }
 
 namespace {
 
+}  // namespace
+
+// CPSD_ETIMEOUT when a bounded wait of the digit path timed out on this
+// thread since the last check (the word is cleared): the results of the
+// operations since then are invalid.  Synchronises the stream.
+int digit_error_check() {
+    if (!ctx().oz_err) return CPSD_OK;
+    int h = 0;
+    CPSD_TRY(read_back(&h, ctx().oz_err, sizeof h));
+    if (!h) return CPSD_OK;
+    CPSD_TRY(cuda_check(cudaMemsetAsync(ctx().oz_err, 0, sizeof(int), stream()), "clear error word"));
+    return set_error(CPSD_ETIMEOUT, "int8-digit tensor-core path: a bounded device wait timed out; the results "
+                                    "of this call are invalid");
+}
+
+namespace {
+
 int oz_error_word(int **err) {
     if (!ctx().oz_err) {
         CPSD_TRY(cuda_check(cudaMalloc(&ctx().oz_err, sizeof(int)), "cudaMalloc(error word)"));
@@ -322,8 +341,12 @@ int launch_ozaki(const OzPlan *oz, const double *A, const double *B, double *C, 
     CPSD_TRY(digits_of(oz, true, A, &ad, &ea));
     CPSD_TRY(digits_of(oz, false, B, &bd, &eb));
     cudaEvent_t end;
-    // record: groups, bytes of the digit tiles the launch streams, tiles
-    CPSD_TRY(timing_begin(oz->flops, (i64)oz->groups.size(), oz->adig + oz->bdig, (i64)oz->tiles.size(), 12, &end));
+    // record: groups, bytes of the digit tiles the launch streams, bytes of
+    // C read and written (once per K chunk)
+    i64 cbytes = 0;
+    for (const OzGroup &g : oz->groups) cbytes += 16 * g.M * g.N;
+    const i64 nchunk = (oz->kt_max + oz->kt_chunk - 1) / oz->kt_chunk;
+    CPSD_TRY(timing_begin(oz->flops, (i64)oz->groups.size(), oz->adig + oz->bdig, cbytes * nchunk, 12, &end));
     for (int kt0 = 0; kt0 < oz->kt_max; kt0 += oz->kt_chunk)
         CPSD_TRY(oz_gemm(oz->S, oz->dev, ad, bd, ea, eb, C, alpha, kt0, kt0 + oz->kt_chunk, err));
     return timing_end(end);
@@ -793,6 +816,34 @@ int cpsd_mixed_error(int reset) {
     return h;
 }
 
+int cpsd_davidson_stats(int64_t *nonsym_steps, int64_t *imag_warnings, int reset) {
+    if (nonsym_steps) *nonsym_steps = ctx().dav_nonsym_steps;
+    if (imag_warnings) *imag_warnings = ctx().dav_imag_warnings;
+    if (reset) ctx().dav_nonsym_steps = ctx().dav_imag_warnings = 0;
+    return CPSD_OK;
+}
+
+int cpsd_debug_geev(const double *A_host, int64_t n, double *wr, double *wi, double *V_host, int64_t *sweeps) {
+    if (n < 1 || n > DAV_MAXD) return set_error(CPSD_EARG, "n must be 1..32");
+    ScratchScope sc;
+    double *dA, *dwr, *dwi, *dV;
+    int *dsw;
+    CPSD_TRY(scratch(n * n, &dA));
+    CPSD_TRY(scratch(n, &dwr));
+    CPSD_TRY(scratch(n, &dwi));
+    CPSD_TRY(scratch(n * n, &dV));
+    CPSD_TRY(scratch(1, &dsw));
+    CPSD_TRY(cuda_check(cudaMemcpyAsync(dA, A_host, sizeof(double) * n * n, cudaMemcpyHostToDevice, stream()), "geev A"));
+    CPSD_TRY(geev_probe(dA, (int)n, dwr, dwi, dV, dsw));
+    CPSD_TRY(read_back(wr, dwr, sizeof(double) * n));
+    CPSD_TRY(read_back(wi, dwi, sizeof(double) * n));
+    CPSD_TRY(read_back(V_host, dV, sizeof(double) * n * n));
+    int sw = 0;
+    CPSD_TRY(read_back(&sw, dsw, sizeof sw));
+    if (sweeps) *sweeps = sw;
+    return CPSD_OK;
+}
+
 int64_t cpsd_irpdso(int64_t sym, const int64_t *popp, const int64_t *popq, int64_t ioppq) {
     return irpdso(sym, popp, popq, ioppq);
 }
@@ -917,6 +968,61 @@ int cpsd_vv2v_dpd_222(const double *v1, const int64_t *p1_1, const int64_t *p1_2
     return engine(a, t1, b, t2, c, t3, fact1, fact2);
 }
 
+// vv2v_dpd_224 (src/libsrint/vv2v_dpd_224.f90:16-19): V1(pq) and V2(rs)
+// become V1(pq+-) and V2(rs+-) over one-orbital dummy slots, so the
+// contraction over + and - is the outer product V3(pqrs)
+int cpsd_vv2v_dpd_224(const double *v1, const int64_t *p1_1, const int64_t *p1_2, int64_t iop1_12, int64_t sym1,
+                      const char *type1, const double *v2, const int64_t *p2_1, const int64_t *p2_2,
+                      int64_t iop2_12, int64_t sym2, const char *type2, double *v3, const int64_t *p3_1,
+                      const int64_t *p3_2, int64_t iop3_12, const int64_t *p3_3, const int64_t *p3_4,
+                      int64_t iop3_34, int64_t sym3, const char *type3, double fact1, double fact2) {
+    Ten a = ten(p1_1, p1_2, ZORB, ZORB, iop1_12, 1, sym1, (double *)v1);
+    Ten b = ten(p2_1, p2_2, ZORB, ZORB, iop2_12, 1, sym2, (double *)v2);
+    Ten c = ten(p3_1, p3_2, p3_3, p3_4, iop3_12, iop3_34, sym3, v3);
+    char t1[5], t2[5], t3[5];
+    type4(type1, 2, t1);
+    type4(type2, 2, t2);
+    t1[2] = t2[2] = '+';
+    t1[3] = t2[3] = '-';
+    type4(type3, 4, t3);
+    return engine(a, t1, b, t2, c, t3, fact1, fact2);
+}
+
+// Fortran binding: the reference's dispatcher STOPs on a failed check
+// (src/libsrint/vv2v_dpd_444.f90:150-200); this one prints the library's
+// message and ends the program with status 1, so a Fortran caller never
+// continues with V3 untouched.  vv2v_dpd_444_ierr_ returns the code instead.
+static int vv2v_dpd_444_f(const double *v1, const int64_t *p1_1, const int64_t *p1_2, const int64_t *iop1_12,
+                          const int64_t *p1_3, const int64_t *p1_4, const int64_t *iop1_34, const int64_t *sym1,
+                          const char *type1, const double *v2, const int64_t *p2_1, const int64_t *p2_2,
+                          const int64_t *iop2_12, const int64_t *p2_3, const int64_t *p2_4, const int64_t *iop2_34,
+                          const int64_t *sym2, const char *type2, double *v3, const int64_t *p3_1,
+                          const int64_t *p3_2, const int64_t *iop3_12, const int64_t *p3_3, const int64_t *p3_4,
+                          const int64_t *iop3_34, const int64_t *sym3, const char *type3, const double *fact1,
+                          const double *fact2, size_t len_type1, size_t len_type2, size_t len_type3) {
+    char t1[5], t2[5], t3[5];
+    type4(type1, len_type1 < 4 ? (int)len_type1 : 4, t1);
+    type4(type2, len_type2 < 4 ? (int)len_type2 : 4, t2);
+    type4(type3, len_type3 < 4 ? (int)len_type3 : 4, t3);
+    return cpsd_vv2v_dpd_444(v1, p1_1, p1_2, *iop1_12, p1_3, p1_4, *iop1_34, *sym1, t1, v2, p2_1, p2_2, *iop2_12,
+                             p2_3, p2_4, *iop2_34, *sym2, t2, v3, p3_1, p3_2, *iop3_12, p3_3, p3_4, *iop3_34, *sym3,
+                             t3, *fact1, *fact2);
+}
+
+void vv2v_dpd_444_ierr_(const double *v1, const int64_t *p1_1, const int64_t *p1_2, const int64_t *iop1_12,
+                        const int64_t *p1_3, const int64_t *p1_4, const int64_t *iop1_34, const int64_t *sym1,
+                        const char *type1, const double *v2, const int64_t *p2_1, const int64_t *p2_2,
+                        const int64_t *iop2_12, const int64_t *p2_3, const int64_t *p2_4, const int64_t *iop2_34,
+                        const int64_t *sym2, const char *type2, double *v3, const int64_t *p3_1,
+                        const int64_t *p3_2, const int64_t *iop3_12, const int64_t *p3_3, const int64_t *p3_4,
+                        const int64_t *iop3_34, const int64_t *sym3, const char *type3, const double *fact1,
+                        const double *fact2, int64_t *ierr, size_t len_type1, size_t len_type2,
+                        size_t len_type3) {
+    *ierr = vv2v_dpd_444_f(v1, p1_1, p1_2, iop1_12, p1_3, p1_4, iop1_34, sym1, type1, v2, p2_1, p2_2, iop2_12, p2_3,
+                           p2_4, iop2_34, sym2, type2, v3, p3_1, p3_2, iop3_12, p3_3, p3_4, iop3_34, sym3, type3,
+                           fact1, fact2, len_type1, len_type2, len_type3);
+}
+
 void vv2v_dpd_444_(const double *v1, const int64_t *p1_1, const int64_t *p1_2, const int64_t *iop1_12,
                    const int64_t *p1_3, const int64_t *p1_4, const int64_t *iop1_34, const int64_t *sym1,
                    const char *type1, const double *v2, const int64_t *p2_1, const int64_t *p2_2,
@@ -925,14 +1031,14 @@ void vv2v_dpd_444_(const double *v1, const int64_t *p1_1, const int64_t *p1_2, c
                    const int64_t *iop3_12, const int64_t *p3_3, const int64_t *p3_4, const int64_t *iop3_34,
                    const int64_t *sym3, const char *type3, const double *fact1, const double *fact2,
                    size_t len_type1, size_t len_type2, size_t len_type3) {
-    char t1[5], t2[5], t3[5];
-    type4(type1, len_type1 < 4 ? (int)len_type1 : 4, t1);
-    type4(type2, len_type2 < 4 ? (int)len_type2 : 4, t2);
-    type4(type3, len_type3 < 4 ? (int)len_type3 : 4, t3);
-    int rc = cpsd_vv2v_dpd_444(v1, p1_1, p1_2, *iop1_12, p1_3, p1_4, *iop1_34, *sym1, t1, v2, p2_1, p2_2, *iop2_12,
-                               p2_3, p2_4, *iop2_34, *sym2, t2, v3, p3_1, p3_2, *iop3_12, p3_3, p3_4, *iop3_34, *sym3,
-                               t3, *fact1, *fact2);
-    if (rc != CPSD_OK) fprintf(stderr, "vv2v_dpd_444: error %d\n", rc);
+    int rc = vv2v_dpd_444_f(v1, p1_1, p1_2, iop1_12, p1_3, p1_4, iop1_34, sym1, type1, v2, p2_1, p2_2, iop2_12, p2_3,
+                            p2_4, iop2_34, sym2, type2, v3, p3_1, p3_2, iop3_12, p3_3, p3_4, iop3_34, sym3, type3, fact1,
+                            fact2, len_type1, len_type2, len_type3);
+    if (rc != CPSD_OK) {
+        fprintf(stderr, "ERROR: vv2v_dpd_444: %s (code %d)\n", last_error().c_str(), rc);
+        fflush(stderr);
+        exit(1);
+    }
 }
 
 int cpsd_opt_init(cpsd_opt *t, const int64_t *popp, const int64_t *popq, const int64_t *popr, const int64_t *pops,

@@ -148,6 +148,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
     unsigned char *stages = (unsigned char *)(((uintptr_t)oz_smem + 1023) & ~(uintptr_t)1023);
     __shared__ __align__(8) uint64_t full[Cf::NST], empty[Cf::NST], done;
     __shared__ uint32_t tmem_base_sh;
+    __shared__ int fail_sh;  // some wait of this CTA timed out
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const OzTile tl = tiles[blockIdx.x];
     const OzGroup g = groups[tl.g];
@@ -167,6 +168,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
             mbar_init(&empty[s], 1);
         }
         mbar_init(&done, 1);
+        fail_sh = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     tc_fence_before();
@@ -174,12 +176,13 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
     tc_fence_after();
     const uint32_t tmem = tmem_base_sh;
     bool ok = true;
+    int issued = 0;  // producer: stages whose bulk copies it started
 
     if (warp == 4) {
         if (lane == 0) {  // producer
             const int8_t *Ab = Adig + g.aoff + (size_t)tl.mt * KT * Cf::A_STAGE;
             const int8_t *Bb = Bdig + g.boff + (size_t)tl.nt * KT * Cf::B_STAGE;
-            for (int i = 0; i < nk; i++) {
+            for (int i = 0; i < nk; i++, issued++) {
                 const int s = i % Cf::NST, u = i / Cf::NST;
                 if (u > 0 && !mbar_wait(&empty[s], (u - 1) & 1)) {
                     ok = false;
@@ -279,7 +282,23 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
         }
         if (!fin) ok = false;
     }
-    if (!ok) atomicExch(err, 1);
+    if (!ok) {
+        atomicExch(err, 1);
+        atomicOr(&fail_sh, 1);
+    }
+    __syncthreads();
+    if (fail_sh) {
+        // drain before TMEM is freed and the CTA's shared memory is given
+        // back: the producer waits out its bulk copies still in flight (only
+        // the last NST stages can be: every earlier stage was consumed
+        // before its slot was refilled), the MMA issuer waits for the
+        // completion of every MMA it issued (its final commit); both waits
+        // are bounded like the others
+        if (warp == 4 && lane == 0)
+            for (int i = issued > Cf::NST ? issued - Cf::NST : 0; i < issued; i++)
+                mbar_wait(&full[i % Cf::NST], (i / Cf::NST) & 1);
+        if (warp == 5 && lane == 0) mbar_wait(&done, 0);
+    }
     tc_fence_before();
     __syncthreads();
     if (warp == 5) {

@@ -40,6 +40,9 @@ struct Context {
     int oz_digits = 0;
     double oz_min_flops = 1e9;
     int *oz_err = nullptr;
+    // Davidson steps that solved the general (non-symmetric) Ritz problem and
+    // complex Ritz values met (the reference's imaginary-eigenvalue warning)
+    int64_t dav_nonsym_steps = 0, dav_imag_warnings = 0;
     // fraction of the free device memory this thread may plan its scratch
     // for (molecules running side by side share it)
     double mem_share = 1.0;

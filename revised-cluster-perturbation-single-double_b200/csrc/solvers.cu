@@ -247,6 +247,374 @@ __device__ void block_jacobi(double *S, double *V, int n) {
     __syncthreads();
 }
 
+// ------------------------------------------------ general real eigenproblem
+// Eigenvalues and right eigenvectors of a general real n x n matrix (n <= 32)
+// by one warp, in the form LAPACK's dgeev('N', 'V') returns them to the
+// reference's Davidson (src/lib_cc/mod_davidson.f90:185-186): wr / wi the
+// eigenvalues, a complex pair at (k, k + 1) with wi[k] > 0 first; column k
+// of V the eigenvector of a real eigenvalue, columns k and k + 1 the real and
+// imaginary parts of the eigenvector of wr[k] + i wi[k]; every eigenvector
+// of unit 2-norm with its largest component real.  Method (Golub & Van Loan,
+// Matrix Computations, 4th ed., sections 7.4-7.5 and 7.6.4):
+//   1. Householder reduction to upper Hessenberg form, H = Z^T A Z;
+//   2. Francis double-shift QR sweeps on the active window [l, hi] to real
+//      Schur form T, Z accumulated; a subdiagonal element at most eps times
+//      its two diagonal neighbours deflates; sweeps 10 and 20 of a window
+//      use the ad-hoc exceptional shift of the LAPACK/EISPACK QR codes;
+//      a 2 x 2 block with real eigenvalues is rotated to triangular form;
+//   3. eigenvectors of T by back substitution (lane e solves for eigenvalue
+//      e, complex arithmetic for a pair), then V = Z X and normalisation.
+// Lane i owns row i or column i of every update; every lane walks the same
+// control flow (deflation tests, shifts and reflectors are computed from
+// shared values by all lanes alike).  H, Z and X are row-major with leading
+// dimension GL (odd, so that a lane per row hits distinct banks); H is
+// destroyed, Z and X are scratch, V (leading dimension DAV_MAXD, may alias
+// Z) receives the vectors.  Returns the number of QR sweeps, or -1 when a
+// window did not converge within 30 max(10, n) sweeps.
+constexpr int GL = DAV_MAXD + 1;
+
+__device__ __forceinline__ double warp_allsum(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ double warp_allmax(double v) {
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+struct cplx {
+    double re, im;
+};
+__device__ __forceinline__ cplx cmul(cplx a, cplx b) { return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+__device__ __forceinline__ cplx csub(cplx a, cplx b) { return {a.re - b.re, a.im - b.im}; }
+// a / b by Smith's scaling (R. L. Smith, CACM 5 (1962) 435); |b| >= tiny
+__device__ cplx cdiv(cplx a, cplx b, double tiny) {
+    if (fabs(b.re) + fabs(b.im) < tiny) b = {tiny, 0.0};
+    if (fabs(b.re) >= fabs(b.im)) {
+        const double r = b.im / b.re, d = b.re + b.im * r;
+        return {(a.re + a.im * r) / d, (a.im - a.re * r) / d};
+    }
+    const double r = b.re / b.im, d = b.im + b.re * r;
+    return {(a.re * r + a.im) / d, (a.im * r - a.re) / d};
+}
+
+// x of the 2 x 2 system [[t00 - lam, t01], [t10, t11 - lam]] x = -rhs
+// (Cramer's rule with the determinant kept away from zero)
+__device__ void solve2(double t00, double t01, double t10, double t11, cplx lam, cplx r0, cplx r1, double tiny,
+                       cplx *x0, cplx *x1) {
+    const cplx a = {t00 - lam.re, -lam.im}, d = {t11 - lam.re, -lam.im};
+    const cplx det = csub(cmul(a, d), {t01 * t10, 0.0});
+    const cplx b0 = {-r0.re, -r0.im}, b1 = {-r1.re, -r1.im};
+    *x0 = cdiv(csub(cmul(b0, d), {t01 * b1.re, t01 * b1.im}), det, tiny);
+    *x1 = cdiv(csub(cmul(a, b1), {t10 * b0.re, t10 * b0.im}), det, tiny);
+}
+
+__device__ int warp_geev(double *H, double *Z, double *X, double *V, double *wr, double *wi, int n) {
+    const int lane = threadIdx.x & 31;
+    const double eps = 2.220446049250313e-16;
+    for (int i = 0; i < n; i++)
+        if (lane < n) Z[i * GL + lane] = (i == lane) ? 1.0 : 0.0;
+    __syncwarp();
+    // ---- 1. Hessenberg form: reflector k zeroes column k below row k + 1
+    for (int k = 0; k + 2 < n; k++) {
+        const double xi = (lane > k && lane < n) ? H[lane * GL + k] : 0.0;
+        const double tail2 = warp_allsum(lane > k + 1 ? xi * xi : 0.0);
+        if (tail2 == 0.0) continue;  // column already reduced (same on every lane)
+        const double x0 = H[(k + 1) * GL + k];
+        const double alpha = -copysign(sqrt(tail2 + x0 * x0), x0);
+        const double beta = 1.0 / (alpha * (alpha - x0));  // 2 / v^T v
+        if (lane < n) X[lane] = (lane == k + 1) ? x0 - alpha : (lane > k + 1 ? xi : 0.0);
+        __syncwarp();
+        if (lane >= k && lane < n) {  // H <- P H, lane = column
+            double s = 0.0;
+            for (int i = k + 1; i < n; i++) s += X[i] * H[i * GL + lane];
+            s *= beta;
+            for (int i = k + 1; i < n; i++) H[i * GL + lane] -= s * X[i];
+            if (lane == k) {
+                H[(k + 1) * GL + k] = alpha;
+                for (int i = k + 2; i < n; i++) H[i * GL + k] = 0.0;
+            }
+        }
+        __syncwarp();
+        if (lane < n) {  // H <- H P and Z <- Z P, lane = row
+            double s = 0.0, t = 0.0;
+            for (int j = k + 1; j < n; j++) {
+                s += H[lane * GL + j] * X[j];
+                t += Z[lane * GL + j] * X[j];
+            }
+            s *= beta;
+            t *= beta;
+            for (int j = k + 1; j < n; j++) {
+                H[lane * GL + j] -= s * X[j];
+                Z[lane * GL + j] -= t * X[j];
+            }
+        }
+        __syncwarp();
+    }
+    // 1-norm of H: the scale of the deflation test when both diagonal
+    // neighbours vanish
+    double cn = 0.0;
+    if (lane < n)
+        for (int i = 0; i < n; i++) cn += fabs(H[i * GL + lane]);
+    const double anorm = warp_allmax(cn);
+    const double tiny = fmax(eps * anorm, 1.0e-300);
+    // ---- 2. real Schur form
+    const int maxits = 30 * max(10, n);
+    int hi = n - 1, its = 0, sweeps = 0;
+    while (hi >= 0) {
+        int l = hi;
+        for (; l > 0; l--) {
+            double s = fabs(H[(l - 1) * GL + l - 1]) + fabs(H[l * GL + l]);
+            if (s == 0.0) s = anorm;
+            if (fabs(H[l * GL + l - 1]) <= eps * s) break;
+        }
+        __syncwarp();
+        if (l > 0 && lane == 0) H[l * GL + l - 1] = 0.0;
+        __syncwarp();
+        if (l == hi) {  // 1 x 1 block
+            if (lane == 0) {
+                wr[hi] = H[hi * GL + hi];
+                wi[hi] = 0.0;
+            }
+            hi--;
+            its = 0;
+            continue;
+        }
+        if (l == hi - 1) {  // 2 x 2 block
+            const int m = hi - 1;
+            const double a = H[m * GL + m], b = H[m * GL + hi], c = H[hi * GL + m], d = H[hi * GL + hi];
+            const double p = 0.5 * (a - d), disc = p * p + b * c;
+            if (disc >= 0.0) {
+                // real pair: rotate by G = [cs -sn; sn cs] whose first column
+                // is the eigenvector (z, c) of lam1 = d + z
+                const double z = p + copysign(sqrt(disc), p);
+                const double lam1 = d + z, lam2 = (z != 0.0) ? d - (b * c) / z : lam1;
+                const double r = hypot(z, c), cs = z / r, sn = c / r;
+                if (lane >= m && lane < n) {
+                    const double hm = H[m * GL + lane], hh = H[hi * GL + lane];
+                    H[m * GL + lane] = cs * hm + sn * hh;
+                    H[hi * GL + lane] = -sn * hm + cs * hh;
+                }
+                __syncwarp();
+                if (lane < n) {
+                    if (lane <= hi) {
+                        const double hm = H[lane * GL + m], hh = H[lane * GL + hi];
+                        H[lane * GL + m] = cs * hm + sn * hh;
+                        H[lane * GL + hi] = -sn * hm + cs * hh;
+                    }
+                    const double zm = Z[lane * GL + m], zh = Z[lane * GL + hi];
+                    Z[lane * GL + m] = cs * zm + sn * zh;
+                    Z[lane * GL + hi] = -sn * zm + cs * zh;
+                }
+                __syncwarp();
+                if (lane == 0) {
+                    H[hi * GL + m] = 0.0;
+                    H[m * GL + m] = lam1;
+                    H[hi * GL + hi] = lam2;
+                    wr[m] = lam1;
+                    wr[hi] = lam2;
+                    wi[m] = wi[hi] = 0.0;
+                }
+            } else if (lane == 0) {  // complex pair: the block stays
+                wr[m] = wr[hi] = 0.5 * (a + d);
+                wi[m] = sqrt(-disc);
+                wi[hi] = -wi[m];
+            }
+            __syncwarp();
+            hi -= 2;
+            its = 0;
+            continue;
+        }
+        if (its >= maxits) return -1;
+        its++;
+        sweeps++;
+        double h11, h12, h21, h22;  // the shifts are the eigenvalues of [h11 h12; h21 h22]
+        if (its == 10 || its == 20) {
+            const double s = (its == 10) ? fabs(H[(l + 1) * GL + l]) + fabs(H[(l + 2) * GL + l + 1])
+                                         : fabs(H[hi * GL + hi - 1]) + fabs(H[(hi - 1) * GL + hi - 2]);
+            h11 = 0.75 * s + ((its == 10) ? H[l * GL + l] : H[hi * GL + hi]);
+            h12 = -0.4375 * s;
+            h21 = s;
+            h22 = h11;
+        } else {
+            h11 = H[(hi - 1) * GL + hi - 1];
+            h12 = H[(hi - 1) * GL + hi];
+            h21 = H[hi * GL + hi - 1];
+            h22 = H[hi * GL + hi];
+        }
+        const double tr = h11 + h22, det = h11 * h22 - h12 * h21;
+        // first column of (H - s1)(H - s2) in the window
+        const double hll = H[l * GL + l], h1l = H[(l + 1) * GL + l];
+        double x = hll * hll + H[l * GL + l + 1] * h1l - tr * hll + det;
+        double y = h1l * (hll + H[(l + 1) * GL + l + 1] - tr);
+        double z = h1l * H[(l + 2) * GL + l + 1];
+        for (int k = l; k <= hi - 1; k++) {
+            const bool three = k < hi - 1;  // reflector length 3, else 2
+            if (!three) z = 0.0;
+            const double t2 = y * y + z * z;
+            if (t2 != 0.0) {
+                const double alpha = -copysign(sqrt(x * x + t2), x);
+                const double beta = 1.0 / (alpha * (alpha - x));
+                const double v0 = x - alpha, v1 = y, v2 = z;
+                const int q = max(l, k - 1);
+                if (lane >= q && lane < n) {  // rows k.. of columns q..n-1
+                    double a0 = H[k * GL + lane], a1 = H[(k + 1) * GL + lane];
+                    double a2 = three ? H[(k + 2) * GL + lane] : 0.0;
+                    const double s = beta * (v0 * a0 + v1 * a1 + v2 * a2);
+                    a0 -= s * v0;
+                    a1 -= s * v1;
+                    a2 -= s * v2;
+                    if (lane == k - 1) {  // the bulge column: exactly (alpha, 0, 0)
+                        a0 = alpha;
+                        a1 = a2 = 0.0;
+                    }
+                    H[k * GL + lane] = a0;
+                    H[(k + 1) * GL + lane] = a1;
+                    if (three) H[(k + 2) * GL + lane] = a2;
+                }
+                __syncwarp();
+                if (lane < n) {  // columns k.. of rows 0..min(k+3, hi); Z all rows
+                    if (lane <= min(k + 3, hi)) {
+                        const double a0 = H[lane * GL + k], a1 = H[lane * GL + k + 1];
+                        const double a2 = three ? H[lane * GL + k + 2] : 0.0;
+                        const double s = beta * (a0 * v0 + a1 * v1 + a2 * v2);
+                        H[lane * GL + k] = a0 - s * v0;
+                        H[lane * GL + k + 1] = a1 - s * v1;
+                        if (three) H[lane * GL + k + 2] = a2 - s * v2;
+                    }
+                    const double c0 = Z[lane * GL + k], c1 = Z[lane * GL + k + 1];
+                    const double c2 = three ? Z[lane * GL + k + 2] : 0.0;
+                    const double s = beta * (c0 * v0 + c1 * v1 + c2 * v2);
+                    Z[lane * GL + k] = c0 - s * v0;
+                    Z[lane * GL + k + 1] = c1 - s * v1;
+                    if (three) Z[lane * GL + k + 2] = c2 - s * v2;
+                }
+                __syncwarp();
+            }
+            if (three) {
+                x = H[(k + 1) * GL + k];
+                y = H[(k + 2) * GL + k];
+                z = (k < hi - 2) ? H[(k + 3) * GL + k] : 0.0;
+            }
+        }
+    }
+    __syncwarp();
+    // ---- 3. eigenvectors of T (lane e: eigenvalue e; a pair by its first lane)
+    if (lane < n && wi[lane] >= 0.0) {
+        const int e = lane;
+        const cplx lam = {wr[e], wi[e]};
+        const bool pair = wi[e] > 0.0;
+        const int top = pair ? e + 1 : e;  // last nonzero row of x
+        for (int i = top + 1; i < n; i++) {
+            X[i * GL + e] = 0.0;
+            if (pair) X[i * GL + e + 1] = 0.0;
+        }
+        // x[i] kept as (X[i][e], X[i][e+1]) for a pair, X[i][e] otherwise
+        if (pair) {
+            // eigenvector of the block [a b; c d] for lam: (lam - d, c) or
+            // (b, lam - a), whichever is longer
+            const double a = H[e * GL + e], b = H[e * GL + e + 1], c = H[(e + 1) * GL + e], d = H[(e + 1) * GL + e + 1];
+            const cplx u0 = {lam.re - d, lam.im}, w1 = {lam.re - a, lam.im};
+            const double nu = u0.re * u0.re + u0.im * u0.im + c * c, nw = b * b + w1.re * w1.re + w1.im * w1.im;
+            const cplx x0 = (nu >= nw) ? u0 : cplx{b, 0.0}, x1 = (nu >= nw) ? cplx{c, 0.0} : w1;
+            X[e * GL + e] = x0.re;
+            X[e * GL + e + 1] = x0.im;
+            X[(e + 1) * GL + e] = x1.re;
+            X[(e + 1) * GL + e + 1] = x1.im;
+        } else {
+            X[e * GL + e] = 1.0;
+        }
+        auto xval = [&](int j) -> cplx {
+            return pair ? cplx{X[j * GL + e], X[j * GL + e + 1]} : cplx{X[j * GL + e], 0.0};
+        };
+        auto rowsum = [&](int i, int j0) -> cplx {  // sum_{j >= j0} T[i][j] x[j]
+            cplx r = {0.0, 0.0};
+            for (int j = j0; j <= top; j++) {
+                const cplx xj = xval(j);
+                r.re += H[i * GL + j] * xj.re;
+                r.im += H[i * GL + j] * xj.im;
+            }
+            return r;
+        };
+        for (int i = e - 1; i >= 0;) {
+            if (i > 0 && H[i * GL + i - 1] != 0.0) {  // rows i-1, i: a 2 x 2 block
+                const cplx r0 = rowsum(i - 1, i + 1), r1 = rowsum(i, i + 1);
+                cplx x0, x1;
+                solve2(H[(i - 1) * GL + i - 1], H[(i - 1) * GL + i], H[i * GL + i - 1], H[i * GL + i], lam, r0, r1,
+                       tiny, &x0, &x1);
+                X[(i - 1) * GL + e] = x0.re;
+                X[i * GL + e] = x1.re;
+                if (pair) {
+                    X[(i - 1) * GL + e + 1] = x0.im;
+                    X[i * GL + e + 1] = x1.im;
+                }
+                i -= 2;
+            } else {
+                const cplx r = rowsum(i, i + 1);
+                const cplx xi = cdiv({-r.re, -r.im}, {H[i * GL + i] - lam.re, -lam.im}, tiny);
+                X[i * GL + e] = xi.re;
+                if (pair) X[i * GL + e + 1] = xi.im;
+                i -= 1;
+            }
+        }
+    }
+    __syncwarp();
+    // V = Z X into H (T is no longer read); lane e: column e
+    if (lane < n) {
+        const int top = (wi[lane] > 0.0) ? lane + 1 : lane;
+        for (int i = 0; i < n; i++) {
+            double s = 0.0;
+            for (int j = 0; j <= top; j++) s += Z[i * GL + j] * X[j * GL + lane];
+            H[i * GL + lane] = s;
+        }
+    }
+    __syncwarp();
+    // unit 2-norm, largest component real (a pair: by its first lane)
+    if (lane < n && wi[lane] >= 0.0) {
+        const int e = lane;
+        if (wi[e] == 0.0) {
+            double s = 0.0;
+            for (int i = 0; i < n; i++) s += H[i * GL + e] * H[i * GL + e];
+            const double f = 1.0 / sqrt(s);
+            for (int i = 0; i < n; i++) H[i * GL + e] *= f;
+        } else {
+            double s = 0.0, best = -1.0;
+            int kb = 0;
+            for (int i = 0; i < n; i++) {
+                const double m2 = H[i * GL + e] * H[i * GL + e] + H[i * GL + e + 1] * H[i * GL + e + 1];
+                s += m2;
+                if (m2 > best) {
+                    best = m2;
+                    kb = i;
+                }
+            }
+            // multiply by conj(v_kb) / (|v_kb| |v|)
+            const double mk = sqrt(best), f = 1.0 / (sqrt(s) * mk);
+            const double cr = H[kb * GL + e] * f, ci = H[kb * GL + e + 1] * f;
+            for (int i = 0; i < n; i++) {
+                const double re = H[i * GL + e], im = H[i * GL + e + 1];
+                H[i * GL + e] = re * cr + im * ci;
+                H[i * GL + e + 1] = im * cr - re * ci;
+            }
+            H[kb * GL + e + 1] = 0.0;
+        }
+    }
+    __syncwarp();
+    // each column to unit norm where it is off by more than 1e-10, as the
+    // reference does with the real and imaginary parts it keeps
+    // (mod_davidson.f90:211-217); copy out with V's leading dimension
+    if (lane < n) {
+        double s = 0.0;
+        for (int i = 0; i < n; i++) s += H[i * GL + lane] * H[i * GL + lane];
+        const double t = sqrt(s), f = (fabs(t - 1.0) > 1.0e-10) ? 1.0 / t : 1.0;
+        for (int i = 0; i < DAV_MAXD; i++) V[i * DAV_MAXD + lane] = (i < n) ? H[i * GL + lane] * f : 0.0;
+    } else {
+        for (int i = 0; i < DAV_MAXD; i++) V[i * DAV_MAXD + lane] = 0.0;
+    }
+    __syncwarp();
+    return sweeps;
+}
+
 // Schmidt_2D (mod_davidson.f90:642-680) on the dim columns (length len <= 32)
 // of `in`, by one warp: lane k holds row k; modified Gram-Schmidt in the
 // reference's order
@@ -295,7 +663,7 @@ __global__ void __launch_bounds__(DT) k_dav_init(DavState *st, DavBuffers b) {
 }
 
 __global__ void __launch_bounds__(DT) k_dav_step(DavState *st, DavBuffers b) {
-    __shared__ double S[DAV_MAXD * DAV_MAXD], V[DAV_MAXD * DAV_MAXD], ovl[DAV_MAXD];
+    __shared__ double S[DAV_MAXD * GL], V[DAV_MAXD * GL], X[DAV_MAXD * GL], ovl[DAV_MAXD];
     __shared__ double sh[DT / 32 + 1];
     DavState &s = *st;
     const int tid = threadIdx.x;
@@ -313,23 +681,71 @@ __global__ void __launch_bounds__(DT) k_dav_step(DavState *st, DavBuffers b) {
     }
     int dimIter = s.dimIter, cur = s.cur, dimFree = s.dimFree;
     const int dim_exceed = s.dim_exceed;
-    // ---- step 3: eigenpairs of the (symmetrised) Ritz matrix
-    for (int e = tid; e < DAV_MAXD * DAV_MAXD; e += DT) {
-        int i = e / DAV_MAXD, j = e % DAV_MAXD;
-        S[e] = (i < dimIter && j < dimIter) ? 0.5 * (s.Abar[i + j * D] + s.Abar[j + i * D]) : 0.0;
+    // ---- step 3: eigenpairs of Abar, dgeev in the reference
+    // (mod_davidson.f90:185-219).  Abar = B^T A B is symmetric when A is
+    // (spin-flip CIS with real integrals); when it is symmetric to 1e-12 of
+    // its largest element, the parallel Jacobi on 0.5 (Abar + Abar^T) gives
+    // dgeev's eigenpairs (to rounding) fastest; otherwise one warp solves
+    // the general problem (warp_geev: real parts of the eigenvalues, real
+    // and imaginary parts of complex eigenvectors as dgeev returns them,
+    // complex values counted as the reference's imaginary-eigenvalue warning)
+    __shared__ double vR[DAV_MAXD], vI[DAV_MAXD];
+    __shared__ int lw[DAV_MAXD], general;
+    if (tid < 32) {
+        double am = 0.0, ad = 0.0;
+        if (tid < dimIter)
+            for (int i = 0; i < dimIter; i++) {
+                const double aij = s.Abar[i + tid * D], aji = s.Abar[tid + i * D];
+                am = fmax(am, fabs(aij));
+                ad = fmax(ad, fabs(aij - aji));
+            }
+        am = warp_allmax(am);
+        ad = warp_allmax(ad);
+        if (tid == 0) general = ad > 1.0e-12 * am;
     }
     __syncthreads();
-    block_jacobi(S, V, dimIter);
+    if (!general) {
+        for (int e = tid; e < DAV_MAXD * DAV_MAXD; e += DT) {
+            int i = e / DAV_MAXD, j = e % DAV_MAXD;
+            S[e] = (i < dimIter && j < dimIter) ? 0.5 * (s.Abar[i + j * D] + s.Abar[j + i * D]) : 0.0;
+        }
+        __syncthreads();
+        block_jacobi(S, V, dimIter);
+        if (tid < dimIter) vR[tid] = S[tid * DAV_MAXD + tid];
+    } else {
+        for (int e = tid; e < dimIter * dimIter; e += DT) {
+            const int i = e / dimIter, j = e % dimIter;
+            S[i * GL + j] = s.Abar[i + j * D];
+        }
+        __syncthreads();
+        if (tid < 32) {
+            const int sw = warp_geev(S, V, X, V, vR, vI, dimIter);
+            if (tid == 0) {
+                s.nonsym_steps++;
+                if (sw < 0) s.eig_fail = 1;
+                for (int i = 0; i < dimIter; i++)
+                    if (fabs(vI[i]) > 1.0e-10) s.warn_imag++;
+            }
+        }
+    }
+    __syncthreads();
+    if (s.eig_fail) {  // the QR iteration did not converge: stop the solver
+        if (tid == 0) {
+            s.done = 1;
+            if (b.mailbox) {
+                b.mailbox[0] = 0;
+                __threadfence_system();
+            }
+        }
+        return;
+    }
     // eigenvalues, their order and the chosen roots, worked out in shared
     // memory (vecR(i, k) = V[i][k] for i < dimIter, zero below) and then
     // published to the state
-    __shared__ double vR[DAV_MAXD];
-    __shared__ int lw[DAV_MAXD];
     for (int e = tid; e < D * dimIter; e += DT) {
         int i = e % D, k = e / D;
         s.vecR[i + k * D] = (i < dimIter) ? V[i * DAV_MAXD + k] : 0.0;
     }
-    if (tid < dimIter) vR[tid] = S[tid * DAV_MAXD + tid];
     __syncthreads();
     if (tid == 0) {
         // sort (mod_davidson.f90:620-640)
@@ -828,7 +1244,30 @@ __device__ void diis_extrapolate(DiisState &s, const DiisBuffers &b, double *vec
     }
 }
 
+// the general eigen-solve of the Davidson step on one given matrix
+// (row-major, n <= DAV_MAXD), for verification against LAPACK
+__global__ void __launch_bounds__(32) k_geev_probe(const double *A, int n, double *wr, double *wi, double *V,
+                                                    int *sweeps) {
+    __shared__ double H[DAV_MAXD * GL], Z[DAV_MAXD * GL], X[DAV_MAXD * GL], r[DAV_MAXD], im[DAV_MAXD];
+    for (int e = threadIdx.x; e < n * n; e += 32) H[(e / n) * GL + e % n] = A[e];
+    __syncwarp();
+    const int sw = warp_geev(H, Z, X, Z, r, im, n);
+    if (threadIdx.x < n) {
+        wr[threadIdx.x] = r[threadIdx.x];
+        wi[threadIdx.x] = im[threadIdx.x];
+    }
+    for (int e = threadIdx.x; e < n * n; e += 32) V[e] = Z[(e / n) * DAV_MAXD + e % n];
+    if (threadIdx.x == 0) *sweeps = sw;
+}
+
 }  // namespace
+
+int geev_probe(const double *A_dev, int n, double *wr, double *wi, double *V, int *sweeps) {
+    if (n < 1 || n > DAV_MAXD) return set_error(CPSD_EARG, "geev: n must be 1..32");
+    k_geev_probe<<<1, 32, 0, stream()>>>(A_dev, n, wr, wi, V, sweeps);
+    count_launch();
+    return cuda_check(cudaGetLastError(), "k_geev_probe");
+}
 
 int dav_init_launch(DavState *st, const DavBuffers &b) {
     k_dav_init<<<1, DT, 0, stream()>>>(st, b);

@@ -12,7 +12,10 @@ struct DavState {
     int D, dimA, nroot, lowest, maxcyc;
     int dimIter, dimFree, dim_exceed, ndimIter, ndimFree, dimDel;
     int iterations, cur, nNew, newpos, done, converged;
-    int warn_imag;
+    // steps that took the general (non-symmetric) eigen-solve, Ritz values
+    // with an imaginary part above 1e-10 (the reference's warning,
+    // mod_davidson.f90:193-196), QR iteration failure
+    int nonsym_steps, warn_imag, eig_fail, pad;
     double maxError, max_resid;
     int conv[DAV_MAXD];
     int lowestE[DAV_MAXD];
@@ -41,6 +44,10 @@ int dav_init_launch(DavState *st, const DavBuffers &b);      // Abar of the gues
 int dav_step_launch(DavState *st, const DavBuffers &b);
 int dav_abar_launch(DavState *st, const DavBuffers &b);
 int dav_final_launch(DavState *st, const DavBuffers &b);     // eigen test residual
+// the Davidson step's general eigen-solve on one row-major n x n device
+// matrix: eigenvalues wr / wi, eigenvectors V (row-major, dgeev's columns),
+// QR sweeps (-1: no convergence); all device pointers
+int geev_probe(const double *A_dev, int n, double *wr, double *wi, double *V, int *sweeps);
 
 constexpr int DIIS_MAXDIM = 16;
 struct DiisState {

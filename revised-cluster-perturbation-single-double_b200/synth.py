@@ -228,6 +228,23 @@ CONFIGS = {
 }
 
 
+def config_integral_bytes(name):
+    """bytes of the six FP64 integral tensors of a named workload (from its
+    orbital populations alone, without drawing the integrals)"""
+    cfg = CONFIGS[name]
+    nmo, na, nb, nirrep = cfg["nmo"], cfg["nocc_a"], cfg["nocc_b"], cfg["nirrep"]
+    o = np.zeros(8, np.int64)
+    v = np.zeros(8, np.int64)
+    for k in range(nmo):
+        h = k % nirrep
+        o[h] += (k < na) + (k < nb)
+        v[h] += (k >= na) + (k >= nb)
+    sym = Symmetry(nirrep, xor_dirprd(nirrep))
+    n = (sym.idsymsoc(1, o, o, 0, o, o, 0) + sym.idsymsoc(1, o, o, 0, o, v, 1) + sym.idsymsoc(1, v, v, 0, o, o, 0) +
+         sym.idsymsoc(1, v, o, 1, v, o, 1) + sym.idsymsoc(1, v, v, 0, v, o, 1) + sym.idsymsoc(1, v, v, 0, v, v, 0))
+    return 8 * int(n)
+
+
 def batch_draw(n=64, seed=0):
     """Shapes of the batching workload: n independent molecules with
     nmo ~ U{60..240}, nocc_alpha ~ U{4..12}, nocc_beta = nocc_alpha - 2,

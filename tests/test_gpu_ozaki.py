@@ -108,8 +108,16 @@ def test_pipeline_digits_match_oracle(digits, tol):
     ints = api.DeviceIntegrals(s)
     sc, par = api.make_system(s), api.make_params(s, batch_roots=1)
     api.set_mixed(digits, 0.0)
-    om, w2, w3 = api.pipeline(s, sc, ints, par)
+    api.contract_timing(True)
+    try:
+        om, w2, w3 = api.pipeline(s, sc, ints, par)
+        kinds = api.contract_records()[2]
+    finally:
+        api.contract_timing(False)
     assert api.mixed_error() == 0
+    # the int8 digit GEMM (kind 12) and the digit slicing (10 / 11) ran: a
+    # silent fall-back to the FP64 tiles would also pass the energy checks
+    assert np.sum(kinds == 12) > 0 and np.sum((kinds == 10) | (kinds == 11)) > 0
     oom, ow2, ow3 = of.Oracle(s).pipeline()
     np.testing.assert_allclose(om, oom, rtol=0, atol=tol)
     np.testing.assert_allclose(w2, ow2, rtol=0, atol=tol)

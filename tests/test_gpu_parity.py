@@ -116,6 +116,54 @@ def test_cis_matches_oracle(nirrep):
 
 
 @pytest.mark.parametrize("nirrep", [1, 4])
+def test_cis_nonsymmetric_matches_oracle(nirrep):
+    """A non-symmetric CIS matrix: the Davidson step solves the general Ritz
+    problem, as the reference's dgeev does (mod_davidson.f90:185-219), and
+    matches the oracle.  The matrix is A' = D A D^-1 with a positive
+    diagonal D far from the identity (V'(fn,ai) = V(fn,ai) d(ai) / d(fn) in
+    every irrep block of iabj): strongly non-symmetric, with the real
+    eigenvalues of the symmetric A, and right eigenvectors D R.  An
+    eigenvalue's error is first order in the residual for a non-symmetric
+    matrix, so both run to a residual of 1e-12 (davidson_conv = 12).  With
+    the symmetric integrals every step takes the symmetric solve."""
+    s = small(nirrep, roots=3)
+    s.run_opts["davidson_conv"] = 12
+    ints, sc, par, orc = _run_both(s)
+    api.davidson_stats(reset=True)
+    sym_om, sym_R, _ = api.cis_run(s, sc, ints, par)
+    assert api.davidson_stats()[0] == 0
+    rng = np.random.default_rng(11 + nirrep)
+    iabj = s.ints["iabj"].copy()
+    dvec, off = [], 0
+    for h in range(1, s.nirrep + 1):
+        n = s.sym.irpdso(h, s.popv, s.popo, 1)
+        d = 1.0 + 0.3 * rng.uniform(-1.0, 1.0, n)
+        blk = iabj[off:off + n * n].reshape(n, n, order="F")  # (fn, ai), column-major
+        iabj[off:off + n * n] = (blk * d[None, :] / d[:, None]).reshape(-1, order="F")
+        dvec.append(d)
+        off += n * n
+    assert off == len(iabj)
+    s.ints["iabj"] = iabj
+    ints, sc, par, orc = _run_both(s)
+    om, R, it = api.cis_run(s, sc, ints, par)
+    nonsym, imag = api.davidson_stats()
+    assert nonsym > 0 and imag == 0
+    oom, oR, oit = orc.cis()
+    np.testing.assert_allclose(om, oom, rtol=0, atol=1e-10)
+    np.testing.assert_allclose(om, sym_om, rtol=0, atol=1e-9)
+    l1 = s.r1_len(1)
+    Rg, Rs = host(R), host(sym_R)
+    for k in range(len(om)):
+        a, b = Rg[k * l1:(k + 1) * l1], oR[k * l1:(k + 1) * l1]
+        sgn = np.sign(np.dot(a, b))
+        np.testing.assert_allclose(sgn * a, b, rtol=0, atol=1e-9)
+        # right eigenvector of D A D^-1: D R (irrep 1 block of the roots)
+        dr = dvec[0] * Rs[k * l1:(k + 1) * l1]
+        dr /= np.linalg.norm(dr)
+        np.testing.assert_allclose(np.sign(np.dot(a, dr)) * a, dr, rtol=0, atol=1e-8)
+
+
+@pytest.mark.parametrize("nirrep", [1, 4])
 def test_ground_and_intermediates_match_oracle(nirrep):
     s = small(nirrep)
     ints, sc, par, orc = _run_both(s)
@@ -211,3 +259,29 @@ def test_full_size_d2h_nmo200_properties():
     oJ = {k: host(v) for k, v in J.items()}
     r = orc.root(og, oJ, 1, om[0], host(Rg[0]))
     np.testing.assert_allclose(wb[0], r["w"], rtol=0, atol=TOL_E)
+
+
+@pytest.mark.parametrize("digits", [0, 5])
+def test_d2h_nmo200_every_root_matches_oracle(digits):
+    """The precision-form workload (D2h, nmo 200, nocc 10/8, 5 roots),
+    every root against the oracle's whole pipeline on the same inputs: the
+    FP64 path to 1e-9 Eh in each of w0, w^(2), w^(3); the mixed path (5
+    int8 digits on the tensor cores) to 1 micro-Eh, with the per-root
+    errors printed."""
+    import os
+    s = synth.make("d2h_nmo200")
+    api.init(s.nirrep, s.dirprd)
+    ints = api.DeviceIntegrals(s)
+    sc, par = api.make_system(s), api.make_params(s, batch_roots=1)
+    api.set_mixed(digits, 1.0)
+    try:
+        om, w2, w3 = api.pipeline(s, sc, ints, par)
+        assert api.mixed_error() == 0
+    finally:
+        api.set_mixed(0)
+    oom, ow2, ow3 = of.Oracle(s, nthreads=os.cpu_count() or 1).pipeline()
+    tol = TOL_E if digits == 0 else 1e-6
+    err = np.abs(np.stack([om - oom, w2 - ow2, w3 - ow3]))
+    print(f"digits={digits} per-root |gpu - oracle| (w0, w2, w3 rows):\n{err}")
+    assert len(om) == 5
+    assert err.max() < tol, err

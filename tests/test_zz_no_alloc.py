@@ -1,10 +1,12 @@
 """The no-allocation contraction entry point (cpsd_vv2v_dpd_444_noalloc)
 against cpsd_vv2v_dpd_444 through the C-ABI.
 
-Both run the same plan and kernels; the no-allocation one keeps the plan
-tables and split-K partial tiles in the library's fixed 32 MiB device
-region.  Results must agree to 1e-12 absolute (FP64, O(1) data) on two
-calls in a row, the calls after set-up must leave device memory and the
+Both run the same plan; the no-allocation one always on the FP64 tile
+kernel, with the plan tables and split-K partial tiles in the library's
+fixed 32 MiB device region.  It is also checked against the CPU oracle
+directly, with and without the mixed (digit) mode switched on.  Results
+must agree to 1e-12 absolute (FP64, O(1) data) on two calls in a row, the
+calls after set-up must leave device memory and the
 library's scratch arena untouched, and a contraction needing more than the
 region must be rejected without touching V3.  This file is collected last
 so that it also runs after every other GPU test in one process."""
@@ -69,6 +71,34 @@ def test_noalloc_matches_allocating_entry(nmo, nirrep):
                 torch.cuda.synchronize()
                 np.testing.assert_allclose(out.cpu().numpy(), ref.cpu().numpy(), rtol=0, atol=TOL,
                                            err_msg=f"{ta}*{tb}->{tc} f2={f2} call {call}")
+
+
+@pytest.mark.parametrize("nirrep", [1, 4])
+def test_noalloc_matches_oracle(nirrep):
+    """The no-allocation entry point against the CPU oracle directly, on
+    two calls in a row; with the mixed (int8-digit) mode switched on it
+    still computes in FP64 on the tile kernel."""
+    import oracle_ffi as of
+    s = synth.System(nmo=48, nocc_a=4, nocc_b=2, nirrep=nirrep, seed=20 + nirrep)
+    api.init(s.nirrep, s.dirprd)
+    of.set_symmetry(s.nirrep, s.dirprd)
+    rng = np.random.default_rng(nirrep)
+    try:
+        for mixed in (0, 5):
+            api.set_mixed(mixed, 0.0)
+            for case in cases(s):
+                (a, da, ta), (b, db, tb), (c, dc, tc) = operands(s, case, rng)
+                ref = c.copy()
+                assert of.vv2v_dpd(a.cpu().numpy(), of.desc(*da), ta, b.cpu().numpy(), of.desc(*db), tb, ref,
+                                   of.desc(*dc), tc, 0.7, 0.5) == 0
+                for call in range(2):
+                    out = dev(c)
+                    api.vv2v_dpd_444_noalloc(a, da, ta, b, db, tb, out, dc, tc, 0.7, 0.5)
+                    torch.cuda.synchronize()
+                    np.testing.assert_allclose(out.cpu().numpy(), ref, rtol=0, atol=TOL,
+                                               err_msg=f"{ta}*{tb}->{tc} mixed={mixed} call {call}")
+    finally:
+        api.set_mixed(0)
 
 
 def test_noalloc_allocates_nothing():
