@@ -405,6 +405,48 @@ int cpsd_pipeline_batch(int64_t nmol, const cpsd_system *s, const cpsd_integrals
  * calls allocate again as needed. */
 int cpsd_release_device_cache(void);
 
+/* ------------------------------------------ the reference's input files
+ * Host-side readers (and writers) of the files the reference's programs
+ * read their input from; no GPU is needed.  The files are those of its
+ * gfortran / nvfortran builds with 8-byte default integers: sequential
+ * records framed by 4-byte length markers, 32768-byte direct-access records.
+ *
+ * DPD list `<dir>/<name>` + `<dir>/<name>.c` (clmoioso0.f:30-67 writes the
+ * sidecar; getallso_d.f:31-79 / getlstso.f:50-125 read the data): the
+ * sidecar's records, Fortran (10, 20) arrays as [list - 1][irrep - 1]. */
+typedef struct {
+    int64_t irrepx;
+    int64_t popp[8], popq[8], popr[8], pops[8];
+    int64_t ioppq[8], ioprs[8], irrepr[8], irrepi[8];
+    int64_t moionuml[20][10], moionumr[20][10], rectmp[20][10];
+} cpsd_dpd_list_meta;
+int cpsd_dpd_list_meta_read(const char *dir, const char *name, cpsd_dpd_list_meta *m);
+/* getallso(z, 1, name): list 1, all irrep blocks, into host[0..len) (len
+ * must equal the list's DPD length); needs cpsd_init for the symmetry */
+int cpsd_dpd_list_read(const char *dir, const char *name, double *host, int64_t len);
+/* clmoioso0 + putlstso of list 1: writes a whole DPD tensor (host) */
+int cpsd_dpd_list_write(const char *dir, const char *name, int64_t irrepx, const int64_t *popp, const int64_t *popq,
+                        int64_t ioppq, const int64_t *popr, const int64_t *pops, int64_t ioprs, const double *host);
+/* the "interface" node file (src/pyscf2cc/mod_interface.f90): stream file,
+ * header (table position, node count), data, table of 36-byte nodes (name
+ * blank-padded to 20 lower-case characters, 1-based byte position, byte
+ * size).  read_node: the node's size must equal `bytes`; add_node: a new
+ * node's data goes where the table was, the table behind it. */
+int cpsd_interface_size(const char *path, const char *node, int64_t *bytes);
+int cpsd_interface_read(const char *path, const char *node, void *out, int64_t bytes);
+int cpsd_interface_write(const char *path, const char *node, const void *data, int64_t bytes);
+/* readmodule (src/lib_cc/readmodule.f90:17-40): symry, dirprd, nirrep and
+ * the (8, 2) pop / vrt nodes into a cpsd_system */
+int cpsd_load_system(const char *interface_path, cpsd_system *s);
+/* loadSCF (src/EE-CPSd.SF/loadSCF.f90:13-48): the spin-free orbital
+ * energies ('orb_energy_no_spin') and the six integral lists 'ijkl_ns_' ...
+ * 'abcd_ns_' (src/EE-CPSd.SF/mod_variable.f90:37-47, layouts of
+ * allocate_mem.f90:22-43) into host arrays of the cpsd_integrals layouts
+ * (NULL skips one); dir NULL reads the interface's 'tmpdir' node (else the
+ * current directory).  Populations and iops are checked against s. */
+int cpsd_load_inputs(const char *dir, const char *interface_path, const cpsd_system *s, double *ijkl, double *ijka,
+                     double *abij, double *iabj, double *abci, double *abcd, double *eorb);
+
 /* -------------------------------------------- SF-CIS(D) energy gradient
  * No counterpart in the reference (it has no derivative code).
  *

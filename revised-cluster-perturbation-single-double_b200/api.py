@@ -397,3 +397,94 @@ def pipeline_batch(systems, ints_list, params, nworkers=4):
 def release_device_cache():
     """cpsd_release_device_cache: free the library's idle device buffers."""
     check(lib().cpsd_release_device_cache(), "cpsd_release_device_cache")
+
+
+# ------------------------------------------------ the reference's input files
+# DPD lists (getallso / clmoioso0 + putlstso) and the "interface" node file
+# (src/pyscf2cc/mod_interface.f90), read and written on the host.
+LIST_NAMES = {"ijkl": "ijkl_ns_", "ijka": "ijka_ns_", "abij": "abij_ns_", "iabj": "iabj_ns_",
+              "abci": "abci_ns_", "abcd": "abcd_ns_"}
+
+
+class DpdListMeta(ctypes.Structure):
+    _fields_ = [("irrepx", I64), ("popp", I64 * 8), ("popq", I64 * 8), ("popr", I64 * 8), ("pops", I64 * 8),
+                ("ioppq", I64 * 8), ("ioprs", I64 * 8), ("irrepr", I64 * 8), ("irrepi", I64 * 8),
+                ("moionuml", (I64 * 10) * 20), ("moionumr", (I64 * 10) * 20), ("rectmp", (I64 * 10) * 20)]
+
+
+def _b(x):
+    return None if x is None else str(x).encode()
+
+
+def write_dpd_list(dirname, name, irrepx, pops, iops, arr):
+    a = np.ascontiguousarray(arr, dtype=np.float64)
+    check(lib().cpsd_dpd_list_write(_b(dirname), _b(name), I64(irrepx), arr8(pops[0]), arr8(pops[1]), I64(iops[0]),
+                                    arr8(pops[2]), arr8(pops[3]), I64(iops[1]), a.ctypes.data_as(ctypes.c_void_p)),
+          "cpsd_dpd_list_write")
+
+
+def read_dpd_list(dirname, name, n):
+    out = np.zeros(n)
+    check(lib().cpsd_dpd_list_read(_b(dirname), _b(name), out.ctypes.data_as(ctypes.c_void_p), I64(n)),
+          "cpsd_dpd_list_read")
+    return out
+
+
+def read_dpd_list_meta(dirname, name):
+    m = DpdListMeta()
+    check(lib().cpsd_dpd_list_meta_read(_b(dirname), _b(name), ctypes.byref(m)), "cpsd_dpd_list_meta_read")
+    return m
+
+
+def interface_write(path, node, data):
+    a = np.ascontiguousarray(data)
+    check(lib().cpsd_interface_write(_b(path), _b(node), a.ctypes.data_as(ctypes.c_void_p), I64(a.nbytes)),
+          "cpsd_interface_write")
+
+
+def interface_read(path, node, dtype=np.float64):
+    n = I64()
+    check(lib().cpsd_interface_size(_b(path), _b(node), ctypes.byref(n)), "cpsd_interface_size")
+    out = np.zeros(n.value // np.dtype(dtype).itemsize, dtype=dtype)
+    check(lib().cpsd_interface_read(_b(path), _b(node), out.ctypes.data_as(ctypes.c_void_p), n), "cpsd_interface_read")
+    return out
+
+
+def load_system(interface_path):
+    """cpsd_system from the interface file (readmodule)"""
+    sc = System()
+    check(lib().cpsd_load_system(_b(interface_path), ctypes.byref(sc)), "cpsd_load_system")
+    return sc
+
+
+def load_inputs(dirname, interface_path, sysc, lengths, neorb, keys=tuple(LIST_NAMES)):
+    """the six integral lists and the spin-free orbital energies (loadSCF)
+    into host arrays; lengths: DPD length per tensor name"""
+    out = {k: np.zeros(lengths[k]) for k in keys}
+    out["eorb"] = np.zeros(neorb)
+    p = [out[k].ctypes.data_as(ctypes.c_void_p) if k in out else None for k in LIST_NAMES]
+    check(lib().cpsd_load_inputs(_b(dirname), _b(interface_path), ctypes.byref(sysc), *p,
+                                 out["eorb"].ctypes.data_as(ctypes.c_void_p)), "cpsd_load_inputs")
+    return out
+
+
+def write_inputs(dirname, interface_path, s, eps_alpha=None, eps_beta=None):
+    """The files a synth.System's integrals would have in the reference's
+    run directory: the interface nodes readmodule / loadSCF read (the keys
+    py2cc.write_interface writes plus 'orb_energy_no_spin') and the six
+    spin-free integral lists."""
+    init(s.nirrep, s.dirprd)
+    dirprd = np.ascontiguousarray(np.asarray(s.dirprd, dtype=np.int64).reshape(64))
+    interface_write(interface_path, "dirprd", dirprd)
+    interface_write(interface_path, "vrt", np.concatenate([s.vrta, s.vrtb]).astype(np.int64))
+    interface_write(interface_path, "pop", np.concatenate([s.popa, s.popb]).astype(np.int64))
+    for k, v in (("symrx", 1), ("symry", s.symry), ("symrz", 1), ("nirrep", s.nirrep),
+                 ("iprcln", 32768), ("iprcwd", 4096), ("ichcsz", 4096)):
+        interface_write(interface_path, k, np.array([v], dtype=np.int64))
+    interface_write(interface_path, "orb_energy_no_spin", np.asarray(s.eorb, dtype=np.float64))
+    o, v = s.popo, s.popv
+    layout = {"ijkl": ([o, o, o, o], (0, 0)), "ijka": ([o, o, o, v], (0, 1)), "abij": ([v, v, o, o], (0, 0)),
+              "iabj": ([v, o, v, o], (1, 1)), "abci": ([v, v, v, o], (0, 1)), "abcd": ([v, v, v, v], (0, 0))}
+    for k, (pops, iops) in layout.items():
+        if s.ints.get(k) is not None:
+            write_dpd_list(dirname, LIST_NAMES[k], 1, pops, iops, s.ints[k])

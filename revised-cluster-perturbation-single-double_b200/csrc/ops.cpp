@@ -9,6 +9,8 @@
 #include "ozaki.cuh"
 #include "solvers.cuh"
 
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -52,6 +54,27 @@ struct OpScope {
 };
 }
 
+// CPSD_TRACE set in the environment: one line per contraction on stderr
+// with its index specification, the kernel path taken and the shapes of
+// its tasks (a host-side record for profiling; nothing is synchronised)
+static void trace_contraction(const ContractPlan *p, const char *t1, const char *t2, const char *t3, i64 nb,
+                              const char *path) {
+    static const bool on = getenv("CPSD_TRACE") != nullptr;
+    if (!on) return;
+    i64 mM = 0, mN = 0, mK = 0;
+    double out = 0;
+    for (const TaskDev &t : p->h_tasks) {
+        mM = std::max(mM, t.M);
+        mN = std::max(mN, t.N);
+        mK = std::max(mK, t.Ktot);
+        out += (double)t.M * (double)t.N;
+    }
+    fprintf(stderr, "[cpsd] %.4s*%.4s->%.4s nb=%lld path=%s tasks=%d segs=%d tiles=%d cfg=%d flops=%.4g maxM=%lld "
+            "maxN=%lld maxK=%lld outelems=%.4g\n", t1, t2, t3, (long long)nb, path, p->ntasks, p->nsegs, p->ntiles,
+            p->cfg, p->flops * (double)(nb > 1 ? nb : 1), (long long)mM, (long long)mN, (long long)mK,
+            out * (double)(nb > 1 ? nb : 1));
+}
+
 int engine(const Ten &v1, const char *t1, const Ten &v2, const char *t2, Ten &v3, const char *t3, double f1,
            double f2, i64 nb) {
     CPSD_TRY(need_init());
@@ -80,6 +103,7 @@ int engine(const Ten &v1, const char *t1, const Ten &v2, const char *t2, Ten &v3
             for (i64 c = 0; c < nb; c++) CPSD_TRY(launch_scale(v3.arr + c * b.strideC, l3, f2));
     }
     if (oz) {
+        trace_contraction(p, t1, t2, t3, nb, "digits");
         ctx().flops += p->flops;
         return launch_ozaki(oz, v1.arr, v2.arr, v3.arr, f1);
     }
@@ -87,9 +111,11 @@ int engine(const Ten &v1, const char *t1, const Ten &v2, const char *t2, Ten &v3
     const NarrowPlan *np = nullptr;
     if (!p->empty) CPSD_TRY(plan_narrow(p, &np));
     if (np) {
+        trace_contraction(p, t1, t2, t3, nb, np->longk ? "narrow_k" : "narrow_rows");
         ctx().flops += p->flops;
         return launch_narrow(p, np, v1.arr, v2.arr, v3.arr, f1);
     }
+    if (!p->empty) trace_contraction(p, t1, t2, t3, nb, "tiles");
     return launch_contract(p, v1.arr, v2.arr, v3.arr, f1);
 }
 
