@@ -453,9 +453,19 @@ def run_ours(args, rank, world, local_rank):
               "frac": (d_fl / (d_ms / 1e3) / 1e12) / fp64_peak if d_ms > 0 and fp64_peak else None,
               "traffic": None, "peak_source": "measured cuBLAS DGEMM 8192^3 on this GPU",
               "share_of_step": d_ms / step_ms, "launches_per_step": int(sel.sum())}
+    sel = rkind == 22
+    s_ms, s_bytes = float(rms[sel].sum()), 16.0 * float(rshape[sel][:, 2].sum())
+    hbm = hbm_peak_gbs()
+    roof_sk = {"bound": "hbm", "kernel": "k_shortk (short contracted range, output read-modify-write)",
+               "achieved": s_bytes / (s_ms / 1e3) / 1e9 if s_ms > 0 else 0.0, "peak": hbm, "unit": "GB/s",
+               "frac": (s_bytes / (s_ms / 1e3) / 1e9) / hbm if s_ms > 0 else None,
+               "algorithmic_bytes_per_step": s_bytes,
+               "bytes_note": "16 B per output element (read + write of C); the operand tiles are not counted",
+               "peak_source": "MEASURED_PEAKS.json hbm_gbs (copy bandwidth)",
+               "share_of_step": s_ms / step_ms, "launches_per_step": int(sel.sum())}
     shares = {lab: round(float(rms[m].sum()) / step_ms, 4) for lab, m in
               (("digit_gemm", rkind == 12), ("digit_slicing", (rkind == 10) | (rkind == 11)),
-               ("fp64_tiles", rkind < 10), ("narrow", (rkind >= 20) & (rkind < 30)),
+               ("fp64_tiles", rkind < 10), ("narrow", (rkind == 20) | (rkind == 21)), ("shortk", rkind == 22),
                ("davidson", (rkind == 30) | (rkind == 31)), ("diis_solver", rkind == 32),
                ("pair_transforms", rkind == 40))}
 
@@ -500,6 +510,9 @@ def run_ours(args, rank, world, local_rank):
                            "and reads the energies back"}
             api.set_mixed(0)
             del host
+            import gc
+            gc.collect()
+            torch._C._host_emptyCache()  # give the pinned pages back (torch caches them otherwise)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -533,6 +546,7 @@ def run_ours(args, rank, world, local_rank):
                           "gpu_launches": launches64, "contraction_tflops": flops64 / (ms64 / 1e3) / 1e12},
             "roofline": roof or roof64,
             "roofline_fp64_tiles": roof64,
+            "roofline_shortk": roof_sk,
             "contraction_shares_of_step": shares,
             "contraction_tflops": flops / (ms_max / 1e3) / 1e12,
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": ck,

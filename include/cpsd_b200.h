@@ -272,6 +272,7 @@ CPSD_KERNEL(Wmbej_r2abij); /* Wmbej_r2abij.f90:3 W(em,bj) += .5 r(bf,jn) V(fe,nm
 CPSD_KERNEL(Wmbej_r1abci); /* Wmbej_r1abci.f90:3 W(em,bj) += r(f,j) V(fe,bm)        */
 CPSD_KERNEL(Wmbej_r1ijka); /* Wmbej_r1ijka.f90:3 W(em,bj) -= r(b,n) V(nm,je)        */
 CPSD_KERNEL(Wmnij_r1ijka); /* Wmnij_r1ijka.f90:3 W(mn,ij) += P(ij) r(e,j) V(mn,ie)  */
+CPSD_KERNEL(Wmnij_r2abij); /* Wmnij_r2abij.f90:1 W(mn,ij) += .5 V(ef,mn) r(ef,ij)   */
 #undef CPSD_KERNEL
 
 /* --------------------------------------------- planner introspection
@@ -295,6 +296,13 @@ int cpsd_contract_records(double *ms, double *flops, int64_t *shape, int64_t max
 int cpsd_debug_narrow_plan(const cpsd_opt *v1, const char *t1, const cpsd_opt *v2, const char *t2,
                            const cpsd_opt *v3, const char *t3, int64_t nb, int64_t sA, int64_t sB, int64_t sC,
                            const void **items, int64_t *nitems, const void **reds, int64_t *nreds, int64_t *flags);
+/* work items of the short-K kernel for a contraction (layout ShortKItem of
+ * csrc/shortk.cuh); flags = {short-K, f runs along M, tile extent BS along
+ * the other side, largest contracted range}; items = NULL when it does not
+ * qualify */
+int cpsd_debug_shortk_plan(const cpsd_opt *v1, const char *t1, const cpsd_opt *v2, const char *t2,
+                           const cpsd_opt *v3, const char *t3, int64_t nb, int64_t sA, int64_t sB, int64_t sC,
+                           const void **items, int64_t *nitems, int64_t *flags);
 /* tables of the sliced-integer plan of a contraction (layouts OzGroup,
  * OzTile, OzSliceJob of csrc/ozaki.cuh): tables[0..12] = groups, tiles,
  * A jobs, B jobs, A row / K offsets, B row / K offsets, C row / column
@@ -354,6 +362,13 @@ int cpsd_cis_run(const cpsd_system *s, const cpsd_integrals *I, const cpsd_param
 int cpsd_ground(const cpsd_system *s, const cpsd_integrals *I, const cpsd_params *p,
                 double *T2_1, double *T1_2, double *T2_2, double *E2_host, double *E3_host,
                 int64_t *diis_iters);
+
+/* ground CPS(D) third order T^(3) and E^(4) (src/CPSd.SF/run3.f90:8-97)
+ * from T2^(1), T1^(2), T2^(2) of cpsd_ground; device in- and outputs,
+ * E^(4) on the host */
+int cpsd_ground3(const cpsd_system *s, const cpsd_integrals *I, const cpsd_params *p, const double *T2_1,
+                 const double *T1_2, const double *T2_2, double *T1_3, double *T2_3, double *E4_host,
+                 int64_t *diis_iters);
 
 /* J^(2) / J^(3) intermediates (src/EE-CPSd.SF/calJ.f90:6-228); device */
 typedef struct {

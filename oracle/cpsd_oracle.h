@@ -139,6 +139,7 @@ int o_Wmbej_r2abij(o_opt *W, const o_opt *r2, const o_opt *abij, double f);
 int o_Wmbej_r1abci(o_opt *W, const o_opt *r1, const o_opt *abci, double f);
 int o_Wmbej_r1ijka(o_opt *W, const o_opt *r1, const o_opt *ijka, double f);
 int o_Wmnij_r1ijka(o_opt *W, const o_opt *r1, const o_opt *ijka, double f);
+int o_Wmnij_r2abij(o_opt *W, const o_opt *r2, const o_opt *abij, double f);
 
 /* ---------------- molecular system and the pipeline ---------------- */
 typedef struct {
@@ -189,6 +190,10 @@ int o_cis_run(const o_system *s, const o_integrals *I, const o_params *p,
 int o_cpsd_ground(const o_system *s, const o_integrals *I, const o_params *p,
                   double *T2_1, double *T1_2, double *T2_2, double *E2, double *E3,
                   i64 *diis_iters);
+/* third order: T1^(3), T2^(3), E^(4) (src/CPSd.SF/run3.f90) */
+int o_cpsd_ground3(const o_system *s, const o_integrals *I, const o_params *p,
+                   const double *T2_1, const double *T1_2, const double *T2_2,
+                   double *T1_3, double *T2_3, double *E4, i64 *diis_iters);
 
 /* J^(2) / J^(3) intermediates (src/EE-CPSd.SF/calJ.f90:6-228) */
 typedef struct {

@@ -168,6 +168,76 @@ out:
     return rc;
 }
 
+/* ---------------- ground state, third order (src/CPSd.SF/run3.f90:8-97) ----
+ * C1^(3) = calC1_VR2(T2^(2))                               (calC1.f90)
+ * C2^(3) = calC2_VR1(T1^(2)) + calC2_VR2(T2^(2))            (calC2.f90, calC2_VR.f90)
+ *        + calC2_VTT(T2^(1)) with T1^(1) = 0: Fli, Fad, Wkaci, Wklij terms
+ *          (calC2_VTT.f90:82-207)
+ * T2^(3) = denomT2(C2^(3)); T1^(3) by the DIIS loop of run2 on C1^(3);
+ * E^(4) = T2^(3) . abij (calEcorr.f90) */
+int o_cpsd_ground3(const o_system *s, const o_integrals *I, const o_params *p,
+                   const double *T2_1, const double *T1_2, const double *T2_2,
+                   double *T1_3, double *T2_3, double *E4, i64 *diis_iters)
+{
+    ints_t v;
+    ints_view(s, I, &v);
+    const i64 *o = s->popo, *V = s->popv;
+    o_opt t1b, t2a, t2b, t1c, c1, c2, r1, fli, fad, wkaci, wklij;
+    i64 l1 = o_irpdso(1, V, o, 1);
+    i64 l2 = o_idsymsoc(1, V, V, 0, o, o, 0);
+    double *c1a = zalloc(l1), *c2a = zalloc(l2), *r1a = zalloc(l1);
+    double *fo = zalloc(o_irpdso(1, o, o, 1)), *fv = zalloc(o_irpdso(1, V, V, 1));
+    double *wk = zalloc(o_idsymsoc(1, V, o, 1, V, o, 1)), *wl = zalloc(o_idsymsoc(1, o, o, 0, o, o, 0));
+    o_opt_view(&t1b, V, o, Z, Z, 1, 1, 1, (double *)T1_2);
+    o_opt_view(&t2a, V, V, o, o, 0, 0, 1, (double *)T2_1);
+    o_opt_view(&t2b, V, V, o, o, 0, 0, 1, (double *)T2_2);
+    o_opt_view(&t1c, V, o, Z, Z, 1, 1, 1, T1_3);
+    o_opt_view(&c1, V, o, Z, Z, 1, 1, 1, c1a);
+    o_opt_view(&c2, V, V, o, o, 0, 0, 1, c2a);
+    o_opt_view(&r1, V, o, Z, Z, 1, 1, 1, r1a);
+    o_opt_view(&fli, o, o, Z, Z, 1, 1, 1, fo);
+    o_opt_view(&fad, V, V, Z, Z, 1, 1, 1, fv);
+    o_opt_view(&wkaci, V, o, V, o, 1, 1, 1, wk);
+    o_opt_view(&wklij, o, o, o, o, 0, 0, 1, wl);
+    int rc = o_c1_r2abci(&c1, &t2b, &v.abci, 1.0);
+    if (rc == O_OK) rc = o_c1_r2ijka(&c1, &t2b, &v.ijka, 1.0);
+    if (rc == O_OK) rc = o_c2_r1ijka(&c2, &t1b, &v.ijka, 1.0);
+    if (rc == O_OK) rc = o_c2_r1abci(&c2, &t1b, &v.abci, 1.0);
+    if (rc == O_OK) rc = o_c2_r2Wmbej(&c2, &t2b, &v.iabj, 1.0);
+    if (rc == O_OK) rc = o_c2_r2Wmnij(&c2, &t2b, &v.ijkl, 1.0);
+    if (rc == O_OK) rc = o_c2_r2abcd(&c2, &t2b, &v.abcd, 1.0);
+    if (rc == O_OK) rc = o_Fmi_r2abij(&fli, &t2a, &v.abij, 1.0);
+    if (rc == O_OK) rc = o_c2_r2Fmi(&c2, &t2a, &fli, 1.0);
+    if (rc == O_OK) rc = o_Fae_r2abij(&fad, &t2a, &v.abij, 1.0);
+    if (rc == O_OK) rc = o_c2_r2Fae(&c2, &t2a, &fad, 1.0);
+    if (rc == O_OK) rc = o_Wmbej_r2abij(&wkaci, &t2a, &v.abij, 1.0);
+    if (rc == O_OK) rc = o_c2_r2Wmbej(&c2, &t2a, &wkaci, 1.0);
+    if (rc == O_OK) rc = o_Wmnij_r2abij(&wklij, &t2a, &v.abij, 0.5);
+    if (rc == O_OK) rc = o_c2_r2Wmnij(&c2, &t2a, &wklij, 2.0);
+    if (rc != O_OK) goto out;
+    o_denomT2(T2_3, c2a, I->eorb, V, o, 1, 0);
+    memcpy(r1a, c1a, sizeof(double) * (size_t)l1);
+    o_diis dst;
+    o_diis_init(&dst, l1, p->diis_dim);
+    i64 iter = 0;
+    for (;;) {
+        iter++;
+        o_denomT1(T1_3, r1a, I->eorb, V, o, 1);
+        double err = o_diis_step(&dst, iter, T1_3);
+        if (iter > 1 && fabs(err) < p->diis_max_err) break;
+        if (iter > p->diis_cyc) break;
+        memcpy(r1a, c1a, sizeof(double) * (size_t)l1);
+        rc = o_c1_r1iabj(&r1, &t1c, &v.iabj, 1.0);
+        if (rc != O_OK) break;
+    }
+    o_diis_free(&dst);
+    if (diis_iters) *diis_iters = iter;
+    *E4 = o_ddot(l2, T2_3, I->abij);
+out:
+    free(c1a); free(c2a); free(r1a); free(fo); free(fv); free(wk); free(wl);
+    return rc;
+}
+
 /* ---------------- J^(2), J^(3) (src/EE-CPSd.SF/calJ.f90) ---------------- */
 int o_calJ(const o_system *s, const o_integrals *I, const double *T2_1,
            const double *T1_2, const double *T2_2, o_jints *J)

@@ -338,4 +338,9 @@ int o_Wmbej_r1ijka(o_opt *W, const o_opt *r1, const o_opt *ijka, double f)
 int o_Wmnij_r1ijka(o_opt *W, const o_opt *r1, const o_opt *ijka, double f)
 { return o_vv2v_424(ijka, r1, W, f, "mnie", "ej", "mnij", 2); }
 
+/* Wmnij_r2abij.f90:1-20: W(mn,ij) += f*0.5*V(ef,mn)*r(ef,ij) (full e,f sums;
+ * a packed ef pair sums each pair once, so the factor is f there) */
+int o_Wmnij_r2abij(o_opt *W, const o_opt *r2, const o_opt *abij, double f)
+{ return o_vv2v_444(abij, r2, W, r2->d.iop[0] == 0 ? f : 0.5 * f, "efmn", "efij", "mnij", 0); }
+
 const i64 *o_zorb(void) { return ZORB; }

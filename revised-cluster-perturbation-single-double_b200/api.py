@@ -278,6 +278,20 @@ def ground(s, sysc, ints, par):
     return dict(T2_1=T2_1, T1_2=T1_2, T2_2=T2_2, E2=E2.value, E3=E3.value, iters=it.value)
 
 
+def ground3(s, sysc, ints, par, g):
+    """third-order ground state (run3.f90) from ground()'s T: T1^(3),
+    T2^(3) (device) and E^(4)"""
+    import torch
+    l1, l2 = s.r1_len(1), s.r2_len(1)
+    T1_3 = torch.zeros(l1, dtype=torch.float64, device="cuda")
+    T2_3 = torch.zeros(l2, dtype=torch.float64, device="cuda")
+    E4, it = ctypes.c_double(), I64()
+    check(lib().cpsd_ground3(ctypes.byref(sysc), ctypes.byref(ints.struct), ctypes.byref(par), dptr(g["T2_1"]),
+                             dptr(g["T1_2"]), dptr(g["T2_2"]), dptr(T1_3), dptr(T2_3), ctypes.byref(E4),
+                             ctypes.byref(it)), "cpsd_ground3")
+    return dict(T1_3=T1_3, T2_3=T2_3, E4=E4.value, iters=it.value)
+
+
 def calJ(s, sysc, ints, g):
     import torch
     sym, o, v = s.sym, s.popo, s.popv

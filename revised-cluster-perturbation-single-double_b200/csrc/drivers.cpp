@@ -450,6 +450,65 @@ int cpsd_ground(const cpsd_system *s, const cpsd_integrals *I, const cpsd_params
     return digit_error_check();
 }
 
+// run3 (src/CPSd.SF/run3.f90:8-97): C1^(3) = calC1_VR2(T2^(2)); C2^(3) =
+// calC2_VR1(T1^(2)) + calC2_VR2(T2^(2)) + calC2_VTT(T2^(1)) (T1^(1) = 0:
+// the Fli, Fad, Wkaci and Wklij terms of calC2_VTT.f90:82-207); T2^(3) =
+// denomT2(C2^(3)); T1^(3) by the device-driven DIIS loop of run2; E^(4) =
+// T2^(3) . abij (calEcorr.f90, compensated sum)
+int cpsd_ground3(const cpsd_system *s, const cpsd_integrals *I, const cpsd_params *p, const double *T2_1,
+                 const double *T1_2, const double *T2_2, double *T1_3, double *T2_3, double *E4_host,
+                 int64_t *diis_iters) {
+    Sys S;
+    CPSD_TRY(make_sys(s, &S));
+    Ints X = make_ints(S, I);
+    IntegralScope keep(I);
+    const i64 *o = S.popo, *v = S.popv;
+    ScratchScope sc;
+    const i64 l1 = irpdso(1, v, o, 1), l2 = idsymsoc(1, v, v, 0, o, o, 0);
+    double *c1, *c2, *dE, *fo, *fv, *wk, *wl;
+    CPSD_TRY(scratch(l1, &c1));
+    CPSD_TRY(scratch(l2, &c2));
+    CPSD_TRY(scratch(1, &dE));
+    CPSD_TRY(scratch(irpdso(1, o, o, 1), &fo));
+    CPSD_TRY(scratch(irpdso(1, v, v, 1), &fv));
+    CPSD_TRY(scratch(idsymsoc(1, v, o, 1, v, o, 1), &wk));
+    CPSD_TRY(scratch(idsymsoc(1, o, o, 0, o, o, 0), &wl));
+    Desc d2 = make_desc(v, v, o, o, 0, 0, 1), d1 = make_desc(v, o, ZORB, ZORB, 1, 1, 1);
+    const EnergyPlan *e2, *e1;
+    CPSD_TRY(plan_energy(d2, "vvoo", &e2));
+    CPSD_TRY(plan_energy(d1, "vozz", &e1));
+    Ten t2a = ten(v, v, o, o, 0, 0, 1, (double *)T2_1), t1b = ten(v, o, ZORB, ZORB, 1, 1, 1, (double *)T1_2);
+    Ten t2b = ten(v, v, o, o, 0, 0, 1, (double *)T2_2);
+    Ten C1 = ten(v, o, ZORB, ZORB, 1, 1, 1, c1), C2 = ten(v, v, o, o, 0, 0, 1, c2);
+    Ten fli = ten(o, o, ZORB, ZORB, 1, 1, 1, fo), fad = ten(v, v, ZORB, ZORB, 1, 1, 1, fv);
+    Ten wkaci = ten(v, o, v, o, 1, 1, 1, wk), wklij = ten(o, o, o, o, 0, 0, 1, wl);
+    for (Ten *t : {&C1, &C2, &fli, &fad, &wkaci, &wklij}) CPSD_TRY(zero(t->arr, t->len()));
+    CPSD_TRY(k_c1_r2abci(C1, t2b, X.abci, 1.0));  // calC1 -> calC1_VR2
+    CPSD_TRY(k_c1_r2ijka(C1, t2b, X.ijka, 1.0));
+    CPSD_TRY(k_c2_r1ijka(C2, t1b, X.ijka, 1.0));  // calC2_VR1
+    CPSD_TRY(k_c2_r1abci(C2, t1b, X.abci, 1.0));
+    CPSD_TRY(k_c2_r2Wmbej(C2, t2b, X.iabj, 1.0));  // calC2_VR2
+    CPSD_TRY(k_c2_r2Wmnij(C2, t2b, X.ijkl, 1.0));
+    CPSD_TRY(k_c2_r2abcd(C2, t2b, X.abcd, 1.0));
+    CPSD_TRY(k_Fmi_r2abij(fli, t2a, X.abij, 1.0));  // calC2_VTT
+    CPSD_TRY(k_c2_r2Fmi(C2, t2a, fli, 1.0));
+    CPSD_TRY(k_Fae_r2abij(fad, t2a, X.abij, 1.0));
+    CPSD_TRY(k_c2_r2Fae(C2, t2a, fad, 1.0));
+    CPSD_TRY(k_Wmbej_r2abij(wkaci, t2a, X.abij, 1.0));
+    CPSD_TRY(k_c2_r2Wmbej(C2, t2a, wkaci, 1.0));
+    CPSD_TRY(k_Wmnij_r2abij(wklij, t2a, X.abij, 0.5));
+    CPSD_TRY(k_c2_r2Wmnij(C2, t2a, wklij, 2.0));
+    CPSD_TRY(launch_energy(e2, 2, X.eorb, c2, T2_3));
+    i64 iter = 0;
+    CPSD_TRY(solve_r1(S, X, p, 1, 1, l1, e1, c1, nullptr, nullptr, T1_3, &iter));
+    if (diis_iters) *diis_iters = iter;
+    CPSD_TRY(launch_dot(T2_3, I->abij, l2, dE, true));
+    double h = 0;
+    CPSD_TRY(read_back(&h, dE, sizeof h));
+    if (E4_host) *E4_host = h;
+    return digit_error_check();
+}
+
 int cpsd_calJ(const cpsd_system *s, const cpsd_integrals *I, const double *T2_1, const double *T1_2,
               const double *T2_2, cpsd_jints *J) {
     Sys S;

@@ -7,6 +7,7 @@
 #include "drivers.hpp"
 #include "narrow.cuh"
 #include "ozaki.cuh"
+#include "shortk.cuh"
 #include "solvers.cuh"
 
 #include <cstdio>
@@ -114,6 +115,15 @@ int engine(const Ten &v1, const char *t1, const Ten &v2, const char *t2, Ten &v3
         trace_contraction(p, t1, t2, t3, nb, np->longk ? "narrow_k" : "narrow_rows");
         ctx().flops += p->flops;
         return launch_narrow(p, np, v1.arr, v2.arr, v3.arr, f1);
+    }
+    // a contracted range of at most 64 everywhere: the output's
+    // read-modify-write bounds it, streaming kernel instead of tiles
+    const ShortKPlan *sp = nullptr;
+    if (!p->empty) CPSD_TRY(plan_shortk(p, &sp));
+    if (sp) {
+        trace_contraction(p, t1, t2, t3, nb, "shortk");
+        ctx().flops += p->flops;
+        return launch_shortk(p, sp, v1.arr, v2.arr, v3.arr, f1);
     }
     if (!p->empty) trace_contraction(p, t1, t2, t3, nb, "tiles");
     return launch_contract(p, v1.arr, v2.arr, v3.arr, f1);
@@ -730,6 +740,9 @@ int k_Wmbej_r1ijka(Ten &W, const Ten &r1, const Ten &V, double f, i64 nb) {
 int k_Wmnij_r1ijka(Ten &W, const Ten &r1, const Ten &V, double f, i64 nb) {
     return w424(V, r1, W, f, "mnie", "ej", "mnij", 2, nb);
 }
+int k_Wmnij_r2abij(Ten &W, const Ten &r2, const Ten &V, double f, i64 nb) {
+    return w444(V, r2, W, r2.d.iop[0] == 0 ? f : 0.5 * f, "efmn", "efij", "mnij", 0, nb);
+}
 
 // ------------------------------------------ adjoints of the lib_cc kernels
 // vjp_<name>(a, b, Y, G, which, f): G += d<Y, out>/da (which 0) or /db
@@ -1151,6 +1164,28 @@ int cpsd_debug_narrow_plan(const cpsd_opt *v1, const char *t1, const cpsd_opt *v
     return CPSD_OK;
 }
 
+int cpsd_debug_shortk_plan(const cpsd_opt *v1, const char *t1, const cpsd_opt *v2, const char *t2,
+                           const cpsd_opt *v3, const char *t3, int64_t nb, int64_t sA, int64_t sB, int64_t sC,
+                           const void **items, int64_t *nitems, int64_t *flags) {
+    CPSD_TRY(need_init());
+    Batch b;
+    b.nb = nb;
+    b.strideA = sA;
+    b.strideB = sB;
+    b.strideC = sC;
+    const ContractPlan *p;
+    CPSD_TRY(plan_contract(desc_of(v1), t1, desc_of(v2), t2, desc_of(v3), t3, b, &p));
+    const ShortKPlan *sp = nullptr;
+    if (!p->empty) CPSD_TRY(plan_shortk(p, &sp));
+    *items = sp ? sp->items.data() : nullptr;
+    *nitems = sp ? (int64_t)sp->items.size() : 0;
+    flags[0] = sp ? 1 : 0;
+    flags[1] = sp && sp->fm ? 1 : 0;
+    flags[2] = sp ? sp->bs : 0;
+    flags[3] = sp ? sp->kmax : 0;
+    return CPSD_OK;
+}
+
 int cpsd_debug_ozaki_plan(const cpsd_opt *v1, const char *t1, const cpsd_opt *v2, const char *t2,
                           const cpsd_opt *v3, const char *t3, int64_t nb, int64_t sA, int64_t sB, int64_t sC,
                           int digits, const void **tables, int64_t *sizes) {
@@ -1263,5 +1298,6 @@ KER(Wmbej_r2abij)
 KER(Wmbej_r1abci)
 KER(Wmbej_r1ijka)
 KER(Wmnij_r1ijka)
+KER(Wmnij_r2abij)
 
 }  // extern "C"

@@ -69,6 +69,7 @@ CPSD_IK(Wmbej_r2abij);
 CPSD_IK(Wmbej_r1abci);
 CPSD_IK(Wmbej_r1ijka);
 CPSD_IK(Wmnij_r1ijka);
+CPSD_IK(Wmnij_r2abij);
 #undef CPSD_IK
 
 // Vector-Jacobian product of the vv2v_444 form v3 += fact * P{v1 v2}:

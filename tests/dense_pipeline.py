@@ -67,6 +67,29 @@ class DenseSystem:
         T1_2[idx[:, 0], idx[:, 1]] = x
         return dict(T2_1=T2_1, T1_2=T1_2, T2_2=T2_2, E2=E2, E3=E3)
 
+    def ground3(self, g):
+        """run3.f90: T^(3) and E^(4) from T2^(1), T1^(2), T2^(2) (T1^(1) = 0)"""
+        T2_1, T1_2, T2_2 = g["T2_1"], g["T1_2"], g["T2_2"]
+        C1 = K("c1_r2abci", T2_2, self.abci) + K("c1_r2ijka", T2_2, self.ijka)
+        C2 = (K("c2_r1ijka", T1_2, self.ijka) + K("c2_r1abci", T1_2, self.abci)
+              + K("c2_r2Wmbej", T2_2, self.iabj) + K("c2_r2Wmnij", T2_2, self.ijkl)
+              + K("c2_r2abcd", T2_2, self.abcd))
+        Fli = K("Fmi_r2abij", T2_1, self.abij)
+        C2 = C2 + K("c2_r2Fmi", T2_1, Fli)
+        Fad = K("Fae_r2abij", T2_1, self.abij)
+        C2 = C2 + K("c2_r2Fae", T2_1, Fad)
+        Wkaci = K("Wmbej_r2abij", T2_1, self.abij)
+        C2 = C2 + K("c2_r2Wmbej", T2_1, Wkaci)
+        Wklij = K("Wmnij_r2abij", T2_1, self.abij, 0.5)
+        C2 = C2 + K("c2_r2Wmnij", T2_1, Wklij, 2.0)
+        T2_3 = -C2 / self.e2
+        E4 = 0.25 * np.sum(T2_3 * self.abij)
+        A, idx = self._sigma_matrix(1)
+        x = np.linalg.solve(A, -C1[idx[:, 0], idx[:, 1]])
+        T1_3 = np.zeros_like(C1)
+        T1_3[idx[:, 0], idx[:, 1]] = x
+        return dict(T1_3=T1_3, T2_3=T2_3, E4=E4)
+
     def _sigma_matrix(self, symR):
         m = self.mask1(symR)
         idx = np.argwhere(m)

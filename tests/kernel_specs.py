@@ -55,6 +55,7 @@ KERNELS = {
     "Wmbej_r1abci": ("iabj", "ai", "abci", lambda r, V, f: f * np.einsum("fj,febm->embj", r, V)),
     "Wmbej_r1ijka": ("iabj", "ai", "ijka", lambda r, V, f: -f * np.einsum("bn,nmje->embj", r, V)),
     "Wmnij_r1ijka": ("ijkl", "ai", "ijka", lambda r, V, f: f * RS(np.einsum("ej,mnie->mnij", r, V))),
+    "Wmnij_r2abij": ("ijkl", "abij", "abij", lambda r, V, f: 0.5 * f * np.einsum("efmn,efij->mnij", V, r)),
 }
 
 

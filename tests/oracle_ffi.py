@@ -189,6 +189,18 @@ class Oracle:
         assert rc == 0, rc
         return dict(T2_1=T2_1, T1_2=T1_2, T2_2=T2_2, E2=E2.value, E3=E3.value, iters=it.value)
 
+    def ground3(self, g):
+        """third order ground state (run3.f90) from the T of ground()"""
+        s = self.s
+        l1, l2 = s.r1_len(1), s.r2_len(1)
+        T1_3, T2_3 = np.zeros(l1), np.zeros(l2)
+        E4, it = ctypes.c_double(), I64()
+        rc = lib().o_cpsd_ground3(ctypes.byref(self.osys), ctypes.byref(self.oint), ctypes.byref(self.par),
+                                  ptr(g["T2_1"]), ptr(g["T1_2"]), ptr(g["T2_2"]), ptr(T1_3), ptr(T2_3),
+                                  ctypes.byref(E4), ctypes.byref(it))
+        assert rc == 0, rc
+        return dict(T1_3=T1_3, T2_3=T2_3, E4=E4.value, iters=it.value)
+
     def jints(self, g):
         s, sym = self.s, self.s.sym
         o, v = s.popo, s.popv

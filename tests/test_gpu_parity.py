@@ -180,6 +180,22 @@ def test_ground_and_intermediates_match_oracle(nirrep):
         np.testing.assert_allclose(host(J[k]), oJ[k], rtol=0, atol=1e-9, err_msg=k)
 
 
+@pytest.mark.parametrize("nirrep", [1, 4, 8])
+def test_ground_third_order_matches_oracle(nirrep):
+    """run3.f90: T2^(3) and E^(4) to the oracle's rounding, T1^(3) to the
+    DIIS tolerance, the same DIIS step count."""
+    s = small(nirrep) if nirrep < 8 else synth.System(nmo=24, nocc_a=4, nocc_b=2, nirrep=8, seed=3)
+    ints, sc, par, orc = _run_both(s)
+    g = api.ground(s, sc, ints, par)
+    g3 = api.ground3(s, sc, ints, par, g)
+    og = orc.ground()
+    og3 = orc.ground3(og)
+    assert abs(g3["E4"] - og3["E4"]) < 1e-11
+    np.testing.assert_allclose(host(g3["T2_3"]), og3["T2_3"], rtol=0, atol=1e-11)
+    np.testing.assert_allclose(host(g3["T1_3"]), og3["T1_3"], rtol=0, atol=1e-8)
+    assert g3["iters"] == og3["iters"]
+
+
 @pytest.mark.parametrize("batch", [0, 1])
 @pytest.mark.parametrize("nirrep", [1, 4])
 def test_eecpsd_roots_match_oracle(nirrep, batch):

@@ -49,6 +49,24 @@ def test_cis_matches_dense_diagonalisation(nirrep, lowest):
 
 
 @pytest.mark.parametrize("nirrep", [1, 4])
+def test_ground_third_order_matches_dense(nirrep):
+    """run3.f90: T2^(3) and E^(4) exactly (closed form), T1^(3) to the
+    DIIS convergence of its loop; every term of C2^(3) is exercised."""
+    s = small(nirrep)
+    orc = of.Oracle(s, diis_max_err=1e-12, diis_cyc=200)
+    g = orc.ground()
+    g3 = orc.ground3(g)
+    ds = dp.DenseSystem(s)
+    d = ds.ground()
+    # the dense third order from the oracle's own (DIIS-converged) T1^(2)
+    d3 = ds.ground3(dict(T2_1=d["T2_1"], T1_2=vo_dense(s, g["T1_2"], 1), T2_2=d["T2_2"]))
+    np.testing.assert_allclose(vvoo_dense(s, g3["T2_3"], 1), d3["T2_3"], rtol=0, atol=1e-12)
+    assert abs(g3["E4"] - d3["E4"]) < 1e-12
+    np.testing.assert_allclose(vo_dense(s, g3["T1_3"], 1), d3["T1_3"], rtol=0, atol=1e-10)
+    assert abs(g3["E4"]) > 1e-8  # the terms are not trivially zero
+
+
+@pytest.mark.parametrize("nirrep", [1, 4])
 def test_ground_matches_dense(nirrep):
     s = small(nirrep)
     g = of.Oracle(s).ground()

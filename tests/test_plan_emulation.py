@@ -133,6 +133,7 @@ KSPEC = {
     "Wmbej_r2abij": ("444", "ba", "fenm", "bfjn", "embj", 0),
     "Wmbej_r1abci": ("424", "ba", "febm", "fj", "embj", 0), "Wmbej_r1ijka": ("424", "ba", "nmje", "bn", "embj", 0),
     "Wmnij_r1ijka": ("424", "ba", "mnie", "ej", "mnij", 2),
+    "Wmnij_r2abij": ("444", "ba", "efmn", "efij", "mnij", 0),
 }
 
 
