@@ -75,6 +75,10 @@ int cpsd_mixed_error(int reset);
  * above 1e-10 (the reference prints a warning for each; their real parts
  * are used, as there). */
 int cpsd_davidson_stats(int64_t *nonsym_steps, int64_t *imag_warnings, int reset);
+/* bytes of each of the two device staging buffers through which a
+ * host-resident abcd is streamed (default 1 GiB; no counterpart in the
+ * reference, which sizes its row blocks by the free iCore) */
+int cpsd_set_host_panel_bytes(size_t bytes);
 
 /* -------------------------------------------------------------- size math */
 /* irpdso (src/libsrint/irpdso.f:1-52) */
@@ -334,7 +338,13 @@ typedef struct {
 } cpsd_system;
 
 /* spin-free integrals in DPD layout, iop 0 on antisymmetric pairs, device
- * pointers (allocate_mem, src/EE-CPSd.SF/allocate_mem.f90:14-44) */
+ * pointers (allocate_mem, src/EE-CPSd.SF/allocate_mem.f90:14-44).  abcd
+ * may instead be host memory, for systems whose abcd does not fit in HBM
+ * (the reference keeps it on disk then, vvvv_incore = .false.,
+ * allocate_mem.f90:38-43): the particle ladder then streams it through two
+ * device staging buffers (cpsd_set_host_panel_bytes), FP64 also in the
+ * mixed mode; pinned host memory (cudaHostAlloc / cudaHostRegister) keeps
+ * the copies at full link speed. */
 typedef struct {
     const double *ijkl, *ijka, *abij, *iabj, *abci, *abcd;
     const double *eorb; /* spin-free orbital energies (src/getHF/resortEorb.f90) */

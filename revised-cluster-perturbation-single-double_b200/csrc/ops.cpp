@@ -686,8 +686,100 @@ int k_c2_r2Wmbej(Ten &c2, const Ten &r2, const Ten &W, double f, i64 nb) {
 int k_c2_r2Wmnij(Ten &c2, const Ten &r2, const Ten &W, double f, i64 nb) {
     return w444(r2, W, c2, r2.d.iop[0] == 0 ? f : 0.5 * f, "abmn", "mnij", "abij", 0, nb);
 }
+namespace {
+// ------------------------------------------- out-of-core particle ladder
+// abcd in host memory (too large for HBM): the reference streams it from
+// disk in blocks of rows (p_c2_r2abcd_h, src/lib_cc/c2_r2abcd.f90:29-95);
+// here each irrep block V_h (n_ab x n_ef, column-major) is streamed in
+// panels of whole columns (contiguous in host memory) through two device
+// staging buffers on a copy stream, each panel's GEMM
+//   C_g(ab, ij) += f V_h(ab, ef0..ef1) R_g(ef0..ef1, ij)   (g = h x sym(R))
+// queued on the library stream as soon as its copy has landed, so the copy
+// of the next panel overlaps the GEMM of this one.  Host memory allocated
+// pinned (cudaHostAlloc / cudaHostRegister) is read at full PCIe / C2C
+// speed; pageable memory works too, with staged copies.
+std::atomic<size_t> g_panel_bytes{(size_t)1 << 30};
+
+bool host_resident(const void *p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return true;
+    }
+    return a.type == cudaMemoryTypeHost || a.type == cudaMemoryTypeUnregistered;
+}
+
+struct CopyLane {  // per host thread: copy stream and events
+    cudaStream_t cs = nullptr;
+    cudaEvent_t start = nullptr, copied[2] = {}, used[2] = {};
+    int init() {
+        if (cs) return CPSD_OK;
+        CPSD_TRY(cuda_check(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "copy stream"));
+        CPSD_TRY(cuda_check(cudaEventCreateWithFlags(&start, cudaEventDisableTiming), "event"));
+        for (int b = 0; b < 2; b++) {
+            CPSD_TRY(cuda_check(cudaEventCreateWithFlags(&copied[b], cudaEventDisableTiming), "event"));
+            CPSD_TRY(cuda_check(cudaEventCreateWithFlags(&used[b], cudaEventDisableTiming), "event"));
+        }
+        return CPSD_OK;
+    }
+};
+
+int stream_abcd(Ten &c2, const Ten &r2, const Ten &V, double f, i64 nb) {
+    OpScope op;
+    const Desc &dv = V.d, &dr = r2.d, &dc = c2.d;
+    bool ok = dv.sym == 1 && dv.iop[0] == dc.iop[0] && dv.iop[1] == dr.iop[0] && dc.iop[1] == dr.iop[1] &&
+              dc.sym == dr.sym;
+    for (int h = 0; h < 8 && ok; h++)
+        ok = dv.pop[0][h] == dc.pop[0][h] && dv.pop[1][h] == dc.pop[1][h] && dv.pop[2][h] == dr.pop[0][h] &&
+             dv.pop[3][h] == dr.pop[1][h] && dc.pop[2][h] == dr.pop[2][h] && dc.pop[3][h] == dr.pop[3][h];
+    if (!ok)
+        return set_error(CPSD_ELAYOUT, "host-resident abcd: the ab / ef pairs of V, R2 and C2 must match (packed alike)");
+    thread_local CopyLane lane;
+    CPSD_TRY(lane.init());
+    ScratchScope sc;
+    const i64 words = std::max<i64>(1, (i64)(g_panel_bytes.load() / sizeof(double)));
+    double *stg[2];
+    CPSD_TRY(scratch(words, &stg[0]));
+    CPSD_TRY(scratch(words, &stg[1]));
+    // the staging memory may still be read by earlier work on the library
+    // stream: the copy stream starts after it
+    CPSD_TRY(cuda_check(cudaEventRecord(lane.start, stream()), "event record"));
+    CPSD_TRY(cuda_check(cudaStreamWaitEvent(lane.cs, lane.start, 0), "stream wait"));
+    int buf = 0;
+    bool used[2] = {false, false};
+    const i64 sB = nb > 1 ? (r2.bs ? r2.bs : dr.len()) : 0, sC = nb > 1 ? (c2.bs ? c2.bs : dc.len()) : 0;
+    for (i64 h = 1; h <= ctx().nirrep; h++) {
+        const i64 nab = dv.nleft(h), nef = dv.nright(h), g = dp(h, dr.sym), nij = dr.nright(g);
+        if (nab == 0 || nef == 0 || nij == 0) continue;
+        const double *Vh = V.arr + dv.block_base(h);
+        const double *Rg = r2.arr + dr.block_base(g);
+        double *Cg = c2.arr + dc.block_base(g);
+        const i64 kc = std::max<i64>(1, std::min<i64>(nef, words / nab));
+        if (nab > words) return set_error(CPSD_EARG, "host-resident abcd: one column exceeds the staging buffer");
+        for (i64 k0 = 0; k0 < nef; k0 += kc) {
+            const i64 kn = std::min(kc, nef - k0);
+            if (used[buf]) CPSD_TRY(cuda_check(cudaStreamWaitEvent(lane.cs, lane.used[buf], 0), "stream wait"));
+            CPSD_TRY(cuda_check(cudaMemcpyAsync(stg[buf], Vh + k0 * nab, sizeof(double) * (size_t)(nab * kn),
+                                                cudaMemcpyHostToDevice, lane.cs),
+                                "abcd panel copy"));
+            CPSD_TRY(cuda_check(cudaEventRecord(lane.copied[buf], lane.cs), "event record"));
+            CPSD_TRY(cuda_check(cudaStreamWaitEvent(stream(), lane.copied[buf], 0), "stream wait"));
+            const ContractPlan *p;
+            CPSD_TRY(plan_gemm(nab, nij, kn, nab, nef, nab, nb, sB, sC, &p));
+            CPSD_TRY(launch_contract(p, stg[buf], Rg + k0, Cg, f));
+            CPSD_TRY(cuda_check(cudaEventRecord(lane.used[buf], stream()), "event record"));
+            used[buf] = true;
+            buf ^= 1;
+        }
+    }
+    return CPSD_OK;
+}
+}  // namespace
+
 int k_c2_r2abcd(Ten &c2, const Ten &r2, const Ten &V, double f, i64 nb) {
-    return w444(V, r2, c2, r2.d.iop[0] == 1 ? 0.5 * f : f, "abef", "efij", "abij", 0, nb);
+    const double fr = r2.d.iop[0] == 1 ? 0.5 * f : f;
+    if (V.arr && host_resident(V.arr)) return stream_abcd(c2, r2, V, fr, nb);
+    return w444(V, r2, c2, fr, "abef", "efij", "abij", 0, nb);
 }
 int k_c2_r2Fae(Ten &c2, const Ten &r2, const Ten &F, double f, i64 nb) {
     return w424(r2, F, c2, f, "aeij", "be", "abij", 1, nb);
@@ -853,6 +945,12 @@ int cpsd_mixed_error(int reset) {
     if (reset && h)
         CPSD_TRY(cuda_check(cudaMemsetAsync(ctx().oz_err, 0, sizeof(int), stream()), "clear error word"));
     return h;
+}
+
+int cpsd_set_host_panel_bytes(size_t bytes) {
+    if (bytes < 4096) return set_error(CPSD_EARG, "staging buffers of at least 4096 bytes");
+    g_panel_bytes.store(bytes);
+    return CPSD_OK;
 }
 
 int cpsd_davidson_stats(int64_t *nonsym_steps, int64_t *imag_warnings, int reset) {

@@ -92,6 +92,77 @@ int EnergyPlan::upload() {
     return CPSD_OK;
 }
 
+// Tile shape, tiles and split-K groups of a plan whose tasks and segments
+// are built: the shape with the least estimated time counting the padded
+// tensor-pipe work (FP64 ~35 TFLOP/s) and the operand re-reads (~6 TB/s);
+// split-K so that small outputs with long K still fill the GPU
+void finish_plan(ContractPlan *plan, std::vector<TaskDev> tasks, std::vector<SegDev> dsegs) {
+    int cfg = 0;
+    double best = 1e300;
+    for (int c = 0; c < 4; c++) {
+        double fl = 0, by = 0;
+        for (auto &tk : tasks) {
+            double mt = (double)((tk.M + TILE_BM[c] - 1) / TILE_BM[c]), nt = (double)((tk.N + TILE_BN[c] - 1) / TILE_BN[c]);
+            fl += 2.0 * mt * TILE_BM[c] * nt * TILE_BN[c] * (double)tk.Ktot;
+            by += 8.0 * (double)tk.Ktot * ((double)tk.M * nt + (double)tk.N * mt);
+        }
+        double t = fl / 35e12 + by / 6e12;
+        if (t < best * 0.999) {
+            best = t;
+            cfg = c;
+        }
+    }
+    const i64 TBM = TILE_BM[cfg], TBN = TILE_BN[cfg];
+    plan->cfg = cfg;
+    // tiles, with split-K so that small outputs with long K still fill the GPU
+    std::vector<TileDev> tiles;
+    std::vector<int> red;
+    i64 mn_tiles = 0;
+    for (auto &tk : tasks) mn_tiles += ((tk.M + TBM - 1) / TBM) * ((tk.N + TBN - 1) / TBN);
+    const i64 target = 4 * 148;
+    i64 part = 0;
+    for (int ti = 0; ti < (int)tasks.size(); ti++) {
+        const TaskDev &tk = tasks[ti];
+        i64 mt = (tk.M + TBM - 1) / TBM, nt = (tk.N + TBN - 1) / TBN;
+        i64 want = (mn_tiles >= target) ? 1 : (target + mn_tiles - 1) / mn_tiles;
+        i64 maxsplit = std::max<i64>(1, tk.Ktot / 256);
+        i64 ns = std::min(want, maxsplit);
+        if (ns > 64) ns = 64;
+        for (i64 a = 0; a < mt; a++)
+            for (i64 b = 0; b < nt; b++) {
+                if (ns > 1) {
+                    red.push_back(ti);
+                    red.push_back((int)a);
+                    red.push_back((int)b);
+                    red.push_back((int)part);
+                    red.push_back((int)ns);
+                }
+                for (i64 s = 0; s < ns; s++) {
+                    TileDev t{};
+                    t.task = ti;
+                    t.mt = (int)a;
+                    t.nt = (int)b;
+                    t.nsplit = (int)ns;
+                    t.k_lo = tk.Ktot * s / ns;
+                    t.k_hi = tk.Ktot * (s + 1) / ns;
+                    t.part = ns > 1 ? part + s : -1;
+                    tiles.push_back(t);
+                }
+                if (ns > 1) part += ns;
+            }
+    }
+    plan->ntasks = (int)tasks.size();
+    plan->nsegs = (int)dsegs.size();
+    plan->ntiles = (int)tiles.size();
+    plan->nparts = part;
+    plan->nreduce = (int)red.size() / 5;
+    plan->empty = tiles.empty();
+    plan->h_tasks = std::move(tasks);
+    plan->h_segs = std::move(dsegs);
+    plan->h_tiles = std::move(tiles);
+    plan->h_reduce = std::move(red);
+}
+
 int plan_contract(const Desc &d1, const char *t1, const Desc &d2, const char *t2, const Desc &d3,
                   const char *t3, const Batch &batch, const ContractPlan **out) {
     static std::mutex m;
@@ -383,72 +454,56 @@ int plan_contract(const Desc &d1, const char *t1, const Desc &d2, const char *t2
         }
         i = j;
     }
-    // tile shape: the one with the least estimated time, counting the padded
-    // tensor-pipe work (FP64 ~35 TFLOP/s) and the operand re-reads (~6 TB/s)
-    int cfg = 0;
-    double best = 1e300;
-    for (int c = 0; c < 4; c++) {
-        double fl = 0, by = 0;
-        for (auto &tk : tasks) {
-            double mt = (double)((tk.M + TILE_BM[c] - 1) / TILE_BM[c]), nt = (double)((tk.N + TILE_BN[c] - 1) / TILE_BN[c]);
-            fl += 2.0 * mt * TILE_BM[c] * nt * TILE_BN[c] * (double)tk.Ktot;
-            by += 8.0 * (double)tk.Ktot * ((double)tk.M * nt + (double)tk.N * mt);
-        }
-        double t = fl / 35e12 + by / 6e12;
-        if (t < best * 0.999) {
-            best = t;
-            cfg = c;
-        }
+    finish_plan(plan.get(), std::move(tasks), std::move(dsegs));
+    *out = plan.get();
+    cache[key] = std::move(plan);
+    return CPSD_OK;
+}
+
+// A strided GEMM as a one-task plan: C[m + n ldc + r sC] += A[m + k lda]
+// B[k + n ldb + r sB] for m < M, n < N, k < K and r < nb copies of B and C
+// (the panels of the out-of-core particle ladder)
+int plan_gemm(i64 M, i64 N, i64 K, i64 lda, i64 ldb, i64 ldc, i64 nb, i64 sB, i64 sC, const ContractPlan **out) {
+    static std::mutex m;
+    std::lock_guard<std::mutex> lock(m);
+    static std::map<std::string, std::unique_ptr<ContractPlan>> cache;
+    const std::string key = std::to_string(M) + "," + std::to_string(N) + "," + std::to_string(K) + "," +
+                            std::to_string(lda) + "," + std::to_string(ldb) + "," + std::to_string(ldc) + "," +
+                            std::to_string(nb) + "," + std::to_string(sB) + "," + std::to_string(sC);
+    auto it = cache.find(key);
+    if (it != cache.end()) {
+        *out = it->second.get();
+        return CPSD_OK;
     }
-    const i64 TBM = TILE_BM[cfg], TBN = TILE_BN[cfg];
-    plan->cfg = cfg;
-    // tiles, with split-K so that small outputs with long K still fill the GPU
-    std::vector<TileDev> tiles;
-    std::vector<int> red;
-    i64 mn_tiles = 0;
-    for (auto &tk : tasks) mn_tiles += ((tk.M + TBM - 1) / TBM) * ((tk.N + TBN - 1) / TBN);
-    const i64 target = 4 * 148;
-    i64 part = 0;
-    for (int ti = 0; ti < (int)tasks.size(); ti++) {
-        const TaskDev &tk = tasks[ti];
-        i64 mt = (tk.M + TBM - 1) / TBM, nt = (tk.N + TBN - 1) / TBN;
-        i64 want = (mn_tiles >= target) ? 1 : (target + mn_tiles - 1) / mn_tiles;
-        i64 maxsplit = std::max<i64>(1, tk.Ktot / 256);
-        i64 ns = std::min(want, maxsplit);
-        if (ns > 64) ns = 64;
-        for (i64 a = 0; a < mt; a++)
-            for (i64 b = 0; b < nt; b++) {
-                if (ns > 1) {
-                    red.push_back(ti);
-                    red.push_back((int)a);
-                    red.push_back((int)b);
-                    red.push_back((int)part);
-                    red.push_back((int)ns);
-                }
-                for (i64 s = 0; s < ns; s++) {
-                    TileDev t{};
-                    t.task = ti;
-                    t.mt = (int)a;
-                    t.nt = (int)b;
-                    t.nsplit = (int)ns;
-                    t.k_lo = tk.Ktot * s / ns;
-                    t.k_hi = tk.Ktot * (s + 1) / ns;
-                    t.part = ns > 1 ? part + s : -1;
-                    tiles.push_back(t);
-                }
-                if (ns > 1) part += ns;
-            }
-    }
-    plan->ntasks = (int)tasks.size();
-    plan->nsegs = (int)dsegs.size();
-    plan->ntiles = (int)tiles.size();
-    plan->nparts = part;
-    plan->nreduce = (int)red.size() / 5;
-    plan->empty = tiles.empty();
-    plan->h_tasks = std::move(tasks);
-    plan->h_segs = std::move(dsegs);
-    plan->h_tiles = std::move(tiles);
-    plan->h_reduce = std::move(red);
+    if (M <= 0 || N <= 0 || K <= 0 || nb <= 0) return set_error(CPSD_EARG, "plan_gemm: empty GEMM");
+    TaskDev tk{};
+    tk.nm = 1;
+    tk.mExt[0] = M;
+    tk.mSC[0] = 1;
+    tk.nn = nb > 1 ? 2 : 1;
+    tk.nExt[0] = N;
+    tk.nSC[0] = ldc;
+    tk.nExt[1] = nb;
+    tk.nSC[1] = sC;
+    tk.M = M;
+    tk.N = N * nb;
+    tk.Ktot = K;
+    tk.seg0 = 0;
+    tk.nseg = 1;
+    SegDev sd{};
+    sd.nk = 1;
+    sd.K = K;
+    sd.mSA[0] = 1;
+    sd.nSB[0] = ldb;
+    sd.nSB[1] = sB;
+    sd.kExt[0] = K;
+    sd.kSA[0] = lda;
+    sd.kSB[0] = 1;
+    sd.aMfast = 1;
+    sd.bKfast = 1;
+    auto plan = std::make_unique<ContractPlan>();
+    plan->flops = 2.0 * (double)M * (double)N * (double)nb * (double)K;
+    finish_plan(plan.get(), {tk}, {sd});
     *out = plan.get();
     cache[key] = std::move(plan);
     return CPSD_OK;

@@ -185,6 +185,10 @@ struct Batch {
 int plan_contract(const Desc &d1, const char *t1, const Desc &d2, const char *t2, const Desc &d3,
                   const char *t3, const Batch &batch, const ContractPlan **out);
 
+// C[m + n ldc + r sC] += A[m + k lda] B[k + n ldb + r sB] (m < M, n < N,
+// k < K, r < nb) as a one-task plan of the tile kernel
+int plan_gemm(i64 M, i64 N, i64 K, i64 lda, i64 ldb, i64 ldc, i64 nb, i64 sB, i64 sC, const ContractPlan **out);
+
 // ------------------------------------------------------- pair-map plans
 // out[ob + r*nlo + l] = beta*out + alpha * sum_terms s_l s_r in[ib + ri*nli + li]
 struct PMBlockDev {

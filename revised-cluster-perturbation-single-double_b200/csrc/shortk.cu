@@ -34,6 +34,49 @@ __device__ __forceinline__ i64 sdecode(i64 x, int n, const i64 *ext, const i64 *
     return n > 0 ? off + x * st[n - 1] : off;
 }
 
+// operand tile dst[(kk + k) * R + r] = src[offR[r] + offK[k]] (0 outside
+// the task), r < R, k < K; consecutive threads walk r when rfast (else k),
+// the source's contiguous side; eight loads of a thread are in flight
+// before their stores
+template <int R>
+__device__ __forceinline__ void stage(double *dst, const double *__restrict__ src, const i64 *offR, const i64 *offK,
+                                      int K, int kk, bool rfast) {
+    constexpr int U = 8;
+    const int total = R * K;
+    auto split = [&](int e, int &r, int &k) {
+        if (rfast) {
+            r = e % R;
+            k = e / R;
+        } else {
+            k = e % K;
+            r = e / K;
+        }
+    };
+    for (int e0 = threadIdx.x; e0 < total; e0 += ST * U) {
+        double v[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int e = e0 + u * ST;
+            v[u] = 0.0;
+            if (e < total) {
+                int r, k;
+                split(e, r, k);
+                const i64 o = offR[r];
+                if (o >= 0) v[u] = __ldg(src + o + offK[k]);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int e = e0 + u * ST;
+            if (e < total) {
+                int r, k;
+                split(e, r, k);
+                dst[(size_t)(kk + k) * R + r] = v[u];
+            }
+        }
+    }
+}
+
 template <int BS, bool FM>
 __global__ void __launch_bounds__(ST, 3) k_shortk(const double *__restrict__ A, const double *__restrict__ B,
                                                double *__restrict__ C, const TaskDev *__restrict__ tasks,
@@ -49,7 +92,9 @@ __global__ void __launch_bounds__(ST, 3) k_shortk(const double *__restrict__ A, 
     __shared__ SegDev sg;
     const int tid = threadIdx.x;
     const ShortKItem it = items[blockIdx.x];
+    // the task and its first segment are fetched side by side
     if (tid == 0) tk = tasks[it.task];
+    if (tid == 32) sg = segs[it.seg0];
     __syncthreads();
     const i64 m0 = FM ? it.f0 : it.s0, n0 = FM ? it.s0 : it.f0;
     for (int i = tid; i < BM; i += ST) {
@@ -76,9 +121,11 @@ __global__ void __launch_bounds__(ST, 3) k_shortk(const double *__restrict__ A, 
     // the operand tiles, segment after segment along K
     int kk = 0;
     for (int si = 0; si < tk.nseg; si++) {
-        __syncthreads();
-        if (tid == 0) sg = segs[tk.seg0 + si];
-        __syncthreads();
+        if (si > 0) {
+            __syncthreads();
+            if (tid == 0) sg = segs[tk.seg0 + si];
+            __syncthreads();
+        }
         const int K = (int)sg.K;
         for (int i = tid; i < BM; i += ST) {
             const i64 m = m0 + i;
@@ -105,30 +152,8 @@ __global__ void __launch_bounds__(ST, 3) k_shortk(const double *__restrict__ A, 
             offKB[k] = b;
         }
         __syncthreads();
-        for (int e = tid; e < BM * K; e += ST) {
-            int m, k;
-            if (sg.aMfast) {
-                m = e % BM;
-                k = e / BM;
-            } else {
-                k = e % K;
-                m = e / K;
-            }
-            const i64 om = offAM[m];
-            As[(size_t)(kk + k) * BM + m] = om >= 0 ? __ldg(A + om + offKA[k]) : 0.0;
-        }
-        for (int e = tid; e < BN * K; e += ST) {
-            int n, k;
-            if (sg.bKfast) {
-                k = e % K;
-                n = e / K;
-            } else {
-                n = e % BN;
-                k = e / BN;
-            }
-            const i64 on = offBN[n];
-            Bs[(size_t)(kk + k) * BN + n] = on >= 0 ? __ldg(B + on + offKB[k]) : 0.0;
-        }
+        stage<BM>(As, A, offAM, offKA, K, kk, sg.aMfast != 0);
+        stage<BN>(Bs, B, offBN, offKB, K, kk, sg.bKfast == 0);
         kk += K;
     }
     __syncthreads();
@@ -234,7 +259,7 @@ int plan_shortk(const ContractPlan *cp, const ShortKPlan **out) {
             const TaskDev &t = cp->h_tasks[ti];
             const i64 F = p.fm ? t.M : t.N, S = p.fm ? t.N : t.M;
             for (i64 s0 = 0; s0 < S; s0 += p.bs)
-                for (i64 f0 = 0; f0 < F; f0 += bf) p.items.push_back(ShortKItem{ti, 0, f0, s0});
+                for (i64 f0 = 0; f0 < F; f0 += bf) p.items.push_back(ShortKItem{ti, t.seg0, f0, s0});
         }
         *out = P.get();
     }

@@ -12,9 +12,10 @@ namespace cpsd {
 constexpr int SHORTK_KMAX = 64;
 
 // one CTA's work: the BF x BS output tile of a task starting at (f0, s0)
-// along the output's contiguous side (f) and the other side (s)
+// along the output's contiguous side (f) and the other side (s); seg0 = the
+// task's first segment (fetched beside the task)
 struct ShortKItem {
-    int task, pad;
+    int task, seg0;
     i64 f0, s0;
 };
 

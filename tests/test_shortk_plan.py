@@ -22,7 +22,7 @@ from test_plan_emulation import KSPEC, to_engine, norm, I64, get_plan, decode
 
 
 class ShortKItem(ctypes.Structure):
-    _fields_ = [("task", ctypes.c_int), ("pad", ctypes.c_int), ("f0", I64), ("s0", I64)]
+    _fields_ = [("task", ctypes.c_int), ("seg0", ctypes.c_int), ("f0", I64), ("s0", I64)]
 
 
 def get_shortk(o1, t1, o2, t2, o3, t3, nb, sA, sB, sC):
@@ -47,6 +47,7 @@ def emulate(tasks, segs, plan, A, B, C, alpha):
         tk = tasks[it.task]
         F, S = (tk.M, tk.N) if plan["fm"] else (tk.N, tk.M)
         assert 0 <= it.f0 < F and 0 <= it.s0 < S and it.f0 % bf == 0 and it.s0 % bs == 0
+        assert it.seg0 == tk.seg0 and tk.nseg >= 1
         f = np.arange(it.f0, min(it.f0 + bf, F))
         s = np.arange(it.s0, min(it.s0 + bs, S))
         m, n = (f, s) if plan["fm"] else (s, f)
