@@ -300,6 +300,15 @@ int cpsd_contract_records(double *ms, double *flops, int64_t *shape, int64_t max
 int cpsd_debug_narrow_plan(const cpsd_opt *v1, const char *t1, const cpsd_opt *v2, const char *t2,
                            const cpsd_opt *v3, const char *t3, int64_t nb, int64_t sA, int64_t sB, int64_t sC,
                            const void **items, int64_t *nitems, const void **reds, int64_t *nreds, int64_t *flags);
+/* work items of the row-dot kernel for a contraction (layout RowDotItem of
+ * csrc/rowdot.cuh) and the task / segment tables it reads (the plan's,
+ * row units reordered by stride); flags = {row-dot, rows over N, K / 32
+ * rounded up, columns per item rounded up}; items = NULL when it does not
+ * qualify */
+int cpsd_debug_rowdot_plan(const cpsd_opt *v1, const char *t1, const cpsd_opt *v2, const char *t2,
+                           const cpsd_opt *v3, const char *t3, int64_t nb, int64_t sA, int64_t sB, int64_t sC,
+                           const void **items, int64_t *nitems, const void **tasks, const void **segs,
+                           int64_t *flags);
 /* work items of the short-K kernel for a contraction (layout ShortKItem of
  * csrc/shortk.cuh); flags = {short-K, f runs along M, tile extent BS along
  * the other side, largest contracted range}; items = NULL when it does not

@@ -184,6 +184,10 @@ void o_denomT2(double *t2, const double *r2, const double *eorb, const i64 *pop_
  * Returns the number of Davidson iterations summed over irreps in *iters. */
 int o_cis_run(const o_system *s, const o_integrals *I, const o_params *p,
               double *omega, double *R, i64 *iters);
+/* CIS(D-infinity) (src/CISdoo.SD.SF/run.f90): roots of the (R1, R2) problem;
+ * R receives per root the R1 (l1) and R2 (l2, packed) of its irrep */
+int o_cisdoo_run(const o_system *s, const o_integrals *I, const o_params *p, double *omega, double *R,
+                 i64 *iters);
 
 /* ground CPS(D) first and second order (src/CPSd.SF/run1.f90, run2.f90):
  * T2^(1), T1^(2), T2^(2), E^(2), E^(3) */

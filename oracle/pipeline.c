@@ -117,6 +117,110 @@ int o_cis_run(const o_system *s, const o_integrals *I, const o_params *p,
     return O_OK;
 }
 
+/* ---------------- CIS(D-infinity) (src/CISdoo.SD.SF/run.f90, calAR.f90) ----
+ * Davidson over (R1, R2) of one irrep with the sigma of calAR.f90:19-49:
+ *   C1 = Fac R1 - R1 Fki + Wkaci R1 + c1_r2abci(R2) + c1_r2ijka(R2)
+ *   C2 = e(ab,ij) R2 + c2_r1abci(R1) + c2_r1ijka(R1)
+ * with MP2t = denomT2(abij), Fac = diag(e_v) + Fae_r2abij(MP2t),
+ * Fki = diag(e_o) + Fmi_r2abij(MP2t), Wkaci = iabj + 2 Wmbej_r2abij(MP2t)
+ * (run.f90:25-39, putDiagFock.f90); the diagonal preconditioner is
+ * (Eorb_diff1, Eorb_diff2) and the guesses the singles' (run.f90:42-60). */
+typedef struct {
+    const o_system *s;
+    const ints_t *I;
+    const o_opt *fac, *fki, *wk;
+    const double *oed2;
+    i64 sym, l1, l2;
+} doo_ctx;
+
+static void doo_sigma(void *vctx, const double *R, double *AR)
+{
+    doo_ctx *c = (doo_ctx *)vctx;
+    const i64 *o = c->s->popo, *V = c->s->popv;
+    o_opt r1, r2, c1, c2;
+    o_opt_view(&r1, V, o, Z, Z, 1, 1, c->sym, (double *)R);
+    o_opt_view(&r2, V, V, o, o, 0, 0, c->sym, (double *)R + c->l1);
+    o_opt_view(&c1, V, o, Z, Z, 1, 1, c->sym, AR);
+    o_opt_view(&c2, V, V, o, o, 0, 0, c->sym, AR + c->l1);
+    memset(AR, 0, sizeof(double) * (size_t)c->l1);
+    o_c1_r1Fae(&c1, &r1, c->fac, 1.0);
+    o_c1_r1Fmi(&c1, &r1, c->fki, 1.0);
+    o_c1_r1iabj(&c1, &r1, c->wk, 1.0);
+    o_c1_r2abci(&c1, &r2, &c->I->abci, 1.0);
+    o_c1_r2ijka(&c1, &r2, &c->I->ijka, 1.0);
+    for (i64 k = 0; k < c->l2; k++) AR[c->l1 + k] = c->oed2[k] * R[c->l1 + k];
+    o_c2_r1abci(&c2, &r1, &c->I->abci, 1.0);
+    o_c2_r1ijka(&c2, &r1, &c->I->ijka, 1.0);
+}
+
+/* putDiagFock (src/lib_cc/putDiagFock.f90:6-56): f(p,p) = e_p on the
+ * diagonal of the (pop, pop) block of every irrep; eorb holds the occupied
+ * orbitals of all irreps, then the virtual ones */
+static void put_diag(double *F, const double *eorb, const o_system *s, int vir)
+{
+    const i64 *pp = vir ? s->popv : s->popo;
+    i64 e0 = 0;
+    if (vir)
+        for (i64 h = 0; h < s->nirrep; h++) e0 += s->popo[h];
+    i64 off = 0;
+    for (i64 h = 0; h < s->nirrep; h++) {
+        for (i64 p = 0; p < pp[h]; p++) F[off + p * pp[h] + p] = eorb[e0 + p];
+        off += pp[h] * pp[h];
+        e0 += pp[h];
+    }
+}
+
+int o_cisdoo_run(const o_system *s, const o_integrals *I, const o_params *p, double *omega, double *R,
+                 i64 *iters)
+{
+    ints_t v;
+    ints_view(s, I, &v);
+    const i64 *o = s->popo, *V = s->popv;
+    i64 l2g = o_idsymsoc(1, V, V, 0, o, o, 0);
+    double *mp2 = zalloc(l2g), *fa = zalloc(o_irpdso(1, V, V, 1)), *fk = zalloc(o_irpdso(1, o, o, 1));
+    double *wka = zalloc(v.iabj.len);
+    o_opt mp2t, fac, fki, wk;
+    o_opt_view(&mp2t, V, V, o, o, 0, 0, 1, mp2);
+    o_opt_view(&fac, V, V, Z, Z, 1, 1, 1, fa);
+    o_opt_view(&fki, o, o, Z, Z, 1, 1, 1, fk);
+    o_opt_view(&wk, V, o, V, o, 1, 1, 1, wka);
+    o_denomT2(mp2, I->abij, I->eorb, V, o, 1, 0);
+    put_diag(fa, I->eorb, s, 1);
+    put_diag(fk, I->eorb, s, 0);
+    memcpy(wka, I->iabj, sizeof(double) * (size_t)v.iabj.len);
+    int rc = o_Fae_r2abij(&fac, &mp2t, &v.abij, 1.0);
+    if (rc == O_OK) rc = o_Fmi_r2abij(&fki, &mp2t, &v.abij, 1.0);
+    if (rc == O_OK) rc = o_Wmbej_r2abij(&wk, &mp2t, &v.abij, 2.0);
+    i64 kroot = 0, roff = 0, itsum = 0;
+    for (i64 sym = 1; sym <= s->nirrep && rc == O_OK; sym++) {
+        i64 nroot = p->estate_sym[sym - 1];
+        if (nroot == 0) continue;
+        i64 l1 = o_irpdso(sym, V, o, 1), l2 = o_idsymsoc(sym, V, V, 0, o, o, 0), len = l1 + l2;
+        double *diag = zalloc(len), *g1 = zalloc((1 + l1) * nroot), *file = zalloc((1 + len) * nroot);
+        o_eorb_diff1(diag, I->eorb, V, o, sym);
+        o_eorb_diff2(diag + l1, I->eorb, V, o, sym, 0);
+        rc = o_guess(s, I->eorb, p, sym, nroot, g1);
+        for (i64 k = 0; k < nroot && rc == O_OK; k++)
+            memcpy(file + (1 + len) * k, g1 + (1 + l1) * k, sizeof(double) * (size_t)(1 + l1));
+        doo_ctx ctx = {s, &v, &fac, &fki, &wk, diag + l1, sym, l1, l2};
+        i64 it = 0;
+        if (rc == O_OK) rc = o_davidson(file, diag, len, nroot, 1, p, doo_sigma, &ctx, &it);
+        itsum += it;
+        for (i64 k = 0; k < nroot; k++) {
+            omega[kroot + k] = file[(1 + len) * k];
+            memcpy(R + roff + len * k, file + (1 + len) * k + 1, sizeof(double) * (size_t)len);
+        }
+        kroot += nroot;
+        roff += len * nroot;
+        free(diag);
+        free(g1);
+        free(file);
+    }
+    if (iters) *iters = itsum;
+    free(mp2); free(fa); free(fk); free(wka);
+    return rc;
+}
+
 /* ---------------- ground CPS(D) ---------------- */
 int o_cpsd_ground(const o_system *s, const o_integrals *I, const o_params *p,
                   double *T2_1, double *T1_2, double *T2_2, double *E2, double *E3,

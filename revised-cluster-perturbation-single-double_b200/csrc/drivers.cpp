@@ -20,6 +20,9 @@
 #include <vector>
 
 #include "drivers.hpp"
+
+#include <cstdio>
+#include <cstdlib>
 #include "solvers.cuh"
 
 namespace cpsd {
@@ -911,6 +914,9 @@ int cpsd_eecpsd_roots(const cpsd_system *s, const cpsd_integrals *I, const cpsd_
             chunk = std::max<i64>(1, std::min<i64>(nroot, (i64)(0.7 * ctx().mem_share * avail / per_root)));
         }
     }
+    if (getenv("CPSD_TRACE"))
+        fprintf(stderr, "[cpsd] eecpsd_roots symR=%lld nroot=%lld roots per batch=%lld\n", (long long)symR,
+                (long long)nroot, (long long)chunk);
     i64 tot = 0;
     for (i64 r = 0; r < nroot; r += chunk) {
         const i64 nb = std::min(chunk, nroot - r);

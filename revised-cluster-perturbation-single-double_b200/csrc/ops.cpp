@@ -7,6 +7,7 @@
 #include "drivers.hpp"
 #include "narrow.cuh"
 #include "ozaki.cuh"
+#include "rowdot.cuh"
 #include "shortk.cuh"
 #include "solvers.cuh"
 
@@ -115,6 +116,14 @@ int engine(const Ten &v1, const char *t1, const Ten &v2, const char *t2, Ten &v3
         trace_contraction(p, t1, t2, t3, nb, np->longk ? "narrow_k" : "narrow_rows");
         ctx().flops += p->flops;
         return launch_narrow(p, np, v1.arr, v2.arr, v3.arr, f1);
+    }
+    // a narrow output whose rows are strided but contiguous along a short K
+    const RowDotPlan *rp = nullptr;
+    if (!p->empty) CPSD_TRY(plan_rowdot(p, &rp));
+    if (rp) {
+        trace_contraction(p, t1, t2, t3, nb, "rowdot");
+        ctx().flops += p->flops;
+        return launch_rowdot(p, rp, v1.arr, v2.arr, v3.arr, f1);
     }
     // a contracted range of at most 64 everywhere: the output's
     // read-modify-write bounds it, streaming kernel instead of tiles
@@ -1259,6 +1268,31 @@ int cpsd_debug_narrow_plan(const cpsd_opt *v1, const char *t1, const cpsd_opt *v
     flags[1] = np && np->swap ? 1 : 0;
     flags[2] = np && np->longk ? 1 : 0;
     flags[3] = np ? np->nparts : 0;
+    return CPSD_OK;
+}
+
+int cpsd_debug_rowdot_plan(const cpsd_opt *v1, const char *t1, const cpsd_opt *v2, const char *t2,
+                           const cpsd_opt *v3, const char *t3, int64_t nb, int64_t sA, int64_t sB, int64_t sC,
+                           const void **items, int64_t *nitems, const void **tasks, const void **segs,
+                           int64_t *flags) {
+    CPSD_TRY(need_init());
+    Batch b;
+    b.nb = nb;
+    b.strideA = sA;
+    b.strideB = sB;
+    b.strideC = sC;
+    const ContractPlan *p;
+    CPSD_TRY(plan_contract(desc_of(v1), t1, desc_of(v2), t2, desc_of(v3), t3, b, &p));
+    const RowDotPlan *rp = nullptr;
+    if (!p->empty) CPSD_TRY(plan_rowdot(p, &rp));
+    *items = rp ? rp->items.data() : nullptr;
+    *nitems = rp ? (int64_t)rp->items.size() : 0;
+    *tasks = rp ? rp->tasks.data() : nullptr;
+    *segs = rp ? rp->segs.data() : nullptr;
+    flags[0] = rp ? 1 : 0;
+    flags[1] = rp && rp->swap ? 1 : 0;
+    flags[2] = rp ? rp->kq : 0;
+    flags[3] = rp ? rp->nc : 0;
     return CPSD_OK;
 }
 

@@ -220,7 +220,8 @@ size_t contract_noalloc_bytes(const ContractPlan *p);
 // CUDA-event record of one more launch in the timing buffer (when timing is
 // on): kind 0-3 DMMA tile shapes, 10 / 11 digit slicing of A / B, 12 digit
 // GEMM, 20 / 21 narrow-output kernels (rows / K), 22 short-K kernel (tasks,
-// tiles, output elements), 30 / 31 Davidson step /
+// tiles, output elements), 23 row-dot kernel (tasks, warps, output
+// elements), 30 / 31 Davidson step /
 // Ritz update, 32 solver step, 40 pair transform; a, b, c describe its
 // size.  Kinds below 30 are contraction work (cpsd_contract_time).
 int timing_begin(double flops, int64_t a, int64_t b, int64_t c, int64_t kind, cudaEvent_t *end);

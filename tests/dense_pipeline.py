@@ -158,3 +158,37 @@ class DenseSystem:
         C1_3 = C1_3 + K("c1_r1iabj", L, J["J3_Wovvo"]) + K("c1_r1Fmi", L, J["J3_Foo"]) + K("c1_r1Fae", L, J["J3_Fvv"])
         w3 = np.sum(L * C1_3)
         return dict(w=np.array([w1, w2, w3]), R2_1=R2_1, R1_2=R1_2, R2_2=R2_2)
+
+    def cisdoo_matrix(self, symR):
+        """CIS(D-infinity) (src/CISdoo.SD.SF/run.f90:25-39, calAR.f90:19-49)
+        as a dense matrix over the packed (R1, R2) coordinates of irrep symR,
+        with each coordinate's spin change (occupied spin 0 -> virtual spin 1
+        counts +1)."""
+        s, sym = self.s, self.s.sym
+        z = np.array([1, 0, 0, 0, 0, 0, 0, 0])
+        MP2t = -self.abij / self.e2
+        Fac = np.diag(self.ev) + K("Fae_r2abij", MP2t, self.abij)
+        Fki = np.diag(self.eo) + K("Fmi_r2abij", MP2t, self.abij)
+        W = self.iabj + K("Wmbej_r2abij", MP2t, self.abij, 2.0)
+        p1 = ([s.popv, s.popo, z, z], (1, 1), symR)
+        p2 = ([s.popv, s.popv, s.popo, s.popo], (0, 0), symR)
+        l1, l2 = s.r1_len(symR), s.r2_len(symR)
+        n = l1 + l2
+        A = np.zeros((n, n))
+        for k in range(n):
+            x = np.zeros(n)
+            x[k] = 1.0
+            R1 = dense.dpd_to_dense(x[:l1], sym, *p1)[:, :, 0, 0]
+            R2 = dense.dpd_to_dense(x[l1:], sym, *p2)
+            C1 = (K("c1_r1Fae", R1, Fac) + K("c1_r1Fmi", R1, Fki) + K("c1_r1iabj", R1, W)
+                  + K("c1_r2abci", R2, self.abci) + K("c1_r2ijka", R2, self.ijka))
+            C2 = self.e2 * R2 + K("c2_r1abci", R1, self.abci) + K("c2_r1ijka", R1, self.ijka)
+            A[:l1, k] = dense.dense_to_dpd(C1[:, :, None, None], sym, *p1)
+            A[l1:, k] = dense.dense_to_dpd(C2, sym, *p2)
+        rows1, _ = dense.dpd_index_lists(sym, *p1)
+        rows2, _ = dense.dpd_index_lists(sym, *p2)
+        dms = np.zeros(n, np.int64)
+        dms[rows1[:, 0]] = self.spin_v[rows1[:, 1]] - self.spin_o[rows1[:, 2]]
+        dms[l1 + rows2[:, 0]] = (self.spin_v[rows2[:, 1]] + self.spin_v[rows2[:, 2]]
+                                 - self.spin_o[rows2[:, 3]] - self.spin_o[rows2[:, 4]])
+        return A, dms

@@ -178,6 +178,19 @@ class Oracle:
         assert rc == 0, rc
         return om[:nroot], R[:rlen], it.value
 
+    def cisdoo(self):
+        """CIS(D-infinity) roots: omega and per root (R1, R2) of its irrep"""
+        s = self.s
+        nroot = s.nroots
+        rlen = sum(int(s.estate_sym[h]) * (s.r1_len(h + 1) + s.r2_len(h + 1)) for h in range(8))
+        om = np.zeros(max(nroot, 1))
+        R = np.zeros(max(rlen, 1))
+        it = I64(0)
+        rc = lib().o_cisdoo_run(ctypes.byref(self.osys), ctypes.byref(self.oint), ctypes.byref(self.par),
+                                ptr(om), ptr(R), ctypes.byref(it))
+        assert rc == 0, rc
+        return om[:nroot], R[:rlen], it.value
+
     def ground(self):
         s = self.s
         l1, l2 = s.r1_len(1), s.r2_len(1)

@@ -126,3 +126,37 @@ def test_intermediates_match_dense():
         if D.ndim == 2:
             D = D[:, :, None, None]
         np.testing.assert_allclose(J[k], dense.dense_to_dpd(D, sym, pops, iops, 1), atol=1e-12, err_msg=k)
+
+
+@pytest.mark.parametrize("nirrep", [1, 4])
+def test_cisdoo_matches_dense_eigenvalues(nirrep):
+    """CIS(D-infinity): the (R1, R2) sigma is not symmetric (Fac, Fki and
+    Wkaci carry the MP2 amplitudes); the oracle's lowest roots are the
+    lowest eigenvalues of the dense operator on the spin-flip sector and
+    each returned vector satisfies the Davidson self-test."""
+    s = synth.System(nmo=10, nocc_a=3, nocc_b=1, nirrep=nirrep, seed=7, roots=2)
+    orc = of.Oracle(s, lowest=1, davidson_conv=10)
+    om, R, it = orc.cisdoo()
+    ds = dp.DenseSystem(s)
+    off = 0
+    k = 0
+    for h in range(8):
+        nr = int(s.estate_sym[h])
+        if nr == 0:
+            continue
+        A, dms = ds.cisdoo_matrix(h + 1)
+        assert np.max(np.abs(A - A.T)) > 1e-6  # the operator is not symmetric
+        sel = np.flatnonzero(dms == 1)
+        ev = np.linalg.eigvals(A[np.ix_(sel, sel)])
+        assert np.max(np.abs(ev.imag)) < 1e-9
+        ev = np.sort(ev.real)
+        n = A.shape[0]
+        for r in range(nr):
+            x = R[off + r * n:off + (r + 1) * n]
+            assert abs(np.linalg.norm(x) - 1) < 1e-10
+            assert np.max(np.abs(A @ x - om[k + r] * x)) < 1e-8
+            assert np.all(x[dms != 1] == 0)
+        np.testing.assert_allclose(om[k:k + nr], ev[:nr], rtol=0, atol=1e-9)
+        off += nr * n
+        k += nr
+    assert k == len(om) and k > 0
