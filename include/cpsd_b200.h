@@ -61,7 +61,8 @@ int cpsd_contract_time(double *ms, int64_t *launches, double *flops, int reset);
  * per element is below (digits+1) K 128^-digits max|a_row| max|b_col|.
  * digits = 0 (default) keeps the FP64 tensor-pipe path everywhere.
  * cpsd_mixed_error returns 1 if a wait in that path timed out since the
- * last reset; cpsd_cis_run, cpsd_ground, cpsd_eecpsd_roots and so
+ * last reset; cpsd_cis_run, cpsd_cisdoo_run, cpsd_ground, cpsd_ground3,
+ * cpsd_eecpsd_roots and so
  * cpsd_pipeline / cpsd_pipeline_batch check it themselves and return
  * CPSD_ETIMEOUT instead of results. */
 int cpsd_set_mixed(int digits, double min_gflop);
@@ -277,6 +278,20 @@ CPSD_KERNEL(Wmbej_r1abci); /* Wmbej_r1abci.f90:3 W(em,bj) += r(f,j) V(fe,bm)    
 CPSD_KERNEL(Wmbej_r1ijka); /* Wmbej_r1ijka.f90:3 W(em,bj) -= r(b,n) V(nm,je)        */
 CPSD_KERNEL(Wmnij_r1ijka); /* Wmnij_r1ijka.f90:3 W(mn,ij) += P(ij) r(e,j) V(mn,ie)  */
 CPSD_KERNEL(Wmnij_r2abij); /* Wmnij_r2abij.f90:1 W(mn,ij) += .5 V(ef,mn) r(ef,ij)   */
+/* the second-order ground state's (src/grCPSd.SF/calL1_VTT.f90, calL2_VTT.f90) */
+CPSD_KERNEL(Wkbij_r1iabj);  /* Wkbij_r1iabj.f90:1  W(ij,kb) -= P(ij) V(ck,bj) r(c,i) */
+CPSD_KERNEL(Wabdj_r1abcd);  /* Wabdj_r1abcd.f90:1  W(ab,dj) += V(ab,dc) r(c,j)       */
+CPSD_KERNEL(Wkbij_r1Uklij); /* Wkbij_r1Uklij.f90:1 W(ij,kb) -= U(kl,ij) r(b,l)       */
+CPSD_KERNEL(Fme_r1abij);    /* Fme_r1abij.f90:1    F(e,m) += r(f,n) V(ef,mn)         */
+CPSD_KERNEL(c1_r2Fme);      /* c1_r2Fme.f90:1      c(a,i) += r(ae,im) F(e,m)         */
+/* the excited-state grCPS(D)'s (src/EE-grCPSd.SF/calEigenCISDoo.f90, calJ.f90, calC_VTTR.f90) */
+CPSD_KERNEL(c1d_l1Wibaj);   /* c1d_l1Wibaj.f90:1 c(a,i) += W(ai,bj) l(b,j) */
+CPSD_KERNEL(c1d_l1fab);     /* c1d_l1fab.f90:1 c(a,i) -= f(b,a) l(b,i) */
+CPSD_KERNEL(c1d_l1fij);     /* c1d_l1fij.f90:1 c(a,i) += f(i,j) l(a,j) */
+CPSD_KERNEL(Fae_r1fia);     /* Fae_r1fia.f90:1 F(a,e) -= f(e,l) r(a,l) */
+CPSD_KERNEL(Fmi_r1fia);     /* Fmi_r1fia.f90:1 F(m,i) += r(d,i) f(d,m) */
+CPSD_KERNEL(Wkbij_r2Fkc);   /* Wkbij_r2Fkc.f90:1 W(ij,kb) -= F(c,k) r(cb,ij) */
+CPSD_KERNEL(Wlkjd_r1abij);  /* Wlkjd_r1abij.f90:1 W(lk,jd) += r(c,j) V(cd,lk) */
 #undef CPSD_KERNEL
 
 /* --------------------------------------------- planner introspection
@@ -376,6 +391,23 @@ void cpsd_params_default(cpsd_params *p);
  * R1 of every requested root (irrep 1 first) into R_dev (device). */
 int cpsd_cis_run(const cpsd_system *s, const cpsd_integrals *I, const cpsd_params *p,
                  double *omega_host, double *R_dev, int64_t *iterations);
+
+/* CIS(D-infinity) (src/CISdoo.SD.SF/run.f90:25-110, calAR.f90:19-49): the
+ * (R1, R2) eigenproblem with the MP2-dressed Fac, Fki and Wkaci; per
+ * requested root omega_host[k] and its unit-norm R1 then R2 (lengths
+ * irpdso(sym,v,o) and idsymsoc(sym,v,v,0,o,o,0) of its irrep) into R_dev
+ * (device), irrep 1 first.  The matrix is not symmetric: the Ritz steps
+ * take the general eigen-solve (cpsd_davidson_stats counts them). */
+int cpsd_cisdoo_run(const cpsd_system *s, const cpsd_integrals *I, const cpsd_params *p,
+                    double *omega_host, double *R_dev, int64_t *iterations);
+
+/* grCPS(D) ground state (src/grCPSd.SF/run.f90): orders k = 1..3 of the
+ * coupled (T1, T2) equations with the MP2-dressed Fli, Fad, Wkaci and their
+ * DIIS loops (solver.f90).  T_dev (device) receives per order T1 (l1 =
+ * irpdso(1,v,o)) then T2 (l2 = idsymsoc(1,v,v,0,o,o,0)); E_host[k-1] =
+ * E^(k+1) of calEcorr.f90; iters[k-1] the DIIS iterations of order k. */
+int cpsd_grcpsd_ground(const cpsd_system *s, const cpsd_integrals *I, const cpsd_params *p, double *T_dev,
+                       double *E_host, int64_t *iters);
 
 /* ground CPS(D) T^(1), T^(2) (src/CPSd.SF/run1.f90, run2.f90); device outputs */
 int cpsd_ground(const cpsd_system *s, const cpsd_integrals *I, const cpsd_params *p,

@@ -137,6 +137,24 @@ int o_Wkbij_r2ijka(o_opt *W, const o_opt *r2, const o_opt *ijka, double f);
 int o_Wkbij_r2abci(o_opt *W, const o_opt *r2, const o_opt *abci, double f);
 int o_Wmbej_r2abij(o_opt *W, const o_opt *r2, const o_opt *abij, double f);
 int o_Wmbej_r1abci(o_opt *W, const o_opt *r1, const o_opt *abci, double f);
+/* second-order ground state kernels (src/lib_cc/Wkbij_r1iabj.f90,
+ * Wabdj_r1abcd.f90, Wkbij_r1Uklij.f90, Fme_r1abij.f90, c1_r2Fme.f90) */
+int o_Wkbij_r1iabj(o_opt *W, const o_opt *r1, const o_opt *iabj, double f);
+int o_Wabdj_r1abcd(o_opt *W, const o_opt *r1, const o_opt *abcd, double f);
+int o_Wkbij_r1Uklij(o_opt *W, const o_opt *r1, const o_opt *U, double f);
+int o_Fme_r1abij(o_opt *F, const o_opt *r1, const o_opt *abij, double f);
+int o_c1_r2Fme(o_opt *c1, const o_opt *r2, const o_opt *F, double f);
+/* excited-state grCPS(D) kernels (src/lib_cc/c1d_l1Wibaj.f90, c1d_l1fab.f90,
+ * c1d_l1fij.f90, Fae_r1fia.f90, Fmi_r1fia.f90, Wkbij_r2Fkc.f90, Wlkjd_r1abij.f90) */
+int o_c1d_l1Wibaj(o_opt *c1, const o_opt *l1, const o_opt *W, double f);
+int o_c1d_l1fab(o_opt *c1, const o_opt *l1, const o_opt *F, double f);
+int o_c1d_l1fij(o_opt *c1, const o_opt *l1, const o_opt *F, double f);
+int o_Fae_r1fia(o_opt *c1, const o_opt *r1, const o_opt *F, double f);
+int o_Fmi_r1fia(o_opt *c1, const o_opt *r1, const o_opt *F, double f);
+int o_Wkbij_r2Fkc(o_opt *c1, const o_opt *r2, const o_opt *F, double f);
+int o_Wlkjd_r1abij(o_opt *c1, const o_opt *r1, const o_opt *V, double f);
+/* effectT2 (src/lib_cc/effectT2.f90:47-140), types 1 and 2 */
+int o_effectT2(o_opt *t2, const o_opt *x, const o_opt *y, double f, int type);
 int o_Wmbej_r1ijka(o_opt *W, const o_opt *r1, const o_opt *ijka, double f);
 int o_Wmnij_r1ijka(o_opt *W, const o_opt *r1, const o_opt *ijka, double f);
 int o_Wmnij_r2abij(o_opt *W, const o_opt *r2, const o_opt *abij, double f);
@@ -195,6 +213,13 @@ int o_cpsd_ground(const o_system *s, const o_integrals *I, const o_params *p,
                   double *T2_1, double *T1_2, double *T2_2, double *E2, double *E3,
                   i64 *diis_iters);
 /* third order: T1^(3), T2^(3), E^(4) (src/CPSd.SF/run3.f90) */
+/* second-order-dressed ground state grCPS(D) (src/grCPSd.SF/run.f90): for
+ * order k = 1, 2, 3 the coupled (T1, T2)^(k) of solver.f90 with their DIIS
+ * loop; T receives per order T1 (l1) then T2 (l2) of irrep 1, E[k-1] the
+ * energy E^(k+1) of calEcorr.f90 at convergence, iters[k-1] the DIIS
+ * iterations */
+int o_grcpsd_ground(const o_system *s, const o_integrals *I, const o_params *p, double *T, double *E,
+                    i64 *iters);
 int o_cpsd_ground3(const o_system *s, const o_integrals *I, const o_params *p,
                    const double *T2_1, const double *T1_2, const double *T2_2,
                    double *T1_3, double *T2_3, double *E4, i64 *diis_iters);

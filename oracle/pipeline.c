@@ -342,6 +342,239 @@ out:
     return rc;
 }
 
+/* ---------------- grCPS(D) ground state (src/grCPSd.SF) ----------------
+ * Intermediates (run.f90:27-47): MP2t = denomT2(abij), Fli = -Fmi_r2abij(MP2t),
+ * Fad = -Fae_r2abij(MP2t), Wkaci = iabj + 2 Wmbej_r2abij(MP2t).
+ * Order k solves (solver.f90:1-77), from R = C^(k):
+ *   T1 = denomT1(R1), T2 = denomT2(R2), DIIS on (T1, T2),
+ *   E = calEcorr(k), R1 = C1 + calA0R1(T), R2 = C2 + calA0R2(T1)
+ * with calA0R1 = Wkaci T1 - Fli T1 + Fad T1 + c1_r2ijka(T2) + c1_r2abci(T2)
+ * (calA0R1.f90:19-30) and calA0R2 = c2_r1ijka(T1) + c2_r1abci(T1)
+ * (calA0R2.f90:13-19).  Constants: C^(1) = (0, abij) (run1.f90:17-19);
+ * C^(2) = (0, calA1R2(T2^(1))) (run2.f90, calA1R2.f90:30-37); C^(3) =
+ * (calA2R1(T1^(1)) + calL1_VTT(T^(1)), calA1R2(T2^(2)) + calL2_VTT(T^(1)))
+ * (run3.f90, calC1.f90, calC2.f90). */
+typedef struct {
+    const o_system *s;
+    const ints_t *v;
+    o_opt fli, fad, wk;
+    i64 l1, l2;
+} gr_ctx;
+
+/* <ab,ij|[V,T2]|0> = c2_r2Wmbej + c2_r2Wmnij + c2_r2abcd (calA1R2.f90:30-37) */
+static int gr_A1R2(const gr_ctx *g, o_opt *C2, const double *T2)
+{
+    const i64 *o = g->s->popo, *V = g->s->popv;
+    o_opt t2;
+    o_opt_view(&t2, V, V, o, o, 0, 0, 1, (double *)T2);
+    int rc = o_c2_r2Wmbej(C2, &t2, &g->v->iabj, 1.0);
+    if (rc == O_OK) rc = o_c2_r2Wmnij(C2, &t2, &g->v->ijkl, 1.0);
+    if (rc == O_OK) rc = o_c2_r2abcd(C2, &t2, &g->v->abcd, 1.0);
+    return rc;
+}
+
+/* calA2R1.f90:27-47: C1 -= (Wkaci - iabj) T1 + Fli T1 - Fad T1, i.e.
+ * c1_r1iabj(Wkaci - iabj, -1), c1_r1Fmi(Fli, +1), c1_r1Fae(Fad, +1).  The
+ * reference forms Wkaci - iabj in place and adds iabj back afterwards, so
+ * Wkaci leaves rounded as (Wkaci - iabj) + iabj; so does this. */
+static int gr_A2R1(gr_ctx *g, o_opt *C1, const double *T1)
+{
+    const i64 *o = g->s->popo, *V = g->s->popv;
+    o_opt t1;
+    o_opt_view(&t1, V, o, Z, Z, 1, 1, 1, (double *)T1);
+    for (i64 k = 0; k < g->wk.len; k++) g->wk.arr[k] -= g->v->iabj.arr[k];
+    int rc = o_c1_r1iabj(C1, &t1, &g->wk, -1.0);
+    for (i64 k = 0; k < g->wk.len; k++) g->wk.arr[k] += g->v->iabj.arr[k];
+    if (rc == O_OK) rc = o_c1_r1Fmi(C1, &t1, &g->fli, 1.0);
+    if (rc == O_OK) rc = o_c1_r1Fae(C1, &t1, &g->fad, 1.0);
+    return rc;
+}
+
+/* calL1_VTT.f90:30-75: L1 += Gli t(a,l) - Gad t(d,i) + Gld t(da,li) with
+ * Gli = -Fmi_r1ijka(T1) - Fmi_r2abij(T2), Gad = -Fae_r1abci(T1) -
+ * Fae_r2abij(T2), Gld = Fme_r1abij(T1) */
+static int gr_L1_VTT(const gr_ctx *g, o_opt *L1, const double *T1, const double *T2)
+{
+    const i64 *o = g->s->popo, *V = g->s->popv;
+    o_opt t1, t2, gli, gad, gld;
+    o_opt_view(&t1, V, o, Z, Z, 1, 1, 1, (double *)T1);
+    o_opt_view(&t2, V, V, o, o, 0, 0, 1, (double *)T2);
+    double *a = zalloc(o_irpdso(1, o, o, 1)), *b = zalloc(o_irpdso(1, V, V, 1)), *c = zalloc(g->l1);
+    o_opt_view(&gli, o, o, Z, Z, 1, 1, 1, a);
+    o_opt_view(&gad, V, V, Z, Z, 1, 1, 1, b);
+    o_opt_view(&gld, V, o, Z, Z, 1, 1, 1, c);
+    int rc = o_Fmi_r1ijka(&gli, &t1, &g->v->ijka, -1.0);
+    if (rc == O_OK) rc = o_Fmi_r2abij(&gli, &t2, &g->v->abij, -1.0);
+    if (rc == O_OK) rc = o_Fae_r1abci(&gad, &t1, &g->v->abci, -1.0);
+    if (rc == O_OK) rc = o_Fae_r2abij(&gad, &t2, &g->v->abij, -1.0);
+    if (rc == O_OK) rc = o_Fme_r1abij(&gld, &t1, &g->v->abij, 1.0);
+    if (rc == O_OK) rc = o_c1_r1Fmi(L1, &t1, &gli, -1.0);
+    if (rc == O_OK) rc = o_c1_r1Fae(L1, &t1, &gad, -1.0);
+    if (rc == O_OK) rc = o_c1_r2Fme(L1, &t2, &gld, 1.0);
+    free(a); free(b); free(c);
+    return rc;
+}
+
+/* calL2_VTT.f90:50-163, the eight terms of 0.5 <ab,ij|[[V,T],T]|0> */
+static int gr_L2_VTT(const gr_ctx *g, o_opt *L2, const double *T1, const double *T2)
+{
+    const o_system *s = g->s;
+    const i64 *o = s->popo, *V = s->popv;
+    const ints_t *v = g->v;
+    o_opt t1, t2, w;
+    o_opt_view(&t1, V, o, Z, Z, 1, 1, 1, (double *)T1);
+    o_opt_view(&t2, V, V, o, o, 0, 0, 1, (double *)T2);
+    i64 n = v->abci.len;
+    if (v->ijka.len > n) n = v->ijka.len;
+    if (v->iabj.len > n) n = v->iabj.len;
+    if (v->ijkl.len > n) n = v->ijkl.len;
+    double *buf = zalloc(n);
+#define GR_TMP(P0, P1, P2, P3, I0, I1)                                   \
+    do {                                                                \
+        o_opt_view(&w, P0, P1, P2, P3, I0, I1, 1, buf);                 \
+        memset(buf, 0, sizeof(double) * (size_t)w.len);                 \
+    } while (0)
+    int rc = O_OK;
+    /* -PijPab{V(kb,cj) t(c,i) t(a,k)}: W(ij,kb) = Wkbij_r1iabj(T1); c2_r1ijka(W, -1) */
+    GR_TMP(o, o, o, V, 0, 1);
+    rc = o_Wkbij_r1iabj(&w, &t1, &v->iabj, 1.0);
+    if (rc == O_OK) rc = o_c2_r1ijka(L2, &t1, &w, -1.0);
+    /* 0.5 Pij{V(ab,cd) t(c,i) t(d,j)}: W(ab,dj) = Wabdj_r1abcd(T1); c2_r1abci(W, 0.5) */
+    if (rc == O_OK) {
+        GR_TMP(V, V, V, o, 0, 1);
+        rc = o_Wabdj_r1abcd(&w, &t1, &v->abcd, 1.0);
+    }
+    if (rc == O_OK) rc = o_c2_r1abci(L2, &t1, &w, 0.5);
+    /* 0.5 Pab{V(kl,ij) t(a,k) t(b,l)}: W(ij,kb) = Wkbij_r1Uklij(T1); c2_r1ijka(W, 0.5) */
+    if (rc == O_OK) {
+        GR_TMP(o, o, o, V, 0, 1);
+        rc = o_Wkbij_r1Uklij(&w, &t1, &v->ijkl, 1.0);
+    }
+    if (rc == O_OK) rc = o_c2_r1ijka(L2, &t1, &w, 0.5);
+    /* -Pij{Gli t(ab,lj)}, Gli = Fmi_r1ijka(T1) + Fmi_r2abij(T2) */
+    if (rc == O_OK) {
+        GR_TMP(o, o, Z, Z, 1, 1);
+        rc = o_Fmi_r1ijka(&w, &t1, &v->ijka, 1.0);
+    }
+    if (rc == O_OK) rc = o_Fmi_r2abij(&w, &t2, &v->abij, 1.0);
+    if (rc == O_OK) rc = o_c2_r2Fmi(L2, &t2, &w, 1.0);
+    /* Pab{Gad t(db,ij)}, Gad = Fae_r1abci(T1) + Fae_r2abij(T2) */
+    if (rc == O_OK) {
+        GR_TMP(V, V, Z, Z, 1, 1);
+        rc = o_Fae_r1abci(&w, &t1, &v->abci, 1.0);
+    }
+    if (rc == O_OK) rc = o_Fae_r2abij(&w, &t2, &v->abij, 1.0);
+    if (rc == O_OK) rc = o_c2_r2Fae(L2, &t2, &w, 1.0);
+    /* PijPab{Wkbcj t(ac,ik)}, W = Wmbej_r1ijka(T1) + Wmbej_r1abci(T1) + Wmbej_r2abij(T2) */
+    if (rc == O_OK) {
+        GR_TMP(V, o, V, o, 1, 1);
+        rc = o_Wmbej_r1ijka(&w, &t1, &v->ijka, 1.0);
+    }
+    if (rc == O_OK) rc = o_Wmbej_r1abci(&w, &t1, &v->abci, 1.0);
+    if (rc == O_OK) rc = o_Wmbej_r2abij(&w, &t2, &v->abij, 1.0);
+    if (rc == O_OK) rc = o_c2_r2Wmbej(L2, &t2, &w, 1.0);
+    /* -0.5 Pab{V(kb,cd) t(cd,ij) t(a,k)}: W(ij,kb) = Wkbij_r2abci(T2); c2_r1ijka(W, 1) */
+    if (rc == O_OK) {
+        GR_TMP(o, o, o, V, 0, 1);
+        rc = o_Wkbij_r2abci(&w, &t2, &v->abci, 1.0);
+    }
+    if (rc == O_OK) rc = o_c2_r1ijka(L2, &t1, &w, 1.0);
+    /* Wklij t(ab,kl), Wklij = Wmnij_r1ijka(T1, 0.5) + Wmnij_r2abij(T2, 0.5); c2_r2Wmnij(W, 2) */
+    if (rc == O_OK) {
+        GR_TMP(o, o, o, o, 0, 0);
+        rc = o_Wmnij_r1ijka(&w, &t1, &v->ijka, 0.5);
+    }
+    if (rc == O_OK) rc = o_Wmnij_r2abij(&w, &t2, &v->abij, 0.5);
+    if (rc == O_OK) rc = o_c2_r2Wmnij(L2, &t2, &w, 2.0);
+#undef GR_TMP
+    free(buf);
+    return rc;
+}
+
+int o_grcpsd_ground(const o_system *s, const o_integrals *I, const o_params *p, double *T, double *E,
+                    i64 *iters)
+{
+    ints_t v;
+    ints_view(s, I, &v);
+    const i64 *o = s->popo, *V = s->popv;
+    const i64 l1 = o_irpdso(1, V, o, 1), l2 = o_idsymsoc(1, V, V, 0, o, o, 0), lt = l1 + l2;
+    gr_ctx g;
+    g.s = s;
+    g.v = &v;
+    g.l1 = l1;
+    g.l2 = l2;
+    double *mp2 = zalloc(l2), *fo = zalloc(o_irpdso(1, o, o, 1)), *fv = zalloc(o_irpdso(1, V, V, 1));
+    double *wk = zalloc(v.iabj.len), *C = zalloc(lt), *R = zalloc(lt), *tau = zalloc(l2);
+    o_opt mp2t, c1, c2, r1, r2, t1, t2, ta, x1, y1;
+    o_opt_view(&mp2t, V, V, o, o, 0, 0, 1, mp2);
+    o_opt_view(&g.fli, o, o, Z, Z, 1, 1, 1, fo);
+    o_opt_view(&g.fad, V, V, Z, Z, 1, 1, 1, fv);
+    o_opt_view(&g.wk, V, o, V, o, 1, 1, 1, wk);
+    o_opt_view(&c1, V, o, Z, Z, 1, 1, 1, C);
+    o_opt_view(&c2, V, V, o, o, 0, 0, 1, C + l1);
+    o_opt_view(&r1, V, o, Z, Z, 1, 1, 1, R);
+    o_opt_view(&r2, V, V, o, o, 0, 0, 1, R + l1);
+    o_opt_view(&ta, V, V, o, o, 0, 0, 1, tau);
+    o_denomT2(mp2, I->abij, I->eorb, V, o, 1, 0);
+    memcpy(wk, I->iabj, sizeof(double) * (size_t)v.iabj.len);
+    int rc = o_Fmi_r2abij(&g.fli, &mp2t, &v.abij, -1.0);
+    if (rc == O_OK) rc = o_Fae_r2abij(&g.fad, &mp2t, &v.abij, -1.0);
+    if (rc == O_OK) rc = o_Wmbej_r2abij(&g.wk, &mp2t, &v.abij, 2.0);
+    for (int k = 1; k <= 3 && rc == O_OK; k++) {
+        double *Tk = T + (k - 1) * lt;
+        o_opt_view(&t1, V, o, Z, Z, 1, 1, 1, Tk);
+        o_opt_view(&t2, V, V, o, o, 0, 0, 1, Tk + l1);
+        /* the constant C^(k) */
+        memset(C, 0, sizeof(double) * (size_t)lt);
+        if (k == 1) memcpy(C + l1, I->abij, sizeof(double) * (size_t)l2);
+        if (k >= 2) rc = gr_A1R2(&g, &c2, T + (k - 2) * lt + l1);
+        if (k == 3 && rc == O_OK) rc = gr_A2R1(&g, &c1, T);
+        if (k == 3 && rc == O_OK) rc = gr_L1_VTT(&g, &c1, T, T + l1);
+        if (k == 3 && rc == O_OK) rc = gr_L2_VTT(&g, &c2, T, T + l1);
+        if (rc != O_OK) break;
+        /* solver.f90:24-73 */
+        memcpy(R, C, sizeof(double) * (size_t)lt);
+        o_diis dst;
+        o_diis_init(&dst, lt, p->diis_dim);
+        i64 iter = 0;
+        double Ek = 0.0;
+        for (;;) {
+            iter++;
+            o_denomT1(Tk, R, I->eorb, V, o, 1);
+            o_denomT2(Tk + l1, R + l1, I->eorb, V, o, 1, 0);
+            double err = o_diis_step(&dst, iter, Tk);
+            /* calEcorr.f90:21-52 */
+            memcpy(tau, Tk + l1, sizeof(double) * (size_t)l2);
+            if (k == 2) {
+                o_opt_view(&x1, V, o, Z, Z, 1, 1, 1, T);
+                rc = o_effectT2(&ta, &x1, &x1, 1.0, 1);
+            } else if (k == 3) {
+                o_opt_view(&x1, V, o, Z, Z, 1, 1, 1, T + lt);
+                o_opt_view(&y1, V, o, Z, Z, 1, 1, 1, T);
+                rc = o_effectT2(&ta, &x1, &y1, 1.0, 2);
+            }
+            if (rc != O_OK) break;
+            Ek = o_ddot(l2, tau, I->abij);
+            if (iter > 1 && fabs(err) < p->diis_max_err) break;
+            if (iter > p->diis_cyc) break;
+            memcpy(R, C, sizeof(double) * (size_t)lt);
+            rc = o_c1_r1iabj(&r1, &t1, &g.wk, 1.0); /* calA0R1 */
+            if (rc == O_OK) rc = o_c1_r1Fmi(&r1, &t1, &g.fli, -1.0);
+            if (rc == O_OK) rc = o_c1_r1Fae(&r1, &t1, &g.fad, -1.0);
+            if (rc == O_OK) rc = o_c1_r2ijka(&r1, &t2, &v.ijka, 1.0);
+            if (rc == O_OK) rc = o_c1_r2abci(&r1, &t2, &v.abci, 1.0);
+            if (rc == O_OK) rc = o_c2_r1ijka(&r2, &t1, &v.ijka, 1.0); /* calA0R2 */
+            if (rc == O_OK) rc = o_c2_r1abci(&r2, &t1, &v.abci, 1.0);
+            if (rc != O_OK) break;
+        }
+        o_diis_free(&dst);
+        E[k - 1] = Ek;
+        if (iters) iters[k - 1] = iter;
+    }
+    free(mp2); free(fo); free(fv); free(wk); free(C); free(R); free(tau);
+    return rc;
+}
+
 /* ---------------- J^(2), J^(3) (src/EE-CPSd.SF/calJ.f90) ---------------- */
 int o_calJ(const o_system *s, const o_integrals *I, const double *T2_1,
            const double *T1_2, const double *T2_2, o_jints *J)

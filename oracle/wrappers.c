@@ -344,3 +344,68 @@ int o_Wmnij_r2abij(o_opt *W, const o_opt *r2, const o_opt *abij, double f)
 { return o_vv2v_444(abij, r2, W, r2->d.iop[0] == 0 ? f : 0.5 * f, "efmn", "efij", "mnij", 0); }
 
 const i64 *o_zorb(void) { return ZORB; }
+
+/* ---- kernels of the second-order ground state (src/grCPSd.SF/calL1_VTT.f90,
+ * calL2_VTT.f90) ---- */
+
+/* Wkbij_r1iabj.f90:1-16: W(ij,kb) -= f*P(ij){V(ck,bj)*r(c,i)} */
+int o_Wkbij_r1iabj(o_opt *W, const o_opt *r1, const o_opt *iabj, double f)
+{ return o_vv2v_424(iabj, r1, W, -f, "ckbj", "ci", "ijkb", 1); }
+
+/* Wabdj_r1abcd.f90:1-18 (incore branch): W(ab,dj) += f*V(ab,dc)*r(c,j) */
+int o_Wabdj_r1abcd(o_opt *W, const o_opt *r1, const o_opt *abcd, double f)
+{ return o_vv2v_424(abcd, r1, W, f, "abdc", "cj", "abdj", 0); }
+
+/* Wkbij_r1Uklij.f90:1-16: W(ij,kb) -= f*U(kl,ij)*r(b,l) */
+int o_Wkbij_r1Uklij(o_opt *W, const o_opt *r1, const o_opt *U, double f)
+{ return o_vv2v_424(U, r1, W, -f, "klij", "bl", "ijkb", 0); }
+
+/* Fme_r1abij.f90:1-16: F(e,m) += f*r(f,n)*V(ef,mn) */
+int o_Fme_r1abij(o_opt *F, const o_opt *r1, const o_opt *abij, double f)
+{ return o_vv2v_422(abij, r1, F, f, "efmn", "fn", "em"); }
+
+/* c1_r2Fme.f90:1-16: c(a,i) += f*r(ae,im)*F(e,m) */
+int o_c1_r2Fme(o_opt *c1, const o_opt *r2, const o_opt *F, double f)
+{ return o_vv2v_422(r2, F, c1, f, "aeim", "em", "ai"); }
+
+/* p_effectT2 (effectT2.f90:47-140) types 1 and 2 on an antisymmetric
+ * t(ab,ij): type 1 t += f [x(a,i) x(b,j) - x(a,j) x(b,i)] (x = y),
+ * type 2 t += f P(ab) P(ij) {x(a,i) y(b,j)}.  Both are the outer product
+ * antisymmetrised in both pairs (vv2v_224 with anti 3); for x = y the
+ * double antisymmetrisation counts each term twice, hence f / 2. */
+int o_effectT2(o_opt *t2, const o_opt *x, const o_opt *y, double f, int type)
+{
+    if (type != 1 && type != 2) return O_EARG;
+    return o_vv2v_224(x, y, t2, type == 1 ? 0.5 * f : f, "ai", "bj", "abij", 3);
+}
+
+/* ---- kernels of the excited-state grCPS(D) (src/EE-grCPSd.SF: the left
+ * vector of calEigenCISDoo.f90, calJ.f90, calC_VTTR.f90) ---- */
+
+/* c1d_l1Wibaj.f90:1-16: c(a,i) += W(ai,bj) l(b,j) */
+int o_c1d_l1Wibaj(o_opt *c1, const o_opt *l1, const o_opt *W, double f)
+{ return o_vv2v_422(W, l1, c1, f, "aibj", "bj", "ai"); }
+
+/* c1d_l1fab.f90:1-16: c(a,i) -= f(b,a) l(b,i) */
+int o_c1d_l1fab(o_opt *c1, const o_opt *l1, const o_opt *F, double f)
+{ return o_vv2v_222(F, l1, c1, -f, "ba", "bi", "ai"); }
+
+/* c1d_l1fij.f90:1-16: c(a,i) += f(i,j) l(a,j) */
+int o_c1d_l1fij(o_opt *c1, const o_opt *l1, const o_opt *F, double f)
+{ return o_vv2v_222(l1, F, c1, f, "aj", "ij", "ai"); }
+
+/* Fae_r1fia.f90:1-16: F(a,e) -= f(e,l) r(a,l) */
+int o_Fae_r1fia(o_opt *c1, const o_opt *r1, const o_opt *F, double f)
+{ return o_vv2v_222(r1, F, c1, -f, "al", "el", "ae"); }
+
+/* Fmi_r1fia.f90:1-16: F(m,i) += r(d,i) f(d,m) */
+int o_Fmi_r1fia(o_opt *c1, const o_opt *r1, const o_opt *F, double f)
+{ return o_vv2v_222(F, r1, c1, f, "dm", "di", "mi"); }
+
+/* Wkbij_r2Fkc.f90:1-16: W(ij,kb) -= F(c,k) r(cb,ij) */
+int o_Wkbij_r2Fkc(o_opt *c1, const o_opt *r2, const o_opt *F, double f)
+{ return o_vv2v_424(r2, F, c1, -f, "cbij", "ck", "ijkb", 0); }
+
+/* Wlkjd_r1abij.f90:1-16: W(lk,jd) += r(c,j) V(cd,lk) */
+int o_Wlkjd_r1abij(o_opt *c1, const o_opt *r1, const o_opt *V, double f)
+{ return o_vv2v_424(V, r1, c1, f, "cdlk", "cj", "lkjd", 0); }

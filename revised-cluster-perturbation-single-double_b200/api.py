@@ -265,6 +265,19 @@ def cis_run(s, sysc, ints, par):
     return om[:n], R[:rlen], it.value
 
 
+def cisdoo_run(s, sysc, ints, par):
+    """CIS(D-infinity): omega and per root (R1, R2) of its irrep (device)"""
+    import torch
+    n = s.nroots
+    rlen = sum(int(s.estate_sym[h]) * (s.r1_len(h + 1) + s.r2_len(h + 1)) for h in range(8))
+    om = np.zeros(max(n, 1))
+    R = torch.zeros(max(rlen, 1), dtype=torch.float64, device="cuda")
+    it = I64()
+    check(lib().cpsd_cisdoo_run(ctypes.byref(sysc), ctypes.byref(ints.struct), ctypes.byref(par),
+                                om.ctypes.data_as(ctypes.c_void_p), dptr(R), ctypes.byref(it)), "cpsd_cisdoo_run")
+    return om[:n], R[:rlen], it.value
+
+
 def ground(s, sysc, ints, par):
     import torch
     l1, l2 = s.r1_len(1), s.r2_len(1)
@@ -276,6 +289,19 @@ def ground(s, sysc, ints, par):
                             dptr(T1_2), dptr(T2_2), ctypes.byref(E2), ctypes.byref(E3), ctypes.byref(it)),
           "cpsd_ground")
     return dict(T2_1=T2_1, T1_2=T1_2, T2_2=T2_2, E2=E2.value, E3=E3.value, iters=it.value)
+
+
+def grcpsd_ground(s, sysc, ints, par):
+    """grCPS(D) ground state: per order (T1, T2) on the device, E^(2..4), DIIS iterations"""
+    import torch
+    l1, l2 = s.r1_len(1), s.r2_len(1)
+    T = torch.zeros(3 * (l1 + l2), dtype=torch.float64, device="cuda")
+    E = np.zeros(3)
+    it = (I64 * 3)()
+    check(lib().cpsd_grcpsd_ground(ctypes.byref(sysc), ctypes.byref(ints.struct), ctypes.byref(par), dptr(T),
+                                   E.ctypes.data_as(ctypes.c_void_p), it), "cpsd_grcpsd_ground")
+    T = T.view(3, l1 + l2)
+    return dict(T1=[T[k, :l1] for k in range(3)], T2=[T[k, l1:] for k in range(3)], E=E, iters=list(it))
 
 
 def ground3(s, sysc, ints, par, g):

@@ -268,30 +268,26 @@ int make_guess(const Sys &S, const std::vector<double> &eorb, const cpsd_params 
     return CPSD_OK;
 }
 
-// Davidson (src/lib_cc/mod_davidson.f90:40-561) for one irrep; fileEV holds
-// the guess records on entry and the roots on exit (device)
-int davidson(const Sys &S, const Ints &I, const cpsd_params *p, i64 sym, i64 nroot, double *fileEV,
+// Davidson (src/lib_cc/mod_davidson.f90:40-561) over vectors of length n:
+// fileEV holds the guess records on entry and the roots on exit (device),
+// diag the preconditioner's diagonal (device, n), sigma(R, sR, AR, sAR, nb)
+// the product AR = A R for nb vectors sR / sAR elements apart
+using SigmaFn = std::function<int(const double *, i64, double *, i64, i64)>;
+int davidson(const cpsd_params *p, i64 n, i64 nroot, double *fileEV, const double *diag, const SigmaFn &sigma,
              i64 *iters, double *max_resid) {
     ScratchScope sc;
-    const i64 n = irpdso(sym, S.popv, S.popo, 1);
     const i64 D = p->davidson_dim;
     if (D > DAV_MAXD) return set_error(CPSD_EARG, "davidson_dim above 32");
     if (nroot >= D) return set_error(CPSD_EARG, "too many roots for davidson_dim");
     DavBuffers b;
-    double *diag;
-    CPSD_TRY(scratch(n, &diag));
     for (int k = 0; k < 2; k++) {
         CPSD_TRY(scratch(D * n, &b.B[k]));
         CPSD_TRY(scratch(D * n, &b.AB[k]));
     }
     CPSD_TRY(scratch(nroot * n, &b.w0));  // one slice per root
     CPSD_TRY(scratch(nroot * n, &b.w1));
-    b.diag = diag;
+    b.diag = (double *)diag;
     b.fileEV = fileEV;
-    Desc d = make_desc(S.popv, S.popo, ZORB, ZORB, 1, 1, sym);
-    const EnergyPlan *ep;
-    CPSD_TRY(plan_energy(d, "vozz", &ep));
-    CPSD_TRY(launch_energy(ep, 0, I.eorb, nullptr, diag));  // Eorb_diff1 (OED1)
     DavState hs;
     memset(&hs, 0, sizeof hs);
     hs.D = (int)D;
@@ -308,7 +304,7 @@ int davidson(const Sys &S, const Ints &I, const cpsd_params *p, i64 sym, i64 nro
     CPSD_TRY(cuda_check(cudaMemcpy2DAsync(b.B[0], n * sizeof(double), fileEV + 1, (n + 1) * sizeof(double),
                                           n * sizeof(double), nroot, cudaMemcpyDeviceToDevice, stream()),
                         "guess copy"));
-    CPSD_TRY(cis_sigma(S, I, sym, b.B[0], n, b.AB[0], n, nroot));
+    CPSD_TRY(sigma(b.B[0], n, b.AB[0], n, nroot));
     CPSD_TRY(dav_init_launch(st, b));
     // device-driven iterations: every step stages its new vectors (zero
     // padded to nroot), one sigma launch of fixed size, the Ritz update puts
@@ -325,7 +321,7 @@ int davidson(const Sys &S, const Ints &I, const cpsd_params *p, i64 sym, i64 nro
         CPSD_TRY(dav_step_launch(st, b));
         CPSD_TRY(th.mark(it));
         if (((volatile int *)mb)[0] == 0) break;
-        CPSD_TRY(cis_sigma(S, I, sym, b.W, n, b.AW, n, nroot));
+        CPSD_TRY(sigma(b.W, n, b.AW, n, nroot));
         CPSD_TRY(dav_abar_launch(st, b));
         CPSD_TRY(th.wait(it));
     }
@@ -338,7 +334,7 @@ int davidson(const Sys &S, const Ints &I, const cpsd_params *p, i64 sym, i64 nro
     ctx().dav_imag_warnings += hst->warn_imag;
     if (hst->eig_fail) return set_error(CPSD_ENUM, "Davidson: QR iteration on the Ritz matrix did not converge");
     // eigen test of the converged roots (mod_davidson.f90:525-542)
-    CPSD_TRY(cis_sigma(S, I, sym, fileEV + 1, n + 1, b.AB[0], n, nroot));
+    CPSD_TRY(sigma(fileEV + 1, n + 1, b.AB[0], n, nroot));
     CPSD_TRY(dav_final_launch(st, b));
     double mr;
     CPSD_TRY(read_back(&mr, &st->max_resid, sizeof(double)));
@@ -391,9 +387,17 @@ int cpsd_cis_run(const cpsd_system *s, const cpsd_integrals *I, const cpsd_param
         CPSD_TRY(cuda_check(cudaMemcpyAsync(fileEV, rec.data(), sizeof(double) * rec.size(), cudaMemcpyHostToDevice,
                                             stream()),
                             "guess upload"));
+        double *diag;
+        CPSD_TRY(scratch(n, &diag));
+        const EnergyPlan *ep;
+        CPSD_TRY(plan_energy(make_desc(S.popv, S.popo, ZORB, ZORB, 1, 1, sym), "vozz", &ep));
+        CPSD_TRY(launch_energy(ep, 0, X.eorb, nullptr, diag));  // Eorb_diff1 (OED1)
+        SigmaFn sig = [&](const double *R, i64 sR, double *AR, i64 sAR, i64 nb) {
+            return cis_sigma(S, X, sym, R, sR, AR, sAR, nb);
+        };
         i64 it = 0;
         double mr = 0;
-        CPSD_TRY(davidson(S, X, p, sym, nroot, fileEV, &it, &mr));
+        CPSD_TRY(davidson(p, n, nroot, fileEV, diag, sig, &it, &mr));
         itsum += it;
         CPSD_TRY(read_back(rec.data(), fileEV, sizeof(double) * rec.size()));
         for (i64 k = 0; k < nroot; k++) omega_host[kroot + k] = rec[k * (n + 1)];
@@ -406,6 +410,117 @@ int cpsd_cis_run(const cpsd_system *s, const cpsd_integrals *I, const cpsd_param
     }
     if (iterations) *iterations = itsum;
     CPSD_TRY(cuda_check(cudaStreamSynchronize(stream()), "cis sync"));
+    return digit_error_check();
+}
+
+// CIS(D-infinity) (src/CISdoo.SD.SF/run.f90:25-110): MP2t = denomT2(abij),
+// Fac = diag(e_v) + Fae_r2abij(MP2t), Fki = diag(e_o) + Fmi_r2abij(MP2t),
+// Wkaci = iabj + 2 Wmbej_r2abij(MP2t), then per irrep a Davidson over
+// (R1, R2) with the sigma of calAR.f90:19-49 and the diagonal (OED1, OED2);
+// the guesses are the singles' records with a zero R2.  A is not symmetric:
+// the Ritz step takes the general eigen-solve.
+int cpsd_cisdoo_run(const cpsd_system *s, const cpsd_integrals *I, const cpsd_params *p, double *omega_host,
+                    double *R_dev, int64_t *iterations) {
+    Sys S;
+    CPSD_TRY(make_sys(s, &S));
+    Ints X = make_ints(S, I);
+    IntegralScope keep(I);
+    const i64 *o = S.popo, *v = S.popv;
+    i64 ne = 0;
+    for (int r = 0; r < 8; r++) ne += o[r] + v[r];
+    std::vector<double> eorb((size_t)ne);
+    CPSD_TRY(read_back(eorb.data(), I->eorb, sizeof(double) * (size_t)ne));
+    ScratchScope sc;
+    // putDiagFock (src/lib_cc/putDiagFock.f90:6-56): e_p on the diagonal of
+    // each irrep's (pop, pop) block; eorb = occupied of all irreps, then virtual
+    auto diag_fock = [&](const i64 *pop, i64 e0) {
+        i64 len = 0;
+        for (int h = 0; h < 8; h++) len += pop[h] * pop[h];
+        std::vector<double> f((size_t)len, 0.0);
+        i64 off = 0;
+        for (i64 h = 0; h < S.nirrep; h++) {
+            for (i64 k = 0; k < pop[h]; k++) f[(size_t)(off + k * pop[h] + k)] = eorb[(size_t)(e0 + k)];
+            off += pop[h] * pop[h];
+            e0 += pop[h];
+        }
+        return f;
+    };
+    i64 nocc = 0;
+    for (int h = 0; h < 8; h++) nocc += o[h];
+    const std::vector<double> hfa = diag_fock(v, nocc), hfk = diag_fock(o, 0);
+    const i64 l2g = idsymsoc(1, v, v, 0, o, o, 0);
+    double *mp2, *fa, *fk, *wka;
+    CPSD_TRY(scratch(l2g, &mp2));
+    CPSD_TRY(scratch((i64)hfa.size(), &fa));
+    CPSD_TRY(scratch((i64)hfk.size(), &fk));
+    CPSD_TRY(scratch(X.iabj.len(), &wka));
+    CPSD_TRY(cuda_check(cudaMemcpyAsync(fa, hfa.data(), sizeof(double) * hfa.size(), cudaMemcpyHostToDevice, stream()),
+                        "Fac upload"));
+    CPSD_TRY(cuda_check(cudaMemcpyAsync(fk, hfk.data(), sizeof(double) * hfk.size(), cudaMemcpyHostToDevice, stream()),
+                        "Fki upload"));
+    CPSD_TRY(launch_copy(wka, X.iabj.arr, X.iabj.len()));
+    const EnergyPlan *e2g;
+    CPSD_TRY(plan_energy(make_desc(v, v, o, o, 0, 0, 1), "vvoo", &e2g));
+    CPSD_TRY(launch_energy(e2g, 2, X.eorb, I->abij, mp2));  // MP2t = <ab||ij> / (ei+ej-ea-eb)
+    Ten mp2t = ten(v, v, o, o, 0, 0, 1, mp2);
+    Ten fac = ten(v, v, ZORB, ZORB, 1, 1, 1, fa), fki = ten(o, o, ZORB, ZORB, 1, 1, 1, fk);
+    Ten wk = ten(v, o, v, o, 1, 1, 1, wka);
+    CPSD_TRY(k_Fae_r2abij(fac, mp2t, X.abij, 1.0));
+    CPSD_TRY(k_Fmi_r2abij(fki, mp2t, X.abij, 1.0));
+    CPSD_TRY(k_Wmbej_r2abij(wk, mp2t, X.abij, 2.0));
+    i64 kroot = 0, roff = 0, itsum = 0;
+    for (i64 sym = 1; sym <= S.nirrep; sym++) {
+        const i64 nroot = p->estate_sym[sym - 1];
+        if (nroot == 0) continue;
+        const i64 l1 = irpdso(sym, v, o, 1), l2 = idsymsoc(sym, v, v, 0, o, o, 0), n = l1 + l2;
+        std::vector<double> g1;
+        CPSD_TRY(make_guess(S, eorb, p, sym, nroot, g1));
+        std::vector<double> rec((size_t)((n + 1) * nroot), 0.0);
+        for (i64 k = 0; k < nroot; k++)
+            std::copy(g1.begin() + k * (l1 + 1), g1.begin() + (k + 1) * (l1 + 1), rec.begin() + k * (n + 1));
+        ScratchScope sc2;
+        double *fileEV, *diag;
+        CPSD_TRY(scratch((i64)rec.size(), &fileEV));
+        CPSD_TRY(scratch(n, &diag));
+        CPSD_TRY(cuda_check(cudaMemcpyAsync(fileEV, rec.data(), sizeof(double) * rec.size(), cudaMemcpyHostToDevice,
+                                            stream()),
+                            "guess upload"));
+        const EnergyPlan *e1, *e2;
+        CPSD_TRY(plan_energy(make_desc(v, o, ZORB, ZORB, 1, 1, sym), "vozz", &e1));
+        CPSD_TRY(plan_energy(make_desc(v, v, o, o, 0, 0, sym), "vvoo", &e2));
+        CPSD_TRY(launch_energy(e1, 0, X.eorb, nullptr, diag));       // OED1
+        CPSD_TRY(launch_energy(e2, 0, X.eorb, nullptr, diag + l1));  // OED2
+        SigmaFn sig = [&](const double *R, i64 sR, double *AR, i64 sAR, i64 nb) {
+            Ten r1 = ten(v, o, ZORB, ZORB, 1, 1, sym, (double *)R, sR);
+            Ten r2 = ten(v, v, o, o, 0, 0, sym, (double *)R + l1, sR);
+            Ten c1 = ten(v, o, ZORB, ZORB, 1, 1, sym, AR, sAR);
+            Ten c2 = ten(v, v, o, o, 0, 0, sym, AR + l1, sAR);
+            CPSD_TRY(cuda_check(cudaMemset2DAsync(AR, sAR * sizeof(double), 0, l1 * sizeof(double), nb, stream()),
+                                "C1 clear"));
+            CPSD_TRY(k_c1_r1Fae(c1, r1, fac, 1.0, nb));
+            CPSD_TRY(k_c1_r1Fmi(c1, r1, fki, 1.0, nb));
+            CPSD_TRY(k_c1_r1iabj(c1, r1, wk, 1.0, nb));
+            CPSD_TRY(k_c1_r2abci(c1, r2, X.abci, 1.0, nb));
+            CPSD_TRY(k_c1_r2ijka(c1, r2, X.ijka, 1.0, nb));
+            CPSD_TRY(launch_energy(e2, 4, X.eorb, R + l1, AR + l1, nullptr, nb, sR, sAR));  // e(ab,ij) R2
+            CPSD_TRY(k_c2_r1abci(c2, r1, X.abci, 1.0, nb));
+            return k_c2_r1ijka(c2, r1, X.ijka, 1.0, nb);
+        };
+        i64 it = 0;
+        double mr = 0;
+        CPSD_TRY(davidson(p, n, nroot, fileEV, diag, sig, &it, &mr));
+        itsum += it;
+        CPSD_TRY(read_back(rec.data(), fileEV, sizeof(double) * rec.size()));
+        for (i64 k = 0; k < nroot; k++) omega_host[kroot + k] = rec[(size_t)(k * (n + 1))];
+        if (R_dev)
+            CPSD_TRY(cuda_check(cudaMemcpy2DAsync(R_dev + roff, n * sizeof(double), fileEV + 1, (n + 1) * sizeof(double),
+                                                  n * sizeof(double), nroot, cudaMemcpyDeviceToDevice, stream()),
+                                "R copy"));
+        kroot += nroot;
+        roff += n * nroot;
+    }
+    if (iterations) *iterations = itsum;
+    CPSD_TRY(cuda_check(cudaStreamSynchronize(stream()), "cisdoo sync"));
     return digit_error_check();
 }
 
@@ -509,6 +624,256 @@ int cpsd_ground3(const cpsd_system *s, const cpsd_integrals *I, const cpsd_param
     double h = 0;
     CPSD_TRY(read_back(&h, dE, sizeof h));
     if (E4_host) *E4_host = h;
+    return digit_error_check();
+}
+
+}  // extern "C"
+
+namespace cpsd {
+namespace {
+
+// The grCPS(D) ground state (src/grCPSd.SF): the intermediates of run.f90
+// and the four operator pieces of its orders
+struct GrState {
+    const Sys &S;
+    const Ints &X;
+    i64 l1, l2;
+    Ten fli, fad, wk;  // Fli, Fad, Wkaci
+};
+
+// <ab,ij|[V,T2]|0> (calA1R2.f90:30-37)
+int gr_a1r2(const GrState &g, Ten &C2, const double *T2) {
+    const i64 *o = g.S.popo, *v = g.S.popv;
+    Ten t2 = ten(v, v, o, o, 0, 0, 1, (double *)T2);
+    CPSD_TRY(k_c2_r2Wmbej(C2, t2, g.X.iabj, 1.0));
+    CPSD_TRY(k_c2_r2Wmnij(C2, t2, g.X.ijkl, 1.0));
+    return k_c2_r2abcd(C2, t2, g.X.abcd, 1.0);
+}
+
+// calA2R1.f90:27-47, Wkaci - iabj formed in place and restored as the
+// reference does
+int gr_a2r1(GrState &g, Ten &C1, const double *T1) {
+    const i64 *o = g.S.popo, *v = g.S.popv;
+    Ten t1 = ten(v, o, ZORB, ZORB, 1, 1, 1, (double *)T1);
+    const i64 n = g.wk.len();
+    CPSD_TRY(launch_axpy(n, -1.0, g.X.iabj.arr, g.wk.arr));
+    CPSD_TRY(k_c1_r1iabj(C1, t1, g.wk, -1.0));
+    CPSD_TRY(launch_axpy(n, 1.0, g.X.iabj.arr, g.wk.arr));
+    CPSD_TRY(k_c1_r1Fmi(C1, t1, g.fli, 1.0));
+    return k_c1_r1Fae(C1, t1, g.fad, 1.0);
+}
+
+// calL1_VTT.f90:30-75
+int gr_l1_vtt(const GrState &g, Ten &L1, const double *T1, const double *T2) {
+    const i64 *o = g.S.popo, *v = g.S.popv;
+    ScratchScope sc;
+    Ten t1 = ten(v, o, ZORB, ZORB, 1, 1, 1, (double *)T1), t2 = ten(v, v, o, o, 0, 0, 1, (double *)T2);
+    double *a, *b, *c;
+    CPSD_TRY(scratch(irpdso(1, o, o, 1), &a));
+    CPSD_TRY(scratch(irpdso(1, v, v, 1), &b));
+    CPSD_TRY(scratch(g.l1, &c));
+    Ten gli = ten(o, o, ZORB, ZORB, 1, 1, 1, a), gad = ten(v, v, ZORB, ZORB, 1, 1, 1, b);
+    Ten gld = ten(v, o, ZORB, ZORB, 1, 1, 1, c);
+    for (Ten *t : {&gli, &gad, &gld}) CPSD_TRY(zero(t->arr, t->len()));
+    CPSD_TRY(k_Fmi_r1ijka(gli, t1, g.X.ijka, -1.0));
+    CPSD_TRY(k_Fmi_r2abij(gli, t2, g.X.abij, -1.0));
+    CPSD_TRY(k_Fae_r1abci(gad, t1, g.X.abci, -1.0));
+    CPSD_TRY(k_Fae_r2abij(gad, t2, g.X.abij, -1.0));
+    CPSD_TRY(k_Fme_r1abij(gld, t1, g.X.abij, 1.0));
+    CPSD_TRY(k_c1_r1Fmi(L1, t1, gli, -1.0));
+    CPSD_TRY(k_c1_r1Fae(L1, t1, gad, -1.0));
+    return k_c1_r2Fme(L1, t2, gld, 1.0);
+}
+
+// calL2_VTT.f90:50-163: the eight terms of 0.5 <ab,ij|[[V,T],T]|0>
+int gr_l2_vtt(const GrState &g, Ten &L2, const double *T1, const double *T2) {
+    const i64 *o = g.S.popo, *v = g.S.popv;
+    const Ints &X = g.X;
+    ScratchScope sc;
+    Ten t1 = ten(v, o, ZORB, ZORB, 1, 1, 1, (double *)T1), t2 = ten(v, v, o, o, 0, 0, 1, (double *)T2);
+    const i64 n = std::max({X.abci.len(), X.ijka.len(), X.iabj.len(), X.ijkl.len()});
+    double *buf;
+    CPSD_TRY(scratch(n, &buf));
+    auto tmp = [&](const i64 *p0, const i64 *p1, const i64 *p2, const i64 *p3, i64 i0, i64 i1, Ten *w) {
+        *w = ten(p0, p1, p2, p3, i0, i1, 1, buf);
+        return zero(buf, w->len());
+    };
+    Ten w;
+    CPSD_TRY(tmp(o, o, o, v, 0, 1, &w));  // -PijPab{V(kb,cj) t(c,i) t(a,k)}
+    CPSD_TRY(k_Wkbij_r1iabj(w, t1, X.iabj, 1.0));
+    CPSD_TRY(k_c2_r1ijka(L2, t1, w, -1.0));
+    CPSD_TRY(tmp(v, v, v, o, 0, 1, &w));  // 0.5 Pij{V(ab,cd) t(c,i) t(d,j)}
+    CPSD_TRY(k_Wabdj_r1abcd(w, t1, X.abcd, 1.0));
+    CPSD_TRY(k_c2_r1abci(L2, t1, w, 0.5));
+    CPSD_TRY(tmp(o, o, o, v, 0, 1, &w));  // 0.5 Pab{V(kl,ij) t(a,k) t(b,l)}
+    CPSD_TRY(k_Wkbij_r1Uklij(w, t1, X.ijkl, 1.0));
+    CPSD_TRY(k_c2_r1ijka(L2, t1, w, 0.5));
+    CPSD_TRY(tmp(o, o, ZORB, ZORB, 1, 1, &w));  // -Pij{Gli t(ab,lj)}
+    CPSD_TRY(k_Fmi_r1ijka(w, t1, X.ijka, 1.0));
+    CPSD_TRY(k_Fmi_r2abij(w, t2, X.abij, 1.0));
+    CPSD_TRY(k_c2_r2Fmi(L2, t2, w, 1.0));
+    CPSD_TRY(tmp(v, v, ZORB, ZORB, 1, 1, &w));  // Pab{Gad t(db,ij)}
+    CPSD_TRY(k_Fae_r1abci(w, t1, X.abci, 1.0));
+    CPSD_TRY(k_Fae_r2abij(w, t2, X.abij, 1.0));
+    CPSD_TRY(k_c2_r2Fae(L2, t2, w, 1.0));
+    CPSD_TRY(tmp(v, o, v, o, 1, 1, &w));  // PijPab{Wkbcj t(ac,ik)}
+    CPSD_TRY(k_Wmbej_r1ijka(w, t1, X.ijka, 1.0));
+    CPSD_TRY(k_Wmbej_r1abci(w, t1, X.abci, 1.0));
+    CPSD_TRY(k_Wmbej_r2abij(w, t2, X.abij, 1.0));
+    CPSD_TRY(k_c2_r2Wmbej(L2, t2, w, 1.0));
+    CPSD_TRY(tmp(o, o, o, v, 0, 1, &w));  // -0.5 Pab{V(kb,cd) t(cd,ij) t(a,k)}
+    CPSD_TRY(k_Wkbij_r2abci(w, t2, X.abci, 1.0));
+    CPSD_TRY(k_c2_r1ijka(L2, t1, w, 1.0));
+    CPSD_TRY(tmp(o, o, o, o, 0, 0, &w));  // Wklij t(ab,kl)
+    CPSD_TRY(k_Wmnij_r1ijka(w, t1, X.ijka, 0.5));
+    CPSD_TRY(k_Wmnij_r2abij(w, t2, X.abij, 0.5));
+    return k_c2_r2Wmnij(L2, t2, w, 2.0);
+}
+
+// solver.f90:24-73 on the device: T = denomT(R) with DIIS over (T1, T2),
+// R = C + (calA0R1(T), calA0R2(T1)), one device-driven step per iteration
+int gr_solve(const GrState &g, const cpsd_params *p, const double *C, double *T, i64 *iters) {
+    const i64 *o = g.S.popo, *v = g.S.popv;
+    const Ints &X = g.X;
+    const i64 l1 = g.l1, len = g.l1 + g.l2;
+    const int md = (int)p->diis_dim;
+    if (md > DIIS_MAXDIM) return set_error(CPSD_EARG, "diis_dim above 16");
+    if (len > 0x7fffffffLL) return set_error(CPSD_EARG, "amplitude vector too long");
+    ScratchScope sc;
+    double *pr, *sg, *den, *prev, *err, *amp;
+    CPSD_TRY(scratch(len, &pr));
+    CPSD_TRY(scratch(len, &sg));
+    CPSD_TRY(scratch(len, &den));
+    CPSD_TRY(scratch(len, &prev));
+    CPSD_TRY(scratch(md * len, &err));
+    CPSD_TRY(scratch(md * len, &amp));
+    SolverState *ss;
+    DiisState *ds;
+    CPSD_TRY(arena().alloc(sizeof(SolverState), (void **)&ss));
+    CPSD_TRY(arena().alloc(sizeof(DiisState), (void **)&ds));
+    SolverState hss{0, 1, 0, 0, 0.0};
+    DiisState hds{(int)len, md, 1, 1, 1.0, {}};
+    CPSD_TRY(cuda_check(cudaMemcpyAsync(ss, &hss, sizeof hss, cudaMemcpyHostToDevice, stream()), "solver state"));
+    CPSD_TRY(cuda_check(cudaMemcpyAsync(ds, &hds, sizeof hds, cudaMemcpyHostToDevice, stream()), "diis state"));
+    const EnergyPlan *e1, *e2;
+    CPSD_TRY(plan_energy(make_desc(v, o, ZORB, ZORB, 1, 1, 1), "vozz", &e1));
+    CPSD_TRY(plan_energy(make_desc(v, v, o, o, 0, 0, 1), "vvoo", &e2));
+    CPSD_TRY(launch_energy(e1, 5, X.eorb, nullptr, den));       // ei - ea
+    CPSD_TRY(launch_energy(e2, 5, X.eorb, nullptr, den + l1));  // ei + ej - ea - eb
+    CPSD_TRY(launch_copy(pr, C, len));
+    SolverArgs a;
+    a.len = (int)len;
+    a.nb = 1;
+    a.cyc = (int)p->diis_cyc;
+    a.tol = p->diis_max_err;
+    a.ss = ss;
+    a.ds = ds;
+    a.db.prev = prev;
+    a.db.err = err;
+    a.db.amp = amp;
+    a.sprev = len;
+    a.serr = md * len;
+    a.pr = pr;
+    a.R1 = T;
+    a.cc = C;
+    a.S = sg;
+    a.den = den;
+    int *mb, *mb_dev;
+    CPSD_TRY(mapped_mailbox(&mb, &mb_dev));
+    mb[0] = 1;
+    a.mailbox = mb_dev;
+    StepThrottle &th = throttle();
+    CPSD_TRY(th.init());
+    Ten s1 = ten(v, o, ZORB, ZORB, 1, 1, 1, sg), s2 = ten(v, v, o, o, 0, 0, 1, sg + l1);
+    Ten t1 = ten(v, o, ZORB, ZORB, 1, 1, 1, T), t2 = ten(v, v, o, o, 0, 0, 1, T + l1);
+    for (i64 it = 1; it <= p->diis_cyc + 1; it++) {
+        CPSD_TRY(solver_step_launch(a));
+        CPSD_TRY(th.mark(it));
+        if (((volatile int *)mb)[0] == 0) break;
+        CPSD_TRY(zero(sg, len));
+        CPSD_TRY(k_c1_r1iabj(s1, t1, g.wk, 1.0));  // calA0R1
+        CPSD_TRY(k_c1_r1Fmi(s1, t1, g.fli, -1.0));
+        CPSD_TRY(k_c1_r1Fae(s1, t1, g.fad, -1.0));
+        CPSD_TRY(k_c1_r2ijka(s1, t2, X.ijka, 1.0));
+        CPSD_TRY(k_c1_r2abci(s1, t2, X.abci, 1.0));
+        CPSD_TRY(k_c2_r1ijka(s2, t1, X.ijka, 1.0));  // calA0R2
+        CPSD_TRY(k_c2_r1abci(s2, t1, X.abci, 1.0));
+        CPSD_TRY(th.wait(it));
+    }
+    CPSD_TRY(read_back(&hss, ss, sizeof hss));
+    if (iters) *iters = hss.iter;
+    return CPSD_OK;
+}
+
+}  // namespace
+}  // namespace cpsd
+
+extern "C" {
+
+// grCPS(D) (src/grCPSd.SF/run.f90): intermediates (run.f90:27-47), then
+// orders 1..3 (run1/run2/run3.f90) with C^(1) = (0, abij), C^(2) = (0,
+// calA1R2(T2^(1))), C^(3) = (calA2R1(T1^(1)) + calL1_VTT(T^(1)),
+// calA1R2(T2^(2)) + calL2_VTT(T^(1))); E^(k+1) = (T2^(k) + effectT2) . abij
+// (calEcorr.f90:21-52)
+int cpsd_grcpsd_ground(const cpsd_system *s, const cpsd_integrals *I, const cpsd_params *p, double *T_dev,
+                       double *E_host, int64_t *iters) {
+    Sys S;
+    CPSD_TRY(make_sys(s, &S));
+    Ints X = make_ints(S, I);
+    IntegralScope keep(I);
+    const i64 *o = S.popo, *v = S.popv;
+    ScratchScope sc;
+    const i64 l1 = irpdso(1, v, o, 1), l2 = idsymsoc(1, v, v, 0, o, o, 0), lt = l1 + l2;
+    double *mp2, *fo, *fv, *wk, *C, *tau, *dE;
+    CPSD_TRY(scratch(l2, &mp2));
+    CPSD_TRY(scratch(irpdso(1, o, o, 1), &fo));
+    CPSD_TRY(scratch(irpdso(1, v, v, 1), &fv));
+    CPSD_TRY(scratch(X.iabj.len(), &wk));
+    CPSD_TRY(scratch(lt, &C));
+    CPSD_TRY(scratch(l2, &tau));
+    CPSD_TRY(scratch(3, &dE));
+    GrState g{S, X, l1, l2, ten(o, o, ZORB, ZORB, 1, 1, 1, fo), ten(v, v, ZORB, ZORB, 1, 1, 1, fv),
+              ten(v, o, v, o, 1, 1, 1, wk)};
+    const EnergyPlan *e2;
+    CPSD_TRY(plan_energy(make_desc(v, v, o, o, 0, 0, 1), "vvoo", &e2));
+    CPSD_TRY(launch_energy(e2, 2, X.eorb, I->abij, mp2));  // MP2t
+    Ten mp2t = ten(v, v, o, o, 0, 0, 1, mp2);
+    CPSD_TRY(zero(fo, g.fli.len()));
+    CPSD_TRY(zero(fv, g.fad.len()));
+    CPSD_TRY(launch_copy(wk, X.iabj.arr, X.iabj.len()));
+    CPSD_TRY(k_Fmi_r2abij(g.fli, mp2t, X.abij, -1.0));
+    CPSD_TRY(k_Fae_r2abij(g.fad, mp2t, X.abij, -1.0));
+    CPSD_TRY(k_Wmbej_r2abij(g.wk, mp2t, X.abij, 2.0));
+    Ten c1 = ten(v, o, ZORB, ZORB, 1, 1, 1, C), c2 = ten(v, v, o, o, 0, 0, 1, C + l1);
+    Ten ta = ten(v, v, o, o, 0, 0, 1, tau);
+    for (int k = 1; k <= 3; k++) {
+        double *Tk = T_dev + (k - 1) * lt;
+        CPSD_TRY(zero(C, lt));
+        if (k == 1) CPSD_TRY(launch_copy(C + l1, I->abij, l2));
+        if (k >= 2) CPSD_TRY(gr_a1r2(g, c2, T_dev + (k - 2) * lt + l1));
+        if (k == 3) {
+            CPSD_TRY(gr_a2r1(g, c1, T_dev));
+            CPSD_TRY(gr_l1_vtt(g, c1, T_dev, T_dev + l1));
+            CPSD_TRY(gr_l2_vtt(g, c2, T_dev, T_dev + l1));
+        }
+        i64 it = 0;
+        CPSD_TRY(gr_solve(g, p, C, Tk, &it));
+        if (iters) iters[k - 1] = it;
+        // calEcorr: tau = T2^(k) (+ effectT2 of the fixed lower-order T1)
+        CPSD_TRY(launch_copy(tau, Tk + l1, l2));
+        if (k == 2) {  // type 1 of T1^(1): t(a,i) t(b,j) - t(a,j) t(b,i)
+            Ten x = ten(v, o, ZORB, ZORB, 1, 1, 1, T_dev);
+            CPSD_TRY(w224(x, x, ta, 0.5, "ai", "bj", "abij", 3));
+        } else if (k == 3) {  // type 2: P(ab) P(ij) t^(2)(a,i) t^(1)(b,j)
+            Ten x = ten(v, o, ZORB, ZORB, 1, 1, 1, T_dev + lt), y = ten(v, o, ZORB, ZORB, 1, 1, 1, T_dev);
+            CPSD_TRY(w224(x, y, ta, 1.0, "ai", "bj", "abij", 3));
+        }
+        CPSD_TRY(launch_dot(tau, I->abij, l2, dE + (k - 1), true));
+    }
+    double h[3];
+    CPSD_TRY(read_back(h, dE, sizeof h));
+    if (E_host)
+        for (int k = 0; k < 3; k++) E_host[k] = h[k];
     return digit_error_check();
 }
 

@@ -118,7 +118,9 @@ __global__ void k_energy(const i64 *__restrict__ blk, int nblocks, i64 n, const 
             double ea = eorb[ia], eb = eorb[ib], ei = eorb[ii], ej = eorb[ij];
             if (mode == 0) v = ea + eb - ei - ej;
             else if (mode == 1) v = in[e] / ((ea + eb - ei - ej) - w0);
-            else v = in[e] / (ei + ej - ea - eb);  // mode 2
+            else if (mode == 4) v = (ea + eb - ei - ej) * in[e];
+            else if (mode == 5) v = ei + ej - ea - eb;  // the divisor of mode 2
+            else v = in[e] / (ei + ej - ea - eb);       // mode 2
         }
         out[e] = v;
     }

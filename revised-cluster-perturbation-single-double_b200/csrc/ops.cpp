@@ -844,6 +844,44 @@ int k_Wmnij_r1ijka(Ten &W, const Ten &r1, const Ten &V, double f, i64 nb) {
 int k_Wmnij_r2abij(Ten &W, const Ten &r2, const Ten &V, double f, i64 nb) {
     return w444(V, r2, W, r2.d.iop[0] == 0 ? f : 0.5 * f, "efmn", "efij", "mnij", 0, nb);
 }
+// kernels of the second-order ground state (grCPSd.SF calL1_VTT / calL2_VTT)
+int k_Wkbij_r1iabj(Ten &W, const Ten &r1, const Ten &V, double f, i64 nb) {
+    return w424(V, r1, W, -f, "ckbj", "ci", "ijkb", 1, nb);
+}
+int k_Wabdj_r1abcd(Ten &W, const Ten &r1, const Ten &V, double f, i64 nb) {
+    return w424(V, r1, W, f, "abdc", "cj", "abdj", 0, nb);
+}
+int k_Wkbij_r1Uklij(Ten &W, const Ten &r1, const Ten &U, double f, i64 nb) {
+    return w424(U, r1, W, -f, "klij", "bl", "ijkb", 0, nb);
+}
+int k_Fme_r1abij(Ten &F, const Ten &r1, const Ten &V, double f, i64 nb) {
+    return w422(V, r1, F, f, "efmn", "fn", "em", nb);
+}
+int k_c1_r2Fme(Ten &c1, const Ten &r2, const Ten &F, double f, i64 nb) {
+    return w422(r2, F, c1, f, "aeim", "em", "ai", nb);
+}
+// kernels of the excited-state grCPS(D) (EE-grCPSd.SF calEigenCISDoo, calJ, calC_VTTR)
+int k_c1d_l1Wibaj(Ten &c1, const Ten &l1, const Ten &W, double f, i64 nb) {
+    return w422(W, l1, c1, f, "aibj", "bj", "ai", nb);
+}
+int k_c1d_l1fab(Ten &c1, const Ten &l1, const Ten &F, double f, i64 nb) {
+    return w222(F, l1, c1, -f, "ba", "bi", "ai", nb);
+}
+int k_c1d_l1fij(Ten &c1, const Ten &l1, const Ten &F, double f, i64 nb) {
+    return w222(l1, F, c1, f, "aj", "ij", "ai", nb);
+}
+int k_Fae_r1fia(Ten &c1, const Ten &r1, const Ten &F, double f, i64 nb) {
+    return w222(r1, F, c1, -f, "al", "el", "ae", nb);
+}
+int k_Fmi_r1fia(Ten &c1, const Ten &r1, const Ten &F, double f, i64 nb) {
+    return w222(F, r1, c1, f, "dm", "di", "mi", nb);
+}
+int k_Wkbij_r2Fkc(Ten &c1, const Ten &r2, const Ten &F, double f, i64 nb) {
+    return w424(r2, F, c1, -f, "cbij", "ck", "ijkb", 0, nb);
+}
+int k_Wlkjd_r1abij(Ten &c1, const Ten &r1, const Ten &V, double f, i64 nb) {
+    return w424(V, r1, c1, f, "cdlk", "cj", "lkjd", 0, nb);
+}
 
 // ------------------------------------------ adjoints of the lib_cc kernels
 // vjp_<name>(a, b, Y, G, which, f): G += d<Y, out>/da (which 0) or /db
@@ -1431,5 +1469,17 @@ KER(Wmbej_r1abci)
 KER(Wmbej_r1ijka)
 KER(Wmnij_r1ijka)
 KER(Wmnij_r2abij)
+KER(Wkbij_r1iabj)
+KER(Wabdj_r1abcd)
+KER(Wkbij_r1Uklij)
+KER(Fme_r1abij)
+KER(c1_r2Fme)
+KER(c1d_l1Wibaj)
+KER(c1d_l1fab)
+KER(c1d_l1fij)
+KER(Fae_r1fia)
+KER(Fmi_r1fia)
+KER(Wkbij_r2Fkc)
+KER(Wlkjd_r1abij)
 
 }  // extern "C"

@@ -70,6 +70,18 @@ CPSD_IK(Wmbej_r1abci);
 CPSD_IK(Wmbej_r1ijka);
 CPSD_IK(Wmnij_r1ijka);
 CPSD_IK(Wmnij_r2abij);
+CPSD_IK(Wkbij_r1iabj);
+CPSD_IK(Wabdj_r1abcd);
+CPSD_IK(Wkbij_r1Uklij);
+CPSD_IK(Fme_r1abij);
+CPSD_IK(c1_r2Fme);
+CPSD_IK(c1d_l1Wibaj);
+CPSD_IK(c1d_l1fab);
+CPSD_IK(c1d_l1fij);
+CPSD_IK(Fae_r1fia);
+CPSD_IK(Fmi_r1fia);
+CPSD_IK(Wkbij_r2Fkc);
+CPSD_IK(Wlkjd_r1abij);
 #undef CPSD_IK
 
 // Vector-Jacobian product of the vv2v_444 form v3 += fact * P{v1 v2}:

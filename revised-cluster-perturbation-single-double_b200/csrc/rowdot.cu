@@ -10,12 +10,18 @@
 // A warp owns a run of rows of one task and one group of up to 8 columns:
 // lane l keeps the column operand's values y[q][c] = Y(k = l + 32 q, c) in
 // registers for the whole run (one segment per task, so they do not
-// change), then takes the rows RB = 32 / ncol at a time: each lane loads
-// its K elements of the RB rows (coalesced along K), forms the RB x ncol
-// partial dot products, and one transpose reduction across the warp leaves
-// output (row l / ncol, column l % ncol) in lane l, which adds it to C.
-// Sums run over k in lane order then the fixed butterfly, deterministic.
+// change), then takes the rows RB = 32 / ncol at a time.  Each lane copies
+// its K elements of a batch's RB rows (coalesced along K) with 8-byte
+// cp.async into its own slots of a per-warp ring of NS batches in shared
+// memory, NS - 1 batches ahead of the one it works on, so the loads in
+// flight do not hold registers; it forms the RB x ncol partial dot
+// products from its slots, and one transpose reduction across the warp
+// leaves output (row l / ncol, column l % ncol) in lane l, which adds it
+// to C.  A lane only ever reads the slots it filled itself, so the
+// cp.async group wait is the only synchronisation.  Sums run over k in
+// lane order then the fixed butterfly, deterministic.
 #include <algorithm>
+#include <atomic>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -55,14 +61,35 @@ __device__ __forceinline__ double reduce32(double (&v)[32]) {
     return v[0];
 }
 
+__device__ __forceinline__ void cp_async8(double *dst, const double *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+template <int KQ, int NC>
+struct RdCfg {
+    static constexpr int RB = 32 / NC < 8 ? 32 / NC : 8;  // rows per batch
+    static constexpr int SLOT = RB * KQ * 32;             // doubles of one batch of one warp
+    // ring depth: about 24 KB per warp, 2..6 batches
+    static constexpr int NS = 24576 / (SLOT * 8) < 2 ? 2 : 24576 / (SLOT * 8) > 6 ? 6 : 24576 / (SLOT * 8);
+    static constexpr int SMEM = RW * NS * SLOT * (int)sizeof(double);
+};
+
 // KQ = K / 32 rounded up (1..4); NC = columns per item rounded up to 2, 4
-// or 8, RB = min(32 / NC, 8) rows per batch; SWAP: rows over the N side
+// or 8; SWAP: rows over the N side
 template <int KQ, int NC, bool SWAP>
 __global__ void __launch_bounds__(RW * 32) k_rowdot(const TaskDev *__restrict__ tasks, const SegDev *__restrict__ segs,
                                                     const RowDotItem *__restrict__ items, int nitems,
                                                     const double *__restrict__ A, const double *__restrict__ B,
                                                     double *__restrict__ C, double alpha) {
-    constexpr int RB = 32 / NC < 8 ? 32 / NC : 8;  // at most 8 rows in flight (registers)
+    using Cf = RdCfg<KQ, NC>;
+    constexpr int RB = Cf::RB, RD_NS = Cf::NS;
+    extern __shared__ double rd_ring[];
     __shared__ TaskDev tks[RW];
     __shared__ SegDev sgs[RW];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -87,6 +114,31 @@ __global__ void __launch_bounds__(RW * 32) k_rowdot(const TaskDev *__restrict__ 
     const i64 kyst = SWAP ? sg.kSA[0] : sg.kSB[0];  // the contracted unit's stride in Y (1 in X)
     const i64 xb = SWAP ? sg.baseB : sg.baseA, yb = SWAP ? sg.baseA : sg.baseB;
     const int K = (int)sg.K, ncol = item.ncol;
+    double *ring = rd_ring + (size_t)warp * RD_NS * Cf::SLOT;
+    // batch b covers rows item.r0 + b RB ..; its copies go to slot b % RD_NS,
+    // element (row i, k = lane + 32 q) at [(i KQ + q) 32 + lane]
+    const i64 nrows = item.r1 - item.r0;
+    const int nbatch = (int)((nrows + RB - 1) / RB);
+    auto issue = [&](int b) {
+        if (b < nbatch) {
+            const i64 r0 = item.r0 + (i64)b * RB;
+            const int nr = (int)min((i64)RB, item.r1 - r0);
+            const i64 myrow = lane < nr ? xb + rdecode(r0 + lane, rn, rext, rsx) : 0;
+            double *buf = ring + (size_t)(b % RD_NS) * Cf::SLOT + lane;
+#pragma unroll
+            for (int i = 0; i < RB; i++) {
+                const i64 ox = __shfl_sync(0xffffffffu, myrow, i);
+#pragma unroll
+                for (int q = 0; q < KQ; q++) {
+                    const int k = lane + 32 * q;
+                    double *d = buf + (i * KQ + q) * 32;
+                    if (i < nr && k < K) cp_async8(d, X + ox + k);
+                    else *d = 0.0;
+                }
+            }
+        }
+        cp_async_commit();  // an empty group past the end keeps the count
+    };
     // column operand values of this lane (k = lane + 32 q), held for the run
     double y[KQ][NC];
 #pragma unroll
@@ -98,54 +150,38 @@ __global__ void __launch_bounds__(RW * 32) k_rowdot(const TaskDev *__restrict__ 
             y[q][c] = (c < ncol && k < K) ? __ldg(Y + oy + (i64)k * kyst) : 0.0;
         }
     }
-    // batches of RB rows; the next batch's loads are issued before the
-    // current batch is reduced, so they overlap the shuffles
-    auto rowoff = [&](i64 r0, int nr) -> i64 { return lane < nr ? xb + rdecode(r0 + lane, rn, rext, rsx) : 0; };
-    auto load = [&](double (&x)[KQ][RB], i64 myrow, int nr) {
 #pragma unroll
-        for (int i = 0; i < RB; i++) {
-            const i64 ox = __shfl_sync(0xffffffffu, myrow, i);
-#pragma unroll
-            for (int q = 0; q < KQ; q++) {
-                const int k = lane + 32 * q;
-                x[q][i] = (i < nr && k < K) ? __ldg(X + ox + k) : 0.0;
-            }
-        }
-    };
-    i64 r0 = item.r0;
-    int nr = (int)min((i64)RB, item.r1 - r0);
-    double x[KQ][RB];
-    load(x, rowoff(r0, nr), nr);
-    for (;;) {
-        const i64 rn0 = r0 + RB;
-        const bool more = rn0 < item.r1;
-        const int nrn = more ? (int)min((i64)RB, item.r1 - rn0) : 0;
-        double xn[KQ][RB];
-        if (more) load(xn, rowoff(rn0, nrn), nrn);
+    for (int b = 0; b < RD_NS - 1; b++) issue(b);
+    const int ri = lane / NC, ci = lane % NC;
+    const i64 ccol = ci < ncol ? rdecode(item.c0 + ci, cn, cext, csc) : 0;
+    for (int b = 0; b < nbatch; b++) {
+        issue(b + RD_NS - 1);  // into the slot consumed by batch b - 1
+        cp_async_wait<RD_NS - 1>();
+        const i64 r0 = item.r0 + (i64)b * RB;
+        const int nr = (int)min((i64)RB, item.r1 - r0);
+        // the output this lane updates, its old value fetched before the sums
+        const bool mine = ri < nr && ci < ncol;
+        const i64 o = mine ? tk.baseC + rdecode(r0 + ri, rn, rext, rsc) + ccol : 0;
+        const double cold = mine ? C[o] : 0.0;
+        const double *buf = ring + (size_t)(b % RD_NS) * Cf::SLOT + lane;
         double acc[32];
 #pragma unroll
-        for (int i = 0; i < RB; i++)
+        for (int i = 0; i < RB; i++) {
+            double x[KQ];
+#pragma unroll
+            for (int q = 0; q < KQ; q++) x[q] = buf[(i * KQ + q) * 32];
 #pragma unroll
             for (int c = 0; c < NC; c++) {
                 double t = 0.0;
 #pragma unroll
-                for (int q = 0; q < KQ; q++) t = fma(x[q][i], y[q][c], t);
+                for (int q = 0; q < KQ; q++) t = fma(x[q], y[q][c], t);
                 acc[i * NC + c] = t;
             }
-        const double s = reduce32(acc);
-        const int ri = lane / NC, ci = lane % NC;
-        if (ri < nr && ci < ncol) {
-            const i64 o = tk.baseC + rdecode(r0 + ri, rn, rext, rsc) + rdecode(item.c0 + ci, cn, cext, csc);
-            C[o] += alpha * s;
         }
-        if (!more) break;
-#pragma unroll
-        for (int q = 0; q < KQ; q++)
-#pragma unroll
-            for (int i = 0; i < RB; i++) x[q][i] = xn[q][i];
-        r0 = rn0;
-        nr = nrn;
+        const double s = reduce32(acc);
+        if (mine) C[o] = cold + alpha * s;
     }
+    cp_async_wait<0>();  // no copy outlives the warp
 }
 
 template <class T>
@@ -251,6 +287,23 @@ int plan_rowdot(const ContractPlan *cp, const RowDotPlan **out) {
     return CPSD_OK;
 }
 
+namespace {
+template <int KQ, int NC, bool SWAP>
+int rowdot_go(int grid, const RowDotPlan *rp, int ni, const double *A, const double *B, double *C, double alpha) {
+    using Cf = RdCfg<KQ, NC>;
+    static std::atomic<bool> attr{false};
+    if (!attr.load(std::memory_order_acquire)) {
+        CPSD_TRY(cuda_check(cudaFuncSetAttribute(k_rowdot<KQ, NC, SWAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 Cf::SMEM),
+                            "row-dot smem attr"));
+        attr.store(true, std::memory_order_release);
+    }
+    k_rowdot<KQ, NC, SWAP><<<grid, RW * 32, Cf::SMEM, stream()>>>(rp->d_tasks, rp->d_segs, rp->d_items, ni, A, B, C,
+                                                                  alpha);
+    return CPSD_OK;
+}
+}  // namespace
+
 int launch_rowdot(const ContractPlan *cp, const RowDotPlan *rp, const double *A, const double *B, double *C,
                   double alpha) {
     if (rp->items.empty()) return CPSD_OK;
@@ -262,11 +315,9 @@ int launch_rowdot(const ContractPlan *cp, const RowDotPlan *rp, const double *A,
     const int ni = (int)rp->items.size(), grid = (ni + RW - 1) / RW;
 #define CPSD_ROWDOT(KQ, NC)                                                                                          \
     if (rp->swap)                                                                                                    \
-        k_rowdot<KQ, NC, true><<<grid, RW * 32, 0, stream()>>>(rp->d_tasks, rp->d_segs, rp->d_items, ni, A, B, C,    \
-                                                             alpha);                                              \
+        CPSD_TRY((rowdot_go<KQ, NC, true>(grid, rp, ni, A, B, C, alpha)));                                           \
     else                                                                                                             \
-        k_rowdot<KQ, NC, false><<<grid, RW * 32, 0, stream()>>>(rp->d_tasks, rp->d_segs, rp->d_items, ni, A, B, C,   \
-                                                              alpha);
+        CPSD_TRY((rowdot_go<KQ, NC, false>(grid, rp, ni, A, B, C, alpha)));
 #define CPSD_ROWDOT_K(KQ)                                                                                            \
     switch (rp->nc) {                                                                                                \
     case 2: CPSD_ROWDOT(KQ, 2) break;                                                                                \

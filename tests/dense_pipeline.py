@@ -192,3 +192,84 @@ class DenseSystem:
         dms[l1 + rows2[:, 0]] = (self.spin_v[rows2[:, 1]] + self.spin_v[rows2[:, 2]]
                                  - self.spin_o[rows2[:, 3]] - self.spin_o[rows2[:, 4]])
         return A, dms
+
+    def grcpsd(self):
+        """grCPS(D) ground state (src/grCPSd.SF/run.f90, solver.f90) with
+        each order's coupled (T1, T2) equations solved exactly: T2 =
+        -(C2 + A0R2 T1) / e2 eliminated, the (a,i) system of irrep 1 solved
+        densely.  Returns T1, T2 per order and E^(2..4)."""
+        e1, e2 = self.e1, self.e2
+        MP2t = -self.abij / e2
+        Fli = K("Fmi_r2abij", MP2t, self.abij, -1.0)
+        Fad = K("Fae_r2abij", MP2t, self.abij, -1.0)
+        W = self.iabj + K("Wmbej_r2abij", MP2t, self.abij, 2.0)
+
+        def a0r1(T1, T2):
+            return (K("c1_r1iabj", T1, W) + K("c1_r1Fmi", T1, Fli, -1.0) + K("c1_r1Fae", T1, Fad, -1.0)
+                    + K("c1_r2ijka", T2, self.ijka) + K("c1_r2abci", T2, self.abci))
+
+        def a0r2(T1):
+            return K("c2_r1ijka", T1, self.ijka) + K("c2_r1abci", T1, self.abci)
+
+        def a1r2(T2):
+            return (K("c2_r2Wmbej", T2, self.iabj) + K("c2_r2Wmnij", T2, self.ijkl)
+                    + K("c2_r2abcd", T2, self.abcd))
+
+        def a2r1(T1):
+            return (K("c1_r1iabj", T1, W - self.iabj, -1.0) + K("c1_r1Fmi", T1, Fli, 1.0)
+                    + K("c1_r1Fae", T1, Fad, 1.0))
+
+        def l1_vtt(T1, T2):
+            Gli = K("Fmi_r1ijka", T1, self.ijka, -1.0) + K("Fmi_r2abij", T2, self.abij, -1.0)
+            Gad = K("Fae_r1abci", T1, self.abci, -1.0) + K("Fae_r2abij", T2, self.abij, -1.0)
+            Gld = K("Fme_r1abij", T1, self.abij, 1.0)
+            return K("c1_r1Fmi", T1, Gli, -1.0) + K("c1_r1Fae", T1, Gad, -1.0) + K("c1_r2Fme", T2, Gld, 1.0)
+
+        def l2_vtt(T1, T2):
+            L = K("c2_r1ijka", T1, K("Wkbij_r1iabj", T1, self.iabj), -1.0)
+            L = L + K("c2_r1abci", T1, K("Wabdj_r1abcd", T1, self.abcd), 0.5)
+            L = L + K("c2_r1ijka", T1, K("Wkbij_r1Uklij", T1, self.ijkl), 0.5)
+            G = K("Fmi_r1ijka", T1, self.ijka) + K("Fmi_r2abij", T2, self.abij)
+            L = L + K("c2_r2Fmi", T2, G)
+            G = K("Fae_r1abci", T1, self.abci) + K("Fae_r2abij", T2, self.abij)
+            L = L + K("c2_r2Fae", T2, G)
+            G = (K("Wmbej_r1ijka", T1, self.ijka) + K("Wmbej_r1abci", T1, self.abci)
+                 + K("Wmbej_r2abij", T2, self.abij))
+            L = L + K("c2_r2Wmbej", T2, G)
+            L = L + K("c2_r1ijka", T1, K("Wkbij_r2abci", T2, self.abci))
+            G = K("Wmnij_r1ijka", T1, self.ijka, 0.5) + K("Wmnij_r2abij", T2, self.abij, 0.5)
+            return L + K("c2_r2Wmnij", T2, G, 2.0)
+
+        idx = np.argwhere(self.mask1(1))
+
+        def solve(C1, C2):
+            # -e1 T1 = C1 + a0r1(T1, T2), T2 = -(C2 + a0r2(T1)) / e2
+            def t2_of(T1):
+                return -(C2 + a0r2(T1)) / e2
+
+            def resid(x):
+                T1 = np.zeros_like(e1)
+                T1[idx[:, 0], idx[:, 1]] = x
+                r = e1 * T1 + C1 + a0r1(T1, t2_of(T1))
+                return r[idx[:, 0], idx[:, 1]]
+
+            n = len(idx)
+            r0 = resid(np.zeros(n))
+            M = np.column_stack([resid(np.eye(n)[k]) - r0 for k in range(n)])
+            x = np.linalg.solve(M, -r0)
+            T1 = np.zeros_like(e1)
+            T1[idx[:, 0], idx[:, 1]] = x
+            return T1, t2_of(T1)
+
+        out = []
+        zero1, zero2 = np.zeros_like(e1), np.zeros_like(e2)
+        T1a, T2a = solve(zero1, self.abij)
+        E2 = 0.25 * np.sum(T2a * self.abij)
+        T1b, T2b = solve(zero1, a1r2(T2a))
+        tau = T2b + (np.einsum("ai,bj->abij", T1a, T1a) - np.einsum("aj,bi->abij", T1a, T1a))
+        E3 = 0.25 * np.sum(tau * self.abij)
+        T1c, T2c = solve(a2r1(T1a) + l1_vtt(T1a, T2a), a1r2(T2b) + l2_vtt(T1a, T2a))
+        X = np.einsum("ai,bj->abij", T1b, T1a)
+        tau = T2c + (X - X.transpose(0, 1, 3, 2) - X.transpose(1, 0, 2, 3) + X.transpose(1, 0, 3, 2))
+        E4 = 0.25 * np.sum(tau * self.abij)
+        return dict(T1=[T1a, T1b, T1c], T2=[T2a, T2b, T2c], E=np.array([E2, E3, E4]))

@@ -56,6 +56,20 @@ KERNELS = {
     "Wmbej_r1ijka": ("iabj", "ai", "ijka", lambda r, V, f: -f * np.einsum("bn,nmje->embj", r, V)),
     "Wmnij_r1ijka": ("ijkl", "ai", "ijka", lambda r, V, f: f * RS(np.einsum("ej,mnie->mnij", r, V))),
     "Wmnij_r2abij": ("ijkl", "abij", "abij", lambda r, V, f: 0.5 * f * np.einsum("efmn,efij->mnij", V, r)),
+    # the second-order ground state's (src/grCPSd.SF/calL1_VTT.f90, calL2_VTT.f90)
+    "Wkbij_r1iabj": ("ijka", "ai", "iabj", lambda r, V, f: -f * PQ(np.einsum("ckbj,ci->ijkb", V, r))),
+    "Wabdj_r1abcd": ("abci", "ai", "abcd", lambda r, V, f: f * np.einsum("abdc,cj->abdj", V, r)),
+    "Wkbij_r1Uklij": ("ijka", "ai", "ijkl", lambda r, U, f: -f * np.einsum("klij,bl->ijkb", U, r)),
+    "Fme_r1abij": ("ai", "ai", "abij", lambda r, V, f: f * np.einsum("efmn,fn->em", V, r)),
+    "c1_r2Fme": ("ai", "abij", "ai", lambda r, F, f: f * np.einsum("aeim,em->ai", r, F)),
+    # the excited-state grCPS(D)'s (src/EE-grCPSd.SF)
+    "c1d_l1Wibaj": ("ai", "ai", "iabj", lambda l, W, f: f * np.einsum("aibj,bj->ai", W, l)),
+    "c1d_l1fab": ("ai", "ai", "vv", lambda l, F, f: -f * np.einsum("ba,bi->ai", F, l)),
+    "c1d_l1fij": ("ai", "ai", "oo", lambda l, F, f: f * np.einsum("aj,ij->ai", l, F)),
+    "Fae_r1fia": ("vv", "ai", "ai", lambda r, F, f: -f * np.einsum("al,el->ae", r, F)),
+    "Fmi_r1fia": ("oo", "ai", "ai", lambda r, F, f: f * np.einsum("dm,di->mi", F, r)),
+    "Wkbij_r2Fkc": ("ijka", "abij", "ai", lambda r, F, f: -f * np.einsum("cbij,ck->ijkb", r, F)),
+    "Wlkjd_r1abij": ("ijka", "ai", "abij", lambda r, V, f: f * np.einsum("cdlk,cj->lkjd", V, r)),
 }
 
 

@@ -202,6 +202,20 @@ class Oracle:
         assert rc == 0, rc
         return dict(T2_1=T2_1, T1_2=T1_2, T2_2=T2_2, E2=E2.value, E3=E3.value, iters=it.value)
 
+    def grcpsd(self):
+        """grCPS(D) ground state: per order (T1, T2), E^(2..4), DIIS iterations"""
+        s = self.s
+        l1, l2 = s.r1_len(1), s.r2_len(1)
+        T = np.zeros(3 * (l1 + l2))
+        E = np.zeros(3)
+        it = (I64 * 3)()
+        rc = lib().o_grcpsd_ground(ctypes.byref(self.osys), ctypes.byref(self.oint), ctypes.byref(self.par),
+                                   ptr(T), ptr(E), it)
+        assert rc == 0, rc
+        T = T.reshape(3, l1 + l2)
+        return dict(T1=[T[k, :l1] for k in range(3)], T2=[T[k, l1:] for k in range(3)], E=E,
+                    iters=list(it))
+
     def ground3(self, g):
         """third order ground state (run3.f90) from the T of ground()"""
         s = self.s

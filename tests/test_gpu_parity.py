@@ -94,6 +94,39 @@ def test_kernel_matches_oracle(name, nirrep):
     np.testing.assert_allclose(host(to), ref, rtol=0, atol=1e-12, err_msg=name)
 
 
+@pytest.mark.parametrize("nirrep", [1, 4, 8])
+@pytest.mark.parametrize("name,kind", [("Wmbej_r1abci", 23), ("Wmbej_r1ijka", 22), ("c2_r2Fae", 22)])
+def test_streaming_kernels_ran_and_match_oracle(name, kind, nirrep):
+    """The row-dot (kind 23) and short-K (kind 22) kernels are the ones that
+    ran for these shapes (their timing records), and they match the oracle."""
+    rng = np.random.default_rng(17 + nirrep)
+    s = synth.System(nmo=16 if nirrep < 8 else 24, nocc_a=3, nocc_b=2, nirrep=nirrep, seed=2)
+    api.init(s.nirrep, s.dirprd)
+    of.set_symmetry(s.nirrep, s.dirprd)
+    sym = s.sym
+    lo, la, lb = ks.KERNELS[name][:3]
+    symR = min(2, nirrep)
+    sa, sb = (symR, 1) if not name.startswith("c2_r2") else (1, symR)
+    so = sym.dp(sa, sb)
+    po, io = ks.pops_of(lo, s.popo, s.popv)
+    pa, ia = ks.pops_of(la, s.popo, s.popv)
+    pb, ib = ks.pops_of(lb, s.popo, s.popv)
+    va = rng.standard_normal(sym.idsymsoc(sa, pa[0], pa[1], ia[0], pa[2], pa[3], ia[1]))
+    vb = rng.standard_normal(sym.idsymsoc(sb, pb[0], pb[1], ib[0], pb[2], pb[3], ib[1]))
+    vo = rng.standard_normal(sym.idsymsoc(so, po[0], po[1], io[0], po[2], po[3], io[1]))
+    ref = vo.copy()
+    assert of.call_kernel(name, of.opt(po, io, so, ref), of.opt(pa, ia, sa, va), of.opt(pb, ib, sb, vb), 0.8) == 0
+    ta, tb, to = dev(va), dev(vb), dev(vo)
+    api.contract_timing(True)
+    try:
+        api.kernel(name, api.opt(po, io, so, to), api.opt(pa, ia, sa, ta), api.opt(pb, ib, sb, tb), 0.8)
+        _, _, kinds, _ = api.contract_records()
+    finally:
+        api.contract_timing(False)
+    assert kind in set(int(k) for k in kinds), (name, sorted(set(int(k) for k in kinds)))
+    np.testing.assert_allclose(host(to), ref, rtol=0, atol=1e-12, err_msg=name)
+
+
 def _run_both(s, batch_roots=1, **kw):
     api.init(s.nirrep, s.dirprd)
     ints = api.DeviceIntegrals(s)
@@ -163,6 +196,36 @@ def test_cis_nonsymmetric_matches_oracle(nirrep):
         np.testing.assert_allclose(np.sign(np.dot(a, dr)) * a, dr, rtol=0, atol=1e-8)
 
 
+@pytest.mark.parametrize("lowest", [0, 1])
+@pytest.mark.parametrize("nirrep", [1, 4, 8])
+def test_cisdoo_matches_oracle(nirrep, lowest):
+    """CIS(D-infinity) (src/CISdoo.SD.SF/run.f90): the non-symmetric (R1, R2)
+    problem; roots and vectors against the oracle, both converged to a
+    residual of 1e-12, every Ritz step through the general eigen-solve."""
+    s = small(nirrep, roots=2) if nirrep < 8 else synth.System(nmo=24, nocc_a=4, nocc_b=2, nirrep=8, seed=3, roots=2)
+    s.run_opts["davidson_conv"] = 12
+    s.run_opts["lowest"] = lowest
+    ints, sc, par, orc = _run_both(s)
+    api.davidson_stats(reset=True)
+    om, R, it = api.cisdoo_run(s, sc, ints, par)
+    nonsym, imag = api.davidson_stats()
+    assert nonsym > 0 and imag == 0
+    oom, oR, oit = orc.cisdoo()
+    np.testing.assert_allclose(om, oom, rtol=0, atol=1e-10)
+    assert abs(it - oit) <= 1
+    Rg = host(R)
+    off, k = 0, 0
+    for h in range(8):
+        n = s.r1_len(h + 1) + s.r2_len(h + 1)
+        for _ in range(int(s.estate_sym[h])):
+            a, b = Rg[off:off + n], oR[off:off + n]
+            sgn = np.sign(np.dot(a, b))
+            np.testing.assert_allclose(sgn * a, b, rtol=0, atol=1e-9)
+            off += n
+            k += 1
+    assert k == len(om) > 0
+
+
 @pytest.mark.parametrize("nirrep", [1, 4])
 def test_ground_and_intermediates_match_oracle(nirrep):
     s = small(nirrep)
@@ -194,6 +257,22 @@ def test_ground_third_order_matches_oracle(nirrep):
     np.testing.assert_allclose(host(g3["T2_3"]), og3["T2_3"], rtol=0, atol=1e-11)
     np.testing.assert_allclose(host(g3["T1_3"]), og3["T1_3"], rtol=0, atol=1e-8)
     assert g3["iters"] == og3["iters"]
+
+
+@pytest.mark.parametrize("nirrep", [1, 4, 8])
+def test_grcpsd_ground_matches_oracle(nirrep):
+    """grCPS(D) (src/grCPSd.SF): the three orders' (T1, T2) and E^(2..4)
+    against the oracle, the same DIIS iteration counts."""
+    s = small(nirrep) if nirrep < 8 else synth.System(nmo=24, nocc_a=4, nocc_b=2, nirrep=8, seed=3)
+    s.run_opts["diis_max_err"] = 1e-10
+    ints, sc, par, orc = _run_both(s)
+    g = api.grcpsd_ground(s, sc, ints, par)
+    og = orc.grcpsd()
+    np.testing.assert_allclose(g["E"], og["E"], rtol=0, atol=1e-11)
+    for k in range(3):
+        np.testing.assert_allclose(host(g["T1"][k]), og["T1"][k], rtol=0, atol=1e-9, err_msg=str(k))
+        np.testing.assert_allclose(host(g["T2"][k]), og["T2"][k], rtol=0, atol=1e-9, err_msg=str(k))
+    assert g["iters"] == og["iters"]
 
 
 @pytest.mark.parametrize("batch", [0, 1])

@@ -160,3 +160,19 @@ def test_cisdoo_matches_dense_eigenvalues(nirrep):
         off += nr * n
         k += nr
     assert k == len(om) and k > 0
+
+
+@pytest.mark.parametrize("nirrep", [1, 4])
+def test_grcpsd_ground_matches_dense(nirrep):
+    """grCPS(D) (src/grCPSd.SF): every order's coupled (T1, T2) and the
+    energies E^(2), E^(3), E^(4) against the exact dense solution; the DIIS
+    loops run to 1e-12."""
+    s = small(nirrep)
+    orc = of.Oracle(s, diis_max_err=1e-12, diis_cyc=300)
+    g = orc.grcpsd()
+    d = dp.DenseSystem(s).grcpsd()
+    for k in range(3):
+        np.testing.assert_allclose(vo_dense(s, g["T1"][k], 1), d["T1"][k], rtol=0, atol=1e-9, err_msg=str(k))
+        np.testing.assert_allclose(vvoo_dense(s, g["T2"][k], 1), d["T2"][k], rtol=0, atol=1e-9, err_msg=str(k))
+    np.testing.assert_allclose(g["E"], d["E"], rtol=0, atol=1e-10)
+    assert np.all(np.abs(d["E"]) > 1e-8) and np.abs(d["T1"][0]).max() > 1e-6

@@ -134,6 +134,16 @@ KSPEC = {
     "Wmbej_r1abci": ("424", "ba", "febm", "fj", "embj", 0), "Wmbej_r1ijka": ("424", "ba", "nmje", "bn", "embj", 0),
     "Wmnij_r1ijka": ("424", "ba", "mnie", "ej", "mnij", 2),
     "Wmnij_r2abij": ("444", "ba", "efmn", "efij", "mnij", 0),
+    "Wkbij_r1iabj": ("424", "ba", "ckbj", "ci", "ijkb", 1), "Wabdj_r1abcd": ("424", "ba", "abdc", "cj", "abdj", 0),
+    "Wkbij_r1Uklij": ("424", "ba", "klij", "bl", "ijkb", 0), "Fme_r1abij": ("422", "ba", "efmn", "fn", "em", 0),
+    "c1_r2Fme": ("422", "ab", "aeim", "em", "ai", 0),
+    "c1d_l1Wibaj": ("422", "ba", "aibj", "bj", "ai", 0),
+    "c1d_l1fab": ("222", "ba", "ba", "bi", "ai", 0),
+    "c1d_l1fij": ("222", "ab", "aj", "ij", "ai", 0),
+    "Fae_r1fia": ("222", "ab", "al", "el", "ae", 0),
+    "Fmi_r1fia": ("222", "ba", "dm", "di", "mi", 0),
+    "Wkbij_r2Fkc": ("424", "ab", "cbij", "ck", "ijkb", 0),
+    "Wlkjd_r1abij": ("424", "ba", "cdlk", "cj", "lkjd", 0),
 }
 
 
