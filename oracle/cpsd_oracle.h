@@ -220,6 +220,15 @@ int o_cpsd_ground(const o_system *s, const o_integrals *I, const o_params *p,
  * iterations */
 int o_grcpsd_ground(const o_system *s, const o_integrals *I, const o_params *p, double *T, double *E,
                     i64 *iters);
+/* excited-state grCPS(D) (src/EE-grCPSd.SF/run.f90) from the grCPS(D)
+ * amplitudes T (orders 1, 2 used; layout of o_grcpsd_ground) and the
+ * CIS(D-infinity) roots omega / R0 (layout of o_cisdoo_run): w[3k..3k+2] =
+ * w^(1), w^(2), w^(3) of root k; Lout (nullable) the normalised left vectors
+ * (R0's layout), Rout (nullable) R^(1) of every root then R^(2) of every
+ * root; *iters the DIIS iterations summed */
+int o_eegrcpsd_roots(const o_system *s, const o_integrals *I, const o_params *p, const double *T,
+                     const double *omega, const double *R0, double *w, double *Lout, double *Rout,
+                     i64 *iters);
 int o_cpsd_ground3(const o_system *s, const o_integrals *I, const o_params *p,
                    const double *T2_1, const double *T1_2, const double *T2_2,
                    double *T1_3, double *T2_3, double *E4, i64 *diis_iters);

@@ -575,6 +575,448 @@ int o_grcpsd_ground(const o_system *s, const o_integrals *I, const o_params *p, 
     return rc;
 }
 
+/* ---------------- EE-grCPS(D) (src/EE-grCPSd.SF) ----------------
+ * Per root of the CIS(D-infinity) problem (R^(0), w0): the left vector L
+ * (calEigenCISDoo.f90: L1 by DIIS on L1 [Ass - Asd (Add - w)^-1 Ads - w] = 0,
+ * L2 = L1 Asd (w - Add)^-1, <L|R> = 1), w^(1) = L J^(1) R^(0); then orders
+ * 1, 2 (run1.f90, run2.f90): (A0 - w0) R^(n) = sum_k w^(k) R^(n-k) - C^(n)
+ * by the DIIS solver with R orthogonal to L (solver.f90), w^(n+1) =
+ * L C^(n+1) with C^(n) of calE_C.f90. */
+static double *opt_new(o_opt *t, const i64 *p0, const i64 *p1, const i64 *p2, const i64 *p3, i64 i0, i64 i1,
+                       i64 sym)
+{
+    o_opt_view(t, p0, p1, p2, p3, i0, i1, sym, NULL);
+    t->arr = zalloc(t->len);
+    return t->arr;
+}
+
+/* one J^(k) set: Foo, Fvv, Fov, Woooo, Wooov, Wovoo, Wovvo (allocate_mem.f90:54-81) */
+typedef struct {
+    o_opt Foo, Fvv, Fov, Woooo, Wooov, Wovoo, Wovvo;
+} ee_J;
+
+static void ee_J_alloc(const o_system *s, ee_J *J)
+{
+    const i64 *o = s->popo, *V = s->popv;
+    opt_new(&J->Foo, o, o, Z, Z, 1, 1, 1);
+    opt_new(&J->Fvv, V, V, Z, Z, 1, 1, 1);
+    opt_new(&J->Fov, V, o, Z, Z, 1, 1, 1);
+    opt_new(&J->Woooo, o, o, o, o, 0, 0, 1);
+    opt_new(&J->Wooov, o, o, o, V, 0, 1, 1);
+    opt_new(&J->Wovoo, o, o, o, V, 0, 1, 1);
+    opt_new(&J->Wovvo, V, o, V, o, 1, 1, 1);
+}
+static void ee_J_free(ee_J *J)
+{
+    free(J->Foo.arr); free(J->Fvv.arr); free(J->Fov.arr); free(J->Woooo.arr);
+    free(J->Wooov.arr); free(J->Wovoo.arr); free(J->Wovvo.arr);
+}
+
+/* the [V,T] part of calJ2 / calJ3 (calJ.f90:14-95, 104-170) */
+static int ee_J_VT(const ints_t *v, ee_J *J, const o_opt *t1, const o_opt *t2)
+{
+    int rc = o_Fmi_r1ijka(&J->Foo, t1, &v->ijka, 1.0);
+    if (rc == O_OK) rc = o_Fmi_r2abij(&J->Foo, t2, &v->abij, 1.0);
+    if (rc == O_OK) rc = o_Fae_r1abci(&J->Fvv, t1, &v->abci, 1.0);
+    if (rc == O_OK) rc = o_Fae_r2abij(&J->Fvv, t2, &v->abij, 1.0);
+    if (rc == O_OK) rc = o_Fme_r1abij(&J->Fov, t1, &v->abij, 1.0);
+    if (rc == O_OK) rc = o_Wkbij_r1iabj(&J->Wovoo, t1, &v->iabj, -1.0);
+    if (rc == O_OK) rc = o_Wkbij_r1Uklij(&J->Wovoo, t1, &v->ijkl, 1.0);
+    if (rc == O_OK) rc = o_Wkbij_r2ijka(&J->Wovoo, t2, &v->ijka, 1.0);
+    if (rc == O_OK) rc = o_Wkbij_r2abci(&J->Wovoo, t2, &v->abci, 1.0);
+    if (rc == O_OK) rc = o_Wmbej_r1ijka(&J->Wovvo, t1, &v->ijka, 1.0);
+    if (rc == O_OK) rc = o_Wmbej_r1abci(&J->Wovvo, t1, &v->abci, 1.0);
+    if (rc == O_OK) rc = o_Wmbej_r2abij(&J->Wovvo, t2, &v->abij, 2.0);
+    if (rc == O_OK) rc = o_Wmnij_r1ijka(&J->Woooo, t1, &v->ijka, 1.0);
+    if (rc == O_OK) rc = o_Wmnij_r2abij(&J->Woooo, t2, &v->abij, 1.0);
+    if (rc == O_OK) rc = o_Wlkjd_r1abij(&J->Wooov, t1, &v->abij, 1.0);
+    return rc;
+}
+
+/* the [[V,T^(1)],T^(1)] part of calJ3 (calJ.f90:172-218) */
+static int ee_J_VTT(const o_system *s, const ints_t *v, ee_J *J, const o_opt *t1, const o_opt *t2)
+{
+    const i64 *o = s->popo, *V = s->popv;
+    o_opt w;
+    opt_new(&w, V, o, Z, Z, 1, 1, 1);
+    int rc = o_Fme_r1abij(&w, t1, &v->abij, 1.0);
+    if (rc == O_OK) rc = o_Fmi_r1fia(&J->Foo, t1, &w, 1.0);
+    if (rc == O_OK) rc = o_Fae_r1fia(&J->Fvv, t1, &w, 1.0);
+    if (rc == O_OK) rc = o_Wkbij_r2Fkc(&J->Wovoo, t2, &w, -1.0);
+    free(w.arr);
+    if (rc != O_OK) return rc;
+    opt_new(&w, o, o, o, V, 0, 1, 1);
+    rc = o_Wlkjd_r1abij(&w, t1, &v->abij, 1.0);
+    if (rc == O_OK) rc = o_Wmbej_r1ijka(&J->Wovvo, t1, &w, 1.0);
+    if (rc == O_OK) rc = o_Wmnij_r1ijka(&J->Woooo, t1, &w, 0.5);
+    if (rc == O_OK) rc = o_Wkbij_r2ijka(&J->Wovoo, t2, &w, 1.0);
+    free(w.arr);
+    if (rc != O_OK) return rc;
+    opt_new(&w, o, o, o, o, 0, 0, 1);
+    rc = o_Wmnij_r1ijka(&w, t1, &v->ijka, 1.0);
+    if (rc == O_OK) rc = o_Wmnij_r2abij(&w, t2, &v->abij, 1.0);
+    if (rc == O_OK) rc = o_Wkbij_r1Uklij(&J->Wovoo, t1, &w, 1.0);
+    free(w.arr);
+    if (rc != O_OK) return rc;
+    opt_new(&w, V, o, V, o, 1, 1, 1);
+    rc = o_Wmbej_r1abci(&w, t1, &v->abci, 1.0);
+    if (rc == O_OK) rc = o_Wkbij_r1iabj(&J->Wovoo, t1, &w, -0.5);
+    free(w.arr);
+    return rc;
+}
+
+/* calC_J2R / calC_J3R (calC_JR.f90:3-29, 32-58) */
+static int ee_CJR(const ee_J *J, o_opt *C1, o_opt *C2, const o_opt *r1, const o_opt *r2, double f)
+{
+    int rc = o_c2_r1ijka(C2, r1, &J->Wovoo, f);
+    if (rc == O_OK) rc = o_c1_r1iabj(C1, r1, &J->Wovvo, f);
+    if (rc == O_OK) rc = o_c2_r2Wmbej(C2, r2, &J->Wovvo, f);
+    if (rc == O_OK) rc = o_c2_r2Wmnij(C2, r2, &J->Woooo, f);
+    if (rc == O_OK) rc = o_c1_r1Fmi(C1, r1, &J->Foo, f);
+    if (rc == O_OK) rc = o_c2_r2Fmi(C2, r2, &J->Foo, f);
+    if (rc == O_OK) rc = o_c1_r1Fae(C1, r1, &J->Fvv, f);
+    if (rc == O_OK) rc = o_c2_r2Fae(C2, r2, &J->Fvv, f);
+    if (rc == O_OK) rc = o_c1_r2ijka(C1, r2, &J->Wooov, f);
+    if (rc == O_OK) rc = o_c1_r2Fme(C1, r2, &J->Fov, f);
+    return rc;
+}
+
+/* calC_VTR.f90:3-78: C += f <u|[[V,T],R]|0> without intermediates */
+static int ee_VTR(const o_system *s, const ints_t *v, o_opt *C1, o_opt *C2, const o_opt *t1, const o_opt *t2,
+                  const o_opt *r1, const o_opt *r2, i64 symR, double f)
+{
+    const i64 *o = s->popo, *V = s->popv;
+    o_opt w;
+    int rc;
+    opt_new(&w, o, o, Z, Z, 1, 1, symR);
+    rc = o_Fmi_r2abij(&w, r2, &v->abij, 1.0);
+    if (rc == O_OK) rc = o_c1_r1Fmi(C1, t1, &w, f);
+    free(w.arr);
+    if (rc != O_OK) return rc;
+    opt_new(&w, o, o, o, V, 0, 1, symR);
+    rc = o_Wkbij_r1iabj(&w, r1, &v->iabj, -1.0);
+    if (rc == O_OK) rc = o_Wkbij_r2abci(&w, r2, &v->abci, 1.0);
+    if (rc == O_OK) rc = o_c2_r1ijka(C2, t1, &w, f);
+    free(w.arr);
+    if (rc != O_OK) return rc;
+    opt_new(&w, V, V, V, o, 0, 1, 1);
+    rc = o_Wabdj_r1abcd(&w, t1, &v->abcd, 1.0);
+    if (rc == O_OK) rc = o_c2_r1abci(C2, r1, &w, f);
+    free(w.arr);
+    if (rc != O_OK) return rc;
+    opt_new(&w, o, o, o, o, 0, 0, symR);
+    rc = o_Wmnij_r2abij(&w, r2, &v->abij, 1.0);
+    if (rc == O_OK) rc = o_Wmnij_r1ijka(&w, r1, &v->ijka, 1.0);
+    if (rc == O_OK) rc = o_c2_r2Wmnij(C2, t2, &w, f);
+    free(w.arr);
+    if (rc != O_OK) return rc;
+    opt_new(&w, V, o, V, o, 1, 1, symR);
+    rc = o_Wmbej_r1abci(&w, r1, &v->abci, 1.0);
+    if (rc == O_OK) rc = o_c2_r2Wmbej(C2, t2, &w, f);
+    free(w.arr);
+    if (rc != O_OK) return rc;
+    opt_new(&w, o, o, Z, Z, 1, 1, symR);
+    rc = o_Fmi_r1ijka(&w, r1, &v->ijka, 1.0);
+    if (rc == O_OK) rc = o_Fmi_r2abij(&w, r2, &v->abij, 1.0);
+    if (rc == O_OK) rc = o_c2_r2Fmi(C2, t2, &w, f);
+    free(w.arr);
+    if (rc != O_OK) return rc;
+    opt_new(&w, V, V, Z, Z, 1, 1, symR);
+    rc = o_Fae_r1abci(&w, r1, &v->abci, 1.0);
+    if (rc == O_OK) rc = o_Fae_r2abij(&w, r2, &v->abij, 1.0);
+    if (rc == O_OK) rc = o_c2_r2Fae(C2, t2, &w, f);
+    free(w.arr);
+    return rc;
+}
+
+/* calC_VTTR.f90:3-86: C2 += f <u|[[[V,T],T],R]|0> */
+static int ee_VTTR(const o_system *s, const ints_t *v, o_opt *C2, const o_opt *t1, const o_opt *t2,
+                   const o_opt *r1, const o_opt *r2, i64 symR, double f)
+{
+    const i64 *o = s->popo, *V = s->popv;
+    o_opt a, b, c;
+    int rc;
+    opt_new(&a, V, o, Z, Z, 1, 1, symR);  /* Gld = V(kl,cd) r(c,k) */
+    rc = o_Fme_r1abij(&a, r1, &v->abij, 1.0);
+    opt_new(&b, V, V, Z, Z, 1, 1, symR);  /* F(a,d) -= Gld t(a,l) */
+    if (rc == O_OK) rc = o_Fae_r1fia(&b, t1, &a, 1.0);
+    if (rc == O_OK) rc = o_c2_r2Fae(C2, t2, &b, f);
+    free(b.arr);
+    opt_new(&b, o, o, Z, Z, 1, 1, symR);  /* F(l,i) = Gld t(d,i) + Fld r(d,i) */
+    if (rc == O_OK) rc = o_Fmi_r1fia(&b, t1, &a, 1.0);
+    opt_new(&c, V, o, Z, Z, 1, 1, 1);     /* F(l,d) = V(kl,cd) t(c,k) */
+    if (rc == O_OK) rc = o_Fme_r1abij(&c, t1, &v->abij, 1.0);
+    if (rc == O_OK) rc = o_Fmi_r1fia(&b, r1, &c, 1.0);
+    if (rc == O_OK) rc = o_c2_r2Fmi(C2, t2, &b, f);
+    free(a.arr); free(b.arr); free(c.arr);
+    if (rc != O_OK) return rc;
+    /* 0.5 V(kl,cd) r(c,i) t(d,j) t(ab,kl) */
+    opt_new(&a, o, o, o, V, 0, 1, symR);
+    rc = o_Wlkjd_r1abij(&a, r1, &v->abij, 1.0);
+    opt_new(&b, o, o, o, o, 0, 0, symR);
+    if (rc == O_OK) rc = o_Wmnij_r1ijka(&b, t1, &a, 1.0);
+    if (rc == O_OK) rc = o_c2_r2Wmnij(C2, t2, &b, f);
+    free(a.arr); free(b.arr);
+    if (rc != O_OK) return rc;
+    /* W(kb,ij) = -0.5 W(kl,ij) t(b,l) + W(kb,cj) r(c,i) + W(kl,id) t(db,lj) */
+    opt_new(&a, o, o, o, V, 0, 1, symR);
+    opt_new(&b, o, o, o, o, 0, 0, symR);
+    rc = o_Wmnij_r2abij(&b, r2, &v->abij, 1.0);
+    if (rc == O_OK) rc = o_Wmnij_r1ijka(&b, r1, &v->ijka, 1.0);
+    if (rc == O_OK) rc = o_Wkbij_r1Uklij(&a, t1, &b, 0.5);
+    free(b.arr);
+    opt_new(&b, V, o, V, o, 1, 1, 1);
+    if (rc == O_OK) rc = o_Wmbej_r1abci(&b, t1, &v->abci, 1.0);
+    if (rc == O_OK) rc = o_Wkbij_r1iabj(&a, r1, &b, -1.0);
+    free(b.arr);
+    opt_new(&b, o, o, o, V, 0, 1, symR);
+    if (rc == O_OK) rc = o_Wlkjd_r1abij(&b, r1, &v->abij, 1.0);
+    if (rc == O_OK) rc = o_Wkbij_r2ijka(&a, t2, &b, 1.0);
+    free(b.arr);
+    if (rc == O_OK) rc = o_c2_r1ijka(C2, t1, &a, f);
+    free(a.arr);
+    return rc;
+}
+
+/* calC2_VR2.f90:3-24: C2 += f <ab,ij|[V,R2]|0> */
+static int ee_C2VR2(const ints_t *v, o_opt *C2, const o_opt *r2, double f)
+{
+    int rc = o_c2_r2Wmbej(C2, r2, &v->iabj, f);
+    if (rc == O_OK) rc = o_c2_r2Wmnij(C2, r2, &v->ijkl, f);
+    if (rc == O_OK) rc = o_c2_r2abcd(C2, r2, &v->abcd, f);
+    return rc;
+}
+
+/* calC1_VMP2R1.f90:9-30: C1 -= f <a,i|[[V,MP2t],R1]|0>, Wkaci - iabj formed
+ * in place and restored */
+static int ee_VMP2R1(gr_ctx *g, o_opt *C1, const o_opt *r1, double f)
+{
+    for (i64 k = 0; k < g->wk.len; k++) g->wk.arr[k] -= g->v->iabj.arr[k];
+    int rc = o_c1_r1iabj(C1, r1, &g->wk, -f);
+    for (i64 k = 0; k < g->wk.len; k++) g->wk.arr[k] += g->v->iabj.arr[k];
+    if (rc == O_OK) rc = o_c1_r1Fmi(C1, r1, &g->fli, f);
+    if (rc == O_OK) rc = o_c1_r1Fae(C1, r1, &g->fad, f);
+    return rc;
+}
+
+/* calE_C.f90:4-66: C^(n) of one root (C, R^(k) as (R1, R2) vectors of irrep
+ * symR; T^(1), T^(2) of irrep 1) */
+static int ee_calE_C(gr_ctx *g, const ee_J *J2, const ee_J *J3, const double *T, i64 lt, double *C,
+                     double *const *R, i64 symR, i64 l1, int order)
+{
+    const o_system *s = g->s;
+    const i64 *o = s->popo, *V = s->popv;
+    const ints_t *v = g->v;
+    const i64 g1 = o_irpdso(1, V, o, 1);
+    o_opt c1, c2, r1, r2, t1, t2;
+    o_opt_view(&c1, V, o, Z, Z, 1, 1, symR, C);
+    o_opt_view(&c2, V, V, o, o, 0, 0, symR, C + l1);
+    memset(C, 0, sizeof(double) * (size_t)(c1.len + c2.len));
+    o_opt_view(&r2, V, V, o, o, 0, 0, symR, R[order - 1] + l1);
+    int rc = ee_C2VR2(v, &c2, &r2, 1.0);
+    if (order == 1 || rc != O_OK) return rc;
+    o_opt_view(&r1, V, o, Z, Z, 1, 1, symR, R[order - 2]);
+    o_opt_view(&r2, V, V, o, o, 0, 0, symR, R[order - 2] + l1);
+    o_opt_view(&t1, V, o, Z, Z, 1, 1, 1, (double *)T);
+    o_opt_view(&t2, V, V, o, o, 0, 0, 1, (double *)T + g1);
+    rc = ee_VMP2R1(g, &c1, &r1, 1.0);
+    if (rc == O_OK) rc = ee_CJR(J2, &c1, &c2, &r1, &r2, 1.0);
+    if (rc == O_OK) rc = ee_VTR(s, v, &c1, &c2, &t1, &t2, &r1, &r2, symR, 1.0);
+    if (order == 2 || rc != O_OK) return rc;
+    o_opt_view(&r1, V, o, Z, Z, 1, 1, symR, R[0]);
+    o_opt_view(&r2, V, V, o, o, 0, 0, symR, R[0] + l1);
+    rc = ee_CJR(J3, &c1, &c2, &r1, &r2, 1.0);
+    o_opt_view(&t1, V, o, Z, Z, 1, 1, 1, (double *)T + lt);
+    o_opt_view(&t2, V, V, o, o, 0, 0, 1, (double *)T + lt + g1);
+    if (rc == O_OK) rc = ee_VTR(s, v, &c1, &c2, &t1, &t2, &r1, &r2, symR, 1.0);
+    o_opt_view(&t1, V, o, Z, Z, 1, 1, 1, (double *)T);
+    o_opt_view(&t2, V, V, o, o, 0, 0, 1, (double *)T + g1);
+    if (rc == O_OK) rc = ee_VTTR(s, v, &c2, &t1, &t2, &r1, &r2, symR, 1.0);
+    return rc;
+}
+
+/* orthogonalR2L.f90:5-21: R -= (<L|R> / |L|) L (the reference divides by the
+ * norm, not its square) */
+static void ee_orth(double *R, const double *L, i64 n)
+{
+    double nrm = o_dnrm2(n, L), dot = o_ddot(n, L, R);
+    o_daxpy(n, -dot / nrm, L, R);
+}
+
+int o_eegrcpsd_roots(const o_system *s, const o_integrals *I, const o_params *p, const double *T,
+                     const double *omega, const double *R0, double *w, double *Lout, double *Rout,
+                     i64 *iters)
+{
+    ints_t v;
+    ints_view(s, I, &v);
+    const i64 *o = s->popo, *V = s->popv;
+    const i64 g1 = o_irpdso(1, V, o, 1), lt = g1 + o_idsymsoc(1, V, V, 0, o, o, 0);
+    gr_ctx g;
+    g.s = s;
+    g.v = &v;
+    g.l1 = g1;
+    g.l2 = lt - g1;
+    double *mp2 = zalloc(g.l2), *fo = zalloc(o_irpdso(1, o, o, 1)), *fv = zalloc(o_irpdso(1, V, V, 1));
+    double *wk = zalloc(v.iabj.len);
+    o_opt mp2t;
+    o_opt_view(&mp2t, V, V, o, o, 0, 0, 1, mp2);
+    o_opt_view(&g.fli, o, o, Z, Z, 1, 1, 1, fo);
+    o_opt_view(&g.fad, V, V, Z, Z, 1, 1, 1, fv);
+    o_opt_view(&g.wk, V, o, V, o, 1, 1, 1, wk);
+    /* run.f90:41-60 */
+    o_denomT2(mp2, I->abij, I->eorb, V, o, 1, 0);
+    memcpy(wk, I->iabj, sizeof(double) * (size_t)v.iabj.len);
+    int rc = o_Fmi_r2abij(&g.fli, &mp2t, &v.abij, -1.0);
+    if (rc == O_OK) rc = o_Fae_r2abij(&g.fad, &mp2t, &v.abij, -1.0);
+    if (rc == O_OK) rc = o_Wmbej_r2abij(&g.wk, &mp2t, &v.abij, 2.0);
+    i64 nroot = 0, rlen = 0, itsum = 0;
+    for (i64 h = 0; h < s->nirrep; h++) {
+        nroot += p->estate_sym[h];
+        rlen += p->estate_sym[h] * (o_irpdso(h + 1, V, o, 1) + o_idsymsoc(h + 1, V, V, 0, o, o, 0));
+    }
+    /* per root: R^(0..2), L, C^(n) */
+    double *Rall = zalloc(3 * rlen), *Lall = zalloc(rlen), *Call = zalloc(rlen);
+    memcpy(Rall, R0, sizeof(double) * (size_t)rlen);
+    /* calEigenCISDoo for every root (run.f90:64-69) */
+    i64 off = 0, k = 0;
+    for (i64 sym = 1; sym <= s->nirrep && rc == O_OK; sym++) {
+        const i64 l1 = o_irpdso(sym, V, o, 1), l2 = o_idsymsoc(sym, V, V, 0, o, o, 0), n = l1 + l2;
+        double *oed1 = zalloc(l1), *demw = zalloc(l2), *c = zalloc(n);
+        o_eorb_diff1(oed1, I->eorb, V, o, sym);
+        for (i64 r = 0; r < p->estate_sym[sym - 1] && rc == O_OK; r++, k++, off += n) {
+            const double wv = omega[k];
+            double *R = Rall + off, *L = Lall + off;
+            double nrm = o_dnrm2(n, R);
+            if (fabs(nrm - 1.0) > p->diis_max_err) /* dscal by 1/norm */
+                for (i64 q = 0; q < n; q++) R[q] *= 1.0 / nrm;
+            o_eorb_diff2(demw, I->eorb, V, o, sym, 0);
+            for (i64 q = 0; q < l2; q++) demw[q] = 1.0 / (wv - demw[q]);
+            o_opt L1, L2, C1, R1, R2;
+            o_opt_view(&L1, V, o, Z, Z, 1, 1, sym, L);
+            o_opt_view(&L2, V, V, o, o, 0, 0, sym, L + l1);
+            o_opt_view(&C1, V, o, Z, Z, 1, 1, sym, c);
+            o_opt_view(&R1, V, o, Z, Z, 1, 1, sym, R);
+            o_opt_view(&R2, V, V, o, o, 0, 0, sym, R + l1);
+            memcpy(L, R, sizeof(double) * (size_t)l1);
+            o_diis dst;
+            o_diis_init(&dst, l1, p->diis_dim);
+            i64 iter = 0;
+            for (;;) { /* calEigenCISDoo.f90:94-140 */
+                iter++;
+                double d = 1.0 / o_ddot(l1, L, R);
+                for (i64 q = 0; q < l1; q++) L[q] *= d;
+                double err = o_diis_step(&dst, iter, L);
+                d = 1.0 / o_ddot(l1, L, R);
+                for (i64 q = 0; q < l1; q++) L[q] *= d;
+                if (fabs(err) < p->diis_max_err && iter > 1) break;
+                if (iter > p->diis_cyc) break;
+                for (i64 q = 0; q < l1; q++) c[q] = -wv * L[q];
+                rc = o_c1d_l1Wibaj(&C1, &L1, &g.wk, 1.0);
+                if (rc == O_OK) rc = o_c1d_l1fab(&C1, &L1, &g.fad, 1.0);
+                if (rc == O_OK) rc = o_c1d_l1fij(&C1, &L1, &g.fli, 1.0);
+                memset(L + l1, 0, sizeof(double) * (size_t)l2);
+                if (rc == O_OK) rc = o_c2_r1ijka(&L2, &L1, &v.ijka, 1.0); /* calL2d_VL1 */
+                if (rc == O_OK) rc = o_c2_r1abci(&L2, &L1, &v.abci, 1.0);
+                for (i64 q = 0; q < l2; q++) L[l1 + q] *= demw[q];
+                if (rc == O_OK) rc = o_c1_r2ijka(&C1, &L2, &v.ijka, 1.0); /* calL1d_VL2 */
+                if (rc == O_OK) rc = o_c1_r2abci(&C1, &L2, &v.abci, 1.0);
+                if (rc != O_OK) break;
+                o_denomT1(L, c, I->eorb, V, o, sym);
+            }
+            o_diis_free(&dst);
+            itsum += iter;
+            if (rc != O_OK) break;
+            /* L2 = L1 Asd (w - Add)^-1, L /= 1 + <L2|R2> (calEigenCISDoo.f90:142-157) */
+            memset(L + l1, 0, sizeof(double) * (size_t)l2);
+            rc = o_c2_r1ijka(&L2, &L1, &v.ijka, 1.0);
+            if (rc == O_OK) rc = o_c2_r1abci(&L2, &L1, &v.abci, 1.0);
+            for (i64 q = 0; q < l2; q++) L[l1 + q] *= demw[q];
+            double nl = 1.0 / (1.0 + o_ddot(l2, L + l1, R + l1));
+            for (i64 q = 0; q < n; q++) L[q] *= nl;
+            /* w^(1) = L J^(1) R^(0) (calEigenCISDoo.f90:170-186) */
+            double *Rk[3] = {R, NULL, NULL};
+            if (rc == O_OK) rc = ee_calE_C(&g, NULL, NULL, T, lt, Call + off, Rk, sym, l1, 1);
+            w[3 * k] = o_ddot(n, L, Call + off);
+        }
+        free(oed1); free(demw); free(c);
+    }
+    ee_J J2, J3;
+    ee_J_alloc(s, &J2);
+    ee_J_alloc(s, &J3);
+    if (rc == O_OK) { /* calJ2 / calJ3 (run.f90:72-73) */
+        o_opt t1, t2;
+        o_opt_view(&t1, V, o, Z, Z, 1, 1, 1, (double *)T + lt);
+        o_opt_view(&t2, V, V, o, o, 0, 0, 1, (double *)T + lt + g1);
+        rc = ee_J_VT(&v, &J3, &t1, &t2);
+        o_opt_view(&t1, V, o, Z, Z, 1, 1, 1, (double *)T);
+        o_opt_view(&t2, V, V, o, o, 0, 0, 1, (double *)T + g1);
+        if (rc == O_OK) rc = ee_J_VT(&v, &J2, &t1, &t2);
+        if (rc == O_OK) rc = ee_J_VTT(s, &v, &J3, &t1, &t2);
+    }
+    /* run1 / run2 per root (run.f90:75-82) */
+    off = 0;
+    k = 0;
+    for (i64 sym = 1; sym <= s->nirrep && rc == O_OK; sym++) {
+        const i64 l1 = o_irpdso(sym, V, o, 1), l2 = o_idsymsoc(sym, V, V, 0, o, o, 0), n = l1 + l2;
+        double *C = zalloc(n), *pr = zalloc(n);
+        o_opt r1, r2, p1, p2;
+        for (i64 r = 0; r < p->estate_sym[sym - 1] && rc == O_OK; r++, k++, off += n) {
+            const double w0 = omega[k];
+            double *L = Lall + off;
+            double *Rk[3] = {Rall + off, Rall + rlen + off, Rall + 2 * rlen + off};
+            for (int order = 1; order <= 2 && rc == O_OK; order++) {
+                /* calV_C: Ctilde = -C^(n) + sum_k w^(k) R^(n-k); solver.f90 negates it */
+                for (i64 q = 0; q < n; q++) C[q] = -Call[off + q];
+                for (int kk = 1; kk <= order; kk++) o_daxpy(n, w[3 * k + kk - 1], Rk[order - kk], C);
+                for (i64 q = 0; q < n; q++) C[q] = -C[q];
+                double *Rn = Rk[order];
+                o_opt_view(&r1, V, o, Z, Z, 1, 1, sym, Rn);
+                o_opt_view(&r2, V, V, o, o, 0, 0, sym, Rn + l1);
+                o_opt_view(&p1, V, o, Z, Z, 1, 1, sym, pr);
+                o_opt_view(&p2, V, V, o, o, 0, 0, sym, pr + l1);
+                memcpy(pr, C, sizeof(double) * (size_t)n);
+                o_diis dst;
+                o_diis_init(&dst, n, p->diis_dim);
+                i64 iter = 0;
+                for (;;) { /* solver.f90:31-77 */
+                    iter++;
+                    o_denomT1(Rn, pr, I->eorb, V, o, sym);
+                    o_denomT2(Rn + l1, pr + l1, I->eorb, V, o, sym, 0);
+                    ee_orth(Rn, L, n);
+                    double err = o_diis_step(&dst, iter, Rn);
+                    ee_orth(Rn, L, n);
+                    if (iter > 1 && fabs(err) < p->diis_max_err) break;
+                    if (iter > p->diis_cyc) break;
+                    memcpy(pr, C, sizeof(double) * (size_t)n);
+                    o_daxpy(n, -w0, Rn, pr);
+                    rc = o_c1_r1iabj(&p1, &r1, &g.wk, 1.0); /* calA0R1 */
+                    if (rc == O_OK) rc = o_c1_r1Fmi(&p1, &r1, &g.fli, -1.0);
+                    if (rc == O_OK) rc = o_c1_r1Fae(&p1, &r1, &g.fad, -1.0);
+                    if (rc == O_OK) rc = o_c1_r2ijka(&p1, &r2, &v.ijka, 1.0);
+                    if (rc == O_OK) rc = o_c1_r2abci(&p1, &r2, &v.abci, 1.0);
+                    if (rc == O_OK) rc = o_c2_r1ijka(&p2, &r1, &v.ijka, 1.0); /* calA0R2 */
+                    if (rc == O_OK) rc = o_c2_r1abci(&p2, &r1, &v.abci, 1.0);
+                    if (rc != O_OK) break;
+                }
+                o_diis_free(&dst);
+                itsum += iter;
+                if (rc != O_OK) break;
+                rc = ee_calE_C(&g, &J2, &J3, T, lt, Call + off, Rk, sym, l1, order + 1);
+                w[3 * k + order] = o_ddot(n, L, Call + off);
+            }
+        }
+        free(C); free(pr);
+    }
+    if (rc == O_OK && Lout) memcpy(Lout, Lall, sizeof(double) * (size_t)rlen);
+    if (rc == O_OK && Rout) memcpy(Rout, Rall + rlen, sizeof(double) * (size_t)(2 * rlen));
+    if (iters) *iters = itsum;
+    ee_J_free(&J2);
+    ee_J_free(&J3);
+    free(Rall); free(Lall); free(Call);
+    free(mp2); free(fo); free(fv); free(wk);
+    return rc;
+}
+
 /* ---------------- J^(2), J^(3) (src/EE-CPSd.SF/calJ.f90) ---------------- */
 int o_calJ(const o_system *s, const o_integrals *I, const double *T2_1,
            const double *T1_2, const double *T2_2, o_jints *J)

@@ -273,3 +273,132 @@ class DenseSystem:
         tau = T2c + (X - X.transpose(0, 1, 3, 2) - X.transpose(1, 0, 2, 3) + X.transpose(1, 0, 3, 2))
         E4 = 0.25 * np.sum(tau * self.abij)
         return dict(T1=[T1a, T1b, T1c], T2=[T2a, T2b, T2c], E=np.array([E2, E3, E4]))
+
+    # ---------------------------------------------------------- EE-grCPS(D)
+    def _gr_intermediates(self):
+        MP2t = -self.abij / self.e2
+        Fli = K("Fmi_r2abij", MP2t, self.abij, -1.0)
+        Fad = K("Fae_r2abij", MP2t, self.abij, -1.0)
+        W = self.iabj + K("Wmbej_r2abij", MP2t, self.abij, 2.0)
+        return Fli, Fad, W
+
+    def _jset(self, t1, t2):
+        """the [V,T] part of calJ2 / calJ3 (src/EE-grCPSd.SF/calJ.f90)"""
+        return dict(
+            Foo=K("Fmi_r1ijka", t1, self.ijka) + K("Fmi_r2abij", t2, self.abij),
+            Fvv=K("Fae_r1abci", t1, self.abci) + K("Fae_r2abij", t2, self.abij),
+            Fov=K("Fme_r1abij", t1, self.abij),
+            Wovoo=(K("Wkbij_r1iabj", t1, self.iabj, -1.0) + K("Wkbij_r1Uklij", t1, self.ijkl)
+                   + K("Wkbij_r2ijka", t2, self.ijka) + K("Wkbij_r2abci", t2, self.abci)),
+            Wovvo=(K("Wmbej_r1ijka", t1, self.ijka) + K("Wmbej_r1abci", t1, self.abci)
+                   + K("Wmbej_r2abij", t2, self.abij, 2.0)),
+            Woooo=K("Wmnij_r1ijka", t1, self.ijka) + K("Wmnij_r2abij", t2, self.abij),
+            Wooov=K("Wlkjd_r1abij", t1, self.abij))
+
+    def _jset_vtt(self, J, t1, t2):
+        """the [[V,T^(1)],T^(1)] part of calJ3"""
+        w = K("Fme_r1abij", t1, self.abij)
+        J["Foo"] = J["Foo"] + K("Fmi_r1fia", t1, w)
+        J["Fvv"] = J["Fvv"] + K("Fae_r1fia", t1, w)
+        J["Wovoo"] = J["Wovoo"] + K("Wkbij_r2Fkc", t2, w, -1.0)
+        w = K("Wlkjd_r1abij", t1, self.abij)
+        J["Wovvo"] = J["Wovvo"] + K("Wmbej_r1ijka", t1, w)
+        J["Woooo"] = J["Woooo"] + K("Wmnij_r1ijka", t1, w, 0.5)
+        J["Wovoo"] = J["Wovoo"] + K("Wkbij_r2ijka", t2, w)
+        w = K("Wmnij_r1ijka", t1, self.ijka) + K("Wmnij_r2abij", t2, self.abij)
+        J["Wovoo"] = J["Wovoo"] + K("Wkbij_r1Uklij", t1, w)
+        w = K("Wmbej_r1abci", t1, self.abci)
+        J["Wovoo"] = J["Wovoo"] + K("Wkbij_r1iabj", t1, w, -0.5)
+        return J
+
+    def _cjr(self, J, r1, r2):
+        c1 = (K("c1_r1iabj", r1, J["Wovvo"]) + K("c1_r1Fmi", r1, J["Foo"]) + K("c1_r1Fae", r1, J["Fvv"])
+              + K("c1_r2ijka", r2, J["Wooov"]) + K("c1_r2Fme", r2, J["Fov"]))
+        c2 = (K("c2_r1ijka", r1, J["Wovoo"]) + K("c2_r2Wmbej", r2, J["Wovvo"]) + K("c2_r2Wmnij", r2, J["Woooo"])
+              + K("c2_r2Fmi", r2, J["Foo"]) + K("c2_r2Fae", r2, J["Fvv"]))
+        return c1, c2
+
+    def _vtr(self, t1, t2, r1, r2):
+        c1 = K("c1_r1Fmi", t1, K("Fmi_r2abij", r2, self.abij))
+        c2 = K("c2_r1ijka", t1, K("Wkbij_r1iabj", r1, self.iabj, -1.0) + K("Wkbij_r2abci", r2, self.abci))
+        c2 = c2 + K("c2_r1abci", r1, K("Wabdj_r1abcd", t1, self.abcd))
+        c2 = c2 + K("c2_r2Wmnij", t2, K("Wmnij_r2abij", r2, self.abij) + K("Wmnij_r1ijka", r1, self.ijka))
+        c2 = c2 + K("c2_r2Wmbej", t2, K("Wmbej_r1abci", r1, self.abci))
+        c2 = c2 + K("c2_r2Fmi", t2, K("Fmi_r1ijka", r1, self.ijka) + K("Fmi_r2abij", r2, self.abij))
+        c2 = c2 + K("c2_r2Fae", t2, K("Fae_r1abci", r1, self.abci) + K("Fae_r2abij", r2, self.abij))
+        return c1, c2
+
+    def _vttr(self, t1, t2, r1, r2):
+        a = K("Fme_r1abij", r1, self.abij)
+        c2 = K("c2_r2Fae", t2, K("Fae_r1fia", t1, a))
+        b = K("Fmi_r1fia", t1, a) + K("Fmi_r1fia", r1, K("Fme_r1abij", t1, self.abij))
+        c2 = c2 + K("c2_r2Fmi", t2, b)
+        c2 = c2 + K("c2_r2Wmnij", t2, K("Wmnij_r1ijka", t1, K("Wlkjd_r1abij", r1, self.abij)))
+        W = (K("Wkbij_r1Uklij", t1, K("Wmnij_r2abij", r2, self.abij) + K("Wmnij_r1ijka", r1, self.ijka), 0.5)
+             + K("Wkbij_r1iabj", r1, K("Wmbej_r1abci", t1, self.abci), -1.0)
+             + K("Wkbij_r2ijka", t2, K("Wlkjd_r1abij", r1, self.abij)))
+        return c2 + K("c2_r1ijka", t1, W)
+
+    def eegrcpsd(self, symR, w0, R0, L, T):
+        """EE-grCPS(D) orders of one root (src/EE-grCPSd.SF): R0, L packed
+        (R1, R2) vectors of irrep symR with <L|R0> = 1, T the dense grCPS(D)
+        amplitudes (dict of grcpsd()).  Each order's (A - w0) R^(n) =
+        sum_k w^(k) R^(n-k) - C^(n) is solved exactly with <L|R^(n)> = 0.
+        Returns w^(1..3) and the packed R^(1), R^(2)."""
+        s, sym = self.s, self.s.sym
+        z = np.array([1, 0, 0, 0, 0, 0, 0, 0])
+        p1 = ([s.popv, s.popo, z, z], (1, 1), symR)
+        p2 = ([s.popv, s.popv, s.popo, s.popo], (0, 0), symR)
+        l1 = s.r1_len(symR)
+
+        def unpack(x):
+            return dense.dpd_to_dense(x[:l1], sym, *p1)[:, :, 0, 0], dense.dpd_to_dense(x[l1:], sym, *p2)
+
+        def pack(c1, c2):
+            return np.concatenate([dense.dense_to_dpd(c1[:, :, None, None], sym, *p1), dense.dense_to_dpd(c2, sym, *p2)])
+
+        A, _ = self.cisdoo_matrix(symR)
+        n = A.shape[0]
+        Fli, Fad, W = self._gr_intermediates()
+        t1a, t2a, t1b, t2b = T["T1"][0], T["T2"][0], T["T1"][1], T["T2"][1]
+        J2 = self._jset(t1a, t2a)
+        J3 = self._jset_vtt(self._jset(t1b, t2b), t1a, t2a)
+
+        def c2vr2(r2):
+            return (K("c2_r2Wmbej", r2, self.iabj) + K("c2_r2Wmnij", r2, self.ijkl) + K("c2_r2abcd", r2, self.abcd))
+
+        def vmp2r1(r1):
+            return (K("c1_r1iabj", r1, W - self.iabj, -1.0) + K("c1_r1Fmi", r1, Fli, 1.0)
+                    + K("c1_r1Fae", r1, Fad, 1.0))
+
+        def cterm(order, R):
+            r1, r2 = unpack(R[order - 1])
+            c1, c2 = np.zeros_like(r1), c2vr2(r2)
+            if order >= 2:
+                r1, r2 = unpack(R[order - 2])
+                c1 = c1 + vmp2r1(r1)
+                x1, x2 = self._cjr(J2, r1, r2)
+                y1, y2 = self._vtr(t1a, t2a, r1, r2)
+                c1, c2 = c1 + x1 + y1, c2 + x2 + y2
+            if order == 3:
+                r1, r2 = unpack(R[0])
+                x1, x2 = self._cjr(J3, r1, r2)
+                y1, y2 = self._vtr(t1b, t2b, r1, r2)
+                c1, c2 = c1 + x1 + y1, c2 + x2 + y2 + self._vttr(t1a, t2a, r1, r2)
+            return pack(c1, c2)
+
+        M = np.zeros((n + 1, n + 1))
+        M[:n, :n] = A - w0 * np.eye(n)
+        M[:n, n] = L
+        M[n, :n] = L
+        R = [np.asarray(R0, float)]
+        w = []
+        C = cterm(1, R)
+        w.append(L @ C)
+        for order in (1, 2):
+            rhs = -C + sum(w[k - 1] * R[order - k] for k in range(1, order + 1))
+            x = np.linalg.solve(M, np.concatenate([rhs, [0.0]]))
+            R.append(x[:n])
+            C = cterm(order + 1, R)
+            w.append(L @ C)
+        return np.array(w), R[1], R[2]

@@ -216,6 +216,25 @@ class Oracle:
         return dict(T1=[T[k, :l1] for k in range(3)], T2=[T[k, l1:] for k in range(3)], E=E,
                     iters=list(it))
 
+    def eegrcpsd(self, g, om, R0):
+        """EE-grCPS(D) of every root from grcpsd() and cisdoo() results:
+        w (nroot x 3), left vectors and R^(1), R^(2) (cisdoo's layout)"""
+        s = self.s
+        nroot = s.nroots
+        rlen = sum(int(s.estate_sym[h]) * (s.r1_len(h + 1) + s.r2_len(h + 1)) for h in range(8))
+        T = np.concatenate([np.concatenate([g["T1"][k], g["T2"][k]]) for k in range(3)])
+        w = np.zeros(3 * max(nroot, 1))
+        L = np.zeros(max(rlen, 1))
+        R = np.zeros(2 * max(rlen, 1))
+        it = I64()
+        om = np.ascontiguousarray(om, dtype=np.float64)
+        R0 = np.ascontiguousarray(R0, dtype=np.float64)
+        rc = lib().o_eegrcpsd_roots(ctypes.byref(self.osys), ctypes.byref(self.oint), ctypes.byref(self.par),
+                                    ptr(T), ptr(om), ptr(R0), ptr(w), ptr(L), ptr(R), ctypes.byref(it))
+        assert rc == 0, rc
+        return dict(w=w[:3 * nroot].reshape(nroot, 3), L=L[:rlen], R1=R[:rlen], R2=R[rlen:2 * rlen],
+                    iters=it.value)
+
     def ground3(self, g):
         """third order ground state (run3.f90) from the T of ground()"""
         s = self.s

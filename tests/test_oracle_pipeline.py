@@ -176,3 +176,34 @@ def test_grcpsd_ground_matches_dense(nirrep):
         np.testing.assert_allclose(vvoo_dense(s, g["T2"][k], 1), d["T2"][k], rtol=0, atol=1e-9, err_msg=str(k))
     np.testing.assert_allclose(g["E"], d["E"], rtol=0, atol=1e-10)
     assert np.all(np.abs(d["E"]) > 1e-8) and np.abs(d["T1"][0]).max() > 1e-6
+
+
+@pytest.mark.parametrize("nirrep", [1, 2])
+def test_eegrcpsd_matches_dense(nirrep):
+    """EE-grCPS(D) (src/EE-grCPSd.SF): the left vector of each CIS(D-infinity)
+    root is the left eigenvector of the dense (R1, R2) operator with
+    <L|R> = 1, and w^(1), w^(2), w^(3) and R^(1), R^(2) match the dense
+    chain solved exactly with <L|R^(n)> = 0; all DIIS loops run to 1e-12."""
+    s = synth.System(nmo=10, nocc_a=3, nocc_b=1, nirrep=nirrep, seed=7, roots=2)
+    orc = of.Oracle(s, lowest=1, davidson_conv=12, diis_max_err=1e-12, diis_cyc=400)
+    om, R0, _ = orc.cisdoo()
+    g = orc.grcpsd()
+    e = orc.eegrcpsd(g, om, R0)
+    ds = dp.DenseSystem(s)
+    dg = ds.grcpsd()
+    off, k = 0, 0
+    for h in range(8):
+        for _ in range(int(s.estate_sym[h])):
+            n = s.r1_len(h + 1) + s.r2_len(h + 1)
+            A, _ = ds.cisdoo_matrix(h + 1)
+            R, L = R0[off:off + n], e["L"][off:off + n]
+            assert abs(L @ R - 1.0) < 1e-10
+            np.testing.assert_allclose(A.T @ L, om[k] * L, rtol=0, atol=1e-8 * np.abs(L).max())
+            w, R1, R2 = ds.eegrcpsd(h + 1, om[k], R, L, dg)
+            np.testing.assert_allclose(e["w"][k], w, rtol=0, atol=1e-9, err_msg=str(k))
+            np.testing.assert_allclose(e["R1"][off:off + n], R1, rtol=0, atol=1e-8)
+            np.testing.assert_allclose(e["R2"][off:off + n], R2, rtol=0, atol=1e-8)
+            assert np.all(np.abs(w) > 1e-7)
+            off += n
+            k += 1
+    assert k == len(om) > 0
