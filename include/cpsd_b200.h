@@ -409,6 +409,17 @@ int cpsd_cisdoo_run(const cpsd_system *s, const cpsd_integrals *I, const cpsd_pa
 int cpsd_grcpsd_ground(const cpsd_system *s, const cpsd_integrals *I, const cpsd_params *p, double *T_dev,
                        double *E_host, int64_t *iters);
 
+/* excited-state grCPS(D) (src/EE-grCPSd.SF/run.f90) from the grCPS(D)
+ * amplitudes T_dev (cpsd_grcpsd_ground's layout; orders 1, 2 used) and the
+ * CIS(D-infinity) roots (omega_host, R0_dev in cpsd_cisdoo_run's layout):
+ * per root k the left vector (calEigenCISDoo.f90) and w_host[3k..3k+2] =
+ * w^(1), w^(2), w^(3); L_dev (nullable) receives the left vectors (R0's
+ * layout, <L|R0> = 1), R_dev (nullable) R^(1) of every root then R^(2);
+ * iterations = DIIS iterations summed. */
+int cpsd_eegrcpsd_roots(const cpsd_system *s, const cpsd_integrals *I, const cpsd_params *p, const double *T_dev,
+                        const double *omega_host, const double *R0_dev, double *w_host, double *L_dev, double *R_dev,
+                        int64_t *iterations);
+
 /* ground CPS(D) T^(1), T^(2) (src/CPSd.SF/run1.f90, run2.f90); device outputs */
 int cpsd_ground(const cpsd_system *s, const cpsd_integrals *I, const cpsd_params *p,
                 double *T2_1, double *T1_2, double *T2_2, double *E2_host, double *E3_host,

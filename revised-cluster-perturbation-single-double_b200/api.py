@@ -304,6 +304,24 @@ def grcpsd_ground(s, sysc, ints, par):
     return dict(T1=[T[k, :l1] for k in range(3)], T2=[T[k, l1:] for k in range(3)], E=E, iters=list(it))
 
 
+def eegrcpsd_roots(s, sysc, ints, par, g, om, R0):
+    """EE-grCPS(D) of every root from grcpsd_ground() and cisdoo_run()
+    results: w (nroot x 3), left vectors, R^(1), R^(2) (device), iterations"""
+    import torch
+    n = s.nroots
+    rlen = sum(int(s.estate_sym[h]) * (s.r1_len(h + 1) + s.r2_len(h + 1)) for h in range(8))
+    T = torch.cat([torch.cat([g["T1"][k], g["T2"][k]]) for k in range(3)]).contiguous()
+    w = np.zeros(3 * max(n, 1))
+    L = torch.zeros(max(rlen, 1), dtype=torch.float64, device="cuda")
+    R = torch.zeros(2 * max(rlen, 1), dtype=torch.float64, device="cuda")
+    it = I64()
+    om = np.ascontiguousarray(om, dtype=np.float64)
+    check(lib().cpsd_eegrcpsd_roots(ctypes.byref(sysc), ctypes.byref(ints.struct), ctypes.byref(par), dptr(T),
+                                    om.ctypes.data_as(ctypes.c_void_p), dptr(R0), w.ctypes.data_as(ctypes.c_void_p),
+                                    dptr(L), dptr(R), ctypes.byref(it)), "cpsd_eegrcpsd_roots")
+    return dict(w=w[:3 * n].reshape(n, 3), L=L[:rlen], R1=R[:rlen], R2=R[rlen:2 * rlen], iters=it.value)
+
+
 def ground3(s, sysc, ints, par, g):
     """third-order ground state (run3.f90) from ground()'s T: T1^(3),
     T2^(3) (device) and E^(4)"""

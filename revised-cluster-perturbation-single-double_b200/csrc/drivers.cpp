@@ -641,26 +641,30 @@ struct GrState {
     Ten fli, fad, wk;  // Fli, Fad, Wkaci
 };
 
-// <ab,ij|[V,T2]|0> (calA1R2.f90:30-37)
-int gr_a1r2(const GrState &g, Ten &C2, const double *T2) {
-    const i64 *o = g.S.popo, *v = g.S.popv;
-    Ten t2 = ten(v, v, o, o, 0, 0, 1, (double *)T2);
+// <ab,ij|[V,T2]|0> (calA1R2.f90:30-37; calC2_VR2.f90:3-24)
+int gr_a1r2_sym(const GrState &g, Ten &C2, const Ten &t2) {
     CPSD_TRY(k_c2_r2Wmbej(C2, t2, g.X.iabj, 1.0));
     CPSD_TRY(k_c2_r2Wmnij(C2, t2, g.X.ijkl, 1.0));
     return k_c2_r2abcd(C2, t2, g.X.abcd, 1.0);
 }
-
-// calA2R1.f90:27-47, Wkaci - iabj formed in place and restored as the
-// reference does
-int gr_a2r1(GrState &g, Ten &C1, const double *T1) {
+int gr_a1r2(const GrState &g, Ten &C2, const double *T2) {
     const i64 *o = g.S.popo, *v = g.S.popv;
-    Ten t1 = ten(v, o, ZORB, ZORB, 1, 1, 1, (double *)T1);
+    return gr_a1r2_sym(g, C2, ten(v, v, o, o, 0, 0, 1, (double *)T2));
+}
+
+// calA2R1.f90:27-47 (also calC1_VMP2R1.f90:9-30), Wkaci - iabj formed in
+// place and restored as the reference does
+int gr_a2r1_ten(GrState &g, Ten &C1, const Ten &t1) {
     const i64 n = g.wk.len();
     CPSD_TRY(launch_axpy(n, -1.0, g.X.iabj.arr, g.wk.arr));
     CPSD_TRY(k_c1_r1iabj(C1, t1, g.wk, -1.0));
     CPSD_TRY(launch_axpy(n, 1.0, g.X.iabj.arr, g.wk.arr));
     CPSD_TRY(k_c1_r1Fmi(C1, t1, g.fli, 1.0));
     return k_c1_r1Fae(C1, t1, g.fad, 1.0);
+}
+int gr_a2r1(GrState &g, Ten &C1, const double *T1) {
+    const i64 *o = g.S.popo, *v = g.S.popv;
+    return gr_a2r1_ten(g, C1, ten(v, o, ZORB, ZORB, 1, 1, 1, (double *)T1));
 }
 
 // calL1_VTT.f90:30-75
@@ -730,12 +734,15 @@ int gr_l2_vtt(const GrState &g, Ten &L2, const double *T1, const double *T2) {
     return k_c2_r2Wmnij(L2, t2, w, 2.0);
 }
 
-// solver.f90:24-73 on the device: T = denomT(R) with DIIS over (T1, T2),
-// R = C + (calA0R1(T), calA0R2(T1)), one device-driven step per iteration
-int gr_solve(const GrState &g, const cpsd_params *p, const double *C, double *T, i64 *iters) {
+// solver.f90:24-73 (src/grCPSd.SF) on the device: T = denomT(R) with DIIS
+// over (T1, T2), R = C + (calA0R1(T), calA0R2(T1)), one device-driven step
+// per iteration; with w0 / L (src/EE-grCPSd.SF/solver.f90:31-77) the
+// iteration also subtracts w0 T and keeps T orthogonal to L
+int gr_solve(const GrState &g, const cpsd_params *p, i64 symR, const double *C, double *T, const double *w0_dev,
+             const double *L, i64 *iters) {
     const i64 *o = g.S.popo, *v = g.S.popv;
     const Ints &X = g.X;
-    const i64 l1 = g.l1, len = g.l1 + g.l2;
+    const i64 l1 = irpdso(symR, v, o, 1), len = l1 + idsymsoc(symR, v, v, 0, o, o, 0);
     const int md = (int)p->diis_dim;
     if (md > DIIS_MAXDIM) return set_error(CPSD_EARG, "diis_dim above 16");
     if (len > 0x7fffffffLL) return set_error(CPSD_EARG, "amplitude vector too long");
@@ -756,8 +763,8 @@ int gr_solve(const GrState &g, const cpsd_params *p, const double *C, double *T,
     CPSD_TRY(cuda_check(cudaMemcpyAsync(ss, &hss, sizeof hss, cudaMemcpyHostToDevice, stream()), "solver state"));
     CPSD_TRY(cuda_check(cudaMemcpyAsync(ds, &hds, sizeof hds, cudaMemcpyHostToDevice, stream()), "diis state"));
     const EnergyPlan *e1, *e2;
-    CPSD_TRY(plan_energy(make_desc(v, o, ZORB, ZORB, 1, 1, 1), "vozz", &e1));
-    CPSD_TRY(plan_energy(make_desc(v, v, o, o, 0, 0, 1), "vvoo", &e2));
+    CPSD_TRY(plan_energy(make_desc(v, o, ZORB, ZORB, 1, 1, symR), "vozz", &e1));
+    CPSD_TRY(plan_energy(make_desc(v, v, o, o, 0, 0, symR), "vvoo", &e2));
     CPSD_TRY(launch_energy(e1, 5, X.eorb, nullptr, den));       // ei - ea
     CPSD_TRY(launch_energy(e2, 5, X.eorb, nullptr, den + l1));  // ei + ej - ea - eb
     CPSD_TRY(launch_copy(pr, C, len));
@@ -778,14 +785,16 @@ int gr_solve(const GrState &g, const cpsd_params *p, const double *C, double *T,
     a.cc = C;
     a.S = sg;
     a.den = den;
+    a.L = L;
+    a.w0 = w0_dev;
     int *mb, *mb_dev;
     CPSD_TRY(mapped_mailbox(&mb, &mb_dev));
     mb[0] = 1;
     a.mailbox = mb_dev;
     StepThrottle &th = throttle();
     CPSD_TRY(th.init());
-    Ten s1 = ten(v, o, ZORB, ZORB, 1, 1, 1, sg), s2 = ten(v, v, o, o, 0, 0, 1, sg + l1);
-    Ten t1 = ten(v, o, ZORB, ZORB, 1, 1, 1, T), t2 = ten(v, v, o, o, 0, 0, 1, T + l1);
+    Ten s1 = ten(v, o, ZORB, ZORB, 1, 1, symR, sg), s2 = ten(v, v, o, o, 0, 0, symR, sg + l1);
+    Ten t1 = ten(v, o, ZORB, ZORB, 1, 1, symR, T), t2 = ten(v, v, o, o, 0, 0, symR, T + l1);
     for (i64 it = 1; it <= p->diis_cyc + 1; it++) {
         CPSD_TRY(solver_step_launch(a));
         CPSD_TRY(th.mark(it));
@@ -803,6 +812,187 @@ int gr_solve(const GrState &g, const cpsd_params *p, const double *C, double *T,
     CPSD_TRY(read_back(&hss, ss, sizeof hss));
     if (iters) *iters = hss.iter;
     return CPSD_OK;
+}
+
+// ------------------------------------------------------------ EE-grCPS(D)
+// One J^(k) set of src/EE-grCPSd.SF (allocate_mem.f90:54-81)
+struct EeJ {
+    Ten Foo, Fvv, Fov, Woooo, Wooov, Wovoo, Wovvo;
+};
+int ee_j_alloc(const Sys &S, EeJ *J) {
+    const i64 *o = S.popo, *v = S.popv;
+    auto mk = [&](Ten *t, const i64 *p0, const i64 *p1, const i64 *p2, const i64 *p3, i64 i0, i64 i1) {
+        *t = ten(p0, p1, p2, p3, i0, i1, 1, nullptr);
+        CPSD_TRY(scratch(t->len(), &t->arr));
+        return zero(t->arr, t->len());
+    };
+    CPSD_TRY(mk(&J->Foo, o, o, ZORB, ZORB, 1, 1));
+    CPSD_TRY(mk(&J->Fvv, v, v, ZORB, ZORB, 1, 1));
+    CPSD_TRY(mk(&J->Fov, v, o, ZORB, ZORB, 1, 1));
+    CPSD_TRY(mk(&J->Woooo, o, o, o, o, 0, 0));
+    CPSD_TRY(mk(&J->Wooov, o, o, o, v, 0, 1));
+    CPSD_TRY(mk(&J->Wovoo, o, o, o, v, 0, 1));
+    return mk(&J->Wovvo, v, o, v, o, 1, 1);
+}
+
+// the [V,T] part of calJ2 / calJ3 (calJ.f90:14-95, 104-170)
+int ee_j_vt(const Ints &X, EeJ &J, const Ten &t1, const Ten &t2) {
+    CPSD_TRY(k_Fmi_r1ijka(J.Foo, t1, X.ijka, 1.0));
+    CPSD_TRY(k_Fmi_r2abij(J.Foo, t2, X.abij, 1.0));
+    CPSD_TRY(k_Fae_r1abci(J.Fvv, t1, X.abci, 1.0));
+    CPSD_TRY(k_Fae_r2abij(J.Fvv, t2, X.abij, 1.0));
+    CPSD_TRY(k_Fme_r1abij(J.Fov, t1, X.abij, 1.0));
+    CPSD_TRY(k_Wkbij_r1iabj(J.Wovoo, t1, X.iabj, -1.0));
+    CPSD_TRY(k_Wkbij_r1Uklij(J.Wovoo, t1, X.ijkl, 1.0));
+    CPSD_TRY(k_Wkbij_r2ijka(J.Wovoo, t2, X.ijka, 1.0));
+    CPSD_TRY(k_Wkbij_r2abci(J.Wovoo, t2, X.abci, 1.0));
+    CPSD_TRY(k_Wmbej_r1ijka(J.Wovvo, t1, X.ijka, 1.0));
+    CPSD_TRY(k_Wmbej_r1abci(J.Wovvo, t1, X.abci, 1.0));
+    CPSD_TRY(k_Wmbej_r2abij(J.Wovvo, t2, X.abij, 2.0));
+    CPSD_TRY(k_Wmnij_r1ijka(J.Woooo, t1, X.ijka, 1.0));
+    CPSD_TRY(k_Wmnij_r2abij(J.Woooo, t2, X.abij, 1.0));
+    return k_Wlkjd_r1abij(J.Wooov, t1, X.abij, 1.0);
+}
+
+// a zeroed scratch tensor of the given layout
+int ee_tmp(Ten *t, const i64 *p0, const i64 *p1, const i64 *p2, const i64 *p3, i64 i0, i64 i1, i64 sym) {
+    *t = ten(p0, p1, p2, p3, i0, i1, sym, nullptr);
+    CPSD_TRY(scratch(t->len(), &t->arr));
+    return zero(t->arr, t->len());
+}
+
+// the [[V,T^(1)],T^(1)] part of calJ3 (calJ.f90:172-218)
+int ee_j_vtt(const Sys &S, const Ints &X, EeJ &J, const Ten &t1, const Ten &t2) {
+    const i64 *o = S.popo, *v = S.popv;
+    ScratchScope sc;
+    Ten w;
+    CPSD_TRY(ee_tmp(&w, v, o, ZORB, ZORB, 1, 1, 1));
+    CPSD_TRY(k_Fme_r1abij(w, t1, X.abij, 1.0));
+    CPSD_TRY(k_Fmi_r1fia(J.Foo, t1, w, 1.0));
+    CPSD_TRY(k_Fae_r1fia(J.Fvv, t1, w, 1.0));
+    CPSD_TRY(k_Wkbij_r2Fkc(J.Wovoo, t2, w, -1.0));
+    CPSD_TRY(ee_tmp(&w, o, o, o, v, 0, 1, 1));
+    CPSD_TRY(k_Wlkjd_r1abij(w, t1, X.abij, 1.0));
+    CPSD_TRY(k_Wmbej_r1ijka(J.Wovvo, t1, w, 1.0));
+    CPSD_TRY(k_Wmnij_r1ijka(J.Woooo, t1, w, 0.5));
+    CPSD_TRY(k_Wkbij_r2ijka(J.Wovoo, t2, w, 1.0));
+    CPSD_TRY(ee_tmp(&w, o, o, o, o, 0, 0, 1));
+    CPSD_TRY(k_Wmnij_r1ijka(w, t1, X.ijka, 1.0));
+    CPSD_TRY(k_Wmnij_r2abij(w, t2, X.abij, 1.0));
+    CPSD_TRY(k_Wkbij_r1Uklij(J.Wovoo, t1, w, 1.0));
+    CPSD_TRY(ee_tmp(&w, v, o, v, o, 1, 1, 1));
+    CPSD_TRY(k_Wmbej_r1abci(w, t1, X.abci, 1.0));
+    return k_Wkbij_r1iabj(J.Wovoo, t1, w, -0.5);
+}
+
+// calC_J2R / calC_J3R (calC_JR.f90:3-58)
+int ee_cjr(const EeJ &J, Ten &C1, Ten &C2, const Ten &r1, const Ten &r2) {
+    CPSD_TRY(k_c2_r1ijka(C2, r1, J.Wovoo, 1.0));
+    CPSD_TRY(k_c1_r1iabj(C1, r1, J.Wovvo, 1.0));
+    CPSD_TRY(k_c2_r2Wmbej(C2, r2, J.Wovvo, 1.0));
+    CPSD_TRY(k_c2_r2Wmnij(C2, r2, J.Woooo, 1.0));
+    CPSD_TRY(k_c1_r1Fmi(C1, r1, J.Foo, 1.0));
+    CPSD_TRY(k_c2_r2Fmi(C2, r2, J.Foo, 1.0));
+    CPSD_TRY(k_c1_r1Fae(C1, r1, J.Fvv, 1.0));
+    CPSD_TRY(k_c2_r2Fae(C2, r2, J.Fvv, 1.0));
+    CPSD_TRY(k_c1_r2ijka(C1, r2, J.Wooov, 1.0));
+    return k_c1_r2Fme(C1, r2, J.Fov, 1.0);
+}
+
+// calC_VTR.f90:3-78
+int ee_vtr(const Sys &S, const Ints &X, Ten &C1, Ten &C2, const Ten &t1, const Ten &t2, const Ten &r1, const Ten &r2,
+           i64 symR) {
+    const i64 *o = S.popo, *v = S.popv;
+    ScratchScope sc;
+    Ten w;
+    CPSD_TRY(ee_tmp(&w, o, o, ZORB, ZORB, 1, 1, symR));
+    CPSD_TRY(k_Fmi_r2abij(w, r2, X.abij, 1.0));
+    CPSD_TRY(k_c1_r1Fmi(C1, t1, w, 1.0));
+    CPSD_TRY(ee_tmp(&w, o, o, o, v, 0, 1, symR));
+    CPSD_TRY(k_Wkbij_r1iabj(w, r1, X.iabj, -1.0));
+    CPSD_TRY(k_Wkbij_r2abci(w, r2, X.abci, 1.0));
+    CPSD_TRY(k_c2_r1ijka(C2, t1, w, 1.0));
+    CPSD_TRY(ee_tmp(&w, v, v, v, o, 0, 1, 1));
+    CPSD_TRY(k_Wabdj_r1abcd(w, t1, X.abcd, 1.0));
+    CPSD_TRY(k_c2_r1abci(C2, r1, w, 1.0));
+    CPSD_TRY(ee_tmp(&w, o, o, o, o, 0, 0, symR));
+    CPSD_TRY(k_Wmnij_r2abij(w, r2, X.abij, 1.0));
+    CPSD_TRY(k_Wmnij_r1ijka(w, r1, X.ijka, 1.0));
+    CPSD_TRY(k_c2_r2Wmnij(C2, t2, w, 1.0));
+    CPSD_TRY(ee_tmp(&w, v, o, v, o, 1, 1, symR));
+    CPSD_TRY(k_Wmbej_r1abci(w, r1, X.abci, 1.0));
+    CPSD_TRY(k_c2_r2Wmbej(C2, t2, w, 1.0));
+    CPSD_TRY(ee_tmp(&w, o, o, ZORB, ZORB, 1, 1, symR));
+    CPSD_TRY(k_Fmi_r1ijka(w, r1, X.ijka, 1.0));
+    CPSD_TRY(k_Fmi_r2abij(w, r2, X.abij, 1.0));
+    CPSD_TRY(k_c2_r2Fmi(C2, t2, w, 1.0));
+    CPSD_TRY(ee_tmp(&w, v, v, ZORB, ZORB, 1, 1, symR));
+    CPSD_TRY(k_Fae_r1abci(w, r1, X.abci, 1.0));
+    CPSD_TRY(k_Fae_r2abij(w, r2, X.abij, 1.0));
+    return k_c2_r2Fae(C2, t2, w, 1.0);
+}
+
+// calC_VTTR.f90:3-86
+int ee_vttr(const Sys &S, const Ints &X, Ten &C2, const Ten &t1, const Ten &t2, const Ten &r1, const Ten &r2,
+            i64 symR) {
+    const i64 *o = S.popo, *v = S.popv;
+    ScratchScope sc;
+    Ten a, b, c;
+    CPSD_TRY(ee_tmp(&a, v, o, ZORB, ZORB, 1, 1, symR));  // Gld = V(kl,cd) r(c,k)
+    CPSD_TRY(k_Fme_r1abij(a, r1, X.abij, 1.0));
+    CPSD_TRY(ee_tmp(&b, v, v, ZORB, ZORB, 1, 1, symR));  // F(a,d) -= Gld t(a,l)
+    CPSD_TRY(k_Fae_r1fia(b, t1, a, 1.0));
+    CPSD_TRY(k_c2_r2Fae(C2, t2, b, 1.0));
+    CPSD_TRY(ee_tmp(&b, o, o, ZORB, ZORB, 1, 1, symR));  // F(l,i) = Gld t(d,i) + Fld r(d,i)
+    CPSD_TRY(k_Fmi_r1fia(b, t1, a, 1.0));
+    CPSD_TRY(ee_tmp(&c, v, o, ZORB, ZORB, 1, 1, 1));
+    CPSD_TRY(k_Fme_r1abij(c, t1, X.abij, 1.0));
+    CPSD_TRY(k_Fmi_r1fia(b, r1, c, 1.0));
+    CPSD_TRY(k_c2_r2Fmi(C2, t2, b, 1.0));
+    CPSD_TRY(ee_tmp(&a, o, o, o, v, 0, 1, symR));  // 0.5 V(kl,cd) r(c,i) t(d,j) t(ab,kl)
+    CPSD_TRY(k_Wlkjd_r1abij(a, r1, X.abij, 1.0));
+    CPSD_TRY(ee_tmp(&b, o, o, o, o, 0, 0, symR));
+    CPSD_TRY(k_Wmnij_r1ijka(b, t1, a, 1.0));
+    CPSD_TRY(k_c2_r2Wmnij(C2, t2, b, 1.0));
+    CPSD_TRY(ee_tmp(&a, o, o, o, v, 0, 1, symR));  // W(kb,ij)
+    CPSD_TRY(ee_tmp(&b, o, o, o, o, 0, 0, symR));
+    CPSD_TRY(k_Wmnij_r2abij(b, r2, X.abij, 1.0));
+    CPSD_TRY(k_Wmnij_r1ijka(b, r1, X.ijka, 1.0));
+    CPSD_TRY(k_Wkbij_r1Uklij(a, t1, b, 0.5));
+    CPSD_TRY(ee_tmp(&b, v, o, v, o, 1, 1, 1));
+    CPSD_TRY(k_Wmbej_r1abci(b, t1, X.abci, 1.0));
+    CPSD_TRY(k_Wkbij_r1iabj(a, r1, b, -1.0));
+    CPSD_TRY(ee_tmp(&b, o, o, o, v, 0, 1, symR));
+    CPSD_TRY(k_Wlkjd_r1abij(b, r1, X.abij, 1.0));
+    CPSD_TRY(k_Wkbij_r2ijka(a, t2, b, 1.0));
+    return k_c2_r1ijka(C2, t1, a, 1.0);
+}
+
+// calE_C.f90:4-66: C^(n) of one root; R[k] = R^(k) (irrep symR), T the
+// grCPS(D) amplitudes (irrep 1, lt per order)
+int ee_cale_c(GrState &g, const EeJ *J2, const EeJ *J3, const double *T, i64 lt, double *C, double *const *R,
+              i64 symR, int order) {
+    const i64 *o = g.S.popo, *v = g.S.popv;
+    const Ints &X = g.X;
+    const i64 l1 = irpdso(symR, v, o, 1), n = l1 + idsymsoc(symR, v, v, 0, o, o, 0), g1 = g.l1;
+    Ten c1 = ten(v, o, ZORB, ZORB, 1, 1, symR, C), c2 = ten(v, v, o, o, 0, 0, symR, C + l1);
+    CPSD_TRY(zero(C, n));
+    Ten r2 = ten(v, v, o, o, 0, 0, symR, R[order - 1] + l1);
+    CPSD_TRY(gr_a1r2_sym(g, c2, r2));  // calC2_VR2
+    if (order == 1) return CPSD_OK;
+    Ten r1 = ten(v, o, ZORB, ZORB, 1, 1, symR, R[order - 2]);
+    r2 = ten(v, v, o, o, 0, 0, symR, R[order - 2] + l1);
+    Ten t1 = ten(v, o, ZORB, ZORB, 1, 1, 1, (double *)T), t2 = ten(v, v, o, o, 0, 0, 1, (double *)T + g1);
+    CPSD_TRY(gr_a2r1_ten(g, c1, r1));  // calC1_VMP2R1
+    CPSD_TRY(ee_cjr(*J2, c1, c2, r1, r2));
+    CPSD_TRY(ee_vtr(g.S, X, c1, c2, t1, t2, r1, r2, symR));
+    if (order == 2) return CPSD_OK;
+    r1 = ten(v, o, ZORB, ZORB, 1, 1, symR, R[0]);
+    r2 = ten(v, v, o, o, 0, 0, symR, R[0] + l1);
+    CPSD_TRY(ee_cjr(*J3, c1, c2, r1, r2));
+    Ten u1 = ten(v, o, ZORB, ZORB, 1, 1, 1, (double *)T + lt), u2 = ten(v, v, o, o, 0, 0, 1, (double *)T + lt + g1);
+    CPSD_TRY(ee_vtr(g.S, X, c1, c2, u1, u2, r1, r2, symR));
+    return ee_vttr(g.S, X, c2, t1, t2, r1, r2, symR);
 }
 
 }  // namespace
@@ -857,7 +1047,7 @@ int cpsd_grcpsd_ground(const cpsd_system *s, const cpsd_integrals *I, const cpsd
             CPSD_TRY(gr_l2_vtt(g, c2, T_dev, T_dev + l1));
         }
         i64 it = 0;
-        CPSD_TRY(gr_solve(g, p, C, Tk, &it));
+        CPSD_TRY(gr_solve(g, p, 1, C, Tk, nullptr, nullptr, &it));
         if (iters) iters[k - 1] = it;
         // calEcorr: tau = T2^(k) (+ effectT2 of the fixed lower-order T1)
         CPSD_TRY(launch_copy(tau, Tk + l1, l2));
@@ -874,6 +1064,208 @@ int cpsd_grcpsd_ground(const cpsd_system *s, const cpsd_integrals *I, const cpsd
     CPSD_TRY(read_back(h, dE, sizeof h));
     if (E_host)
         for (int k = 0; k < 3; k++) E_host[k] = h[k];
+    return digit_error_check();
+}
+
+// EE-grCPS(D) (src/EE-grCPSd.SF/run.f90): per CIS(D-infinity) root the left
+// vector (calEigenCISDoo.f90) and w^(1), J^(2) / J^(3) of the grCPS(D)
+// amplitudes (calJ.f90), then orders 1, 2 (run1.f90, run2.f90) with
+// w^(2), w^(3) (calE_C.f90)
+int cpsd_eegrcpsd_roots(const cpsd_system *s, const cpsd_integrals *I, const cpsd_params *p, const double *T_dev,
+                        const double *omega_host, const double *R0_dev, double *w_host, double *L_dev, double *R_dev,
+                        int64_t *iters) {
+    Sys S;
+    CPSD_TRY(make_sys(s, &S));
+    Ints X = make_ints(S, I);
+    IntegralScope keep(I);
+    const i64 *o = S.popo, *v = S.popv;
+    const int md = (int)p->diis_dim;
+    if (md > DIIS_MAXDIM) return set_error(CPSD_EARG, "diis_dim above 16");
+    ScratchScope sc;
+    const i64 g1 = irpdso(1, v, o, 1), lt = g1 + idsymsoc(1, v, v, 0, o, o, 0);
+    double *mp2, *fo, *fv, *wk;
+    CPSD_TRY(scratch(lt - g1, &mp2));
+    CPSD_TRY(scratch(irpdso(1, o, o, 1), &fo));
+    CPSD_TRY(scratch(irpdso(1, v, v, 1), &fv));
+    CPSD_TRY(scratch(X.iabj.len(), &wk));
+    GrState g{S, X, g1, lt - g1, ten(o, o, ZORB, ZORB, 1, 1, 1, fo), ten(v, v, ZORB, ZORB, 1, 1, 1, fv),
+              ten(v, o, v, o, 1, 1, 1, wk)};
+    {  // run.f90:41-60
+        const EnergyPlan *e2;
+        CPSD_TRY(plan_energy(make_desc(v, v, o, o, 0, 0, 1), "vvoo", &e2));
+        CPSD_TRY(launch_energy(e2, 2, X.eorb, I->abij, mp2));
+        Ten mp2t = ten(v, v, o, o, 0, 0, 1, mp2);
+        CPSD_TRY(zero(fo, g.fli.len()));
+        CPSD_TRY(zero(fv, g.fad.len()));
+        CPSD_TRY(launch_copy(wk, X.iabj.arr, X.iabj.len()));
+        CPSD_TRY(k_Fmi_r2abij(g.fli, mp2t, X.abij, -1.0));
+        CPSD_TRY(k_Fae_r2abij(g.fad, mp2t, X.abij, -1.0));
+        CPSD_TRY(k_Wmbej_r2abij(g.wk, mp2t, X.abij, 2.0));
+    }
+    i64 nroot = 0, rlen = 0;
+    for (i64 h = 1; h <= S.nirrep; h++) {
+        nroot += p->estate_sym[h - 1];
+        rlen += p->estate_sym[h - 1] * (irpdso(h, v, o, 1) + idsymsoc(h, v, v, 0, o, o, 0));
+    }
+    if (nroot == 0) return CPSD_OK;
+    double *Rall, *Lall, *Call, *dev_w0, *dd;
+    CPSD_TRY(scratch(3 * rlen, &Rall));
+    CPSD_TRY(scratch(rlen, &Lall));
+    CPSD_TRY(scratch(rlen, &Call));
+    CPSD_TRY(scratch(nroot, &dev_w0));
+    CPSD_TRY(scratch(1, &dd));
+    CPSD_TRY(launch_copy(Rall, R0_dev, rlen));
+    CPSD_TRY(cuda_check(cudaMemcpyAsync(dev_w0, omega_host, sizeof(double) * nroot, cudaMemcpyHostToDevice, stream()),
+                        "omega upload"));
+    std::vector<double> w((size_t)(3 * nroot), 0.0);
+    i64 itsum = 0;
+    auto dot = [&](const double *x, const double *y, i64 n, double *out) {
+        CPSD_TRY(launch_dot(x, y, n, dd, false));
+        return read_back(out, dd, sizeof(double));
+    };
+    // calEigenCISDoo for every root (run.f90:64-69)
+    i64 off = 0, k = 0;
+    for (i64 sym = 1; sym <= S.nirrep; sym++) {
+        const i64 nr = p->estate_sym[sym - 1];
+        if (nr == 0) continue;
+        const i64 l1 = irpdso(sym, v, o, 1), l2 = idsymsoc(sym, v, v, 0, o, o, 0), n = l1 + l2;
+        ScratchScope sc2;
+        const EnergyPlan *e1, *e2;
+        CPSD_TRY(plan_energy(make_desc(v, o, ZORB, ZORB, 1, 1, sym), "vozz", &e1));
+        CPSD_TRY(plan_energy(make_desc(v, v, o, o, 0, 0, sym), "vvoo", &e2));
+        double *pr, *sg, *den, *prev, *err, *amp, *l2b, *zc;
+        CPSD_TRY(scratch(l1, &pr));
+        CPSD_TRY(scratch(l1, &sg));
+        CPSD_TRY(scratch(l1, &den));
+        CPSD_TRY(scratch(l1, &prev));
+        CPSD_TRY(scratch(md * l1, &err));
+        CPSD_TRY(scratch(md * l1, &amp));
+        CPSD_TRY(scratch(l2, &l2b));
+        CPSD_TRY(scratch(l1, &zc));
+        CPSD_TRY(zero(zc, l1));
+        CPSD_TRY(launch_energy(e1, 5, X.eorb, nullptr, den));  // ei - ea
+        for (i64 r = 0; r < nr; r++, k++, off += n) {
+            double *R = Rall + off, *L = Lall + off;
+            double nrm = 0.0;
+            CPSD_TRY(dot(R, R, n, &nrm));
+            nrm = std::sqrt(nrm);
+            if (std::fabs(nrm - 1.0) > p->diis_max_err) CPSD_TRY(launch_scale(R, n, 1.0 / nrm));
+            CPSD_TRY(launch_copy(L, R, l1));
+            // L1 loop (calEigenCISDoo.f90:94-140) as device-driven solver steps:
+            // pr = -w L1 + S, L1 = pr / (ei - ea), <L1|R1> = 1 around the DIIS step
+            SolverState *ss;
+            DiisState *ds;
+            CPSD_TRY(arena().alloc(sizeof(SolverState), (void **)&ss));
+            CPSD_TRY(arena().alloc(sizeof(DiisState), (void **)&ds));
+            SolverState hss{0, 1, 0, 0, 0.0};
+            DiisState hds{(int)l1, md, 1, 1, 1.0, {}};
+            CPSD_TRY(cuda_check(cudaMemcpyAsync(ss, &hss, sizeof hss, cudaMemcpyHostToDevice, stream()), "state"));
+            CPSD_TRY(cuda_check(cudaMemcpyAsync(ds, &hds, sizeof hds, cudaMemcpyHostToDevice, stream()), "diis"));
+            SolverArgs a;
+            a.len = (int)l1;
+            a.nb = 1;
+            a.cyc = (int)p->diis_cyc;
+            a.tol = p->diis_max_err;
+            a.ss = ss;
+            a.ds = ds;
+            a.db.prev = prev;
+            a.db.err = err;
+            a.db.amp = amp;
+            a.sprev = l1;
+            a.serr = md * l1;
+            a.pr = pr;
+            a.R1 = L;
+            a.cc = zc;
+            a.S = sg;
+            a.den = den;
+            a.w0 = dev_w0 + k;
+            a.nrmv = R;
+            a.keep_first = 1;
+            int *mb, *mb_dev;
+            CPSD_TRY(mapped_mailbox(&mb, &mb_dev));
+            mb[0] = 1;
+            a.mailbox = mb_dev;
+            Ten l1t = ten(v, o, ZORB, ZORB, 1, 1, sym, L), s1 = ten(v, o, ZORB, ZORB, 1, 1, sym, sg);
+            Ten l2t = ten(v, v, o, o, 0, 0, sym, l2b);
+            // L2 = dEmw (Ads L1) (calL2d_VL1, vdmul)
+            auto make_l2 = [&]() {
+                CPSD_TRY(zero(l2b, l2));
+                CPSD_TRY(k_c2_r1ijka(l2t, l1t, X.ijka, 1.0));
+                CPSD_TRY(k_c2_r1abci(l2t, l1t, X.abci, 1.0));
+                return launch_energy(e2, 6, X.eorb, l2b, l2b, dev_w0 + k);
+            };
+            StepThrottle &th = throttle();
+            CPSD_TRY(th.init());
+            for (i64 it = 1; it <= p->diis_cyc + 1; it++) {
+                CPSD_TRY(solver_step_launch(a));
+                CPSD_TRY(th.mark(it));
+                if (((volatile int *)mb)[0] == 0) break;
+                CPSD_TRY(zero(sg, l1));
+                CPSD_TRY(k_c1d_l1Wibaj(s1, l1t, g.wk, 1.0));
+                CPSD_TRY(k_c1d_l1fab(s1, l1t, g.fad, 1.0));
+                CPSD_TRY(k_c1d_l1fij(s1, l1t, g.fli, 1.0));
+                CPSD_TRY(make_l2());
+                CPSD_TRY(k_c1_r2ijka(s1, l2t, X.ijka, 1.0));  // calL1d_VL2
+                CPSD_TRY(k_c1_r2abci(s1, l2t, X.abci, 1.0));
+                CPSD_TRY(th.wait(it));
+            }
+            CPSD_TRY(read_back(&hss, ss, sizeof hss));
+            itsum += hss.iter;
+            // L2 and <L|R> = 1 (calEigenCISDoo.f90:142-157)
+            CPSD_TRY(make_l2());
+            CPSD_TRY(launch_copy(L + l1, l2b, l2));
+            double lr = 0.0;
+            CPSD_TRY(dot(L + l1, R + l1, l2, &lr));
+            CPSD_TRY(launch_scale(L, n, 1.0 / (1.0 + lr)));
+            // w^(1) = L J^(1) R^(0)
+            double *Rk[3] = {R, nullptr, nullptr};
+            CPSD_TRY(ee_cale_c(g, nullptr, nullptr, T_dev, lt, Call + off, Rk, sym, 1));
+            CPSD_TRY(dot(L, Call + off, n, &w[(size_t)(3 * k)]));
+        }
+    }
+    // calJ2 / calJ3 (run.f90:72-73)
+    EeJ J2, J3;
+    CPSD_TRY(ee_j_alloc(S, &J2));
+    CPSD_TRY(ee_j_alloc(S, &J3));
+    {
+        Ten t1 = ten(v, o, ZORB, ZORB, 1, 1, 1, (double *)T_dev), t2 = ten(v, v, o, o, 0, 0, 1, (double *)T_dev + g1);
+        Ten u1 = ten(v, o, ZORB, ZORB, 1, 1, 1, (double *)T_dev + lt);
+        Ten u2 = ten(v, v, o, o, 0, 0, 1, (double *)T_dev + lt + g1);
+        CPSD_TRY(ee_j_vt(X, J3, u1, u2));
+        CPSD_TRY(ee_j_vt(X, J2, t1, t2));
+        CPSD_TRY(ee_j_vtt(S, X, J3, t1, t2));
+    }
+    // run1 / run2 per root (run.f90:75-82)
+    off = 0;
+    k = 0;
+    for (i64 sym = 1; sym <= S.nirrep; sym++) {
+        const i64 nr = p->estate_sym[sym - 1];
+        if (nr == 0) continue;
+        const i64 n = irpdso(sym, v, o, 1) + idsymsoc(sym, v, v, 0, o, o, 0);
+        ScratchScope sc2;
+        double *C;
+        CPSD_TRY(scratch(n, &C));
+        for (i64 r = 0; r < nr; r++, k++, off += n) {
+            double *L = Lall + off;
+            double *Rk[3] = {Rall + off, Rall + rlen + off, Rall + 2 * rlen + off};
+            for (int order = 1; order <= 2; order++) {
+                // calV_C and the solver's sign: C = C^(n) - sum_k w^(k) R^(n-k)
+                CPSD_TRY(launch_copy(C, Call + off, n));
+                for (int kk = 1; kk <= order; kk++)
+                    CPSD_TRY(launch_axpy(n, -w[(size_t)(3 * k + kk - 1)], Rk[order - kk], C));
+                i64 it = 0;
+                CPSD_TRY(gr_solve(g, p, sym, C, Rk[order], dev_w0 + k, L, &it));
+                itsum += it;
+                CPSD_TRY(ee_cale_c(g, &J2, &J3, T_dev, lt, Call + off, Rk, sym, order + 1));
+                CPSD_TRY(dot(L, Call + off, n, &w[(size_t)(3 * k + order)]));
+            }
+        }
+    }
+    for (i64 q = 0; q < 3 * nroot; q++) w_host[q] = w[(size_t)q];
+    if (L_dev) CPSD_TRY(launch_copy(L_dev, Lall, rlen));
+    if (R_dev) CPSD_TRY(launch_copy(R_dev, Rall + rlen, 2 * rlen));
+    if (iters) *iters = itsum;
+    CPSD_TRY(cuda_check(cudaStreamSynchronize(stream()), "eegrcpsd sync"));
     return digit_error_check();
 }
 

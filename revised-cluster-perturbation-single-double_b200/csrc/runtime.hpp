@@ -259,6 +259,7 @@ int plan_energy(const Desc &d, const char *kinds, const EnergyPlan **out);
 // mode 4: out = e(a,i) * in, e(ab,ij) * in     (calAR vdmul: src/EE-CIS.SF/calAR.f90:29,
 //                                               src/CISdoo.SD.SF/calAR.f90:69)
 // mode 5: out = ei-ea, ei+ej-ea-eb              (the divisor of mode 3 / mode 2)
+// mode 6: out = in * (1 / (w0 - e(ab,ij)))      (dEmw, calEigenCISDoo.f90:80-86)
 int launch_energy(const EnergyPlan *p, int mode, const double *eorb, const double *in, double *out,
                   const double *w0_dev = nullptr, i64 nb = 1, i64 in_stride = 0, i64 out_stride = 0);
 // gorb[k] += d/d eorb[k] of sum_e alpha x(e) y(e) e(pq,rs) (y null: y = 1),

@@ -1089,8 +1089,8 @@ __device__ void warp_dgesl(const double *a, int lda, int n, const int *ipvt, dou
     }
 }
 
-// R -= (<L|R> / ||L||) L, the reference's orthogonalR2L (L is normalised,
-// so it divides by the norm)
+// R -= (<L|R> / ||L||) L, the reference's orthogonalR2L (which divides by
+// the norm, not its square)
 __device__ void block_orth(double *R, const double *L, int n, double *sh) {
     // L.L and L.R in one pass and one reduction, each summed in
     // block_dot's order (strided per-thread sums, shuffle-down, warp totals
@@ -1129,6 +1129,15 @@ __device__ void block_orth(double *R, const double *L, int n, double *sh) {
 __device__ void diis_extrapolate(DiisState &s, const DiisBuffers &b, double *vec, double *sh, int *shi, double *Bm,
                                  double *coef, double *aug, double *rhs, int *ipvt);
 
+// R *= 1 / <R|V> (the left vector's normalisation to the right one,
+// calEigenCISDoo.f90:99-104: a dscal by the reciprocal)
+__device__ void block_unit_dot(double *R, const double *V, int n, double *sh) {
+    const double d = 1.0 / block_dot(R, V, n, sh);
+    __syncthreads();
+    for (int k = threadIdx.x; k < n; k += DT) R[k] *= d;
+    __syncthreads();
+}
+
 // one step of the device-driven solver for root blockIdx.x (see solvers.cuh)
 __global__ void __launch_bounds__(DT) k_solver_step(SolverArgs a) {
     __shared__ double sh[DT / 32 + 1];
@@ -1153,14 +1162,17 @@ __global__ void __launch_bounds__(DT) k_solver_step(SolverArgs a) {
         }
         __syncthreads();
     }
-    for (int k = tid; k < len; k += DT) R1[k] = pr[k] / a.den[k];
+    if (iter > 1 || !a.keep_first)
+        for (int k = tid; k < len; k += DT) R1[k] = pr[k] / a.den[k];
     __syncthreads();
+    const double *NV = a.nrmv ? a.nrmv + (size_t)r * len : nullptr;
     DiisState &ds = a.ds[r];
     DiisBuffers b;
     b.prev = a.db.prev + (size_t)r * a.sprev;
     b.err = a.db.err + (size_t)r * a.serr;
     b.amp = a.db.amp + (size_t)r * a.serr;
     if (L) block_orth(R1, L, len, sh);
+    if (NV) block_unit_dot(R1, NV, len, sh);
     if (iter == 1) {
         for (int k = tid; k < len; k += DT) b.prev[k] = R1[k];
         if (tid == 0) {
@@ -1173,6 +1185,7 @@ __global__ void __launch_bounds__(DT) k_solver_step(SolverArgs a) {
     }
     __syncthreads();
     if (L) block_orth(R1, L, len, sh);
+    if (NV) block_unit_dot(R1, NV, len, sh);
     if (tid == 0) {
         const double res = ds.res;
         ss.iter = iter;

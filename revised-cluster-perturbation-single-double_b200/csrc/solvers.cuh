@@ -59,11 +59,15 @@ struct DiisBuffers {
     double *prev, *err, *amp;  // len, maxdim*len, maxdim*len
 };
 // Device-driven solver steps for nb independent roots: the EE solver
-// (solver.f90:4-66) and, without L and w0, the ground T1^(2) DIIS loop
-// (run2.f90).  One CTA per root and step does
+// (solver.f90:4-66), without L and w0 the ground T1^(2) DIIS loop
+// (run2.f90) and the grCPS(D) (T1, T2) loop, with nrmv the CIS(D-infinity)
+// left-vector loop (src/EE-grCPSd.SF/calEigenCISDoo.f90:94-140).  One CTA
+// per root and step does
 //   pr = cc - w0 R1 + S      (S = the sigma of the previous step's R1; from step 2)
-//   R1 = pr / (ei - ea);  orthogonalR2L; dosodiis2_d (LINPACK solve of the
-//   bordered -1e-4 system, dodiis.f / minv.f); orthogonalR2L
+//   R1 = pr / den (den = ei - ea, or ei + ej - ea - eb on the doubles; kept
+//   as given at step 1 with keep_first);  orthogonalR2L or the <R1|nrmv> = 1
+//   scaling; dosodiis2_d (LINPACK solve of the bordered -1e-4 system,
+//   dodiis.f / minv.f); orthogonalR2L or the scaling again
 // (orthogonalR2L: R -= (<L|R>/||L||) L, orthogonalR2L.f90:5-34)
 // and stops the root (active = 0) once |DIIS residual| < tol after step 1 or
 // after step cyc + 1, exactly where the reference's loop exits.  The host
@@ -83,6 +87,8 @@ struct SolverArgs {
     double *pr = nullptr, *R1 = nullptr;  // nb x len
     const double *cc = nullptr, *S = nullptr, *den = nullptr, *L = nullptr, *w0 = nullptr;
     int *mailbox = nullptr;         // nb (device view of mapped host memory)
+    const double *nrmv = nullptr;   // nb x len: scale R1 to <R1|nrmv> = 1 around the DIIS step
+    int keep_first = 0;             // iteration 1 keeps R1 as given instead of pr / den
 };
 int solver_step_launch(const SolverArgs &a);
 

@@ -275,6 +275,37 @@ def test_grcpsd_ground_matches_oracle(nirrep):
     assert g["iters"] == og["iters"]
 
 
+@pytest.mark.parametrize("nirrep", [1, 2, 4])
+def test_eegrcpsd_matches_oracle(nirrep):
+    """EE-grCPS(D) (src/EE-grCPSd.SF): the device chain CIS(D-infinity) ->
+    grCPS(D) -> left vectors and w^(1..3) against the oracle's, every loop
+    converged tightly (Davidson 1e-12, DIIS 1e-11)."""
+    s = synth.System(nmo=10 if nirrep < 4 else 14, nocc_a=3, nocc_b=1, nirrep=nirrep, seed=7, roots=2)
+    s.run_opts.update(lowest=1, davidson_conv=12, diis_max_err=1e-11, diis_cyc=400)
+    ints, sc, par, orc = _run_both(s)
+    om, R0, _ = api.cisdoo_run(s, sc, ints, par)
+    g = api.grcpsd_ground(s, sc, ints, par)
+    e = api.eegrcpsd_roots(s, sc, ints, par, g, om, R0)
+    oom, oR0, _ = orc.cisdoo()
+    og = orc.grcpsd()
+    oe = orc.eegrcpsd(og, oom, oR0)
+    np.testing.assert_allclose(om, oom, rtol=0, atol=1e-10)
+    np.testing.assert_allclose(e["w"], oe["w"], rtol=0, atol=1e-8)
+    # vectors up to the sign of each root's R0 (and so of L, R^(1), R^(2))
+    Rg, L, R1, R2 = host(R0), host(e["L"]), host(e["R1"]), host(e["R2"])
+    off = 0
+    for h in range(8):
+        n = s.r1_len(h + 1) + s.r2_len(h + 1)
+        for _ in range(int(s.estate_sym[h])):
+            sl = slice(off, off + n)
+            sg = np.sign(np.dot(Rg[sl], oR0[sl]))
+            np.testing.assert_allclose(sg * L[sl], oe["L"][sl], rtol=0, atol=1e-7)
+            np.testing.assert_allclose(sg * R1[sl], oe["R1"][sl], rtol=0, atol=1e-7)
+            np.testing.assert_allclose(sg * R2[sl], oe["R2"][sl], rtol=0, atol=1e-7)
+            off += n
+    assert np.all(np.abs(e["w"]) > 1e-7)
+
+
 @pytest.mark.parametrize("batch", [0, 1])
 @pytest.mark.parametrize("nirrep", [1, 4])
 def test_eecpsd_roots_match_oracle(nirrep, batch):
