@@ -420,6 +420,22 @@ int cpsd_eegrcpsd_roots(const cpsd_system *s, const cpsd_integrals *I, const cps
                         const double *omega_host, const double *R0_dev, double *w_host, double *L_dev, double *R_dev,
                         int64_t *iterations);
 
+/* The spin-free DPD lists as a linear function of the spatial integrals
+ * (pq|rs), and its adjoint (no counterpart in the reference, whose lists
+ * come from src/pyscf2cc/py2cc.py).  orb_mo / orb_spin (host, one entry per
+ * spin-free orbital in the lists' order: occupied orbitals of irreps 1..n,
+ * then virtual ones) give each orbital's spatial index (< nmo) and spin
+ * (0 alpha, 1 beta); a list element is <PQ||RS> = [sP=sR, sQ=sS] (PR|QS) -
+ * [sP=sS, sQ=sR] (PS|QR), iabj(b,i,a,j) = <ia||bj>.  The dense (pq|rs) array
+ * is nmo^4 doubles on the device, (pr|qs) at ((p*nmo + r)*nmo + q)*nmo + s.
+ * cpsd_eri_lists fills every non-NULL list of `lists` (device, irrep 1);
+ * cpsd_eri_adjoint adds d/d(pq|rs) of sum_e g(e) list(e) over the non-NULL
+ * lists g of `grads` into geri_dev (atomic adds: the last bits vary). */
+int cpsd_eri_lists(const cpsd_system *s, const int64_t *orb_mo, const int64_t *orb_spin, int64_t nmo,
+                   const double *eri_dev, const cpsd_integrals *lists);
+int cpsd_eri_adjoint(const cpsd_system *s, const int64_t *orb_mo, const int64_t *orb_spin, int64_t nmo,
+                     const cpsd_integrals *grads, double *geri_dev);
+
 /* ground CPS(D) T^(1), T^(2) (src/CPSd.SF/run1.f90, run2.f90); device outputs */
 int cpsd_ground(const cpsd_system *s, const cpsd_integrals *I, const cpsd_params *p,
                 double *T2_1, double *T1_2, double *T2_2, double *E2_host, double *E3_host,

@@ -396,6 +396,40 @@ def integrals_struct(t):
     return st
 
 
+def orbital_map(s):
+    """(mo, spin) of every spin-free orbital of a synth.System in the DPD
+    lists' order: per irrep the alpha then the beta occupied orbitals, then
+    the virtual ones likewise"""
+    occ, vir = [], []
+    for h in range(1, s.nirrep + 1):
+        for spin, nocc in ((0, s.nocc_a), (1, s.nocc_b)):
+            occ += [(m, spin) for m in range(s.nmo) if s.mo_irrep[m] == h and m < nocc]
+        for spin, nocc in ((0, s.nocc_a), (1, s.nocc_b)):
+            vir += [(m, spin) for m in range(s.nmo) if s.mo_irrep[m] == h and m >= nocc]
+    mo = np.array([m for m, _ in occ + vir], np.int64)
+    sp = np.array([x for _, x in occ + vir], np.int64)
+    return mo, sp
+
+
+def eri_lists(sysc, orb_mo, orb_spin, nmo, eri, lists):
+    """cpsd_eri_lists: fill the device lists (dict name -> tensor) from the
+    dense (pq|rs) tensor eri (nmo^4, device)"""
+    orb_mo = np.ascontiguousarray(orb_mo, np.int64)
+    orb_spin = np.ascontiguousarray(orb_spin, np.int64)
+    check(lib().cpsd_eri_lists(ctypes.byref(sysc), orb_mo.ctypes.data_as(ctypes.c_void_p),
+                               orb_spin.ctypes.data_as(ctypes.c_void_p), I64(nmo), dptr(eri),
+                               ctypes.byref(integrals_struct(lists))), "cpsd_eri_lists")
+
+
+def eri_adjoint(sysc, orb_mo, orb_spin, nmo, grads, geri):
+    """cpsd_eri_adjoint: geri (nmo^4, device) += d/d(pq|rs) of sum g.list"""
+    orb_mo = np.ascontiguousarray(orb_mo, np.int64)
+    orb_spin = np.ascontiguousarray(orb_spin, np.int64)
+    check(lib().cpsd_eri_adjoint(ctypes.byref(sysc), orb_mo.ctypes.data_as(ctypes.c_void_p),
+                                 orb_spin.ctypes.data_as(ctypes.c_void_p), I64(nmo),
+                                 ctypes.byref(integrals_struct(grads)), dptr(geri)), "cpsd_eri_adjoint")
+
+
 def cisd_energies(s, sysc, ints_struct, par, symR, nroot):
     """SF-CIS roots of irrep symR and their w^(2): (w0, w2, L) with L the
     unit CIS vectors (nroot x lenR1, CUDA)."""

@@ -87,87 +87,6 @@ __global__ void __launch_bounds__(PM_T) k_pairmap(const PMBlockDev *__restrict__
     }
 }
 
-// The same map with LT x RT <= 2 terms per element in three phases per
-// thread: the element positions and their input addresses first (the index
-// table loads of all PM_PER elements in flight together), then every input
-// load, then the stores, so that a thread's loads no longer wait on one
-// another element after element.  Same sums in the same order as k_pairmap.
-template <int LT, int RT>
-__global__ void __launch_bounds__(PM_T) k_pairmap_batched(const PMBlockDev *__restrict__ blocks, int nblocks,
-                                                          i64 total, const long long *__restrict__ idx,
-                                                          const double *__restrict__ sgn,
-                                                          const double *__restrict__ in0, double *__restrict__ out0,
-                                                          double alpha, double beta, i64 nb, i64 sin, i64 sout) {
-    constexpr int NT = LT * RT;
-    const i64 tiles = (total + PM_TILE - 1) / PM_TILE;
-    for (i64 tile = blockIdx.x; tile < tiles * nb; tile += gridDim.x) {
-        const i64 cpy = tile / tiles;
-        const i64 e0 = (tile - cpy * tiles) * PM_TILE + threadIdx.x;
-        if (e0 >= total) continue;
-        const double *in = in0 + cpy * sin;
-        double *out = out0 + cpy * sout;
-        int b = pm_block(blocks, nblocks, e0);
-        PMBlockDev B = blocks[b];
-        i64 next = b + 1 < nblocks ? blocks[b + 1].start : total;
-        i64 r = (e0 - B.start) / B.nlo, l = (e0 - B.start) - r * B.nlo;
-        i64 oa[PM_PER], ia[PM_PER][NT];
-        double sg[PM_PER][NT];
-        int nj = 0;
-#pragma unroll
-        for (int j = 0; j < PM_PER; j++) {
-            const i64 e = e0 + (i64)j * PM_T;
-            if (e >= total) break;
-            if (j > 0) {
-                if (e >= next) {
-                    while (e >= next) {
-                        b++;
-                        next = b + 1 < nblocks ? blocks[b + 1].start : total;
-                    }
-                    B = blocks[b];
-                    r = (e - B.start) / B.nlo;
-                    l = (e - B.start) - r * B.nlo;
-                } else {
-                    l += PM_T;
-                    if (l >= B.nlo) {
-                        if (B.nlo >= PM_T) {
-                            l -= B.nlo;
-                            r++;
-                        } else {
-                            r = (e - B.start) / B.nlo;
-                            l = (e - B.start) - r * B.nlo;
-                        }
-                    }
-                }
-            }
-#pragma unroll
-            for (int tr = 0; tr < RT; tr++) {
-                const i64 ri = idx[B.rmap + r * RT + tr];
-                const double sr = sgn[B.rmap + r * RT + tr];
-#pragma unroll
-                for (int tq = 0; tq < LT; tq++) {
-                    const i64 li = idx[B.lmap + l * LT + tq];
-                    ia[j][tr * LT + tq] = (ri < 0 || li < 0) ? -1 : B.inBase + ri * B.nli + li;
-                    sg[j][tr * LT + tq] = sr * sgn[B.lmap + l * LT + tq];
-                }
-            }
-            oa[j] = B.outBase + r * B.nlo + l;
-            nj = j + 1;
-        }
-        double v[PM_PER];
-#pragma unroll
-        for (int j = 0; j < PM_PER; j++) {
-            v[j] = 0.0;
-            if (j < nj)
-#pragma unroll
-                for (int t = 0; t < NT; t++)
-                    if (ia[j][t] >= 0) v[j] += sg[j][t] * in[ia[j][t]];
-        }
-#pragma unroll
-        for (int j = 0; j < PM_PER; j++)
-            if (j < nj) out[oa[j]] = (beta == 0.0) ? alpha * v[j] : beta * out[oa[j]] + alpha * v[j];
-    }
-}
-
 __global__ void k_energy(const i64 *__restrict__ blk, int nblocks, i64 n, const i64 *__restrict__ lidx,
                          const i64 *__restrict__ ridx, const double *__restrict__ eorb, int mode,
                          const double *__restrict__ in0, double *__restrict__ out0, const double *__restrict__ w0v,
@@ -323,19 +242,10 @@ int launch_pairmap(const PairMapPlan *p, const double *in, double *out, double a
     cudaEvent_t end;
     CPSD_TRY(timing_begin(0.0, p->total, nb, p->lterms * p->rterms, 40, &end));
     const i64 tiles = (p->total + PM_TILE - 1) / PM_TILE * nb;
-    const unsigned grid = (unsigned)std::min<i64>(tiles, 148 * 16);
-    if (p->lterms == 1 && p->rterms == 1)
-        k_pairmap_batched<1, 1><<<grid, PM_T, 0, stream()>>>(p->d_blocks, p->nblocks, p->total, p->d_idx, p->d_sgn,
-                                                             in, out, alpha, beta, nb, in_stride, out_stride);
-    else if (p->lterms == 2 && p->rterms == 1)
-        k_pairmap_batched<2, 1><<<grid, PM_T, 0, stream()>>>(p->d_blocks, p->nblocks, p->total, p->d_idx, p->d_sgn,
-                                                             in, out, alpha, beta, nb, in_stride, out_stride);
-    else if (p->lterms == 1 && p->rterms == 2)
-        k_pairmap_batched<1, 2><<<grid, PM_T, 0, stream()>>>(p->d_blocks, p->nblocks, p->total, p->d_idx, p->d_sgn,
-                                                             in, out, alpha, beta, nb, in_stride, out_stride);
-    else
-        k_pairmap<<<grid, PM_T, 0, stream()>>>(p->d_blocks, p->nblocks, p->total, p->d_idx, p->d_sgn, p->lterms,
-                                               p->rterms, in, out, alpha, beta, nb, in_stride, out_stride);
+    k_pairmap<<<(unsigned)std::min<i64>(tiles, 148 * 16), PM_T, 0, stream()>>>(p->d_blocks, p->nblocks, p->total,
+                                                                              p->d_idx, p->d_sgn, p->lterms,
+                                                                              p->rterms, in, out, alpha, beta, nb,
+                                                                              in_stride, out_stride);
     count_launch();
     CPSD_TRY(cuda_check(cudaGetLastError(), "k_pairmap"));
     return timing_end(end);

@@ -306,14 +306,21 @@ int plan_narrow(const ContractPlan *cp, const NarrowPlan **out) {
             for (int ti = 0; ti < (int)cp->h_tasks.size(); ti++) {
                 const TaskDev &t = cp->h_tasks[ti];
                 const i64 ns = std::max<i64>(1, std::min<i64>(want, t.Ktot / 256));
-                for (i64 c0 = 0; c0 < CN(t); c0 += NARROW_COLS)
-                    for (i64 r0 = 0; r0 < R(t); r0 += NARROW_ROWS) {
-                        if (ns > 1) p.reds.push_back(NarrowRed{ti, (int)c0, (int)ns, 0, r0, p.nparts});
-                        for (i64 q = 0; q < ns; q++)
+                // the row groups of one K part are neighbours in the item
+                // list, so the warps running together read the same stretch
+                // of the column operand (it stays in L2 across the row groups)
+                for (i64 c0 = 0; c0 < CN(t); c0 += NARROW_COLS) {
+                    const i64 part0 = p.nparts;
+                    if (ns > 1)
+                        for (i64 r0 = 0; r0 < R(t); r0 += NARROW_ROWS) {
+                            p.reds.push_back(NarrowRed{ti, (int)c0, (int)ns, 0, r0, p.nparts});
+                            p.nparts += ns;
+                        }
+                    for (i64 q = 0; q < ns; q++)
+                        for (i64 r0 = 0, ri = 0; r0 < R(t); r0 += NARROW_ROWS, ri++)
                             p.items.push_back(NarrowItem{ti, (int)c0, r0, t.Ktot * q / ns, t.Ktot * (q + 1) / ns,
-                                                         ns > 1 ? p.nparts + q : -1});
-                        if (ns > 1) p.nparts += ns;
-                    }
+                                                         ns > 1 ? part0 + ri * ns + q : -1});
+                }
             }
         }
         *out = P.get();

@@ -510,10 +510,6 @@ int plan_gemm(i64 M, i64 N, i64 K, i64 lda, i64 ldb, i64 ldc, i64 nb, i64 sB, i6
 }
 
 // ------------------------------------------------------------ pair maps
-namespace {
-struct PairEl {
-    i64 ip, p, iq, q;
-};
 std::vector<PairEl> pair_list(const i64 *pp, const i64 *pq, i64 iop, i64 irr) {
     std::vector<PairEl> v;
     for (i64 iq = 1; iq <= ctx().nirrep; iq++) {
@@ -528,6 +524,7 @@ std::vector<PairEl> pair_list(const i64 *pp, const i64 *pq, i64 iop, i64 irr) {
     }
     return v;
 }
+namespace {
 // offset of (ip,p,iq,q) inside the pair space of a pair with pops/iop; -1
 // if structurally zero; sign for packed partner
 i64 pair_off(const i64 *pp, const i64 *pq, i64 iop, i64 ip, i64 p, i64 iq, i64 q, double *sgn) {

@@ -208,6 +208,13 @@ struct PairMapPlan {
     int upload();
 };
 enum PairOp { PAIR_ID = 0, PAIR_EXPAND, PAIR_COMPRESS, PAIR_ANTI, PAIR_ANTI_COMPRESS, PAIR_SWAP };
+// the stored (irrep, index) pairs of the pair space of irrep irr, in DPD
+// storage order (blocks by the second index's irrep, first index fastest,
+// p<q packing for iop 0, p<=q for iop 2)
+struct PairEl {
+    i64 ip, p, iq, q;
+};
+std::vector<PairEl> pair_list(const i64 *pp, const i64 *pq, i64 iop, i64 irr);
 int plan_pairmap(const Desc &din, int op0, int op1, i64 target_iop0, i64 target_iop1, Desc *dout,
                  const PairMapPlan **out);
 
