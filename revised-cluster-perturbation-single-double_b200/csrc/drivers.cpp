@@ -1671,9 +1671,15 @@ int cpsd_eecpsd_roots(const cpsd_system *s, const cpsd_integrals *I, const cpsd_
             chunk = std::max<i64>(1, std::min<i64>(nroot, (i64)(0.7 * ctx().mem_share * avail / per_root)));
         }
     }
-    if (getenv("CPSD_TRACE"))
-        fprintf(stderr, "[cpsd] eecpsd_roots symR=%lld nroot=%lld roots per batch=%lld\n", (long long)symR,
-                (long long)nroot, (long long)chunk);
+    if (getenv("CPSD_TRACE")) {
+        size_t fr = 0, tot_mem = 0;
+        cudaMemGetInfo(&fr, &tot_mem);
+        fprintf(stderr,
+                "[cpsd] eecpsd_roots symR=%lld nroot=%lld roots per batch=%lld (free %.2f GB, arena spare %.2f GB, "
+                "idle pool %.2f GB)\n",
+                (long long)symR, (long long)nroot, (long long)chunk, fr / 1e9, arena().spare() / 1e9,
+                pool_idle_bytes() / 1e9);
+    }
     i64 tot = 0;
     for (i64 r = 0; r < nroot; r += chunk) {
         const i64 nb = std::min(chunk, nroot - r);

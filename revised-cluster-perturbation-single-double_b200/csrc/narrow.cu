@@ -10,6 +10,7 @@
 // there are too few rows to fill the GPU.  Both use the planner's task /
 // segment tables of the grouped contraction, so every layout that the
 // tensor-core path handles is handled here too.
+#include <atomic>
 #include <mutex>
 #include <algorithm>
 #include <map>
@@ -160,7 +161,26 @@ __device__ __forceinline__ double transpose_reduce(double (&v)[32]) {
     return v[0];
 }
 
-// long K: warp = 4 rows x 8 columns over the K range of the item
+__device__ __forceinline__ void nk_cp8(double *dst, const double *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void nk_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void nk_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// long K: warp = 4 rows x 8 columns over the K range of the item.  Lane l
+// takes the indices k = kb + l + 32 s of each segment; the 4 + 8 operand
+// values of step s are copied by cp.async into the lane's own slots of a
+// per-warp ring of NK_NS steps, NK_NS - 1 steps ahead of the FMAs, so the
+// loads in flight hold no registers (the lane reads back only what it
+// copied itself: the group wait is the only synchronisation).  Per lane the
+// sums run over its indices in order, then the fixed transpose reduction.
+constexpr int NK_NS = 6;                                   // ring depth (steps)
+constexpr int NK_VALS = NARROW_ROWS + NARROW_COLS;         // values per lane and step
+constexpr int NK_SMEM = NW * NK_NS * NK_VALS * 32 * 8;     // dynamic shared memory per CTA
 template <bool SWAP>
 __global__ void __launch_bounds__(NW * 32) k_narrow_k(const TaskDev *__restrict__ tasks,
                                                       const SegDev *__restrict__ segs,
@@ -168,6 +188,7 @@ __global__ void __launch_bounds__(NW * 32) k_narrow_k(const TaskDev *__restrict_
                                                       const double *__restrict__ A, const double *__restrict__ B,
                                                       double *__restrict__ C, double alpha,
                                                       double *__restrict__ partial) {
+    extern __shared__ double ring_all[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int it = blockIdx.x * NW + warp;
     if (it >= nitems) return;
@@ -177,6 +198,8 @@ __global__ void __launch_bounds__(NW * 32) k_narrow_k(const TaskDev *__restrict_
     const double *X = SWAP ? B : A, *Y = SWAP ? A : B;
     const int nrow = (int)min((i64)NARROW_ROWS, v.R() - item.r0);
     const int ncol = (int)min((i64)NARROW_COLS, v.CN() - item.c0);
+    // slot (step, value) of this lane at ring[(step * NK_VALS + value) * 32 + lane]
+    double *ring = ring_all + (size_t)warp * NK_NS * NK_VALS * 32 + lane;
     double acc[32];
 #pragma unroll
     for (int j = 0; j < 32; j++) acc[j] = 0.0;
@@ -192,20 +215,48 @@ __global__ void __launch_bounds__(NW * 32) k_narrow_k(const TaskDev *__restrict_
 #pragma unroll
         for (int c = 0; c < NARROW_COLS; c++) oy[c] = c < ncol ? v.ycol(sg, item.c0 + c) : 0;
         const i64 *kx = v.kx(sg), *ky = v.ky(sg);
-#pragma unroll 2
-        for (i64 k = kb + lane; k < ke; k += 32) {
-            i64 fx, fy;
-            kdecode(k, sg, kx, ky, &fx, &fy);
+        const i64 nsteps = (ke - kb + 31) / 32;
+        auto issue = [&](i64 st) {
+            if (st < nsteps) {
+                const i64 k = kb + lane + 32 * st;
+                double *d = ring + (size_t)(st % NK_NS) * NK_VALS * 32;
+                if (k < ke) {
+                    i64 fx, fy;
+                    kdecode(k, sg, kx, ky, &fx, &fy);
+#pragma unroll
+                    for (int i = 0; i < NARROW_ROWS; i++) {
+                        if (i < nrow) nk_cp8(d + i * 32, X + ox[i] + fx);
+                        else d[i * 32] = 0.0;
+                    }
+#pragma unroll
+                    for (int c = 0; c < NARROW_COLS; c++) {
+                        if (c < ncol) nk_cp8(d + (NARROW_ROWS + c) * 32, Y + oy[c] + fy);
+                        else d[(NARROW_ROWS + c) * 32] = 0.0;
+                    }
+                } else {
+#pragma unroll
+                    for (int j = 0; j < NK_VALS; j++) d[j * 32] = 0.0;
+                }
+            }
+            nk_commit();  // an empty group past the end keeps the count
+        };
+#pragma unroll
+        for (int st = 0; st < NK_NS - 1; st++) issue(st);
+        for (i64 st = 0; st < nsteps; st++) {
+            issue(st + NK_NS - 1);  // into the slot step st - 1 used
+            nk_wait<NK_NS - 1>();
+            const double *d = ring + (size_t)(st % NK_NS) * NK_VALS * 32;
             double x[NARROW_ROWS], y[NARROW_COLS];
 #pragma unroll
-            for (int i = 0; i < NARROW_ROWS; i++) x[i] = i < nrow ? __ldg(X + ox[i] + fx) : 0.0;
+            for (int i = 0; i < NARROW_ROWS; i++) x[i] = d[i * 32];
 #pragma unroll
-            for (int c = 0; c < NARROW_COLS; c++) y[c] = c < ncol ? __ldg(Y + oy[c] + fy) : 0.0;
+            for (int c = 0; c < NARROW_COLS; c++) y[c] = d[(NARROW_ROWS + c) * 32];
 #pragma unroll
             for (int i = 0; i < NARROW_ROWS; i++)
 #pragma unroll
                 for (int c = 0; c < NARROW_COLS; c++) acc[i * NARROW_COLS + c] = fma(x[i], y[c], acc[i * NARROW_COLS + c]);
         }
+        nk_wait<0>();
     }
     const double s = transpose_reduce(acc);
     if (item.part >= 0) {
@@ -348,10 +399,22 @@ int launch_narrow(const ContractPlan *cp, const NarrowPlan *np, const double *A,
         ScratchScope sc;
         double *part = nullptr;
         if (np->nparts > 0) CPSD_TRY(scratch(np->nparts * 32, &part));
+        static std::atomic<bool> attr{false};
+        if (!attr.load(std::memory_order_acquire)) {
+            CPSD_TRY(cuda_check(cudaFuncSetAttribute(k_narrow_k<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                     NK_SMEM),
+                                "narrow smem attr"));
+            CPSD_TRY(cuda_check(cudaFuncSetAttribute(k_narrow_k<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                     NK_SMEM),
+                                "narrow smem attr"));
+            attr.store(true, std::memory_order_release);
+        }
         if (np->swap)
-            k_narrow_k<true><<<grid, NW * 32, 0, stream()>>>(cp->d_tasks, cp->d_segs, np->d_items, ni, A, B, C, alpha, part);
+            k_narrow_k<true><<<grid, NW * 32, NK_SMEM, stream()>>>(cp->d_tasks, cp->d_segs, np->d_items, ni, A, B, C,
+                                                                   alpha, part);
         else
-            k_narrow_k<false><<<grid, NW * 32, 0, stream()>>>(cp->d_tasks, cp->d_segs, np->d_items, ni, A, B, C, alpha, part);
+            k_narrow_k<false><<<grid, NW * 32, NK_SMEM, stream()>>>(cp->d_tasks, cp->d_segs, np->d_items, ni, A, B, C,
+                                                                    alpha, part);
         count_launch();
         if (nr > 0) {
             const int rg = (nr + NW - 1) / NW;

@@ -279,6 +279,17 @@ bool evict_const_except(const double *keep) {
     for (const DigEntry &e : c.dig)
         if (kept_d(e)) kd.push_back(e);
     if (ke.size() == c.exp.size() && kd.size() == c.dig.size()) return false;
+    if (getenv("CPSD_TRACE")) {  // what gives way, for the memory picture of a run
+        size_t eb = 0, db = 0;
+        for (const ExpEntry &e : c.exp)
+            if (!kept_e(e)) eb += e.bytes;
+        for (const DigEntry &e : c.dig)
+            if (!kept_d(e)) db += e.dbytes + e.ebytes;
+        size_t fr = 0, tot = 0;
+        cudaMemGetInfo(&fr, &tot);
+        fprintf(stderr, "[cpsd] evict: expanded copies %.2f GB (%zu), digit tiles %.2f GB (%zu); free %.2f GB\n",
+                eb / 1e9, c.exp.size() - ke.size(), db / 1e9, c.dig.size() - kd.size(), fr / 1e9);
+    }
     cudaStreamSynchronize(stream());
     for (const ExpEntry &e : c.exp)
         if (!kept_e(e)) pool_put(e.buf, e.bytes);
