@@ -68,7 +68,9 @@ def parse():
     ap.add_argument("--directions", type=int, default=200, help="finite-difference directions of --case grad")
     ap.add_argument("--workers", type=int, default=8, help="concurrent molecules of --case batch")
     ap.add_argument("--wave-gb", type=float, default=140.0, help="device-memory budget of one --case batch wave")
-    ap.add_argument("--case", default="", choices=["", "ladder", "grad", "batch"],
+    ap.add_argument("--kernel", default="c1_r2abci", choices=sorted(KERNEL_CASES),
+                    help="lib_cc kernel of --case kernel")
+    ap.add_argument("--case", default="", choices=["", "ladder", "grad", "batch", "kernel"],
                     help="time one contraction on its own (kernel profiling) instead of the pipeline")
     a = ap.parse_args()
     if a.digits < 0:
@@ -605,6 +607,58 @@ def run_case(args):
           flush=True)
 
 
+# --case kernel: lib_cc kernels on the workload's integrals, operand layouts
+# as (pop letters, iops): out, amplitude, integral list
+KERNEL_CASES = {
+    "c1_r2abci": (("vozz", (1, 1)), ("vvoo", (0, 0)), "abci"),   # long-K narrow kernel
+    "c2_r1abci": (("vvoo", (0, 0)), ("vozz", (1, 1)), "abci"),   # short-K narrow kernel
+    "Wmbej_r1abci": (("vovo", (1, 1)), ("vozz", (1, 1)), "abci"),  # row-dot kernel
+    "c1_r1iabj": (("vozz", (1, 1)), ("vozz", (1, 1)), "iabj"),   # CIS sigma
+}
+
+
+def run_kernel_case(args):
+    """One lib_cc kernel (--kernel) of the pipeline on its own, on the
+    integrals of --config (resident in HBM) and a random amplitude of irrep
+    1: --warmup untimed calls, then --steps timed ones (CUDA events).  For
+    kernel profiling: the launches are the kernel's own (and, for an integral
+    the engine expands, the pair transform of the first call)."""
+    import torch
+    import __graft_entry__ as ge
+    ge.load_package()
+    from cpsd_b200 import api, synth
+    big, s = big_workload(args.config)
+    api.init(s.nirrep, s.dirprd)
+    api.use_torch_stream()
+    ints = api.DeviceIntegrals.from_tensors(synth.device_integrals(s)) if big else api.DeviceIntegrals(s)
+    zorb = np.array([1, 0, 0, 0, 0, 0, 0, 0], np.int64)
+    space = {"o": s.popo, "v": s.popv, "z": zorb}
+    (lo, io), (la, ia), vname = KERNEL_CASES[args.kernel]
+    po, pa = [space[c] for c in lo], [space[c] for c in la]
+    g = torch.Generator(device="cuda").manual_seed(0)
+    na = s.sym.idsymsoc(1, pa[0], pa[1], ia[0], pa[2], pa[3], ia[1])
+    no = s.sym.idsymsoc(1, po[0], po[1], io[0], po[2], po[3], io[1])
+    a = torch.randn(na, dtype=torch.float64, device="cuda", generator=g)
+    out = torch.zeros(no, dtype=torch.float64, device="cuda")
+    V = ints.t[vname]
+    vpops = {"abci": ("vvvo", (0, 1)), "iabj": ("vovo", (1, 1))}[vname]
+    pv = [space[c] for c in vpops[0]]
+    O, A, B = api.opt(po, io, 1, out), api.opt(pa, ia, 1, a), api.opt(pv, vpops[1], 1, V)
+    for _ in range(args.warmup):
+        api.kernel(args.kernel, O, A, B, 1.0)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        api.kernel(args.kernel, O, A, B, 1.0)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    vb = V.numel() * 8
+    print(json.dumps({"case": "kernel", "kernel": args.kernel, "config": args.config, "ms_per_call": ms,
+                      "integral_bytes": vb, "integral_GBps": vb / (ms / 1e3) / 1e9}), flush=True)
+
+
 def run_grad(args):
     """Differentiation form: C2v, nmo 120, nocc 8/6, 4 roots of irrep 1.
     Times the SF-CIS(D) energies (cpsd_cisd_energies: Davidson to 1e-12 and
@@ -804,6 +858,9 @@ def main():
         return
     if args.case == "batch":
         run_batch(args)
+        return
+    if args.case == "kernel":
+        run_kernel_case(args)
         return
     if args.case:
         run_case(args)

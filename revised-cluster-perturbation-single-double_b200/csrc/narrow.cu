@@ -178,7 +178,7 @@ __device__ __forceinline__ void nk_wait() {
 // loads in flight hold no registers (the lane reads back only what it
 // copied itself: the group wait is the only synchronisation).  Per lane the
 // sums run over its indices in order, then the fixed transpose reduction.
-constexpr int NK_NS = 6;                                   // ring depth (steps)
+constexpr int NK_NS = 4;                                   // ring depth (steps)
 constexpr int NK_VALS = NARROW_ROWS + NARROW_COLS;         // values per lane and step
 constexpr int NK_SMEM = NW * NK_NS * NK_VALS * 32 * 8;     // dynamic shared memory per CTA
 template <bool SWAP>

@@ -3,6 +3,7 @@
 #include "ops.hpp"
 
 #include <algorithm>
+#include <tuple>
 
 #include "drivers.hpp"
 #include "narrow.cuh"
@@ -261,43 +262,80 @@ bool is_const_operand(const double *a) {
     return false;
 }
 
-// Cached copies give way when device memory runs out: every copy the
-// running program keeps, except those handed to the operation in progress
-// and those made of `keep` (the operand being requested), goes back to the
-// pool once the stream has finished the kernels that read it, and the idle
-// pool is freed.  Returns false when there was nothing to evict.
-bool evict_const_except(const double *keep) {
+// Cached copies give way when device memory runs out: copies the running
+// program keeps, except those handed to the operation in progress and those
+// made of `keep` (the operand being requested), go back to the pool once the
+// stream has finished the kernels that read it, and the idle pool is freed.
+// With a request of `need` bytes only what covers it goes: the smallest copy
+// that does alone, else the smallest ones together (a copy is rebuilt at a
+// cost that grows with its size, so the large digit tiles of abcd stay while
+// smaller copies can make room); with need 0, all of them.  Returns false
+// when there was nothing to evict.
+bool evict_const_except(const double *keep, size_t need) {
     ConstOps &c = const_ops();
     auto kept_e = [&](const ExpEntry &e) { return e.used == c.epoch || e.src == keep || e.buf == keep; };
     auto kept_d = [&](const DigEntry &e) { return e.used == c.epoch || e.src == keep; };
+    // candidates: (bytes, expanded copy?, index)
+    std::vector<std::tuple<size_t, int, size_t>> cand;
+    for (size_t i = 0; i < c.exp.size(); i++)
+        if (!kept_e(c.exp[i])) cand.emplace_back(c.exp[i].bytes, 1, i);
+    for (size_t i = 0; i < c.dig.size(); i++)
+        if (!kept_d(c.dig[i])) cand.emplace_back(c.dig[i].dbytes + c.dig[i].ebytes, 0, i);
+    if (cand.empty()) return false;
+    std::sort(cand.begin(), cand.end());
+    size_t fr = 0, tot = 0;
+    if (need) cudaMemGetInfo(&fr, &tot);
+    const size_t target = need + ((size_t)256 << 20);  // 256 MB to spare
+    const size_t deficit = need ? (target > fr ? target - fr : 1) : 0;
+    std::vector<char> drop_e(c.exp.size(), 0), drop_d(c.dig.size(), 0);
+    auto drop = [&](const std::tuple<size_t, int, size_t> &t) {
+        (std::get<1>(t) ? drop_e : drop_d)[std::get<2>(t)] = 1;
+    };
+    if (!need) {
+        for (const auto &t : cand) drop(t);
+    } else {
+        auto one = std::find_if(cand.begin(), cand.end(), [&](const auto &t) { return std::get<0>(t) >= deficit; });
+        if (one != cand.end()) {
+            drop(*one);
+        } else {
+            size_t freed = 0;
+            for (const auto &t : cand) {
+                if (freed >= deficit) break;
+                drop(t);
+                freed += std::get<0>(t);
+            }
+        }
+    }
+    if (getenv("CPSD_TRACE")) {  // what gives way, for the memory picture of a run
+        size_t eb = 0, db = 0, ne = 0, nd = 0;
+        for (size_t i = 0; i < c.exp.size(); i++)
+            if (drop_e[i]) eb += c.exp[i].bytes, ne++;
+        for (size_t i = 0; i < c.dig.size(); i++)
+            if (drop_d[i]) db += c.dig[i].dbytes + c.dig[i].ebytes, nd++;
+        fprintf(stderr,
+                "[cpsd] evict: expanded copies %.2f GB (%zu), digit tiles %.2f GB (%zu) for %.2f GB; free %.2f GB\n",
+                eb / 1e9, ne, db / 1e9, nd, need / 1e9, fr / 1e9);
+    }
+    cudaStreamSynchronize(stream());
     std::vector<ExpEntry> ke;
     std::vector<DigEntry> kd;
     std::vector<const double *> dropped;
-    for (const ExpEntry &e : c.exp)
-        if (kept_e(e)) ke.push_back(e);
-        else dropped.push_back(e.buf);
-    for (const DigEntry &e : c.dig)
-        if (kept_d(e)) kd.push_back(e);
-    if (ke.size() == c.exp.size() && kd.size() == c.dig.size()) return false;
-    if (getenv("CPSD_TRACE")) {  // what gives way, for the memory picture of a run
-        size_t eb = 0, db = 0;
-        for (const ExpEntry &e : c.exp)
-            if (!kept_e(e)) eb += e.bytes;
-        for (const DigEntry &e : c.dig)
-            if (!kept_d(e)) db += e.dbytes + e.ebytes;
-        size_t fr = 0, tot = 0;
-        cudaMemGetInfo(&fr, &tot);
-        fprintf(stderr, "[cpsd] evict: expanded copies %.2f GB (%zu), digit tiles %.2f GB (%zu); free %.2f GB\n",
-                eb / 1e9, c.exp.size() - ke.size(), db / 1e9, c.dig.size() - kd.size(), fr / 1e9);
-    }
-    cudaStreamSynchronize(stream());
-    for (const ExpEntry &e : c.exp)
-        if (!kept_e(e)) pool_put(e.buf, e.bytes);
-    for (const DigEntry &e : c.dig)
-        if (!kept_d(e)) {
-            pool_put(e.dig, e.dbytes);
-            pool_put(e.expo, e.ebytes);
+    for (size_t i = 0; i < c.exp.size(); i++) {
+        if (drop_e[i]) {
+            pool_put(c.exp[i].buf, c.exp[i].bytes);
+            dropped.push_back(c.exp[i].buf);
+        } else {
+            ke.push_back(c.exp[i]);
         }
+    }
+    for (size_t i = 0; i < c.dig.size(); i++) {
+        if (drop_d[i]) {
+            pool_put(c.dig[i].dig, c.dig[i].dbytes);
+            pool_put(c.dig[i].expo, c.dig[i].ebytes);
+        } else {
+            kd.push_back(c.dig[i]);
+        }
+    }
     c.exp.swap(ke);
     c.dig.swap(kd);
     // an evicted expanded copy is no longer a constant operand
@@ -312,7 +350,7 @@ bool evict_const_except(const double *keep) {
 
 }  // namespace
 
-bool evict_cached_copies() { return evict_const_except(nullptr); }
+bool evict_cached_copies(size_t need) { return evict_const_except(nullptr, need); }
 
 namespace {
 
@@ -370,7 +408,7 @@ int digits_of(const OzPlan *oz, bool sideA, const double *src, int8_t **dig, int
         if (!(d && x)) {
             pool_put(d, db);
             d = nullptr;
-            if (evict_const_except(src)) {
+            if (evict_const_except(src, db + eb)) {
                 d = (int8_t *)pool_get(db);
                 x = d ? (int *)pool_get(eb) : nullptr;
             }
@@ -430,7 +468,7 @@ int expand_cached(const Ten &v, bool e0, bool e1, Ten *out, bool *done) {
     CPSD_TRY(plan_pairmap(v.d, e0 ? PAIR_EXPAND : PAIR_ID, e1 ? PAIR_EXPAND : PAIR_ID, 1, 1, &d, &pm));
     const size_t bytes = sizeof(double) * (size_t)std::max<i64>(d.len(), 1);
     double *buf = (double *)pool_get(bytes);
-    if (!buf && evict_const_except(v.arr)) buf = (double *)pool_get(bytes);
+    if (!buf && evict_const_except(v.arr, bytes)) buf = (double *)pool_get(bytes);
     if (!buf) return CPSD_OK;  // no room to keep it: expand into scratch as usual
     c.exp.push_back({v.arr, key, d, buf, bytes, c.epoch});
     c.arrs.push_back(buf);  // derived from a constant operand: constant too

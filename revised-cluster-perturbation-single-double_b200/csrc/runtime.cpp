@@ -161,7 +161,7 @@ int Arena::alloc(size_t bytes, void **out) {
             if (cudaMalloc(&p, sz) != cudaSuccess) {
                 cudaGetLastError();
                 // then the copies this run keeps for later operations
-                if (!evict_cached_copies() || cudaMalloc(&p, sz) != cudaSuccess) {
+                if (!evict_cached_copies(sz) || cudaMalloc(&p, sz) != cudaSuccess) {
                     cudaGetLastError();
                     return set_error(CPSD_EMEM,
                                      "cudaMalloc of scratch failed (" + std::to_string(bytes) + " bytes)");

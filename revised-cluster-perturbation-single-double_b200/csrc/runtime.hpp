@@ -117,7 +117,7 @@ std::mutex &upload_mutex();
 void pool_release_idle();
 // frees the constant-operand copies a program keeps that the operation in
 // progress was not handed (false: nothing to free)
-bool evict_cached_copies();
+bool evict_cached_copies(size_t need = 0);  // least recently used first until `need` bytes are free (0: all)
 size_t pool_idle_bytes();
 struct ScratchScope {
     Arena::Mark m;
