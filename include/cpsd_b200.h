@@ -477,6 +477,16 @@ int cpsd_pipeline(const cpsd_system *s, const cpsd_integrals *I, const cpsd_para
 /* on = 0: run the pipeline's phases one after the other on the caller's
  * stream (default 1: SF-CIS beside the ground state) */
 int cpsd_set_phase_overlap(int on);
+/* Empirical tile-shape choice for the FP64 tile kernel (off by default):
+ * with it on, the first launch of each contraction plan runs its four tile
+ * shapes (128x64, 128x32, 64x128, 64x64) on a scratch copy of the output,
+ * times them with CUDA events and keeps the fastest (the cost model's shape
+ * unless another is 3 % faster) for every later launch of that plan.  The
+ * sums of different shapes differ in rounding, and the choice can differ
+ * from run to run.  cpsd_tile_autotune_stats: plans tuned, plans whose
+ * shape the tuning changed, since the process started. */
+int cpsd_set_tile_autotune(int on);
+int cpsd_tile_autotune_stats(int64_t *tuned, int64_t *changed);
 
 /* Independent molecules in one call (no counterpart in the reference, which
  * runs one molecule per program invocation): cpsd_pipeline of molecule m

@@ -142,6 +142,18 @@ def contract_timing(on=True, reset=True):
         check(lib().cpsd_contract_time(None, None, None, ctypes.c_int(1)), "cpsd_contract_time")
 
 
+def set_tile_autotune(on=True):
+    """empirical tile-shape choice of the FP64 tile kernel on / off"""
+    check(lib().cpsd_set_tile_autotune(ctypes.c_int(1 if on else 0)), "cpsd_set_tile_autotune")
+
+
+def tile_autotune_stats():
+    """(plans tuned, plans whose tile shape the tuning changed)"""
+    a, b = I64(), I64()
+    check(lib().cpsd_tile_autotune_stats(ctypes.byref(a), ctypes.byref(b)), "cpsd_tile_autotune_stats")
+    return a.value, b.value
+
+
 def davidson_stats(reset=True):
     """(steps that solved the general non-symmetric Ritz problem, complex Ritz
     values met) on this thread since the last reset"""

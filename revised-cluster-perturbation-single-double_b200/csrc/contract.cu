@@ -13,6 +13,9 @@
 #include <array>
 #include <vector>
 
+#include <map>
+#include <memory>
+#include <mutex>
 #include "runtime.hpp"
 
 namespace cpsd {
@@ -333,8 +336,111 @@ int contract_time(double *ms, int64_t *launches, double *flops, int reset) {
     return CPSD_OK;
 }
 
+namespace {
+// the empirical tile-shape choice: per plan, the variant that ran fastest
+std::atomic<int> g_autotune{0};
+std::atomic<int64_t> g_tuned{0}, g_changed{0};
+std::mutex &tune_mutex() {
+    static std::mutex m;
+    return m;
+}
+std::map<const ContractPlan *, const ContractPlan *> &tuned_plans() {
+    static std::map<const ContractPlan *, const ContractPlan *> m;
+    return m;
+}
+std::vector<std::unique_ptr<ContractPlan>> &tuned_variants() {
+    static std::vector<std::unique_ptr<ContractPlan>> v;
+    return v;
+}
+// one past the largest output offset a plan writes
+i64 plan_c_extent(const ContractPlan *p) {
+    i64 hi = 0;
+    for (const TaskDev &t : p->h_tasks) {
+        i64 e = t.baseC;
+        for (int u = 0; u < t.nm; u++) e += (t.mExt[u] - 1) * t.mSC[u];
+        for (int u = 0; u < t.nn; u++) e += (t.nExt[u] - 1) * t.nSC[u];
+        hi = std::max(hi, e + 1);
+    }
+    return hi;
+}
+int launch_tiles(const ContractPlan *p, const double *A, const double *B, double *C, double alpha);
+// the fastest of the four tile shapes for plan p, timed on a scratch output
+int tune_plan(const ContractPlan *p, const double *A, const double *B, const ContractPlan **best) {
+    *best = p;
+    const i64 n = plan_c_extent(p);
+    ScratchScope sc;
+    double *Ct;
+    CPSD_TRY(scratch(n, &Ct));
+    CPSD_TRY(cuda_check(cudaMemsetAsync(Ct, 0, sizeof(double) * (size_t)n, stream()), "tune scratch"));
+    cudaEvent_t e0, e1;
+    CPSD_TRY(cuda_check(cudaEventCreate(&e0), "event"));
+    CPSD_TRY(cuda_check(cudaEventCreate(&e1), "event"));
+    float best_ms = 1e30f;
+    int rc = CPSD_OK;
+    for (int c = 0; c < 4 && rc == CPSD_OK; c++) {
+        const ContractPlan *q = p;
+        if (c != p->cfg) {
+            auto v = std::make_unique<ContractPlan>();
+            v->flops = p->flops;
+            v->task_mkey = p->task_mkey;
+            v->task_nkey = p->task_nkey;
+            v->seg_kkey = p->seg_kkey;
+            finish_plan(v.get(), p->h_tasks, p->h_segs, c);
+            q = v.get();
+            tuned_variants().push_back(std::move(v));
+        }
+        float ms = 0.f;
+        for (int rep = 0; rep < 2 && rc == CPSD_OK; rep++) {  // the second run is timed
+            rc = cuda_check(cudaEventRecord(e0, stream()), "event record");
+            if (rc == CPSD_OK) rc = launch_tiles(q, A, B, Ct, 1.0);
+            if (rc == CPSD_OK) rc = cuda_check(cudaEventRecord(e1, stream()), "event record");
+            if (rc == CPSD_OK) rc = cuda_check(cudaEventSynchronize(e1), "event sync");
+            if (rc == CPSD_OK) rc = cuda_check(cudaEventElapsedTime(&ms, e0, e1), "event time");
+        }
+        if (rc == CPSD_OK && ms < best_ms * 0.97f) {  // the cost model's shape unless 3 % faster
+            best_ms = ms;
+            *best = q;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return rc;
+}
+}  // namespace
+
+int set_tile_autotune(int on) {
+    g_autotune.store(on ? 1 : 0);
+    return CPSD_OK;
+}
+int tile_autotune_stats(int64_t *tuned, int64_t *changed) {
+    if (tuned) *tuned = g_tuned.load();
+    if (changed) *changed = g_changed.load();
+    return CPSD_OK;
+}
+
 int launch_contract(const ContractPlan *p, const double *A, const double *B, double *C, double alpha) {
     if (p->empty) return CPSD_OK;
+    if (g_autotune.load()) {
+        const ContractPlan *q = nullptr;
+        {
+            std::lock_guard<std::mutex> lock(tune_mutex());
+            auto it = tuned_plans().find(p);
+            if (it != tuned_plans().end()) q = it->second;
+        }
+        if (!q) {
+            std::lock_guard<std::mutex> lock(tune_mutex());
+            CPSD_TRY(tune_plan(p, A, B, &q));
+            tuned_plans()[p] = q;
+            g_tuned++;
+            if (q != p) g_changed++;
+        }
+        p = q;
+    }
+    return launch_tiles(p, A, B, C, alpha);
+}
+
+namespace {
+int launch_tiles(const ContractPlan *p, const double *A, const double *B, double *C, double alpha) {
     CPSD_TRY(const_cast<ContractPlan *>(p)->upload());
     const int bm = TILE_BM[p->cfg], bn = TILE_BN[p->cfg];
     double *part = nullptr;
@@ -388,6 +494,7 @@ int launch_contract(const ContractPlan *p, const double *A, const double *B, dou
     }
     return cuda_check(cudaGetLastError(), "k_contract");
 }
+}  // namespace
 
 // ------------------------------------------- contraction without allocation
 // Some callers may not allocate device memory while they run a contraction:

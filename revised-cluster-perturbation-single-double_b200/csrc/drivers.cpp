@@ -1771,6 +1771,9 @@ int cpsd_pipeline(const cpsd_system *s, const cpsd_integrals *I, const cpsd_para
     return CPSD_OK;
 }
 
+int cpsd_set_tile_autotune(int on) { return set_tile_autotune(on); }
+int cpsd_tile_autotune_stats(int64_t *tuned, int64_t *changed) { return tile_autotune_stats(tuned, changed); }
+
 int cpsd_set_phase_overlap(int on) {
     g_phase_overlap.store(on != 0);
     return CPSD_OK;

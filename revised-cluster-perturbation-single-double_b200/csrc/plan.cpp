@@ -94,12 +94,14 @@ int EnergyPlan::upload() {
 
 // Tile shape, tiles and split-K groups of a plan whose tasks and segments
 // are built: the shape with the least estimated time counting the padded
-// tensor-pipe work (FP64 ~35 TFLOP/s) and the operand re-reads (~6 TB/s);
-// split-K so that small outputs with long K still fill the GPU
-void finish_plan(ContractPlan *plan, std::vector<TaskDev> tasks, std::vector<SegDev> dsegs) {
+// tensor-pipe work (FP64 ~35 TFLOP/s) and the operand re-reads (~6 TB/s),
+// or force_cfg when it is >= 0; split-K so that small outputs with long K
+// still fill the GPU
+void finish_plan(ContractPlan *plan, std::vector<TaskDev> tasks, std::vector<SegDev> dsegs, int force_cfg) {
     int cfg = 0;
     double best = 1e300;
     for (int c = 0; c < 4; c++) {
+        if (force_cfg >= 0 && c != force_cfg) continue;
         double fl = 0, by = 0;
         for (auto &tk : tasks) {
             double mt = (double)((tk.M + TILE_BM[c] - 1) / TILE_BM[c]), nt = (double)((tk.N + TILE_BN[c] - 1) / TILE_BN[c]);

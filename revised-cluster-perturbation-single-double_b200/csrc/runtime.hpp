@@ -184,6 +184,14 @@ struct Batch {
 };
 int plan_contract(const Desc &d1, const char *t1, const Desc &d2, const char *t2, const Desc &d3,
                   const char *t3, const Batch &batch, const ContractPlan **out);
+// tiles of a plan whose tasks and segments are built (force_cfg >= 0: that
+// tile shape instead of the cost model's)
+void finish_plan(ContractPlan *plan, std::vector<TaskDev> tasks, std::vector<SegDev> dsegs, int force_cfg = -1);
+// empirical tile-shape choice (off by default): with it on, the first
+// launch of each FP64 tile plan times the four tile shapes on a scratch
+// copy of the output and later launches use the fastest
+int set_tile_autotune(int on);
+int tile_autotune_stats(int64_t *tuned, int64_t *changed);
 
 // C[m + n ldc + r sC] += A[m + k lda] B[k + n ldb + r sB] (m < M, n < N,
 // k < K, r < nb) as a one-task plan of the tile kernel

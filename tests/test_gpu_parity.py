@@ -127,6 +127,26 @@ def test_streaming_kernels_ran_and_match_oracle(name, kind, nirrep):
     np.testing.assert_allclose(host(to), ref, rtol=0, atol=1e-12, err_msg=name)
 
 
+def test_tile_autotune_matches_oracle():
+    """With the empirical tile-shape choice on, the FP64 pipeline still
+    matches the oracle and the tuner timed the tile plans it met."""
+    s = synth.make("c2v_nmo48")
+    ints, sc, par, orc = _run_both(s)
+    api.set_mixed(0, 1.0)
+    t0, _ = api.tile_autotune_stats()
+    api.set_tile_autotune(True)
+    try:
+        om, w2, w3 = api.pipeline(s, sc, ints, par)
+    finally:
+        api.set_tile_autotune(False)
+    t1, c1 = api.tile_autotune_stats()
+    assert t1 > t0
+    oom, ow2, ow3 = orc.pipeline()
+    np.testing.assert_allclose(om, oom, rtol=0, atol=TOL_E)
+    np.testing.assert_allclose(w2, ow2, rtol=0, atol=TOL_E)
+    np.testing.assert_allclose(w3, ow3, rtol=0, atol=TOL_E)
+
+
 def _run_both(s, batch_roots=1, **kw):
     api.init(s.nirrep, s.dirprd)
     ints = api.DeviceIntegrals(s)
