@@ -126,11 +126,15 @@ struct OzCfg {
     static constexpr int A_STAGE = S * 128 * OZ_BK;  // bytes of the A digit tiles of one stage
     static constexpr int B_STAGE = S * BN * OZ_BK;
     static constexpr int STAGE = A_STAGE + B_STAGE;
-    static constexpr int NST = (200 * 1024) / STAGE >= 4 ? 4 : (200 * 1024) / STAGE;
+    // stages in the ring: as many as fit in 220 KB (at most 4); the CTA's
+    // dynamic shared memory is NST stages + 1 KB of alignment slack, within
+    // the 227 KB a CTA may have
+    static constexpr int NST = (220 * 1024) / STAGE >= 4 ? 4 : (220 * 1024) / STAGE;
     static constexpr int SMEM = NST * STAGE + 1024;
     static constexpr int NCOL_RAW = S * BN;
     static constexpr int NCOL = NCOL_RAW <= 32 ? 32 : NCOL_RAW <= 64 ? 64 : NCOL_RAW <= 128 ? 128 : NCOL_RAW <= 256 ? 256 : 512;
     static_assert(NST >= 2, "at least two pipeline stages");
+    static_assert(SMEM <= 227 * 1024, "dynamic shared memory above the per-CTA limit");
     static_assert(NCOL_RAW <= 512, "accumulators exceed TMEM");
 };
 
