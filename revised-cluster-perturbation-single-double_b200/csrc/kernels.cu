@@ -87,6 +87,65 @@ __global__ void __launch_bounds__(PM_T) k_pairmap(const PMBlockDev *__restrict__
     }
 }
 
+// The same map over tiles of 256 rows x 8 columns of one block (plans whose
+// elements sit mostly in blocks of at least 256 rows): thread t takes row
+// l = 256 tl + t, reads its row map entries once, then issues the input
+// loads of the tile's 8 columns together and stores them (coalesced along
+// the rows).  Same sums in the same order as k_pairmap.
+template <int LT, int RT>
+__global__ void __launch_bounds__(PM_T) k_pairmap_cols(const PMBlockDev *__restrict__ blocks, int nblocks,
+                                                       const i64 *__restrict__ tstart, i64 ntiles,
+                                                       const long long *__restrict__ idx,
+                                                       const double *__restrict__ sgn,
+                                                       const double *__restrict__ in0, double *__restrict__ out0,
+                                                       double alpha, double beta, i64 nb, i64 sin, i64 sout) {
+    constexpr int NC = 8;
+    for (i64 tile = blockIdx.x; tile < ntiles * nb; tile += gridDim.x) {
+        const i64 cpy = tile / ntiles, t = tile - cpy * ntiles;
+        int b = 0, hi = nblocks - 1;  // last block whose tiles start at or before t
+        while (b < hi) {
+            const int mid = (b + hi + 1) >> 1;
+            if (tstart[mid] <= t) b = mid;
+            else hi = mid - 1;
+        }
+        const PMBlockDev B = blocks[b];
+        const i64 ntl = (B.nlo + PM_T - 1) / PM_T, loc = t - tstart[b];
+        const i64 r0 = (loc / ntl) * NC, l = (loc % ntl) * PM_T + threadIdx.x;
+        if (l >= B.nlo) continue;
+        const double *in = in0 + cpy * sin;
+        double *out = out0 + cpy * sout;
+        long long li[LT];
+        double sl[LT];
+#pragma unroll
+        for (int tq = 0; tq < LT; tq++) {
+            li[tq] = idx[B.lmap + l * LT + tq];
+            sl[tq] = sgn[B.lmap + l * LT + tq];
+        }
+        const int nc = (int)min((i64)NC, B.nro - r0);
+        double v[NC];
+#pragma unroll
+        for (int c = 0; c < NC; c++) {
+            v[c] = 0.0;
+            if (c < nc)
+#pragma unroll
+                for (int tr = 0; tr < RT; tr++) {
+                    const i64 ri = idx[B.rmap + (r0 + c) * RT + tr];
+                    if (ri < 0) continue;
+                    const double sr = sgn[B.rmap + (r0 + c) * RT + tr];
+#pragma unroll
+                    for (int tq = 0; tq < LT; tq++)
+                        if (li[tq] >= 0) v[c] += sr * sl[tq] * in[B.inBase + ri * B.nli + li[tq]];
+                }
+        }
+#pragma unroll
+        for (int c = 0; c < NC; c++)
+            if (c < nc) {
+                const i64 o = B.outBase + (r0 + c) * B.nlo + l;
+                out[o] = (beta == 0.0) ? alpha * v[c] : beta * out[o] + alpha * v[c];
+            }
+    }
+}
+
 __global__ void k_energy(const i64 *__restrict__ blk, int nblocks, i64 n, const i64 *__restrict__ lidx,
                          const i64 *__restrict__ ridx, const double *__restrict__ eorb, int mode,
                          const double *__restrict__ in0, double *__restrict__ out0, const double *__restrict__ w0v,
@@ -242,10 +301,25 @@ int launch_pairmap(const PairMapPlan *p, const double *in, double *out, double a
     cudaEvent_t end;
     CPSD_TRY(timing_begin(0.0, p->total, nb, p->lterms * p->rterms, 40, &end));
     const i64 tiles = (p->total + PM_TILE - 1) / PM_TILE * nb;
-    k_pairmap<<<(unsigned)std::min<i64>(tiles, 148 * 16), PM_T, 0, stream()>>>(p->d_blocks, p->nblocks, p->total,
-                                                                              p->d_idx, p->d_sgn, p->lterms,
-                                                                              p->rterms, in, out, alpha, beta, nb,
-                                                                              in_stride, out_stride);
+    if (p->tiled) {
+        const unsigned grid = (unsigned)std::min<i64>(p->ntiles * nb, 148 * 16);
+        if (p->lterms == 1 && p->rterms == 1)
+            k_pairmap_cols<1, 1><<<grid, PM_T, 0, stream()>>>(p->d_blocks, p->nblocks, p->d_tstart, p->ntiles,
+                                                              p->d_idx, p->d_sgn, in, out, alpha, beta, nb,
+                                                              in_stride, out_stride);
+        else if (p->lterms == 2)
+            k_pairmap_cols<2, 1><<<grid, PM_T, 0, stream()>>>(p->d_blocks, p->nblocks, p->d_tstart, p->ntiles,
+                                                              p->d_idx, p->d_sgn, in, out, alpha, beta, nb,
+                                                              in_stride, out_stride);
+        else
+            k_pairmap_cols<1, 2><<<grid, PM_T, 0, stream()>>>(p->d_blocks, p->nblocks, p->d_tstart, p->ntiles,
+                                                              p->d_idx, p->d_sgn, in, out, alpha, beta, nb,
+                                                              in_stride, out_stride);
+    } else {
+        k_pairmap<<<(unsigned)std::min<i64>(tiles, 148 * 16), PM_T, 0, stream()>>>(
+            p->d_blocks, p->nblocks, p->total, p->d_idx, p->d_sgn, p->lterms, p->rterms, in, out, alpha, beta, nb,
+            in_stride, out_stride);
+    }
     count_launch();
     CPSD_TRY(cuda_check(cudaGetLastError(), "k_pairmap"));
     return timing_end(end);

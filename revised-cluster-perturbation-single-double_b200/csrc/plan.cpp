@@ -74,6 +74,7 @@ int PairMapPlan::upload() {
     CPSD_TRY(cpsd::upload(h_blocks, &d_blocks));
     CPSD_TRY(cpsd::upload(h_idx, &d_idx));
     CPSD_TRY(cpsd::upload(h_sgn, &d_sgn));
+    if (tiled) CPSD_TRY(cpsd::upload(h_tstart, &d_tstart));
     // the tables may next be read by kernels on another thread's stream
     CPSD_TRY(cuda_check(cudaStreamSynchronize(stream()), "plan upload"));
     uploaded.store(true, std::memory_order_release);
@@ -637,6 +638,19 @@ int plan_pairmap(const Desc &din, int op0, int op1, i64 target_iop0, i64 target_
     }
     plan->nblocks = (int)blocks.size();
     plan->total = start;
+    // column tiling pays when most elements sit in blocks of at least 256
+    // rows: each tile reads its rows' map entries once for 8 columns
+    {
+        i64 tall = 0, nt = 0;
+        for (const PMBlockDev &b : blocks) {
+            if (b.nlo >= 256) tall += b.nlo * b.nro;
+            plan->h_tstart.push_back(nt);
+            nt += ((b.nlo + 255) / 256) * ((b.nro + 7) / 8);
+        }
+        plan->ntiles = nt;
+        plan->tiled = start > 0 && tall >= start * 9 / 10 && plan->lterms * plan->rterms <= 2;
+        if (!plan->tiled) plan->h_tstart.clear();
+    }
     plan->h_blocks = std::move(blocks);
     plan->h_idx = std::move(idx);
     plan->h_sgn = std::move(sgn);

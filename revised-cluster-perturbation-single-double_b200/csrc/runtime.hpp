@@ -213,6 +213,12 @@ struct PairMapPlan {
     PMBlockDev *d_blocks = nullptr;
     long long *d_idx = nullptr;  // index maps (terms interleaved)
     double *d_sgn = nullptr;
+    // column tiling (256 rows x 8 columns per tile) when the blocks are
+    // tall: first tile of each block and the tile count
+    bool tiled = false;
+    std::vector<i64> h_tstart;
+    i64 ntiles = 0;
+    i64 *d_tstart = nullptr;
     int upload();
 };
 enum PairOp { PAIR_ID = 0, PAIR_EXPAND, PAIR_COMPRESS, PAIR_ANTI, PAIR_ANTI_COMPRESS, PAIR_SWAP };

@@ -131,3 +131,17 @@ def test_synthetic_inputs_round_trip(tmp_path):
         s.sym.idsymsoc(1, s.popv, s.popv, 1, s.popo, s.popo, 1)))
     with pytest.raises(api.CpsdError, match="iops"):
         api.load_inputs(str(tmp_path), ipath, sc, s.lengths(), len(s.eorb))
+
+
+def test_orbital_map_matches_spin_orbital_order():
+    """api.orbital_map (the (mo, spin) map of cpsd_eri_lists /
+    cpsd_eri_adjoint) lists the spin-free orbitals in the DPD lists' order,
+    the order of the independent dense reference."""
+    import dense
+    from cpsd_b200 import api, synth
+    for nirrep in (1, 2, 4, 8):
+        s = synth.System(nmo=16 if nirrep < 8 else 24, nocc_a=4, nocc_b=2, nirrep=nirrep, seed=1)
+        mo, sp = api.orbital_map(s)
+        occ, vir = dense.spin_orbitals(s)
+        assert list(zip(mo.tolist(), sp.tolist())) == occ + vir
+        assert len(mo) == int(sum(s.popo) + sum(s.popv))
