@@ -307,12 +307,16 @@ int launch_pairmap(const PairMapPlan *p, const double *in, double *out, double a
             k_pairmap_cols<1, 1><<<grid, PM_T, 0, stream()>>>(p->d_blocks, p->nblocks, p->d_tstart, p->ntiles,
                                                               p->d_idx, p->d_sgn, in, out, alpha, beta, nb,
                                                               in_stride, out_stride);
-        else if (p->lterms == 2)
+        else if (p->lterms == 2 && p->rterms == 1)
             k_pairmap_cols<2, 1><<<grid, PM_T, 0, stream()>>>(p->d_blocks, p->nblocks, p->d_tstart, p->ntiles,
                                                               p->d_idx, p->d_sgn, in, out, alpha, beta, nb,
                                                               in_stride, out_stride);
-        else
+        else if (p->lterms == 1)
             k_pairmap_cols<1, 2><<<grid, PM_T, 0, stream()>>>(p->d_blocks, p->nblocks, p->d_tstart, p->ntiles,
+                                                              p->d_idx, p->d_sgn, in, out, alpha, beta, nb,
+                                                              in_stride, out_stride);
+        else
+            k_pairmap_cols<2, 2><<<grid, PM_T, 0, stream()>>>(p->d_blocks, p->nblocks, p->d_tstart, p->ntiles,
                                                               p->d_idx, p->d_sgn, in, out, alpha, beta, nb,
                                                               in_stride, out_stride);
     } else {

@@ -648,7 +648,7 @@ int plan_pairmap(const Desc &din, int op0, int op1, i64 target_iop0, i64 target_
             nt += ((b.nlo + 255) / 256) * ((b.nro + 7) / 8);
         }
         plan->ntiles = nt;
-        plan->tiled = start > 0 && tall >= start * 9 / 10 && plan->lterms * plan->rterms <= 2;
+        plan->tiled = start > 0 && tall >= start * 9 / 10;
         if (!plan->tiled) plan->h_tstart.clear();
     }
     plan->h_blocks = std::move(blocks);

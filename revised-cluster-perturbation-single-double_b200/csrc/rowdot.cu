@@ -75,8 +75,8 @@ template <int KQ, int NC>
 struct RdCfg {
     static constexpr int RB = 32 / NC < 8 ? 32 / NC : 8;  // rows per batch
     static constexpr int SLOT = RB * KQ * 32;             // doubles of one batch of one warp
-    // ring depth: about 24 KB per warp, 2..6 batches
-    static constexpr int NS = 24576 / (SLOT * 8) < 2 ? 2 : 24576 / (SLOT * 8) > 6 ? 6 : 24576 / (SLOT * 8);
+    // ring depth: about 12 KB per warp (48 KB a CTA, leaving L1 room), 2..6 batches
+    static constexpr int NS = 12288 / (SLOT * 8) < 2 ? 2 : 12288 / (SLOT * 8) > 6 ? 6 : 12288 / (SLOT * 8);
     static constexpr int SMEM = RW * NS * SLOT * (int)sizeof(double);
 };
 
