@@ -1,5 +1,5 @@
 // Short-K contractions (FP64): every output block has a contracted range of
-// at most 64 (128 for 32-wide tiles), so one CTA holds the whole K extent of its operand
+// at most SHORTK_KMAX, so one CTA holds the whole K extent of its operand
 // tiles in shared memory and the kernel's cost is the read-modify-write of
 // the output.  Each CTA owns a BF x BS tile of one task, BF along the side
 // that is contiguous in the output (so a warp's 32 output loads and stores
@@ -201,7 +201,7 @@ int launch_one(const ContractPlan *cp, const ShortKPlan *sp, const double *A, co
     const size_t smem = shortk_smem<BS, FM>(sp->kmax);
     if (!attr.load()) {
         CPSD_TRY(cuda_check(cudaFuncSetAttribute(k_shortk<BS, FM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)shortk_smem<BS, FM>(shortk_kmax(BS))),
+                                                 (int)shortk_smem<BS, FM>(SHORTK_KMAX)),
                             "short-K smem attribute"));
         attr.store(true);
     }
@@ -224,8 +224,7 @@ int ShortKPlan::upload() {
     return CPSD_OK;
 }
 
-// A contraction qualifies when every task's contracted range is 1..64
-// (1..128 when the tiles are 32 wide);
+// A contraction qualifies when every task's contracted range is 1..KMAX;
 // the output side whose first unit has stride 1 in C (in most tasks) runs
 // along the tile's contiguous side, and the other side's extent picks BS.
 int plan_shortk(const ContractPlan *cp, const ShortKPlan **out) {
@@ -247,17 +246,14 @@ int plan_shortk(const ContractPlan *cp, const ShortKPlan **out) {
         mfast += (t.nm > 0 && t.mSC[0] == 1);
         nfast += (t.nn > 0 && t.nSC[0] == 1);
     }
-    const bool fm = mfast >= nfast;
-    i64 smax = 0;
-    for (const TaskDev &t : cp->h_tasks) smax = std::max(smax, fm ? t.N : t.M);
-    const int bs = smax <= 8 ? 8 : smax <= 16 ? 16 : 32;
-    ok = ok && kmax <= shortk_kmax(bs);
     if (ok) {
         P = std::make_unique<ShortKPlan>();
         ShortKPlan &p = *P;
-        p.fm = fm;
+        p.fm = mfast >= nfast;
         p.kmax = (int)kmax;
-        p.bs = bs;
+        i64 smax = 0;
+        for (const TaskDev &t : cp->h_tasks) smax = std::max(smax, p.fm ? t.N : t.M);
+        p.bs = smax <= 8 ? 8 : smax <= 16 ? 16 : 32;
         const i64 bf = 2048 / p.bs;
         for (int ti = 0; ti < (int)cp->h_tasks.size(); ti++) {
             const TaskDev &t = cp->h_tasks[ti];

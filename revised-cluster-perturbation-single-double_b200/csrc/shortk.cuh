@@ -1,5 +1,5 @@
-// Contractions with a short contracted range (at most shortk_kmax(BS) over
-// the K segments of every output block) and a wide output: the updates of
+// Contractions with a short contracted range (at most SHORTK_KMAX over the
+// K segments of every output block) and a wide output: the updates of
 // doubles-sized tensors by singles or by small intermediates
 // (c2_r1ijka, c2_r2Fmi/Fae, the Wmbej_r1 terms, the hole ladder).  Their
 // cost is the read-modify-write of the output, not the arithmetic.
@@ -9,10 +9,7 @@
 
 namespace cpsd {
 
-constexpr int SHORTK_KMAX = 128;  // 32-wide tiles (BS = 32); 64 for BS = 8 or 16
-// largest contracted range of a tile width: the K slots of both operand
-// tiles stay within the shared memory a CTA may have (96 KB at BS = 32)
-constexpr int shortk_kmax(int bs) { return bs == 32 ? 128 : 64; }
+constexpr int SHORTK_KMAX = 64;
 
 // one CTA's work: the BF x BS output tile of a task starting at (f0, s0)
 // along the output's contiguous side (f) and the other side (s); seg0 = the

@@ -41,7 +41,7 @@ def emulate(tasks, segs, plan, A, B, C, alpha):
     C = C.copy()
     bs = plan["bs"]
     bf = 2048 // bs
-    assert bs in (8, 16, 32) and 1 <= plan["kmax"] <= (128 if bs == 32 else 64)
+    assert bs in (8, 16, 32) and 1 <= plan["kmax"] <= 64
     written = set()
     for it in plan["items"]:
         tk = tasks[it.task]
@@ -77,19 +77,11 @@ def emulate(tasks, segs, plan, A, B, C, alpha):
     return C, written
 
 
-@pytest.mark.parametrize("nirrep", [1, 4, 8, 0])
+@pytest.mark.parametrize("nirrep", [1, 4, 8])
 @pytest.mark.parametrize("name", sorted(KSPEC))
 @pytest.mark.parametrize("nb", [1, 3])
 def test_kernel_shortk_plans(name, nirrep, nb):
-    # nirrep 0: one irrep with 112 virtual and 8 occupied orbitals (contracted
-    # ranges of 65..128 on 32-wide tiles)
-    if nirrep == 0:
-        if nb > 1:
-            pytest.skip("one batch size is enough at this size")
-        s = synth.System(nmo=60, nocc_a=5, nocc_b=3, nirrep=1, seed=2)
-        nirrep = 1
-    else:
-        s = synth.System(nmo=16 if nirrep < 8 else 24, nocc_a=3, nocc_b=2, nirrep=nirrep, seed=2)
+    s = synth.System(nmo=16 if nirrep < 8 else 24, nocc_a=3, nocc_b=2, nirrep=nirrep, seed=2)
     api.init(s.nirrep, s.dirprd)
     of.set_symmetry(s.nirrep, s.dirprd)
     sym = s.sym
@@ -127,7 +119,7 @@ def test_kernel_shortk_plans(name, nirrep, nb):
         pytest.skip("narrow output: the narrow kernels take it")
     plan = get_shortk(*args)
     if plan is None:
-        pytest.skip("contracted range above the short-K limit: tensor-core tiles")
+        pytest.skip("contracted range above 64: tensor-core tiles")
     tasks, segs, _, _ = get_plan(*args)
     out, written = emulate(tasks, segs, plan, A, B, C, 0.9)
     assert len(written) == sum(t.M * t.N for t in tasks)
