@@ -70,7 +70,7 @@ def parse():
     ap.add_argument("--wave-gb", type=float, default=140.0, help="device-memory budget of one --case batch wave")
     ap.add_argument("--kernel", default="c1_r2abci", choices=sorted(KERNEL_CASES),
                     help="lib_cc kernel of --case kernel")
-    ap.add_argument("--case", default="", choices=["", "ladder", "grad", "batch", "kernel"],
+    ap.add_argument("--case", default="", choices=["", "ladder", "grad", "grad3", "batch", "kernel"],
                     help="time one contraction on its own (kernel profiling) instead of the pipeline")
     a = ap.parse_args()
     if a.digits < 0:
@@ -349,6 +349,8 @@ def run_ours(args, rank, world, local_rank):
     def step():
         return api.pipeline(s, sysc, ints, par)
 
+    step_each = {}  # per-step times of each mode (events between the steps; diagnostics)
+
     def timed(mode_digits):
         api.set_mixed(mode_digits, 1.0)
         for _ in range(args.warmup):
@@ -361,20 +363,22 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(args.steps):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+        ev[0].record(stream)
+        for i in range(args.steps):
             out = step()
-        e1.record(stream)
+            ev[i + 1].record(stream)
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
-        ms = e0.elapsed_time(e1)
+        ms = ev[0].elapsed_time(ev[-1])
+        each = [ev[i].elapsed_time(ev[i + 1]) for i in range(args.steps)]
         launches = api.launch_count(True)
         flops = api.flop_count(True)
         t = torch.tensor([ms], dtype=torch.float64, device="cuda")
         if world > 1:
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        step_each[mode_digits] = each
         return float(t.item()), out, launches, flops
 
     clocks = ClockSampler(local_rank)
@@ -545,7 +549,9 @@ def run_ours(args, rank, world, local_rank):
             "per_root_dev_vs_fp64_eh": [float(x) for x in per_root_dev],
             "gate": gate,
             "fp64_path": {"value": value64, "unit": "roots/s", "ms_per_step": ms64 / args.steps,
-                          "gpu_launches": launches64, "contraction_tflops": flops64 / (ms64 / 1e3) / 1e12},
+                          "gpu_launches": launches64, "contraction_tflops": flops64 / (ms64 / 1e3) / 1e12,
+                          "ms_each_step": step_each.get(0)},
+            "ms_each_step": step_each.get(digits),
             "roofline": roof or roof64,
             "roofline_fp64_tiles": roof64,
             "roofline_shortk": roof_sk,
@@ -740,6 +746,115 @@ def run_grad(args):
     }), flush=True)
 
 
+def run_grad3(args):
+    """Differentiation form with the third-order correction: C2v, nmo 120,
+    nocc 8/6, 4 roots of irrep 1, the six DPD lists built on the device from
+    a dense (pq|rs) (cpsd_eri_lists).  Times cpsd_cpsd3_energies (Davidson to
+    1e-12, w^(2), w^(3) with its ground state) and one adjoint gradient per
+    root (cpsd_cpsd3_gradient chained to (pq|rs) by cpsd_eri_adjoint), then
+    checks every root's d(w0 + w2 + w3)/d(pq|rs) against central finite
+    differences of the device energies (step 1e-5) along --directions seeded
+    random (pq|rs) directions with the integrals' 8-fold symmetry."""
+    import torch
+    import __graft_entry__ as ge
+    ge.load_package()
+    from cpsd_b200 import api, synth
+    lists = ("ijkl", "ijka", "abij", "iabj", "abci", "abcd")
+    s = synth.make("c2v_nmo120", skip_abcd=True, host_ints=False)
+    api.init(s.nirrep, s.dirprd)
+    symR, nroot, n = 1, int(s.estate_sym[0]), s.nmo
+    api.use_torch_stream()
+    Lf = torch.from_numpy(s.L).cuda()
+    eri0 = torch.einsum("Ppr,Pqs->prqs", Lf, Lf).contiguous().reshape(-1)
+    del Lf
+    eorb = torch.from_numpy(s.eorb).cuda()
+    mo, sp = api.orbital_map(s)
+    lens = s.lengths()
+    sysc = api.make_system(s)
+    par = api.make_params(s, davidson_conv=12, davidson_cyc=100, diis_max_err=1e-12, diis_cyc=200)
+
+    def lists_of(e):
+        out = {k: torch.zeros(lens[k], dtype=torch.float64, device="cuda") for k in lists}
+        api.eri_lists(sysc, mo, sp, n, e, out)
+        out["eorb"] = eorb
+        return out
+
+    t = lists_of(eri0)
+    st = api.integrals_struct(t)
+
+    def forward(tt=None):
+        return api.cpsd3_energies(s, sysc, api.integrals_struct(tt) if tt else st, par, symR, nroot)
+
+    def backward(w0, L):
+        out = []
+        for r in range(nroot):
+            g = np.zeros(nroot)
+            g[r] = 1.0
+            G = {k: torch.zeros_like(v) for k, v in t.items()}
+            api.cpsd3_gradient(sysc, st, par, symR, w0, L, g, g, g, G)
+            out.append(G)
+        return out
+
+    def timed(fn, k):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(k):
+            res = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / k, res
+
+    for _ in range(args.warmup):
+        w0, w2, w3, L = forward()
+        backward(w0, L)
+    f_ms, (w0, w2, w3, L) = timed(forward, args.steps)
+    b_ms, Gs = timed(lambda: backward(w0, L), args.steps)
+    geri = []
+    for r in range(nroot):
+        G = torch.zeros(n ** 4, dtype=torch.float64, device="cuda")
+        api.eri_adjoint(sysc, mo, sp, n, {k: Gs[r][k] for k in lists}, G)
+        geri.append(G)
+    del Gs
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(0)
+    h = 1e-5
+    rel, absn, fds = [], [], []
+    t0 = time.time()
+    for _ in range(args.directions):
+        D = torch.randn((n, n, n, n), generator=gen, dtype=torch.float64, device="cuda")
+        D = D + D.permute(1, 0, 2, 3)
+        D = D + D.permute(0, 1, 3, 2)
+        D = D + D.permute(2, 3, 0, 1)
+        D = (D / D.abs().max()).reshape(-1)
+        E = []
+        for sg in (1.0, -1.0):
+            a, b, c, _ = forward(lists_of(eri0 + sg * h * D))
+            E.append(a + b + c)
+        fd = (E[0] - E[1]) / (2 * h)
+        for r in range(nroot):
+            pred = float(torch.dot(geri[r], D))
+            rel.append(abs(pred - fd[r]) / abs(fd[r]))
+            absn.append(abs(pred - fd[r]))
+            fds.append(abs(fd[r]))
+        del D
+    rel, absn = np.array(rel), np.array(absn)
+    print(json.dumps({
+        "case": "grad3", "workload": "c2v_nmo120", "config": (
+            f"c2v_nmo120: SF-CIS (Davidson residual 1e-12) + w^(2) + w^(3) and d(w0 + w2 + w3)/d(pq|rs) per root "
+            f"(six DPD lists and Eorb, chained to the dense (pq|rs)); C2v nirrep={s.nirrep}, nmo={s.nmo}, nocc "
+            f"{s.nocc_a}/{s.nocc_b}, o={int(s.popo.sum())}, v={int(s.popv.sum())}"), "roots": nroot,
+        "dtype": "f64", "data": "synthetic (seeded generator; lists from its dense (pq|rs) on the device)",
+        "forward_ms": f_ms, "backward_ms_all_roots": b_ms, "backward_ms_per_root": b_ms / nroot,
+        "w0": [float(x) for x in w0], "w2": [float(x) for x in w2], "w3": [float(x) for x in w3],
+        "fd": {"directions": args.directions, "direction": "random (pq|rs), 8-fold symmetric, max |D| = 1",
+               "step": h, "checks": int(rel.size), "max_rel_err": float(rel.max()),
+               "median_rel_err": float(np.median(rel)), "max_abs_err": float(absn.max()),
+               "median_abs_derivative": float(np.median(fds)), "within_1e-6": int((rel < 1e-6).sum()),
+               "seconds": time.time() - t0},
+    }), flush=True)
+
+
 def run_batch(args):
     """Batching workload: synth.batch_draw() - 64 independent molecules,
     nmo ~ U{60..240}, nocc_alpha ~ U{4..12}, nocc_beta = nocc_alpha - 2,
@@ -855,6 +970,8 @@ def main():
         return
     if args.case == "grad":
         run_grad(args)
+    elif args.case == "grad3":
+        run_grad3(args)
         return
     if args.case == "batch":
         run_batch(args)

@@ -578,6 +578,28 @@ int cpsd_cisd_gradient(const cpsd_system *s, const cpsd_integrals *I, const cpsd
                        int64_t symR, int64_t nroot, const double *w0_host, const double *L_dev,
                        const double *g0_host, const double *g2_host, cpsd_integral_grads *G);
 
+/* The same with the third-order correction (run_order.f90 order 3):
+ *
+ * cpsd_cpsd3_energies: w0, w^(2) and w^(3) per root of irrep symR, the terms
+ * of cpsd_eecpsd_roots with the ground state (T2^(1), T1^(2), T2^(2), J^(2),
+ * J^(3)) computed inside; all six integral lists are read (abcd in device
+ * or host memory).
+ *
+ * cpsd_cpsd3_gradient: ADDS to G the gradient of
+ *     sum_k g0_host[k] w0_k + g2_host[k] w2_k + g3_host[k] w3_k
+ * with respect to all six DPD integral lists and Eorb (every member of G
+ * required; abcd must be in device memory).  Besides the Z-vector solve of
+ * the CIS vector, the ground state's T1^(2) (a DIIS solve in the forward
+ * direction) is reversed by one more solve of the same operator; both
+ * tolerances bound the gradient's accuracy.  FP64 contractions. */
+int cpsd_cpsd3_energies(const cpsd_system *s, const cpsd_integrals *I, const cpsd_params *p,
+                        int64_t symR, int64_t nroot, double *w0_host, double *w2_host, double *w3_host,
+                        double *L_dev);
+int cpsd_cpsd3_gradient(const cpsd_system *s, const cpsd_integrals *I, const cpsd_params *p,
+                        int64_t symR, int64_t nroot, const double *w0_host, const double *L_dev,
+                        const double *g0_host, const double *g2_host, const double *g3_host,
+                        cpsd_integral_grads *G);
+
 #ifdef __cplusplus
 }
 #endif

@@ -470,6 +470,33 @@ def cisd_gradient(sysc, ints_struct, par, symR, w0, L, g0, g2, grads):
                                    ctypes.byref(G)), "cpsd_cisd_gradient")
 
 
+def cpsd3_energies(s, sysc, ints_struct, par, symR, nroot):
+    """SF-CIS roots of irrep symR with their w^(2) and w^(3): (w0, w2, w3, L),
+    L the unit CIS vectors (nroot x lenR1, CUDA)."""
+    import torch
+    l1 = s.r1_len(symR)
+    L = torch.zeros(nroot * l1, dtype=torch.float64, device="cuda")
+    w0, w2, w3 = np.zeros(nroot), np.zeros(nroot), np.zeros(nroot)
+    check(lib().cpsd_cpsd3_energies(ctypes.byref(sysc), ctypes.byref(ints_struct), ctypes.byref(par), I64(symR),
+                                    I64(nroot), w0.ctypes.data_as(ctypes.c_void_p),
+                                    w2.ctypes.data_as(ctypes.c_void_p), w3.ctypes.data_as(ctypes.c_void_p),
+                                    dptr(L)), "cpsd_cpsd3_energies")
+    return w0, w2, w3, L
+
+
+def cpsd3_gradient(sysc, ints_struct, par, symR, w0, L, g0, g2, g3, grads):
+    """Adds d(sum g0 w0 + g2 w2 + g3 w3) to grads (dict of CUDA tensors: all
+    six lists and eorb)."""
+    w0, g0, g2, g3 = (np.ascontiguousarray(x, dtype=np.float64) for x in (w0, g0, g2, g3))
+    G = IntegralGrads()
+    for k in ("ijkl", "ijka", "abij", "iabj", "abci", "abcd", "eorb"):
+        setattr(G, k, dptr(grads[k]).value)
+    check(lib().cpsd_cpsd3_gradient(ctypes.byref(sysc), ctypes.byref(ints_struct), ctypes.byref(par), I64(symR),
+                                    I64(len(w0)), w0.ctypes.data_as(ctypes.c_void_p), dptr(L),
+                                    g0.ctypes.data_as(ctypes.c_void_p), g2.ctypes.data_as(ctypes.c_void_p),
+                                    g3.ctypes.data_as(ctypes.c_void_p), ctypes.byref(G)), "cpsd_cpsd3_gradient")
+
+
 def set_phase_overlap(on=True):
     """SF-CIS beside the ground state on two library worker streams (True,
     the default) or all phases in order on the caller's stream"""

@@ -967,6 +967,57 @@ int vjp_Fae_r2abij(const Ten &r2, const Ten &V, const Ten &Y, Ten &G, int which,
 int vjp_Wmbej_r2abij(const Ten &r2, const Ten &V, const Ten &Y, Ten &G, int which, double f) {
     return vjp444(V, r2, Y, G, 1 - which, 0.5 * f, "fenm", "bfjn", "embj", 0);
 }
+int vjp_c2_r2Wmbej(const Ten &r2, const Ten &W, const Ten &Y, Ten &G, int which, double f) {
+    return vjp444(r2, W, Y, G, which, f, "aeim", "embj", "abij", 3);
+}
+int vjp_c2_r2Wmnij(const Ten &r2, const Ten &W, const Ten &Y, Ten &G, int which, double f) {
+    return vjp444(r2, W, Y, G, which, r2.d.iop[0] == 0 ? f : 0.5 * f, "abmn", "mnij", "abij", 0);
+}
+int vjp_c2_r2abcd(const Ten &r2, const Ten &V, const Ten &Y, Ten &G, int which, double f) {
+    if (V.arr && host_resident(V.arr))
+        return set_error(CPSD_EARG, "adjoint of c2_r2abcd: abcd must be in device memory");
+    return vjp444(V, r2, Y, G, 1 - which, r2.d.iop[0] == 1 ? 0.5 * f : f, "abef", "efij", "abij", 0);
+}
+int vjp_c2_r2Fae(const Ten &r2, const Ten &F, const Ten &Y, Ten &G, int which, double f) {
+    return vjp444(r2, F, Y, G, which, f, "aeij", "be..", "abij", 1);
+}
+int vjp_c2_r2Fmi(const Ten &r2, const Ten &F, const Ten &Y, Ten &G, int which, double f) {
+    return vjp444(r2, F, Y, G, which, -f, "abim", "mj..", "abij", 2);
+}
+int vjp_Fmi_r1ijka(const Ten &r1, const Ten &V, const Ten &Y, Ten &G, int which, double f) {
+    return vjp444(V, r1, Y, G, 1 - which, f, "mnie", "en+-", "mi+-", 0);
+}
+int vjp_Fae_r1abci(const Ten &r1, const Ten &V, const Ten &Y, Ten &G, int which, double f) {
+    return vjp444(V, r1, Y, G, 1 - which, f, "efam", "fm+-", "ae+-", 0);
+}
+int vjp_Wkbij_r2ijka(const Ten &r2, const Ten &V, const Ten &Y, Ten &G, int which, double f) {
+    return vjp444(V, r2, Y, G, 1 - which, f, "klic", "bcjl", "ijkb", 1);
+}
+// the forward wrote tmp(ij,bk) and swapped its right pair into W(ij,kb): the
+// cotangent is swapped back (a permutation's adjoint is its inverse), then
+// the contraction tmp(ij,bk) = fr r(cd,ij) V(cd,bk) is reversed
+int vjp_Wkbij_r2abci(const Ten &r2, const Ten &V, const Ten &Y, Ten &G, int which, double f) {
+    OpScope op;
+    ScratchScope sc;
+    const PairMapPlan *pm;
+    Desc d;
+    CPSD_TRY(plan_pairmap(Y.d, PAIR_ID, PAIR_SWAP, 1, 1, &d, &pm));
+    Ten Yt = Y;
+    Yt.d = d;
+    Yt.bs = 0;
+    CPSD_TRY(scratch(d.len(), &Yt.arr));
+    CPSD_TRY(launch_pairmap(pm, Y.arr, Yt.arr, 1.0, 0.0));
+    return vjp444(r2, V, Yt, G, which, r2.d.iop[0] == 0 ? -f : -0.5 * f, "cdij", "cdbk", "ijbk", 0);
+}
+int vjp_Wmbej_r1abci(const Ten &r1, const Ten &V, const Ten &Y, Ten &G, int which, double f) {
+    return vjp444(V, r1, Y, G, 1 - which, f, "febm", "fj..", "embj", 0);
+}
+int vjp_Wmbej_r1ijka(const Ten &r1, const Ten &V, const Ten &Y, Ten &G, int which, double f) {
+    return vjp444(V, r1, Y, G, 1 - which, -f, "nmje", "bn..", "embj", 0);
+}
+int vjp_Wmnij_r1ijka(const Ten &r1, const Ten &V, const Ten &Y, Ten &G, int which, double f) {
+    return vjp444(V, r1, Y, G, 1 - which, f, "mnie", "ej..", "mnij", 2);
+}
 
 }  // namespace cpsd
 

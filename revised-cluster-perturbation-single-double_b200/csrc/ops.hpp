@@ -102,6 +102,19 @@ CPSD_VJP(c2_r1ijka);
 CPSD_VJP(Fmi_r2abij);
 CPSD_VJP(Fae_r2abij);
 CPSD_VJP(Wmbej_r2abij);
+// and the further ones of the third-order correction w^(3)
+CPSD_VJP(c2_r2Wmbej);
+CPSD_VJP(c2_r2Wmnij);
+CPSD_VJP(c2_r2abcd);
+CPSD_VJP(c2_r2Fae);
+CPSD_VJP(c2_r2Fmi);
+CPSD_VJP(Fmi_r1ijka);
+CPSD_VJP(Fae_r1abci);
+CPSD_VJP(Wkbij_r2ijka);
+CPSD_VJP(Wkbij_r2abci);
+CPSD_VJP(Wmbej_r1abci);
+CPSD_VJP(Wmbej_r1ijka);
+CPSD_VJP(Wmnij_r1ijka);
 #undef CPSD_VJP
 
 }  // namespace cpsd

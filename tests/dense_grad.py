@@ -138,3 +138,117 @@ def shifted(s, d, h):
     """integrals and Eorb of s moved by h along the DPD direction d"""
     ints = {k: (None if v is None else v + h * d[k]) if k in d else v for k, v in s.ints.items()}
     return ints, s.eorb + h * d["eorb"]
+
+
+def _e(spec, *ops):
+    return torch.einsum(spec, *ops)
+
+
+# the kernels' dense formulas (tests/kernel_specs.py) on torch tensors:
+# name -> fn(a, b, f) with a, b in the kernel's operand order
+TK = {
+    "c1_r1iabj": lambda r, V, f: f * _e("fn,fnai->ai", r, V),
+    "c1_r1Fae": lambda r, F, f: f * _e("ae,ei->ai", F, r),
+    "c1_r1Fmi": lambda r, F, f: -f * _e("am,mi->ai", r, F),
+    "c1_r2abci": lambda r, V, f: 0.5 * f * _e("feam,feim->ai", V, r),
+    "c1_r2ijka": lambda r, V, f: -0.5 * f * _e("aemn,mnie->ai", r, V),
+    "c2_r1abci": lambda r, V, f: f * _rs(_e("abej,ei->abij", V, r)),
+    "c2_r1ijka": lambda r, V, f: -f * _pq(_e("ijmb,am->abij", V, r)),
+    "c2_r2Wmbej": lambda r, W, f: f * _rs(_pq(_e("aeim,embj->abij", r, W))),
+    "c2_r2Wmnij": lambda r, W, f: 0.5 * f * _e("abmn,mnij->abij", r, W),
+    "c2_r2abcd": lambda r, V, f: 0.5 * f * _e("abef,efij->abij", V, r),
+    "c2_r2Fae": lambda r, F, f: f * _pq(_e("aeij,be->abij", r, F)),
+    "c2_r2Fmi": lambda r, F, f: -f * _rs(_e("abim,mj->abij", r, F)),
+    "Fmi_r2abij": lambda r, V, f: 0.5 * f * _e("efin,efmn->mi", r, V),
+    "Fae_r2abij": lambda r, V, f: -0.5 * f * _e("afmn,efmn->ae", r, V),
+    "Fmi_r1ijka": lambda r, V, f: f * _e("en,mnie->mi", r, V),
+    "Fae_r1abci": lambda r, V, f: f * _e("fm,efam->ae", r, V),
+    "Wkbij_r2ijka": lambda r, V, f: f * _pq(_e("klic,bcjl->ijkb", V, r)),
+    "Wkbij_r2abci": lambda r, V, f: 0.5 * f * _e("dcbk,cdij->ijkb", V, r),
+    "Wmbej_r2abij": lambda r, V, f: 0.5 * f * _e("bfjn,fenm->embj", r, V),
+    "Wmbej_r1abci": lambda r, V, f: f * _e("fj,febm->embj", r, V),
+    "Wmbej_r1ijka": lambda r, V, f: -f * _e("bn,nmje->embj", r, V),
+    "Wmnij_r1ijka": lambda r, V, f: f * _rs(_e("ej,mnie->mnij", r, V)),
+}
+
+
+def K(name, a, b, f=1.0):
+    return TK[name](a, b, f)
+
+
+class DenseCpsd3(DenseCisd):
+    """Dense w0 / w^(2) / w^(3) of the roots of irrep symR: the order-3 chain
+    of src/EE-CPSd.SF/run_order.f90 (calE_C.f90, calC_JR.f90, calC_VTR.f90)
+    with the ground state of src/CPSd.SF/run1.f90 / run2.f90 (T1^(2) by an
+    exact dense solve) and calJ.f90's J^(2) / J^(3), all six lists read."""
+
+    LAYOUTS = dict(DenseCisd.LAYOUTS, ijkl=("oooo", (0, 0)), abcd=("vvvv", (0, 0)))
+
+    def __init__(self, s, symR):
+        super().__init__(s, symR)
+        sym = s.sym
+        irr_o, irr_v = dense.orbital_irreps(s.popo), dense.orbital_irreps(s.popv)
+        mask = np.array([[sym.dp(a, i) == 1 for i in irr_o] for a in irr_v])
+        self.idx1 = torch.from_numpy(np.argwhere(mask))
+
+    def energies3(self, ints, eorb, L0, w0_start, iters=4, shift=1e-7):
+        D = {k: self.to_dense(k, ints[k]) for k in self.LAYOUTS}
+        ijkl, ijka, abij, iabj, abci, abcd = (D[k] for k in ("ijkl", "ijka", "abij", "iabj", "abci", "abcd"))
+        eo, ev = eorb[:self.no], eorb[self.no:]
+        e1 = ev[:, None] - eo[None, :]
+        e2 = ev[:, None, None, None] + ev[None, :, None, None] - eo[None, None, :, None] - eo[None, None, None, :]
+        # SF-CIS root by shifted inverse iteration (as DenseCisd.energies)
+        a, i = self.idx[:, 0], self.idx[:, 1]
+        A = iabj[:, :, a, i][a, i].T + torch.diag(e1[a, i])
+        L0d = self.r1_to_dense(torch.as_tensor(L0, dtype=T))[a, i]
+        x = L0d / torch.linalg.norm(L0d)
+        M = A - (float(w0_start) + shift) * torch.eye(len(a), dtype=T)
+        for _ in range(iters):
+            x = torch.linalg.solve(M, x)
+            x = x / torch.linalg.norm(x)
+        if float(torch.dot(x.detach(), L0d)) < 0:
+            x = -x
+        w0 = torch.dot(x, A @ x)
+        L = torch.zeros((self.nv, self.no), dtype=T).index_put((a, i), x)
+        # ground state: T2^(1), T2^(2), T1^(2) (run1.f90, run2.f90)
+        T2 = -abij / e2
+        C1g = K("c1_r2abci", T2, abci) + K("c1_r2ijka", T2, ijka)
+        C2g = K("c2_r2Wmbej", T2, iabj) + K("c2_r2Wmnij", T2, ijkl) + K("c2_r2abcd", T2, abcd)
+        T2b = -C2g / e2
+        a1, i1 = self.idx1[:, 0], self.idx1[:, 1]
+        A1 = iabj[:, :, a1, i1][a1, i1].T + torch.diag(e1[a1, i1])
+        T1b = torch.zeros((self.nv, self.no), dtype=T).index_put((a1, i1), torch.linalg.solve(A1, -C1g[a1, i1]))
+        # J^(2), J^(3) (calJ.f90)
+        Foo, Fvv = K("Fmi_r2abij", T2, abij), K("Fae_r2abij", T2, abij)
+        Woo = K("Wkbij_r2ijka", T2, ijka) + K("Wkbij_r2abci", T2, abci)
+        Wvo = K("Wmbej_r2abij", T2, abij, 2.0)
+        Foo3 = K("Fmi_r1ijka", T1b, ijka) + K("Fmi_r2abij", T2b, abij)
+        Fvv3 = K("Fae_r1abci", T1b, abci) + K("Fae_r2abij", T2b, abij)
+        Wvo3 = K("Wmbej_r1ijka", T1b, ijka) + K("Wmbej_r1abci", T1b, abci) + K("Wmbej_r2abij", T2b, abij, 2.0)
+        # orders 1-3 of run_order.f90
+        C2 = K("c2_r1ijka", L, ijka) + K("c2_r1abci", L, abci)
+        R2 = -C2 / (e2 - w0)
+        C1 = (K("c1_r2abci", R2, abci) + K("c1_r2ijka", R2, ijka) + K("c1_r1iabj", L, Wvo)
+              + K("c1_r1Fmi", L, Foo) + K("c1_r1Fae", L, Fvv))
+        w2 = torch.sum(L * C1)
+        C2b = (K("c2_r2Wmbej", R2, iabj) + K("c2_r2Wmnij", R2, ijkl) + K("c2_r2abcd", R2, abcd)
+               + K("c2_r1ijka", L, Woo)
+               + K("c2_r2Wmnij", T2, K("Wmnij_r1ijka", L, ijka)) + K("c2_r2Wmbej", T2, K("Wmbej_r1abci", L, abci))
+               + K("c2_r2Fmi", T2, K("Fmi_r1ijka", L, ijka)) + K("c2_r2Fae", T2, K("Fae_r1abci", L, abci)))
+        R22 = -C2b / (e2 - w0)
+        C1c = (K("c1_r2abci", R22, abci) + K("c1_r2ijka", R22, ijka) + K("c1_r1iabj", L, Wvo3)
+               + K("c1_r1Fmi", L, Foo3) + K("c1_r1Fae", L, Fvv3))
+        w3 = torch.sum(L * C1c)
+        return w0, w2, w3, self.r1_to_dpd(L.detach())
+
+    def gradient3(self, s, L0, w0_start, g0, g2, g3):
+        """d(g0 w0 + g2 w2 + g3 w3) / d(six lists, eorb) as numpy vectors."""
+        keys = list(self.LAYOUTS)
+        leaves = {k: torch.tensor(s.ints[k], dtype=T, requires_grad=True) for k in keys}
+        eorb = torch.tensor(s.eorb, dtype=T, requires_grad=True)
+        w0, w2, w3, _ = self.energies3(leaves, eorb, L0, w0_start)
+        E = g0 * w0 + g2 * w2 + g3 * w3
+        grads = torch.autograd.grad(E, [leaves[k] for k in keys] + [eorb])
+        out = {k: g.numpy() for k, g in zip(keys, grads[:-1])}
+        out["eorb"] = grads[-1].numpy()
+        return out, float(w0.detach()), float(w2.detach()), float(w3.detach())

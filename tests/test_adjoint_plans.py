@@ -35,6 +35,18 @@ ADJ = {
     "Fmi_r2abij": ("b", "efmn", "efin", "mi.."),
     "Fae_r2abij": ("a", "afmn", "efmn", "ae.."),
     "Wmbej_r2abij": ("b", "fenm", "bfjn", "embj"),
+    # the further ones of the third-order correction
+    "c2_r2Wmbej": ("a", "aeim", "embj", "abij"),
+    "c2_r2Wmnij": ("a", "abmn", "mnij", "abij"),
+    "c2_r2abcd": ("b", "abef", "efij", "abij"),
+    "c2_r2Fae": ("a", "aeij", "be..", "abij"),
+    "c2_r2Fmi": ("a", "abim", "mj..", "abij"),
+    "Fmi_r1ijka": ("b", "mnie", "en+-", "mi+-"),
+    "Fae_r1abci": ("b", "efam", "fm+-", "ae+-"),
+    "Wkbij_r2ijka": ("b", "klic", "bcjl", "ijkb"),
+    "Wmbej_r1abci": ("b", "febm", "fj..", "embj"),
+    "Wmbej_r1ijka": ("b", "nmje", "bn..", "embj"),
+    "Wmnij_r1ijka": ("b", "mnie", "ej..", "mnij"),
 }
 
 

@@ -77,3 +77,59 @@ def test_reference_gradient_matches_oracle_fd(case):
                 vals.append(g0 * a[k] + g2 * b[k])
             fd = (vals[0] - vals[1]) / (2 * h)
             assert abs(pred - fd) <= 1e-7 * abs(fd) + 1e-10, (symR, r, pred, fd)
+
+
+def oracle_run3(s):
+    of.set_symmetry(s.nirrep, s.dirprd)
+    o = of.Oracle(s, **TIGHT)
+    _, R, _ = o.cis()
+    w0, w2, w3 = o.pipeline()
+    return w0, w2, w3, R
+
+
+CASES3 = [
+    dict(nmo=12, nocc_a=3, nocc_b=1, nirrep=1, seed=4, roots={1: 2}),
+    dict(nmo=14, nocc_a=4, nocc_b=2, nirrep=2, seed=3, roots={1: 1, 2: 1}),
+]
+
+
+@pytest.mark.parametrize("case", range(len(CASES3)))
+def test_dense_order3_matches_oracle(case):
+    """the dense w^(3) chain (DenseCpsd3) gives the oracle pipeline's w0, w^(2), w^(3)"""
+    s = synth.System(**CASES3[case])
+    w0, w2, w3, R = oracle_run3(s)
+    for symR, r, k, L0 in roots_of(s, R):
+        ref = dg.DenseCpsd3(s, symR)
+        ints = {key: torch.tensor(s.ints[key]) for key in ref.LAYOUTS}
+        a, b, c, _ = ref.energies3(ints, torch.tensor(s.eorb), L0, w0[k])
+        assert abs(float(a) - w0[k]) < 1e-12
+        assert abs(float(b) - w2[k]) < 1e-12
+        assert abs(float(c) - w3[k]) < 1e-11 * max(1.0, abs(w3[k])), (float(c), w3[k])
+
+
+@pytest.mark.parametrize("case", range(len(CASES3)))
+def test_reference_order3_gradient_matches_oracle_fd(case):
+    """its autograd gradient of g0 w0 + g2 w2 + g3 w3 (all six lists and
+    Eorb) equals central finite differences of the oracle pipeline"""
+    s = synth.System(**CASES3[case])
+    w0, w2, w3, R = oracle_run3(s)
+    rng = np.random.default_rng(200 + case)
+    h = 1e-5
+    for symR, r, k, L0 in roots_of(s, R):
+        ref = dg.DenseCpsd3(s, symR)
+        g0, g2, g3 = rng.uniform(0.5, 1.5, 3)
+        G, _, _, _ = ref.gradient3(s, L0, w0[k], g0, g2, g3)
+        assert set(G) == {"ijkl", "ijka", "abij", "iabj", "abci", "abcd", "eorb"}
+        d = s.integral_direction(*s.input_direction(rng))
+        pred = sum(float(np.dot(G[key], d[key])) for key in G)
+        vals = []
+        for ints, eo in (dg.shifted(s, d, h), dg.shifted(s, d, -h)):
+            saved = s.ints, s.eorb
+            s.ints, s.eorb = ints, eo
+            try:
+                a, b, c = oracle_run3(s)[:3]
+            finally:
+                s.ints, s.eorb = saved
+            vals.append(g0 * a[k] + g2 * b[k] + g3 * c[k])
+        fd = (vals[0] - vals[1]) / (2 * h)
+        assert abs(pred - fd) <= 1e-7 * abs(fd) + 1e-10, (symR, r, pred, fd)
