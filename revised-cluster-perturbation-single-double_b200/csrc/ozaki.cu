@@ -136,6 +136,7 @@ struct OzCfg {
     static_assert(NST >= 2, "at least two pipeline stages");
     static_assert(SMEM <= 227 * 1024, "dynamic shared memory above the per-CTA limit");
     static_assert(NCOL_RAW <= 512, "accumulators exceed TMEM");
+    static_assert(BN % 16 == 0 && BN <= 256 && 256 / BN >= 1, "MMA N: multiples of 16 up to 256");
 };
 
 // One output tile per CTA: 128 rows (TMEM lanes) x BN columns, S diagonal
@@ -200,10 +201,15 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
         }
     } else if (warp == 5) {
         if (lane == 0) {  // MMA issuer
-            constexpr uint32_t idesc = umma_idesc_i8(BN);
-            bool init[S];
-#pragma unroll
-            for (int d = 0; d < S; d++) init[d] = false;
+            // The products A_t B_v (t + v < S) go to accumulator d = t + v at
+            // TMEM columns d*BN.  For one t the B digit tiles v = v0..v0+nv-1
+            // lie back to back in shared memory (one canonical tile of nv*BN
+            // rows) and their accumulators back to back in TMEM, so one MMA
+            // of N = nv*BN (at most 256) does them all: A_t is read from
+            // shared memory once per MMA instead of once per digit pair.
+            // Every accumulator is first written by t = 0 at the first stage
+            // (no accumulation there), later MMAs accumulate.
+            constexpr int VPER = 256 / BN;
             for (int i = 0; i < nk; i++) {
                 const int s = i % Cf::NST, u = i / Cf::NST;
                 if (!mbar_wait(&full[s], u & 1)) {
@@ -213,18 +219,17 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                 tc_fence_after();
                 const uint32_t sa = smem_u32(stages + (size_t)s * Cf::STAGE), sb = sa + Cf::A_STAGE;
 #pragma unroll
-                for (int t = 0; t < S; t++)
+                for (int kk = 0; kk < OZ_BK / 32; kk++)
 #pragma unroll
-                    for (int v = 0; v < S - t; v++) {
-                        const int d = t + v;
+                    for (int t = 0; t < S; t++)
 #pragma unroll
-                        for (int kk = 0; kk < OZ_BK / 32; kk++) {
-                            uint64_t ad = umma_desc(sa + t * 128 * OZ_BK + kk * 256, 128, 8 * OZ_BK);
-                            uint64_t bd = umma_desc(sb + v * BN * OZ_BK + kk * 256, 128, 8 * OZ_BK);
-                            umma_i8(tmem + (uint32_t)(d * BN), ad, bd, idesc, init[d] ? 1u : 0u);
-                            init[d] = true;
+                        for (int v0 = 0; v0 < S - t; v0 += VPER) {
+                            const int nv = S - t - v0 < VPER ? S - t - v0 : VPER;
+                            const uint64_t ad = umma_desc(sa + t * 128 * OZ_BK + kk * 256, 128, 8 * OZ_BK);
+                            const uint64_t bd = umma_desc(sb + v0 * BN * OZ_BK + kk * 256, 128, 8 * OZ_BK);
+                            const uint32_t acc = (i > 0 || kk > 0 || t > 0) ? 1u : 0u;
+                            umma_i8(tmem + (uint32_t)((t + v0) * BN), ad, bd, umma_idesc_i8(nv * BN), acc);
                         }
-                    }
                 umma_commit(&empty[s]);  // frees the stage once these MMAs are done
             }
             umma_commit(&done);
