@@ -1380,9 +1380,12 @@ int solve_r1(const Sys &S, const Ints &X, const cpsd_params *p, i64 symR, i64 nb
 }
 
 // EE-CPS(D-3) for nb roots of irrep symR sharing every contraction launch
+// (rhs_out non-null: the order-3 solver's right-hand side, nb x l1, goes
+// there and the solve is left to the caller; R1_2o is then not written)
 static int ee_roots_batch(const Sys &S, const Ints &X, const cpsd_params *p, const double *T2_1,
                           const cpsd_jints *J, i64 symR, i64 nb, const double *w0_host, const double *L,
-                          double *w_host, double *R2_1o, double *R1_2o, double *R2_2o, i64 *sit_out) {
+                          double *w_host, double *R2_1o, double *R1_2o, double *R2_2o, i64 *sit_out,
+                          double *rhs_out = nullptr) {
     const i64 *o = S.popo, *v = S.popv;
     ScratchScope sc;
     const i64 l1 = irpdso(symR, v, o, 1), l2 = idsymsoc(symR, v, v, 0, o, o, 0);
@@ -1483,7 +1486,8 @@ static int ee_roots_batch(const Sys &S, const Ints &X, const cpsd_params *p, con
     // convergence test); the sigma of every step is one batched launch
     i64 sit = 0;
     CPSD_TRY(launch_scale(cn1, nb * l1, -1.0));
-    CPSD_TRY(solve_r1(S, X, p, symR, nb, l1, e1, cn1, L, w0d, r12, &sit));
+    if (rhs_out) CPSD_TRY(launch_copy(rhs_out, cn1, nb * l1));
+    else CPSD_TRY(solve_r1(S, X, p, symR, nb, l1, e1, cn1, L, w0d, r12, &sit));
     // C^(3) = J^(1) R^(2) + J^(3) R^(0), C1 only (calE_C.f90:37-79)
     CPSD_TRY(zero(c1, nb * l1));
     CPSD_TRY(k_c1_r2abci(C1, R22, X.abci, 1.0, nb));
@@ -1497,7 +1501,7 @@ static int ee_roots_batch(const Sys &S, const Ints &X, const cpsd_params *p, con
     for (i64 r = 0; r < nb; r++)
         for (int k = 0; k < 3; k++) w_host[3 * r + k] = wh[k * nb + r];
     if (R2_1o) CPSD_TRY(launch_copy(R2_1o, r21, nb * l2));
-    if (R1_2o) CPSD_TRY(launch_copy(R1_2o, r12, nb * l1));
+    if (R1_2o && !rhs_out) CPSD_TRY(launch_copy(R1_2o, r12, nb * l1));
     if (R2_2o) CPSD_TRY(launch_copy(R2_2o, r22, nb * l2));
     if (sit_out) *sit_out = sit;
     return cuda_check(cudaStreamSynchronize(stream()), "ee sync");
@@ -1680,13 +1684,34 @@ int cpsd_eecpsd_roots(const cpsd_system *s, const cpsd_integrals *I, const cpsd_
                 (long long)symR, (long long)nroot, (long long)chunk, fr / 1e9, arena().spare() / 1e9,
                 pool_idle_bytes() / 1e9);
     }
+    // Roots in several batches: the order-3 solves (R1^(2), R1-sized, with
+    // one sigma V(fn,ai) R1 a step) run for all roots at once after the
+    // batches, each root with its own DIIS and convergence test as before,
+    // so the solver's steps are not repeated batch after batch.
+    ScratchScope sc;
+    const bool defer = chunk < nroot;
+    double *rhs = nullptr, *w0d = nullptr, *r12 = R1_2;
+    if (defer) {
+        CPSD_TRY(scratch(nroot * l1, &rhs));
+        CPSD_TRY(scratch(nroot, &w0d));
+        if (!r12) CPSD_TRY(scratch(nroot * l1, &r12));
+        CPSD_TRY(cuda_check(cudaMemcpyAsync(w0d, w0_host, sizeof(double) * nroot, cudaMemcpyHostToDevice, stream()),
+                            "w0"));
+    }
     i64 tot = 0;
     for (i64 r = 0; r < nroot; r += chunk) {
         const i64 nb = std::min(chunk, nroot - r);
         i64 it = 0;
         CPSD_TRY(ee_roots_batch(S, X, p, T2_1, J, symR, nb, w0_host + r, L_dev + r * l1, w_host + 3 * r,
                                 R2_1 ? R2_1 + r * l2 : nullptr, R1_2 ? R1_2 + r * l1 : nullptr,
-                                R2_2 ? R2_2 + r * l2 : nullptr, &it));
+                                R2_2 ? R2_2 + r * l2 : nullptr, &it, defer ? rhs + r * l1 : nullptr));
+        tot += it;
+    }
+    if (defer) {
+        const EnergyPlan *e1;
+        CPSD_TRY(plan_energy(make_desc(S.popv, S.popo, ZORB, ZORB, 1, 1, symR), "vozz", &e1));
+        i64 it = 0;
+        CPSD_TRY(solve_r1(S, X, p, symR, nroot, l1, e1, rhs, L_dev, w0d, r12, &it));
         tot += it;
     }
     if (solver_iters) *solver_iters = tot;
