@@ -222,12 +222,25 @@ void *pool_get(size_t bytes) {
         return p;
     }
     void *p = nullptr;
-    if (cudaMalloc(&p, bytes) == cudaSuccess) return p;
+    double t = mem_trace_on() ? host_ms() : 0.0;
+    if (cudaMalloc(&p, bytes) == cudaSuccess) {
+        mem_trace("pool cudaMalloc", bytes, mem_trace_on() ? host_ms() - t : 0.0);
+        return p;
+    }
     cudaGetLastError();
-    for (PoolBuf &b : f) cudaFree(b.p);  // out of memory: give back the idle buffers and retry
+    size_t idle = 0;
+    for (PoolBuf &b : f) {  // out of memory: give back the idle buffers and retry
+        idle += b.bytes;
+        cudaFree(b.p);
+    }
     f.clear();
     arena().trim();  // and this thread's unused scratch chunks
-    if (cudaMalloc(&p, bytes) == cudaSuccess) return p;
+    const bool ok = cudaMalloc(&p, bytes) == cudaSuccess;
+    if (mem_trace_on()) {
+        mem_trace("pool: idle buffers released", idle, 0.0);
+        mem_trace("pool cudaMalloc after release", bytes, host_ms() - t, ok);
+    }
+    if (ok) return p;
     cudaGetLastError();
     return nullptr;
 }
@@ -248,8 +261,14 @@ size_t pool_idle_bytes() {
 
 void pool_release_idle() {
     std::lock_guard<std::mutex> lock(pool_mutex());
-    for (PoolBuf &b : pool_free()) cudaFree(b.p);
+    const double t = mem_trace_on() ? host_ms() : 0.0;
+    size_t idle = 0;
+    for (PoolBuf &b : pool_free()) {
+        idle += b.bytes;
+        cudaFree(b.p);
+    }
     pool_free().clear();
+    if (mem_trace_on() && idle) mem_trace("pool release idle (cudaFree)", idle, host_ms() - t);
 }
 
 namespace {

@@ -2,6 +2,7 @@
 #include "runtime.hpp"
 
 #include <algorithm>
+#include <chrono>
 #include <cstdio>
 #include <cstring>
 
@@ -104,6 +105,22 @@ std::mutex &upload_mutex() {
     return m;
 }
 
+bool mem_trace_on() {
+    static const bool on = getenv("CPSD_TRACE_MEM") != nullptr;
+    return on;
+}
+
+double host_ms() {
+    static const auto t0 = std::chrono::steady_clock::now();
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+void mem_trace(const char *what, size_t bytes, double ms, bool ok) {
+    if (!mem_trace_on()) return;
+    fprintf(stderr, "[cpsd mem] t=%.1f ms %s %.3f GB%s (%.2f ms)\n", host_ms(), what, bytes / 1e9, ok ? "" : " FAILED",
+            ms);
+}
+
 // ------------------------------------------------------------------ arena
 Arena &arena() {
     thread_local Arena a;
@@ -126,7 +143,9 @@ void Arena::free_all() {
 
 void Arena::trim() {
     while (chunks.size() > cur_chunk + 1 && chunks.back().owned) {
+        const double t = mem_trace_on() ? host_ms() : 0.0;
         cudaFree(chunks.back().base);
+        if (mem_trace_on()) mem_trace("arena trim cudaFree", chunks.back().size, host_ms() - t);
         chunks.pop_back();
     }
 }
@@ -152,7 +171,10 @@ int Arena::alloc(size_t bytes, void **out) {
     size_t sz = bytes + std::min(bytes, (size_t)1 << 30);
     if (sz < ((size_t)256 << 20)) sz = (size_t)256 << 20;
     void *p = nullptr;
-    if (cudaMalloc(&p, sz) != cudaSuccess) {
+    const double t0 = mem_trace_on() ? host_ms() : 0.0;
+    const bool first_ok = cudaMalloc(&p, sz) == cudaSuccess;
+    if (mem_trace_on()) mem_trace("arena cudaMalloc", sz, host_ms() - t0, first_ok);
+    if (!first_ok) {
         cudaGetLastError();
         sz = bytes;
         if (cudaMalloc(&p, sz) != cudaSuccess) {

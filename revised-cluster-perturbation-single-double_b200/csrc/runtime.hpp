@@ -76,6 +76,14 @@ extern const i64 ZORB[8];
 // -------------------------------------------------------- scratch arena
 // Bump allocator over device memory.  A caller-provided workspace is used
 // as is; otherwise chunks are cudaMalloc'ed on demand and kept.
+// CPSD_TRACE_MEM set in the environment: one line on stderr per device
+// allocation or release of the scratch arena and the buffer pool, with the
+// host time since the first line and the call's own duration (a profiling
+// record of where a run meets the memory limit)
+bool mem_trace_on();
+void mem_trace(const char *what, size_t bytes, double ms, bool ok = true);
+double host_ms();
+
 struct Arena {
     struct Chunk {
         char *base;
