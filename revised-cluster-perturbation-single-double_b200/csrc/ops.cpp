@@ -15,6 +15,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 
@@ -161,6 +162,7 @@ struct ExpEntry {
     double *buf;
     size_t bytes;
     int64_t used;  // operation (epoch) that was last handed this copy
+    int uses;      // operations handed this copy in this run
 };
 // digit tiles (and their exponents) made of a constant operand
 struct DigEntry {
@@ -170,7 +172,29 @@ struct DigEntry {
     int *expo;
     size_t dbytes, ebytes;
     int64_t used;
+    int uses;
 };
+// Uses per run of each copy (source array and layout / digit plan): a copy
+// that served one operation in the last run is not kept in the next one,
+// where it would only hold memory that later work then has to take back
+// (at the memory limit that cost a cudaMalloc / cudaFree of gigabytes and
+// a rebuild every run).  Counted per host thread over one run, merged into
+// the process-wide record when the run ends.
+using UseKey = std::pair<const void *, std::string>;
+std::map<UseKey, int> &uses_last_run() {
+    static std::map<UseKey, int> m;
+    return m;
+}
+std::mutex &uses_mutex() {
+    static std::mutex m;
+    return m;
+}
+bool single_use_last_run(const void *src, const std::string &key) {
+    std::lock_guard<std::mutex> lock(uses_mutex());
+    auto it = uses_last_run().find({src, key});
+    return it != uses_last_run().end() && it->second == 1;
+}
+std::string dig_key(uint64_t h) { return "digits:" + std::to_string(h); }
 struct ConstOps {
     int depth = 0;
     std::vector<const double *> arrs;
@@ -178,6 +202,12 @@ struct ConstOps {
     std::vector<DigEntry> dig;
     int64_t epoch = 0;  // outermost operations so far
     int op_depth = 0;
+    std::map<UseKey, int> uses;  // this run's counts (copies given way included)
+    void note(const void *src, const std::string &key, int n) {  // a copy's count
+        int &u = uses[{src, key}];
+        u = std::max(u, n);
+    }
+    void bump(const void *src, const std::string &key) { uses[{src, key}]++; }  // a use made in scratch
 };
 ConstOps &const_ops() {
     thread_local ConstOps c;
@@ -208,49 +238,95 @@ std::mutex &pool_mutex() {
     static std::mutex m;
     return m;
 }
+// actual size of every buffer handed out (a request may be served by a
+// larger idle buffer; pool_put gives back the whole buffer)
+std::map<void *, size_t> &pool_sizes() {
+    static std::map<void *, size_t> m;
+    return m;
+}
 void *pool_get(size_t bytes) {
     std::lock_guard<std::mutex> lock(pool_mutex());
     auto &f = pool_free();
+    auto take = [&](int i) {
+        void *p = f[i].p;
+        pool_sizes()[p] = f[i].bytes;
+        f.erase(f.begin() + i);
+        return p;
+    };
     int best = -1;
     for (int i = 0; i < (int)f.size(); i++)
         if (f[i].bytes >= bytes && f[i].bytes <= 2 * bytes + (1u << 20) &&
             (best < 0 || f[i].bytes < f[best].bytes))
             best = i;
-    if (best >= 0) {
-        void *p = f[best].p;
-        f.erase(f.begin() + best);
-        return p;
-    }
+    if (best >= 0) return take(best);
     void *p = nullptr;
     double t = mem_trace_on() ? host_ms() : 0.0;
     if (cudaMalloc(&p, bytes) == cudaSuccess) {
         mem_trace("pool cudaMalloc", bytes, mem_trace_on() ? host_ms() - t : 0.0);
+        pool_sizes()[p] = bytes;
         return p;
     }
     cudaGetLastError();
-    size_t idle = 0;
-    for (PoolBuf &b : f) {  // out of memory: give back the idle buffers and retry
-        idle += b.bytes;
-        cudaFree(b.p);
+    // out of memory: a larger idle buffer serves the request whole (memory
+    // changing hands without a driver call; a cudaFree at the memory limit
+    // waits for the whole device)
+    for (int i = 0; i < (int)f.size(); i++)
+        if (f[i].bytes >= bytes && (best < 0 || f[i].bytes < f[best].bytes)) best = i;
+    if (best >= 0) {
+        mem_trace("pool: larger idle buffer handed out", f[best].bytes, 0.0);
+        return take(best);
     }
-    f.clear();
-    arena().trim();  // and this thread's unused scratch chunks
-    const bool ok = cudaMalloc(&p, bytes) == cudaSuccess;
+    // else give back idle buffers, smallest first, until the allocation fits
+    std::sort(f.begin(), f.end(), [](const PoolBuf &a, const PoolBuf &b) { return a.bytes < b.bytes; });
+    size_t idle = 0;
+    bool ok = false;
+    while (!f.empty() && !ok) {
+        idle += f.front().bytes;
+        cudaFree(f.front().p);
+        f.erase(f.begin());
+        ok = cudaMalloc(&p, bytes) == cudaSuccess;
+        if (!ok) cudaGetLastError();
+    }
+    if (!ok) {
+        arena().trim();  // and this thread's unused scratch chunks
+        ok = cudaMalloc(&p, bytes) == cudaSuccess;
+    }
     if (mem_trace_on()) {
         mem_trace("pool: idle buffers released", idle, 0.0);
         mem_trace("pool cudaMalloc after release", bytes, host_ms() - t, ok);
     }
-    if (ok) return p;
+    if (ok) {
+        pool_sizes()[p] = bytes;
+        return p;
+    }
     cudaGetLastError();
     return nullptr;
 }
 void pool_put(void *p, size_t bytes) {
     if (!p) return;
     std::lock_guard<std::mutex> lock(pool_mutex());
+    auto it = pool_sizes().find(p);
+    if (it != pool_sizes().end()) {
+        bytes = it->second;
+        pool_sizes().erase(it);
+    }
     pool_free().push_back({p, bytes});
 }
 
 }  // namespace
+
+void *pool_take_idle(size_t min_bytes, size_t max_bytes, size_t *bytes) {
+    std::lock_guard<std::mutex> lock(pool_mutex());
+    auto &f = pool_free();
+    int best = -1;
+    for (int i = 0; i < (int)f.size(); i++)
+        if (f[i].bytes >= min_bytes && f[i].bytes <= max_bytes && (best < 0 || f[i].bytes < f[best].bytes)) best = i;
+    if (best < 0) return nullptr;
+    void *p = f[best].p;
+    *bytes = f[best].bytes;
+    f.erase(f.begin() + best);
+    return p;
+}
 
 size_t pool_idle_bytes() {
     std::lock_guard<std::mutex> lock(pool_mutex());
@@ -341,6 +417,7 @@ bool evict_const_except(const double *keep, size_t need) {
     std::vector<const double *> dropped;
     for (size_t i = 0; i < c.exp.size(); i++) {
         if (drop_e[i]) {
+            c.note(c.exp[i].src, c.exp[i].key, c.exp[i].uses);
             pool_put(c.exp[i].buf, c.exp[i].bytes);
             dropped.push_back(c.exp[i].buf);
         } else {
@@ -349,6 +426,7 @@ bool evict_const_except(const double *keep, size_t need) {
     }
     for (size_t i = 0; i < c.dig.size(); i++) {
         if (drop_d[i]) {
+            c.note(c.dig[i].src, dig_key(c.dig[i].hash), c.dig[i].uses);
             pool_put(c.dig[i].dig, c.dig[i].dbytes);
             pool_put(c.dig[i].expo, c.dig[i].ebytes);
         } else {
@@ -408,8 +486,12 @@ int slice_timed(const OzPlan *oz, bool sideA, const double *src, int8_t *dig, in
 }
 
 // digit tiles of one operand: kept for the program run when the operand is
-// constant, otherwise made in scratch (released with the caller's scope)
-int digits_of(const OzPlan *oz, bool sideA, const double *src, int8_t **dig, int **expo) {
+// constant, otherwise made in scratch (released with the caller's scope).
+// A constant operand whose tiles served a single launch in the last run
+// gets pool buffers that go back to the pool right after this launch (into
+// *release): its memory then serves the next request without a driver call.
+int digits_of(const OzPlan *oz, bool sideA, const double *src, int8_t **dig, int **expo,
+              std::vector<void *> *release) {
     const uint64_t h = sideA ? oz->ahash : oz->bhash;
     const i64 bytes = sideA ? oz->adig : oz->bdig, ne = sideA ? oz->nea : oz->neb;
     if (is_const_operand(src)) {
@@ -417,11 +499,28 @@ int digits_of(const OzPlan *oz, bool sideA, const double *src, int8_t **dig, int
         for (DigEntry &e : c.dig)
             if (e.src == src && e.hash == h) {
                 e.used = c.epoch;
+                e.uses++;
                 *dig = e.dig;
                 *expo = e.expo;
                 return CPSD_OK;
             }
         const size_t db = (size_t)std::max<i64>(bytes, 16), eb = sizeof(int) * (size_t)std::max<i64>(ne, 1);
+        if (single_use_last_run(src, dig_key(h))) {
+            c.bump(src, dig_key(h));
+            int8_t *d = (int8_t *)pool_get(db);
+            int *x = d ? (int *)pool_get(eb) : nullptr;
+            if (d && x) {
+                release->push_back(d);
+                release->push_back(x);
+                *dig = d;
+                *expo = x;
+                return slice_timed(oz, sideA, src, d, x);
+            }
+            pool_put(d, db);
+            CPSD_TRY(scratch(bytes, dig));
+            CPSD_TRY(scratch(ne, expo));
+            return slice_timed(oz, sideA, src, *dig, *expo);
+        }
         int8_t *d = (int8_t *)pool_get(db);
         int *x = d ? (int *)pool_get(eb) : nullptr;
         if (!(d && x)) {
@@ -433,7 +532,7 @@ int digits_of(const OzPlan *oz, bool sideA, const double *src, int8_t **dig, int
             }
         }
         if (d && x) {
-            c.dig.push_back({src, h, d, x, db, eb, c.epoch});
+            c.dig.push_back({src, h, d, x, db, eb, c.epoch, 1});
             *dig = d;
             *expo = x;
             return slice_timed(oz, sideA, src, d, x);
@@ -451,8 +550,17 @@ int launch_ozaki(const OzPlan *oz, const double *A, const double *B, double *C, 
     int8_t *ad, *bd;
     int *ea, *eb, *err;
     CPSD_TRY(oz_error_word(&err));
-    CPSD_TRY(digits_of(oz, true, A, &ad, &ea));
-    CPSD_TRY(digits_of(oz, false, B, &bd, &eb));
+    std::vector<void *> release;
+    struct Release {  // after the launch's kernels are done
+        std::vector<void *> &r;
+        ~Release() {
+            if (r.empty()) return;
+            cudaStreamSynchronize(stream());
+            for (void *p : r) pool_put(p, 0);
+        }
+    } rel{release};
+    CPSD_TRY(digits_of(oz, true, A, &ad, &ea, &release));
+    CPSD_TRY(digits_of(oz, false, B, &bd, &eb, &release));
     cudaEvent_t end;
     // record: groups, bytes of the digit tiles the launch streams, bytes of
     // C read and written (once per K chunk)
@@ -476,12 +584,17 @@ int expand_cached(const Ten &v, bool e0, bool e1, Ten *out, bool *done) {
     for (ExpEntry &e : c.exp)
         if (e.src == v.arr && e.key == key) {
             e.used = c.epoch;
+            e.uses++;
             *out = v;
             out->d = e.d;
             out->arr = e.buf;
             *done = true;
             return CPSD_OK;
         }
+    if (single_use_last_run(v.arr, key)) {  // expand into scratch as usual
+        c.bump(v.arr, key);
+        return CPSD_OK;
+    }
     const PairMapPlan *pm;
     Desc d;
     CPSD_TRY(plan_pairmap(v.d, e0 ? PAIR_EXPAND : PAIR_ID, e1 ? PAIR_EXPAND : PAIR_ID, 1, 1, &d, &pm));
@@ -489,7 +602,7 @@ int expand_cached(const Ten &v, bool e0, bool e1, Ten *out, bool *done) {
     double *buf = (double *)pool_get(bytes);
     if (!buf && evict_const_except(v.arr, bytes)) buf = (double *)pool_get(bytes);
     if (!buf) return CPSD_OK;  // no room to keep it: expand into scratch as usual
-    c.exp.push_back({v.arr, key, d, buf, bytes, c.epoch});
+    c.exp.push_back({v.arr, key, d, buf, bytes, c.epoch, 1});
     c.arrs.push_back(buf);  // derived from a constant operand: constant too
     CPSD_TRY(launch_pairmap(pm, v.arr, buf, 1.0, 0.0, 1, 0, d.len()));
     *out = v;
@@ -549,11 +662,20 @@ ConstOperands::~ConstOperands() {
     // the buffers go back to the pool once the kernels that read them are
     // done (the next user may run on another stream)
     if (!c.exp.empty() || !c.dig.empty()) cudaStreamSynchronize(stream());
-    for (ExpEntry &e : c.exp) pool_put(e.buf, e.bytes);
+    for (ExpEntry &e : c.exp) {
+        c.note(e.src, e.key, e.uses);
+        pool_put(e.buf, e.bytes);
+    }
     for (DigEntry &e : c.dig) {
+        c.note(e.src, dig_key(e.hash), e.uses);
         pool_put(e.dig, e.dbytes);
         pool_put(e.expo, e.ebytes);
     }
+    {
+        std::lock_guard<std::mutex> lock(uses_mutex());
+        for (const auto &u : c.uses) uses_last_run()[u.first] = u.second;
+    }
+    c.uses.clear();
     c.exp.clear();
     c.dig.clear();
     c.arrs.clear();

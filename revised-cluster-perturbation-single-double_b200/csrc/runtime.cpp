@@ -179,8 +179,19 @@ int Arena::alloc(size_t bytes, void **out) {
         sz = bytes;
         if (cudaMalloc(&p, sz) != cudaSuccess) {
             cudaGetLastError();
-            pool_release_idle();  // idle cached copies of earlier runs give way to scratch
-            if (cudaMalloc(&p, sz) != cudaSuccess) {
+            // an idle pool buffer of up to twice the size (plus 1 GiB)
+            // becomes the chunk (no driver call: at the memory limit a
+            // cudaFree would wait for the whole device), else the idle cached
+            // copies of earlier runs give way
+            size_t got = 0;
+            p = pool_take_idle(sz, 2 * sz + ((size_t)1 << 30), &got);
+            if (p) {
+                sz = got;
+                mem_trace("arena chunk from an idle pool buffer", sz, 0.0);
+            } else {
+                pool_release_idle();
+            }
+            if (!p && cudaMalloc(&p, sz) != cudaSuccess) {
                 cudaGetLastError();
                 // then the copies this run keeps for later operations
                 if (!evict_cached_copies(sz) || cudaMalloc(&p, sz) != cudaSuccess) {

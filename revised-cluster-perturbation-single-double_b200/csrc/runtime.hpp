@@ -127,6 +127,10 @@ void pool_release_idle();
 // progress was not handed (false: nothing to free)
 bool evict_cached_copies(size_t need = 0);  // least recently used first until `need` bytes are free (0: all)
 size_t pool_idle_bytes();
+// takes the smallest idle pool buffer of min_bytes .. max_bytes out of the
+// pool (its size in *bytes; nullptr if none): device memory that changes
+// hands without a cudaFree / cudaMalloc
+void *pool_take_idle(size_t min_bytes, size_t max_bytes, size_t *bytes);
 struct ScratchScope {
     Arena::Mark m;
     ScratchScope() : m(arena().mark()) {}
