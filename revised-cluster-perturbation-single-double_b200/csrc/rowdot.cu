@@ -80,8 +80,9 @@ struct RdCfg {
     static constexpr int SMEM = RW * NS * SLOT * (int)sizeof(double);
 };
 
-// KQ = K / 32 rounded up (1..4); NC = columns per item rounded up to 2, 4
-// or 8; SWAP: rows over the N side
+// KQ = K / 32 rounded up (1..4); NC = columns per item rounded up to 2, 4,
+// 5, 6 or 8 (RB x NC <= 32 outputs per batch: 5 and 6 columns take 6 and 5
+// rows a batch instead of 4); SWAP: rows over the N side
 template <int KQ, int NC, bool SWAP>
 __global__ void __launch_bounds__(RW * 32) k_rowdot(const TaskDev *__restrict__ tasks, const SegDev *__restrict__ segs,
                                                     const RowDotItem *__restrict__ items, int nitems,
@@ -166,6 +167,8 @@ __global__ void __launch_bounds__(RW * 32) k_rowdot(const TaskDev *__restrict__ 
         const double *buf = ring + (size_t)(b % RD_NS) * Cf::SLOT + lane;
         double acc[32];
 #pragma unroll
+        for (int j = RB * NC; j < 32; j++) acc[j] = 0.0;  // lanes past the batch's outputs
+#pragma unroll
         for (int i = 0; i < RB; i++) {
             double x[KQ];
 #pragma unroll
@@ -246,7 +249,7 @@ int plan_rowdot(const ContractPlan *cp, const RowDotPlan **out) {
         p.swap = swap;
         p.kq = (int)((maxK + 31) / 32);
         const i64 cmax = std::min<i64>(8, swap ? maxM : maxN);
-        p.nc = cmax <= 2 ? 2 : cmax <= 4 ? 4 : 8;
+        p.nc = cmax <= 2 ? 2 : cmax <= 4 ? 4 : cmax <= 5 ? 5 : cmax <= 6 ? 6 : 8;
         // own copies of the tables with each task's row units reordered by
         // ascending stride in the row operand: consecutive rows are then
         // neighbours in memory (the same (row, column) -> (X, C) pairs, in
@@ -322,6 +325,8 @@ int launch_rowdot(const ContractPlan *cp, const RowDotPlan *rp, const double *A,
     switch (rp->nc) {                                                                                                \
     case 2: CPSD_ROWDOT(KQ, 2) break;                                                                                \
     case 4: CPSD_ROWDOT(KQ, 4) break;                                                                                \
+    case 5: CPSD_ROWDOT(KQ, 5) break;                                                                                \
+    case 6: CPSD_ROWDOT(KQ, 6) break;                                                                                \
     default: CPSD_ROWDOT(KQ, 8) break;                                                                               \
     }
     switch (rp->kq) {
