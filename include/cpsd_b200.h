@@ -309,9 +309,10 @@ int cpsd_debug_contract_plan(const cpsd_opt *v1, const char *t1, const cpsd_opt 
  * useful flops and (tasks, segments, tiles, tile shape) */
 int cpsd_contract_records(double *ms, double *flops, int64_t *shape, int64_t maxrec, int64_t *nrec);
 /* work items of the narrow-output kernels for a contraction (layouts
- * NarrowItem / NarrowRed of csrc/narrow.cuh); flags = {narrow, rows over
- * the second operand, lanes over K, partial slots}; items = NULL when the
- * contraction runs on the tensor-core tiles instead */
+ * NarrowItem / NarrowRed of csrc/narrow.cuh); flags[5] = {narrow, rows over
+ * the second operand, lanes over K, partial slots, columns per long-K item
+ * (its rows: 32 / columns)}; items = NULL when the contraction runs on the
+ * tensor-core tiles instead */
 int cpsd_debug_narrow_plan(const cpsd_opt *v1, const char *t1, const cpsd_opt *v2, const char *t2,
                            const cpsd_opt *v3, const char *t3, int64_t nb, int64_t sA, int64_t sB, int64_t sC,
                            const void **items, int64_t *nitems, const void **reds, int64_t *nreds, int64_t *flags);

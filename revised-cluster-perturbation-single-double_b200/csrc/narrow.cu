@@ -171,17 +171,19 @@ __device__ __forceinline__ void nk_wait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-// long K: warp = 4 rows x 8 columns over the K range of the item.  Lane l
-// takes the indices k = kb + l + 32 s of each segment; the 4 + 8 operand
-// values of step s are copied by cp.async into the lane's own slots of a
-// per-warp ring of NK_NS steps, NK_NS - 1 steps ahead of the FMAs, so the
-// loads in flight hold no registers (the lane reads back only what it
-// copied itself: the group wait is the only synchronisation).  Per lane the
-// sums run over its indices in order, then the fixed transpose reduction.
+// long K: warp = KR rows x KC columns (KR x KC <= 32: 8 x 4, 6 x 5, 5 x 6 or
+// 4 x 8, the plan's choice by the column count) over the K range of the
+// item.  Lane l takes the indices k = kb + l + 32 s of each segment; the
+// KR + KC operand values of step s are copied by cp.async into the lane's
+// own slots of a per-warp ring of NK_NS steps, NK_NS - 1 steps ahead of the
+// FMAs, so the loads in flight hold no registers (the lane reads back only
+// what it copied itself: the group wait is the only synchronisation).  Per
+// lane the sums run over its indices in order, then the fixed transpose
+// reduction leaves output (row l / KC, column l % KC) in lane l.
 constexpr int NK_NS = 4;                                   // ring depth (steps)
-constexpr int NK_VALS = NARROW_ROWS + NARROW_COLS;         // values per lane and step
+constexpr int NK_VALS = 12;                                // slots per lane and step (KR + KC <= 12)
 constexpr int NK_SMEM = NW * NK_NS * NK_VALS * 32 * 8;     // dynamic shared memory per CTA
-template <bool SWAP>
+template <bool SWAP, int KC>
 __global__ void __launch_bounds__(NW * 32) k_narrow_k(const TaskDev *__restrict__ tasks,
                                                       const SegDev *__restrict__ segs,
                                                       const NarrowItem *__restrict__ items, int nitems,
@@ -196,8 +198,10 @@ __global__ void __launch_bounds__(NW * 32) k_narrow_k(const TaskDev *__restrict_
     const TaskDev &tk = tasks[item.task];
     const View<SWAP> v(tk);
     const double *X = SWAP ? B : A, *Y = SWAP ? A : B;
-    const int nrow = (int)min((i64)NARROW_ROWS, v.R() - item.r0);
-    const int ncol = (int)min((i64)NARROW_COLS, v.CN() - item.c0);
+    constexpr int KR = 32 / KC;
+    static_assert(KR + KC <= NK_VALS, "ring slots");
+    const int nrow = (int)min((i64)KR, v.R() - item.r0);
+    const int ncol = (int)min((i64)KC, v.CN() - item.c0);
     // slot (step, value) of this lane at ring[(step * NK_VALS + value) * 32 + lane]
     double *ring = ring_all + (size_t)warp * NK_NS * NK_VALS * 32 + lane;
     double acc[32];
@@ -209,11 +213,11 @@ __global__ void __launch_bounds__(NW * 32) k_narrow_k(const TaskDev *__restrict_
         if (kb < 0) kb = 0;
         if (ke > sg.K) ke = sg.K;
         if (kb >= ke) continue;
-        i64 ox[NARROW_ROWS], oy[NARROW_COLS];
+        i64 ox[KR], oy[KC];
 #pragma unroll
-        for (int i = 0; i < NARROW_ROWS; i++) ox[i] = i < nrow ? v.xrow(sg, item.r0 + i) : 0;
+        for (int i = 0; i < KR; i++) ox[i] = i < nrow ? v.xrow(sg, item.r0 + i) : 0;
 #pragma unroll
-        for (int c = 0; c < NARROW_COLS; c++) oy[c] = c < ncol ? v.ycol(sg, item.c0 + c) : 0;
+        for (int c = 0; c < KC; c++) oy[c] = c < ncol ? v.ycol(sg, item.c0 + c) : 0;
         const i64 *kx = v.kx(sg), *ky = v.ky(sg);
         const i64 nsteps = (ke - kb + 31) / 32;
         auto issue = [&](i64 st) {
@@ -224,18 +228,18 @@ __global__ void __launch_bounds__(NW * 32) k_narrow_k(const TaskDev *__restrict_
                     i64 fx, fy;
                     kdecode(k, sg, kx, ky, &fx, &fy);
 #pragma unroll
-                    for (int i = 0; i < NARROW_ROWS; i++) {
+                    for (int i = 0; i < KR; i++) {
                         if (i < nrow) nk_cp8(d + i * 32, X + ox[i] + fx);
                         else d[i * 32] = 0.0;
                     }
 #pragma unroll
-                    for (int c = 0; c < NARROW_COLS; c++) {
-                        if (c < ncol) nk_cp8(d + (NARROW_ROWS + c) * 32, Y + oy[c] + fy);
-                        else d[(NARROW_ROWS + c) * 32] = 0.0;
+                    for (int c = 0; c < KC; c++) {
+                        if (c < ncol) nk_cp8(d + (KR + c) * 32, Y + oy[c] + fy);
+                        else d[(KR + c) * 32] = 0.0;
                     }
                 } else {
 #pragma unroll
-                    for (int j = 0; j < NK_VALS; j++) d[j * 32] = 0.0;
+                    for (int j = 0; j < KR + KC; j++) d[j * 32] = 0.0;
                 }
             }
             nk_commit();  // an empty group past the end keeps the count
@@ -246,15 +250,15 @@ __global__ void __launch_bounds__(NW * 32) k_narrow_k(const TaskDev *__restrict_
             issue(st + NK_NS - 1);  // into the slot step st - 1 used
             nk_wait<NK_NS - 1>();
             const double *d = ring + (size_t)(st % NK_NS) * NK_VALS * 32;
-            double x[NARROW_ROWS], y[NARROW_COLS];
+            double x[KR], y[KC];
 #pragma unroll
-            for (int i = 0; i < NARROW_ROWS; i++) x[i] = d[i * 32];
+            for (int i = 0; i < KR; i++) x[i] = d[i * 32];
 #pragma unroll
-            for (int c = 0; c < NARROW_COLS; c++) y[c] = d[(NARROW_ROWS + c) * 32];
+            for (int c = 0; c < KC; c++) y[c] = d[(KR + c) * 32];
 #pragma unroll
-            for (int i = 0; i < NARROW_ROWS; i++)
+            for (int i = 0; i < KR; i++)
 #pragma unroll
-                for (int c = 0; c < NARROW_COLS; c++) acc[i * NARROW_COLS + c] = fma(x[i], y[c], acc[i * NARROW_COLS + c]);
+                for (int c = 0; c < KC; c++) acc[i * KC + c] = fma(x[i], y[c], acc[i * KC + c]);
         }
         nk_wait<0>();
     }
@@ -263,12 +267,12 @@ __global__ void __launch_bounds__(NW * 32) k_narrow_k(const TaskDev *__restrict_
         partial[item.part * 32 + lane] = s;
         return;
     }
-    const int i = lane / NARROW_COLS, c = lane % NARROW_COLS;
+    const int i = lane / KC, c = lane % KC;
     if (i < nrow && c < ncol) C[tk.baseC + v.crow(item.r0 + i) + v.ccol(item.c0 + c)] += alpha * s;
 }
 
 // split items of one output block, summed in K order
-template <bool SWAP>
+template <bool SWAP, int KC>
 __global__ void __launch_bounds__(NW * 32) k_narrow_reduce(const TaskDev *__restrict__ tasks,
                                                            const NarrowRed *__restrict__ reds, int nreds,
                                                            const double *__restrict__ partial,
@@ -281,8 +285,9 @@ __global__ void __launch_bounds__(NW * 32) k_narrow_reduce(const TaskDev *__rest
     const View<SWAP> v(tk);
     double s = 0.0;
     for (int q = 0; q < rd.nparts; q++) s += partial[(rd.part0 + q) * 32 + lane];
-    const int i = lane / NARROW_COLS, c = lane % NARROW_COLS;
-    if (rd.r0 + i < v.R() && rd.c0 + c < v.CN())
+    // lanes past the KR x KC outputs (KC = 5, 6) hold nothing and write nothing
+    const int i = lane / KC, c = lane % KC;
+    if (i < 32 / KC && rd.r0 + i < v.R() && rd.c0 + c < v.CN())
         C[tk.baseC + v.crow(rd.r0 + i) + v.ccol(rd.c0 + c)] += alpha * s;
 }
 
@@ -350,9 +355,14 @@ int plan_narrow(const ContractPlan *cp, const NarrowPlan **out) {
                     for (i64 r0 = 0; r0 < R(t); r0 += 32) p.items.push_back(NarrowItem{ti, (int)c0, r0, 0, t.Ktot, -1});
             }
         } else {
+            // item shape by the column count: 8 x 4, 6 x 5, 5 x 6 or 4 x 8
+            // rows x columns, so that few of a warp's 32 sums go unused
+            i64 cmax = 0;
+            for (const TaskDev &t : cp->h_tasks) cmax = std::max(cmax, CN(t));
+            p.kc = cmax <= 4 ? 4 : cmax == 5 ? 5 : cmax == 6 ? 6 : 8;
+            const int KC = p.kc, KR = 32 / p.kc;
             i64 base = 0;
-            for (const TaskDev &t : cp->h_tasks)
-                base += ((R(t) + NARROW_ROWS - 1) / NARROW_ROWS) * ((CN(t) + NARROW_COLS - 1) / NARROW_COLS);
+            for (const TaskDev &t : cp->h_tasks) base += ((R(t) + KR - 1) / KR) * ((CN(t) + KC - 1) / KC);
             // K parts: about 8192 warp items (measured: 3552 and 16384 are
             // slower or no faster on d2h_nmo400)
             const i64 want = std::max<i64>(1, (8192 + base - 1) / base);
@@ -362,15 +372,15 @@ int plan_narrow(const ContractPlan *cp, const NarrowPlan **out) {
                 // the row groups of one K part are neighbours in the item
                 // list, so the warps running together read the same stretch
                 // of the column operand (it stays in L2 across the row groups)
-                for (i64 c0 = 0; c0 < CN(t); c0 += NARROW_COLS) {
+                for (i64 c0 = 0; c0 < CN(t); c0 += KC) {
                     const i64 part0 = p.nparts;
                     if (ns > 1)
-                        for (i64 r0 = 0; r0 < R(t); r0 += NARROW_ROWS) {
+                        for (i64 r0 = 0; r0 < R(t); r0 += KR) {
                             p.reds.push_back(NarrowRed{ti, (int)c0, (int)ns, 0, r0, p.nparts});
                             p.nparts += ns;
                         }
                     for (i64 q = 0; q < ns; q++)
-                        for (i64 r0 = 0, ri = 0; r0 < R(t); r0 += NARROW_ROWS, ri++)
+                        for (i64 r0 = 0, ri = 0; r0 < R(t); r0 += KR, ri++)
                             p.items.push_back(NarrowItem{ti, (int)c0, r0, t.Ktot * q / ns, t.Ktot * (q + 1) / ns,
                                                          ns > 1 ? part0 + ri * ns + q : -1});
                 }
@@ -381,6 +391,46 @@ int plan_narrow(const ContractPlan *cp, const NarrowPlan **out) {
     cache[cp] = std::move(P);
     return CPSD_OK;
 }
+
+namespace {
+template <bool SWAP, int KC>
+int narrow_k_launch(int grid, int ni, int nr, const ContractPlan *cp, const NarrowPlan *np, const double *A,
+                    const double *B, double *C, double alpha, double *part) {
+    static std::atomic<bool> attr{false};
+    if (!attr.load(std::memory_order_acquire)) {
+        CPSD_TRY(cuda_check(cudaFuncSetAttribute(k_narrow_k<SWAP, KC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 NK_SMEM),
+                            "narrow smem attr"));
+        attr.store(true, std::memory_order_release);
+    }
+    k_narrow_k<SWAP, KC><<<grid, NW * 32, NK_SMEM, stream()>>>(cp->d_tasks, cp->d_segs, np->d_items, ni, A, B, C,
+                                                               alpha, part);
+    count_launch();
+    if (nr > 0) {
+        const int rg = (nr + NW - 1) / NW;
+        k_narrow_reduce<SWAP, KC><<<rg, NW * 32, 0, stream()>>>(cp->d_tasks, np->d_reds, nr, part, C, alpha);
+        count_launch();
+    }
+    return CPSD_OK;
+}
+
+template <bool SWAP>
+int narrow_k_kc(const NarrowPlan *np, int grid, int ni, int nr, const ContractPlan *cp, const double *A,
+                const double *B, double *C, double alpha, double *part) {
+    switch (np->kc) {
+    case 4: return narrow_k_launch<SWAP, 4>(grid, ni, nr, cp, np, A, B, C, alpha, part);
+    case 5: return narrow_k_launch<SWAP, 5>(grid, ni, nr, cp, np, A, B, C, alpha, part);
+    case 6: return narrow_k_launch<SWAP, 6>(grid, ni, nr, cp, np, A, B, C, alpha, part);
+    default: return narrow_k_launch<SWAP, 8>(grid, ni, nr, cp, np, A, B, C, alpha, part);
+    }
+}
+
+int narrow_k_go(const NarrowPlan *np, int grid, int ni, int nr, const ContractPlan *cp, const double *A,
+                const double *B, double *C, double alpha, double *part) {
+    return np->swap ? narrow_k_kc<true>(np, grid, ni, nr, cp, A, B, C, alpha, part)
+                    : narrow_k_kc<false>(np, grid, ni, nr, cp, A, B, C, alpha, part);
+}
+}  // namespace
 
 int launch_narrow(const ContractPlan *cp, const NarrowPlan *np, const double *A, const double *B, double *C,
                   double alpha) {
@@ -401,31 +451,7 @@ int launch_narrow(const ContractPlan *cp, const NarrowPlan *np, const double *A,
         ScratchScope sc;
         double *part = nullptr;
         if (np->nparts > 0) CPSD_TRY(scratch(np->nparts * 32, &part));
-        static std::atomic<bool> attr{false};
-        if (!attr.load(std::memory_order_acquire)) {
-            CPSD_TRY(cuda_check(cudaFuncSetAttribute(k_narrow_k<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                     NK_SMEM),
-                                "narrow smem attr"));
-            CPSD_TRY(cuda_check(cudaFuncSetAttribute(k_narrow_k<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                     NK_SMEM),
-                                "narrow smem attr"));
-            attr.store(true, std::memory_order_release);
-        }
-        if (np->swap)
-            k_narrow_k<true><<<grid, NW * 32, NK_SMEM, stream()>>>(cp->d_tasks, cp->d_segs, np->d_items, ni, A, B, C,
-                                                                   alpha, part);
-        else
-            k_narrow_k<false><<<grid, NW * 32, NK_SMEM, stream()>>>(cp->d_tasks, cp->d_segs, np->d_items, ni, A, B, C,
-                                                                    alpha, part);
-        count_launch();
-        if (nr > 0) {
-            const int rg = (nr + NW - 1) / NW;
-            if (np->swap)
-                k_narrow_reduce<true><<<rg, NW * 32, 0, stream()>>>(cp->d_tasks, np->d_reds, nr, part, C, alpha);
-            else
-                k_narrow_reduce<false><<<rg, NW * 32, 0, stream()>>>(cp->d_tasks, np->d_reds, nr, part, C, alpha);
-            count_launch();
-        }
+        CPSD_TRY(narrow_k_go(np, grid, ni, nr, cp, A, B, C, alpha, part));
     }
     CPSD_TRY(cuda_check(cudaGetLastError(), "k_narrow"));
     return timing_end(end);

@@ -8,8 +8,8 @@
 
 namespace cpsd {
 
-constexpr int NARROW_COLS = 8;  // output columns per work item
-constexpr int NARROW_ROWS = 4;  // rows per warp in the long-K kernel
+constexpr int NARROW_COLS = 8;  // output columns per work item (short K; at most, long K)
+constexpr int NARROW_ROWS = 4;  // rows per warp in the long-K kernel at 8 columns
 
 // one warp's work: rows [r0, r0 + rows) of a task, columns [c0, c0 + 8),
 // contracted range [k0, k1) of the task's concatenated K; partial slot when
@@ -27,6 +27,7 @@ struct NarrowRed {  // split items of one (task, r0, c0), in K order
 struct NarrowPlan {
     bool swap = false;   // rows run over the N side (the second operand)
     bool longk = false;  // lanes over K (warp reductions) instead of over rows
+    int kc = NARROW_COLS;  // long K: columns per item (4, 5, 6 or 8), rows 32 / kc
     std::vector<NarrowItem> items;
     std::vector<NarrowRed> reds;
     i64 nparts = 0;

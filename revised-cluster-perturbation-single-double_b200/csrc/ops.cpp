@@ -1547,6 +1547,7 @@ int cpsd_debug_narrow_plan(const cpsd_opt *v1, const char *t1, const cpsd_opt *v
     flags[1] = np && np->swap ? 1 : 0;
     flags[2] = np && np->longk ? 1 : 0;
     flags[3] = np ? np->nparts : 0;
+    flags[4] = np ? np->kc : 0;
     return CPSD_OK;
 }
 

@@ -18,7 +18,7 @@ import oracle_ffi as of
 from cpsd_b200 import api, synth
 from test_plan_emulation import KSPEC, to_engine, norm, I64, get_plan, decode
 
-COLS, ROWS = 8, 4
+COLS = 8  # short-K items: 32 rows x 8 columns
 
 
 class NarrowItem(ctypes.Structure):
@@ -32,7 +32,7 @@ class NarrowRed(ctypes.Structure):
 
 def get_narrow(o1, t1, o2, t2, o3, t3, nb, sA, sB, sC):
     it, ni, rd, nr = ctypes.c_void_p(), I64(), ctypes.c_void_p(), I64()
-    flags = (I64 * 4)()
+    flags = (I64 * 5)()
     api.check(api.lib().cpsd_debug_narrow_plan(ctypes.byref(o1), t1.encode(), ctypes.byref(o2), t2.encode(),
                                                ctypes.byref(o3), t3.encode(), I64(nb), I64(sA), I64(sB), I64(sC),
                                                ctypes.byref(it), ctypes.byref(ni), ctypes.byref(rd), ctypes.byref(nr),
@@ -41,14 +41,18 @@ def get_narrow(o1, t1, o2, t2, o3, t3, nb, sA, sB, sC):
         return None
     items = list((NarrowItem * ni.value).from_address(it.value)) if ni.value else []
     reds = list((NarrowRed * nr.value).from_address(rd.value)) if nr.value else []
-    return dict(items=items, reds=reds, swap=bool(flags[1]), longk=bool(flags[2]), nparts=flags[3])
+    return dict(items=items, reds=reds, swap=bool(flags[1]), longk=bool(flags[2]), nparts=flags[3], kc=int(flags[4]))
 
 
 def emulate(tasks, segs, plan, A, B, C, alpha):
     C = C.copy()
     swap = plan["swap"]
     X, Y = (B, A) if swap else (A, B)
-    partial = np.full((plan["nparts"], ROWS, COLS), np.nan)
+    # long K: items of 32 / kc rows x kc columns; short K: 32 rows x 8 columns
+    kc = plan.get("kc", COLS) if plan["longk"] else COLS
+    assert kc in (4, 5, 6, 8)
+    krows = 32 // kc
+    partial = np.full((plan["nparts"], krows, kc), np.nan)
     written = set()
 
     def views(tk):
@@ -97,8 +101,8 @@ def emulate(tasks, segs, plan, A, B, C, alpha):
     for it in plan["items"]:
         tk = tasks[it.task]
         R, CN, _, _ = views(tk)
-        nrow = min(ROWS if plan["longk"] else 32, R - it.r0)
-        ncol = min(COLS, CN - it.c0)
+        nrow = min(krows if plan["longk"] else 32, R - it.r0)
+        ncol = min(kc, CN - it.c0)
         assert nrow > 0 and ncol > 0 and 0 <= it.k0 <= it.k1 <= tk.Ktot
         val = block(tk, it.r0, nrow, it.c0, ncol, it.k0, it.k1)
         if it.part >= 0:
@@ -111,7 +115,7 @@ def emulate(tasks, segs, plan, A, B, C, alpha):
     for rd in plan["reds"]:
         tk = tasks[rd.task]
         R, CN, _, _ = views(tk)
-        nrow, ncol = min(ROWS, R - rd.r0), min(COLS, CN - rd.c0)
+        nrow, ncol = min(krows, R - rd.r0), min(kc, CN - rd.c0)
         parts = [it for it in plan["items"] if it.part >= rd.part0 and it.part < rd.part0 + rd.nparts]
         assert len(parts) == rd.nparts and all(p.task == rd.task and p.r0 == rd.r0 and p.c0 == rd.c0 for p in parts)
         ranges = sorted((p.k0, p.k1) for p in parts)
