@@ -175,11 +175,11 @@ struct DigEntry {
     int uses;
 };
 // Uses per run of each copy (source array and layout / digit plan): a copy
-// that served one operation in the last run is not kept in the next one,
-// where it would only hold memory that later work then has to take back
-// (at the memory limit that cost a cudaMalloc / cudaFree of gigabytes and
-// a rebuild every run).  Counted per host thread over one run, merged into
-// the process-wide record when the run ends.
+// that served one operation in the last run is not kept for the next run
+// (expanded copies go to scratch, digit tiles to pool buffers returned
+// right after their launch), where it would only hold memory that later
+// work then has to take back.  Counted per host thread over one run, merged
+// into the process-wide record when the run ends.
 using UseKey = std::pair<const void *, std::string>;
 std::map<UseKey, int> &uses_last_run() {
     static std::map<UseKey, int> m;
@@ -228,8 +228,9 @@ struct PoolBuf {
     size_t bytes;
 };
 // The pool is shared by all host threads (concurrent molecules of a batch):
-// an idle buffer may serve any of them, and a thread short of memory gives
-// back every idle buffer.
+// an idle buffer may serve any of them.  When the driver has no room, a
+// larger idle buffer serves a request whole, and only then are idle buffers
+// given back (smallest first) until the allocation fits.
 std::vector<PoolBuf> &pool_free() {
     static std::vector<PoolBuf> v;
     return v;
