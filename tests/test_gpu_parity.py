@@ -96,12 +96,14 @@ def test_kernel_matches_oracle(name, nirrep):
 
 @pytest.mark.parametrize("nocc", [(3, 2), (4, 2)])
 @pytest.mark.parametrize("nirrep", [1, 4, 8])
-@pytest.mark.parametrize("name,kind", [("Wmbej_r1abci", 23), ("Wmbej_r1ijka", 22), ("c2_r2Fae", 22)])
+@pytest.mark.parametrize("name,kind", [("Wmbej_r1abci", 23), ("Wmbej_r1ijka", 22), ("c2_r2Fae", 22),
+                                       ("c1_r2abci", 21)])
 def test_streaming_kernels_ran_and_match_oracle(name, kind, nirrep, nocc):
-    """The row-dot (kind 23) and short-K (kind 22) kernels are the ones that
-    ran for these shapes (their timing records), and they match the oracle
-    (at nirrep 1 the row-dot's output has 5 or 6 columns: its 5- and
-    6-column instances)."""
+    """The row-dot (kind 23), short-K (kind 22) and long-K narrow (kind 21)
+    kernels are the ones that ran for these shapes (their timing records),
+    and they match the oracle (at nirrep 1 the row-dot's and the long-K
+    kernel's outputs have 5 or 6 columns: their 5- and 6-column item
+    shapes)."""
     rng = np.random.default_rng(17 + nirrep)
     s = synth.System(nmo=16 if nirrep < 8 else 24, nocc_a=nocc[0], nocc_b=nocc[1], nirrep=nirrep, seed=2)
     api.init(s.nirrep, s.dirprd)
