@@ -406,8 +406,9 @@ def test_full_size_d2h_nmo200_properties():
         a, b = host(ob[key]), host(ou[key])
         np.testing.assert_allclose(a, b, rtol=0, atol=1e-12 * max(1.0, np.abs(a).max()))
     # R1^(2) is DIIS-converged (diis_max_err): rounding-level differences in
-    # its right-hand side move it within that tolerance, as against the oracle
-    np.testing.assert_allclose(host(ob["R1_2"]), host(ou["R1_2"]), rtol=0, atol=1e-6)
+    # its right-hand side move it within that tolerance, relative to its size
+    a, b = host(ob["R1_2"]), host(ou["R1_2"])
+    np.testing.assert_allclose(a, b, rtol=0, atol=1e-6 * max(1.0, np.abs(a).max()))
     R12 = host(ob["R1_2"]).reshape(len(om), l1)
     for k in range(len(om)):
         assert abs(np.dot(host(Rg[k]), R12[k])) < 1e-10
